@@ -1,0 +1,13 @@
+"""emergence_b200: B200-native (sm_100a) compressible-Euler step.
+
+Drop-in for the explicit finite-volume step of the emergence workspace's
+``compressible`` crate (WCNS WENO5-Z reconstruction, HLLC, positivity
+limiter, SSP-RK3, ghost fill, CFL reduction), behind the C ABI of
+``include/emergence_b200.h``.
+"""
+from .physics import Bc, Euler, FluxMode, Mesh, Nasg, Precision, initial_state
+from .solver import GpuSolver, device_count
+from ._abi import EmgError, LIB_PATH
+
+__all__ = ["Bc", "Euler", "FluxMode", "Mesh", "Nasg", "Precision", "initial_state", "GpuSolver", "device_count",
+           "EmgError", "LIB_PATH"]

@@ -1,0 +1,105 @@
+"""ctypes declarations of the C ABI in include/emergence_b200.h.
+
+The library is the in-tree ``libemergence_b200.so`` built by
+``emergence_b200/build.py``. There is no fallback: if the library is missing,
+every solver call raises ``RuntimeError``.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libemergence_b200.so")
+
+EMG_OK = 0
+STATUS_NAMES = {
+    1: "EMG_ERR_INVALID",
+    2: "EMG_ERR_CUDA",
+    3: "EMG_ERR_DT_COLLAPSED",
+    4: "EMG_ERR_INADMISSIBLE",
+    5: "EMG_ERR_UNFILLABLE",
+    6: "EMG_ERR_BOUNDS",
+    7: "EMG_ERR_NO_DEVICE",
+    8: "EMG_ERR_TIMEOUT",
+}
+
+
+class EmgEos(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("p_inf", C.c_double), ("b", C.c_double), ("q", C.c_double), ("cv", C.c_double)]
+
+
+class EmgMesh(C.Structure):
+    _fields_ = [("n", C.c_int64 * 3), ("lo", C.c_double * 3), ("dx", C.c_double * 3), ("ng", C.c_int64)]
+
+
+class EmgBc(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("state", C.c_double * 5)]
+
+
+class EmgOpts(C.Structure):
+    _fields_ = [("cfl", C.c_double), ("tol", C.c_double), ("mode", C.c_int32), ("positivity", C.c_int32),
+                ("precision", C.c_int32), ("reserved", C.c_int32)]
+
+
+EMG_K_COUNT = 5
+KERNEL_KINDS = ("ghost", "axis0", "axis1", "axis2", "cfl")
+
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_U64 = C.POINTER(C.c_uint64)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "emg_last_error": (C.c_char_p, []),
+    "emg_version": (C.c_char_p, []),
+    "emg_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+    "emg_uniform_create": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc), C.POINTER(EmgOpts),
+                                     _D, C.c_size_t, C.POINTER(_P)]),
+    "emg_uniform_destroy": (C.c_int, [_P]),
+    "emg_uniform_step": (C.c_int, [_P, C.c_double]),
+    "emg_uniform_dt_cfl": (C.c_int, [_P, _D]),
+    "emg_uniform_run_to": (C.c_int, [_P, C.c_double, _U64]),
+    "emg_uniform_advance": (C.c_int, [_P, C.c_uint64, C.c_double, _U64]),
+    "emg_uniform_download": (C.c_int, [_P, _D, C.c_size_t]),
+    "emg_uniform_upload": (C.c_int, [_P, _D, C.c_size_t]),
+    "emg_uniform_totals": (C.c_int, [_P, _D]),
+    "emg_uniform_counters": (C.c_int, [_P, _U64]),
+    "emg_uniform_get_time": (C.c_int, [_P, _D]),
+    "emg_uniform_set_time": (C.c_int, [_P, C.c_double]),
+    "emg_uniform_synchronize": (C.c_int, [_P]),
+    "emg_uniform_stream": (C.c_int, [_P, C.POINTER(_P)]),
+    "emg_uniform_set_profiling": (C.c_int, [_P, C.c_int]),
+    "emg_uniform_kernel_times": (C.c_int, [_P, _D, _U64]),
+    "emg_uniform_launch_count": (C.c_int, [_P, _U64]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load the in-tree CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                "libemergence_b200.so is missing: build it with `python -m emergence_b200.build` "
+                "(there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class EmgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def check(code):
+    if code != EMG_OK:
+        msg = lib().emg_last_error()
+        raise EmgError(code, msg.decode() if msg else "")
+    return code

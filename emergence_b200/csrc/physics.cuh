@@ -1,0 +1,157 @@
+// Device-side physics of the compressible Euler step: NASG equation of state,
+// Euler conserved/primitive maps, primitive characteristic eigenvectors,
+// WENO5-Z interpolation and the HLLC flux.
+//
+// Formulas and their operation order follow the reference CPU solver
+// (fluid/crates/compressible/src/{eos,system,scheme}.rs) so that the plain FP64
+// instantiation, compiled without FMA contraction, rounds exactly as the CPU
+// does. The same templates instantiated with R = float give the FP32 flux
+// arithmetic of the mixed-precision form.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace emg {
+
+// NASG parameters (fluid/crates/compressible/src/eos.rs:12-25).
+struct EosD {
+    double gamma, p_inf, b, q;
+};
+
+template <typename R> struct Eos {
+    R gamma, p_inf, b, q;
+    __host__ __device__ static Eos from(const EosD& e) { return Eos{R(e.gamma), R(e.p_inf), R(e.b), R(e.q)}; }
+    // eos.rs:37-41
+    __device__ __forceinline__ R pressure(R rho, R e) const {
+        R v = R(1) / rho;
+        return (gamma - R(1)) * (e - q) / (v - b) - gamma * p_inf;
+    }
+    // eos.rs:44-54 (ρe = ρ·energy(ρ, p))
+    __device__ __forceinline__ R rho_e(R rho, R p) const {
+        R v = R(1) / rho;
+        return rho * ((p + gamma * p_inf) * (v - b) / (gamma - R(1)) + q);
+    }
+    // eos.rs:56-60
+    __device__ __forceinline__ R sound_speed_sq(R rho, R p) const {
+        R v = R(1) / rho;
+        return gamma * (p + p_inf) * v * v / (v - b);
+    }
+};
+
+template <typename R> __device__ __forceinline__ R rmax(R a, R b) { return fmax(a, b); }
+template <typename R> __device__ __forceinline__ R rmin(R a, R b) { return fmin(a, b); }
+__device__ __forceinline__ float rmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ float rmin(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
+__device__ __forceinline__ float rsqrt_(float x) { return sqrtf(x); }
+__device__ __forceinline__ double rabs(double x) { return fabs(x); }
+__device__ __forceinline__ float rabs(float x) { return fabsf(x); }
+
+// Euler system, w = (ρ,u,v,w,p), u = (ρ,ρu,ρv,ρw,E): system.rs:196-217.
+template <typename R> __device__ __forceinline__ void to_prim(const Eos<R>& e, const R* u, R* w) {
+    R rho = u[0];
+    R vx = u[1] / rho, vy = u[2] / rho, vz = u[3] / rho;
+    R ein = u[4] / rho - R(0.5) * (vx * vx + vy * vy + vz * vz);
+    w[0] = rho;
+    w[1] = vx;
+    w[2] = vy;
+    w[3] = vz;
+    w[4] = e.pressure(rho, ein);
+}
+template <typename R> __device__ __forceinline__ void to_cons(const Eos<R>& e, const R* w, R* u) {
+    R rho = w[0];
+    R ke = R(0.5) * rho * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+    u[0] = rho;
+    u[1] = rho * w[1];
+    u[2] = rho * w[2];
+    u[3] = rho * w[3];
+    u[4] = e.rho_e(rho, w[4]) + ke;
+}
+// system.rs:219-222
+template <typename R> __device__ __forceinline__ R sound_speed(const Eos<R>& e, R rho, R p) {
+    return rsqrt_(rmax(e.sound_speed_sq(rho, p), R(0)));
+}
+// system.rs:404-407 with eos.rs:75-79
+template <typename R> __device__ __forceinline__ bool admissible(const Eos<R>& e, R rho, R p) {
+    return isfinite(rho) && isfinite(p) && rho > R(0) && R(1) / rho > e.b && p + e.p_inf > R(0);
+}
+// physical flux from primitive w and its conserved q along normal index un (system.rs:268-278)
+template <typename R> __device__ __forceinline__ void flux_wq(const R* w, const R* q, int un, R* f) {
+    R u = w[un];
+    f[0] = q[0] * u;
+    f[1] = q[1] * u;
+    f[2] = q[2] * u;
+    f[3] = q[3] * u;
+    f[un] = f[un] + w[4];
+    f[4] = (q[4] + w[4]) * u;
+}
+
+// HLLC with Davis wave-speed bounds (system.rs:260-312). Returns the contact speed.
+template <typename R>
+__device__ __forceinline__ R hllc(const Eos<R>& e, const R* wl, const R* wr, int un, R* f) {
+    R cl = sound_speed(e, wl[0], wl[4]), cr = sound_speed(e, wr[0], wr[4]);
+    R ul = wl[un], ur = wr[un];
+    R sl = rmin(ul - cl, ur - cr);
+    R sr = rmax(ul + cl, ur + cr);
+    R ql[5], qr[5];
+    to_cons(e, wl, ql);
+    to_cons(e, wr, qr);
+    if (sl >= R(0)) {
+        flux_wq(wl, ql, un, f);
+        return ul;
+    }
+    if (sr <= R(0)) {
+        flux_wq(wr, qr, un, f);
+        return ur;
+    }
+    R rl = wl[0], rr = wr[0], pl = wl[4], pr = wr[4];
+    R ss = (pr - pl + rl * ul * (sl - ul) - rr * ur * (sr - ur)) / (rl * (sl - ul) - rr * (sr - ur));
+    const bool left = ss >= R(0);
+    const R* w = left ? wl : wr;
+    const R* q = left ? ql : qr;
+    R s = left ? sl : sr;
+    R fx[5];
+    flux_wq(w, q, un, fx);
+    R rho = w[0], u = w[un];
+    R fac = rho * (s - u) / (s - ss);
+    R qs[5];
+    qs[0] = fac;
+    qs[1] = fac * w[1];
+    qs[2] = fac * w[2];
+    qs[3] = fac * w[3];
+    qs[un] = fac * ss;
+    qs[4] = fac * (q[4] / rho + (ss - u) * (ss + w[4] / (rho * (s - u))));
+#pragma unroll
+    for (int k = 0; k < 5; k++) f[k] = fx[k] + s * (qs[k] - q[k]);
+    return ss;
+}
+
+// WENO-Z combination (scheme.rs:76-86); eps 1e-40 in f64 (scheme.rs:55), 1e-30 in f32.
+template <typename R> struct WenoEps;
+template <> struct WenoEps<double> { static constexpr double v = 1e-40; };
+template <> struct WenoEps<float> { static constexpr float v = 1e-30f; };
+
+template <typename R> __device__ __forceinline__ R sq(R x) { return x * x; }
+
+// WENO5-Z interpolation of point values to the midpoint x_{2+1/2} (scheme.rs:67-74).
+template <typename R> __device__ __forceinline__ R weno5z_interp(R v0, R v1, R v2, R v3, R v4) {
+    const R eps = WenoEps<R>::v;
+    R q0 = (R(3) * v0 - R(10) * v1 + R(15) * v2) / R(8);
+    R q1 = (-v1 + R(6) * v2 + R(3) * v3) / R(8);
+    R q2 = (R(3) * v2 + R(6) * v3 - v4) / R(8);
+    R b0 = R(13.0 / 12.0) * sq(v0 - R(2) * v1 + v2) + R(0.25) * sq(v0 - R(4) * v1 + R(3) * v2);
+    R b1 = R(13.0 / 12.0) * sq(v1 - R(2) * v2 + v3) + R(0.25) * sq(v1 - v3);
+    R b2 = R(13.0 / 12.0) * sq(v2 - R(2) * v3 + v4) + R(0.25) * sq(R(3) * v2 - R(4) * v3 + v4);
+    R tau = rabs(b0 - b2);
+    R a0 = R(1.0 / 16.0) * (R(1) + sq(tau / (b0 + eps)));
+    R a1 = R(10.0 / 16.0) * (R(1) + sq(tau / (b1 + eps)));
+    R a2 = R(5.0 / 16.0) * (R(1) + sq(tau / (b2 + eps)));
+    return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+}
+
+// Coefficients of the 6th-order schemes (scheme.rs:88-92).
+__device__ __forceinline__ double s6(int s) {
+    return s == 0 ? (75.0 / 64.0 - 25.0 / 384.0 + 3.0 / 640.0) : (s == 1 ? (-25.0 / 384.0 + 3.0 / 640.0) : 3.0 / 640.0);
+}
+
+}  // namespace emg

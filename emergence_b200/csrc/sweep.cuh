@@ -1,0 +1,424 @@
+// Fused per-axis sweep of the WCNS / HLLC / positivity scheme on sm_100a.
+//
+// One CTA owns P adjacent pencils (along the "lane" axis) over one segment
+// of L interior cells along the sweep axis d. It streams the segment in
+// rounds of RM = 256/P rows through shared-memory rings:
+//
+//   A  load RM new cell rows of the conserved state (SoA f64, coalesced),
+//      recover primitives in f64, keep them in the W ring;
+//   B  one thread per (midpoint, pencil): characteristic WENO5-Z
+//      interpolation to the midpoint and the HLLC flux (MF ring);
+//   C  one thread per (face, pencil): 6th-order WCNS combination of five
+//      midpoint fluxes, then the Hu–Adams–Shu positivity limiter (F ring);
+//   D  one thread per (cell, pencil): the divergence −(F⁺ − F⁻)/dx added to
+//      the stage residual; on the last active axis the SSP-RK3 combination
+//      is applied in f64 and written straight to the next stage state, and on
+//      the third stage the CFL rate of the new state is reduced as well.
+//
+// Nothing but the state, the residual and the next state touches HBM: the
+// primitive array, the midpoint fluxes and the face fluxes of the reference
+// GPU design (G/kernels.cu:364-510, each a round trip through global memory)
+// live only in shared memory. Midpoints are computed once per pencil segment
+// (the reference CPU memoises them per line, C/scheme.rs:148-154).
+//
+// Index conventions inside a segment with first interior cell s0 (0-based)
+// and Ls cells: local row r is padded cell g + s0 − 5 + r along d (row 5 is
+// the first interior cell); midpoint m sits between rows m+2 and m+3 and
+// reads rows m..m+5; face f (f = 0..Ls) sits between rows f+4 and f+5 and
+// combines midpoints f..f+4; cell c (0..Ls−1) is row c+5 and reads faces c
+// and c+1.
+#pragma once
+#include "physics.cuh"
+#include <stdint.h>
+
+namespace emg {
+
+constexpr int SWEEP_THREADS = 256;
+
+// Device control block of one solver: the time step of the stage kernels is
+// read from here so that whole steps can run without a host round trip.
+struct StepCtl {
+    double dt;                    // step size of the step in flight
+    double t;                     // simulation time
+    double t_end;                 // stop time of device-driven stepping (+inf: none)
+    unsigned long long rate_bits; // max CFL rate of the latest state, as ordered bits of a non-negative double
+    unsigned long long steps;     // steps taken on the device
+    int done;                     // 1: no further steps (t_end reached or error)
+    int status;                   // EMG_* error code raised on the device (0: ok)
+    unsigned long long counters[4]; // faces, shock-path faces, fallbacks, limited faces
+};
+
+struct SweepParams {
+    const double* __restrict__ uin;  // stage input (ghost-filled along d), SoA with field stride ncell
+    double* rhs;                     // stage residual, same indexing as uin
+    const double* base;              // RK base state ("old"), last axis only
+    const double* cur;               // previous value of the RK destination, last axis stages 2-3
+    double* dest;                    // RK destination, last axis only
+    StepCtl* ctl;
+    int64_t ncell;
+    int64_t sd, sl, so;  // strides of the sweep, lane and other axes
+    int nd, nl, no;      // interior extents
+    int gd, gl, go;      // ghost offsets
+    int d;               // sweep axis (momentum index 1+d)
+    int seg;             // segment length L
+    int first, last;     // first / last active axis of the residual
+    int stage;           // SSP-RK3 stage 1..3
+    int rows_contig;     // sd == 1: rows contiguous in memory
+    int cfl_fuse;        // stage 3 of the last axis: reduce the CFL rate
+    double dx;           // cell size along d
+    double ndim;         // number of active axes (λ = ndim·dt/dx)
+    int positivity;      // limiter on/off
+    int cfl_active[3];   // active axes for the fused CFL rate
+    double cfl_dx[3];
+    // which of the three padded axes the sweep / lane / other axes are (for the CFL rate)
+    EosD eos;
+};
+
+template <typename R> struct RingTypes {
+    static constexpr bool MIXED = false;
+};
+template <> struct RingTypes<float> {
+    static constexpr bool MIXED = true;
+};
+
+// ring slots: power of two ≥ RM + 5
+template <int RM> struct RingSize {
+    static constexpr int value = RM + 5 <= 16 ? 16 : (RM + 5 <= 32 ? 32 : 64);
+};
+
+template <typename RF, int P> struct SweepSmem {
+    static constexpr int RM = SWEEP_THREADS / P;
+    static constexpr int RS = RingSize<RM>::value;
+    static constexpr int STR = 5 * P + 1;  // row stride in elements (odd: conflict-free column access)
+    static constexpr size_t bytes() {
+        return (size_t)RS * STR * sizeof(double)          // W (f64 primitives)
+               + (RingTypes<RF>::MIXED ? (size_t)RS * STR * sizeof(float) : 0)  // Wf (f32 copy)
+               + (size_t)RS * STR * sizeof(RF)            // MF (midpoint fluxes)
+               + (size_t)RS * STR * sizeof(double);       // F (face fluxes)
+    }
+};
+
+template <typename RF, int P, int D>
+struct Sweep {
+    static constexpr int T = SWEEP_THREADS;
+    static constexpr int RM = T / P;
+    static constexpr int RS = RingSize<RM>::value;
+    static constexpr int STR = 5 * P + 1;
+    static constexpr bool MIXED = RingTypes<RF>::MIXED;
+
+    __device__ static __forceinline__ int slot(int x) { return x & (RS - 1); }
+    // element (row x, field k, lane l) of a ring
+    __device__ static __forceinline__ int at(int x, int k, int l) { return slot(x) * STR + k * P + l; }
+
+    // Characteristic WENO5-Z interpolation to midpoint m and its HLLC flux:
+    // sparse form of C/scheme.rs:286-333. The zero entries of the Euler
+    // eigenvectors (C/system.rs:232-258) are skipped, which leaves every
+    // non-zero sum of the dense products unchanged.
+    __device__ static __forceinline__ void midpoint(const Eos<RF>& e, const RF* __restrict__ Wr, int m, int l,
+                                                    RF* f, bool& fb) {
+        constexpr int un = 1 + D;
+        constexpr int t1 = 1 + (D + 1) % 3, t2 = 1 + (D + 2) % 3;
+        const int j = m + 2;
+        // arithmetic-mean state and its eigenvectors
+        RF avg[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) avg[k] = RF(0.5) * (Wr[at(j, k, l)] + Wr[at(j + 1, k, l)]);
+        const RF rho = avg[0];
+        const RF c = sound_speed(e, avg[0], avg[4]);
+        const RF l0un = -rho / (RF(2) * c);
+        const RF l04 = RF(1) / (RF(2) * c * c);
+        const RF l14 = -RF(1) / (c * c);
+        const RF l4un = rho / (RF(2) * c);
+        const RF run0 = -c / rho;
+        const RF r40 = c * c;
+        const RF run4 = c / rho;
+        // characteristic variables of the six stencil cells
+        RF ch0[6], ch1[6], ch2[6], ch3[6], ch4[6];
+#pragma unroll
+        for (int s = 0; s < 6; s++) {
+            const int row = m + s;
+            const RF w0 = Wr[at(row, 0, l)];
+            const RF wn = Wr[at(row, un, l)];
+            const RF w4 = Wr[at(row, 4, l)];
+            ch0[s] = l0un * wn + l04 * w4;
+            ch1[s] = w0 + l14 * w4;
+            ch2[s] = Wr[at(row, t1, l)];
+            ch3[s] = Wr[at(row, t2, l)];
+            ch4[s] = l4un * wn + l04 * w4;
+        }
+        RF cl[5], cr[5];
+        cl[0] = weno5z_interp(ch0[0], ch0[1], ch0[2], ch0[3], ch0[4]);
+        cr[0] = weno5z_interp(ch0[5], ch0[4], ch0[3], ch0[2], ch0[1]);
+        cl[1] = weno5z_interp(ch1[0], ch1[1], ch1[2], ch1[3], ch1[4]);
+        cr[1] = weno5z_interp(ch1[5], ch1[4], ch1[3], ch1[2], ch1[1]);
+        cl[2] = weno5z_interp(ch2[0], ch2[1], ch2[2], ch2[3], ch2[4]);
+        cr[2] = weno5z_interp(ch2[5], ch2[4], ch2[3], ch2[2], ch2[1]);
+        cl[3] = weno5z_interp(ch3[0], ch3[1], ch3[2], ch3[3], ch3[4]);
+        cr[3] = weno5z_interp(ch3[5], ch3[4], ch3[3], ch3[2], ch3[1]);
+        cl[4] = weno5z_interp(ch4[0], ch4[1], ch4[2], ch4[3], ch4[4]);
+        cr[4] = weno5z_interp(ch4[5], ch4[4], ch4[3], ch4[2], ch4[1]);
+        // back to primitives: rows of R (columns are the waves)
+        RF wl[5], wr[5];
+        wl[0] = (cl[0] + cl[1]) + cl[4];
+        wr[0] = (cr[0] + cr[1]) + cr[4];
+        wl[un] = run0 * cl[0] + run4 * cl[4];
+        wr[un] = run0 * cr[0] + run4 * cr[4];
+        wl[t1] = cl[2];
+        wr[t1] = cr[2];
+        wl[t2] = cl[3];
+        wr[t2] = cr[3];
+        wl[4] = r40 * cl[0] + r40 * cl[4];
+        wr[4] = r40 * cr[0] + r40 * cr[4];
+        fb = false;
+        if (!admissible(e, wl[0], wl[4]) || !admissible(e, wr[0], wr[4])) {
+            fb = true;
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                wl[k] = Wr[at(j, k, l)];
+                wr[k] = Wr[at(j + 1, k, l)];
+            }
+        }
+        hllc(e, wl, wr, un, f);
+    }
+
+    // One-sided admissibility of the limiter (C/scheme.rs:408-416), in f64.
+    __device__ static __forceinline__ bool lim_ok(const Eos<double>& e, const double* fx, const double* ul,
+                                                  const double* fl, const double* ur, const double* fr, double lam2) {
+        double a[5], w[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) a[k] = ul[k] - lam2 * (fx[k] - fl[k]);
+        to_prim(e, a, w);
+        if (!admissible(e, w[0], w[4])) return false;
+#pragma unroll
+        for (int k = 0; k < 5; k++) a[k] = ur[k] + lam2 * (fx[k] - fr[k]);
+        to_prim(e, a, w);
+        return admissible(e, w[0], w[4]);
+    }
+
+    __device__ static void run(const SweepParams& p) {
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        double* W = reinterpret_cast<double*>(smem_raw);
+        RF* Wf;
+        RF* MF;
+        if constexpr (MIXED) {
+            Wf = reinterpret_cast<RF*>(W + RS * STR);
+            MF = Wf + RS * STR;
+        } else {
+            Wf = reinterpret_cast<RF*>(W);
+            MF = reinterpret_cast<RF*>(W + RS * STR);
+        }
+        double* F = reinterpret_cast<double*>(MF + RS * STR);
+        __shared__ unsigned int s_fallback, s_limited;
+        __shared__ double s_rate[T / 32];
+
+        const StepCtl* ctl = p.ctl;
+        if (ctl->done) return;
+        const double dt = ctl->dt;
+        const int tid = threadIdx.x;
+        if (tid == 0) {
+            s_fallback = 0;
+            s_limited = 0;
+        }
+
+        const int lane0 = blockIdx.x * P;
+        const int s0 = blockIdx.y * p.seg;
+        const int Ls = min(p.seg, p.nd - s0);
+        const int oc = blockIdx.z;
+        // padded offset of (row 0, lane 0)
+        const int64_t base0 = (int64_t)(p.gd + s0 - 5) * p.sd + (int64_t)(p.gl + lane0) * p.sl + (int64_t)(p.go + oc) * p.so;
+        const int nlanes = min(P, p.nl - lane0);
+        // neighbouring segments recompute the 5 midpoints and 1 face they
+        // share; only the owner counts them in the statistics
+        const bool tail = s0 + Ls == p.nd;
+        const Eos<double> ed = Eos<double>::from(p.eos);
+        const Eos<RF> ef = Eos<RF>::from(p.eos);
+        constexpr int un = 1 + D;
+        const double lam = (p.ndim * dt) / p.dx;  // λ = ndim·dt/dx (C/solver.rs:393)
+        const double lam2 = 2.0 * lam;
+        const bool lim_on = p.positivity && lam > 0.0;  // C/scheme.rs:278
+        const double inv = 1.0 / p.dx;
+        const int nrounds = (Ls + 5 + RM - 1) / RM;
+        const int nrows = Ls + 10;
+        double rate_max = 0.0;
+
+        for (int r = 0; r < nrounds; r++) {
+            // ---- A: load rows [lo, hi) and recover primitives
+            {
+                const int lo = r == 0 ? 0 : RM * r + 5;
+                const int hi = min(RM * r + RM + 5, nrows);
+                const int cnt = (hi - lo) * P;
+                for (int idx = tid; idx < cnt; idx += T) {
+                    int rr, l;
+                    if (p.rows_contig) {
+                        rr = idx % (hi - lo);
+                        l = idx / (hi - lo);
+                    } else {
+                        rr = idx / P;
+                        l = idx % P;
+                    }
+                    if (l < nlanes) {
+                        const int row = lo + rr;
+                        const int64_t g = base0 + (int64_t)row * p.sd + (int64_t)l * p.sl;
+                        double u[5], w[5];
+#pragma unroll
+                        for (int k = 0; k < 5; k++) u[k] = __ldg(p.uin + k * p.ncell + g);
+                        to_prim(ed, u, w);
+#pragma unroll
+                        for (int k = 0; k < 5; k++) {
+                            W[at(row, k, l)] = w[k];
+                            if constexpr (MIXED) Wf[at(row, k, l)] = RF(w[k]);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            // ---- B: midpoints [RM r, RM r + RM)
+            {
+                const int m = RM * r + tid / P;
+                const int l = tid % P;
+                if (m < Ls + 5 && l < nlanes) {
+                    RF f[5];
+                    bool fb;
+                    midpoint(ef, Wf, m, l, f, fb);
+#pragma unroll
+                    for (int k = 0; k < 5; k++) MF[at(m, k, l)] = f[k];
+                    if (fb && (m < Ls || tail)) atomicAdd(&s_fallback, 1u);
+                }
+            }
+            __syncthreads();
+            // ---- C: faces [RM r − 4, RM r + RM − 4)
+            {
+                const int fidx = RM * r - 4 + tid / P;
+                const int l = tid % P;
+                if (fidx >= 0 && fidx <= Ls && l < nlanes) {
+                    double fh[5];
+                    // F̃ = Σ_s S6[s] (F̂_{+s} + F̂_{−s}), order as C/scheme.rs:230-246
+#pragma unroll
+                    for (int k = 0; k < 5; k++) {
+                        double acc = 0.0;
+                        acc = acc + s6(0) * double(MF[at(fidx + 2, k, l)]);
+                        acc = acc + s6(1) * double(MF[at(fidx + 3, k, l)]);
+                        acc = acc + s6(1) * double(MF[at(fidx + 1, k, l)]);
+                        acc = acc + s6(2) * double(MF[at(fidx + 4, k, l)]);
+                        acc = acc + s6(2) * double(MF[at(fidx, k, l)]);
+                        fh[k] = acc;
+                    }
+                    if (lim_on) {
+                        // Hu–Adams–Shu limiter (C/scheme.rs:395-464) between rows i = f+4 and i+1
+                        const int i = fidx + 4;
+                        double wi[5], wj[5], ul[5], ur[5], flp[5], frp[5];
+#pragma unroll
+                        for (int k = 0; k < 5; k++) {
+                            wi[k] = W[at(i, k, l)];
+                            wj[k] = W[at(i + 1, k, l)];
+                        }
+                        to_cons(ed, wi, ul);
+                        to_cons(ed, wj, ur);
+                        flux_wq(wi, ul, un, flp);
+                        flux_wq(wj, ur, un, frp);
+                        bool finite = true;
+#pragma unroll
+                        for (int k = 0; k < 5; k++) finite = finite && isfinite(fh[k]);
+                        if (!(finite && lim_ok(ed, fh, ul, flp, ur, frp, lam2))) {
+                            const double alpha = fmax(fabs(wi[un]) + sound_speed(ed, wi[0], wi[4]),
+                                                      fabs(wj[un]) + sound_speed(ed, wj[0], wj[4]));
+                            double flf[5], bl[5];
+#pragma unroll
+                            for (int k = 0; k < 5; k++) flf[k] = 0.5 * (flp[k] + frp[k]) - 0.5 * alpha * (ur[k] - ul[k]);
+                            double lo = 0.0, hi = 1.0;
+                            for (int it = 0; it < 30; it++) {
+                                const double mid = 0.5 * (lo + hi);
+#pragma unroll
+                                for (int k = 0; k < 5; k++)
+                                    bl[k] = isfinite(fh[k]) ? mid * fh[k] + (1.0 - mid) * flf[k] : flf[k];
+                                if (lim_ok(ed, bl, ul, flp, ur, frp, lam2))
+                                    lo = mid;
+                                else
+                                    hi = mid;
+                            }
+#pragma unroll
+                            for (int k = 0; k < 5; k++) fh[k] = isfinite(fh[k]) ? lo * fh[k] + (1.0 - lo) * flf[k] : flf[k];
+                            if (fidx < Ls || tail) atomicAdd(&s_limited, 1u);
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < 5; k++) F[at(fidx, k, l)] = fh[k];
+                }
+            }
+            __syncthreads();
+            // ---- D: cells [RM r − 5, RM r + RM − 5)
+            {
+                int c, l;
+                if (p.rows_contig) {
+                    c = RM * r - 5 + tid % RM;
+                    l = tid / RM;
+                } else {
+                    c = RM * r - 5 + tid / P;
+                    l = tid % P;
+                }
+                if (c >= 0 && c < Ls && l < nlanes) {
+                    const int64_t g = base0 + (int64_t)(c + 5) * p.sd + (int64_t)l * p.sl;
+                    double res[5];
+#pragma unroll
+                    for (int k = 0; k < 5; k++) {
+                        const double x = (F[at(c + 1, k, l)] - F[at(c, k, l)]) * inv;
+                        const double prev = p.first ? 0.0 : p.rhs[k * p.ncell + g];
+                        res[k] = prev - x;
+                    }
+                    if (!p.last) {
+#pragma unroll
+                        for (int k = 0; k < 5; k++) p.rhs[k * p.ncell + g] = res[k];
+                    } else {
+                        double un_[5];
+#pragma unroll
+                        for (int k = 0; k < 5; k++) {
+                            const double o = p.base[k * p.ncell + g];
+                            double v;
+                            if (p.stage == 1) {
+                                v = o + dt * res[k];
+                            } else if (p.stage == 2) {
+                                v = 0.75 * o + 0.25 * (p.cur[k * p.ncell + g] + dt * res[k]);
+                            } else {
+                                v = p.cur[k * p.ncell + g] / 3.0 + (2.0 / 3.0) * (o + dt * res[k]);
+                            }
+                            p.dest[k * p.ncell + g] = v;
+                            un_[k] = v;
+                        }
+                        if (p.cfl_fuse) {
+                            // CFL rate Σ_d (|u_d| + c)/dx_d of the new state (C/solver.rs:485-497)
+                            double w[5];
+                            to_prim(ed, un_, w);
+                            const double cs = sound_speed(ed, w[0], w[4]);
+                            double acc = -0.0;
+#pragma unroll
+                            for (int dd = 0; dd < 3; dd++)
+                                if (p.cfl_active[dd]) acc = acc + (fabs(w[1 + dd]) + cs) / p.cfl_dx[dd];
+                            rate_max = fmax(rate_max, acc);
+                        }
+                    }
+                }
+            }
+            // next round's loads only touch W slots that C has finished with,
+            // and C of the next round writes F slots after the barrier below A.
+        }
+        // block-level counters and CFL rate
+        if (p.cfl_fuse) {
+            double v = rate_max;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+            if ((tid & 31) == 0) s_rate[tid >> 5] = v;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            if (s_fallback) atomicAdd(&p.ctl->counters[2], (unsigned long long)s_fallback);
+            if (s_limited) atomicAdd(&p.ctl->counters[3], (unsigned long long)s_limited);
+            if (p.cfl_fuse) {
+                double v = s_rate[0];
+                for (int w = 1; w < T / 32; w++) v = fmax(v, s_rate[w]);
+                if (!isnan(v) && v > 0.0) atomicMax(&p.ctl->rate_bits, (unsigned long long)__double_as_longlong(v));
+            }
+        }
+    }
+};
+
+}  // namespace emg

@@ -1,0 +1,14 @@
+// Launchers of the fused sweep kernels (instantiated in sweep_f64.cu, which is
+// compiled without FMA contraction so its f64 arithmetic rounds like the
+// reference CPU solver, and in sweep_mixed.cu, FP32 flux arithmetic).
+#pragma once
+#include "sweep.cuh"
+
+namespace emg {
+// P = pencils per CTA (8, 16 or 32). Returns the launch error.
+cudaError_t sweep_launch_f64(int P, const SweepParams& p, dim3 grid, cudaStream_t s);
+cudaError_t sweep_launch_mixed(int P, const SweepParams& p, dim3 grid, cudaStream_t s);
+// Opt the kernels into their dynamic shared memory size (once per device).
+cudaError_t sweep_prepare_f64();
+cudaError_t sweep_prepare_mixed();
+}  // namespace emg

@@ -1,0 +1,981 @@
+// Uniform-grid solver: host object, auxiliary kernels and the C ABI of
+// include/emergence_b200.h (emg_uniform_*).
+//
+// Replaces compressible-cuda's GpuSolver (fluid/crates/compressible-cuda/src/
+// lib.rs:155-477) for the Euler system. Per RK stage the device runs one
+// ghost-fill launch per active axis and one fused sweep per active axis
+// (sweep.cuh); the reference runs ghost + prim + 4 launches per axis + rk
+// (G/lib.rs:332-400). The CFL rate of each new state is reduced inside the
+// last sweep of stage 3 and dt is formed on the device, so steps chain
+// without host round trips (the reference copies the rates to the host every
+// step, G/lib.rs:430).
+//
+// Built with -fmad=false: the ghost, CFL and control arithmetic must round as
+// the reference CPU solver does.
+#include "../../include/emergence_b200.h"
+#include "sweep_launch.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace emg {
+
+thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define EMG_CUDA(call)                                                                                 \
+    do {                                                                                               \
+        cudaError_t _e = (call);                                                                       \
+        if (_e != cudaSuccess)                                                                         \
+            return set_error(EMG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e));      \
+    } while (0)
+
+// ------------------------------------------------------------------ auxiliary kernels
+
+// AoS [cell][5] → SoA [5][cell]
+__global__ void aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, int64_t ncell) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncell; c += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) soa[k * ncell + c] = aos[5 * c + k];
+    }
+}
+__global__ void soa_to_aos(const double* __restrict__ soa, double* __restrict__ aos, int64_t ncell) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncell; c += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) aos[5 * c + k] = soa[k * ncell + c];
+    }
+}
+
+struct GhostParams {
+    double* u;
+    const StepCtl* ctl;
+    int64_t ncell;
+    int64_t m[3];
+    int64_t stride[3];
+    int64_t n, ng;
+    int d, e0, e1;
+    int deep;  // a short reflecting axis exists (C/solver.rs:261-262)
+    int kind[2];
+    double state[2][5];
+    EosD eos;
+};
+
+// Characteristic ghost stencil (C/boundary.rs:48-96), dense as the reference.
+struct CharStencilD {
+    double wi[5], wf[5], w1[5];
+    double l[5][5], r[5][5];
+    bool outgoing[5];
+    __device__ void init(const Eos<double>& e, const double* ub, const double* ub1, const double* uf, int d, int side) {
+        to_prim(e, ub, wi);
+        to_prim(e, uf, wf);
+        to_prim(e, ub1, w1);
+        const double rho = wi[0], c = sound_speed(e, wi[0], wi[4]);
+        const int un = 1 + d, t1 = 1 + (d + 1) % 3, t2 = 1 + (d + 2) % 3;
+        for (int i = 0; i < 5; i++)
+            for (int j = 0; j < 5; j++) l[i][j] = r[i][j] = 0.0;
+        l[0][un] = -rho / (2.0 * c);
+        l[0][4] = 1.0 / (2.0 * c * c);
+        l[1][0] = 1.0;
+        l[1][4] = -1.0 / (c * c);
+        l[2][t1] = 1.0;
+        l[3][t2] = 1.0;
+        l[4][un] = rho / (2.0 * c);
+        l[4][4] = 1.0 / (2.0 * c * c);
+        r[0][0] = 1.0;
+        r[un][0] = -c / rho;
+        r[4][0] = c * c;
+        r[0][1] = 1.0;
+        r[t1][2] = 1.0;
+        r[t2][3] = 1.0;
+        r[0][4] = 1.0;
+        r[un][4] = c / rho;
+        r[4][4] = c * c;
+        const double u = wi[un];
+        const double lam[5] = {u - c, u, u, u, u + c};
+        const double outward = side == 1 ? 1.0 : -1.0;
+        for (int k = 0; k < 5; k++) outgoing[k] = lam[k] * outward > 0.0;
+    }
+    __device__ void conserved(const Eos<double>& e, double m, double* out) const {
+        double dw[5], wg[5];
+        for (int k = 0; k < 5; k++) dw[k] = wi[k] - wf[k] + m * (wi[k] - w1[k]);
+        for (int k = 0; k < 5; k++) wg[k] = wf[k];
+        for (int kf = 0; kf < 5; kf++) {
+            if (outgoing[kf]) {
+                double amp = -0.0;
+                for (int q = 0; q < 5; q++) amp = amp + l[kf][q] * dw[q];
+                for (int q = 0; q < 5; q++) wg[q] = wg[q] + r[q][kf] * amp;
+            }
+        }
+        to_cons(e, wg, out);
+    }
+};
+
+// Ghost layers along axis d for every (a, b) of the two other padded axes
+// (C/solver.rs:278-348; G/kernels.cu:567-614). Only interior cells along d
+// are read, so threads are independent.
+__global__ void ghost_kernel(const GhostParams p) {
+    if (p.ctl->done) return;
+    const Eos<double> e = Eos<double>::from(p.eos);
+    const int64_t total = p.m[p.e0] * p.m[p.e1] * p.ng;
+    const int64_t n = p.n, ng = p.ng;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t gi = t % ng;
+        const int64_t pq = t / ng;
+        const int64_t b = pq % p.m[p.e1];
+        const int64_t a = pq / p.m[p.e1];
+        const int64_t off = a * p.stride[p.e0] + b * p.stride[p.e1];
+        const int64_t sd = p.stride[p.d];
+        auto at = [&](int64_t c) { return off + c * sd; };
+        auto load = [&](int64_t c, double* v) {
+            for (int k = 0; k < 5; k++) v[k] = p.u[k * p.ncell + at(c)];
+        };
+        CharStencilD ch[2];
+        if (p.kind[0] == EMG_BC_CHARACTERISTIC) {
+            double ub[5], ub1[5];
+            load(ng, ub);
+            load(ng + 1, ub1);
+            ch[0].init(e, ub, ub1, p.state[0], p.d, 0);
+        }
+        if (p.kind[1] == EMG_BC_CHARACTERISTIC) {
+            double ub[5], ub1[5];
+            load(n + ng - 1, ub);
+            load(n + ng - 2, ub1);
+            ch[1].init(e, ub, ub1, p.state[1], p.d, 1);
+        }
+        // deep reflected image on a short axis (C/boundary.rs:98-145)
+        auto reflected = [&](int64_t x, double* v) {
+            bool flip = false;
+            for (int k = 0; k < 5; k++) v[k] = __longlong_as_double(0x7ff8000000000000ll);
+            for (int it = 0; it < 4096; it++) {
+                if (x >= 0 && x < n) {
+                    load(ng + x, v);
+                    break;
+                }
+                const int side = x >= n ? 1 : 0;
+                const int kind = p.kind[side];
+                if (kind == EMG_BC_REFLECT) {
+                    x = side == 0 ? -1 - x : 2 * n - 1 - x;
+                    flip = !flip;
+                } else if (kind == EMG_BC_PERIODIC) {
+                    int64_t r = x % n;
+                    if (r < 0) r += n;
+                    load(ng + r, v);
+                    break;
+                } else if (kind == EMG_BC_OUTFLOW) {
+                    load(ng + (side == 0 ? 0 : n - 1), v);
+                    break;
+                } else if (kind == EMG_BC_DIRICHLET) {
+                    for (int k = 0; k < 5; k++) v[k] = p.state[side][k];
+                    break;
+                } else {
+                    const int64_t layer = side == 0 ? -x : x - n + 1;
+                    ch[side].conserved(e, (double)layer, v);
+                    break;
+                }
+            }
+            if (flip) v[1 + p.d] = -v[1 + p.d];
+        };
+        // periodic sources (C/solver.rs:62-70)
+        int64_t lo_s, hi_s;
+        if (n >= ng) {
+            lo_s = n + gi;
+            hi_s = ng + gi;
+        } else {
+            lo_s = ng + (gi + n - ng % n) % n;
+            hi_s = ng + gi % n;
+        }
+        double v[5];
+        switch (p.kind[0]) {
+            case EMG_BC_PERIODIC: load(lo_s, v); break;
+            case EMG_BC_OUTFLOW: load(ng, v); break;
+            case EMG_BC_DIRICHLET:
+                for (int k = 0; k < 5; k++) v[k] = p.state[0][k];
+                break;
+            case EMG_BC_CHARACTERISTIC: ch[0].conserved(e, (double)(ng - gi), v); break;
+            default:
+                if (p.deep && n < ng) {
+                    reflected(gi - ng, v);
+                } else {
+                    load(2 * ng - 1 - gi, v);
+                    v[1 + p.d] = -v[1 + p.d];
+                }
+        }
+        for (int k = 0; k < 5; k++) p.u[k * p.ncell + at(gi)] = v[k];
+        switch (p.kind[1]) {
+            case EMG_BC_PERIODIC: load(hi_s, v); break;
+            case EMG_BC_OUTFLOW: load(n + ng - 1, v); break;
+            case EMG_BC_DIRICHLET:
+                for (int k = 0; k < 5; k++) v[k] = p.state[1][k];
+                break;
+            case EMG_BC_CHARACTERISTIC: ch[1].conserved(e, (double)(gi + 1), v); break;
+            default:
+                if (p.deep && n < ng) {
+                    reflected(n + gi, v);
+                } else {
+                    load(n + ng - 1 - gi, v);
+                    v[1 + p.d] = -v[1 + p.d];
+                }
+        }
+        for (int k = 0; k < 5; k++) p.u[k * p.ncell + at(n + ng + gi)] = v[k];
+    }
+}
+
+struct CellRange {
+    int64_t n[3], g[3], stride[3];
+    int64_t cells;
+    __device__ int64_t index(int64_t t) const {
+        const int64_t k = t % n[2];
+        const int64_t j = (t / n[2]) % n[1];
+        const int64_t i = t / (n[1] * n[2]);
+        return (i + g[0]) * stride[0] + (j + g[1]) * stride[1] + (k + g[2]) * stride[2];
+    }
+};
+
+// CFL rate max over interior cells of Σ_d (|u_d| + c)/dx_d (C/solver.rs:478-516).
+__global__ void cfl_kernel(const double* __restrict__ u, int64_t ncell, CellRange cr, int a0, int a1, int a2, double dx0,
+                           double dx1, double dx2, EosD eosd, StepCtl* ctl) {
+    const Eos<double> e = Eos<double>::from(eosd);
+    const int act[3] = {a0, a1, a2};
+    const double dx[3] = {dx0, dx1, dx2};
+    double rate = 0.0;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < cr.cells; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = cr.index(t);
+        double q[5], w[5];
+        for (int k = 0; k < 5; k++) q[k] = u[k * ncell + c];
+        to_prim(e, q, w);
+        const double cs = sound_speed(e, w[0], w[4]);
+        double acc = -0.0;
+        for (int d = 0; d < 3; d++)
+            if (act[d]) acc = acc + (fabs(w[1 + d]) + cs) / dx[d];
+        rate = fmax(rate, acc);
+    }
+    for (int o = 16; o > 0; o >>= 1) rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, o));
+    __shared__ double s[32];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = rate;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = s[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) v = fmax(v, s[w]);
+        if (!isnan(v) && v > 0.0) atomicMax(&ctl->rate_bits, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+__global__ void ctl_reset_rate(StepCtl* ctl) { ctl->rate_bits = 0ull; }
+
+// Host-given dt (Solver::step / GpuSolver::step).
+__global__ void ctl_begin_host(StepCtl* ctl, double dt) {
+    ctl->dt = dt;
+    ctl->done = 0;
+    ctl->rate_bits = 0ull;
+}
+
+// Device dt = min(cfl / rate, t_end − t) with the stopping rule and collapse
+// check of Solver::run_to (C/solver.rs:758-768).
+__global__ void ctl_begin_device(StepCtl* ctl, double cfl) {
+    if (ctl->done) return;
+    const double rate = __longlong_as_double((long long)ctl->rate_bits);
+    const double t = ctl->t, t_end = ctl->t_end;
+    double dt = cfl / rate;
+    if (isinf(t_end)) {
+        if (!(isfinite(dt) && dt > 0.0)) {
+            ctl->status = EMG_ERR_DT_COLLAPSED;
+            ctl->done = 1;
+            return;
+        }
+    } else {
+        if (!(t < t_end - 1e-10 * fabs(t_end))) {
+            ctl->done = 1;
+            return;
+        }
+        dt = fmin(dt, t_end - t);
+        if (!(isfinite(dt) && dt > 1e-12 * fmax(fabs(t_end), 1e-300))) {
+            ctl->status = EMG_ERR_DT_COLLAPSED;
+            ctl->done = 1;
+            return;
+        }
+    }
+    ctl->dt = dt;
+    ctl->rate_bits = 0ull;
+}
+
+__global__ void ctl_end(StepCtl* ctl) {
+    if (ctl->done) return;
+    ctl->t = ctl->t + ctl->dt;
+    ctl->steps += 1;
+}
+
+// Σ u·vol over interior cells: per-block partial sums, then one block adds
+// the partials in a fixed order (deterministic).
+__global__ void totals_partial(const double* __restrict__ u, int64_t ncell, CellRange cr, double vol, double* partial) {
+    double s[5] = {0, 0, 0, 0, 0};
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < cr.cells; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = cr.index(t);
+        for (int k = 0; k < 5; k++) s[k] = s[k] + u[k * ncell + c] * vol;
+    }
+    __shared__ double sh[5][256];
+    for (int k = 0; k < 5; k++) sh[k][threadIdx.x] = s[k];
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h)
+            for (int k = 0; k < 5; k++) sh[k][threadIdx.x] = sh[k][threadIdx.x] + sh[k][threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 5; k++) partial[5 * blockIdx.x + k] = sh[k][0];
+}
+__global__ void totals_final(const double* partial, int nblocks, double* out) {
+    if (threadIdx.x < 5) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; b++) s = s + partial[5 * b + threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+}
+
+}  // namespace emg
+
+using namespace emg;
+
+// ------------------------------------------------------------------ solver object
+
+struct emg_uniform {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    emg_mesh mesh{};
+    emg_eos eos{};
+    emg_bc bc[6]{};
+    emg_opts opts{};
+    int64_t m[3]{}, stride[3]{}, ncell = 0, cells = 0;
+    int active[3]{};
+    int ndim = 0;
+    bool deep = false;
+    double* u = nullptr;
+    double* sa = nullptr;
+    double* sb = nullptr;
+    double* rhs = nullptr;
+    double* staging = nullptr;
+    double* partial = nullptr;
+    StepCtl* ctl = nullptr;
+    StepCtl* ctl_host = nullptr;  // pinned mirror
+    bool rate_valid = false;
+    double t_host = 0.0;          // mirror of ctl->t when the device is idle
+    uint64_t faces = 0, weno_faces = 0;  // host-side face counts
+    uint64_t launches = 0;
+    // profiling
+    bool profiling = false;
+    struct Rec {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    double prof_ms[EMG_K_COUNT]{};
+    uint64_t prof_n[EMG_K_COUNT]{};
+    // sweep shapes per axis
+    int sweepP[3]{}, sweepSeg[3]{};
+    dim3 sweepGrid[3];
+    int lane_axis[3]{}, other_axis[3]{};
+};
+
+namespace {
+
+int kernel_grid(int64_t work, int threads) {
+    int64_t b = (work + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > 148 * 16) b = 148 * 16;
+    return (int)b;
+}
+
+cudaEvent_t take_event(emg_uniform* h) {
+    if (!h->pool.empty()) {
+        cudaEvent_t e = h->pool.back();
+        h->pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct ProfScope {
+    emg_uniform* h;
+    int kind;
+    cudaEvent_t a = nullptr;
+    ProfScope(emg_uniform* hh, int k) : h(hh), kind(k) {
+        h->launches++;
+        if (h->profiling) {
+            a = take_event(h);
+            cudaEventRecord(a, h->stream);
+        }
+    }
+    ~ProfScope() {
+        if (h->profiling) {
+            cudaEvent_t b = take_event(h);
+            cudaEventRecord(b, h->stream);
+            h->recs.push_back({kind, a, b});
+        }
+    }
+};
+
+void plan_sweeps(emg_uniform* h) {
+    for (int d = 0; d < 3; d++) {
+        if (!h->active[d]) continue;
+        // lane axis: the active other axis with the smallest stride
+        int o[2], no = 0;
+        for (int e = 0; e < 3; e++)
+            if (e != d) o[no++] = e;
+        int lane = o[1], other = o[0];  // o[1] has the smaller stride
+        if (!h->active[o[1]] && h->active[o[0]]) {
+            lane = o[0];
+            other = o[1];
+        }
+        h->lane_axis[d] = lane;
+        h->other_axis[d] = other;
+        const int64_t nd = h->mesh.n[d], nl = h->mesh.n[lane], nother = h->mesh.n[other];
+        int P = 32;
+        if (nl <= 8)
+            P = 8;
+        else if (nl <= 16)
+            P = 16;
+        const int64_t lane_tiles = (nl + P - 1) / P;
+        // segment length: whole pencils when that already gives enough CTAs
+        int64_t seg = nd;
+        const int64_t target = 4 * 148;
+        while (seg > 16 && lane_tiles * ((nd + seg - 1) / seg) * nother < target) seg = (seg + 1) / 2;
+        h->sweepP[d] = P;
+        h->sweepSeg[d] = (int)seg;
+        h->sweepGrid[d] = dim3((unsigned)lane_tiles, (unsigned)((nd + seg - 1) / seg), (unsigned)nother);
+    }
+}
+
+int launch_ghosts(emg_uniform* h, double* arr) {
+    for (int d = 0; d < 3; d++) {
+        if (!h->active[d]) continue;
+        GhostParams p{};
+        p.u = arr;
+        p.ctl = h->ctl;
+        p.ncell = h->ncell;
+        for (int k = 0; k < 3; k++) {
+            p.m[k] = h->m[k];
+            p.stride[k] = h->stride[k];
+        }
+        p.n = h->mesh.n[d];
+        p.ng = h->mesh.ng;
+        p.d = d;
+        p.e0 = d == 0 ? 1 : 0;
+        p.e1 = d == 2 ? 1 : 2;
+        p.deep = h->deep ? 1 : 0;
+        for (int s = 0; s < 2; s++) {
+            p.kind[s] = h->bc[2 * d + s].kind;
+            for (int k = 0; k < 5; k++) p.state[s][k] = h->bc[2 * d + s].state[k];
+        }
+        p.eos = EosD{h->eos.gamma, h->eos.p_inf, h->eos.b, h->eos.q};
+        const int64_t work = h->m[p.e0] * h->m[p.e1] * p.ng;
+        ProfScope ps(h, EMG_K_GHOST);
+        ghost_kernel<<<kernel_grid(work, 256), 256, 0, h->stream>>>(p);
+        EMG_CUDA(cudaGetLastError());
+    }
+    return EMG_OK;
+}
+
+int launch_stage(emg_uniform* h, int stage) {
+    double* in = stage == 1 ? h->u : (stage == 2 ? h->sa : h->sb);
+    int rc = launch_ghosts(h, in);
+    if (rc) return rc;
+    int first_axis = -1, last_axis = -1;
+    for (int d = 0; d < 3; d++)
+        if (h->active[d]) {
+            if (first_axis < 0) first_axis = d;
+            last_axis = d;
+        }
+    for (int d = 0; d < 3; d++) {
+        if (!h->active[d]) continue;
+        SweepParams p{};
+        p.uin = in;
+        p.rhs = h->rhs;
+        p.ctl = h->ctl;
+        p.ncell = h->ncell;
+        const int l = h->lane_axis[d], o = h->other_axis[d];
+        p.sd = h->stride[d];
+        p.sl = h->stride[l];
+        p.so = h->stride[o];
+        p.nd = (int)h->mesh.n[d];
+        p.nl = (int)h->mesh.n[l];
+        p.no = (int)h->mesh.n[o];
+        p.gd = h->active[d] ? (int)h->mesh.ng : 0;
+        p.gl = h->active[l] ? (int)h->mesh.ng : 0;
+        p.go = h->active[o] ? (int)h->mesh.ng : 0;
+        p.d = d;
+        p.seg = h->sweepSeg[d];
+        p.first = d == first_axis;
+        p.last = d == last_axis;
+        p.stage = stage;
+        p.rows_contig = p.sd == 1;
+        p.dx = h->mesh.dx[d];
+        p.ndim = (double)h->ndim;
+        p.positivity = h->opts.positivity ? 1 : 0;
+        p.eos = EosD{h->eos.gamma, h->eos.p_inf, h->eos.b, h->eos.q};
+        if (p.last) {
+            if (stage == 1) {
+                p.base = h->u;
+                p.cur = nullptr;
+                p.dest = h->sa;
+            } else if (stage == 2) {
+                p.base = h->u;
+                p.cur = h->sa;
+                p.dest = h->sb;
+            } else {
+                p.base = h->sb;
+                p.cur = h->u;
+                p.dest = h->u;
+                p.cfl_fuse = 1;
+                for (int k = 0; k < 3; k++) {
+                    p.cfl_active[k] = h->active[k];
+                    p.cfl_dx[k] = h->mesh.dx[k];
+                }
+            }
+        }
+        ProfScope ps(h, EMG_K_AXIS_0 + d);
+        cudaError_t e = h->opts.precision == EMG_PRECISION_MIXED
+                            ? sweep_launch_mixed(h->sweepP[d], p, h->sweepGrid[d], h->stream)
+                            : sweep_launch_f64(h->sweepP[d], p, h->sweepGrid[d], h->stream);
+        if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("sweep launch: ") + cudaGetErrorString(e));
+    }
+    return EMG_OK;
+}
+
+int launch_step_body(emg_uniform* h) {
+    for (int s = 1; s <= 3; s++) {
+        int rc = launch_stage(h, s);
+        if (rc) return rc;
+    }
+    {
+        ProfScope ps(h, EMG_K_CFL);
+        ctl_end<<<1, 1, 0, h->stream>>>(h->ctl);
+        EMG_CUDA(cudaGetLastError());
+    }
+    // host-side face statistics (every face of every pencil, each stage)
+    uint64_t f = 0;
+    for (int d = 0; d < 3; d++)
+        if (h->active[d]) f += (uint64_t)(h->cells / h->mesh.n[d]) * (uint64_t)(h->mesh.n[d] + 1);
+    h->faces += 3 * f;
+    if (h->opts.mode == EMG_MODE_WENO) h->weno_faces += 3 * f;
+    return EMG_OK;
+}
+
+int ensure_rate(emg_uniform* h) {
+    if (h->rate_valid) return EMG_OK;
+    ctl_reset_rate<<<1, 1, 0, h->stream>>>(h->ctl);
+    EMG_CUDA(cudaGetLastError());
+    CellRange cr{};
+    for (int d = 0; d < 3; d++) {
+        cr.n[d] = h->mesh.n[d];
+        cr.g[d] = h->active[d] ? h->mesh.ng : 0;
+        cr.stride[d] = h->stride[d];
+    }
+    cr.cells = h->cells;
+    {
+        ProfScope ps(h, EMG_K_CFL);
+        cfl_kernel<<<kernel_grid(h->cells, 256), 256, 0, h->stream>>>(
+            h->u, h->ncell, cr, h->active[0], h->active[1], h->active[2], h->mesh.dx[0], h->mesh.dx[1], h->mesh.dx[2],
+            EosD{h->eos.gamma, h->eos.p_inf, h->eos.b, h->eos.q}, h->ctl);
+        EMG_CUDA(cudaGetLastError());
+    }
+    h->rate_valid = true;
+    return EMG_OK;
+}
+
+int sync_ctl(emg_uniform* h) {
+    EMG_CUDA(cudaMemcpyAsync(h->ctl_host, h->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, h->stream));
+    EMG_CUDA(cudaStreamSynchronize(h->stream));
+    h->t_host = h->ctl_host->t;
+    return EMG_OK;
+}
+
+double bits_to_double(unsigned long long b) {
+    double v;
+    std::memcpy(&v, &b, sizeof v);
+    return v;
+}
+
+int check_handle(emg_uniform* h) {
+    if (!h) return set_error(EMG_ERR_INVALID, "null handle");
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    return EMG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* emg_last_error(void) { return g_last_error.c_str(); }
+
+const char* emg_version(void) { return "0.1.0"; }
+
+int emg_device_count(int* count) {
+    if (!count) return set_error(EMG_ERR_INVALID, "null count");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        *count = 0;
+        cudaGetLastError();
+        return EMG_OK;
+    }
+    int c = 0;
+    for (int i = 0; i < n; i++) {
+        cudaDeviceProp pr;
+        if (cudaGetDeviceProperties(&pr, i) == cudaSuccess && pr.major == 10) c++;
+    }
+    *count = c;
+    return EMG_OK;
+}
+
+int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
+                       const double* u_aos, size_t len, emg_uniform** out) {
+    if (!mesh || !eos || !bc || !opts || !u_aos || !out) return set_error(EMG_ERR_INVALID, "null argument");
+    *out = nullptr;
+    int dev = 0;
+    {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+            cudaGetLastError();
+            return set_error(EMG_ERR_NO_DEVICE, "no CUDA device visible");
+        }
+        EMG_CUDA(cudaGetDevice(&dev));
+        cudaDeviceProp pr;
+        EMG_CUDA(cudaGetDeviceProperties(&pr, dev));
+        if (pr.major != 10) return set_error(EMG_ERR_NO_DEVICE, "device is not sm_100 (B200)");
+    }
+    if (mesh->ng < 5) return set_error(EMG_ERR_INVALID, "the WCNS stencil needs ng >= 5 ghost layers");
+    int ndim = 0;
+    for (int d = 0; d < 3; d++) {
+        if (mesh->n[d] < 1) return set_error(EMG_ERR_INVALID, "mesh extents must be >= 1");
+        if (mesh->n[d] > 1) {
+            ndim++;
+            if (!(mesh->dx[d] > 0.0)) return set_error(EMG_ERR_INVALID, "dx must be > 0 on active axes");
+            if (mesh->n[d] > (1 << 30)) return set_error(EMG_ERR_INVALID, "axis too long");
+        }
+    }
+    if (ndim == 0) return set_error(EMG_ERR_INVALID, "mesh has no active axis");
+    if (opts->mode != EMG_MODE_WENO)
+        return set_error(EMG_ERR_INVALID, "flux mode not supported by the device kernels (use EMG_MODE_WENO)");
+    if (opts->precision != EMG_PRECISION_F64 && opts->precision != EMG_PRECISION_MIXED)
+        return set_error(EMG_ERR_INVALID, "unknown precision");
+    for (int i = 0; i < 6; i++)
+        if (bc[i].kind < 0 || bc[i].kind > 4) return set_error(EMG_ERR_INVALID, "unknown boundary condition");
+    for (int d = 0; d < 3; d++) {
+        const bool per0 = bc[2 * d].kind == EMG_BC_PERIODIC, per1 = bc[2 * d + 1].kind == EMG_BC_PERIODIC;
+        if (mesh->n[d] > 1 && per0 != per1) return set_error(EMG_ERR_INVALID, "periodic boundaries must be paired");
+    }
+    emg_uniform* h = new emg_uniform();
+    h->device = dev;
+    h->mesh = *mesh;
+    h->eos = *eos;
+    for (int i = 0; i < 6; i++) h->bc[i] = bc[i];
+    h->opts = *opts;
+    h->ndim = ndim;
+    for (int d = 0; d < 3; d++) {
+        h->active[d] = mesh->n[d] > 1;
+        h->m[d] = h->active[d] ? mesh->n[d] + 2 * mesh->ng : 1;
+    }
+    h->stride[2] = 1;
+    h->stride[1] = h->m[2];
+    h->stride[0] = h->m[1] * h->m[2];
+    h->ncell = h->m[0] * h->m[1] * h->m[2];
+    h->cells = mesh->n[0] * mesh->n[1] * mesh->n[2];
+    for (int d = 0; d < 3; d++)
+        if (h->active[d] && mesh->n[d] < mesh->ng &&
+            (bc[2 * d].kind == EMG_BC_REFLECT || bc[2 * d + 1].kind == EMG_BC_REFLECT))
+            h->deep = true;
+    if ((size_t)h->ncell != len) {
+        delete h;
+        return set_error(EMG_ERR_INVALID, "state length does not match the padded mesh");
+    }
+    auto bail = [&](int rc) {
+        emg_uniform_destroy(h);
+        return rc;
+    };
+    static bool prepared[64] = {false};
+    if (dev < 64 && !prepared[dev]) {
+        cudaError_t e = sweep_prepare_f64();
+        if (e == cudaSuccess) e = sweep_prepare_mixed();
+        if (e != cudaSuccess) return bail(set_error(EMG_ERR_CUDA, std::string("sweep setup: ") + cudaGetErrorString(e)));
+        prepared[dev] = true;
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(set_error(EMG_ERR_CUDA, "cudaStreamCreate failed"));
+    const size_t bytes = (size_t)h->ncell * 5 * sizeof(double);
+    if (cudaMalloc(&h->u, bytes) != cudaSuccess || cudaMalloc(&h->sa, bytes) != cudaSuccess ||
+        cudaMalloc(&h->sb, bytes) != cudaSuccess || cudaMalloc(&h->rhs, bytes) != cudaSuccess ||
+        cudaMalloc(&h->staging, bytes) != cudaSuccess || cudaMalloc(&h->partial, 5 * 4096 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&h->ctl, sizeof(StepCtl)) != cudaSuccess ||
+        cudaMallocHost(&h->ctl_host, sizeof(StepCtl)) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(set_error(EMG_ERR_CUDA, "device allocation failed"));
+    }
+    // ghosts of the stage buffers are always rewritten before they are read; zero them once anyway
+    cudaMemsetAsync(h->sa, 0, bytes, h->stream);
+    cudaMemsetAsync(h->sb, 0, bytes, h->stream);
+    cudaMemsetAsync(h->rhs, 0, bytes, h->stream);
+    std::memset(h->ctl_host, 0, sizeof(StepCtl));
+    h->ctl_host->t_end = INFINITY;
+    if (cudaMemcpyAsync(h->ctl, h->ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
+        return bail(set_error(EMG_ERR_CUDA, "control block upload failed"));
+    plan_sweeps(h);
+    for (int d = 0; d < 3; d++)
+        if (h->active[d] && (h->sweepGrid[d].y > 65535u || h->sweepGrid[d].z > 65535u))
+            return bail(set_error(EMG_ERR_INVALID, "mesh too large for the sweep grid (an axis above 65535 pencils)"));
+    int rc = emg_uniform_upload(h, u_aos, len);
+    if (rc) return bail(rc);
+    *out = h;
+    return EMG_OK;
+}
+
+int emg_uniform_destroy(emg_uniform* h) {
+    if (!h) return EMG_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->u);
+    cudaFree(h->sa);
+    cudaFree(h->sb);
+    cudaFree(h->rhs);
+    cudaFree(h->staging);
+    cudaFree(h->partial);
+    cudaFree(h->ctl);
+    if (h->ctl_host) cudaFreeHost(h->ctl_host);
+    for (auto& r : h->recs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : h->pool) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return EMG_OK;
+}
+
+int emg_uniform_upload(emg_uniform* h, const double* u_aos, size_t len) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!u_aos || len != (size_t)h->ncell) return set_error(EMG_ERR_INVALID, "state length does not match the padded mesh");
+    const size_t bytes = (size_t)h->ncell * 5 * sizeof(double);
+    EMG_CUDA(cudaMemcpyAsync(h->staging, u_aos, bytes, cudaMemcpyHostToDevice, h->stream));
+    aos_to_soa<<<kernel_grid(h->ncell, 256), 256, 0, h->stream>>>(h->staging, h->u, h->ncell);
+    EMG_CUDA(cudaGetLastError());
+    h->launches++;
+    EMG_CUDA(cudaStreamSynchronize(h->stream));
+    h->rate_valid = false;
+    return EMG_OK;
+}
+
+int emg_uniform_download(emg_uniform* h, double* u_aos, size_t len) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!u_aos || len != (size_t)h->ncell) return set_error(EMG_ERR_INVALID, "state length does not match the padded mesh");
+    soa_to_aos<<<kernel_grid(h->ncell, 256), 256, 0, h->stream>>>(h->u, h->staging, h->ncell);
+    EMG_CUDA(cudaGetLastError());
+    h->launches++;
+    EMG_CUDA(cudaMemcpyAsync(u_aos, h->staging, (size_t)h->ncell * 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    EMG_CUDA(cudaStreamSynchronize(h->stream));
+    return EMG_OK;
+}
+
+int emg_uniform_step(emg_uniform* h, double dt) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    ctl_begin_host<<<1, 1, 0, h->stream>>>(h->ctl, dt);
+    EMG_CUDA(cudaGetLastError());
+    h->launches++;
+    rc = launch_step_body(h);
+    if (rc) return rc;
+    h->rate_valid = true;
+    return sync_ctl(h);
+}
+
+int emg_uniform_dt_cfl(emg_uniform* h, double* dt) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!dt) return set_error(EMG_ERR_INVALID, "null dt");
+    rc = ensure_rate(h);
+    if (rc) return rc;
+    rc = sync_ctl(h);
+    if (rc) return rc;
+    const double rate = bits_to_double(h->ctl_host->rate_bits);
+    *dt = h->opts.cfl / rate;
+    return EMG_OK;
+}
+
+int emg_uniform_advance(emg_uniform* h, uint64_t nsteps, double t_end, uint64_t* taken) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    rc = ensure_rate(h);
+    if (rc) return rc;
+    // arm device-driven stepping
+    rc = sync_ctl(h);
+    if (rc) return rc;
+    StepCtl c = *h->ctl_host;
+    c.t_end = t_end;
+    c.done = 0;
+    c.status = 0;
+    const uint64_t steps0 = c.steps;
+    EMG_CUDA(cudaMemcpyAsync(h->ctl, &c, sizeof(StepCtl), cudaMemcpyHostToDevice, h->stream));
+    EMG_CUDA(cudaStreamSynchronize(h->stream));
+    const bool bounded = !std::isinf(t_end);
+    uint64_t issued = 0;
+    while (issued < nsteps) {
+        const uint64_t batch = bounded ? std::min<uint64_t>(nsteps - issued, 8) : nsteps - issued;
+        for (uint64_t s = 0; s < batch; s++) {
+            ctl_begin_device<<<1, 1, 0, h->stream>>>(h->ctl, h->opts.cfl);
+            EMG_CUDA(cudaGetLastError());
+            h->launches++;
+            rc = launch_step_body(h);
+            if (rc) return rc;
+        }
+        issued += batch;
+        if (bounded) {
+            rc = sync_ctl(h);
+            if (rc) return rc;
+            if (h->ctl_host->done) break;
+        }
+    }
+    rc = sync_ctl(h);
+    if (rc) return rc;
+    // face statistics were counted for every issued step; correct for skipped ones
+    const uint64_t done_steps = h->ctl_host->steps - steps0;
+    if (issued > done_steps) {
+        uint64_t f = 0;
+        for (int d = 0; d < 3; d++)
+            if (h->active[d]) f += (uint64_t)(h->cells / h->mesh.n[d]) * (uint64_t)(h->mesh.n[d] + 1);
+        h->faces -= 3 * f * (issued - done_steps);
+        if (h->opts.mode == EMG_MODE_WENO) h->weno_faces -= 3 * f * (issued - done_steps);
+    }
+    if (taken) *taken = done_steps;
+    h->rate_valid = true;
+    if (h->ctl_host->status) {
+        const int st = h->ctl_host->status;
+        return set_error(st, st == EMG_ERR_DT_COLLAPSED ? "time step collapsed: the solution lost admissibility"
+                                                        : "device error");
+    }
+    return EMG_OK;
+}
+
+int emg_uniform_run_to(emg_uniform* h, double t_end, uint64_t* steps) {
+    if (!std::isfinite(t_end)) return set_error(EMG_ERR_INVALID, "t_end must be finite");
+    uint64_t taken = 0;
+    int rc = emg_uniform_advance(h, UINT64_MAX / 2, t_end, &taken);
+    if (steps) *steps = taken;
+    return rc;
+}
+
+int emg_uniform_totals(emg_uniform* h, double out[5]) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!out) return set_error(EMG_ERR_INVALID, "null out");
+    CellRange cr{};
+    double vol = 1.0;
+    for (int d = 0; d < 3; d++) {
+        cr.n[d] = h->mesh.n[d];
+        cr.g[d] = h->active[d] ? h->mesh.ng : 0;
+        cr.stride[d] = h->stride[d];
+        if (h->active[d]) vol = vol * h->mesh.dx[d];
+    }
+    cr.cells = h->cells;
+    const int nb = (int)std::min<int64_t>(4095, std::max<int64_t>(1, (h->cells + 255) / 256));
+    totals_partial<<<nb, 256, 0, h->stream>>>(h->u, h->ncell, cr, vol, h->partial);
+    EMG_CUDA(cudaGetLastError());
+    totals_final<<<1, 32, 0, h->stream>>>(h->partial, nb, h->partial + 5 * 4095);
+    EMG_CUDA(cudaGetLastError());
+    h->launches += 2;
+    EMG_CUDA(cudaMemcpyAsync(out, h->partial + 5 * 4095, 5 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    EMG_CUDA(cudaStreamSynchronize(h->stream));
+    return EMG_OK;
+}
+
+int emg_uniform_counters(emg_uniform* h, uint64_t out[4]) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!out) return set_error(EMG_ERR_INVALID, "null out");
+    rc = sync_ctl(h);
+    if (rc) return rc;
+    out[0] = h->faces;
+    out[1] = h->weno_faces;
+    out[2] = h->ctl_host->counters[2];
+    out[3] = h->ctl_host->counters[3];
+    return EMG_OK;
+}
+
+int emg_uniform_get_time(emg_uniform* h, double* t) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    if (!t) return set_error(EMG_ERR_INVALID, "null t");
+    rc = sync_ctl(h);
+    if (rc) return rc;
+    *t = h->ctl_host->t;
+    return EMG_OK;
+}
+
+int emg_uniform_set_time(emg_uniform* h, double t) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    rc = sync_ctl(h);
+    if (rc) return rc;
+    h->ctl_host->t = t;
+    EMG_CUDA(cudaMemcpyAsync(h->ctl, h->ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice, h->stream));
+    EMG_CUDA(cudaStreamSynchronize(h->stream));
+    return EMG_OK;
+}
+
+int emg_uniform_synchronize(emg_uniform* h) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    EMG_CUDA(cudaStreamSynchronize(h->stream));
+    return EMG_OK;
+}
+
+int emg_uniform_stream(emg_uniform* h, void** stream) {
+    if (!h || !stream) return set_error(EMG_ERR_INVALID, "null argument");
+    *stream = (void*)h->stream;
+    return EMG_OK;
+}
+
+int emg_uniform_set_profiling(emg_uniform* h, int on) {
+    if (!h) return set_error(EMG_ERR_INVALID, "null handle");
+    h->profiling = on != 0;
+    return EMG_OK;
+}
+
+int emg_uniform_kernel_times(emg_uniform* h, double* ms, uint64_t* launches) {
+    int rc = check_handle(h);
+    if (rc) return rc;
+    EMG_CUDA(cudaStreamSynchronize(h->stream));
+    for (auto& r : h->recs) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, r.a, r.b);
+        h->prof_ms[r.kind] += t;
+        h->prof_n[r.kind] += 1;
+        h->pool.push_back(r.a);
+        h->pool.push_back(r.b);
+    }
+    h->recs.clear();
+    for (int k = 0; k < EMG_K_COUNT; k++) {
+        if (ms) ms[k] = h->prof_ms[k];
+        if (launches) launches[k] = h->prof_n[k];
+        h->prof_ms[k] = 0.0;
+        h->prof_n[k] = 0;
+    }
+    return EMG_OK;
+}
+
+int emg_uniform_launch_count(emg_uniform* h, uint64_t* launches) {
+    if (!h || !launches) return set_error(EMG_ERR_INVALID, "null argument");
+    *launches = h->launches;
+    return EMG_OK;
+}
+
+}  // extern "C"

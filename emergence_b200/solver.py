@@ -1,0 +1,184 @@
+"""GpuSolver: the device solver of one uniform grid, mirroring
+compressible-cuda's ``GpuSolver`` (fluid/crates/compressible-cuda/src/
+lib.rs:155-477) and the stepping API of ``compressible::Solver``
+(fluid/crates/compressible/src/solver.rs:139-795).
+
+All work runs in ``libemergence_b200.so`` on the current CUDA device; this
+module only marshals arguments through the C ABI.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _abi
+from ._abi import EmgBc, EmgEos, EmgMesh, EmgOpts, check, lib
+from .physics import Bc, FluxMode, Precision
+
+
+def _c_mesh(mesh):
+    m = EmgMesh()
+    for d in range(3):
+        m.n[d] = mesh.n[d]
+        m.lo[d] = mesh.lo[d]
+        m.dx[d] = mesh.dx[d]
+    m.ng = mesh.ng
+    return m
+
+
+def _c_eos(eos):
+    return EmgEos(eos.gamma, eos.p_inf, eos.b, eos.q, eos.cv)
+
+
+def _c_bcs(bc):
+    arr = (EmgBc * 6)()
+    for d in range(3):
+        for s in range(2):
+            b = bc[d][s]
+            arr[2 * d + s].kind = b.kind
+            for k in range(5):
+                arr[2 * d + s].state[k] = b.state[k]
+    return arr
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class GpuSolver:
+    """Device solver of a ghost-padded conserved state.
+
+    ``GpuSolver(sys, mesh, u, bc=..., cfl=0.5, mode=FluxMode.Weno, tol=1e-3,
+    positivity=True, precision=Precision.F64)`` uploads ``u`` (float64
+    ``[mesh.len(), 5]``) like ``GpuSolver::from_cpu``.
+    """
+
+    def __init__(self, sys, mesh, u, bc=None, cfl=0.5, mode=FluxMode.Weno, tol=1e-3, positivity=True,
+                 precision=Precision.F64):
+        self.sys = sys
+        self.mesh = mesh
+        self.bc = bc if bc is not None else [[Bc.Periodic, Bc.Periodic] for _ in range(3)]
+        self.cfl = cfl
+        self.mode = mode
+        self.tol = tol
+        self.positivity = positivity
+        self.precision = precision
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        if u.shape != (mesh.len(), 5):
+            raise ValueError(f"state must have shape {(mesh.len(), 5)}, got {u.shape}")
+        self._m = _c_mesh(mesh)
+        self._e = _c_eos(sys.eos)
+        self._b = _c_bcs(self.bc)
+        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, precision, 0)
+        h = C.c_void_p()
+        check(lib().emg_uniform_create(C.byref(self._m), C.byref(self._e), self._b, C.byref(self._o), _dptr(u),
+                                       mesh.len(), C.byref(h)))
+        self._h = h
+
+    @classmethod
+    def from_cpu(cls, cpu, precision=Precision.F64):
+        """Build from any object with the fields of ``compressible::Solver``
+        (sys, mesh, u, bc, cfl, mode, tol, positivity, t)."""
+        s = cls(cpu.sys, cpu.mesh, cpu.u, bc=cpu.bc, cfl=cpu.cfl, mode=cpu.mode, tol=cpu.tol,
+                positivity=cpu.positivity, precision=precision)
+        if getattr(cpu, "t", 0.0):
+            s.t = cpu.t
+        return s
+
+    # ---- lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().emg_uniform_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- stepping (Solver / GpuSolver API)
+    def step(self, dt):
+        check(lib().emg_uniform_step(self._h, float(dt)))
+
+    def dt_cfl(self):
+        v = C.c_double()
+        check(lib().emg_uniform_dt_cfl(self._h, C.byref(v)))
+        return v.value
+
+    def run_to(self, t_end):
+        n = C.c_uint64()
+        check(lib().emg_uniform_run_to(self._h, float(t_end), C.byref(n)))
+        return n.value
+
+    def advance(self, nsteps, t_end=math.inf):
+        """Take up to ``nsteps`` CFL steps with dt computed on the device."""
+        n = C.c_uint64()
+        check(lib().emg_uniform_advance(self._h, int(nsteps), float(t_end), C.byref(n)))
+        return n.value
+
+    # ---- state
+    def download(self):
+        out = np.empty((self.mesh.len(), 5), dtype=np.float64)
+        check(lib().emg_uniform_download(self._h, _dptr(out), self.mesh.len()))
+        return out
+
+    def upload(self, u):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        check(lib().emg_uniform_upload(self._h, _dptr(u), self.mesh.len()))
+
+    def totals(self):
+        out = np.empty(5, dtype=np.float64)
+        check(lib().emg_uniform_totals(self._h, _dptr(out)))
+        return out
+
+    def counters(self):
+        """[faces, shock-path faces, first-order fallbacks, limited faces]."""
+        out = (C.c_uint64 * 4)()
+        check(lib().emg_uniform_counters(self._h, out))
+        return list(out)
+
+    @property
+    def t(self):
+        v = C.c_double()
+        check(lib().emg_uniform_get_time(self._h, C.byref(v)))
+        return v.value
+
+    @t.setter
+    def t(self, value):
+        check(lib().emg_uniform_set_time(self._h, float(value)))
+
+    def synchronize(self):
+        check(lib().emg_uniform_synchronize(self._h))
+
+    def stream(self):
+        p = C.c_void_p()
+        check(lib().emg_uniform_stream(self._h, C.byref(p)))
+        return p.value
+
+    def set_profiling(self, on=True):
+        check(lib().emg_uniform_set_profiling(self._h, 1 if on else 0))
+
+    def kernel_times(self):
+        """{kind: (ms, launches)} accumulated since the last call."""
+        ms = (C.c_double * _abi.EMG_K_COUNT)()
+        n = (C.c_uint64 * _abi.EMG_K_COUNT)()
+        check(lib().emg_uniform_kernel_times(self._h, ms, n))
+        return {k: (ms[i], n[i]) for i, k in enumerate(_abi.KERNEL_KINDS)}
+
+    def launch_count(self):
+        n = C.c_uint64()
+        check(lib().emg_uniform_launch_count(self._h, C.byref(n)))
+        return n.value
+
+
+def device_count():
+    n = C.c_int()
+    check(lib().emg_device_count(C.byref(n)))
+    return n.value

@@ -1,0 +1,196 @@
+/*
+ * emergence_b200 — B200-native (sm_100a) compressible-Euler step: C ABI.
+ *
+ * This is the drop-in boundary for the explicit finite-volume step of the
+ * emergence workspace's `compressible` crate (characteristic WENO5-Z / WCNS
+ * reconstruction, HLLC flux, Hu–Adams–Shu positivity limiter, SSP-RK3
+ * stages, ghost fill and the CFL max-wavespeed reduction). Each entry point
+ * names the reference interface it replaces (paths relative to the
+ * reference repository; `G/` = fluid/crates/compressible-cuda/src,
+ * `C/` = fluid/crates/compressible/src).
+ *
+ * Conventions
+ *  - Plain C types only: pointers, sizes, doubles, fixed-width integers.
+ *  - Every function returns an `int` status: EMG_OK (0) or an EMG_ERR_* code.
+ *    `emg_last_error()` returns a thread-local message for the last failure.
+ *    Nothing aborts or traps.
+ *  - Host state layout (what `create` takes and `download` returns) is the
+ *    reference CPU layout: array-of-structures `double[len][5]` of conserved
+ *    variables (ρ, ρu, ρv, ρw, E), ghost-padded with `ng` layers on active
+ *    axes only, last axis contiguous: cell (i,j,k) (padded indices) sits at
+ *    `(i*m1 + j)*m2 + k` with `m_d = n_d + 2 ng` on active axes, 1 otherwise
+ *    (C/solver.rs:22-86).
+ *  - A handle owns its device memory and one CUDA stream; caller buffers are
+ *    only borrowed for the duration of a call. Handles are not thread-safe;
+ *    distinct handles may be used concurrently from different threads.
+ */
+#ifndef EMERGENCE_B200_H
+#define EMERGENCE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+enum emg_status {
+    EMG_OK = 0,
+    EMG_ERR_INVALID = 1,      /* invalid argument (null pointer, size mismatch, unsupported option) */
+    EMG_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    EMG_ERR_DT_COLLAPSED = 3, /* time step not finite or ≤ 1e-12·|t_end| (C/solver.rs:763, G/lib.rs:447) */
+    EMG_ERR_INADMISSIBLE = 4, /* non-finite or inadmissible state met by the CFL reduction */
+    EMG_ERR_UNFILLABLE = 5,   /* AMR ghost cell with no source (G/kernels.cu:845-848) */
+    EMG_ERR_BOUNDS = 6,       /* device-side bounds check failed */
+    EMG_ERR_NO_DEVICE = 7,    /* no CUDA device of compute capability 10.x visible */
+    EMG_ERR_TIMEOUT = 8       /* a bounded device-side wait ran out */
+};
+
+/* ------------------------------------------------------------------ types */
+/* Noble–Abel stiffened-gas EOS (C/eos.rs:12-25). Ideal gas: p_inf = b = q = 0. */
+typedef struct emg_eos {
+    double gamma;
+    double p_inf;
+    double b;
+    double q;
+    double cv;
+} emg_eos;
+
+/* Uniform mesh (C/solver.rs:22-28): n cells per axis (1 = inactive axis),
+ * lower corner, cell size, ghost layers (≥ 5 for the WCNS path). */
+typedef struct emg_mesh {
+    int64_t n[3];
+    double lo[3];
+    double dx[3];
+    int64_t ng;
+} emg_mesh;
+
+/* Boundary conditions (C/solver.rs:8-20). `state` is the conserved
+ * Dirichlet / far-field state (ignored by the other kinds). */
+enum emg_bc_kind {
+    EMG_BC_PERIODIC = 0,
+    EMG_BC_OUTFLOW = 1, /* zero-gradient extrapolation (transmissive) */
+    EMG_BC_REFLECT = 2,
+    EMG_BC_DIRICHLET = 3,
+    EMG_BC_CHARACTERISTIC = 4
+};
+typedef struct emg_bc {
+    int32_t kind;
+    int32_t reserved;
+    double state[5];
+} emg_bc;
+
+/* Flux modes (C/scheme.rs:39-47). */
+enum emg_flux_mode { EMG_MODE_HYBRID = 0, EMG_MODE_WENO = 1, EMG_MODE_CENTRAL = 2 };
+
+/* Arithmetic of the flux evaluation. The conserved state, the RK stage
+ * accumulation and the conservation sums are always f64. */
+enum emg_precision {
+    EMG_PRECISION_F64 = 0,  /* plain FP64 form: all scheme arithmetic in f64 */
+    EMG_PRECISION_MIXED = 1 /* FP32 reconstruction / HLLC / central flux; FP64 state, pressure recovery, limiter checks */
+};
+
+/* Scheme knobs mirroring the public fields of `Solver` (C/solver.rs:139-160). */
+typedef struct emg_opts {
+    double cfl;         /* CFL number (0.5 in the reference) */
+    double tol;         /* hybrid sensor tolerance (1e-3) */
+    int32_t mode;       /* emg_flux_mode */
+    int32_t positivity; /* Hu–Adams–Shu limiter on/off (1) */
+    int32_t precision;  /* emg_precision */
+    int32_t reserved;
+} emg_opts;
+
+/* ------------------------------------------------------------------ misc */
+
+/* Message of the last failed call on this thread ("" if none). */
+const char* emg_last_error(void);
+
+/* Library version as "major.minor.patch". */
+const char* emg_version(void);
+
+/* Number of visible sm_100 devices. */
+int emg_device_count(int* count);
+
+/* ------------------------------------------------------------------ uniform grids */
+typedef struct emg_uniform emg_uniform;
+
+/* Upload a ghost-padded AoS conserved state and build a device solver on the
+ * current CUDA device. Replaces `GpuSolver::<f64|f32>::from_cpu(&Solver,
+ * GpuSystem::Euler(eos))` (G/lib.rs:184-282). `bc` is [axis][side] flattened
+ * (6 entries); `len` counts cells (not doubles) and must equal the padded
+ * cell count of `mesh`. Time starts at 0. */
+int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
+                       const double* u_aos, size_t len, emg_uniform** out);
+
+/* Free the handle and its device memory (Drop of GpuSolver). */
+int emg_uniform_destroy(emg_uniform* h);
+
+/* One SSP-RK3 step of size dt (G/lib.rs:402-412; C/solver.rs:659-738). */
+int emg_uniform_step(emg_uniform* h, double dt);
+
+/* CFL time step cfl / max_cells Σ_d (|u_d|+c)/dx_d (G/lib.rs:415-441; C/solver.rs:478-523). */
+int emg_uniform_dt_cfl(emg_uniform* h, double* dt);
+
+/* Advance to t_end with CFL steps (G/lib.rs:443-455; C/solver.rs:758-768).
+ * The step count is written to *steps. Stops within 1e-10·|t_end| of t_end. */
+int emg_uniform_run_to(emg_uniform* h, double t_end, uint64_t* steps);
+
+/* Take `nsteps` CFL steps, each with dt = min(dt_cfl, t_end − t) computed on
+ * the device (no host round trip per step), stopping early at t_end. Pass
+ * t_end = +inf for a fixed number of steps. The number of steps actually
+ * taken is written to *taken (may be NULL). New in this library: the
+ * reference's `run_to` reads dt back to the host every step (G/lib.rs:430). */
+int emg_uniform_advance(emg_uniform* h, uint64_t nsteps, double t_end, uint64_t* taken);
+
+/* Download the full padded AoS state, ghosts included (G/lib.rs:457-461). */
+int emg_uniform_download(emg_uniform* h, double* u_aos, size_t len);
+
+/* Replace the device state by a padded AoS host state (time unchanged). */
+int emg_uniform_upload(emg_uniform* h, const double* u_aos, size_t len);
+
+/* Conserved totals Σ u·vol over interior cells (C/solver.rs:784-794), in f64. */
+int emg_uniform_totals(emg_uniform* h, double out[5]);
+
+/* Face statistics since creation: [faces, shock-path faces, first-order
+ * fallbacks, positivity-limited faces] (C/scheme.rs:101-117; G/lib.rs:464-467
+ * reports the last three). */
+int emg_uniform_counters(emg_uniform* h, uint64_t out[4]);
+
+/* Simulation time t (Solver::t). */
+int emg_uniform_get_time(emg_uniform* h, double* t);
+int emg_uniform_set_time(emg_uniform* h, double t);
+
+/* Block until the handle's stream is idle (G/lib.rs:469-472). */
+int emg_uniform_synchronize(emg_uniform* h);
+
+/* The handle's CUDA stream (cudaStream_t) as an opaque pointer. */
+int emg_uniform_stream(emg_uniform* h, void** stream);
+
+/* Per-kernel CUDA-event timing of subsequent launches: on = 1 enables. Times
+ * accumulate per kernel kind until read with emg_uniform_kernel_times. */
+int emg_uniform_set_profiling(emg_uniform* h, int on);
+
+/* Kernel kinds reported by emg_uniform_kernel_times. */
+enum emg_kernel_kind {
+    EMG_K_GHOST = 0,   /* ghost-layer fill, one launch per active axis per stage */
+    EMG_K_AXIS_0 = 1,  /* fused WCNS/HLLC/limiter/divergence sweep along axis 0 */
+    EMG_K_AXIS_1 = 2,
+    EMG_K_AXIS_2 = 3,
+    EMG_K_CFL = 4,     /* CFL reduction and device dt */
+    EMG_K_COUNT = 5
+};
+
+/* Accumulated device milliseconds and launch counts per kernel kind since the
+ * last call (synchronizes the stream; resets the accumulators).
+ * `ms` and `launches` hold EMG_K_COUNT entries each. */
+int emg_uniform_kernel_times(emg_uniform* h, double* ms, uint64_t* launches);
+
+/* Number of kernel launches issued by the handle since creation. */
+int emg_uniform_launch_count(emg_uniform* h, uint64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EMERGENCE_B200_H */

@@ -1,0 +1,276 @@
+// CPU ORACLE — test infrastructure only (see oracle.hpp).
+//
+// C entry points over the C++ restatement of the reference CPU solver, with
+// the same argument types as the product ABI in include/emergence_b200.h, so
+// the tests drive the oracle and the CUDA library through identical calls.
+// Loaded only by tests/, __graft_entry__.smoke() and bench.py's CPU leg.
+#include "oracle.hpp"
+#include "../include/emergence_b200.h"
+
+#include <cstdio>
+#include <string>
+
+using namespace oracle;
+
+namespace {
+thread_local std::string g_err;
+int fail(int code, const char* msg) {
+    g_err = msg;
+    return code;
+}
+struct Handle {
+    Solver<double> s;
+    Handle(const Euler<double>& sys, const Mesh& m) : s(sys, m) {}
+};
+Mesh to_mesh(const emg_mesh* m) {
+    Mesh r;
+    for (int d = 0; d < 3; d++) {
+        r.n[d] = m->n[d];
+        r.lo[d] = m->lo[d];
+        r.dx[d] = m->dx[d];
+    }
+    r.ng = m->ng;
+    return r;
+}
+Euler<double> to_sys(const emg_eos* e) { return Euler<double>{Nasg<double>{e->gamma, e->p_inf, e->b, e->q, e->cv}}; }
+}  // namespace
+
+extern "C" {
+
+const char* emgo_last_error(void) { return g_err.c_str(); }
+
+int emgo_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+void emgo_set_num_threads(int n) {
+#ifdef _OPENMP
+    omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+int emgo_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
+                        const double* u_aos, size_t len, void** out) {
+    if (!mesh || !eos || !bc || !opts || !u_aos || !out) return fail(EMG_ERR_INVALID, "null argument");
+    Mesh m = to_mesh(mesh);
+    if ((size_t)m.len() != len) return fail(EMG_ERR_INVALID, "state length does not match the padded mesh");
+    Handle* h = new Handle(to_sys(eos), m);
+    for (int d = 0; d < 3; d++)
+        for (int s = 0; s < 2; s++) {
+            h->s.bc[d][s].kind = bc[2 * d + s].kind;
+            for (int k = 0; k < 5; k++) h->s.bc[d][s].state[k] = bc[2 * d + s].state[k];
+        }
+    h->s.cfl = opts->cfl;
+    h->s.tol = opts->tol;
+    h->s.mode = opts->mode;
+    h->s.positivity = opts->positivity != 0;
+    std::memcpy(h->s.u.data(), u_aos, len * 5 * sizeof(double));
+    *out = h;
+    return EMG_OK;
+}
+int emgo_uniform_destroy(void* h) {
+    delete (Handle*)h;
+    return EMG_OK;
+}
+int emgo_uniform_step(void* h, double dt) {
+    ((Handle*)h)->s.step(dt);
+    return EMG_OK;
+}
+int emgo_uniform_dt_cfl(void* h, double* dt) {
+    *dt = ((Handle*)h)->s.dt_cfl();
+    return EMG_OK;
+}
+int emgo_uniform_run_to(void* h, double t_end, uint64_t* steps) {
+    int64_t n = ((Handle*)h)->s.run_to(t_end);
+    if (n < 0) return fail(EMG_ERR_DT_COLLAPSED, "time step collapsed");
+    if (steps) *steps = (uint64_t)n;
+    return EMG_OK;
+}
+int emgo_uniform_download(void* h, double* u_aos, size_t len) {
+    Handle* hh = (Handle*)h;
+    if (len != hh->s.u.size()) return fail(EMG_ERR_INVALID, "length mismatch");
+    std::memcpy(u_aos, hh->s.u.data(), len * 5 * sizeof(double));
+    return EMG_OK;
+}
+int emgo_uniform_upload(void* h, const double* u_aos, size_t len) {
+    Handle* hh = (Handle*)h;
+    if (len != hh->s.u.size()) return fail(EMG_ERR_INVALID, "length mismatch");
+    std::memcpy(hh->s.u.data(), u_aos, len * 5 * sizeof(double));
+    return EMG_OK;
+}
+int emgo_uniform_totals(void* h, double out[5]) {
+    V5<double> t = ((Handle*)h)->s.totals();
+    for (int k = 0; k < 5; k++) out[k] = t[k];
+    return EMG_OK;
+}
+int emgo_uniform_counters(void* h, uint64_t out[4]) {
+    Stats& s = ((Handle*)h)->s.stats;
+    out[0] = s.faces;
+    out[1] = s.weno_faces;
+    out[2] = s.fallback_faces;
+    out[3] = s.limited_faces;
+    return EMG_OK;
+}
+int emgo_uniform_get_time(void* h, double* t) {
+    *t = ((Handle*)h)->s.t;
+    return EMG_OK;
+}
+int emgo_uniform_set_time(void* h, double t) {
+    ((Handle*)h)->s.t = t;
+    return EMG_OK;
+}
+// Ghost fill of the handle's own state (C/solver.rs:252-348).
+int emgo_uniform_fill_ghosts(void* h) {
+    Handle* hh = (Handle*)h;
+    hh->s.fill_ghosts(hh->s.u);
+    return EMG_OK;
+}
+// Ghost fill of a caller array with the handle's mesh and boundary conditions.
+int emgo_uniform_fill_ghosts_of(void* h, double* u_aos, size_t len) {
+    Handle* hh = (Handle*)h;
+    if (len != hh->s.u.size()) return fail(EMG_ERR_INVALID, "length mismatch");
+    std::vector<V5<double>> tmp(len);
+    std::memcpy(tmp.data(), u_aos, len * 5 * sizeof(double));
+    hh->s.fill_ghosts(tmp);
+    std::memcpy(u_aos, tmp.data(), len * 5 * sizeof(double));
+    return EMG_OK;
+}
+
+// ---- unit-level entry points (scheme / boundary / physics)
+
+// Face fluxes of one line of primitive states (C/scheme.rs:132-281).
+int emgo_line_fluxes(const emg_eos* eos, const double* w, int len, int d, int ng, int mode, double tol, double lambda,
+                     double* out, double* uface, uint64_t stats[4]) {
+    Euler<double> sys = to_sys(eos);
+    SchemeOpts o{mode, tol, lambda};
+    Stats s;
+    line_fluxes(sys, (const V5<double>*)w, len, d, ng, o, (V5<double>*)out, uface, s);
+    stats[0] = s.faces;
+    stats[1] = s.weno_faces;
+    stats[2] = s.fallback_faces;
+    stats[3] = s.limited_faces;
+    return EMG_OK;
+}
+
+// Positivity limiter on given face fluxes (C/scheme.rs:395-464).
+int emgo_positivity_limit(const emg_eos* eos, const double* w, int len, int d, int ng, double lambda, double* out,
+                          double* uface, uint64_t* limited) {
+    Euler<double> sys = to_sys(eos);
+    Stats s;
+    positivity_limit(sys, (const V5<double>*)w, len, d, ng, lambda, (V5<double>*)out, uface, s);
+    *limited = s.limited_faces;
+    return EMG_OK;
+}
+
+// Midpoint flux between cells j and j+1 of a primitive line (C/scheme.rs:286-333).
+int emgo_midpoint_flux(const emg_eos* eos, const double* w, int j, int d, double f[5], double* us, int* fb) {
+    Euler<double> sys = to_sys(eos);
+    MidResult<double> m = midpoint_flux(sys, (const V5<double>*)w, j, d);
+    for (int k = 0; k < 5; k++) f[k] = m.f[k];
+    *us = m.us;
+    *fb = m.fb;
+    return EMG_OK;
+}
+
+// HLLC flux (C/system.rs:260-312).
+int emgo_riemann_flux(const emg_eos* eos, const double wl[5], const double wr[5], int d, double f[5], double* ss) {
+    Euler<double> sys = to_sys(eos);
+    V5<double> a, b;
+    for (int k = 0; k < 5; k++) {
+        a[k] = wl[k];
+        b[k] = wr[k];
+    }
+    V5<double> r = sys.riemann_flux(a, b, d, ss);
+    for (int k = 0; k < 5; k++) f[k] = r[k];
+    return EMG_OK;
+}
+
+int emgo_weno5z_interp(double v0, double v1, double v2, double v3, double v4, double* out) {
+    *out = weno5z_interp(v0, v1, v2, v3, v4);
+    return EMG_OK;
+}
+
+int emgo_to_prim(const emg_eos* eos, const double u[5], double w[5]) {
+    Euler<double> sys = to_sys(eos);
+    V5<double> a;
+    for (int k = 0; k < 5; k++) a[k] = u[k];
+    V5<double> r = sys.to_prim(a);
+    for (int k = 0; k < 5; k++) w[k] = r[k];
+    return EMG_OK;
+}
+int emgo_to_cons(const emg_eos* eos, const double w[5], double u[5]) {
+    Euler<double> sys = to_sys(eos);
+    V5<double> a;
+    for (int k = 0; k < 5; k++) a[k] = w[k];
+    V5<double> r = sys.to_cons(a);
+    for (int k = 0; k < 5; k++) u[k] = r[k];
+    return EMG_OK;
+}
+int emgo_eigen(const emg_eos* eos, const double w[5], int d, double l[25], double r[25]) {
+    Euler<double> sys = to_sys(eos);
+    V5<double> a;
+    for (int k = 0; k < 5; k++) a[k] = w[k];
+    Mat5<double> L, R;
+    sys.eigen(a, d, L, R);
+    for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 5; j++) {
+            l[5 * i + j] = L[i][j];
+            r[5 * i + j] = R[i][j];
+        }
+    return EMG_OK;
+}
+int emgo_max_speed(const emg_eos* eos, const double w[5], int d, double* s) {
+    Euler<double> sys = to_sys(eos);
+    V5<double> a;
+    for (int k = 0; k < 5; k++) a[k] = w[k];
+    *s = sys.max_speed(a, d);
+    return EMG_OK;
+}
+int emgo_admissible(const emg_eos* eos, const double w[5]) {
+    Euler<double> sys = to_sys(eos);
+    V5<double> a;
+    for (int k = 0; k < 5; k++) a[k] = w[k];
+    return sys.admissible(a) ? 1 : 0;
+}
+
+// Characteristic ghost layer (C/boundary.rs:34-44).
+int emgo_characteristic_ghost_layer(const emg_eos* eos, const double u_b[5], const double u_b1[5],
+                                    const double u_far[5], int d, int side, double m, double out[5]) {
+    Euler<double> sys = to_sys(eos);
+    V5<double> a, b, c;
+    for (int k = 0; k < 5; k++) {
+        a[k] = u_b[k];
+        b[k] = u_b1[k];
+        c[k] = u_far[k];
+    }
+    V5<double> r = characteristic_ghost_layer(sys, a, b, c, d, side, m);
+    for (int k = 0; k < 5; k++) out[k] = r[k];
+    return EMG_OK;
+}
+
+// Exact Riemann star state and sampling (C/exact.rs:45-109).
+int emgo_exact_star(const double l[3], const double r[3], const emg_eos* eos_l, const emg_eos* eos_r, double out[4]) {
+    Side L{l[0], l[1], l[2], Nasg<double>{eos_l->gamma, eos_l->p_inf, eos_l->b, eos_l->q, eos_l->cv}};
+    Side R{r[0], r[1], r[2], Nasg<double>{eos_r->gamma, eos_r->p_inf, eos_r->b, eos_r->q, eos_r->cv}};
+    Star s = star(L, R);
+    out[0] = s.p;
+    out[1] = s.u;
+    out[2] = s.rho_l;
+    out[3] = s.rho_r;
+    return EMG_OK;
+}
+int emgo_exact_sample(const double l[3], const double r[3], const emg_eos* eos_l, const emg_eos* eos_r,
+                      const double* xi, size_t n, double* out) {
+    Side L{l[0], l[1], l[2], Nasg<double>{eos_l->gamma, eos_l->p_inf, eos_l->b, eos_l->q, eos_l->cv}};
+    Side R{r[0], r[1], r[2], Nasg<double>{eos_r->gamma, eos_r->p_inf, eos_r->b, eos_r->q, eos_r->cv}};
+    Star s = star(L, R);
+    for (size_t i = 0; i < n; i++) sample(L, R, s, xi[i], out + 3 * i);
+    return EMG_OK;
+}
+
+}  // extern "C"

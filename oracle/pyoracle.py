@@ -1,0 +1,301 @@
+"""CPU ORACLE — test infrastructure only.
+
+ctypes wrapper of ``liboracle.so``, the C++ restatement of the reference CPU
+f64 solver (oracle.hpp). Used only by tests/, ``__graft_entry__.smoke()`` and
+the CPU-baseline leg of bench.py, as the checker and the timed CPU baseline;
+the product package never imports it.
+
+``OracleSolver`` has the same constructor and methods as
+``emergence_b200.GpuSolver`` so that parity tests drive both identically.
+"""
+import ctypes as C
+import math
+import os
+import subprocess
+
+import numpy as np
+
+from emergence_b200._abi import EmgBc, EmgEos, EmgMesh, EmgOpts
+from emergence_b200.physics import Bc, FluxMode
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+_D = C.POINTER(C.c_double)
+_U64 = C.POINTER(C.c_uint64)
+_P = C.c_void_p
+SIGS = {
+    "emgo_last_error": (C.c_char_p, []),
+    "emgo_num_threads": (C.c_int, []),
+    "emgo_set_num_threads": (None, [C.c_int]),
+    "emgo_uniform_create": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc), C.POINTER(EmgOpts),
+                                      _D, C.c_size_t, C.POINTER(_P)]),
+    "emgo_uniform_destroy": (C.c_int, [_P]),
+    "emgo_uniform_step": (C.c_int, [_P, C.c_double]),
+    "emgo_uniform_dt_cfl": (C.c_int, [_P, _D]),
+    "emgo_uniform_run_to": (C.c_int, [_P, C.c_double, _U64]),
+    "emgo_uniform_download": (C.c_int, [_P, _D, C.c_size_t]),
+    "emgo_uniform_upload": (C.c_int, [_P, _D, C.c_size_t]),
+    "emgo_uniform_totals": (C.c_int, [_P, _D]),
+    "emgo_uniform_counters": (C.c_int, [_P, _U64]),
+    "emgo_uniform_get_time": (C.c_int, [_P, _D]),
+    "emgo_uniform_set_time": (C.c_int, [_P, C.c_double]),
+    "emgo_uniform_fill_ghosts": (C.c_int, [_P]),
+    "emgo_uniform_fill_ghosts_of": (C.c_int, [_P, _D, C.c_size_t]),
+    "emgo_line_fluxes": (C.c_int, [C.POINTER(EmgEos), _D, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                   _D, _D, _U64]),
+    "emgo_positivity_limit": (C.c_int, [C.POINTER(EmgEos), _D, C.c_int, C.c_int, C.c_int, C.c_double, _D, _D, _U64]),
+    "emgo_midpoint_flux": (C.c_int, [C.POINTER(EmgEos), _D, C.c_int, C.c_int, _D, _D, C.POINTER(C.c_int)]),
+    "emgo_riemann_flux": (C.c_int, [C.POINTER(EmgEos), _D, _D, C.c_int, _D, _D]),
+    "emgo_weno5z_interp": (C.c_int, [C.c_double] * 5 + [_D]),
+    "emgo_to_prim": (C.c_int, [C.POINTER(EmgEos), _D, _D]),
+    "emgo_to_cons": (C.c_int, [C.POINTER(EmgEos), _D, _D]),
+    "emgo_eigen": (C.c_int, [C.POINTER(EmgEos), _D, C.c_int, _D, _D]),
+    "emgo_max_speed": (C.c_int, [C.POINTER(EmgEos), _D, C.c_int, _D]),
+    "emgo_admissible": (C.c_int, [C.POINTER(EmgEos), _D]),
+    "emgo_characteristic_ghost_layer": (C.c_int, [C.POINTER(EmgEos), _D, _D, _D, C.c_int, C.c_int, C.c_double, _D]),
+    "emgo_exact_star": (C.c_int, [_D, _D, C.POINTER(EmgEos), C.POINTER(EmgEos), _D]),
+    "emgo_exact_sample": (C.c_int, [_D, _D, C.POINTER(EmgEos), C.POINTER(EmgEos), _D, C.c_size_t, _D]),
+}
+
+_lib = None
+
+
+def build():
+    """Compile liboracle.so from oracle.hpp / oracle_capi.cpp (make)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _chk(code):
+    if code != 0:
+        raise RuntimeError(f"oracle error {code}: {lib().emgo_last_error().decode()}")
+
+
+def dptr(a):
+    return a.ctypes.data_as(_D)
+
+
+def c_eos(eos):
+    return EmgEos(eos.gamma, eos.p_inf, eos.b, eos.q, eos.cv)
+
+
+def arr(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+
+
+def set_threads(n):
+    lib().emgo_set_num_threads(int(n))
+
+
+def num_threads():
+    return lib().emgo_num_threads()
+
+
+class OracleSolver:
+    """C++ restatement of ``compressible::Solver`` (Euler system)."""
+
+    def __init__(self, sys, mesh, u, bc=None, cfl=0.5, mode=FluxMode.Hybrid, tol=1e-3, positivity=True,
+                 precision=0):
+        from emergence_b200.solver import _c_bcs, _c_mesh
+        self.sys, self.mesh = sys, mesh
+        self.bc = bc if bc is not None else [[Bc.Periodic, Bc.Periodic] for _ in range(3)]
+        u = arr(u)
+        self._m = _c_mesh(mesh)
+        self._e = c_eos(sys.eos)
+        self._b = _c_bcs(self.bc)
+        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, 0, 0)
+        h = C.c_void_p()
+        _chk(lib().emgo_uniform_create(C.byref(self._m), C.byref(self._e), self._b, C.byref(self._o), dptr(u),
+                                       mesh.len(), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().emgo_uniform_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, dt):
+        _chk(lib().emgo_uniform_step(self._h, float(dt)))
+
+    def dt_cfl(self):
+        v = C.c_double()
+        _chk(lib().emgo_uniform_dt_cfl(self._h, C.byref(v)))
+        return v.value
+
+    def run_to(self, t_end):
+        n = C.c_uint64()
+        _chk(lib().emgo_uniform_run_to(self._h, float(t_end), C.byref(n)))
+        return n.value
+
+    def advance(self, nsteps, t_end=math.inf):
+        """Same stepping rule as GpuSolver.advance, on the CPU."""
+        taken = 0
+        for _ in range(int(nsteps)):
+            t = self.t
+            if math.isfinite(t_end):
+                if not (t < t_end - 1e-10 * abs(t_end)):
+                    break
+                dt = min(self.dt_cfl(), t_end - t)
+            else:
+                dt = self.dt_cfl()
+            self.step(dt)
+            taken += 1
+        return taken
+
+    def download(self):
+        out = np.empty((self.mesh.len(), 5))
+        _chk(lib().emgo_uniform_download(self._h, dptr(out), self.mesh.len()))
+        return out
+
+    def upload(self, u):
+        u = arr(u)
+        _chk(lib().emgo_uniform_upload(self._h, dptr(u), self.mesh.len()))
+
+    def totals(self):
+        out = np.empty(5)
+        _chk(lib().emgo_uniform_totals(self._h, dptr(out)))
+        return out
+
+    def counters(self):
+        out = (C.c_uint64 * 4)()
+        _chk(lib().emgo_uniform_counters(self._h, out))
+        return list(out)
+
+    @property
+    def t(self):
+        v = C.c_double()
+        _chk(lib().emgo_uniform_get_time(self._h, C.byref(v)))
+        return v.value
+
+    @t.setter
+    def t(self, value):
+        _chk(lib().emgo_uniform_set_time(self._h, float(value)))
+
+    def fill_ghosts(self):
+        _chk(lib().emgo_uniform_fill_ghosts(self._h))
+
+    def fill_ghosts_of(self, u):
+        u = arr(u).copy()
+        _chk(lib().emgo_uniform_fill_ghosts_of(self._h, dptr(u), self.mesh.len()))
+        return u
+
+    def prim(self, i, j, k):
+        m = self.mesh
+        u = self.download()[m.idx(i + m.g(0), j + m.g(1), k + m.g(2))]
+        return to_prim(self.sys.eos, u)
+
+
+# ---- unit-level helpers
+
+def line_fluxes(eos, w, d, ng, mode, tol=1e-3, lam=0.0):
+    w = arr(w)
+    n = w.shape[0] - 2 * ng
+    out = np.zeros((n + 1, 5))
+    uf = np.zeros(n + 1)
+    st = (C.c_uint64 * 4)()
+    e = c_eos(eos)
+    _chk(lib().emgo_line_fluxes(C.byref(e), dptr(w), w.shape[0], d, ng, mode, tol, lam, dptr(out), dptr(uf), st))
+    return out, uf, list(st)
+
+
+def positivity_limit(eos, w, d, ng, lam, flux, uface):
+    w, flux, uface = arr(w), arr(flux).copy(), arr(uface).copy()
+    e = c_eos(eos)
+    n = C.c_uint64()
+    _chk(lib().emgo_positivity_limit(C.byref(e), dptr(w), w.shape[0], d, ng, lam, dptr(flux), dptr(uface),
+                                     C.byref(n)))
+    return flux, uface, n.value
+
+
+def riemann_flux(eos, wl, wr, d):
+    e = c_eos(eos)
+    f = np.zeros(5)
+    ss = C.c_double()
+    _chk(lib().emgo_riemann_flux(C.byref(e), dptr(arr(wl)), dptr(arr(wr)), d, dptr(f), C.byref(ss)))
+    return f, ss.value
+
+
+def to_prim(eos, u):
+    e = c_eos(eos)
+    w = np.zeros(5)
+    _chk(lib().emgo_to_prim(C.byref(e), dptr(arr(u)), dptr(w)))
+    return w
+
+
+def to_cons(eos, w):
+    e = c_eos(eos)
+    u = np.zeros(5)
+    _chk(lib().emgo_to_cons(C.byref(e), dptr(arr(w)), dptr(u)))
+    return u
+
+
+def eigen(eos, w, d):
+    e = c_eos(eos)
+    l, r = np.zeros(25), np.zeros(25)
+    _chk(lib().emgo_eigen(C.byref(e), dptr(arr(w)), d, dptr(l), dptr(r)))
+    return l.reshape(5, 5), r.reshape(5, 5)
+
+
+def max_speed(eos, w, d):
+    e = c_eos(eos)
+    s = C.c_double()
+    _chk(lib().emgo_max_speed(C.byref(e), dptr(arr(w)), d, C.byref(s)))
+    return s.value
+
+
+def admissible(eos, w):
+    e = c_eos(eos)
+    return bool(lib().emgo_admissible(C.byref(e), dptr(arr(w))))
+
+
+def characteristic_ghost_layer(eos, u_b, u_b1, u_far, d, side, m):
+    e = c_eos(eos)
+    out = np.zeros(5)
+    _chk(lib().emgo_characteristic_ghost_layer(C.byref(e), dptr(arr(u_b)), dptr(arr(u_b1)), dptr(arr(u_far)), d, side,
+                                               float(m), dptr(out)))
+    return out
+
+
+def weno5z_interp(v0, v1, v2, v3, v4):
+    o = C.c_double()
+    _chk(lib().emgo_weno5z_interp(v0, v1, v2, v3, v4, C.byref(o)))
+    return o.value
+
+
+def exact_star(left, right, eos_l, eos_r=None):
+    eos_r = eos_r or eos_l
+    out = np.zeros(4)
+    el, er = c_eos(eos_l), c_eos(eos_r)
+    _chk(lib().emgo_exact_star(dptr(arr(left)), dptr(arr(right)), C.byref(el), C.byref(er), dptr(out)))
+    return out  # p*, u*, rho*_L, rho*_R
+
+
+def exact_sample(left, right, xi, eos_l, eos_r=None):
+    eos_r = eos_r or eos_l
+    xi = arr(xi)
+    out = np.zeros((xi.size, 3))
+    el, er = c_eos(eos_l), c_eos(eos_r)
+    _chk(lib().emgo_exact_sample(dptr(arr(left)), dptr(arr(right)), C.byref(el), C.byref(er), dptr(xi), xi.size,
+                                 dptr(out)))
+    return out  # rho, u, p per xi

@@ -1,0 +1,293 @@
+"""Pin the CPU oracle to the reference's own known-answer tests.
+
+Each test restates one test of the reference (Rust) for the Euler system and
+runs it against the C++ restatement in oracle/. CPU only.
+"""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from emergence_b200.physics import Bc, Euler, FluxMode, Mesh, Nasg, initial_state
+from oracle import pyoracle as O
+
+GAS = Nasg.ideal(1.4)
+SYS = Euler(GAS)
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def make_solver(n, ng, init, bc=None, mode=FluxMode.Hybrid, positivity=True, cfl=0.5, lo=(0, 0, 0), hi=(1, 1, 1)):
+    mesh = Mesh.new(n, lo, hi, ng=ng)
+    x = mesh.centres()
+    w = init(x)
+    u = initial_state(SYS, mesh, w)
+    s = O.OracleSolver(SYS, mesh, u, bc=bc, cfl=cfl, mode=mode, positivity=positivity)
+    return s, mesh, u
+
+
+def linear_init(x):
+    w = np.zeros(x[0].shape + (5,))
+    w[..., 0] = 1.0 + x[0] + 2.0 * x[1] + 3.0 * x[2]
+    w[..., 1], w[..., 2], w[..., 3], w[..., 4] = 0.3, -0.2, 0.1, 1.0
+    return w
+
+
+def interior_only(mesh, u):
+    v = np.full_like(u, np.nan)
+    mesh.interior(v)[...] = mesh.interior(u)
+    return v
+
+
+# exact.rs:115-133 (golden table extracted by tests/golden/make_golden.py)
+def test_toro_star_values():
+    data = json.load(open(os.path.join(HERE, "golden", "toro_star.json")))
+    for c in data["cases"]:
+        p, u, _, _ = O.exact_star(c["left"], c["right"], Nasg.ideal(data["gamma"]))
+        ps, us = c["p_star"], c["u_star"]
+        assert abs(p - ps) <= 1e-4 * max(abs(ps), 1.0) + 1e-5, (p, ps)
+        assert abs(u - us) <= 1e-4 * max(abs(us), 1.0), (u, us)
+
+
+# solver.rs:808-848
+@pytest.mark.parametrize("n", [(2, 3, 4), (8, 2, 1)])
+@pytest.mark.parametrize("ng", [6, 10])
+def test_deep_periodic_ghosts_match_the_torus_including_corners(n, ng):
+    s, m, u = make_solver(n, ng, linear_init)
+    g = s.fill_ghosts_of(interior_only(m, u))
+    for i in range(m.m(0)):
+        for j in range(m.m(1)):
+            for k in range(m.m(2)):
+                c = (i, j, k)
+                w = [m.g(d) + (c[d] - m.g(d)) % n[d] for d in range(3)]
+                assert np.array_equal(g[m.idx(i, j, k)], u[m.idx(*w)])
+
+
+# solver.rs:850-880
+@pytest.mark.parametrize("n", [(2, 3, 4), (8, 2, 1)])
+@pytest.mark.parametrize("ng", [6, 10])
+def test_short_reflecting_ghosts_match_mirrored_images_including_corners(n, ng):
+    bc = [[Bc.Reflect, Bc.Reflect] for _ in range(3)]
+    s, m, u = make_solver(n, ng, linear_init, bc=bc)
+    g = s.fill_ghosts_of(interior_only(m, u))
+    for i in range(m.m(0)):
+        for j in range(m.m(1)):
+            for k in range(m.m(2)):
+                c = (i, j, k)
+                img, flips = [], []
+                for d in range(3):
+                    r = (c[d] - m.g(d)) % (2 * n[d])
+                    img.append(m.g(d) + (r if r < n[d] else 2 * n[d] - 1 - r))
+                    flips.append(r >= n[d])
+                expected = u[m.idx(*img)].copy()
+                for d in range(3):
+                    if flips[d]:
+                        expected[1 + d] *= -1.0
+                assert np.array_equal(g[m.idx(i, j, k)], expected)
+
+
+# solver.rs:882-930
+@pytest.mark.parametrize("d", [0, 1, 2])
+@pytest.mark.parametrize("reflecting_side", [0, 1])
+@pytest.mark.parametrize("opposite_kind", [0, 1, 2, 3])
+def test_deep_reflections_use_the_opposite_current_boundary_condition(d, reflecting_side, opposite_kind):
+    n = [1, 1, 1]
+    n[d] = 2
+
+    def init(x):
+        w = np.zeros(x[0].shape + (5,))
+        w[..., 0] = 1.0 + x[d]
+        w[..., 4] = 1.0 + x[d]
+        w[..., 1 + d] = 3.0
+        return w
+
+    far_w = np.array([2.0, 0, 0, 0, 2.0])
+    far_w[1 + d] = 3.0
+    far = SYS.to_cons(far_w)
+    opposite = 1 - reflecting_side
+    obc = [Bc.Outflow, Bc.dirichlet(far), Bc.Periodic, Bc.characteristic(far)][opposite_kind]
+    bc = [[Bc.Periodic, Bc.Periodic] for _ in range(3)]
+    bc[d][reflecting_side] = Bc.Reflect
+    bc[d][opposite] = obc
+    s, m, u = make_solver(tuple(n), 6, init, bc=bc)
+
+    def at(x):
+        c = [0, 0, 0]
+        c[d] = x
+        return m.idx(*c)
+
+    g = s.fill_ghosts_of(interior_only(m, u))
+    for layer in range(1, m.ng + 1):
+        image = layer - 1 if reflecting_side == 0 else n[d] - layer
+        if 0 <= image < 2:
+            expected = u[at(m.ng + image)].copy()
+        elif opposite_kind == 0:
+            expected = u[at(m.ng + (0 if opposite == 0 else 1))].copy()
+        elif opposite_kind == 2:
+            expected = u[at(m.ng + image % 2)].copy()
+        elif opposite_kind == 1:
+            expected = far.copy()
+        else:
+            center = u[at(m.ng + (0 if opposite == 0 else 1))]
+            neighbor = u[at(m.ng + (1 if opposite == 0 else 0))]
+            depth = -image if opposite == 0 else image - 2 + 1
+            expected = O.characteristic_ghost_layer(GAS, center, neighbor, far, d, opposite, depth)
+        expected[1 + d] *= -1.0
+        q = at(m.ng - layer if reflecting_side == 0 else m.ng + 2 + layer - 1)
+        assert np.array_equal(g[q], expected), (layer, g[q], expected)
+
+
+# tests/cpu.rs:54-90
+def test_characteristic_layers_extrapolate_outgoing_waves_and_reject_incoming_waves():
+    w = np.array([1.0, 0.0, 0.0, 0.0, 1.0])
+    far = O.to_cons(GAS, w)
+    for d in range(3):
+        _, r = O.eigen(GAS, w, d)
+        for side in range(2):
+            outgoing = 0 if side == 0 else 4
+            incoming = 4 - outgoing
+            for mode in (outgoing, incoming):
+                amp = 1e-4
+                neighbor = O.to_cons(GAS, w + amp * r[:, mode])
+                for layer in (1.0, 2.0, 6.0):
+                    actual = O.to_prim(GAS, O.characteristic_ghost_layer(GAS, far, neighbor, far, d, side, layer))
+                    expected = w - (layer * amp * r[:, mode] if mode == outgoing else 0.0)
+                    assert np.all(np.abs(actual - expected) < 2e-14)
+
+
+# tests/cpu.rs:266-298
+@pytest.mark.parametrize("n", [(2, 1, 1), (1, 3, 1), (1, 1, 2), (2, 3, 4)])
+@pytest.mark.parametrize("ng", [6, 10])
+def test_periodic_axes_shorter_than_the_ghost_width_preserve_uniform_flow(n, ng):
+    expected = np.array([1.0, 0.3, -0.2, 0.1, 1.0])
+    s, m, _ = make_solver(n, ng, lambda x: np.broadcast_to(expected, x[0].shape + (5,)).copy(),
+                          mode=FluxMode.Central, positivity=False)
+    s.step(1e-5)
+    w = SYS.to_prim(m.interior(s.download()))
+    assert np.all(np.abs(w - expected) < 1e-13)
+
+
+# tests/cpu.rs:336-367
+@pytest.mark.parametrize("n", [(2, 1, 1), (1, 3, 1), (1, 1, 2), (2, 3, 4)])
+@pytest.mark.parametrize("ng", [6, 10])
+def test_short_reflecting_axes_preserve_rest_states_without_positivity_fallback(n, ng):
+    rest = np.array([1.0, 0.0, 0.0, 0.0, 1.0])
+    bc = [[Bc.Reflect, Bc.Reflect] for _ in range(3)]
+    s, m, _ = make_solver(n, ng, lambda x: np.broadcast_to(rest, x[0].shape + (5,)).copy(), bc=bc,
+                          mode=FluxMode.Central, positivity=False)
+    for _ in range(3):
+        s.step(1e-4)
+    w = SYS.to_prim(m.interior(s.download()))
+    assert np.all(np.abs(w - rest) < 1e-13)
+
+
+# tests/cpu.rs:134-152
+def test_strong_pressure_jump_reports_the_limiter_that_keeps_it_admissible():
+    def init(x):
+        w = np.zeros(x[0].shape + (5,))
+        w[..., 0] = 1.0
+        w[..., 4] = np.where(x[0] < 0.5, 1000.0, 0.01)
+        return w
+
+    bc = [[Bc.Outflow, Bc.Outflow], [Bc.Periodic] * 2, [Bc.Periodic] * 2]
+    s, m, _ = make_solver((32, 1, 1), 6, init, bc=bc, mode=FluxMode.Central, cfl=0.2)
+    s.step(s.dt_cfl())
+    assert s.counters()[3] > 0
+    for i in range(32):
+        assert O.admissible(GAS, s.prim(i, 0, 0))
+
+
+# tests/cpu.rs:25-52, restated for the Euler system (no dilatation limit)
+@pytest.mark.parametrize("kind", [Bc.Reflect, Bc.Periodic, Bc.Outflow])
+def test_cfl_is_the_acoustic_limit_and_ignores_poisoned_ghosts(kind):
+    w0 = np.array([1.2, 0.2, 0.0, 0.0, 1e5])
+    bc = [[kind, kind], [Bc.Periodic] * 2, [Bc.Periodic] * 2]
+    s, m, u = make_solver((8, 1, 1), 6, lambda x: np.broadcast_to(w0, x[0].shape + (5,)).copy(), bc=bc)
+    w = s.prim(0, 0, 0)
+    expected = s_cfl = 0.5 * m.dx[0] / O.max_speed(GAS, w, 0)
+    assert abs(s.dt_cfl() / expected - 1.0) < 1e-13
+    poisoned = u.copy()
+    for i in range(m.m(0)):
+        if i < m.g(0) or i >= m.g(0) + 8:
+            poisoned[i] = np.nan
+    s.upload(poisoned)
+    assert abs(s.dt_cfl() / s_cfl - 1.0) < 1e-13
+
+
+# tests/cpu.rs:92-132 (rayon 1 vs 3 threads → OpenMP 1 vs 3 threads)
+@pytest.mark.parametrize("n", [(1, 96, 96), (96, 1, 96), (96, 96, 1)])
+def test_rk_updates_are_reproducible_for_every_2d_mesh_orientation(n):
+    def init(x):
+        w = np.zeros(x[0].shape + (5,))
+        w[..., 0] = 1.0 + 0.01 * (np.sin(2 * math.pi * x[0]) + np.sin(2 * math.pi * x[1]) + np.sin(2 * math.pi * x[2]))
+        w[..., 1], w[..., 2], w[..., 3], w[..., 4] = 0.3, 0.2, 0.1, 1.0
+        return w
+
+    results = []
+    saved = O.num_threads()
+    try:
+        for threads in (1, 3):
+            O.set_threads(threads)
+            s, m, _ = make_solver(n, 6, init, mode=FluxMode.Central)
+            s.step(1e-4)
+            s.step(1e-4)
+            u = s.download()
+            assert all(O.admissible(GAS, w) for w in SYS.to_prim(m.interior(u)).reshape(-1, 5)[::97])
+            results.append(u)
+    finally:
+        O.set_threads(saved)
+    assert np.array_equal(results[0], results[1])
+
+
+# scheme.rs:466-528, restated for the Euler system
+def test_limited_flux_also_limits_the_face_velocity():
+    wi = np.array([1.0, 0.0, 0.0, 0.0, 1.0])
+    w = np.array([wi, wi, wi])  # one interior cell and its two neighbours, ng = 1
+    physical = SYS.to_cons(wi) * 0.0
+    physical[1] = wi[4]  # flux of a fluid at rest: (0, p, 0, 0, 0)
+    flux = np.array([physical, physical])
+    flux[0][4] += 100.0  # would drive a one-sided state negative
+    velocity = np.array([3.0, 0.0])
+    lim, vel, n = O.positivity_limit(GAS, w, 0, 1, 0.1, flux, velocity)
+    assert n == 1
+    theta = (lim[0][4] - physical[4]) / 100.0
+    assert 0.0 < theta < 1.0
+    assert abs(vel[0] - 3.0 * theta) < 1e-14
+    u = SYS.to_cons(wi)
+    for sign in (-1.0, 1.0):
+        nxt = u + sign * 0.2 * (lim[0] - physical)
+        assert O.admissible(GAS, SYS.to_prim(nxt))
+    assert np.array_equal(lim[1], physical)
+
+
+# examples/validate.rs:24-65 (Sod tube, WENO mode, exact solution)
+def test_sod_tube_converges_to_the_exact_solution():
+    left, right, x0, t_end = (1.0, 0.0, 1.0), (0.125, 0.0, 0.1), 0.5, 0.2
+    errs = []
+    for n in (100, 200):
+        def init(x):
+            w = np.zeros(x[0].shape + (5,))
+            w[..., 0] = np.where(x[0] < x0, left[0], right[0])
+            w[..., 4] = np.where(x[0] < x0, left[2], right[2])
+            return w
+
+        bc = [[Bc.Outflow, Bc.Outflow], [Bc.Periodic] * 2, [Bc.Periodic] * 2]
+        s, m, _ = make_solver((n, 1, 1), 6, init, bc=bc, mode=FluxMode.Weno, cfl=0.4)
+        s.run_to(t_end)
+        rho = SYS.to_prim(m.interior(s.download()))[:, 0, 0, 0]
+        xc = m.centres()[0][:, 0, 0]
+        exact = O.exact_sample(left, right, (xc - x0) / t_end, GAS)[:, 0]
+        errs.append(np.mean(np.abs(rho - exact)) / np.mean(np.abs(exact)))
+    assert errs[0] < 2e-2 and errs[1] < errs[0]
+
+
+# The WENO5-Z interpolation reproduces smooth data to high order and stays
+# within the data range at a jump (scheme.rs:67-86).
+def test_weno_interpolation_is_exact_for_constants_and_bounded_at_jumps():
+    assert O.weno5z_interp(2.0, 2.0, 2.0, 2.0, 2.0) == 2.0
+    v = O.weno5z_interp(0.0, 0.0, 0.0, 1.0, 1.0)
+    assert -0.05 < v < 1.05
+    # quadratic data: each candidate stencil is exact, so the result is too
+    f = lambda x: 1.0 + 0.5 * x - 0.25 * x * x
+    assert abs(O.weno5z_interp(f(0), f(1), f(2), f(3), f(4)) - f(2.5)) < 1e-12
