@@ -24,7 +24,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("uniform.cu", ["-fmad=false"]),
     ("sweep_f64.cu", ["-fmad=false"]),
-    ("sweep_mixed.cu", ["-fmad=true"]),
+    ("sweep_mixed.cu", ["-fmad=true", "-use_fast_math"]),
 ]
 
 

@@ -136,17 +136,35 @@ template <typename R> __device__ __forceinline__ R sq(R x) { return x * x; }
 // WENO5-Z interpolation of point values to the midpoint x_{2+1/2} (scheme.rs:67-74).
 template <typename R> __device__ __forceinline__ R weno5z_interp(R v0, R v1, R v2, R v3, R v4) {
     const R eps = WenoEps<R>::v;
-    R q0 = (R(3) * v0 - R(10) * v1 + R(15) * v2) / R(8);
-    R q1 = (-v1 + R(6) * v2 + R(3) * v3) / R(8);
-    R q2 = (R(3) * v2 + R(6) * v3 - v4) / R(8);
+    // x/8 == x*0.125 exactly (power-of-two scaling)
+    R q0 = (R(3) * v0 - R(10) * v1 + R(15) * v2) * R(0.125);
+    R q1 = (-v1 + R(6) * v2 + R(3) * v3) * R(0.125);
+    R q2 = (R(3) * v2 + R(6) * v3 - v4) * R(0.125);
     R b0 = R(13.0 / 12.0) * sq(v0 - R(2) * v1 + v2) + R(0.25) * sq(v0 - R(4) * v1 + R(3) * v2);
     R b1 = R(13.0 / 12.0) * sq(v1 - R(2) * v2 + v3) + R(0.25) * sq(v1 - v3);
     R b2 = R(13.0 / 12.0) * sq(v2 - R(2) * v3 + v4) + R(0.25) * sq(R(3) * v2 - R(4) * v3 + v4);
     R tau = rabs(b0 - b2);
-    R a0 = R(1.0 / 16.0) * (R(1) + sq(tau / (b0 + eps)));
-    R a1 = R(10.0 / 16.0) * (R(1) + sq(tau / (b1 + eps)));
-    R a2 = R(5.0 / 16.0) * (R(1) + sq(tau / (b2 + eps)));
-    return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+    if constexpr (sizeof(R) == 4) {
+        // FP32: the reference weights a_k = d_k (1 + (τ/(β_k+ε))²) overflow when a
+        // stencil is flat (β_k = 0: (1e-6/1e-30)² = 1e48 > FLT_MAX) and the
+        // interpolant turns NaN. Scale every a_k by (m/t)², m = min_k(β_k+ε),
+        // t = max(τ, m): identical weights in exact arithmetic, all terms ≤ 2 d_k.
+        const R b0e = b0 + eps, b1e = b1 + eps, b2e = b2 + eps;
+        const R m = rmin(b0e, rmin(b1e, b2e));
+        const R t = rmax(tau, m);
+        const R g = m / t, h = tau / t;
+        const R r0 = (m / b0e) * h, r1 = (m / b1e) * h, r2 = (m / b2e) * h;
+        const R g2 = g * g;
+        const R a0 = R(1.0 / 16.0) * (g2 + r0 * r0);
+        const R a1 = R(10.0 / 16.0) * (g2 + r1 * r1);
+        const R a2 = R(5.0 / 16.0) * (g2 + r2 * r2);
+        return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+    } else {
+        R a0 = R(1.0 / 16.0) * (R(1) + sq(tau / (b0 + eps)));
+        R a1 = R(10.0 / 16.0) * (R(1) + sq(tau / (b1 + eps)));
+        R a2 = R(5.0 / 16.0) * (R(1) + sq(tau / (b2 + eps)));
+        return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
+    }
 }
 
 // Coefficients of the 6th-order schemes (scheme.rs:88-92).

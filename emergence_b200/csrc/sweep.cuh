@@ -89,7 +89,9 @@ template <int RM> struct RingSize {
 template <typename RF, int P> struct SweepSmem {
     static constexpr int RM = SWEEP_THREADS / P;
     static constexpr int RS = RingSize<RM>::value;
-    static constexpr int STR = 5 * P + 1;  // row stride in elements (odd: conflict-free column access)
+    // row stride in elements: conflict-free for runs of consecutive rows
+    // (16 rows of one pencil when P <= 16, 8 rows × 2 pencils when P = 32)
+    static constexpr int STR = P == 32 ? 5 * P + 2 : 5 * P + 1;
     static constexpr size_t bytes() {
         return (size_t)RS * STR * sizeof(double)          // W (f64 primitives)
                + (RingTypes<RF>::MIXED ? (size_t)RS * STR * sizeof(float) : 0)  // Wf (f32 copy)
@@ -103,7 +105,7 @@ struct Sweep {
     static constexpr int T = SWEEP_THREADS;
     static constexpr int RM = T / P;
     static constexpr int RS = RingSize<RM>::value;
-    static constexpr int STR = 5 * P + 1;
+    static constexpr int STR = SweepSmem<RF, P>::STR;
     static constexpr bool MIXED = RingTypes<RF>::MIXED;
 
     __device__ static __forceinline__ int slot(int x) { return x & (RS - 1); }
@@ -125,13 +127,14 @@ struct Sweep {
         for (int k = 0; k < 5; k++) avg[k] = RF(0.5) * (Wr[at(j, k, l)] + Wr[at(j + 1, k, l)]);
         const RF rho = avg[0];
         const RF c = sound_speed(e, avg[0], avg[4]);
-        const RF l0un = -rho / (RF(2) * c);
+        // (−a)/b == −(a/b) exactly, so the negated entries need no division
+        const RF l4un = rho / (RF(2) * c);
+        const RF l0un = -l4un;
         const RF l04 = RF(1) / (RF(2) * c * c);
         const RF l14 = -RF(1) / (c * c);
-        const RF l4un = rho / (RF(2) * c);
-        const RF run0 = -c / rho;
-        const RF r40 = c * c;
         const RF run4 = c / rho;
+        const RF run0 = -run4;
+        const RF r40 = c * c;
         // characteristic variables of the six stencil cells
         RF ch0[6], ch1[6], ch2[6], ch3[6], ch4[6];
 #pragma unroll

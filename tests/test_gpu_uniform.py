@@ -95,7 +95,7 @@ def test_one_step_matches_the_oracle_bitwise(shape, bcname):
     ug, uo = g.download(), o.download()
     assert np.all(rel_l1(ug, uo, mesh) <= F64_TOL)
     # interior and ghost layers (filled at stage 1) bit for bit, up to the sign of zero
-    assert np.array_equal(ug, uo), float(np.nanmax(np.abs(ug - uo)))
+    assert np.array_equal(ug, uo, equal_nan=True), float(np.nanmax(np.abs(ug - uo)))
     assert g.counters() == o.counters()
     assert g.t == o.t
 
@@ -185,7 +185,9 @@ def test_mixed_precision_error_against_the_fp64_oracle():
         o.step(dt)
     err = rel_l1(g.download(), o.download(), mesh)
     print("mixed rel L1 per field after 20 steps", err)
-    assert np.all(err <= 1e-5)
+    # FP32 midpoint flux (scaled WENO-Z weights, fast division), FP64 state and limiter
+    assert np.all(err <= 5e-6), err
+    assert g.counters()[2] == o.counters()[2] == 0  # no first-order fallbacks in either
 
 
 def test_collapsed_time_step_is_reported_not_trapped():
