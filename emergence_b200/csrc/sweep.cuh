@@ -70,9 +70,12 @@ struct SweepParams {
     int positivity;      // limiter on/off
     int cfl_active[3];   // active axes for the fused CFL rate
     double cfl_dx[3];
-    // which of the three padded axes the sweep / lane / other axes are (for the CFL rate)
+    double tol;          // hybrid sensor tolerance (C/solver.rs:218)
     EosD eos;
 };
+
+// Flux modes (C/scheme.rs:39-47), a compile-time parameter of the sweep.
+enum SweepMode { MODE_HYBRID = 0, MODE_WENO = 1, MODE_CENTRAL = 2 };
 
 template <typename R> struct RingTypes {
     static constexpr bool MIXED = false;
@@ -81,50 +84,64 @@ template <> struct RingTypes<float> {
     static constexpr bool MIXED = true;
 };
 
-// ring slots: power of two ≥ RM + 5
-template <int RM> struct RingSize {
-    static constexpr int value = RM + 5 <= 16 ? 16 : (RM + 5 <= 32 ? 32 : 64);
+// Ring slots: a power of two holding every row one round touches. WENO:
+// RM + 5 rows (midpoint stencils); central: RM + 7 (the split-form stencil
+// reaches two rows behind the round's first face); hybrid: RM + 9 (plus the
+// sensor stencil two rows ahead of the last midpoint).
+template <int RM, int MODE> struct RingSize {
+    static constexpr int need = RM + (MODE == MODE_HYBRID ? 9 : (MODE == MODE_CENTRAL ? 7 : 5));
+    static constexpr int value = need <= 16 ? 16 : (need <= 32 ? 32 : (need <= 64 ? 64 : 128));
 };
 
-template <typename RF, int P> struct SweepSmem {
+template <typename RF, int P, int MODE> struct SweepSmem {
     static constexpr int RM = SWEEP_THREADS / P;
-    static constexpr int RS = RingSize<RM>::value;
-    // row stride in elements: conflict-free for runs of consecutive rows
+    static constexpr int RS = RingSize<RM, MODE>::value;
+    // values per cell in the primitive ring: w(5), plus ρe for the central
+    // flux, plus the two sensor logarithms for the hybrid switch
+    static constexpr int NW = MODE == MODE_WENO ? 5 : (MODE == MODE_CENTRAL ? 6 : 8);
+    // row strides in elements: conflict-free for runs of consecutive rows
     // (16 rows of one pencil when P <= 16, 8 rows × 2 pencils when P = 32)
+    static constexpr int STRW = P == 32 ? NW * P + 2 : NW * P + 1;
     static constexpr int STR = P == 32 ? 5 * P + 2 : 5 * P + 1;
+    static constexpr bool MID = MODE != MODE_CENTRAL;
     static constexpr size_t bytes() {
-        return (size_t)RS * STR * sizeof(double)          // W (f64 primitives)
-               + (RingTypes<RF>::MIXED ? (size_t)RS * STR * sizeof(float) : 0)  // Wf (f32 copy)
-               + (size_t)RS * STR * sizeof(RF)            // MF (midpoint fluxes)
-               + (size_t)RS * STR * sizeof(double);       // F (face fluxes)
+        return (size_t)RS * STRW * sizeof(double)                                    // W (f64 primitives, ρe, sensors)
+               + (RingTypes<RF>::MIXED && MID ? (size_t)RS * STR * sizeof(float) : 0)  // Wf (f32 copy of w)
+               + (MID ? (size_t)RS * STR * sizeof(RF) : 0)                             // MF (midpoint fluxes)
+               + (size_t)RS * STR * sizeof(double)                                    // F (face fluxes)
+               + (MODE == MODE_HYBRID ? (size_t)RS * P * sizeof(double) : 0);         // TH (blend weights)
     }
 };
 
-template <typename RF, int P, int D>
+template <typename RF, int P, int D, int MODE>
 struct Sweep {
+    using SM = SweepSmem<RF, P, MODE>;
     static constexpr int T = SWEEP_THREADS;
     static constexpr int RM = T / P;
-    static constexpr int RS = RingSize<RM>::value;
-    static constexpr int STR = SweepSmem<RF, P>::STR;
+    static constexpr int RS = SM::RS;
+    static constexpr int STR = SM::STR;
+    static constexpr int STRW = SM::STRW;
     static constexpr bool MIXED = RingTypes<RF>::MIXED;
+    static constexpr bool MID = SM::MID;
+    static constexpr int AHEAD = MODE == MODE_HYBRID ? 7 : 5;  // rows loaded beyond the round's midpoints
 
     __device__ static __forceinline__ int slot(int x) { return x & (RS - 1); }
-    // element (row x, field k, lane l) of a ring
-    __device__ static __forceinline__ int at(int x, int k, int l) { return slot(x) * STR + k * P + l; }
+    // element (row x, field k, lane l) of a ring with row stride S
+    template <int S> __device__ static __forceinline__ int at(int x, int k, int l) { return slot(x) * S + k * P + l; }
 
     // Characteristic WENO5-Z interpolation to midpoint m and its HLLC flux:
     // sparse form of C/scheme.rs:286-333. The zero entries of the Euler
     // eigenvectors (C/system.rs:232-258) are skipped, which leaves every
     // non-zero sum of the dense products unchanged.
-    __device__ static __forceinline__ void midpoint(const Eos<RF>& e, const RF* __restrict__ Wr, int m, int l,
-                                                    RF* f, bool& fb) {
+    template <int S>
+    __device__ static __forceinline__ void midpoint(const Eos<RF>& e, const RF* __restrict__ Wr, int m, int l, RF* f,
+                                                    bool& fb) {
         constexpr int un = 1 + D;
         constexpr int t1 = 1 + (D + 1) % 3, t2 = 1 + (D + 2) % 3;
         const int j = m + 2;
-        // arithmetic-mean state and its eigenvectors
         RF avg[5];
 #pragma unroll
-        for (int k = 0; k < 5; k++) avg[k] = RF(0.5) * (Wr[at(j, k, l)] + Wr[at(j + 1, k, l)]);
+        for (int k = 0; k < 5; k++) avg[k] = RF(0.5) * (Wr[at<S>(j, k, l)] + Wr[at<S>(j + 1, k, l)]);
         const RF rho = avg[0];
         const RF c = sound_speed(e, avg[0], avg[4]);
         // (−a)/b == −(a/b) exactly, so the negated entries need no division
@@ -135,18 +152,17 @@ struct Sweep {
         const RF run4 = c / rho;
         const RF run0 = -run4;
         const RF r40 = c * c;
-        // characteristic variables of the six stencil cells
         RF ch0[6], ch1[6], ch2[6], ch3[6], ch4[6];
 #pragma unroll
         for (int s = 0; s < 6; s++) {
             const int row = m + s;
-            const RF w0 = Wr[at(row, 0, l)];
-            const RF wn = Wr[at(row, un, l)];
-            const RF w4 = Wr[at(row, 4, l)];
+            const RF w0 = Wr[at<S>(row, 0, l)];
+            const RF wn = Wr[at<S>(row, un, l)];
+            const RF w4 = Wr[at<S>(row, 4, l)];
             ch0[s] = l0un * wn + l04 * w4;
             ch1[s] = w0 + l14 * w4;
-            ch2[s] = Wr[at(row, t1, l)];
-            ch3[s] = Wr[at(row, t2, l)];
+            ch2[s] = Wr[at<S>(row, t1, l)];
+            ch3[s] = Wr[at<S>(row, t2, l)];
             ch4[s] = l4un * wn + l04 * w4;
         }
         RF cl[5], cr[5];
@@ -160,7 +176,6 @@ struct Sweep {
         cr[3] = weno5z_interp(ch3[5], ch3[4], ch3[3], ch3[2], ch3[1]);
         cl[4] = weno5z_interp(ch4[0], ch4[1], ch4[2], ch4[3], ch4[4]);
         cr[4] = weno5z_interp(ch4[5], ch4[4], ch4[3], ch4[2], ch4[1]);
-        // back to primitives: rows of R (columns are the waves)
         RF wl[5], wr[5];
         wl[0] = (cl[0] + cl[1]) + cl[4];
         wr[0] = (cr[0] + cr[1]) + cr[4];
@@ -177,14 +192,56 @@ struct Sweep {
             fb = true;
 #pragma unroll
             for (int k = 0; k < 5; k++) {
-                wl[k] = Wr[at(j, k, l)];
-                wr[k] = Wr[at(j + 1, k, l)];
+                wl[k] = Wr[at<S>(j, k, l)];
+                wr[k] = Wr[at<S>(j + 1, k, l)];
             }
         }
         hllc(e, wl, wr, un, f);
     }
 
-    // One-sided admissibility of the limiter (C/scheme.rs:408-416), in f64.
+    // KEEP-PE two-point flux with cached ρe (C/system.rs:317-334).
+    __device__ static __forceinline__ void split_flux(const double* __restrict__ W, int ra, int rb, int l, double* f) {
+        constexpr int un = 1 + D;
+        double a[6], b[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            a[k] = W[at<STRW>(ra, k, l)];
+            b[k] = W[at<STRW>(rb, k, l)];
+        }
+        const double rho = 0.5 * (a[0] + b[0]);
+        const double u = 0.5 * (a[un] + b[un]);
+        const double c = rho * u;
+        f[0] = c;
+        f[1] = c * 0.5 * (a[1] + b[1]);
+        f[2] = c * 0.5 * (a[2] + b[2]);
+        f[3] = c * 0.5 * (a[3] + b[3]);
+        f[un] = f[un] + 0.5 * (a[4] + b[4]);
+        const double kin = c * 0.5 * (a[1] * b[1] + a[2] * b[2] + a[3] * b[3]);
+        const double rhoe = 0.5 * (a[5] + b[5]);
+        const double pw = 0.5 * (a[un] * b[4] + b[un] * a[4]);
+        f[4] = kin + u * rhoe + pw;
+    }
+
+    // 6th-order split-form central flux of the face between rows i and i+1
+    // (C/scheme.rs:188-214): Σ over lags 1..3 and their pairs, in order.
+    __device__ static __forceinline__ void central_flux(const double* __restrict__ W, int i, int l, double* cen) {
+        constexpr double A6[3] = {0.75, -0.15, 1.0 / 60.0};
+#pragma unroll
+        for (int k = 0; k < 5; k++) cen[k] = 0.0;
+#pragma unroll
+        for (int li = 0; li < 3; li++) {
+            const int lag = li + 1;
+#pragma unroll
+            for (int m = 0; m < lag; m++) {
+                double ft[5];
+                split_flux(W, i - m, i - m + lag, l, ft);
+#pragma unroll
+                for (int k = 0; k < 5; k++) cen[k] = cen[k] + 2.0 * A6[li] * ft[k];
+            }
+        }
+    }
+
+    // one-sided admissibility of the limiter (C/scheme.rs:408-416), in f64
     __device__ static __forceinline__ bool lim_ok(const Eos<double>& e, const double* fx, const double* ul,
                                                   const double* fl, const double* ur, const double* fr, double lam2) {
         double a[5], w[5];
@@ -198,20 +255,37 @@ struct Sweep {
         return admissible(e, w[0], w[4]);
     }
 
+    __device__ static __forceinline__ double d4(double q0, double q1, double q2, double q3, double q4) {
+        return fabs(q0 - 4.0 * q1 + 6.0 * q2 - 4.0 * q3 + q4);  // C/scheme.rs:97-99
+    }
+
     __device__ static void run(const SweepParams& p) {
         extern __shared__ __align__(16) unsigned char smem_raw[];
-        double* W = reinterpret_cast<double*>(smem_raw);
-        RF* Wf;
-        RF* MF;
-        if constexpr (MIXED) {
-            Wf = reinterpret_cast<RF*>(W + RS * STR);
-            MF = Wf + RS * STR;
-        } else {
-            Wf = reinterpret_cast<RF*>(W);
-            MF = reinterpret_cast<RF*>(W + RS * STR);
+        unsigned char* sp = smem_raw;
+        double* W = reinterpret_cast<double*>(sp);
+        sp += (size_t)RS * STRW * sizeof(double);
+        const RF* Wr;  // primitives read by the midpoint code
+        RF* Wf = nullptr;
+        if constexpr (MIXED && MID) {
+            Wf = reinterpret_cast<RF*>(sp);
+            sp += (size_t)RS * STR * sizeof(float);
         }
-        double* F = reinterpret_cast<double*>(MF + RS * STR);
-        __shared__ unsigned int s_fallback, s_limited;
+        RF* MF = nullptr;
+        if constexpr (MID) {
+            MF = reinterpret_cast<RF*>(sp);
+            sp += (size_t)RS * STR * sizeof(RF);
+        }
+        double* F = reinterpret_cast<double*>(sp);
+        sp += (size_t)RS * STR * sizeof(double);
+        double* TH = reinterpret_cast<double*>(sp);
+        if constexpr (MIXED) {
+            Wr = Wf;
+        } else {
+            Wr = reinterpret_cast<const RF*>(W);
+        }
+        constexpr int SR = MIXED ? STR : STRW;  // row stride of the ring the midpoint code reads
+
+        __shared__ unsigned int s_fallback, s_limited, s_weno;
         __shared__ double s_rate[T / 32];
 
         const StepCtl* ctl = p.ctl;
@@ -221,6 +295,7 @@ struct Sweep {
         if (tid == 0) {
             s_fallback = 0;
             s_limited = 0;
+            s_weno = 0;
         }
 
         const int lane0 = blockIdx.x * P;
@@ -245,10 +320,10 @@ struct Sweep {
         double rate_max = 0.0;
 
         for (int r = 0; r < nrounds; r++) {
-            // ---- A: load rows [lo, hi) and recover primitives
+            // ---- A: load rows [lo, hi) and recover primitives (and ρe, sensors)
             {
-                const int lo = r == 0 ? 0 : RM * r + 5;
-                const int hi = min(RM * r + RM + 5, nrows);
+                const int lo = r == 0 ? 0 : RM * r + AHEAD;
+                const int hi = min(RM * r + RM + AHEAD, nrows);
                 const int cnt = (hi - lo) * P;
                 for (int idx = tid; idx < cnt; idx += T) {
                     int rr, l;
@@ -268,52 +343,106 @@ struct Sweep {
                         to_prim(ed, u, w);
 #pragma unroll
                         for (int k = 0; k < 5; k++) {
-                            W[at(row, k, l)] = w[k];
-                            if constexpr (MIXED) Wf[at(row, k, l)] = RF(w[k]);
+                            W[at<STRW>(row, k, l)] = w[k];
+                            if constexpr (MIXED && MID) Wf[at<STR>(row, k, l)] = RF(w[k]);
+                        }
+                        if constexpr (MODE != MODE_WENO) W[at<STRW>(row, 5, l)] = ed.rho_e(w[0], w[4]);
+                        if constexpr (MODE == MODE_HYBRID) {
+                            // sensor values ln ρ, ln(p + p∞) (C/system.rs:409-413)
+                            W[at<STRW>(row, 6, l)] = log(fmax(w[0], 1e-300));
+                            W[at<STRW>(row, 7, l)] = log(fmax(w[4] + ed.p_inf, 1e-300));
                         }
                     }
                 }
             }
             __syncthreads();
-            // ---- B: midpoints [RM r, RM r + RM)
-            {
+            if constexpr (MODE == MODE_HYBRID) {
+                // ---- Θ: blend weights of faces [RM r, RM r + RM) (C/scheme.rs:171-182)
+                const int f = RM * r + tid / P;
+                const int l = tid % P;
+                if (f <= Ls && l < nlanes) {
+                    const int i = f + 4;
+                    double rr = 0.0;
+#pragma unroll
+                    for (int k = 6; k < 8; k++) {
+                        const double q0 = W[at<STRW>(i - 2, k, l)], q1 = W[at<STRW>(i - 1, k, l)],
+                                     q2 = W[at<STRW>(i, k, l)], q3 = W[at<STRW>(i + 1, k, l)],
+                                     q4 = W[at<STRW>(i + 2, k, l)], q5 = W[at<STRW>(i + 3, k, l)];
+                        rr = fmax(fmax(rr, d4(q0, q1, q2, q3, q4)), d4(q1, q2, q3, q4, q5));
+                    }
+                    double x = (rr / p.tol - 0.5) / 0.5;
+                    if (x < 0.0) x = 0.0;  // Rust clamp(0, 1): NaN stays NaN
+                    if (x > 1.0) x = 1.0;
+                    TH[slot(f) * P + l] = isfinite(rr) ? x * x * (3.0 - 2.0 * x) : 1.0;
+                }
+                __syncthreads();
+            }
+            if constexpr (MID) {
+                // ---- B: midpoints [RM r, RM r + RM)
                 const int m = RM * r + tid / P;
                 const int l = tid % P;
                 if (m < Ls + 5 && l < nlanes) {
-                    RF f[5];
-                    bool fb;
-                    midpoint(ef, Wf, m, l, f, fb);
+                    bool need = true;
+                    if constexpr (MODE == MODE_HYBRID) {
+                        // only midpoints of faces on the shock path (computed on demand, C/scheme.rs:233-238)
+                        need = false;
+                        for (int ff = max(m - 4, 0); ff <= min(m, Ls); ff++) need = need || TH[slot(ff) * P + l] > 0.0;
+                    }
+                    if (need) {
+                        RF f[5];
+                        bool fb;
+                        midpoint<SR>(ef, Wr, m, l, f, fb);
 #pragma unroll
-                    for (int k = 0; k < 5; k++) MF[at(m, k, l)] = f[k];
-                    if (fb && (m < Ls || tail)) atomicAdd(&s_fallback, 1u);
+                        for (int k = 0; k < 5; k++) MF[at<STR>(m, k, l)] = f[k];
+                        if (fb && (m < Ls || tail)) atomicAdd(&s_fallback, 1u);
+                    }
                 }
+                __syncthreads();
             }
-            __syncthreads();
             // ---- C: faces [RM r − 4, RM r + RM − 4)
             {
                 const int fidx = RM * r - 4 + tid / P;
                 const int l = tid % P;
                 if (fidx >= 0 && fidx <= Ls && l < nlanes) {
-                    double fh[5];
-                    // F̃ = Σ_s S6[s] (F̂_{+s} + F̂_{−s}), order as C/scheme.rs:230-246
+                    const int i = fidx + 4;
+                    double theta = MODE == MODE_WENO ? 1.0 : 0.0;
+                    if constexpr (MODE == MODE_HYBRID) theta = TH[slot(fidx) * P + l];
+                    double fh[5], cen[5];
+                    if constexpr (MODE != MODE_WENO) {
+                        if (theta < 1.0) central_flux(W, i, l, cen);
+                    }
+                    if (theta == 0.0) {
 #pragma unroll
-                    for (int k = 0; k < 5; k++) {
-                        double acc = 0.0;
-                        acc = acc + s6(0) * double(MF[at(fidx + 2, k, l)]);
-                        acc = acc + s6(1) * double(MF[at(fidx + 3, k, l)]);
-                        acc = acc + s6(1) * double(MF[at(fidx + 1, k, l)]);
-                        acc = acc + s6(2) * double(MF[at(fidx + 4, k, l)]);
-                        acc = acc + s6(2) * double(MF[at(fidx, k, l)]);
-                        fh[k] = acc;
+                        for (int k = 0; k < 5; k++) fh[k] = cen[k];
+                    } else {
+                        if constexpr (MID) {
+                            if constexpr (MODE == MODE_HYBRID) {
+                                if (fidx < Ls || tail) atomicAdd(&s_weno, 1u);
+                            }
+                            // F̃ = Σ_s S6[s] (F̂_{+s} + F̂_{−s}), order as C/scheme.rs:230-246
+#pragma unroll
+                            for (int k = 0; k < 5; k++) {
+                                double acc = 0.0;
+                                acc = acc + s6(0) * double(MF[at<STR>(fidx + 2, k, l)]);
+                                acc = acc + s6(1) * double(MF[at<STR>(fidx + 3, k, l)]);
+                                acc = acc + s6(1) * double(MF[at<STR>(fidx + 1, k, l)]);
+                                acc = acc + s6(2) * double(MF[at<STR>(fidx + 4, k, l)]);
+                                acc = acc + s6(2) * double(MF[at<STR>(fidx, k, l)]);
+                                fh[k] = acc;
+                            }
+                            if (theta < 1.0) {  // C/scheme.rs:270-276
+#pragma unroll
+                                for (int k = 0; k < 5; k++) fh[k] = theta * fh[k] + (1.0 - theta) * cen[k];
+                            }
+                        }
                     }
                     if (lim_on) {
-                        // Hu–Adams–Shu limiter (C/scheme.rs:395-464) between rows i = f+4 and i+1
-                        const int i = fidx + 4;
+                        // Hu–Adams–Shu limiter (C/scheme.rs:395-464) between rows i and i+1
                         double wi[5], wj[5], ul[5], ur[5], flp[5], frp[5];
 #pragma unroll
                         for (int k = 0; k < 5; k++) {
-                            wi[k] = W[at(i, k, l)];
-                            wj[k] = W[at(i + 1, k, l)];
+                            wi[k] = W[at<STRW>(i, k, l)];
+                            wj[k] = W[at<STRW>(i + 1, k, l)];
                         }
                         to_cons(ed, wi, ul);
                         to_cons(ed, wj, ur);
@@ -345,7 +474,7 @@ struct Sweep {
                         }
                     }
 #pragma unroll
-                    for (int k = 0; k < 5; k++) F[at(fidx, k, l)] = fh[k];
+                    for (int k = 0; k < 5; k++) F[at<STR>(fidx, k, l)] = fh[k];
                 }
             }
             __syncthreads();
@@ -364,7 +493,7 @@ struct Sweep {
                     double res[5];
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
-                        const double x = (F[at(c + 1, k, l)] - F[at(c, k, l)]) * inv;
+                        const double x = (F[at<STR>(c + 1, k, l)] - F[at<STR>(c, k, l)]) * inv;
                         const double prev = p.first ? 0.0 : p.rhs[k * p.ncell + g];
                         res[k] = prev - x;
                     }
@@ -401,10 +530,9 @@ struct Sweep {
                     }
                 }
             }
-            // next round's loads only touch W slots that C has finished with,
-            // and C of the next round writes F slots after the barrier below A.
+            // the next round's loads only touch W slots whose rows C has finished
+            // with (barrier above), and its C writes F slots after two more barriers
         }
-        // block-level counters and CFL rate
         if (p.cfl_fuse) {
             double v = rate_max;
 #pragma unroll
@@ -413,6 +541,7 @@ struct Sweep {
         }
         __syncthreads();
         if (tid == 0) {
+            if (s_weno) atomicAdd(&p.ctl->counters[1], (unsigned long long)s_weno);
             if (s_fallback) atomicAdd(&p.ctl->counters[2], (unsigned long long)s_fallback);
             if (s_limited) atomicAdd(&p.ctl->counters[3], (unsigned long long)s_limited);
             if (p.cfl_fuse) {

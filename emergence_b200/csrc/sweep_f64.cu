@@ -4,39 +4,58 @@
 
 namespace emg {
 
-template <int P, int D>
+template <int P, int D, int MODE>
 __global__ void __launch_bounds__(SWEEP_THREADS, 2) sweep_f64_kernel(const SweepParams p) {
-    Sweep<double, P, D>::run(p);
+    Sweep<double, P, D, MODE>::run(p);
 }
 
-template <int P, int D> static cudaError_t launch(const SweepParams& p, dim3 grid, cudaStream_t s) {
-    sweep_f64_kernel<P, D><<<grid, SWEEP_THREADS, SweepSmem<double, P>::bytes(), s>>>(p);
+template <int P, int D, int MODE> static cudaError_t launch(const SweepParams& p, dim3 grid, cudaStream_t s) {
+    sweep_f64_kernel<P, D, MODE><<<grid, SWEEP_THREADS, SweepSmem<double, P, MODE>::bytes(), s>>>(p);
     return cudaGetLastError();
 }
 
-cudaError_t sweep_launch_f64(int P, const SweepParams& p, dim3 grid, cudaStream_t s) {
-    const int D = p.d;
-#define EMG_CASE(PP) \
-    case PP: return D == 0 ? launch<PP, 0>(p, grid, s) : (D == 1 ? launch<PP, 1>(p, grid, s) : launch<PP, 2>(p, grid, s));
+template <int P, int MODE> static cudaError_t launch_d(const SweepParams& p, dim3 grid, cudaStream_t s) {
+    return p.d == 0 ? launch<P, 0, MODE>(p, grid, s) : (p.d == 1 ? launch<P, 1, MODE>(p, grid, s) : launch<P, 2, MODE>(p, grid, s));
+}
+
+template <int MODE> static cudaError_t launch_p(int P, const SweepParams& p, dim3 grid, cudaStream_t s) {
     switch (P) {
-        EMG_CASE(8)
-        EMG_CASE(16)
-        EMG_CASE(32)
+        case 8: return launch_d<8, MODE>(p, grid, s);
+        case 16: return launch_d<16, MODE>(p, grid, s);
+        case 32: return launch_d<32, MODE>(p, grid, s);
         default: return cudaErrorInvalidValue;
     }
-#undef EMG_CASE
+}
+
+cudaError_t sweep_launch_f64(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s) {
+    switch (mode) {
+        case MODE_WENO: return launch_p<MODE_WENO>(P, p, grid, s);
+        case MODE_HYBRID: return launch_p<MODE_HYBRID>(P, p, grid, s);
+        case MODE_CENTRAL: return launch_p<MODE_CENTRAL>(P, p, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int P, int MODE> static cudaError_t attr_d() {
+    cudaError_t e = cudaSuccess;
+    const int b = (int)SweepSmem<double, P, MODE>::bytes();
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_f64_kernel<P, 0, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_f64_kernel<P, 1, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_f64_kernel<P, 2, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    return e;
+}
+
+template <int MODE> static cudaError_t attr_p() {
+    cudaError_t e = attr_d<8, MODE>();
+    if (e == cudaSuccess) e = attr_d<16, MODE>();
+    if (e == cudaSuccess) e = attr_d<32, MODE>();
+    return e;
 }
 
 cudaError_t sweep_prepare_f64() {
-    cudaError_t e = cudaSuccess;
-#define EMG_ATTR(PP, DD)                                                                              \
-    if (e == cudaSuccess)                                                                             \
-        e = cudaFuncSetAttribute(sweep_f64_kernel<PP, DD>, cudaFuncAttributeMaxDynamicSharedMemorySize,          \
-                                 (int)SweepSmem<double, PP>::bytes());
-    EMG_ATTR(8, 0) EMG_ATTR(8, 1) EMG_ATTR(8, 2)
-    EMG_ATTR(16, 0) EMG_ATTR(16, 1) EMG_ATTR(16, 2)
-    EMG_ATTR(32, 0) EMG_ATTR(32, 1) EMG_ATTR(32, 2)
-#undef EMG_ATTR
+    cudaError_t e = attr_p<MODE_WENO>();
+    if (e == cudaSuccess) e = attr_p<MODE_HYBRID>();
+    if (e == cudaSuccess) e = attr_p<MODE_CENTRAL>();
     return e;
 }
 

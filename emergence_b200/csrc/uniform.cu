@@ -438,7 +438,8 @@ void plan_sweeps(emg_uniform* h) {
         h->lane_axis[d] = lane;
         h->other_axis[d] = other;
         const int64_t nd = h->mesh.n[d], nl = h->mesh.n[lane], nother = h->mesh.n[other];
-        int P = 32;
+        // hybrid rings hold RM + 9 rows: P = 16 keeps them at 2 CTAs per SM
+        int P = h->opts.mode == EMG_MODE_HYBRID ? 16 : 32;
         if (nl <= 8)
             P = 8;
         else if (nl <= 16)
@@ -542,9 +543,10 @@ int launch_stage(emg_uniform* h, int stage) {
             }
         }
         ProfScope ps(h, EMG_K_AXIS_0 + d);
+        p.tol = h->opts.tol;
         cudaError_t e = h->opts.precision == EMG_PRECISION_MIXED
-                            ? sweep_launch_mixed(h->sweepP[d], p, h->sweepGrid[d], h->stream)
-                            : sweep_launch_f64(h->sweepP[d], p, h->sweepGrid[d], h->stream);
+                            ? sweep_launch_mixed(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream)
+                            : sweep_launch_f64(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream);
         if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("sweep launch: ") + cudaGetErrorString(e));
     }
     return EMG_OK;
@@ -664,8 +666,10 @@ int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc
         }
     }
     if (ndim == 0) return set_error(EMG_ERR_INVALID, "mesh has no active axis");
-    if (opts->mode != EMG_MODE_WENO)
-        return set_error(EMG_ERR_INVALID, "flux mode not supported by the device kernels (use EMG_MODE_WENO)");
+    if (opts->mode != EMG_MODE_WENO && opts->mode != EMG_MODE_HYBRID && opts->mode != EMG_MODE_CENTRAL)
+        return set_error(EMG_ERR_INVALID, "unknown flux mode");
+    if (opts->mode == EMG_MODE_HYBRID && !(opts->tol > 0.0))
+        return set_error(EMG_ERR_INVALID, "hybrid mode needs tol > 0");
     if (opts->precision != EMG_PRECISION_F64 && opts->precision != EMG_PRECISION_MIXED)
         return set_error(EMG_ERR_INVALID, "unknown precision");
     for (int i = 0; i < 6; i++)
@@ -904,7 +908,7 @@ int emg_uniform_counters(emg_uniform* h, uint64_t out[4]) {
     rc = sync_ctl(h);
     if (rc) return rc;
     out[0] = h->faces;
-    out[1] = h->weno_faces;
+    out[1] = h->weno_faces + h->ctl_host->counters[1];  // WENO mode counted on the host, hybrid on the device
     out[2] = h->ctl_host->counters[2];
     out[3] = h->ctl_host->counters[3];
     return EMG_OK;

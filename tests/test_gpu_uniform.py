@@ -213,3 +213,65 @@ def test_unsupported_options_are_rejected():
     from emergence_b200 import EmgError
     with pytest.raises(EmgError):
         gpu_solver(sys, mesh.with_ghosts(4), np.zeros((mesh.with_ghosts(4).len(), 5)), bc=bc, mode=FluxMode.Weno)
+
+
+@pytest.mark.parametrize("shape", [(64, 1, 1), (48, 40, 1), (20, 18, 16)])
+def test_central_mode_matches_the_oracle_bitwise(shape):
+    mesh, u = random_state(shape, seed=3, jump=False)
+    bc = BC_SETS["periodic"]
+    g = gpu_solver(SYS, mesh, u, bc=bc, mode=FluxMode.Central)
+    o = O.OracleSolver(SYS, mesh, u, bc=bc, mode=FluxMode.Central)
+    for _ in range(3):
+        dt = o.dt_cfl()
+        g.step(dt)
+        o.step(dt)
+    assert np.array_equal(g.download(), o.download())
+    assert g.counters() == o.counters()
+
+
+@pytest.mark.parametrize("n", [(2, 1, 1), (1, 3, 1), (1, 1, 2), (2, 3, 4)])
+@pytest.mark.parametrize("ng", [6, 10])
+def test_periodic_axes_shorter_than_the_ghost_width_preserve_uniform_flow(n, ng):
+    """tests/cpu.rs:266-298 on the device (central mode, no limiter)."""
+    expected = np.array([1.0, 0.3, -0.2, 0.1, 1.0])
+    mesh = Mesh.new(n, (0, 0, 0), (1, 1, 1), ng=ng)
+    u = initial_state(SYS, mesh, np.broadcast_to(expected, mesh.n + (5,)).copy())
+    g = gpu_solver(SYS, mesh, u, bc=BC_SETS["periodic"], mode=FluxMode.Central, positivity=False)
+    g.step(1e-5)
+    w = SYS.to_prim(mesh.interior(g.download()))
+    assert np.all(np.abs(w - expected) < 1e-13)
+
+
+@pytest.mark.parametrize("shape", [(96, 1, 1), (64, 56, 1), (24, 20, 18)])
+def test_hybrid_mode_matches_the_oracle(shape):
+    """Default reference mode: δ⁴ sensor switch between KEEP-PE central and WCNS."""
+    sys_, mesh, u, bc = W.explosion(shape, 0.3 if shape[2] > 1 else 0.4)
+    g = gpu_solver(sys_, mesh, u, bc=bc, mode=FluxMode.Hybrid)
+    o = O.OracleSolver(sys_, mesh, u, bc=bc, mode=FluxMode.Hybrid)
+    for _ in range(5):
+        dt = o.dt_cfl()
+        g.step(dt)
+        o.step(dt)
+    ug, uo = g.download(), o.download()
+    err = rel_l1(ug, uo, mesh)
+    print("hybrid", shape, "rel L1", err, "bitwise", np.array_equal(mesh.interior(ug), mesh.interior(uo)))
+    assert np.all(err <= F64_TOL)
+    cg, co = g.counters(), o.counters()
+    assert cg[0] == co[0]
+    assert 0 < co[1] <= co[0]
+    if shape[1] > 1:
+        assert co[1] < co[0]  # a genuine mix of central and shock-path faces
+    # the sensor's log may round differently from the host's in the last ulp,
+    # which can move a face across θ = 0 in rare cases
+    assert abs(cg[1] - co[1]) <= 0.001 * co[1]
+
+
+def test_hybrid_explosion_2d_256_short_run():
+    sys_, mesh, u, bc = W.explosion_2d(256)
+    g = gpu_solver(sys_, mesh, u, bc=bc, mode=FluxMode.Hybrid)
+    o = O.OracleSolver(sys_, mesh, u, bc=bc, mode=FluxMode.Hybrid)
+    assert g.advance(20) == 20
+    o.advance(20)
+    err = rel_l1(g.download(), o.download(), mesh)
+    print("hybrid explosion_2d 20 steps rel L1", err)
+    assert np.all(err <= F64_TOL)
