@@ -40,6 +40,14 @@ class EmgOpts(C.Structure):
                 ("precision", C.c_int32), ("reserved", C.c_int32)]
 
 
+class EmgAmrConfig(C.Structure):
+    _fields_ = [("b", C.c_int64), ("levels", C.c_int64), ("eps", C.c_double), ("regrid_every", C.c_int64),
+                ("base_blocks", C.c_int64 * 3), ("ghosts", C.c_int64)]
+
+
+# void (*)(void* ctx, const double* x, int64_t n, double* w)
+INIT_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.c_int64, C.POINTER(C.c_double))
+
 EMG_K_COUNT = 5
 KERNEL_KINDS = ("ghost", "axis0", "axis1", "axis2", "cfl")
 

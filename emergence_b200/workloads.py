@@ -63,3 +63,89 @@ def explosion_2d(n=256, seed=SEED):
 def explosion_3d(n=256, seed=SEED):
     """3-D spherical explosion, radius 0.3."""
     return explosion((n, n, n), 0.3, seed)
+
+
+# ---------------------------------------------------------------- block AMR
+def rankine_hugoniot(mach, gamma=1.4, rho1=1.0, p1=1.0):
+    """Post-shock (ρ, u, p) and shock speed of a shock moving into gas at rest."""
+    m2 = mach * mach
+    rho2 = rho1 * (gamma + 1.0) * m2 / ((gamma - 1.0) * m2 + 2.0)
+    p2 = p1 * (1.0 + 2.0 * gamma / (gamma + 1.0) * (m2 - 1.0))
+    s = mach * np.sqrt(gamma * p1 / rho1)
+    return rho2, s * (1.0 - rho1 / rho2), p2, s
+
+
+def _interface_noise(seed, theta, phi, modes=4):
+    """Seeded low-mode angular perturbation in [-1, 1] (sum of products of
+    cos(nθ) and cos(mφ + φ_nm), n ≤ modes, m ≤ n, normalised)."""
+    rng = np.random.default_rng(seed)
+    xi = np.zeros_like(theta)
+    norm = 0.0
+    for n in range(1, modes + 1):
+        for m in range(0, n + 1):
+            a, ph = rng.uniform(-1.0, 1.0), rng.uniform(0.0, 2 * np.pi)
+            xi = xi + a * np.cos(n * theta) * np.cos(m * phi + ph)
+            norm += abs(a)
+    return xi / norm
+
+
+def shock_bubble(dim=3, base=8, b=16, levels=3, eps=1e-3, regrid_every=4, seed=SEED, x_shock=0.2, radius=0.15,
+                 rho_bubble=0.138, mach=2.0, gamma=1.4, ghosts=5):
+    """Mach-2 planar shock (moving +x) hitting a light bubble in pressure
+    equilibrium on [0,1]^dim. Returns (sys, cfg, lo, hi, bc, init) where
+    init(x[n,3]) -> primitive w[n,5]. Inflow (x low) is Dirichlet at the
+    post-shock state, all other sides outflow."""
+    from .physics import Bc, Euler, Nasg
+    sys_ = Euler(Nasg.ideal(gamma))
+    rho2, u2, p2, _ = rankine_hugoniot(mach, gamma)
+    cfg = dict(b=b, levels=levels, eps=eps, regrid_every=regrid_every,
+               base_blocks=[base] * dim + [0] * (3 - dim), ghosts=ghosts)
+    lo = (0.0, 0.0, 0.0)
+    hi = (1.0, 1.0, 1.0)
+    centre = np.array([0.5, 0.5, 0.5])
+
+    def init(x):
+        rel = x - centre
+        if dim == 2:
+            rel[:, 2] = 0.0
+        r = np.sqrt((rel * rel).sum(axis=1))
+        theta = np.arccos(np.clip(np.where(r > 0, rel[:, 2] / np.where(r > 0, r, 1), 0.0), -1, 1))
+        phi = np.arctan2(rel[:, 1], rel[:, 0])
+        rb = radius * (1.0 + 0.005 * _interface_noise(seed, theta, phi))
+        w = np.zeros((x.shape[0], 5))
+        w[:, 0] = np.where(r < rb, rho_bubble, 1.0)
+        w[:, 4] = 1.0
+        post = x[:, 0] < x_shock
+        w[post, 0] = rho2
+        w[post, 1] = u2
+        w[post, 4] = p2
+        return w
+
+    far = sys_.to_cons(np.array([rho2, u2, 0.0, 0.0, p2]))
+    bc = [[Bc.dirichlet(far), Bc.Outflow], [Bc.Outflow, Bc.Outflow], [Bc.Outflow, Bc.Outflow]]
+    return sys_, cfg, lo, hi, bc, init
+
+
+def amr_explosion(dim=2, base=4, b=16, levels=3, eps=1e-3, regrid_every=4, radius=0.3, seed=SEED, noise=0.0):
+    """Circular/spherical explosion on the block-AMR grid (outflow sides)."""
+    from .physics import Bc, Euler, Nasg
+    sys_ = Euler(Nasg.ideal(1.4))
+    cfg = dict(b=b, levels=levels, eps=eps, regrid_every=regrid_every,
+               base_blocks=[base] * dim + [0] * (3 - dim), ghosts=5)
+
+    def init(x):
+        rel = x - 0.5
+        if dim == 2:
+            rel[:, 2] = 0.0
+        r = np.sqrt((rel * rel).sum(axis=1))
+        w = np.zeros((x.shape[0], 5))
+        w[:, 0] = np.where(r < radius, 1.0, 0.125)
+        w[:, 4] = np.where(r < radius, 1.0, 0.1)
+        if noise:
+            key = np.floor(x * 1e6).astype(np.int64)
+            idx = (key[:, 0] * 73856093 ^ key[:, 1] * 19349663 ^ key[:, 2] * 83492791).astype(np.uint64)
+            w[:, 0] *= 1.0 + noise * uniform_pm1(seed, idx)
+        return w
+
+    bc = [[Bc.Outflow, Bc.Outflow] for _ in range(3)]
+    return sys_, cfg, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), bc, init

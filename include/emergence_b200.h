@@ -189,6 +189,88 @@ int emg_uniform_kernel_times(emg_uniform* h, double* ms, uint64_t* launches);
 /* Number of kernel launches issued by the handle since creation. */
 int emg_uniform_launch_count(emg_uniform* h, uint64_t* launches);
 
+/* ------------------------------------------------------------------ block AMR */
+
+/* Block-AMR configuration (C/amr.rs:49-63). Blocks are b cells per active
+ * side; base_blocks[d] = 0 marks an inactive axis; ghosts ≥ 5 is enforced. */
+typedef struct emg_amr_config {
+    int64_t b;
+    int64_t levels;
+    double eps;
+    int64_t regrid_every;
+    int64_t base_blocks[3];
+    int64_t ghosts;
+} emg_amr_config;
+
+/* Primitive initial condition: fills w[i*5 + 0..4] = (ρ,u,v,w,p) at the n cell
+ * centres x[i*3 + 0..2]; called once per new block (the closure of
+ * Amr::new, C/amr.rs:289). */
+typedef void (*emg_init_fn)(void* ctx, const double* x, int64_t n, double* w);
+
+typedef struct emg_amr emg_amr;
+
+/* Build the hierarchy on the device like Amr::new (base blocks, then refine
+ * on the initial data until the details are resolved, C/amr.rs:289-344) and
+ * keep it there (GpuAmr::new, G/amr.rs:95-212). opts->cfl is the AMR CFL
+ * number (0.4 in the reference). */
+int emg_amr_create(const emg_amr_config* cfg, const emg_eos* eos, const double lo[3], const double hi[3],
+                   const emg_bc bc[6], const emg_opts* opts, emg_init_fn init, void* ctx, emg_amr** out);
+
+/* Adopt an existing hierarchy (what GpuAmr::new receives from a CPU Amr):
+ * nblocks blocks with (level, i, j, k, leaf) in `desc[5*id..]` and conserved
+ * block data `u[id][cell][5]` (b^D cells per block, no ghosts). */
+int emg_amr_create_from_blocks(const emg_amr_config* cfg, const emg_eos* eos, const double lo[3], const double hi[3],
+                               const emg_bc bc[6], const emg_opts* opts, const int64_t* desc, size_t nblocks,
+                               const double* u, emg_amr** out);
+
+int emg_amr_destroy(emg_amr* h);
+
+/* One global SSP-RK3 step of size dt, regridding when due (Amr::step,
+ * C/amr.rs:1470-1512; GpuAmr::step, G/amr.rs:683-700). */
+int emg_amr_step(emg_amr* h, double dt);
+
+/* Global CFL step over the leaves (C/amr.rs:1409-1467; G/amr.rs:769-805). */
+int emg_amr_dt_cfl(emg_amr* h, double* dt);
+
+/* Advance to t_end (C/amr.rs:1639-1652): stops at t ≥ t_end(1 − 1e-14). */
+int emg_amr_run_to(emg_amr* h, double t_end, uint64_t* steps);
+
+/* Regrid now (C/amr.rs:1039-1046). */
+int emg_amr_regrid(emg_amr* h);
+
+/* Number of blocks (leaves and ancestors) and of leaves. */
+int emg_amr_block_count(emg_amr* h, uint64_t* blocks, uint64_t* leaves);
+
+/* Hierarchy: (level, i, j, k, leaf) per block in id order (Amr::structure,
+ * C/amr.rs:1539-1541); `cap` blocks of room. */
+int emg_amr_structure(emg_amr* h, int64_t* desc, size_t cap);
+
+/* Block data u[id][cell][5] of all blocks (GpuAmr::download, G/amr.rs:821-843). */
+int emg_amr_download(emg_amr* h, double* u, size_t nblocks);
+
+/* Σ u·vol over leaves (C/amr.rs:1991-2005). */
+int emg_amr_totals(emg_amr* h, double out[5]);
+
+/* [faces, shock-path faces, fallbacks, limited faces] since creation. */
+int emg_amr_counters(emg_amr* h, uint64_t out[4]);
+
+int emg_amr_get_time(emg_amr* h, double* t);
+
+/* Steps taken so far (Amr::steps). */
+int emg_amr_steps(emg_amr* h, uint64_t* steps);
+
+int emg_amr_synchronize(emg_amr* h);
+
+/* The handle's CUDA stream (cudaStream_t) as an opaque pointer. */
+int emg_amr_stream(emg_amr* h, void** stream);
+
+/* Per-phase device milliseconds since the last call:
+ * [restrict, ghosts, fluxes, reflux+update, regrid] (GpuAmr::prof, G/amr.rs:111-116). */
+int emg_amr_phase_times(emg_amr* h, double out[5]);
+
+/* Kernel launches issued by the handle since creation. */
+int emg_amr_launch_count(emg_amr* h, uint64_t* launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,6 +5,7 @@
 // the tests drive the oracle and the CUDA library through identical calls.
 // Loaded only by tests/, __graft_entry__.smoke() and bench.py's CPU leg.
 #include "oracle.hpp"
+#include "amr_oracle.hpp"
 #include "../include/emergence_b200.h"
 
 #include <cstdio>
@@ -270,6 +271,118 @@ int emgo_exact_sample(const double l[3], const double r[3], const emg_eos* eos_l
     Side R{r[0], r[1], r[2], Nasg<double>{eos_r->gamma, eos_r->p_inf, eos_r->b, eos_r->q, eos_r->cv}};
     Star s = star(L, R);
     for (size_t i = 0; i < n; i++) sample(L, R, s, xi[i], out + 3 * i);
+    return EMG_OK;
+}
+
+
+// ---- block AMR (amr_oracle.hpp)
+namespace {
+InitFn wrap_init(emg_init_fn f, void* ctx) {
+    return [f, ctx](const double* x, int64_t n, double* w) { f(ctx, x, n, w); };
+}
+AmrConfig to_cfg(const emg_amr_config* c) {
+    AmrConfig r;
+    r.b = c->b;
+    r.levels = c->levels;
+    r.eps = c->eps;
+    r.regrid_every = c->regrid_every;
+    for (int d = 0; d < 3; d++) r.base_blocks[d] = c->base_blocks[d];
+    r.ghosts = c->ghosts;
+    return r;
+}
+}  // namespace
+
+int emgo_amr_create(const emg_amr_config* cfg, const emg_eos* eos, const double lo[3], const double hi[3],
+                    const emg_bc bc[6], const emg_opts* opts, emg_init_fn init, void* ctx, void** out) {
+    if (!cfg || !eos || !lo || !hi || !bc || !opts || !init || !out) return fail(EMG_ERR_INVALID, "null argument");
+    Bc<double> b[3][2];
+    for (int d = 0; d < 3; d++)
+        for (int s = 0; s < 2; s++) {
+            b[d][s].kind = bc[2 * d + s].kind;
+            for (int k = 0; k < 5; k++) b[d][s].state[k] = bc[2 * d + s].state[k];
+        }
+    Amr* a = new Amr(to_sys(eos), to_cfg(cfg), lo, hi, b, wrap_init(init, ctx));
+    a->cfl = opts->cfl;
+    a->tol = opts->tol;
+    a->mode = opts->mode;
+    a->positivity = opts->positivity != 0;
+    *out = a;
+    return EMG_OK;
+}
+int emgo_amr_destroy(void* h) {
+    delete (Amr*)h;
+    return EMG_OK;
+}
+int emgo_amr_step(void* h, double dt) {
+    ((Amr*)h)->step(dt);
+    return EMG_OK;
+}
+int emgo_amr_dt_cfl(void* h, double* dt) {
+    *dt = ((Amr*)h)->dt_cfl();
+    return EMG_OK;
+}
+int emgo_amr_run_to(void* h, double t_end, uint64_t* steps) {
+    int64_t n = ((Amr*)h)->run_to(t_end);
+    if (n < 0) return fail(EMG_ERR_DT_COLLAPSED, "time step collapsed");
+    if (steps) *steps = (uint64_t)n;
+    return EMG_OK;
+}
+int emgo_amr_regrid(void* h) {
+    ((Amr*)h)->regrid();
+    return EMG_OK;
+}
+int emgo_amr_block_count(void* h, uint64_t* blocks, uint64_t* leaves) {
+    Amr* a = (Amr*)h;
+    if (blocks) *blocks = a->blocks.size();
+    if (leaves) *leaves = (uint64_t)a->leaf_count();
+    return EMG_OK;
+}
+int emgo_amr_structure(void* h, int64_t* desc, size_t cap) {
+    Amr* a = (Amr*)h;
+    if (cap < a->blocks.size()) return fail(EMG_ERR_INVALID, "structure buffer too small");
+    for (size_t i = 0; i < a->blocks.size(); i++) {
+        desc[5 * i] = a->blocks[i].level;
+        for (int d = 0; d < 3; d++) desc[5 * i + 1 + d] = a->blocks[i].idx[d];
+        desc[5 * i + 4] = a->blocks[i].leaf ? 1 : 0;
+    }
+    return EMG_OK;
+}
+int emgo_amr_download(void* h, double* u, size_t nblocks) {
+    Amr* a = (Amr*)h;
+    if (nblocks < a->blocks.size()) return fail(EMG_ERR_INVALID, "buffer too small");
+    size_t bc_ = (size_t)a->bcells();
+    for (size_t i = 0; i < a->blocks.size(); i++)
+        std::memcpy(u + i * bc_ * 5, a->blocks[i].u.data(), bc_ * 5 * sizeof(double));
+    return EMG_OK;
+}
+int emgo_amr_totals(void* h, double out[5]) {
+    V5<double> t = ((Amr*)h)->totals();
+    for (int k = 0; k < 5; k++) out[k] = t[k];
+    return EMG_OK;
+}
+int emgo_amr_counters(void* h, uint64_t out[4]) {
+    Stats& s = ((Amr*)h)->stats;
+    out[0] = s.faces;
+    out[1] = s.weno_faces;
+    out[2] = s.fallback_faces;
+    out[3] = s.limited_faces;
+    return EMG_OK;
+}
+int emgo_amr_get_time(void* h, double* t) {
+    *t = ((Amr*)h)->t;
+    return EMG_OK;
+}
+int emgo_amr_steps(void* h, uint64_t* s) {
+    *s = (uint64_t)((Amr*)h)->steps;
+    return EMG_OK;
+}
+// per-leaf wavelet details in block id order (ancestors 0), C/amr.rs:823-867
+int emgo_amr_details(void* h, double* out, size_t cap) {
+    Amr* a = (Amr*)h;
+    if (cap < a->blocks.size()) return fail(EMG_ERR_INVALID, "buffer too small");
+    a->restrict_all();
+    std::vector<double> d = a->details();
+    for (size_t i = 0; i < d.size(); i++) out[i] = d[i];
     return EMG_OK;
 }
 

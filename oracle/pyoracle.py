@@ -299,3 +299,147 @@ def exact_sample(left, right, xi, eos_l, eos_r=None):
     _chk(lib().emgo_exact_sample(dptr(arr(left)), dptr(arr(right)), C.byref(el), C.byref(er), dptr(xi), xi.size,
                                  dptr(out)))
     return out  # rho, u, p per xi
+
+
+# ---- block AMR (amr_oracle.hpp)
+from emergence_b200._abi import EmgAmrConfig, INIT_FN  # noqa: E402
+
+SIGS_AMR = {
+    "emgo_amr_create": (C.c_int, [C.POINTER(EmgAmrConfig), C.POINTER(EmgEos), _D, _D, C.POINTER(EmgBc),
+                                  C.POINTER(EmgOpts), INIT_FN, C.c_void_p, C.POINTER(_P)]),
+    "emgo_amr_destroy": (C.c_int, [_P]),
+    "emgo_amr_step": (C.c_int, [_P, C.c_double]),
+    "emgo_amr_dt_cfl": (C.c_int, [_P, _D]),
+    "emgo_amr_run_to": (C.c_int, [_P, C.c_double, _U64]),
+    "emgo_amr_regrid": (C.c_int, [_P]),
+    "emgo_amr_block_count": (C.c_int, [_P, _U64, _U64]),
+    "emgo_amr_structure": (C.c_int, [_P, C.POINTER(C.c_int64), C.c_size_t]),
+    "emgo_amr_download": (C.c_int, [_P, _D, C.c_size_t]),
+    "emgo_amr_totals": (C.c_int, [_P, _D]),
+    "emgo_amr_counters": (C.c_int, [_P, _U64]),
+    "emgo_amr_get_time": (C.c_int, [_P, _D]),
+    "emgo_amr_steps": (C.c_int, [_P, _U64]),
+    "emgo_amr_details": (C.c_int, [_P, _D, C.c_size_t]),
+}
+
+
+def _amr_lib():
+    L = lib()
+    if not getattr(L, "_amr_ready", False):
+        for name, (res, args) in SIGS_AMR.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        L._amr_ready = True
+    return L
+
+
+def make_init(fn):
+    """Wrap a numpy init(x[n,3]) -> w[n,5] as the C callback type."""
+    def cb(ctx, x, n, w):
+        xa = np.ctypeslib.as_array(x, shape=(n, 3)).copy()
+        wa = np.ctypeslib.as_array(w, shape=(n, 5))
+        wa[...] = fn(xa)
+    return INIT_FN(cb)
+
+
+def c_amr_config(cfg):
+    c = EmgAmrConfig()
+    c.b, c.levels, c.eps, c.regrid_every, c.ghosts = cfg["b"], cfg["levels"], cfg["eps"], cfg["regrid_every"], cfg["ghosts"]
+    for d in range(3):
+        c.base_blocks[d] = cfg["base_blocks"][d]
+    return c
+
+
+class OracleAmr:
+    """C++ restatement of ``compressible::amr::Amr`` (global time step)."""
+
+    def __init__(self, sys, cfg, lo, hi, bc, init, cfl=0.4, mode=FluxMode.Hybrid, tol=1e-3, positivity=True):
+        from emergence_b200.solver import _c_bcs
+        L = _amr_lib()
+        self.cfg = dict(cfg)
+        self._c = c_amr_config(cfg)
+        self._e = c_eos(sys.eos)
+        self._b = _c_bcs(bc)
+        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, 0, 0)
+        self._cb = make_init(init)
+        lo_, hi_ = arr(lo), arr(hi)
+        h = C.c_void_p()
+        _chk(L.emgo_amr_create(C.byref(self._c), C.byref(self._e), dptr(lo_), dptr(hi_), self._b, C.byref(self._o),
+                               self._cb, None, C.byref(h)))
+        self._h = h
+        self.bcells = 1
+        for d in range(3):
+            self.bcells *= cfg["b"] if cfg["base_blocks"][d] > 0 else 1
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _amr_lib().emgo_amr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, dt):
+        _chk(_amr_lib().emgo_amr_step(self._h, float(dt)))
+
+    def dt_cfl(self):
+        v = C.c_double()
+        _chk(_amr_lib().emgo_amr_dt_cfl(self._h, C.byref(v)))
+        return v.value
+
+    def run_to(self, t_end):
+        n = C.c_uint64()
+        _chk(_amr_lib().emgo_amr_run_to(self._h, float(t_end), C.byref(n)))
+        return n.value
+
+    def regrid(self):
+        _chk(_amr_lib().emgo_amr_regrid(self._h))
+
+    def block_count(self):
+        b, l = C.c_uint64(), C.c_uint64()
+        _chk(_amr_lib().emgo_amr_block_count(self._h, C.byref(b), C.byref(l)))
+        return b.value, l.value
+
+    def structure(self):
+        nb, _ = self.block_count()
+        out = np.zeros((nb, 5), dtype=np.int64)
+        _chk(_amr_lib().emgo_amr_structure(self._h, out.ctypes.data_as(C.POINTER(C.c_int64)), nb))
+        return out
+
+    def download(self):
+        nb, _ = self.block_count()
+        out = np.zeros((nb, self.bcells, 5))
+        _chk(_amr_lib().emgo_amr_download(self._h, dptr(out), nb))
+        return out
+
+    def totals(self):
+        out = np.zeros(5)
+        _chk(_amr_lib().emgo_amr_totals(self._h, dptr(out)))
+        return out
+
+    def counters(self):
+        out = (C.c_uint64 * 4)()
+        _chk(_amr_lib().emgo_amr_counters(self._h, out))
+        return list(out)
+
+    def details(self):
+        nb, _ = self.block_count()
+        out = np.zeros(nb)
+        _chk(_amr_lib().emgo_amr_details(self._h, dptr(out), nb))
+        return out
+
+    @property
+    def t(self):
+        v = C.c_double()
+        _chk(_amr_lib().emgo_amr_get_time(self._h, C.byref(v)))
+        return v.value
+
+    @property
+    def steps(self):
+        v = C.c_uint64()
+        _chk(_amr_lib().emgo_amr_steps(self._h, C.byref(v)))
+        return v.value
