@@ -35,11 +35,6 @@ class EmgBc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("state", C.c_double * 5)]
 
 
-class EmgOpts(C.Structure):
-    _fields_ = [("cfl", C.c_double), ("tol", C.c_double), ("mode", C.c_int32), ("positivity", C.c_int32),
-                ("precision", C.c_int32), ("reserved", C.c_int32)]
-
-
 class EmgAmrConfig(C.Structure):
     _fields_ = [("b", C.c_int64), ("levels", C.c_int64), ("eps", C.c_double), ("regrid_every", C.c_int64),
                 ("base_blocks", C.c_int64 * 3), ("ghosts", C.c_int64)]
@@ -47,6 +42,11 @@ class EmgAmrConfig(C.Structure):
 
 # void (*)(void* ctx, const double* x, int64_t n, double* w)
 INIT_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.c_int64, C.POINTER(C.c_double))
+
+class EmgOpts(C.Structure):
+    _fields_ = [("cfl", C.c_double), ("tol", C.c_double), ("mode", C.c_int32), ("positivity", C.c_int32),
+                ("precision", C.c_int32), ("reserved", C.c_int32)]
+
 
 EMG_K_COUNT = 5
 KERNEL_KINDS = ("ghost", "axis0", "axis1", "axis2", "cfl")
@@ -78,6 +78,26 @@ SIGNATURES = {
     "emg_uniform_set_profiling": (C.c_int, [_P, C.c_int]),
     "emg_uniform_kernel_times": (C.c_int, [_P, _D, _U64]),
     "emg_uniform_launch_count": (C.c_int, [_P, _U64]),
+    "emg_amr_create": (C.c_int, [C.POINTER(EmgAmrConfig), C.POINTER(EmgEos), _D, _D, C.POINTER(EmgBc),
+                                 C.POINTER(EmgOpts), INIT_FN, C.c_void_p, C.POINTER(_P)]),
+    "emg_amr_create_from_blocks": (C.c_int, [C.POINTER(EmgAmrConfig), C.POINTER(EmgEos), _D, _D, C.POINTER(EmgBc),
+                                             C.POINTER(EmgOpts), C.POINTER(C.c_int64), C.c_size_t, _D, C.POINTER(_P)]),
+    "emg_amr_destroy": (C.c_int, [_P]),
+    "emg_amr_step": (C.c_int, [_P, C.c_double]),
+    "emg_amr_dt_cfl": (C.c_int, [_P, _D]),
+    "emg_amr_run_to": (C.c_int, [_P, C.c_double, _U64]),
+    "emg_amr_regrid": (C.c_int, [_P]),
+    "emg_amr_block_count": (C.c_int, [_P, _U64, _U64]),
+    "emg_amr_structure": (C.c_int, [_P, C.POINTER(C.c_int64), C.c_size_t]),
+    "emg_amr_download": (C.c_int, [_P, _D, C.c_size_t]),
+    "emg_amr_totals": (C.c_int, [_P, _D]),
+    "emg_amr_counters": (C.c_int, [_P, _U64]),
+    "emg_amr_get_time": (C.c_int, [_P, _D]),
+    "emg_amr_steps": (C.c_int, [_P, _U64]),
+    "emg_amr_synchronize": (C.c_int, [_P]),
+    "emg_amr_stream": (C.c_int, [_P, C.POINTER(_P)]),
+    "emg_amr_phase_times": (C.c_int, [_P, _D]),
+    "emg_amr_launch_count": (C.c_int, [_P, _U64]),
 }
 
 _lib = None

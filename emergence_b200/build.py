@@ -4,6 +4,7 @@ Usage: python -m emergence_b200.build  (or import and call build()).
 
 Translation units and their FMA policy:
   uniform.cu      host object, ghost/CFL/control kernels, C ABI  -fmad=false
+  amr.cu          block-AMR host object, AMR kernels, C ABI      -fmad=false
   sweep_f64.cu    plain FP64 fused sweep                          -fmad=false
   sweep_mixed.cu  FP32-flux fused sweep                           -fmad=true
 The FP64 units keep every multiply and add separately rounded so that their
@@ -20,9 +21,10 @@ BUILD = os.path.join(HERE, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-          "--expt-relaxed-constexpr"]
+          "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr"]
 UNITS = [
     ("uniform.cu", ["-fmad=false"]),
+    ("amr.cu", ["-fmad=false"]),
     ("sweep_f64.cu", ["-fmad=false"]),
     ("sweep_mixed.cu", ["-fmad=true", "-use_fast_math"]),
 ]

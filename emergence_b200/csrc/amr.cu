@@ -1,0 +1,1493 @@
+// Block-AMR solver: host object and C ABI (emg_amr_*), replacing
+// compressible-cuda's GpuAmr (fluid/crates/compressible-cuda/src/amr.rs:95-858)
+// for the Euler system.
+//
+// The hierarchy bookkeeping (which blocks exist, block ids, 2:1 balance,
+// refine/coarsen decisions) runs on the host and keeps the block ids of the
+// reference CPU solver (fluid/crates/compressible/src/amr.rs), so the device
+// pool, indexed by block id, mirrors `Amr::blocks`. All numerical work —
+// restriction of edge ancestors, ghost slabs (same-level copies, 6th-order
+// prediction from the coarser level, boundary conditions), the fused WCNS
+// sweeps of every leaf, refluxing, SSP-RK3, the CFL reduction, wavelet details
+// and the data of refined / coarsened blocks — runs on the device; unlike the
+// reference GPU path, a regrid never downloads the solution (only one detail
+// value per block).
+//
+// Built with -fmad=false (FP64 arithmetic rounds as the reference CPU's).
+#include "../../include/emergence_b200.h"
+#include "amr_kernels.cuh"
+#include "sweep_launch.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <set>
+#include <string>
+#include <tuple>
+#include <vector>
+
+namespace emg {
+int set_error(int code, const std::string& msg);
+}
+
+using namespace emg;
+
+#define AMR_CUDA(call)                                                                             \
+    do {                                                                                           \
+        cudaError_t _e = (call);                                                                   \
+        if (_e != cudaSuccess)                                                                     \
+            return set_error(EMG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e));  \
+    } while (0)
+
+namespace {
+
+using Key = std::array<int64_t, 3>;
+
+int64_t ediv(int64_t a, int64_t b) {
+    int64_t q = a / b;
+    return (a % b < 0) ? q - 1 : q;
+}
+int64_t erem(int64_t a, int64_t b) {
+    int64_t r = a % b;
+    return r < 0 ? r + b : r;
+}
+
+// C/amr.rs:41-47
+std::array<double, 6> lagrange6(double x0, double x) {
+    std::array<double, 6> w;
+    for (int k = 0; k < 6; k++) {
+        double xk = x0 + k, p = 1.0;
+        for (int j = 0; j < 6; j++)
+            if (j != k) p = p * ((x - (x0 + j)) / (xk - (x0 + j)));
+        w[k] = p;
+    }
+    return w;
+}
+
+struct HBlock {
+    int level;
+    Key idx;
+    bool leaf;
+};
+
+template <class T> struct DevVec {
+    T* p = nullptr;
+    size_t n = 0, cap = 0;
+    int put(const std::vector<T>& v, cudaStream_t s) {
+        if (v.size() > cap) {
+            if (p) cudaFree(p);
+            cap = std::max<size_t>(v.size(), 2 * cap);
+            if (cudaMalloc(&p, cap * sizeof(T)) != cudaSuccess) {
+                p = nullptr;
+                cap = 0;
+                return set_error(EMG_ERR_CUDA, "device allocation failed");
+            }
+        }
+        n = v.size();
+        if (n && cudaMemcpyAsync(p, v.data(), n * sizeof(T), cudaMemcpyHostToDevice, s) != cudaSuccess)
+            return set_error(EMG_ERR_CUDA, "upload failed");
+        return EMG_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = cap = 0;
+    }
+};
+
+}  // namespace
+
+struct emg_amr {
+    // ---- configuration
+    emg_amr_config cfg{};
+    emg_eos eos{};
+    double lo[3]{}, hi[3]{};
+    emg_bc bc[6]{};
+    emg_opts opts{};
+    int act[3]{}, bd[3]{}, ext[3]{}, gof[3]{};
+    std::vector<int> dims;
+    int ng = 5;
+    int64_t nb0[3]{};
+    int levels = 1;
+    std::vector<double> dxl;  // [level][3]
+    double wp[2][6]{}, wr[6]{}, wrs[5][6]{};
+    // ---- hierarchy (block ids as in the reference's Amr::blocks)
+    std::vector<HBlock> blocks;
+    std::vector<std::vector<int>> map;
+    std::vector<int64_t> mapoff;
+    double t = 0.0;
+    int64_t steps = 0, regrid_interval = 0, next_regrid = 0;
+    uint64_t faces = 0, weno_faces = 0;
+    // ---- device
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int64_t bcell = 0, cap = 0;  // pool capacity in blocks
+    double *u = nullptr, *u0 = nullptr, *rhs = nullptr, *face = nullptr;
+    int npen = 1;
+    unsigned int* err = nullptr;
+    StepCtl* ctl = nullptr;
+    StepCtl* ctl_host = nullptr;
+    double* scr[2] = {nullptr, nullptr};
+    unsigned char* sok[2] = {nullptr, nullptr};
+    int64_t scr_cap = 0;
+    unsigned long long* det = nullptr;
+    int64_t det_cap = 0;
+    DevVec<int> dmap, dleaves, dlevel, dbcleaves, dcell_slot, dtask_start;
+    DevVec<int64_t> didx, dcell_ext;
+    DevVec<double> ddxl;
+    DevVec<CopyTask> dcopy;
+    DevVec<PBox> dpbox;
+    std::vector<DevVec<RBox>> drbox;  // per level
+    DevVec<RefluxTask> dreflux;
+    std::vector<int> rbox_count;
+    int ncopy = 0, npbox = 0, nbcleaves = 0, nrefcells = 0, nleaves = 0;
+    bool layout_valid = false, map_dirty = true;
+    uint64_t launches = 0;
+    double phase_ms[5]{};
+    bool rate_valid = false;
+
+    // ---------------------------------------------------------------- geometry
+    int64_t nbl(int l, int d) const { return act[d] ? nb0[d] << l : 1; }
+    int64_t n_level(int l, int d) const { return act[d] ? nb0[d] * bd[d] * ((int64_t)1 << l) : 1; }
+    int64_t bcells() const { return (int64_t)bd[0] * bd[1] * bd[2]; }
+    int bckind(int d, int s) const { return bc[2 * d + s].kind; }
+
+    // ---------------------------------------------------------------- index
+    int64_t slot_of(int l, const Key& k) const {
+        if (l < 0 || l >= levels) return -1;
+        int64_t s = 0;
+        for (int d = 0; d < 3; d++) {
+            int64_t n = nbl(l, d);
+            if (k[d] < 0 || k[d] >= n) return -1;
+            s = s * n + k[d];
+        }
+        return s;
+    }
+    int get(int l, const Key& k) const {
+        int64_t s = slot_of(l, k);
+        return s < 0 ? -1 : map[l][s];
+    }
+    void insert(int l, const Key& k, int id) {
+        int64_t s = slot_of(l, k);
+        if (s >= 0) map[l][s] = id;
+        map_dirty = true;
+        layout_valid = false;
+    }
+    void remove(int l, const Key& k) {
+        int64_t s = slot_of(l, k);
+        if (s >= 0) map[l][s] = -1;
+        map_dirty = true;
+        layout_valid = false;
+    }
+
+    // same-level neighbour keys with periodic wrap (C/amr.rs:918-947)
+    std::vector<Key> neighbours(int l, const Key& idx) const {
+        std::vector<Key> out;
+        int64_t nb[3];
+        for (int d = 0; d < 3; d++) nb[d] = nbl(l, d);
+        int r[3];
+        for (int d = 0; d < 3; d++) r[d] = act[d] ? 1 : 0;
+        for (int a = -r[0]; a <= r[0]; a++)
+            for (int b = -r[1]; b <= r[1]; b++)
+                for (int c = -r[2]; c <= r[2]; c++) {
+                    if (!a && !b && !c) continue;
+                    Key k = {idx[0] + a, idx[1] + b, idx[2] + c};
+                    bool inside = true;
+                    for (int d = 0; d < 3; d++)
+                        if (k[d] < 0 || k[d] >= nb[d]) {
+                            if (bckind(d, k[d] >= nb[d] ? 1 : 0) == EMG_BC_PERIODIC)
+                                k[d] = erem(k[d], nb[d]);
+                            else
+                                inside = false;
+                        }
+                    if (inside) out.push_back(k);
+                }
+        return out;
+    }
+    // C/amr.rs:894-915
+    std::vector<Key> children(const Key& idx) const {
+        std::vector<Key> out = {Key{0, 0, 0}};
+        for (int d = 0; d < 3; d++) {
+            std::vector<Key> next;
+            for (auto& c : out) {
+                if (act[d]) {
+                    for (int o = 0; o < 2; o++) {
+                        Key cc = c;
+                        cc[d] = 2 * idx[d] + o;
+                        next.push_back(cc);
+                    }
+                } else {
+                    Key cc = c;
+                    cc[d] = 0;
+                    next.push_back(cc);
+                }
+            }
+            out = next;
+        }
+        return out;
+    }
+    bool is_edge_ancestor(int i) const {  // C/amr.rs:741-744
+        const HBlock& b = blocks[i];
+        if (b.leaf) return false;
+        for (auto& nk : neighbours(b.level, b.idx)) {
+            int j = get(b.level, nk);
+            if (j < 0 || blocks[j].leaf) return true;
+        }
+        return false;
+    }
+
+    // ---------------------------------------------------------------- device helpers
+    AmrDev view() const {
+        AmrDev A{};
+        A.u = u;
+        A.ntot = cap * bcell;
+        A.bcell = bcell;
+        for (int d = 0; d < 3; d++) {
+            A.ext[d] = ext[d];
+            A.bd[d] = bd[d];
+            A.gof[d] = gof[d];
+            A.act[d] = act[d];
+            A.nb0[d] = nb0[d];
+            for (int s = 0; s < 2; s++) {
+                A.bc[d][s] = bckind(d, s);
+                for (int k = 0; k < 5; k++) A.bcs[d][s][k] = bc[2 * d + s].state[k];
+            }
+        }
+        A.ndims = (int)dims.size();
+        for (int i = 0; i < 3; i++) A.dims[i] = i < A.ndims ? dims[i] : 0;
+        A.ng = ng;
+        A.levels = levels;
+        A.map = dmap.p;
+        for (int l = 0; l < levels && l < AMR_MAX_LEVELS; l++) A.mapoff[l] = mapoff[l];
+        std::memcpy(A.wp, wp, sizeof wp);
+        std::memcpy(A.wr, wr, sizeof wr);
+        std::memcpy(A.wrs, wrs, sizeof wrs);
+        A.eos = EosD{eos.gamma, eos.p_inf, eos.b, eos.q};
+        A.err = err;
+        return A;
+    }
+
+    int upload_map() {
+        if (!map_dirty) return EMG_OK;
+        std::vector<int> flat;
+        for (auto& m : map) flat.insert(flat.end(), m.begin(), m.end());
+        int rc = dmap.put(flat, stream);
+        if (rc) return rc;
+        map_dirty = false;
+        return EMG_OK;
+    }
+
+    // grow the pool to hold at least n blocks, preserving block data
+    int reserve(int64_t n) {
+        if (n <= cap) return EMG_OK;
+        int64_t nc = std::max<int64_t>(n, cap + cap / 2 + 16);
+        double *nu = nullptr, *nu0 = nullptr, *nr = nullptr, *nf = nullptr;
+        const size_t bytes = (size_t)nc * bcell * 5 * sizeof(double);
+        const size_t fbytes = (size_t)nc * 3 * 2 * 5 * npen * sizeof(double);
+        if (cudaMalloc(&nu, bytes) != cudaSuccess || cudaMalloc(&nu0, bytes) != cudaSuccess ||
+            cudaMalloc(&nr, bytes) != cudaSuccess || cudaMalloc(&nf, fbytes) != cudaSuccess) {
+            cudaFree(nu);
+            cudaFree(nu0);
+            cudaFree(nr);
+            cudaFree(nf);
+            cudaGetLastError();
+            return set_error(EMG_ERR_CUDA, "AMR pool allocation failed");
+        }
+        cudaMemsetAsync(nu, 0, bytes, stream);
+        cudaMemsetAsync(nr, 0, bytes, stream);
+        cudaMemsetAsync(nf, 0, fbytes, stream);
+        if (u) {
+            // fields are strided by the capacity: copy field by field
+            for (int k = 0; k < 5; k++)
+                AMR_CUDA(cudaMemcpyAsync(nu + (size_t)k * nc * bcell, u + (size_t)k * cap * bcell,
+                                         (size_t)cap * bcell * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        }
+        AMR_CUDA(cudaStreamSynchronize(stream));
+        cudaFree(u);
+        cudaFree(u0);
+        cudaFree(rhs);
+        cudaFree(face);
+        u = nu;
+        u0 = nu0;
+        rhs = nr;
+        face = nf;
+        cap = nc;
+        return EMG_OK;
+    }
+
+    int scratch(int64_t cells) {
+        if (cells <= scr_cap) return EMG_OK;
+        int64_t nc = std::max<int64_t>(cells, scr_cap * 2);
+        for (int i = 0; i < 2; i++) {
+            cudaFree(scr[i]);
+            cudaFree(sok[i]);
+            scr[i] = nullptr;
+            sok[i] = nullptr;
+            if (cudaMalloc(&scr[i], (size_t)nc * 5 * sizeof(double)) != cudaSuccess ||
+                cudaMalloc(&sok[i], (size_t)nc) != cudaSuccess) {
+                cudaGetLastError();
+                scr_cap = 0;
+                return set_error(EMG_ERR_CUDA, "AMR scratch allocation failed");
+            }
+        }
+        scr_cap = nc;
+        return EMG_OK;
+    }
+
+    // x = box / task / leaf, y = chunks of its cells
+    static dim3 box_grid(int64_t maxcells, int nbox) {
+        int64_t gy = (maxcells + 255) / 256;
+        if (gy < 1) gy = 1;
+        if (gy > 64) gy = 64;
+        return dim3((unsigned)nbox, (unsigned)gy, 1);
+    }
+
+    // ---------------------------------------------------------------- prediction boxes
+    // predict_box(l, fmin, fmax) written to `slot` at ext coordinates t0 (C/amr.rs:548-586)
+    PBox make_pbox(int l, const Key& fmin, const Key& fmax, int slot, const int* t0) const {
+        PBox b{};
+        b.l = l;
+        b.slot = slot;
+        for (int d = 0; d < 3; d++) {
+            b.fmin[d] = fmin[d];
+            b.fsz[d] = (int)(fmax[d] - fmin[d] + 1);
+            b.cmin[d] = act[d] ? ediv(fmin[d], 2) - 3 : 0;
+            const int64_t cmax = act[d] ? ediv(fmax[d], 2) + 3 : 0;
+            b.csz[d] = (int)(cmax - b.cmin[d] + 1);
+            b.t0[d] = t0[d];
+        }
+        int64_t c = (int64_t)b.csz[0] * b.csz[1] * b.csz[2], mx = c;
+        int s[3] = {b.csz[0], b.csz[1], b.csz[2]};
+        for (int d : dims) {
+            s[d] = b.fsz[d];
+            mx = std::max<int64_t>(mx, (int64_t)s[0] * s[1] * s[2]);
+        }
+        b.cap = mx;
+        return b;
+    }
+
+    int run_pboxes(const PBox* dboxes, int nbox, int64_t maxcells) {
+        if (!nbox) return EMG_OK;
+        AmrDev A = view();
+        const dim3 gr = box_grid(maxcells, nbox);
+        pbox_gather<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0]);
+        for (int di = 0; di < (int)dims.size(); di++) pbox_bc<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], di);
+        pbox_fallback<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0]);
+        int cur = 0;
+        for (int di = 0; di < (int)dims.size(); di++) {
+            pbox_pass<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur], scr[1 - cur], di);
+            cur = 1 - cur;
+        }
+        pbox_scatter<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur]);
+        launches += 3 + 2 * dims.size();
+        AMR_CUDA(cudaGetLastError());
+        return EMG_OK;
+    }
+
+    // a one-off list of prediction boxes (refined children)
+    int predict_now(std::vector<PBox> boxes) {
+        int rc = upload_map();
+        if (rc) return rc;
+        int64_t off = 0, mx = 0;
+        for (auto& b : boxes) {
+            b.off = off;
+            off += b.cap;
+            mx = std::max(mx, b.cap);
+        }
+        if ((rc = scratch(off))) return rc;
+        DevVec<PBox> tmp;
+        if ((rc = tmp.put(boxes, stream))) return rc;
+        rc = run_pboxes(tmp.p, (int)boxes.size(), mx);
+        cudaStreamSynchronize(stream);
+        tmp.release();
+        return rc;
+    }
+
+    // ---------------------------------------------------------------- restriction boxes
+    // boxes of edge ancestor id (C/amr.rs:745-787)
+    std::vector<std::pair<std::array<int, 3>, std::array<int, 3>>> restrict_boxes(int id) const {
+        const HBlock& b = blocks[id];
+        int l = b.level;
+        std::vector<std::pair<std::array<int, 3>, std::array<int, 3>>> bx;
+        int r[3];
+        for (int d = 0; d < 3; d++) r[d] = act[d] ? 1 : 0;
+        for (int o0 = -r[0]; o0 <= r[0]; o0++)
+            for (int o1 = -r[1]; o1 <= r[1]; o1++)
+                for (int o2 = -r[2]; o2 <= r[2]; o2++) {
+                    int o[3] = {o0, o1, o2};
+                    if (!o0 && !o1 && !o2) continue;
+                    Key nk;
+                    bool skip = false;
+                    for (int d = 0; d < 3; d++) {
+                        nk[d] = b.idx[d] + o[d];
+                        const int64_t n = nbl(l, d);
+                        if (nk[d] < 0 || nk[d] >= n) {
+                            if (bckind(d, nk[d] >= n ? 1 : 0) == EMG_BC_PERIODIC)
+                                nk[d] = erem(nk[d], n);
+                            else
+                                skip = true;
+                        }
+                    }
+                    if (skip) continue;
+                    int j = get(l, nk);
+                    if (j >= 0 && !blocks[j].leaf) continue;
+                    const int w = std::min(ng + 3, std::max(bd[0], std::max(bd[1], bd[2])));
+                    std::array<int, 3> lo_, hi_;
+                    for (int d = 0; d < 3; d++) {
+                        lo_[d] = o[d] == 1 ? std::max(bd[d] - w, 0) : 0;
+                        hi_[d] = o[d] == -1 ? std::min(w, bd[d]) : bd[d];
+                    }
+                    bx.push_back({lo_, hi_});
+                }
+        int64_t vol = 0;
+        for (auto& p : bx) vol += (int64_t)(p.second[0] - p.first[0]) * (p.second[1] - p.first[1]) * (p.second[2] - p.first[2]);
+        if (2 * vol > bcells()) {
+            bx.clear();
+            bx.push_back({{0, 0, 0}, {bd[0], bd[1], bd[2]}});
+        }
+        return bx;
+    }
+
+    RBox make_rbox(int l, int slot, const Key& idx, const std::array<int, 3>& lo_, const std::array<int, 3>& hi_) const {
+        RBox b{};
+        b.l = l;
+        b.slot = slot;
+        for (int d = 0; d < 3; d++) {
+            b.lo[d] = lo_[d];
+            b.hi[d] = hi_[d];
+            const int64_t c0 = idx[d] * bd[d] + lo_[d];
+            b.f0[d] = act[d] ? 2 * c0 - 4 : 0;
+            b.sz[d] = act[d] ? 2 * (hi_[d] - lo_[d]) + 8 : 1;
+        }
+        b.cap = (int64_t)b.sz[0] * b.sz[1] * b.sz[2];
+        return b;
+    }
+
+    int run_rboxes(const RBox* dboxes, int nbox, int64_t maxcells) {
+        if (!nbox) return EMG_OK;
+        AmrDev A = view();
+        const dim3 gr = box_grid(maxcells, nbox);
+        rbox_gather<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0]);
+        for (int di = 0; di < (int)dims.size(); di++) rbox_bc<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], di);
+        int cur = 0;
+        for (int di = 0; di < (int)dims.size(); di++) {
+            rbox_pass<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur], sok[cur], scr[1 - cur], sok[1 - cur], di);
+            cur = 1 - cur;
+        }
+        rbox_scatter<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur]);
+        launches += 2 + 2 * dims.size();
+        AMR_CUDA(cudaGetLastError());
+        return EMG_OK;
+    }
+
+    // restrict_all with the current hierarchy (C/amr.rs:737-816), finest first
+    int restrict_all() {
+        int rc = ensure_layout();
+        if (rc) return rc;
+        for (int l = levels - 2; l >= 0; l--) {
+            if (!rbox_count[l]) continue;
+            if ((rc = run_rboxes(drbox[l].p, rbox_count[l], rbox_max[l]))) return rc;
+        }
+        return EMG_OK;
+    }
+    std::vector<int64_t> rbox_max;
+
+    // ---------------------------------------------------------------- layout
+    int ensure_layout() {
+        if (layout_valid) return upload_map();
+        int rc = upload_map();
+        if (rc) return rc;
+        std::vector<int> leaves, lvl(blocks.size()), bcl;
+        std::vector<int64_t> idx(3 * blocks.size());
+        for (size_t i = 0; i < blocks.size(); i++) {
+            lvl[i] = blocks[i].level;
+            for (int d = 0; d < 3; d++) idx[3 * i + d] = blocks[i].idx[d];
+            if (blocks[i].leaf) leaves.push_back((int)i);
+        }
+        nleaves = (int)leaves.size();
+        // ghost slabs of every leaf (C/amr.rs:1148-1203)
+        std::vector<CopyTask> copies;
+        std::vector<PBox> pboxes;
+        int64_t pmax = 0, poff = 0;
+        for (int id : leaves) {
+            const HBlock& b = blocks[id];
+            const int l = b.level;
+            int r[3];
+            for (int d = 0; d < 3; d++) r[d] = act[d] ? 1 : 0;
+            bool touches = false;
+            for (int o0 = -r[0]; o0 <= r[0]; o0++)
+                for (int o1 = -r[1]; o1 <= r[1]; o1++)
+                    for (int o2 = -r[2]; o2 <= r[2]; o2++) {
+                        int o[3] = {o0, o1, o2};
+                        if (!o0 && !o1 && !o2) continue;
+                        Key nk;
+                        bool inside = true;
+                        for (int d = 0; d < 3; d++) {
+                            nk[d] = b.idx[d] + o[d];
+                            const int64_t n = nbl(l, d);
+                            if (nk[d] < 0 || nk[d] >= n) {
+                                if (bckind(d, nk[d] >= n ? 1 : 0) == EMG_BC_PERIODIC)
+                                    nk[d] = erem(nk[d], n);
+                                else
+                                    inside = false;
+                            }
+                        }
+                        if (!inside) {
+                            touches = true;
+                            continue;
+                        }
+                        int nid = get(l, nk);
+                        if (nid >= 0) {
+                            copies.push_back(CopyTask{id, nid, {o[0], o[1], o[2]}});
+                            continue;
+                        }
+                        int rs[3], re[3];
+                        for (int d = 0; d < 3; d++) {
+                            if (!act[d]) {
+                                rs[d] = 0;
+                                re[d] = 1;
+                            } else if (o[d] == -1) {
+                                rs[d] = 0;
+                                re[d] = ng;
+                            } else if (o[d] == 0) {
+                                rs[d] = ng;
+                                re[d] = ng + bd[d];
+                            } else {
+                                rs[d] = ng + bd[d];
+                                re[d] = 2 * ng + bd[d];
+                            }
+                        }
+                        Key fmin, fmax;
+                        for (int d = 0; d < 3; d++) {
+                            fmin[d] = b.idx[d] * bd[d] + rs[d] - gof[d];
+                            fmax[d] = b.idx[d] * bd[d] + (re[d] - 1) - gof[d];
+                        }
+                        PBox pb = make_pbox(l, fmin, fmax, id, rs);
+                        pb.off = poff;
+                        poff += pb.cap;
+                        pmax = std::max(pmax, pb.cap);
+                        pboxes.push_back(pb);
+                    }
+            if (touches) bcl.push_back(id);
+        }
+        // restriction boxes per level
+        rbox_count.assign(levels, 0);
+        rbox_max.assign(levels, 0);
+        if ((int)drbox.size() < levels) drbox.resize(levels);
+        int64_t rneed = 0;
+        for (int l = levels - 2; l >= 0; l--) {
+            std::vector<RBox> rb;
+            int64_t off = 0;
+            for (size_t i = 0; i < blocks.size(); i++) {
+                if (blocks[i].level != l || !is_edge_ancestor((int)i)) continue;
+                for (auto& bx : restrict_boxes((int)i)) {
+                    RBox r = make_rbox(l, (int)i, blocks[i].idx, bx.first, bx.second);
+                    r.off = off;
+                    off += r.cap;
+                    rbox_max[l] = std::max(rbox_max[l], r.cap);
+                    rb.push_back(r);
+                }
+            }
+            rneed = std::max(rneed, off);
+            rbox_count[l] = (int)rb.size();
+            if ((rc = drbox[l].put(rb, stream))) return rc;
+        }
+        // refluxing tasks (C/amr.rs:1327-1406), grouped by target cell in CPU order
+        std::vector<std::tuple<int, int64_t, RefluxTask>> corr;
+        for (size_t id = 0; id < blocks.size(); id++) {
+            const HBlock& b = blocks[id];
+            const int l = b.level;
+            if (!b.leaf || l + 1 >= levels) continue;
+            for (int d : dims) {
+                const int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
+                const int64_t nbk = nb0[d] << l;
+                for (int side = 0; side < 2; side++) {
+                    Key nk = b.idx;
+                    nk[d] += side == 1 ? 1 : -1;
+                    if (nk[d] < 0 || nk[d] >= nbk) {
+                        if (bckind(d, side) != EMG_BC_PERIODIC) continue;
+                        nk[d] = erem(nk[d], nbk);
+                    }
+                    const int nj = get(l, nk);
+                    if (!(nj >= 0 && !blocks[nj].leaf)) continue;
+                    for (int a = 0; a < bd[e0]; a++)
+                        for (int bb = 0; bb < bd[e1]; bb++) {
+                            RefluxTask tk{};
+                            tk.slot = (int)id;
+                            tk.d = d;
+                            tk.side = side;
+                            tk.pen = a * bd[e1] + bb;
+                            tk.dx = dxl[3 * l + d];
+                            for (int fa = 0; fa < (act[e0] ? 2 : 1); fa++)
+                                for (int fb = 0; fb < (act[e1] ? 2 : 1); fb++) {
+                                    const int64_t ga = 2 * (b.idx[e0] * bd[e0] + a) + fa;
+                                    const int64_t gb = 2 * (b.idx[e1] * bd[e1] + bb) + fb;
+                                    Key ck = nk;
+                                    ck[d] = 2 * nk[d] + (side == 1 ? 0 : 1);
+                                    ck[e0] = act[e0] ? ediv(ga, bd[e0]) : 0;
+                                    ck[e1] = act[e1] ? ediv(gb, bd[e1]) : 0;
+                                    const int cid = get(l + 1, ck);
+                                    if (cid < 0 || !blocks[cid].leaf) continue;
+                                    const int la = act[e0] ? (int)erem(ga, bd[e0]) : 0;
+                                    const int lb = act[e1] ? (int)erem(gb, bd[e1]) : 0;
+                                    tk.fslot[tk.nfine] = cid;
+                                    tk.fpen[tk.nfine] = la * bd[e1] + lb;
+                                    tk.nfine++;
+                                }
+                            if (!tk.nfine) continue;
+                            int64_t c[3];
+                            c[d] = side == 1 ? bd[d] - 1 : 0;
+                            c[e0] = a;
+                            c[e1] = bb;
+                            const int64_t ce = ((c[0] + gof[0]) * ext[1] + (c[1] + gof[1])) * ext[2] + (c[2] + gof[2]);
+                            corr.push_back({(int)id, ce, tk});
+                        }
+                }
+            }
+        }
+        std::stable_sort(corr.begin(), corr.end(), [](const auto& x, const auto& y) {
+            return std::get<0>(x) != std::get<0>(y) ? std::get<0>(x) < std::get<0>(y) : std::get<1>(x) < std::get<1>(y);
+        });
+        std::vector<int> cslot, tstart;
+        std::vector<int64_t> cext;
+        std::vector<RefluxTask> tasks;
+        for (size_t i = 0; i < corr.size(); i++) {
+            if (i == 0 || std::get<0>(corr[i]) != std::get<0>(corr[i - 1]) || std::get<1>(corr[i]) != std::get<1>(corr[i - 1])) {
+                cslot.push_back(std::get<0>(corr[i]));
+                cext.push_back(std::get<1>(corr[i]));
+                tstart.push_back((int)tasks.size());
+            }
+            tasks.push_back(std::get<2>(corr[i]));
+        }
+        tstart.push_back((int)tasks.size());
+        nrefcells = (int)cslot.size();
+        if ((rc = dleaves.put(leaves, stream)) || (rc = dlevel.put(lvl, stream)) || (rc = didx.put(idx, stream)) ||
+            (rc = dbcleaves.put(bcl, stream)) || (rc = dcopy.put(copies, stream)) || (rc = dpbox.put(pboxes, stream)) ||
+            (rc = dcell_slot.put(cslot, stream)) || (rc = dcell_ext.put(cext, stream)) ||
+            (rc = dtask_start.put(tstart, stream)) || (rc = dreflux.put(tasks, stream)))
+            return rc;
+        ncopy = (int)copies.size();
+        npbox = (int)pboxes.size();
+        nbcleaves = (int)bcl.size();
+        pbox_max = pmax;
+        if ((rc = scratch(std::max(poff, rneed)))) return rc;
+        layout_valid = true;
+        return EMG_OK;
+    }
+    int64_t pbox_max = 0;
+
+    // ghost-extended boxes of every leaf (fill_scratch, C/amr.rs:1113-1221)
+    int fill_ghosts() {
+        AmrDev A = view();
+        if (ncopy) {
+            ghost_copy<<<box_grid((int64_t)ng * std::max(bd[0], 1) * std::max(bd[1], 1), ncopy), 256, 0, stream>>>(A, dcopy.p);
+            launches++;
+        }
+        int rc = run_pboxes(dpbox.p, npbox, pbox_max);
+        if (rc) return rc;
+        if (nbcleaves)
+            for (int di = 0; di < (int)dims.size(); di++) {
+                ghost_bc<<<box_grid(bcell, nbcleaves), 256, 0, stream>>>(A, dbcleaves.p, dlevel.p, didx.p, di);
+                launches++;
+            }
+        AMR_CUDA(cudaGetLastError());
+        return EMG_OK;
+    }
+
+    int sweeps(int stage) {
+        AmrDev A = view();
+        int first = -1;
+        for (int d : dims) {
+            if (first < 0) first = d;
+            int o[2], no_ = 0;
+            for (int e = 0; e < 3; e++)
+                if (e != d) o[no_++] = e;
+            int lane = o[1], other = o[0];
+            if (!act[o[1]] && act[o[0]]) {
+                lane = o[0];
+                other = o[1];
+            }
+            SweepParams p{};
+            p.uin = u;
+            p.rhs = rhs;
+            p.ctl = ctl;
+            p.ncell = A.ntot;
+            const int64_t st[3] = {(int64_t)ext[1] * ext[2], ext[2], 1};
+            p.sd = st[d];
+            p.sl = st[lane];
+            p.so = st[other];
+            p.nd = bd[d];
+            p.nl = bd[lane];
+            p.no = bd[other];
+            p.gd = gof[d];
+            p.gl = gof[lane];
+            p.go = gof[other];
+            p.d = d;
+            p.seg = bd[d];
+            p.first = d == first;
+            p.last = 0;
+            p.stage = stage;
+            p.rows_contig = p.sd == 1;
+            p.ndim = (double)dims.size();
+            p.positivity = opts.positivity ? 1 : 0;
+            p.tol = opts.tol;
+            p.eos = A.eos;
+            const int P = bd[lane] > 16 ? 32 : (bd[lane] * bd[other] >= 32 ? 32 : 16);
+            p.lw = std::min(P, bd[lane]);
+            p.amr = 1;
+            p.leaf_slot = dleaves.p;
+            p.leaf_level = dlevel.p;
+            p.bcell = bcell;
+            const int rows = P / p.lw;
+            p.ngroups = (bd[other] + rows - 1) / rows;
+            for (int l = 0; l < levels && l < 16; l++) p.dx_level[l] = dxl[3 * l + d];
+            p.dx = dxl[d];
+            p.face = face;
+            p.npen = npen;
+            p.pen_lane_major = lane < other ? 1 : 0;
+            const dim3 grid((unsigned)(nleaves * p.ngroups), 1, 1);
+            cudaError_t e = opts.precision == EMG_PRECISION_MIXED ? sweep_launch_mixed(P, opts.mode, p, grid, stream)
+                                                                   : sweep_launch_f64(P, opts.mode, p, grid, stream);
+            launches++;
+            if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("AMR sweep: ") + cudaGetErrorString(e));
+        }
+        return EMG_OK;
+    }
+
+    int compute_rhs(int stage) {
+        cudaEvent_t ev[5];
+        for (auto& e : ev) cudaEventCreate(&e);
+        cudaEventRecord(ev[0], stream);
+        int rc = restrict_all();
+        if (rc) return rc;
+        cudaEventRecord(ev[1], stream);
+        if ((rc = fill_ghosts())) return rc;
+        cudaEventRecord(ev[2], stream);
+        if ((rc = sweeps(stage))) return rc;
+        cudaEventRecord(ev[3], stream);
+        if (nrefcells) {
+            AmrDev A = view();
+            reflux_kernel<<<(nrefcells + 255) / 256, 256, 0, stream>>>(A, rhs, face, npen, dcell_slot.p, dcell_ext.p,
+                                                                      dtask_start.p, dreflux.p, nrefcells);
+            launches++;
+            AMR_CUDA(cudaGetLastError());
+        }
+        cudaEventRecord(ev[4], stream);
+        pending.push_back({ev[0], ev[1], ev[2], ev[3], ev[4]});
+        return EMG_OK;
+    }
+    std::vector<std::array<cudaEvent_t, 5>> pending;
+    void collect_times() {
+        for (auto& e : pending) {
+            float a = 0, b = 0, c = 0, d = 0;
+            cudaEventElapsedTime(&a, e[0], e[1]);
+            cudaEventElapsedTime(&b, e[1], e[2]);
+            cudaEventElapsedTime(&c, e[2], e[3]);
+            cudaEventElapsedTime(&d, e[3], e[4]);
+            phase_ms[0] += a;
+            phase_ms[1] += b;
+            phase_ms[2] += c;
+            phase_ms[3] += d;
+            for (auto x : e) cudaEventDestroy(x);
+        }
+        pending.clear();
+    }
+
+    int rk(int stage) {
+        AmrDev A = view();
+        amr_rk<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
+            A, u0, rhs, dleaves.p, dlevel.p, ddxl.p, stage, ctl);
+        launches++;
+        AMR_CUDA(cudaGetLastError());
+        return EMG_OK;
+    }
+
+    // ---------------------------------------------------------------- tree edits
+    int add_block(int level, const Key& idx) {
+        int id = (int)blocks.size();
+        int rc = reserve(id + 1);
+        if (rc) return rc;
+        blocks.push_back(HBlock{level, idx, true});
+        insert(level, idx, id);
+        return EMG_OK;
+    }
+
+    int init_block_data(int id, emg_init_fn init, void* ictx) {
+        const HBlock& b = blocks[id];
+        const int64_t n = bcells();
+        std::vector<double> xs(3 * n), ws(5 * n), us(5 * n);
+        for (int64_t i = 0; i < bd[0]; i++)
+            for (int64_t j = 0; j < bd[1]; j++)
+                for (int64_t k = 0; k < bd[2]; k++) {
+                    const int64_t q = (i * bd[1] + j) * bd[2] + k;
+                    const int64_t g[3] = {b.idx[0] * bd[0] + i, b.idx[1] * bd[1] + j, b.idx[2] * bd[2] + k};
+                    for (int d = 0; d < 3; d++)
+                        xs[3 * q + d] = act[d] ? lo[d] + ((double)g[d] + 0.5) * dxl[3 * b.level + d] : 0.5 * (lo[d] + hi[d]);
+                }
+        init(ictx, xs.data(), n, ws.data());
+        // to_cons (C/system.rs:210-217; ρe as C/eos.rs:44-54)
+        for (int64_t q = 0; q < n; q++) {
+            const double* w = &ws[5 * q];
+            const double rho = w[0];
+            const double ke = 0.5 * rho * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+            const double v = 1.0 / rho;
+            const double e = (w[4] + eos.gamma * eos.p_inf) * (v - eos.b) / (eos.gamma - 1.0) + eos.q;
+            us[5 * q] = rho;
+            us[5 * q + 1] = rho * w[1];
+            us[5 * q + 2] = rho * w[2];
+            us[5 * q + 3] = rho * w[3];
+            us[5 * q + 4] = rho * e + ke;
+        }
+        double* tmp = nullptr;
+        AMR_CUDA(cudaMalloc(&tmp, us.size() * sizeof(double)));
+        cudaMemcpyAsync(tmp, us.data(), us.size() * sizeof(double), cudaMemcpyHostToDevice, stream);
+        AmrDev A = view();
+        pool_put_interior<<<16, 256, 0, stream>>>(A, id, tmp);
+        launches++;
+        cudaStreamSynchronize(stream);
+        cudaFree(tmp);
+        AMR_CUDA(cudaGetLastError());
+        return EMG_OK;
+    }
+
+    // C/amr.rs:952-1011
+    int refine_block(int id, emg_init_fn init, void* ictx) {
+        const int l = blocks[id].level;
+        const Key idx = blocks[id].idx;
+        if (!blocks[id].leaf) return EMG_OK;
+        int rc;
+        if (l > 0) {
+            for (auto& nk : neighbours(l, idx)) {
+                if (get(l, nk) < 0) {
+                    for (int m = l - 1; m >= 0; m--) {
+                        Key pk;
+                        for (int d = 0; d < 3; d++) pk[d] = act[d] ? nk[d] >> (l - m) : 0;
+                        int pid = get(m, pk);
+                        if (pid >= 0) {
+                            if ((rc = refine_block(pid, init, ictx))) return rc;
+                            break;
+                        }
+                    }
+                }
+            }
+        }
+        id = get(l, idx);
+        if (id < 0 || !blocks[id].leaf) return EMG_OK;
+        std::vector<Key> kids = children(idx);
+        const int first = (int)blocks.size();
+        if ((rc = reserve(first + (int64_t)kids.size()))) return rc;
+        // children data first (the parent level is unchanged while they are computed)
+        std::vector<PBox> boxes;
+        for (size_t n = 0; n < kids.size(); n++) {
+            const Key& c = kids[n];
+            blocks.push_back(HBlock{l + 1, c, true});  // not yet in the index
+            if (!init) {
+                Key fmin, fmax;
+                for (int d = 0; d < 3; d++) {
+                    fmin[d] = c[d] * bd[d];
+                    fmax[d] = c[d] * bd[d] + bd[d] - 1;
+                }
+                boxes.push_back(make_pbox(l + 1, fmin, fmax, first + (int)n, gof));
+            }
+        }
+        if (init) {
+            for (size_t n = 0; n < kids.size(); n++)
+                if ((rc = init_block_data(first + (int)n, init, ictx))) return rc;
+        } else if ((rc = predict_now(boxes))) {
+            return rc;
+        }
+        blocks[id].leaf = false;
+        for (size_t n = 0; n < kids.size(); n++) insert(l + 1, kids[n], first + (int)n);
+        layout_valid = false;
+        return EMG_OK;
+    }
+
+    // C/amr.rs:1014-1032
+    int coarsen(int l, const Key& idx) {
+        std::vector<Key> kids = children(idx);
+        const int pid = get(l, idx);
+        // restriction of the whole parent from its children
+        {
+            int rc = upload_map();
+            if (rc) return rc;
+            RBox b = make_rbox(l, pid, idx, {0, 0, 0}, {bd[0], bd[1], bd[2]});
+            b.off = 0;
+            if ((rc = scratch(b.cap))) return rc;
+            DevVec<RBox> tmp;
+            if ((rc = tmp.put(std::vector<RBox>{b}, stream))) return rc;
+            rc = run_rboxes(tmp.p, 1, b.cap);
+            cudaStreamSynchronize(stream);
+            tmp.release();
+            if (rc) return rc;
+        }
+        blocks[pid].leaf = true;
+        std::vector<int> ids;
+        for (auto& c : kids) ids.push_back(get(l + 1, c));
+        std::sort(ids.begin(), ids.end(), [](int x, int y) { return x > y; });
+        for (int i : ids) {
+            remove(blocks[i].level, blocks[i].idx);
+            const int last = (int)blocks.size() - 1;
+            if (i != last) {
+                AmrDev A = view();
+                pool_move<<<64, 256, 0, stream>>>(A, last, i);
+                launches++;
+                blocks[i] = blocks[last];
+            }
+            blocks.pop_back();
+            if (i < (int)blocks.size()) insert(blocks[i].level, blocks[i].idx, i);
+        }
+        layout_valid = false;
+        AMR_CUDA(cudaGetLastError());
+        return EMG_OK;
+    }
+
+    // details of all leaves (C/amr.rs:823-867), ancestors 0
+    int details(std::vector<double>& out) {
+        int rc = ensure_layout();
+        if (rc) return rc;
+        if ((rc = fill_ghosts())) return rc;
+        if ((int64_t)blocks.size() > det_cap) {
+            cudaFree(det);
+            det_cap = std::max<int64_t>(blocks.size(), 2 * det_cap);
+            AMR_CUDA(cudaMalloc(&det, det_cap * sizeof(unsigned long long)));
+        }
+        AMR_CUDA(cudaMemsetAsync(det, 0, blocks.size() * sizeof(unsigned long long), stream));
+        AmrDev A = view();
+        amr_detail<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
+            A, dleaves.p, det);
+        launches++;
+        AMR_CUDA(cudaGetLastError());
+        std::vector<unsigned long long> bits(blocks.size());
+        AMR_CUDA(cudaMemcpyAsync(bits.data(), det, bits.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+        AMR_CUDA(cudaStreamSynchronize(stream));
+        out.resize(blocks.size());
+        for (size_t i = 0; i < bits.size(); i++) std::memcpy(&out[i], &bits[i], sizeof(double));
+        return EMG_OK;
+    }
+    // C/amr.rs:877-892
+    std::vector<int8_t> flags_from(const std::vector<double>& det) const {
+        std::vector<int8_t> f(blocks.size(), 0);
+        for (size_t i = 0; i < blocks.size(); i++) {
+            if (!blocks[i].leaf)
+                f[i] = 0;
+            else if (det[i] > cfg.eps && blocks[i].level + 1 < levels)
+                f[i] = 1;
+            else if (det[i] < cfg.eps / 128.0)
+                f[i] = -1;
+        }
+        return f;
+    }
+    int flags(std::vector<int8_t>& f) {
+        int rc = restrict_all();
+        if (rc) return rc;
+        std::vector<double> det;
+        if ((rc = details(det))) return rc;
+        f = flags_from(det);
+        return EMG_OK;
+    }
+
+    // C/amr.rs:1039-1106
+    int regrid() {
+        std::vector<int8_t> f;
+        int rc = flags(f);  // restrict_all + details
+        if (rc) return rc;
+        std::vector<std::pair<int, Key>> want;
+        for (size_t i = 0; i < f.size(); i++) {
+            if (f[i] > 0) {
+                const HBlock& b = blocks[i];
+                want.push_back({b.level, b.idx});
+                for (auto& nk : neighbours(b.level, b.idx)) {
+                    int j = get(b.level, nk);
+                    if (j >= 0 && blocks[j].leaf) want.push_back({b.level, nk});
+                }
+            }
+        }
+        std::sort(want.begin(), want.end());
+        want.erase(std::unique(want.begin(), want.end()), want.end());
+        std::set<std::pair<int, Key>> prot(want.begin(), want.end());
+        for (auto& k : want) {
+            int id = get(k.first, k.second);
+            if (id >= 0 && k.first + 1 < levels)
+                if ((rc = refine_block(id, nullptr, nullptr))) return rc;
+        }
+        if ((rc = flags(f))) return rc;
+        const size_t nkids = (size_t)1 << dims.size();
+        std::vector<std::pair<int, Key>> cand;
+        for (size_t bi = 0; bi < blocks.size(); bi++) {
+            const HBlock& b = blocks[bi];
+            if (b.leaf) continue;
+            std::vector<Key> kids = children(b.idx);
+            bool ok = kids.size() == nkids;
+            for (auto& c : kids) {
+                if (!ok) break;
+                int j = get(b.level + 1, c);
+                ok = j >= 0 && blocks[j].leaf && f[j] < 0 && !prot.count({b.level + 1, c});
+            }
+            if (ok) cand.push_back({b.level, b.idx});
+        }
+        std::stable_sort(cand.begin(), cand.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+        for (auto& c : cand) {
+            const int l = c.first;
+            bool ok = true;
+            for (auto& nk : neighbours(l, c.second))
+                for (auto& ch : children(nk)) {
+                    int j = get(l + 1, ch);
+                    if (j >= 0 && !blocks[j].leaf) ok = false;
+                }
+            if (ok && get(l, c.second) >= 0)
+                if ((rc = coarsen(l, c.second))) return rc;
+        }
+        rate_valid = false;
+        return EMG_OK;
+    }
+
+    std::vector<std::tuple<int, Key, bool>> structure() const {
+        std::vector<std::tuple<int, Key, bool>> s;
+        for (auto& b : blocks) s.push_back({b.level, b.idx, b.leaf});
+        return s;
+    }
+
+    // C/amr.rs:1470-1537
+    int step(double dt) {
+        int rc = ensure_layout();
+        if (rc) return rc;
+        ctl_host->dt = dt;
+        ctl_host->done = 0;
+        ctl_host->rate_bits = 0;
+        AMR_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice, stream));
+        for (int s = 1; s <= 3; s++) {
+            if ((rc = compute_rhs(s))) return rc;
+            cudaEvent_t a, b;
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, stream);
+            if ((rc = rk(s))) return rc;
+            cudaEventRecord(b, stream);
+            rk_events.push_back({a, b});
+        }
+        uint64_t f = 0;
+        for (int d : dims) f += (uint64_t)nleaves * (bcells() / bd[d]) * (bd[d] + 1);
+        faces += 3 * f;
+        if (opts.mode == EMG_MODE_WENO) weno_faces += 3 * f;
+        AMR_CUDA(cudaMemcpyAsync(ctl_host, ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, stream));
+        AMR_CUDA(cudaStreamSynchronize(stream));
+        collect_times();
+        for (auto& e : rk_events) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e.first, e.second);
+            phase_ms[3] += ms;
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        rk_events.clear();
+        rate_valid = true;
+        t += dt;
+        steps += 1;
+        if (steps >= next_regrid) {
+            cudaEvent_t a, b;
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, stream);
+            auto before = structure();
+            if ((rc = regrid())) return rc;
+            const bool changed = structure() != before;
+            regrid_interval = changed ? cfg.regrid_every : std::min(2 * regrid_interval, 2 * cfg.regrid_every);
+            next_regrid = steps + regrid_interval;
+            cudaEventRecord(b, stream);
+            cudaEventSynchronize(b);
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            phase_ms[4] += ms;
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+        unsigned int e = 0;
+        AMR_CUDA(cudaMemcpy(&e, err, sizeof e, cudaMemcpyDeviceToHost));
+        if (e) return set_error(EMG_ERR_UNFILLABLE, "AMR ghost cell without a source (prediction depth or box)");
+        return EMG_OK;
+    }
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> rk_events;
+
+    int dt_cfl(double* dt) {
+        if (!rate_valid) {
+            int rc = ensure_layout();
+            if (rc) return rc;
+            ctl_host->rate_bits = 0;
+            AMR_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice, stream));
+            AmrDev A = view();
+            amr_cfl<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
+                A, dleaves.p, dlevel.p, ddxl.p, ctl);
+            launches++;
+            AMR_CUDA(cudaGetLastError());
+        }
+        AMR_CUDA(cudaMemcpyAsync(ctl_host, ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, stream));
+        AMR_CUDA(cudaStreamSynchronize(stream));
+        rate_valid = true;
+        double rate;
+        std::memcpy(&rate, &ctl_host->rate_bits, sizeof rate);
+        *dt = opts.cfl / rate;
+        return EMG_OK;
+    }
+
+    int setup(const emg_amr_config* c, const emg_eos* e, const double* lo_, const double* hi_, const emg_bc* b,
+              const emg_opts* o) {
+        cfg = *c;
+        eos = *e;
+        opts = *o;
+        for (int d = 0; d < 3; d++) {
+            lo[d] = lo_[d];
+            hi[d] = hi_[d];
+        }
+        for (int i = 0; i < 6; i++) bc[i] = b[i];
+        if (cfg.b < 6 || cfg.levels < 1 || cfg.levels > AMR_MAX_LEVELS || cfg.regrid_every < 1)
+            return set_error(EMG_ERR_INVALID, "invalid AMR configuration (b >= 6, 1 <= levels <= 12, regrid_every >= 1)");
+        for (int i = 0; i < 6; i++)
+            if (bc[i].kind == EMG_BC_CHARACTERISTIC)
+                return set_error(EMG_ERR_INVALID, "characteristic boundaries are not available on the AMR path");
+        if (opts.mode != EMG_MODE_WENO && opts.mode != EMG_MODE_HYBRID && opts.mode != EMG_MODE_CENTRAL)
+            return set_error(EMG_ERR_INVALID, "unknown flux mode");
+        ng = (int)std::max<int64_t>(cfg.ghosts, 5);
+        for (int d = 0; d < 3; d++) {
+            bd[d] = cfg.base_blocks[d] == 0 ? 1 : (int)cfg.b;
+            // C/amr.rs:251-253
+            act[d] = cfg.base_blocks[d] > 0 && (hi[d] - lo[d]) > 0.0 && bd[d] > 1;
+            nb0[d] = std::max<int64_t>(cfg.base_blocks[d], 1);
+            ext[d] = act[d] ? bd[d] + 2 * ng : 1;
+            gof[d] = act[d] ? ng : 0;
+            if (act[d]) dims.push_back(d);
+        }
+        if (dims.empty()) return set_error(EMG_ERR_INVALID, "no active axis");
+        if (cfg.b > 32) return set_error(EMG_ERR_INVALID, "block side above 32");
+        levels = (int)cfg.levels;
+        dxl.assign(3 * levels, 0.0);
+        for (int l = 0; l < levels; l++)
+            for (int d = 0; d < 3; d++) dxl[3 * l + d] = (hi[d] - lo[d]) / (double)n_level(l, d);
+        auto a = lagrange6(-3.0, -0.25), bb = lagrange6(-2.0, 0.25);
+        for (int k = 0; k < 6; k++) {
+            wp[0][k] = a[k];
+            wp[1][k] = bb[k];
+        }
+        const double wr_[6] = {3.0 / 256.0, -25.0 / 256.0, 150.0 / 256.0, 150.0 / 256.0, -25.0 / 256.0, 3.0 / 256.0};
+        std::memcpy(wr, wr_, sizeof wr);
+        const int shifts[5] = {0, -1, 1, -2, 2};
+        for (int m = 0; m < 5; m++) {
+            auto w = m == 0 ? std::array<double, 6>{wr[0], wr[1], wr[2], wr[3], wr[4], wr[5]}
+                            : lagrange6(-2.5 + (double)shifts[m], 0.0);
+            for (int k = 0; k < 6; k++) wrs[m][k] = w[k];
+        }
+        bcell = (int64_t)ext[0] * ext[1] * ext[2];
+        npen = 1;
+        for (int d = 0; d < 3; d++) {
+            int p = 1;
+            for (int e2 = 0; e2 < 3; e2++)
+                if (e2 != d) p *= bd[e2];
+            npen = std::max(npen, p);
+        }
+        map.resize(levels);
+        mapoff.assign(levels, 0);
+        int64_t off = 0;
+        for (int l = 0; l < levels; l++) {
+            map[l].assign(nbl(l, 0) * nbl(l, 1) * nbl(l, 2), -1);
+            mapoff[l] = off;
+            off += (int64_t)map[l].size();
+        }
+        regrid_interval = cfg.regrid_every;
+        next_regrid = cfg.regrid_every;
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+            cudaGetLastError();
+            return set_error(EMG_ERR_NO_DEVICE, "no CUDA device visible");
+        }
+        AMR_CUDA(cudaGetDevice(&device));
+        cudaDeviceProp pr;
+        AMR_CUDA(cudaGetDeviceProperties(&pr, device));
+        if (pr.major != 10) return set_error(EMG_ERR_NO_DEVICE, "device is not sm_100 (B200)");
+        AMR_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        AMR_CUDA(cudaMalloc(&err, sizeof(unsigned int)));
+        AMR_CUDA(cudaMemset(err, 0, sizeof(unsigned int)));
+        AMR_CUDA(cudaMalloc(&ctl, sizeof(StepCtl)));
+        AMR_CUDA(cudaMallocHost(&ctl_host, sizeof(StepCtl)));
+        std::memset(ctl_host, 0, sizeof(StepCtl));
+        ctl_host->t_end = INFINITY;
+        AMR_CUDA(cudaMemcpy(ctl, ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice));
+        // deep predictions recurse through sample/predict
+        size_t stack = 0;
+        cudaDeviceGetLimit(&stack, cudaLimitStackSize);
+        if (stack < 8192) cudaDeviceSetLimit(cudaLimitStackSize, 8192);
+        int rc = ddxl.put(dxl, stream);
+        if (rc) return rc;
+        static bool prepared = false;
+        if (!prepared) {
+            cudaError_t e2 = sweep_prepare_f64();
+            if (e2 == cudaSuccess) e2 = sweep_prepare_mixed();
+            if (e2 != cudaSuccess) return set_error(EMG_ERR_CUDA, "sweep setup failed");
+            prepared = true;
+        }
+        return EMG_OK;
+    }
+
+    void release() {
+        if (stream) cudaStreamSynchronize(stream);
+        collect_times();
+        cudaFree(u);
+        cudaFree(u0);
+        cudaFree(rhs);
+        cudaFree(face);
+        cudaFree(err);
+        cudaFree(ctl);
+        if (ctl_host) cudaFreeHost(ctl_host);
+        for (int i = 0; i < 2; i++) {
+            cudaFree(scr[i]);
+            cudaFree(sok[i]);
+        }
+        cudaFree(det);
+        dmap.release();
+        dleaves.release();
+        dlevel.release();
+        dbcleaves.release();
+        dcell_slot.release();
+        dtask_start.release();
+        didx.release();
+        dcell_ext.release();
+        ddxl.release();
+        dcopy.release();
+        dpbox.release();
+        for (auto& r : drbox) r.release();
+        dreflux.release();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+extern "C" {
+
+int emg_amr_create(const emg_amr_config* cfg, const emg_eos* eos, const double lo[3], const double hi[3],
+                   const emg_bc bc[6], const emg_opts* opts, emg_init_fn init, void* ctx, emg_amr** out) {
+    if (!cfg || !eos || !lo || !hi || !bc || !opts || !init || !out) return set_error(EMG_ERR_INVALID, "null argument");
+    *out = nullptr;
+    emg_amr* h = new emg_amr();
+    int rc = h->setup(cfg, eos, lo, hi, bc, opts);
+    auto bail = [&](int code) {
+        h->release();
+        delete h;
+        return code;
+    };
+    if (rc) return bail(rc);
+    // Amr::new (C/amr.rs:289-344)
+    for (int64_t i = 0; i < h->nb0[0]; i++)
+        for (int64_t j = 0; j < h->nb0[1]; j++)
+            for (int64_t k = 0; k < h->nb0[2]; k++) {
+                const int id = (int)h->blocks.size();
+                if ((rc = h->add_block(0, Key{i, j, k}))) return bail(rc);
+                if ((rc = h->init_block_data(id, init, ctx))) return bail(rc);
+            }
+    for (int it = 0; it < h->levels; it++) {
+        std::vector<int8_t> f;
+        if ((rc = h->flags(f))) return bail(rc);
+        std::vector<std::pair<int, Key>> keys;
+        for (size_t i = 0; i < h->blocks.size(); i++)
+            if (f[i] > 0 && h->blocks[i].leaf) keys.push_back({h->blocks[i].level, h->blocks[i].idx});
+        if (keys.empty()) break;
+        for (auto& k : keys) {
+            int id = h->get(k.first, k.second);
+            if (id >= 0 && (rc = h->refine_block(id, init, ctx))) return bail(rc);
+        }
+    }
+    *out = h;
+    return EMG_OK;
+}
+
+int emg_amr_create_from_blocks(const emg_amr_config* cfg, const emg_eos* eos, const double lo[3], const double hi[3],
+                               const emg_bc bc[6], const emg_opts* opts, const int64_t* desc, size_t nblocks,
+                               const double* u, emg_amr** out) {
+    if (!cfg || !eos || !lo || !hi || !bc || !opts || !desc || !u || !out) return set_error(EMG_ERR_INVALID, "null argument");
+    *out = nullptr;
+    emg_amr* h = new emg_amr();
+    int rc = h->setup(cfg, eos, lo, hi, bc, opts);
+    auto bail = [&](int code) {
+        h->release();
+        delete h;
+        return code;
+    };
+    if (rc) return bail(rc);
+    if ((rc = h->reserve((int64_t)nblocks))) return bail(rc);
+    for (size_t i = 0; i < nblocks; i++) {
+        const int l = (int)desc[5 * i];
+        const Key k = {desc[5 * i + 1], desc[5 * i + 2], desc[5 * i + 3]};
+        if (l < 0 || l >= h->levels || h->slot_of(l, k) < 0) return bail(set_error(EMG_ERR_INVALID, "block outside the hierarchy"));
+        h->blocks.push_back(HBlock{l, k, desc[5 * i + 4] != 0});
+        h->insert(l, k, (int)i);
+    }
+    const int64_t nb = h->bcells();
+    double* tmp = nullptr;
+    if (cudaMalloc(&tmp, (size_t)nb * 5 * sizeof(double)) != cudaSuccess) return bail(set_error(EMG_ERR_CUDA, "alloc"));
+    AmrDev A = h->view();
+    for (size_t i = 0; i < nblocks; i++) {
+        cudaMemcpyAsync(tmp, u + i * nb * 5, (size_t)nb * 5 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+        pool_put_interior<<<16, 256, 0, h->stream>>>(A, (int)i, tmp);
+    }
+    cudaStreamSynchronize(h->stream);
+    cudaFree(tmp);
+    *out = h;
+    return EMG_OK;
+}
+
+int emg_amr_destroy(emg_amr* h) {
+    if (!h) return EMG_OK;
+    cudaSetDevice(h->device);
+    h->release();
+    delete h;
+    return EMG_OK;
+}
+
+static int amr_check(emg_amr* h) {
+    if (!h) return set_error(EMG_ERR_INVALID, "null handle");
+    if (cudaSetDevice(h->device) != cudaSuccess) return set_error(EMG_ERR_CUDA, "cudaSetDevice failed");
+    return EMG_OK;
+}
+
+int emg_amr_step(emg_amr* h, double dt) {
+    int rc = amr_check(h);
+    return rc ? rc : h->step(dt);
+}
+
+int emg_amr_dt_cfl(emg_amr* h, double* dt) {
+    int rc = amr_check(h);
+    if (rc) return rc;
+    if (!dt) return set_error(EMG_ERR_INVALID, "null dt");
+    return h->dt_cfl(dt);
+}
+
+int emg_amr_run_to(emg_amr* h, double t_end, uint64_t* steps) {
+    int rc = amr_check(h);
+    if (rc) return rc;
+    uint64_t n = 0;
+    while (h->t < t_end * (1.0 - 1e-14)) {
+        double dt = 0.0;
+        if ((rc = h->dt_cfl(&dt))) return rc;
+        dt = std::fmin(dt, t_end - h->t);
+        if (!(std::isfinite(dt) && dt > 0.0)) return set_error(EMG_ERR_DT_COLLAPSED, "time step collapsed");
+        if ((rc = h->step(dt))) return rc;
+        n++;
+    }
+    if (steps) *steps = n;
+    return EMG_OK;
+}
+
+int emg_amr_regrid(emg_amr* h) {
+    int rc = amr_check(h);
+    return rc ? rc : h->regrid();
+}
+
+int emg_amr_block_count(emg_amr* h, uint64_t* blocks, uint64_t* leaves) {
+    if (!h) return set_error(EMG_ERR_INVALID, "null handle");
+    uint64_t n = 0;
+    for (auto& b : h->blocks) n += b.leaf ? 1 : 0;
+    if (blocks) *blocks = h->blocks.size();
+    if (leaves) *leaves = n;
+    return EMG_OK;
+}
+
+int emg_amr_structure(emg_amr* h, int64_t* desc, size_t cap) {
+    if (!h || !desc) return set_error(EMG_ERR_INVALID, "null argument");
+    if (cap < h->blocks.size()) return set_error(EMG_ERR_INVALID, "structure buffer too small");
+    for (size_t i = 0; i < h->blocks.size(); i++) {
+        desc[5 * i] = h->blocks[i].level;
+        for (int d = 0; d < 3; d++) desc[5 * i + 1 + d] = h->blocks[i].idx[d];
+        desc[5 * i + 4] = h->blocks[i].leaf ? 1 : 0;
+    }
+    return EMG_OK;
+}
+
+int emg_amr_download(emg_amr* h, double* u, size_t nblocks) {
+    int rc = amr_check(h);
+    if (rc) return rc;
+    if (!u || nblocks < h->blocks.size()) return set_error(EMG_ERR_INVALID, "buffer too small");
+    const size_t n = h->blocks.size() * (size_t)h->bcells() * 5;
+    double* tmp = nullptr;
+    AMR_CUDA(cudaMalloc(&tmp, n * sizeof(double)));
+    AmrDev A = h->view();
+    pool_get_interior<<<256, 256, 0, h->stream>>>(A, (int)h->blocks.size(), tmp);
+    cudaMemcpyAsync(u, tmp, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    cudaStreamSynchronize(h->stream);
+    cudaFree(tmp);
+    AMR_CUDA(cudaGetLastError());
+    return EMG_OK;
+}
+
+int emg_amr_totals(emg_amr* h, double out[5]) {
+    if (!h || !out) return set_error(EMG_ERR_INVALID, "null argument");
+    // host sum in the reference order (C/amr.rs:1991-2005) over downloaded leaves
+    std::vector<double> u(h->blocks.size() * (size_t)h->bcells() * 5);
+    int rc = emg_amr_download(h, u.data(), h->blocks.size());
+    if (rc) return rc;
+    double s[5] = {0, 0, 0, 0, 0};
+    for (size_t i = 0; i < h->blocks.size(); i++) {
+        if (!h->blocks[i].leaf) continue;
+        double vol = 1.0;
+        for (int d : h->dims) vol = vol * h->dxl[3 * h->blocks[i].level + d];
+        const double* b = &u[i * h->bcells() * 5];
+        for (int64_t c = 0; c < h->bcells(); c++)
+            for (int q = 0; q < 5; q++) s[q] = s[q] + b[5 * c + q] * vol;
+    }
+    for (int q = 0; q < 5; q++) out[q] = s[q];
+    return EMG_OK;
+}
+
+int emg_amr_counters(emg_amr* h, uint64_t out[4]) {
+    int rc = amr_check(h);
+    if (rc) return rc;
+    AMR_CUDA(cudaMemcpyAsync(h->ctl_host, h->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, h->stream));
+    AMR_CUDA(cudaStreamSynchronize(h->stream));
+    out[0] = h->faces;
+    out[1] = h->weno_faces + h->ctl_host->counters[1];
+    out[2] = h->ctl_host->counters[2];
+    out[3] = h->ctl_host->counters[3];
+    return EMG_OK;
+}
+
+int emg_amr_get_time(emg_amr* h, double* t) {
+    if (!h || !t) return set_error(EMG_ERR_INVALID, "null argument");
+    *t = h->t;
+    return EMG_OK;
+}
+
+int emg_amr_steps(emg_amr* h, uint64_t* steps) {
+    if (!h || !steps) return set_error(EMG_ERR_INVALID, "null argument");
+    *steps = (uint64_t)h->steps;
+    return EMG_OK;
+}
+
+int emg_amr_synchronize(emg_amr* h) {
+    int rc = amr_check(h);
+    if (rc) return rc;
+    AMR_CUDA(cudaStreamSynchronize(h->stream));
+    return EMG_OK;
+}
+
+int emg_amr_stream(emg_amr* h, void** stream) {
+    if (!h || !stream) return set_error(EMG_ERR_INVALID, "null argument");
+    *stream = (void*)h->stream;
+    return EMG_OK;
+}
+
+int emg_amr_phase_times(emg_amr* h, double out[5]) {
+    int rc = amr_check(h);
+    if (rc) return rc;
+    cudaStreamSynchronize(h->stream);
+    h->collect_times();
+    for (int i = 0; i < 5; i++) {
+        out[i] = h->phase_ms[i];
+        h->phase_ms[i] = 0.0;
+    }
+    return EMG_OK;
+}
+
+int emg_amr_launch_count(emg_amr* h, uint64_t* launches) {
+    if (!h || !launches) return set_error(EMG_ERR_INVALID, "null argument");
+    *launches = h->launches;
+    return EMG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,197 @@
+// Device side of the block-AMR solver: the hierarchy view used by the
+// kernels, sampling with 6th-order prediction, and the box pipelines that
+// predict fine boxes from the coarser level and restrict ancestors from the
+// finer one.
+//
+// Every operator reproduces the arithmetic and order of the reference CPU
+// solver (fluid/crates/compressible/src/amr.rs): `sample` (:384-439),
+// `predict` (:589-613), `gather_box` + `bc_box` (:450-545), `predict_box`
+// (:548-586) and `restrict_box` (:622-731), so that the device hierarchy
+// evolves bit for bit like the CPU one.
+#pragma once
+#include "physics.cuh"
+#include <stdint.h>
+
+namespace emg {
+
+constexpr int AMR_MAX_LEVELS = 12;
+
+// Hierarchy view (pointers into device memory owned by the host object).
+struct AmrDev {
+    double* u;             // pool: u[q*ntot + slot*bcell + ext cell]
+    int64_t ntot;          // field stride
+    int64_t bcell;         // cells per pool block (ghost-extended)
+    int ext[3], bd[3], gof[3];
+    int act[3];
+    int ndims, dims[3];
+    int ng;
+    int levels;
+    int64_t nb0[3];        // level-0 blocks per side
+    const int* map;        // dense per-level block index (−1: absent)
+    int64_t mapoff[AMR_MAX_LEVELS];
+    int bc[3][2];
+    double bcs[3][2][5];   // Dirichlet states
+    double wp[2][6];       // prediction weights by parity (amr.rs:307)
+    double wr[6];          // centred restriction weights (amr.rs:308)
+    double wrs[5][6];      // restriction weights by shift m (amr.rs:670-671)
+    EosD eos;
+    unsigned int* err;     // error word (depth overflow)
+};
+
+__device__ __forceinline__ int64_t amr_ediv(int64_t a, int64_t b) {
+    int64_t q = a / b;
+    return (a % b < 0) ? q - 1 : q;
+}
+__device__ __forceinline__ int64_t amr_erem(int64_t a, int64_t b) {
+    int64_t r = a % b;
+    return r < 0 ? r + b : r;
+}
+
+__device__ __forceinline__ int64_t amr_nbl(const AmrDev& A, int l, int d) { return A.act[d] ? (A.nb0[d] << l) : 1; }
+__device__ __forceinline__ int64_t amr_nlevel(const AmrDev& A, int l, int d) {
+    return A.act[d] ? A.nb0[d] * A.bd[d] * ((int64_t)1 << l) : 1;
+}
+
+// pool slot of block (l, key), or −1
+__device__ __forceinline__ int amr_get(const AmrDev& A, int l, const int64_t* k) {
+    if (l < 0 || l >= A.levels) return -1;
+    int64_t s = 0;
+    for (int d = 0; d < 3; d++) {
+        const int64_t n = amr_nbl(A, l, d);
+        if (k[d] < 0 || k[d] >= n) return -1;
+        s = s * n + k[d];
+    }
+    return A.map[A.mapoff[l] + s];
+}
+
+__device__ __forceinline__ int64_t amr_cell(const AmrDev& A, const int64_t* c) {
+    return ((c[0] + A.gof[0]) * A.ext[1] + (c[1] + A.gof[1])) * A.ext[2] + (c[2] + A.gof[2]);
+}
+
+__device__ __forceinline__ void amr_load(const AmrDev& A, int slot, int64_t cell, double* v) {
+    const double* p = A.u + (int64_t)slot * A.bcell + cell;
+#pragma unroll
+    for (int q = 0; q < 5; q++) v[q] = p[(int64_t)q * A.ntot];
+}
+
+__device__ void amr_predict(const AmrDev& A, int l, const int64_t* g, double* out, int depth);
+
+// Conserved value of global cell g at level l (amr.rs:384-439). Boundary
+// kinds: periodic, outflow, reflect, Dirichlet (the characteristic kind is
+// rejected when the solver is built).
+__device__ void amr_sample(const AmrDev& A, int l, const int64_t* g_in, double* v, int depth) {
+    int64_t g[3] = {g_in[0], g_in[1], g_in[2]};
+    bool flip[3] = {false, false, false};
+    for (int d = 2; d >= 0; d--) {
+        if (!A.act[d]) {
+            g[d] = 0;
+            continue;
+        }
+        const int64_t n = amr_nlevel(A, l, d);
+        if (g[d] < 0 || g[d] >= n) {
+            const int side = g[d] >= n ? 1 : 0;
+            const int kind = A.bc[d][side];
+            if (kind == EMG_BC_PERIODIC) {
+                g[d] = amr_erem(g[d], n);
+            } else if (kind == EMG_BC_OUTFLOW) {
+                g[d] = g[d] < 0 ? 0 : n - 1;
+            } else if (kind == EMG_BC_REFLECT) {
+                g[d] = side == 0 ? -1 - g[d] : 2 * n - 1 - g[d];
+                flip[d] = true;
+            } else {
+#pragma unroll
+                for (int q = 0; q < 5; q++) v[q] = A.bcs[d][side][q];
+                return;
+            }
+        }
+    }
+    int64_t key[3], c[3];
+    for (int d = 0; d < 3; d++) {
+        key[d] = A.act[d] ? amr_ediv(g[d], A.bd[d]) : 0;
+        c[d] = A.act[d] ? amr_erem(g[d], A.bd[d]) : 0;
+    }
+    const int id = amr_get(A, l, key);
+    if (id >= 0) {
+        amr_load(A, id, amr_cell(A, c), v);
+    } else {
+        amr_predict(A, l, g, v, depth + 1);
+    }
+    for (int d = 0; d < 3; d++)
+        if (flip[d]) v[1 + d] = -v[1 + d];
+}
+
+// Direct 6^D prediction of cell g (level l) from level l − 1 (amr.rs:589-613).
+__device__ void amr_predict(const AmrDev& A, int l, const int64_t* g, double* out, int depth) {
+#pragma unroll
+    for (int q = 0; q < 5; q++) out[q] = 0.0;
+    if (depth > 2 * AMR_MAX_LEVELS || l <= 0) {
+        atomicOr(A.err, 1u);
+        return;
+    }
+    int total = 1;
+    for (int i = 0; i < A.ndims; i++) total *= 6;
+    for (int s = 0; s < total; s++) {
+        double w = 1.0;
+        int64_t c[3] = {0, 0, 0};
+        int rem = s;
+        for (int i = 0; i < A.ndims; i++) {
+            const int d = A.dims[i];
+            const int k = rem % 6;
+            rem /= 6;
+            const int odd = (int)amr_erem(g[d], 2);
+            const int64_t base = amr_ediv(g[d], 2) + (odd == 1 ? -2 : -3);
+            c[d] = base + k;
+            w = w * A.wp[odd][k];
+        }
+        double v[5];
+        amr_sample(A, l - 1, c, v, depth);
+#pragma unroll
+        for (int q = 0; q < 5; q++) out[q] = out[q] + w * v[q];
+    }
+}
+
+// ------------------------------------------------------------------ box pipelines
+// A box is a row-major array of cells with its own size per axis; buffers
+// ping-pong between passes. `val` holds 5 doubles per cell (AoS within the
+// box), `ok` one byte.
+
+// Prediction of the level-l fine box [fmin, fmax] from level l − 1
+// (predict_box, amr.rs:548-586), written to a target pool block.
+struct PBox {
+    int l;               // fine level
+    int slot;            // target pool slot
+    int64_t fmin[3];     // fine box, global cell coordinates at level l
+    int64_t cmin[3];     // gathered coarse patch origin (level l − 1)
+    int csz[3];          // coarse patch size
+    int fsz[3];          // fine box size
+    int t0[3];           // ext-local coordinates of fmin in the target block
+    int64_t off;         // scratch offset (cells) of this box's buffers
+    int64_t cap;         // cells per buffer
+};
+
+// Restriction of ancestor (l, idx) cells [lo, hi) from level l + 1
+// (restrict_box, amr.rs:622-731), written into the ancestor's interior.
+struct RBox {
+    int l;               // coarse level
+    int slot;            // ancestor pool slot
+    int lo[3], hi[3];    // local cell box
+    int64_t f0[3];       // fine patch origin (level l + 1)
+    int sz[3];           // fine patch size
+    int64_t off;         // scratch offset (cells)
+    int64_t cap;         // cells per buffer
+};
+
+// thread → (box, cell) over a prefix-sum of box sizes
+__device__ __forceinline__ int find_box(const int64_t* start, int nbox, int64_t t) {
+    int lo = 0, hi = nbox;  // start[lo] <= t < start[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (start[mid] <= t)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+}  // namespace emg

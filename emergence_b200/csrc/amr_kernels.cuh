@@ -1,0 +1,579 @@
+// Block-AMR kernels: box pipelines (prediction from the coarser level,
+// restriction from the finer level), leaf ghost slabs, refluxing, the
+// SSP-RK3 update with the fused CFL rate, and wavelet details. Each kernel
+// follows the reference CPU operator it names (fluid/crates/compressible/
+// src/amr.rs) in arithmetic order.
+#pragma once
+#include "amr_dev.cuh"
+#include "sweep.cuh"
+
+namespace emg {
+
+// row-major cell index within a box of size s
+__device__ __forceinline__ void box_coord(int64_t q, const int* s, int64_t* c) {
+    c[2] = q % s[2];
+    c[1] = (q / s[2]) % s[1];
+    c[0] = q / ((int64_t)s[1] * s[2]);
+}
+__device__ __forceinline__ int64_t box_index(const int64_t* c, const int* s) { return (c[0] * s[1] + c[1]) * s[2] + c[2]; }
+
+// size of a prediction box after `npass` separable passes (active axes in order)
+__device__ __forceinline__ void pbox_size(const AmrDev& A, const PBox& b, int npass, int* s) {
+    for (int d = 0; d < 3; d++) s[d] = b.csz[d];
+    for (int i = 0; i < npass; i++) s[A.dims[i]] = b.fsz[A.dims[i]];
+}
+__device__ __forceinline__ void rbox_size(const AmrDev& A, const RBox& b, int npass, int* s) {
+    for (int d = 0; d < 3; d++) s[d] = b.sz[d];
+    for (int i = 0; i < npass; i++) s[A.dims[i]] = b.hi[A.dims[i]] - b.lo[A.dims[i]];
+}
+
+// gather_box(l−1) inner cells by sampling; cells beyond a non-periodic
+// boundary are left invalid for bc_box (amr.rs:508-530)
+__global__ void pbox_gather(const AmrDev A, const PBox* __restrict__ boxes, double* buf, unsigned char* ok) {
+    const PBox b = boxes[blockIdx.x];
+    const int l = b.l - 1;
+    const int64_t n = (int64_t)b.csz[0] * b.csz[1] * b.csz[2];
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        box_coord(q, b.csz, c);
+        int64_t g[3] = {b.cmin[0] + c[0], b.cmin[1] + c[1], b.cmin[2] + c[2]};
+        bool out = false;
+        for (int i = 0; i < A.ndims; i++) {
+            const int d = A.dims[i];
+            const int64_t nn = amr_nlevel(A, l, d);
+            if ((g[d] < 0 || g[d] >= nn) && A.bc[d][g[d] >= nn ? 1 : 0] != EMG_BC_PERIODIC) out = true;
+        }
+        double* v = buf + (b.off + q) * 5;
+        if (out) {
+            ok[b.off + q] = 0;
+        } else {
+            amr_sample(A, l, g, v, 0);
+            ok[b.off + q] = 1;
+        }
+    }
+}
+
+// bc_box sweep along active axis dims[di] over a box at level l with global
+// origin g0 (amr.rs:450-504): cells outside along that axis and inside along
+// every later one copy their (flipped) source from the same box, or take the
+// Dirichlet state.
+__device__ __forceinline__ void bc_cell(const AmrDev& A, int l, const int64_t* g0, const int* s, int64_t q, int di,
+                                        double* buf, unsigned char* ok, int64_t off) {
+    int64_t c[3];
+    box_coord(q, s, c);
+    const int64_t g[3] = {g0[0] + c[0], g0[1] + c[1], g0[2] + c[2]};
+    const int d = A.dims[di];
+    int64_t n[3];
+    for (int e = 0; e < 3; e++) n[e] = amr_nlevel(A, l, e);
+    auto outside = [&](int e) {
+        return (g[e] < 0 || g[e] >= n[e]) && A.bc[e][g[e] >= n[e] ? 1 : 0] != EMG_BC_PERIODIC;
+    };
+    if (!outside(d)) return;
+    for (int j = di + 1; j < A.ndims; j++)
+        if (outside(A.dims[j])) return;
+    const int side = g[d] >= n[d] ? 1 : 0;
+    const int kind = A.bc[d][side];
+    double* dst = buf + (off + q) * 5;
+    if (kind == EMG_BC_DIRICHLET) {
+        for (int k = 0; k < 5; k++) dst[k] = A.bcs[d][side][k];
+        ok[off + q] = 1;
+        return;
+    }
+    int64_t src_g;
+    if (kind == EMG_BC_OUTFLOW)
+        src_g = g[d] < 0 ? 0 : n[d] - 1;
+    else  // reflect
+        src_g = side == 0 ? -1 - g[d] : 2 * n[d] - 1 - g[d];
+    int64_t sc[3] = {c[0], c[1], c[2]};
+    sc[d] = src_g - g0[d];
+    if (sc[d] < 0 || sc[d] >= s[d]) return;
+    const int64_t sq = box_index(sc, s);
+    if (!ok[off + sq]) return;
+    const double* src = buf + (off + sq) * 5;
+    for (int k = 0; k < 5; k++) dst[k] = src[k];
+    if (kind == EMG_BC_REFLECT) dst[1 + d] = -dst[1 + d];
+    ok[off + q] = 1;
+}
+
+__global__ void pbox_bc(const AmrDev A, const PBox* __restrict__ boxes, double* buf, unsigned char* ok, int di) {
+    const PBox b = boxes[blockIdx.x];
+    const int64_t n = (int64_t)b.csz[0] * b.csz[1] * b.csz[2];
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
+        bc_cell(A, b.l - 1, b.cmin, b.csz, q, di, buf, ok, b.off);
+}
+
+// cells still invalid after bc_box are sampled (amr.rs:531-542)
+__global__ void pbox_fallback(const AmrDev A, const PBox* __restrict__ boxes, double* buf, unsigned char* ok) {
+    const PBox b = boxes[blockIdx.x];
+    const int64_t n = (int64_t)b.csz[0] * b.csz[1] * b.csz[2];
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        if (ok[b.off + q]) continue;
+        int64_t c[3];
+        box_coord(q, b.csz, c);
+        const int64_t g[3] = {b.cmin[0] + c[0], b.cmin[1] + c[1], b.cmin[2] + c[2]};
+        amr_sample(A, b.l - 1, g, buf + (b.off + q) * 5, 0);
+        ok[b.off + q] = 1;
+    }
+}
+
+// one separable 6-point prediction pass along dims[di] (amr.rs:560-583)
+__global__ void pbox_pass(const AmrDev A, const PBox* __restrict__ boxes, const double* in, double* outb, int di) {
+    const PBox b = boxes[blockIdx.x];
+    const int d = A.dims[di];
+    int si[3], so[3];
+    pbox_size(A, b, di, si);
+    pbox_size(A, b, di + 1, so);
+    const int64_t n = (int64_t)so[0] * so[1] * so[2];
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        box_coord(q, so, c);
+        const int64_t f = b.fmin[d] + c[d];
+        const int par = (int)amr_erem(f, 2);
+        const int64_t base = amr_ediv(f, 2) + (par == 1 ? -2 : -3) - b.cmin[d];
+        double acc[5] = {0, 0, 0, 0, 0};
+        for (int kk = 0; kk < 6; kk++) {
+            int64_t sc[3] = {c[0], c[1], c[2]};
+            sc[d] = base + kk;
+            const double* v = in + (b.off + box_index(sc, si)) * 5;
+            const double w = A.wp[par][kk];
+            for (int k = 0; k < 5; k++) acc[k] = acc[k] + w * v[k];
+        }
+        double* o = outb + (b.off + q) * 5;
+        for (int k = 0; k < 5; k++) o[k] = acc[k];
+    }
+}
+
+// write the predicted fine box into its target block
+__global__ void pbox_scatter(const AmrDev A, const PBox* __restrict__ boxes, const double* in) {
+    const PBox b = boxes[blockIdx.x];
+    const int64_t n = (int64_t)b.fsz[0] * b.fsz[1] * b.fsz[2];
+    double* u = A.u + (int64_t)b.slot * A.bcell;
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        box_coord(q, b.fsz, c);
+        const int64_t cell = ((b.t0[0] + c[0]) * A.ext[1] + (b.t0[1] + c[1])) * A.ext[2] + (b.t0[2] + c[2]);
+        const double* v = in + (b.off + q) * 5;
+        for (int k = 0; k < 5; k++) u[(int64_t)k * A.ntot + cell] = v[k];
+    }
+}
+
+// fine patch of a restriction box with validity (amr.rs:632-663)
+__global__ void rbox_gather(const AmrDev A, const RBox* __restrict__ boxes, double* buf, unsigned char* ok) {
+    const RBox b = boxes[blockIdx.x];
+    const int lf = b.l + 1;
+    const int64_t n = (int64_t)b.sz[0] * b.sz[1] * b.sz[2];
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        box_coord(q, b.sz, c);
+        int64_t gw[3];
+        bool out = false;
+        for (int d = 0; d < 3; d++) {
+            const int64_t g = b.f0[d] + c[d];
+            gw[d] = g;
+            if (A.act[d]) {
+                const int64_t nf = amr_nlevel(A, lf, d);
+                if (g < 0 || g >= nf) {
+                    if (A.bc[d][g >= nf ? 1 : 0] == EMG_BC_PERIODIC)
+                        gw[d] = amr_erem(g, nf);
+                    else
+                        out = true;
+                }
+            }
+        }
+        double* v = buf + (b.off + q) * 5;
+        unsigned char o = 0;
+        if (!out) {
+            int64_t key[3], lc[3];
+            for (int d = 0; d < 3; d++) {
+                key[d] = A.act[d] ? amr_ediv(gw[d], A.bd[d]) : 0;
+                lc[d] = A.act[d] ? amr_erem(gw[d], A.bd[d]) : 0;
+            }
+            const int id = amr_get(A, lf, key);
+            if (id >= 0) {
+                amr_load(A, id, amr_cell(A, lc), v);
+                o = 1;
+            }
+        }
+        if (!o)
+            for (int k = 0; k < 5; k++) v[k] = 0.0;
+        ok[b.off + q] = o;
+    }
+}
+
+__global__ void rbox_bc(const AmrDev A, const RBox* __restrict__ boxes, double* buf, unsigned char* ok, int di) {
+    const RBox b = boxes[blockIdx.x];
+    const int64_t n = (int64_t)b.sz[0] * b.sz[1] * b.sz[2];
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
+        bc_cell(A, b.l + 1, b.f0, b.sz, q, di, buf, ok, b.off);
+}
+
+// one restriction pass along dims[di] with the shifted stencils and the
+// child-average fallback (amr.rs:674-727)
+__global__ void rbox_pass(const AmrDev A, const RBox* __restrict__ boxes, const double* in, const unsigned char* okin,
+                          double* outb, unsigned char* okout, int di) {
+    const RBox b = boxes[blockIdx.x];
+    const int d = A.dims[di];
+    int si[3], so[3];
+    rbox_size(A, b, di, si);
+    rbox_size(A, b, di + 1, so);
+    const int shifts[5] = {0, -1, 1, -2, 2};
+    const int64_t n = (int64_t)so[0] * so[1] * so[2];
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        box_coord(q, so, c);
+        auto at_src = [&](int64_t pos) {
+            int64_t s2[3] = {c[0], c[1], c[2]};
+            s2[d] = pos;
+            return b.off + box_index(s2, si);
+        };
+        const int64_t base = 2 * c[d] + 2;
+        double acc[5] = {0, 0, 0, 0, 0};
+        bool done = false;
+        for (int m = 0; m < 5 && !done; m++) {
+            const int64_t st = base + shifts[m];
+            if (st < 0 || st + 5 >= si[d]) continue;
+            bool all = true;
+            for (int kk = 0; kk < 6; kk++) all = all && okin[at_src(st + kk)];
+            if (all) {
+                for (int kk = 0; kk < 6; kk++) {
+                    const double* v = in + at_src(st + kk) * 5;
+                    for (int k = 0; k < 5; k++) acc[k] = acc[k] + A.wrs[m][kk] * v[k];
+                }
+                done = true;
+            }
+        }
+        unsigned char o = done ? 1 : 0;
+        if (!done) {
+            const int64_t pa = at_src(base + 2), pb = at_src(base + 3);
+            if (okin[pa] && okin[pb]) {
+                for (int k = 0; k < 5; k++) acc[k] = 0.5 * (in[pa * 5 + k] + in[pb * 5 + k]);
+                o = 1;
+            }
+        }
+        double* ov = outb + (b.off + q) * 5;
+        for (int k = 0; k < 5; k++) ov[k] = acc[k];
+        okout[b.off + q] = o;
+    }
+}
+
+// write the restricted box into the ancestor's interior cells [lo, hi)
+__global__ void rbox_scatter(const AmrDev A, const RBox* __restrict__ boxes, const double* in) {
+    const RBox b = boxes[blockIdx.x];
+    int so[3];
+    for (int d = 0; d < 3; d++) so[d] = b.hi[d] - b.lo[d];
+    const int64_t n = (int64_t)so[0] * so[1] * so[2];
+    double* u = A.u + (int64_t)b.slot * A.bcell;
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        box_coord(q, so, c);
+        const int64_t ic[3] = {b.lo[0] + c[0], b.lo[1] + c[1], b.lo[2] + c[2]};
+        const int64_t cell = amr_cell(A, ic);
+        const double* v = in + (b.off + q) * 5;
+        for (int k = 0; k < 5; k++) u[(int64_t)k * A.ntot + cell] = v[k];
+    }
+}
+
+// Same-level ghost slab copy (fill_scratch, amr.rs:1176-1187): task =
+// (leaf slot, neighbour slot, direction o[3]).
+struct CopyTask {
+    int slot, src;
+    int o[3];
+};
+__global__ void ghost_copy(const AmrDev A, const CopyTask* __restrict__ tasks) {
+    const CopyTask t = tasks[blockIdx.x];
+    int rs[3], sz[3];
+    for (int d = 0; d < 3; d++) {
+        if (!A.act[d]) {
+            rs[d] = 0;
+            sz[d] = 1;
+        } else if (t.o[d] == -1) {
+            rs[d] = 0;
+            sz[d] = A.ng;
+        } else if (t.o[d] == 0) {
+            rs[d] = A.ng;
+            sz[d] = A.bd[d];
+        } else {
+            rs[d] = A.ng + A.bd[d];
+            sz[d] = A.ng;
+        }
+    }
+    const int64_t n = (int64_t)sz[0] * sz[1] * sz[2];
+    double* dst = A.u + (int64_t)t.slot * A.bcell;
+    const double* src = A.u + (int64_t)t.src * A.bcell;
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        box_coord(q, sz, c);
+        int64_t e[3], s[3];
+        for (int d = 0; d < 3; d++) {
+            e[d] = rs[d] + c[d];
+            s[d] = A.act[d] ? e[d] - t.o[d] * A.bd[d] : 0;  // ext index of the neighbour's interior cell
+        }
+        const int64_t de = (e[0] * A.ext[1] + e[1]) * A.ext[2] + e[2];
+        const int64_t se = (s[0] * A.ext[1] + s[1]) * A.ext[2] + s[2];
+        for (int k = 0; k < 5; k++) dst[(int64_t)k * A.ntot + de] = src[(int64_t)k * A.ntot + se];
+    }
+}
+
+// bc_box over the ghost-extended box of a leaf touching the domain boundary
+// (fill_scratch → bc_box, amr.rs:1205-1217), one active axis per launch.
+__global__ void ghost_bc(const AmrDev A, const int* __restrict__ leaves, const int* __restrict__ level,
+                         const int64_t* __restrict__ idx, int di) {
+    const int slot = leaves[blockIdx.x];
+    const int l = level[slot];
+    const int64_t n = (int64_t)A.ext[0] * A.ext[1] * A.ext[2];
+    int64_t g0[3];
+    for (int d = 0; d < 3; d++) g0[d] = idx[3 * slot + d] * A.bd[d] - A.gof[d];
+    int64_t nl[3];
+    for (int e = 0; e < 3; e++) nl[e] = amr_nlevel(A, l, e);
+    const int d = A.dims[di];
+    double* u = A.u + (int64_t)slot * A.bcell;
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        c[2] = q % A.ext[2];
+        c[1] = (q / A.ext[2]) % A.ext[1];
+        c[0] = q / ((int64_t)A.ext[1] * A.ext[2]);
+        const int64_t g[3] = {g0[0] + c[0], g0[1] + c[1], g0[2] + c[2]};
+        auto outside = [&](int e) {
+            return (g[e] < 0 || g[e] >= nl[e]) && A.bc[e][g[e] >= nl[e] ? 1 : 0] != EMG_BC_PERIODIC;
+        };
+        if (!outside(d)) continue;
+        bool later = false;
+        for (int j = di + 1; j < A.ndims; j++) later = later || outside(A.dims[j]);
+        if (later) continue;
+        const int side = g[d] >= nl[d] ? 1 : 0;
+        const int kind = A.bc[d][side];
+        if (kind == EMG_BC_DIRICHLET) {
+            for (int k = 0; k < 5; k++) u[(int64_t)k * A.ntot + q] = A.bcs[d][side][k];
+            continue;
+        }
+        const int64_t sg = kind == EMG_BC_OUTFLOW ? (g[d] < 0 ? 0 : nl[d] - 1) : (side == 0 ? -1 - g[d] : 2 * nl[d] - 1 - g[d]);
+        int64_t sc[3] = {c[0], c[1], c[2]};
+        sc[d] = sg - g0[d];
+        if (sc[d] < 0 || sc[d] >= A.ext[d]) {  // source outside the box: needs sampling
+            atomicOr(A.err, 2u);
+            continue;
+        }
+        const int64_t sq = (sc[0] * A.ext[1] + sc[1]) * A.ext[2] + sc[2];
+        for (int k = 0; k < 5; k++) {
+            double v = u[(int64_t)k * A.ntot + sq];
+            if (kind == EMG_BC_REFLECT && k == 1 + d) v = -v;
+            u[(int64_t)k * A.ntot + q] = v;
+        }
+    }
+}
+
+// Refluxing (amr.rs:1327-1406): one thread per corrected coarse cell applies
+// its corrections in the CPU's order. A task names the coarse face (slot, d,
+// side, pencil) and up to four fine faces.
+struct RefluxTask {
+    int slot, d, side, pen;
+    int nfine;
+    int fslot[4], fpen[4];
+    double dx;
+};
+__global__ void reflux_kernel(const AmrDev A, double* rhs, const double* __restrict__ face, int npen,
+                              const int* __restrict__ cell_slot, const int64_t* __restrict__ cell_ext,
+                              const int* __restrict__ task_start, const RefluxTask* __restrict__ tasks, int ncells) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ncells) return;
+    double* r = rhs + (int64_t)cell_slot[i] * A.bcell + cell_ext[i];
+    double acc[5];
+    for (int k = 0; k < 5; k++) acc[k] = r[(int64_t)k * A.ntot];
+    for (int t = task_start[i]; t < task_start[i + 1]; t++) {
+        const RefluxTask tk = tasks[t];
+        double sum[5] = {0, 0, 0, 0, 0};
+        double cnt = 0.0;
+        for (int f = 0; f < tk.nfine; f++) {
+            const double* fv = face + ((((int64_t)tk.fslot[f] * 3 + tk.d) * 2 + (1 - tk.side)) * 5) * npen + tk.fpen[f];
+            for (int k = 0; k < 5; k++) sum[k] = sum[k] + fv[(int64_t)k * npen];
+            cnt = cnt + 1.0;
+        }
+        const double* fc = face + ((((int64_t)tk.slot * 3 + tk.d) * 2 + tk.side) * 5) * npen + tk.pen;
+        for (int k = 0; k < 5; k++) {
+            const double df = sum[k] / cnt - fc[(int64_t)k * npen];
+            const double dr = tk.side == 1 ? -df / tk.dx : df / tk.dx;
+            acc[k] = acc[k] + dr;
+        }
+    }
+    for (int k = 0; k < 5; k++) r[(int64_t)k * A.ntot] = acc[k];
+}
+
+// SSP-RK3 stage update of the leaves (amr.rs:1476-1498) and, after the third
+// stage, the CFL rate of the new state (amr.rs:1409-1427).
+__global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rhs, const int* __restrict__ leaves,
+                       const int* __restrict__ level, const double* __restrict__ dxl, int stage, StepCtl* ctl) {
+    const int slot = leaves[blockIdx.x];
+    const int l = level[slot];
+    const double dt = ctl->dt;
+    const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
+    const Eos<double> e = Eos<double>::from(A.eos);
+    double rate = 0.0;
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        c[2] = q % A.bd[2];
+        c[1] = (q / A.bd[2]) % A.bd[1];
+        c[0] = q / ((int64_t)A.bd[1] * A.bd[2]);
+        const int64_t cell = (int64_t)slot * A.bcell + amr_cell(A, c);
+        double un[5];
+        for (int k = 0; k < 5; k++) {
+            const int64_t o = (int64_t)k * A.ntot + cell;
+            const double uu = A.u[o], r = rhs[o];
+            double v;
+            if (stage == 1) {
+                u0[o] = uu;
+                v = uu + dt * r;
+            } else if (stage == 2) {
+                v = 0.75 * u0[o] + 0.25 * (uu + dt * r);
+            } else {
+                v = u0[o] / 3.0 + 2.0 / 3.0 * (uu + dt * r);
+            }
+            A.u[o] = v;
+            un[k] = v;
+        }
+        if (stage == 3) {
+            double w[5];
+            to_prim(e, un, w);
+            const double cs = sound_speed(e, w[0], w[4]);
+            double s = -0.0;
+            for (int i = 0; i < A.ndims; i++) {
+                const int d = A.dims[i];
+                s = s + (fabs(w[1 + d]) + cs) / dxl[3 * l + d];
+            }
+            rate = fmax(rate, s);
+        }
+    }
+    if (stage == 3) {
+        for (int o = 16; o > 0; o >>= 1) rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, o));
+        __shared__ double sr[32];
+        if ((threadIdx.x & 31) == 0) sr[threadIdx.x >> 5] = rate;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double v = sr[0];
+            for (int w = 1; w < (int)(blockDim.x >> 5); w++) v = fmax(v, sr[w]);
+            if (!isnan(v) && v > 0.0) atomicMax(&ctl->rate_bits, (unsigned long long)__double_as_longlong(v));
+        }
+    }
+}
+
+// CFL rate of the current leaves (amr.rs:1409-1427)
+__global__ void amr_cfl(const AmrDev A, const int* __restrict__ leaves, const int* __restrict__ level,
+                        const double* __restrict__ dxl, StepCtl* ctl) {
+    const int slot = leaves[blockIdx.x];
+    const int l = level[slot];
+    const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
+    const Eos<double> e = Eos<double>::from(A.eos);
+    double rate = 0.0;
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        c[2] = q % A.bd[2];
+        c[1] = (q / A.bd[2]) % A.bd[1];
+        c[0] = q / ((int64_t)A.bd[1] * A.bd[2]);
+        double uu[5], w[5];
+        amr_load(A, slot, amr_cell(A, c), uu);
+        to_prim(e, uu, w);
+        const double cs = sound_speed(e, w[0], w[4]);
+        double s = -0.0;
+        for (int i = 0; i < A.ndims; i++) {
+            const int d = A.dims[i];
+            s = s + (fabs(w[1 + d]) + cs) / dxl[3 * l + d];
+        }
+        rate = fmax(rate, s);
+    }
+    for (int o = 16; o > 0; o >>= 1) rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, o));
+    __shared__ double sr[32];
+    if ((threadIdx.x & 31) == 0) sr[threadIdx.x >> 5] = rate;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = sr[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) v = fmax(v, sr[w]);
+        if (!isnan(v) && v > 0.0) atomicMax(&ctl->rate_bits, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+// Largest relative wavelet detail of each leaf on the sensors ln ρ, ln(p+p∞)
+// (block_detail, amr.rs:823-867), over its filled ghost-extended box.
+__device__ __forceinline__ void amr_sensor(const AmrDev& A, const Eos<double>& e, const double* u, int64_t cell, double* s) {
+    double q[5], w[5];
+    for (int k = 0; k < 5; k++) q[k] = u[(int64_t)k * A.ntot + cell];
+    to_prim(e, q, w);
+    s[0] = log(fmax(w[0], 1e-300));
+    s[1] = log(fmax(w[4] + e.p_inf, 1e-300));
+}
+__global__ void amr_detail(const AmrDev A, const int* __restrict__ leaves, unsigned long long* det_bits) {
+    const int slot = leaves[blockIdx.x];
+    const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
+    const Eos<double> e = Eos<double>::from(A.eos);
+    const double* u = A.u + (int64_t)slot * A.bcell;
+    const int offs[6] = {-5, -3, -1, 1, 3, 5};
+    double mx = 0.0;
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        c[2] = q % A.bd[2];
+        c[1] = (q / A.bd[2]) % A.bd[1];
+        c[0] = q / ((int64_t)A.bd[1] * A.bd[2]);
+        const int64_t cell = amr_cell(A, c);
+        double s0[2];
+        amr_sensor(A, e, u, cell, s0);
+        for (int i = 0; i < A.ndims; i++) {
+            const int d = A.dims[i];
+            const int64_t stride = d == 0 ? (int64_t)A.ext[1] * A.ext[2] : (d == 1 ? A.ext[2] : 1);
+            double pred[2] = {0.0, 0.0};
+            for (int m = 0; m < 6; m++) {
+                double sv[2];
+                amr_sensor(A, e, u, cell + offs[m] * stride, sv);
+                for (int k = 0; k < 2; k++) pred[k] = pred[k] + A.wr[m] * sv[k];
+            }
+            for (int k = 0; k < 2; k++) {
+                const double dd = fabs(s0[k] - pred[k]);
+                mx = isfinite(dd) ? fmax(mx, dd) : INFINITY;
+            }
+        }
+    }
+    // max over the CTA; +inf orders above every finite bit pattern
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    __shared__ double sr[32];
+    if ((threadIdx.x & 31) == 0) sr[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = sr[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) v = fmax(v, sr[w]);
+        atomicMax(&det_bits[slot], (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+// copy one pool block's state (swap_remove of a coarsened child, amr.rs:1024-1031)
+__global__ void pool_move(const AmrDev A, int from, int to) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < A.bcell; q += (int64_t)gridDim.x * blockDim.x)
+        for (int k = 0; k < 5; k++)
+            A.u[(int64_t)k * A.ntot + (int64_t)to * A.bcell + q] = A.u[(int64_t)k * A.ntot + (int64_t)from * A.bcell + q];
+}
+
+// interior cells of one block from host AoS data (initial condition)
+__global__ void pool_put_interior(const AmrDev A, int slot, const double* __restrict__ aos) {
+    const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        int64_t c[3];
+        c[2] = q % A.bd[2];
+        c[1] = (q / A.bd[2]) % A.bd[1];
+        c[0] = q / ((int64_t)A.bd[1] * A.bd[2]);
+        const int64_t cell = (int64_t)slot * A.bcell + amr_cell(A, c);
+        for (int k = 0; k < 5; k++) A.u[(int64_t)k * A.ntot + cell] = aos[5 * q + k];
+    }
+}
+
+// interior cells of all blocks into AoS [block][cell][5]
+__global__ void pool_get_interior(const AmrDev A, int nblocks, double* __restrict__ aos) {
+    const int64_t nb = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
+    const int64_t n = nb * nblocks;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t slot = t / nb, q = t % nb;
+        int64_t c[3];
+        c[2] = q % A.bd[2];
+        c[1] = (q / A.bd[2]) % A.bd[1];
+        c[0] = q / ((int64_t)A.bd[1] * A.bd[2]);
+        const int64_t cell = slot * A.bcell + amr_cell(A, c);
+        for (int k = 0; k < 5; k++) aos[5 * t + k] = A.u[(int64_t)k * A.ntot + cell];
+    }
+}
+
+}  // namespace emg

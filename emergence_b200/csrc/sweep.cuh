@@ -72,6 +72,20 @@ struct SweepParams {
     double cfl_dx[3];
     double tol;          // hybrid sensor tolerance (C/solver.rs:218)
     EosD eos;
+    // lanes: lane l sits at lane-axis index lane0 + l % lw and other-axis
+    // index ob0 + l / lw (lw = P unless a CTA spans several rows of the other
+    // axis, as for the 16-wide AMR blocks)
+    int lw;
+    // ---- batched block-AMR leaves (amr != 0)
+    int amr;
+    const int* leaf_slot;   // pool slot of launch leaf z / ngroups
+    const int* leaf_level;  // level of each pool slot
+    int64_t bcell;          // cells per pool block (ghost-extended)
+    int ngroups;            // CTAs per leaf along the other axis
+    double dx_level[16];    // cell size along d per level
+    double* face;           // boundary face fluxes [slot][d][side][q][pencil]
+    int npen;               // pencils per block face (padded)
+    int pen_lane_major;     // pencil index = lane*no + other (lane axis is the lower of the two others)
 };
 
 // Flux modes (C/scheme.rs:39-47), a compile-time parameter of the sweep.
@@ -298,23 +312,44 @@ struct Sweep {
             s_weno = 0;
         }
 
-        const int lane0 = blockIdx.x * P;
+        // uniform grids: x = lane tile, y = segment, z = other-axis row;
+        // AMR batches: x = (leaf, group of other-axis rows), lanes cover the block
+        const int lane0 = p.amr ? 0 : blockIdx.x * P;
         const int s0 = blockIdx.y * p.seg;
         const int Ls = min(p.seg, p.nd - s0);
-        const int oc = blockIdx.z;
-        // padded offset of (row 0, lane 0)
-        const int64_t base0 = (int64_t)(p.gd + s0 - 5) * p.sd + (int64_t)(p.gl + lane0) * p.sl + (int64_t)(p.go + oc) * p.so;
-        const int nlanes = min(P, p.nl - lane0);
+        int64_t blk = 0;   // pool offset of the block (AMR) or 0
+        int ob0 = blockIdx.z;
+        int slot_id = 0;
+        double dx = p.dx;
+        if (p.amr) {
+            const int z = blockIdx.x / p.ngroups;
+            ob0 = (blockIdx.x % p.ngroups) * (P / p.lw);
+            slot_id = p.leaf_slot[z];
+            blk = (int64_t)slot_id * p.bcell;
+            dx = p.dx_level[p.leaf_level[slot_id]];
+        }
+        __shared__ int64_t s_loff[P];
+        __shared__ int s_lok[P];
+        __shared__ int s_pen[P];
+        if (tid < P) {
+            const int la = lane0 + tid % p.lw, ob = ob0 + tid / p.lw;
+            s_lok[tid] = la < p.nl && ob < p.no;
+            s_loff[tid] = (int64_t)(p.gl + la) * p.sl + (int64_t)(p.go + ob) * p.so;
+            s_pen[tid] = p.pen_lane_major ? la * p.no + ob : ob * p.nl + la;
+        }
+        // padded offset of row 0 (lane offsets are added per lane)
+        const int64_t base0 = blk + (int64_t)(p.gd + s0 - 5) * p.sd;
         // neighbouring segments recompute the 5 midpoints and 1 face they
         // share; only the owner counts them in the statistics
         const bool tail = s0 + Ls == p.nd;
         const Eos<double> ed = Eos<double>::from(p.eos);
         const Eos<RF> ef = Eos<RF>::from(p.eos);
         constexpr int un = 1 + D;
-        const double lam = (p.ndim * dt) / p.dx;  // λ = ndim·dt/dx (C/solver.rs:393)
+        const double lam = (p.ndim * dt) / dx;  // λ = ndim·dt/dx (C/solver.rs:393, C/amr.rs:1246)
         const double lam2 = 2.0 * lam;
         const bool lim_on = p.positivity && lam > 0.0;  // C/scheme.rs:278
-        const double inv = 1.0 / p.dx;
+        const double inv = 1.0 / dx;
+        __syncthreads();  // lane table
         const int nrounds = (Ls + 5 + RM - 1) / RM;
         const int nrows = Ls + 10;
         double rate_max = 0.0;
@@ -334,9 +369,9 @@ struct Sweep {
                         rr = idx / P;
                         l = idx % P;
                     }
-                    if (l < nlanes) {
+                    if (s_lok[l]) {
                         const int row = lo + rr;
-                        const int64_t g = base0 + (int64_t)row * p.sd + (int64_t)l * p.sl;
+                        const int64_t g = base0 + (int64_t)row * p.sd + s_loff[l];
                         double u[5], w[5];
 #pragma unroll
                         for (int k = 0; k < 5; k++) u[k] = __ldg(p.uin + k * p.ncell + g);
@@ -360,7 +395,7 @@ struct Sweep {
                 // ---- Θ: blend weights of faces [RM r, RM r + RM) (C/scheme.rs:171-182)
                 const int f = RM * r + tid / P;
                 const int l = tid % P;
-                if (f <= Ls && l < nlanes) {
+                if (f <= Ls && s_lok[l]) {
                     const int i = f + 4;
                     double rr = 0.0;
 #pragma unroll
@@ -381,7 +416,7 @@ struct Sweep {
                 // ---- B: midpoints [RM r, RM r + RM)
                 const int m = RM * r + tid / P;
                 const int l = tid % P;
-                if (m < Ls + 5 && l < nlanes) {
+                if (m < Ls + 5 && s_lok[l]) {
                     bool need = true;
                     if constexpr (MODE == MODE_HYBRID) {
                         // only midpoints of faces on the shock path (computed on demand, C/scheme.rs:233-238)
@@ -403,7 +438,7 @@ struct Sweep {
             {
                 const int fidx = RM * r - 4 + tid / P;
                 const int l = tid % P;
-                if (fidx >= 0 && fidx <= Ls && l < nlanes) {
+                if (fidx >= 0 && fidx <= Ls && s_lok[l]) {
                     const int i = fidx + 4;
                     double theta = MODE == MODE_WENO ? 1.0 : 0.0;
                     if constexpr (MODE == MODE_HYBRID) theta = TH[slot(fidx) * P + l];
@@ -475,6 +510,13 @@ struct Sweep {
                     }
 #pragma unroll
                     for (int k = 0; k < 5; k++) F[at<STR>(fidx, k, l)] = fh[k];
+                    if (p.amr && (fidx == 0 || fidx == Ls)) {
+                        // block boundary faces for refluxing (C/amr.rs:1291-1295)
+                        const int side = fidx == 0 ? 0 : 1;
+                        double* fo = p.face + ((((int64_t)slot_id * 3 + D) * 2 + side) * 5) * p.npen + s_pen[l];
+#pragma unroll
+                        for (int k = 0; k < 5; k++) fo[(int64_t)k * p.npen] = fh[k];
+                    }
                 }
             }
             __syncthreads();
@@ -488,12 +530,14 @@ struct Sweep {
                     c = RM * r - 5 + tid / P;
                     l = tid % P;
                 }
-                if (c >= 0 && c < Ls && l < nlanes) {
-                    const int64_t g = base0 + (int64_t)(c + 5) * p.sd + (int64_t)l * p.sl;
+                if (c >= 0 && c < Ls && s_lok[l]) {
+                    const int64_t g = base0 + (int64_t)(c + 5) * p.sd + s_loff[l];
                     double res[5];
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
-                        const double x = (F[at<STR>(c + 1, k, l)] - F[at<STR>(c, k, l)]) * inv;
+                        // the block solver divides by dx (C/amr.rs:1263), the uniform one multiplies by 1/dx
+                        const double df = F[at<STR>(c + 1, k, l)] - F[at<STR>(c, k, l)];
+                        const double x = p.amr ? df / dx : df * inv;
                         const double prev = p.first ? 0.0 : p.rhs[k * p.ncell + g];
                         res[k] = prev - x;
                     }

@@ -514,6 +514,7 @@ int launch_stage(emg_uniform* h, int stage) {
         p.go = h->active[o] ? (int)h->mesh.ng : 0;
         p.d = d;
         p.seg = h->sweepSeg[d];
+        p.lw = h->sweepP[d];
         p.first = d == first_axis;
         p.last = d == last_axis;
         p.stage = stage;

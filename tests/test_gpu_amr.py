@@ -1,0 +1,129 @@
+"""Parity of the device block-AMR solver with the AMR oracle (needs a B200).
+
+The device keeps the reference's block ids, so hierarchies are compared block
+by block: structure (level, coordinates, leaf flag) exactly, block data to the
+north-star 1e-12 relative L1 (and, where the arithmetic order is the same,
+bit for bit)."""
+import numpy as np
+import pytest
+
+from emergence_b200 import workloads as W
+from emergence_b200.physics import Bc, FluxMode, Precision
+from oracle import pyoracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def gpu_amr(*a, **k):
+    from emergence_b200 import GpuAmr
+    return GpuAmr(*a, **k)
+
+
+def rel_l1_blocks(a, b, structure):
+    leaves = structure[:, 4] == 1
+    da, db = a[leaves], b[leaves]
+    num = np.abs(da - db).reshape(-1, 5).sum(axis=0)
+    den = np.abs(db).reshape(-1, 5).sum(axis=0)
+    return np.where(den > 0, num / np.where(den > 0, den, 1), num)
+
+
+def compare(g, o, bitwise=True):
+    sg, so = g.structure(), o.structure()
+    assert sg.shape == so.shape and np.array_equal(sg, so), "hierarchies differ"
+    ug, uo = g.download(), o.download()
+    err = rel_l1_blocks(ug, uo, so)
+    assert np.all(err <= TOL), err
+    if bitwise:
+        leaves = so[:, 4] == 1
+        assert np.array_equal(ug[leaves], uo[leaves]), float(np.nanmax(np.abs(ug[leaves] - uo[leaves])))
+    return err
+
+
+@pytest.mark.parametrize("case", ["explosion2d", "bubble2d"])
+def test_initial_hierarchy_matches_the_oracle(case):
+    if case == "explosion2d":
+        s, cfg, lo, hi, bc, init = W.amr_explosion(dim=2, base=4, levels=3)
+    else:
+        s, cfg, lo, hi, bc, init = W.shock_bubble(dim=2, base=4, levels=3)
+    o = O.OracleAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno)
+    g = gpu_amr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno)
+    compare(g, o)
+    assert g.block_count() == o.block_count()
+
+
+def test_steps_from_the_same_hierarchy_match_bitwise():
+    s, cfg, lo, hi, bc, init = W.amr_explosion(dim=2, base=4, levels=3)
+    o = O.OracleAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno)
+    g = gpu_amr(s, cfg, lo, hi, bc, mode=FluxMode.Weno, blocks=(o.structure(), o.download()))
+    for _ in range(3):  # no regrid yet (due after step 4)
+        dt = o.dt_cfl()
+        assert g.dt_cfl() == dt
+        g.step(dt)
+        o.step(dt)
+        compare(g, o)
+    assert g.counters() == o.counters()
+
+
+@pytest.mark.parametrize("mode", [FluxMode.Weno, FluxMode.Hybrid])
+def test_shock_bubble_2d_with_regrids(mode):
+    s, cfg, lo, hi, bc, init = W.shock_bubble(dim=2, base=4, levels=3)
+    o = O.OracleAmr(s, cfg, lo, hi, bc, init, mode=mode)
+    g = gpu_amr(s, cfg, lo, hi, bc, init, mode=mode)
+    compare(g, o)
+    for i in range(10):  # regrids after steps 4 and 8
+        dt = o.dt_cfl()
+        assert abs(g.dt_cfl() / dt - 1.0) < 1e-14
+        g.step(dt)
+        o.step(dt)
+        err = compare(g, o, bitwise=False)
+    print("shock-bubble 2-D", "mode", mode, "leaves", o.block_count(), "rel L1", err)
+    assert abs(g.t - o.t) <= 1e-15 * o.t
+
+
+def test_shock_bubble_3d_small():
+    s, cfg, lo, hi, bc, init = W.shock_bubble(dim=3, base=2, levels=2)
+    o = O.OracleAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno)
+    g = gpu_amr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno)
+    compare(g, o)
+    for _ in range(5):
+        dt = o.dt_cfl()
+        g.step(dt)
+        o.step(dt)
+    err = compare(g, o, bitwise=False)
+    print("shock-bubble 3-D small: leaves", o.block_count(), "rel L1", err)
+
+
+def test_amr_mixed_precision_error():
+    s, cfg, lo, hi, bc, init = W.shock_bubble(dim=2, base=4, levels=3)
+    o = O.OracleAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno)
+    g = gpu_amr(s, cfg, lo, hi, bc, mode=FluxMode.Weno, precision=Precision.Mixed,
+                blocks=(o.structure(), o.download()))
+    for _ in range(3):
+        dt = o.dt_cfl()
+        g.step(dt)
+        o.step(dt)
+    st = o.structure()
+    ug, uo = g.download(), o.download()
+    leaves = st[:, 4] == 1
+    num = np.abs(ug[leaves] - uo[leaves]).reshape(-1, 5).sum(axis=0)
+    den = np.abs(uo[leaves]).reshape(-1, 5).sum(axis=0)
+    # fields that are (nearly) zero in the oracle — the transverse momenta
+    # before the shock reaches the bubble — are measured against the density
+    den = np.maximum(den, 1e-3 * den[0])
+    err = num / den
+    print("AMR mixed rel L1", err)
+    assert np.all(err <= 1e-5)
+
+
+def test_conservation_across_levels_on_the_device():
+    s, cfg, lo, hi, bc, init = W.amr_explosion(dim=2, base=4, levels=3, radius=0.25)
+    bc = [[Bc.Periodic, Bc.Periodic] for _ in range(3)]
+    g = gpu_amr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno)
+    t0 = g.totals()
+    for _ in range(3):
+        g.step(g.dt_cfl())
+    t1 = g.totals()
+    assert abs(t1[0] - t0[0]) <= 1e-13 * abs(t0[0])
+    assert abs(t1[4] - t0[4]) <= 1e-13 * abs(t0[4])
