@@ -748,8 +748,8 @@ struct emg_amr {
             p.npen = npen;
             p.pen_lane_major = lane < other ? 1 : 0;
             const dim3 grid((unsigned)(nleaves * p.ngroups), 1, 1);
-            cudaError_t e = opts.precision == EMG_PRECISION_MIXED ? sweep_launch_mixed(P, opts.mode, p, grid, stream)
-                                                                   : sweep_launch_f64(P, opts.mode, p, grid, stream);
+            cudaError_t e = opts.precision == EMG_PRECISION_MIXED ? sweep_launch_amr_mixed(P, opts.mode, p, grid, stream)
+                                                                   : sweep_launch_amr_f64(P, opts.mode, p, grid, stream);
             launches++;
             if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("AMR sweep: ") + cudaGetErrorString(e));
         }

@@ -127,7 +127,7 @@ template <typename RF, int P, int MODE> struct SweepSmem {
     }
 };
 
-template <typename RF, int P, int D, int MODE>
+template <typename RF, int P, int D, int MODE, bool AMR = false>
 struct Sweep {
     using SM = SweepSmem<RF, P, MODE>;
     static constexpr int T = SWEEP_THREADS;
@@ -314,14 +314,14 @@ struct Sweep {
 
         // uniform grids: x = lane tile, y = segment, z = other-axis row;
         // AMR batches: x = (leaf, group of other-axis rows), lanes cover the block
-        const int lane0 = p.amr ? 0 : blockIdx.x * P;
+        const int lane0 = AMR ? 0 : blockIdx.x * P;
         const int s0 = blockIdx.y * p.seg;
         const int Ls = min(p.seg, p.nd - s0);
         int64_t blk = 0;   // pool offset of the block (AMR) or 0
         int ob0 = blockIdx.z;
         int slot_id = 0;
         double dx = p.dx;
-        if (p.amr) {
+        if constexpr (AMR) {
             const int z = blockIdx.x / p.ngroups;
             ob0 = (blockIdx.x % p.ngroups) * (P / p.lw);
             slot_id = p.leaf_slot[z];
@@ -332,10 +332,11 @@ struct Sweep {
         __shared__ int s_lok[P];
         __shared__ int s_pen[P];
         if (tid < P) {
-            const int la = lane0 + tid % p.lw, ob = ob0 + tid / p.lw;
+            const int lw = AMR ? p.lw : P;
+            const int la = lane0 + tid % lw, ob = ob0 + tid / lw;
             s_lok[tid] = la < p.nl && ob < p.no;
             s_loff[tid] = (int64_t)(p.gl + la) * p.sl + (int64_t)(p.go + ob) * p.so;
-            s_pen[tid] = p.pen_lane_major ? la * p.no + ob : ob * p.nl + la;
+            if constexpr (AMR) s_pen[tid] = p.pen_lane_major ? la * p.no + ob : ob * p.nl + la;
         }
         // padded offset of row 0 (lane offsets are added per lane)
         const int64_t base0 = blk + (int64_t)(p.gd + s0 - 5) * p.sd;
@@ -510,7 +511,7 @@ struct Sweep {
                     }
 #pragma unroll
                     for (int k = 0; k < 5; k++) F[at<STR>(fidx, k, l)] = fh[k];
-                    if (p.amr && (fidx == 0 || fidx == Ls)) {
+                    if (AMR && (fidx == 0 || fidx == Ls)) {
                         // block boundary faces for refluxing (C/amr.rs:1291-1295)
                         const int side = fidx == 0 ? 0 : 1;
                         double* fo = p.face + ((((int64_t)slot_id * 3 + D) * 2 + side) * 5) * p.npen + s_pen[l];
@@ -537,11 +538,11 @@ struct Sweep {
                     for (int k = 0; k < 5; k++) {
                         // the block solver divides by dx (C/amr.rs:1263), the uniform one multiplies by 1/dx
                         const double df = F[at<STR>(c + 1, k, l)] - F[at<STR>(c, k, l)];
-                        const double x = p.amr ? df / dx : df * inv;
+                        const double x = AMR ? df / dx : df * inv;
                         const double prev = p.first ? 0.0 : p.rhs[k * p.ncell + g];
                         res[k] = prev - x;
                     }
-                    if (!p.last) {
+                    if (AMR || !p.last) {
 #pragma unroll
                         for (int k = 0; k < 5; k++) p.rhs[k * p.ncell + g] = res[k];
                     } else {
@@ -577,7 +578,7 @@ struct Sweep {
             // the next round's loads only touch W slots whose rows C has finished
             // with (barrier above), and its C writes F slots after two more barriers
         }
-        if (p.cfl_fuse) {
+        if (!AMR && p.cfl_fuse) {
             double v = rate_max;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -588,7 +589,7 @@ struct Sweep {
             if (s_weno) atomicAdd(&p.ctl->counters[1], (unsigned long long)s_weno);
             if (s_fallback) atomicAdd(&p.ctl->counters[2], (unsigned long long)s_fallback);
             if (s_limited) atomicAdd(&p.ctl->counters[3], (unsigned long long)s_limited);
-            if (p.cfl_fuse) {
+            if (!AMR && p.cfl_fuse) {
                 double v = s_rate[0];
                 for (int w = 1; w < T / 32; w++) v = fmax(v, s_rate[w]);
                 if (!isnan(v) && v > 0.0) atomicMax(&p.ctl->rate_bits, (unsigned long long)__double_as_longlong(v));

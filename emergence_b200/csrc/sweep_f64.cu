@@ -4,9 +4,29 @@
 
 namespace emg {
 
-template <int P, int D, int MODE>
+template <int P, int D, int MODE, bool AMR = false>
 __global__ void __launch_bounds__(SWEEP_THREADS, 2) sweep_f64_kernel(const SweepParams p) {
-    Sweep<double, P, D, MODE>::run(p);
+    Sweep<double, P, D, MODE, AMR>::run(p);
+}
+
+// batched block-AMR leaves: P = 16 or 32 pencils, one block per lane set
+template <int P, int D, int MODE> static cudaError_t launch_amr(const SweepParams& p, dim3 grid, cudaStream_t s) {
+    sweep_f64_kernel<P, D, MODE, true><<<grid, SWEEP_THREADS, SweepSmem<double, P, MODE>::bytes(), s>>>(p);
+    return cudaGetLastError();
+}
+template <int P, int MODE> static cudaError_t launch_amr_d(const SweepParams& p, dim3 grid, cudaStream_t s) {
+    return p.d == 0 ? launch_amr<P, 0, MODE>(p, grid, s) : (p.d == 1 ? launch_amr<P, 1, MODE>(p, grid, s) : launch_amr<P, 2, MODE>(p, grid, s));
+}
+template <int MODE> static cudaError_t launch_amr_p(int P, const SweepParams& p, dim3 grid, cudaStream_t s) {
+    return P == 16 ? launch_amr_d<16, MODE>(p, grid, s) : (P == 32 ? launch_amr_d<32, MODE>(p, grid, s) : cudaErrorInvalidValue);
+}
+cudaError_t sweep_launch_amr_f64(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s) {
+    switch (mode) {
+        case MODE_WENO: return launch_amr_p<MODE_WENO>(P, p, grid, s);
+        case MODE_HYBRID: return launch_amr_p<MODE_HYBRID>(P, p, grid, s);
+        case MODE_CENTRAL: return launch_amr_p<MODE_CENTRAL>(P, p, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 template <int P, int D, int MODE> static cudaError_t launch(const SweepParams& p, dim3 grid, cudaStream_t s) {
@@ -42,6 +62,11 @@ template <int P, int MODE> static cudaError_t attr_d() {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_f64_kernel<P, 0, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_f64_kernel<P, 1, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_f64_kernel<P, 2, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if constexpr (P >= 16) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_f64_kernel<P, 0, MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_f64_kernel<P, 1, MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_f64_kernel<P, 2, MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    }
     return e;
 }
 

@@ -8,6 +8,9 @@ namespace emg {
 // P = pencils per CTA (8, 16 or 32); mode = SweepMode. Returns the launch error.
 cudaError_t sweep_launch_f64(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 cudaError_t sweep_launch_mixed(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
+// Batched block-AMR leaves (SweepParams::amr set), P = 16 or 32.
+cudaError_t sweep_launch_amr_f64(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
+cudaError_t sweep_launch_amr_mixed(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 // Opt the kernels into their dynamic shared memory size (once per device).
 cudaError_t sweep_prepare_f64();
 cudaError_t sweep_prepare_mixed();
