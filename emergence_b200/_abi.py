@@ -78,6 +78,8 @@ SIGNATURES = {
     "emg_uniform_set_profiling": (C.c_int, [_P, C.c_int]),
     "emg_uniform_kernel_times": (C.c_int, [_P, _D, _U64]),
     "emg_uniform_launch_count": (C.c_int, [_P, _U64]),
+    "emg_uniform_step_noalloc": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc),
+                                           C.POINTER(EmgOpts), C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
     "emg_amr_create": (C.c_int, [C.POINTER(EmgAmrConfig), C.POINTER(EmgEos), _D, _D, C.POINTER(EmgBc),
                                  C.POINTER(EmgOpts), INIT_FN, C.c_void_p, C.POINTER(_P)]),
     "emg_amr_create_from_blocks": (C.c_int, [C.POINTER(EmgAmrConfig), C.POINTER(EmgEos), _D, _D, C.POINTER(EmgBc),

@@ -305,6 +305,24 @@ __global__ void ctl_begin_device(StepCtl* ctl, double cfl) {
     ctl->rate_bits = 0ull;
 }
 
+// Fixed scratch of the allocation-free step: a 256-byte control block, then
+// the two stage buffers and the residual for grids up to
+// EMG_NOALLOC_MAX_CELLS padded cells.
+constexpr size_t NOALLOC_CTL_DOUBLES = 32;
+static_assert(sizeof(StepCtl) <= NOALLOC_CTL_DOUBLES * sizeof(double), "control block does not fit");
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_CTL_DOUBLES + 3 * 5 * (size_t)EMG_NOALLOC_MAX_CELLS];
+
+// zero the whole control block (status, counters, flags) and set dt
+__global__ void ctl_reset_all(StepCtl* ctl, double dt) {
+    unsigned char* b = reinterpret_cast<unsigned char*>(ctl);
+    for (int i = threadIdx.x; i < (int)sizeof(StepCtl); i += blockDim.x) b[i] = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ctl->dt = dt;
+        ctl->t_end = INFINITY;
+    }
+}
+
 __global__ void ctl_end(StepCtl* ctl) {
     if (ctl->done) return;
     ctl->t = ctl->t + ctl->dt;
@@ -980,6 +998,92 @@ int emg_uniform_kernel_times(emg_uniform* h, double* ms, uint64_t* launches) {
 int emg_uniform_launch_count(emg_uniform* h, uint64_t* launches) {
     if (!h || !launches) return set_error(EMG_ERR_INVALID, "null argument");
     *launches = h->launches;
+    return EMG_OK;
+}
+
+// Allocation-free step: the emg_uniform object lives on the host stack and
+// its device buffers point into g_noalloc_scratch; nothing is allocated.
+int emg_uniform_step_noalloc(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
+                             const double* u_in, double* u_out, double dt, void* stream) {
+    if (!mesh || !eos || !bc || !opts || !u_in || !u_out) return set_error(EMG_ERR_INVALID, "null argument");
+    if (u_in == u_out) return set_error(EMG_ERR_INVALID, "u_in and u_out must be distinct buffers");
+    if (mesh->ng < 5) return set_error(EMG_ERR_INVALID, "the WCNS stencil needs ng >= 5 ghost layers");
+    if (opts->mode != EMG_MODE_WENO && opts->mode != EMG_MODE_HYBRID && opts->mode != EMG_MODE_CENTRAL)
+        return set_error(EMG_ERR_INVALID, "unknown flux mode");
+    if (opts->precision != EMG_PRECISION_F64 && opts->precision != EMG_PRECISION_MIXED)
+        return set_error(EMG_ERR_INVALID, "unknown precision");
+    int ndim = 0;
+    int64_t ncell = 1;
+    for (int d = 0; d < 3; d++) {
+        if (mesh->n[d] < 1) return set_error(EMG_ERR_INVALID, "mesh extents must be >= 1");
+        if (mesh->n[d] > 1) {
+            ndim++;
+            if (!(mesh->dx[d] > 0.0)) return set_error(EMG_ERR_INVALID, "dx must be > 0 on active axes");
+            ncell *= mesh->n[d] + 2 * mesh->ng;
+        }
+        if (ncell > EMG_NOALLOC_MAX_CELLS)
+            return set_error(EMG_ERR_INVALID, "grid exceeds EMG_NOALLOC_MAX_CELLS padded cells (131072)");
+    }
+    if (ndim == 0) return set_error(EMG_ERR_INVALID, "mesh has no active axis");
+    for (int i = 0; i < 6; i++)
+        if (bc[i].kind < 0 || bc[i].kind > 4) return set_error(EMG_ERR_INVALID, "unknown boundary condition");
+    int dev = 0;
+    EMG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(EMG_ERR_INVALID, "device index out of range");
+    // once per device, with that device current: the scratch address and the
+    // sweep kernels' shared-memory attribute
+    static double* scratch_ptr[64] = {nullptr};
+    if (!scratch_ptr[dev]) {
+        double* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return set_error(EMG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        e = sweep_prepare_f64();
+        if (e == cudaSuccess) e = sweep_prepare_mixed();
+        if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("sweep setup: ") + cudaGetErrorString(e));
+        scratch_ptr[dev] = ptr;
+    }
+    double* base = scratch_ptr[dev];
+    emg_uniform h;
+    h.device = dev;
+    h.stream = (cudaStream_t)stream;
+    h.mesh = *mesh;
+    h.eos = *eos;
+    for (int i = 0; i < 6; i++) h.bc[i] = bc[i];
+    h.opts = *opts;
+    h.ndim = ndim;
+    for (int d = 0; d < 3; d++) {
+        h.active[d] = mesh->n[d] > 1;
+        h.m[d] = h.active[d] ? mesh->n[d] + 2 * mesh->ng : 1;
+    }
+    h.stride[2] = 1;
+    h.stride[1] = h.m[2];
+    h.stride[0] = h.m[1] * h.m[2];
+    h.ncell = ncell;
+    h.cells = mesh->n[0] * mesh->n[1] * mesh->n[2];
+    for (int d = 0; d < 3; d++)
+        if (h.active[d] && mesh->n[d] < mesh->ng &&
+            (bc[2 * d].kind == EMG_BC_REFLECT || bc[2 * d + 1].kind == EMG_BC_REFLECT))
+            h.deep = true;
+    h.ctl = reinterpret_cast<StepCtl*>(base);
+    h.sa = base + NOALLOC_CTL_DOUBLES;
+    h.sb = h.sa + 5 * (size_t)EMG_NOALLOC_MAX_CELLS;
+    h.rhs = h.sb + 5 * (size_t)EMG_NOALLOC_MAX_CELLS;
+    h.u = u_out;
+    plan_sweeps(&h);
+    for (int d = 0; d < 3; d++)
+        if (h.active[d] && (h.sweepGrid[d].y > 65535u || h.sweepGrid[d].z > 65535u))
+            return set_error(EMG_ERR_INVALID, "mesh too large for the sweep grid");
+    // u_out starts as a copy of u_in; the stage kernels then work in place on
+    // it (ghosts filled at stage 1, the stage-3 update written back)
+    EMG_CUDA(cudaMemcpyAsync(u_out, u_in, (size_t)ncell * 5 * sizeof(double), cudaMemcpyDeviceToDevice, h.stream));
+    ctl_reset_all<<<1, 128, 0, h.stream>>>(h.ctl, dt);
+    EMG_CUDA(cudaGetLastError());
+    for (int stage = 1; stage <= 3; stage++) {
+        int rc = launch_stage(&h, stage);
+        if (rc) return rc;
+    }
+    EMG_CUDA(cudaGetLastError());
     return EMG_OK;
 }
 

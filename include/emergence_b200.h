@@ -189,6 +189,28 @@ int emg_uniform_kernel_times(emg_uniform* h, double* ms, uint64_t* launches);
 /* Number of kernel launches issued by the handle since creation. */
 int emg_uniform_launch_count(emg_uniform* h, uint64_t* launches);
 
+/* Largest padded cell count (m0·m1·m2) accepted by emg_uniform_step_noalloc. */
+#define EMG_NOALLOC_MAX_CELLS 131072
+
+/* One SSP-RK3 step of size dt on a uniform grid that allocates no memory:
+ * no counterpart in the reference (its GpuSolver always owns device buffers).
+ * For callers that cannot call cudaMalloc — code running where a framework or
+ * an allocator owns all device memory, or between allocator-free phases — the
+ * caller passes device pointers to the input and output states (SoA
+ * u[q·ncell + cell], q = 0..4, the ghost-padded layout of emg_uniform_create)
+ * and the library uses a fixed scratch area in its own static device memory
+ * (3·5·EMG_NOALLOC_MAX_CELLS doubles plus a control block, ≈15.7 MB, held by
+ * every GPU that loads the library until the process exits). u_in is read
+ * only; u_out receives the new state with the ghost layers of the stage-1 fill.
+ * Grids above EMG_NOALLOC_MAX_CELLS padded cells return EMG_ERR_INVALID. The
+ * first call on a device resolves the scratch address and sets kernel
+ * attributes (make it before any stream capture). All calls share the one
+ * scratch area, so calls that overlap on the GPU (other streams, other host
+ * threads) race; serialize them. Work is queued on `stream` (a cudaStream_t,
+ * NULL for the legacy default stream) and the call does not synchronize. */
+int emg_uniform_step_noalloc(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
+                             const double* u_in, double* u_out, double dt, void* stream);
+
 /* ------------------------------------------------------------------ block AMR */
 
 /* Block-AMR configuration (C/amr.rs:49-63). Blocks are b cells per active
