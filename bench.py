@@ -42,8 +42,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg of the uniform workload")
-    ap.add_argument("--workload", default="uniform", choices=["uniform", "amr"],
-                    help="uniform: 3-D explosion 256^3; amr: 3-D shock-bubble on block AMR (base 128^3, 3 levels)")
+    ap.add_argument("--workload", default="uniform", choices=["uniform", "amr", "batch"],
+                    help="uniform: 3-D explosion 256^3; amr: 3-D shock-bubble on block AMR (base 128^3, 3 levels); "
+                         "batch: 4096 independent 1-D Riemann problems")
     ap.add_argument("--amr-base", type=int, default=8, help="AMR base blocks per side (16^3 cells each)")
     return ap.parse_args()
 
@@ -371,6 +372,75 @@ def run_amr(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_batch(args, world, rank, local):
+    """4096 independent 1-D Riemann problems (cells log-uniform in [64, 2048],
+    ρ, p ∈ U[0.1, 2], u ∈ U[−1, 1] on each side, interface at 0.5, outflow),
+    each run to t = 0.15 with its own CFL steps, all instances in one launch
+    per RK stage. One "step" = one whole run; the metric counts the cell
+    updates of every instance."""
+    import numpy as np
+    import torch
+    from emergence_b200 import GpuBatch1D, workloads as W
+    from emergence_b200.physics import FluxMode, Precision
+
+    torch.cuda.set_device(local)
+    dev = torch.cuda.current_device()
+    prec = Precision.F64 if args.precision == "f64" else Precision.Mixed
+    sys_, n, dx, u, st = W.riemann_batch()
+    for _ in range(max(args.warmup, 1)):
+        g = GpuBatch1D(sys_, n, dx, u, precision=prec)
+        g.run_to(0.15)
+        g.close()
+    total_ms, updates = 0.0, 0
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            g = GpuBatch1D(sys_, n, dx, u, precision=prec)
+            stream = torch.cuda.ExternalStream(g.stream())
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record(stream)
+            launched = g.run_to(0.15)
+            b.record(stream)
+            b.synchronize()
+            total_ms += a.elapsed_time(b)
+            t, steps = g.status()
+            updates += int((n * steps.astype(np.int64)).sum())
+            g.close()
+    value = updates * world / (total_ms * 1e-3)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import pyoracle as O
+        from emergence_b200.physics import Bc, Mesh
+        sub = slice(0, 256, 8)  # 32 instances of the same batch
+        cu, tc = 0, time.perf_counter()
+        offs = np.concatenate([[0], np.cumsum(n)])
+        for i in range(*sub.indices(len(n))):
+            mesh = Mesh.new((int(n[i]), 1, 1), (0, 0, 0), (1, 1, 1), ng=6)
+            uu = np.zeros((mesh.len(), 5))
+            uu[6:6 + n[i]] = u[offs[i]:offs[i + 1]]
+            o = O.OracleSolver(sys_, mesh, uu, bc=[[Bc.Outflow] * 2, [Bc.Periodic] * 2, [Bc.Periodic] * 2],
+                               mode=FluxMode.Weno, cfl=0.5)
+            cu += int(n[i]) * o.run_to(0.15)
+        el = time.perf_counter() - tc
+        cpu = {"value": cu / el, "unit": "cell-updates/s", "cores": O.num_threads(), "kind": "port",
+               "sample": "32 of the 4096 instances (every 8th of the first 256), each run to t = 0.15; "
+                         "C++ restatement of the reference CPU solver"}
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == Precision.F64 else "f32-flux/f64-state",
+            "data": "synthetic",
+            "config": {"workload": "4096 independent 1-D Riemann problems, cells log-uniform [64, 2048] (sum %d), "
+                                   "rho,p~U[0.1,2], u~U[-1,1], t_end 0.15, outflow, per-instance CFL 0.5" % int(n.sum()),
+                       "step": "one whole batched run to t_end", "batch_steps": int(launched),
+                       "precision": args.precision},
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_init(args)
@@ -379,6 +449,8 @@ def main():
             run_reference(args, world, rank)
         elif args.workload == "amr":
             run_amr(args, world, rank, local)
+        elif args.workload == "batch":
+            run_batch(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -8,7 +8,8 @@ limiter, SSP-RK3, ghost fill, CFL reduction), behind the C ABI of
 from .physics import Bc, Euler, FluxMode, Mesh, Nasg, Precision, initial_state
 from .solver import GpuSolver, device_count
 from .amr import GpuAmr
+from .batch import GpuBatch1D
 from ._abi import EmgError, LIB_PATH
 
-__all__ = ["Bc", "Euler", "FluxMode", "Mesh", "Nasg", "Precision", "initial_state", "GpuSolver", "GpuAmr", "device_count",
+__all__ = ["Bc", "Euler", "FluxMode", "Mesh", "Nasg", "Precision", "initial_state", "GpuSolver", "GpuAmr", "GpuBatch1D", "device_count",
            "EmgError", "LIB_PATH"]

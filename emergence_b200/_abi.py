@@ -80,6 +80,13 @@ SIGNATURES = {
     "emg_uniform_launch_count": (C.c_int, [_P, _U64]),
     "emg_uniform_step_noalloc": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc),
                                            C.POINTER(EmgOpts), C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
+    "emg_batch1d_create": (C.c_int, [C.POINTER(EmgEos), C.POINTER(EmgOpts), C.POINTER(EmgBc), C.c_size_t,
+                                     C.POINTER(C.c_int64), _D, _D, C.POINTER(_P)]),
+    "emg_batch1d_destroy": (C.c_int, [_P]),
+    "emg_batch1d_run_to": (C.c_int, [_P, C.c_double, _U64]),
+    "emg_batch1d_download": (C.c_int, [_P, _D]),
+    "emg_batch1d_status": (C.c_int, [_P, _D, _U64]),
+    "emg_batch1d_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "emg_amr_create": (C.c_int, [C.POINTER(EmgAmrConfig), C.POINTER(EmgEos), _D, _D, C.POINTER(EmgBc),
                                  C.POINTER(EmgOpts), INIT_FN, C.c_void_p, C.POINTER(_P)]),
     "emg_amr_create_from_blocks": (C.c_int, [C.POINTER(EmgAmrConfig), C.POINTER(EmgEos), _D, _D, C.POINTER(EmgBc),

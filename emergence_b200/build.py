@@ -5,6 +5,7 @@ Usage: python -m emergence_b200.build  (or import and call build()).
 Translation units and their FMA policy:
   uniform.cu      host object, ghost/CFL/control kernels, C ABI  -fmad=false
   amr.cu          block-AMR host object, AMR kernels, C ABI      -fmad=false
+  batch1d.cu      batched independent 1-D lines, C ABI           -fmad=false
   sweep_f64.cu    plain FP64 fused sweep                          -fmad=false
   sweep_mixed.cu  FP32-flux fused sweep                           -fmad=true
 The FP64 units keep every multiply and add separately rounded so that their
@@ -25,6 +26,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("uniform.cu", ["-fmad=false"]),
     ("amr.cu", ["-fmad=false"]),
+    ("batch1d.cu", ["-fmad=false"]),
     ("sweep_f64.cu", ["-fmad=false"]),
     ("sweep_mixed.cu", ["-fmad=true", "-use_fast_math"]),
 ]

@@ -141,6 +141,9 @@ struct emg_amr {
     DevVec<PBox> dpbox;
     std::vector<DevVec<RBox>> drbox;  // per level
     DevVec<RefluxTask> dreflux;
+    DevVec<PBox> dtmp_pbox;    // one-off prediction boxes (refined children)
+    DevVec<RBox> dtmp_rbox;    // one-off restriction boxes (coarsened parents)
+    DevVec<double> dstage;     // host initial data of new blocks
     std::vector<int> rbox_count;
     int ncopy = 0, npbox = 0, nbcleaves = 0, nrefcells = 0, nleaves = 0;
     bool layout_valid = false, map_dirty = true;
@@ -397,12 +400,8 @@ struct emg_amr {
             mx = std::max(mx, b.cap);
         }
         if ((rc = scratch(off))) return rc;
-        DevVec<PBox> tmp;
-        if ((rc = tmp.put(boxes, stream))) return rc;
-        rc = run_pboxes(tmp.p, (int)boxes.size(), mx);
-        cudaStreamSynchronize(stream);
-        tmp.release();
-        return rc;
+        if ((rc = dtmp_pbox.put(boxes, stream))) return rc;
+        return run_pboxes(dtmp_pbox.p, (int)boxes.size(), mx);
     }
 
     // ---------------------------------------------------------------- restriction boxes
@@ -840,14 +839,13 @@ struct emg_amr {
             us[5 * q + 3] = rho * w[3];
             us[5 * q + 4] = rho * e + ke;
         }
-        double* tmp = nullptr;
-        AMR_CUDA(cudaMalloc(&tmp, us.size() * sizeof(double)));
-        cudaMemcpyAsync(tmp, us.data(), us.size() * sizeof(double), cudaMemcpyHostToDevice, stream);
+        // the staging buffer is reused: wait for the previous block's copy-in
+        AMR_CUDA(cudaStreamSynchronize(stream));
+        int rc = dstage.put(us, stream);
+        if (rc) return rc;
         AmrDev A = view();
-        pool_put_interior<<<16, 256, 0, stream>>>(A, id, tmp);
+        pool_put_interior<<<16, 256, 0, stream>>>(A, id, dstage.p);
         launches++;
-        cudaStreamSynchronize(stream);
-        cudaFree(tmp);
         AMR_CUDA(cudaGetLastError());
         return EMG_OK;
     }
@@ -915,12 +913,8 @@ struct emg_amr {
             RBox b = make_rbox(l, pid, idx, {0, 0, 0}, {bd[0], bd[1], bd[2]});
             b.off = 0;
             if ((rc = scratch(b.cap))) return rc;
-            DevVec<RBox> tmp;
-            if ((rc = tmp.put(std::vector<RBox>{b}, stream))) return rc;
-            rc = run_rboxes(tmp.p, 1, b.cap);
-            cudaStreamSynchronize(stream);
-            tmp.release();
-            if (rc) return rc;
+            if ((rc = dtmp_rbox.put(std::vector<RBox>{b}, stream))) return rc;
+            if ((rc = run_rboxes(dtmp_rbox.p, 1, b.cap))) return rc;
         }
         blocks[pid].leaf = true;
         std::vector<int> ids;
@@ -1212,10 +1206,6 @@ struct emg_amr {
         std::memset(ctl_host, 0, sizeof(StepCtl));
         ctl_host->t_end = INFINITY;
         AMR_CUDA(cudaMemcpy(ctl, ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice));
-        // deep predictions recurse through sample/predict
-        size_t stack = 0;
-        cudaDeviceGetLimit(&stack, cudaLimitStackSize);
-        if (stack < 8192) cudaDeviceSetLimit(cudaLimitStackSize, 8192);
         int rc = ddxl.put(dxl, stream);
         if (rc) return rc;
         static bool prepared = false;
@@ -1256,6 +1246,9 @@ struct emg_amr {
         dpbox.release();
         for (auto& r : drbox) r.release();
         dreflux.release();
+        dtmp_pbox.release();
+        dtmp_rbox.release();
+        dstage.release();
         if (stream) cudaStreamDestroy(stream);
     }
 };

@@ -74,14 +74,19 @@ __device__ __forceinline__ void amr_load(const AmrDev& A, int slot, int64_t cell
     for (int q = 0; q < 5; q++) v[q] = p[(int64_t)q * A.ntot];
 }
 
-__device__ void amr_predict(const AmrDev& A, int l, const int64_t* g, double* out, int depth);
+template <int DEPTH> __device__ void amr_predict_t(const AmrDev& A, int l, const int64_t* g, double* out);
 
 // Conserved value of global cell g at level l (amr.rs:384-439). Boundary
 // kinds: periodic, outflow, reflect, Dirichlet (the characteristic kind is
-// rejected when the solver is built).
-__device__ void amr_sample(const AmrDev& A, int l, const int64_t* g_in, double* v, int depth) {
+// rejected when the solver is built). DEPTH bounds the chain of predictions
+// from coarser levels (the reference recurses; with 2:1 balance and kept
+// ancestors one level suffices in practice) so that no kernel recurses; a
+// chain deeper than DEPTH sets the error word.
+template <int DEPTH>
+__device__ __forceinline__ void amr_sample_t(const AmrDev& A, int l, const int64_t* g_in, double* v) {
     int64_t g[3] = {g_in[0], g_in[1], g_in[2]};
     bool flip[3] = {false, false, false};
+#pragma unroll
     for (int d = 2; d >= 0; d--) {
         if (!A.act[d]) {
             g[d] = 0;
@@ -106,6 +111,7 @@ __device__ void amr_sample(const AmrDev& A, int l, const int64_t* g_in, double* 
         }
     }
     int64_t key[3], c[3];
+#pragma unroll
     for (int d = 0; d < 3; d++) {
         key[d] = A.act[d] ? amr_ediv(g[d], A.bd[d]) : 0;
         c[d] = A.act[d] ? amr_erem(g[d], A.bd[d]) : 0;
@@ -114,40 +120,51 @@ __device__ void amr_sample(const AmrDev& A, int l, const int64_t* g_in, double* 
     if (id >= 0) {
         amr_load(A, id, amr_cell(A, c), v);
     } else {
-        amr_predict(A, l, g, v, depth + 1);
+        amr_predict_t<DEPTH>(A, l, g, v);
     }
+#pragma unroll
     for (int d = 0; d < 3; d++)
         if (flip[d]) v[1 + d] = -v[1 + d];
 }
 
 // Direct 6^D prediction of cell g (level l) from level l − 1 (amr.rs:589-613).
-__device__ void amr_predict(const AmrDev& A, int l, const int64_t* g, double* out, int depth) {
+template <int DEPTH> __device__ void amr_predict_t(const AmrDev& A, int l, const int64_t* g, double* out) {
 #pragma unroll
     for (int q = 0; q < 5; q++) out[q] = 0.0;
-    if (depth > 2 * AMR_MAX_LEVELS || l <= 0) {
+    if constexpr (DEPTH <= 0) {
         atomicOr(A.err, 1u);
         return;
-    }
-    int total = 1;
-    for (int i = 0; i < A.ndims; i++) total *= 6;
-    for (int s = 0; s < total; s++) {
-        double w = 1.0;
-        int64_t c[3] = {0, 0, 0};
-        int rem = s;
-        for (int i = 0; i < A.ndims; i++) {
-            const int d = A.dims[i];
-            const int k = rem % 6;
-            rem /= 6;
-            const int odd = (int)amr_erem(g[d], 2);
-            const int64_t base = amr_ediv(g[d], 2) + (odd == 1 ? -2 : -3);
-            c[d] = base + k;
-            w = w * A.wp[odd][k];
+    } else {
+        if (l <= 0) {
+            atomicOr(A.err, 1u);
+            return;
         }
-        double v[5];
-        amr_sample(A, l - 1, c, v, depth);
+        int total = 1;
+        for (int i = 0; i < A.ndims; i++) total *= 6;
+        for (int s = 0; s < total; s++) {
+            double w = 1.0;
+            int64_t c[3] = {0, 0, 0};
+            int rem = s;
+            for (int i = 0; i < A.ndims; i++) {
+                const int d = A.dims[i];
+                const int k = rem % 6;
+                rem /= 6;
+                const int odd = (int)amr_erem(g[d], 2);
+                const int64_t base = amr_ediv(g[d], 2) + (odd == 1 ? -2 : -3);
+                c[d] = base + k;
+                w = w * A.wp[odd][k];
+            }
+            double v[5];
+            amr_sample_t<DEPTH - 1>(A, l - 1, c, v);
 #pragma unroll
-        for (int q = 0; q < 5; q++) out[q] = out[q] + w * v[q];
+            for (int q = 0; q < 5; q++) out[q] = out[q] + w * v[q];
+        }
     }
+}
+
+constexpr int AMR_PREDICT_DEPTH = 3;
+__device__ __forceinline__ void amr_sample(const AmrDev& A, int l, const int64_t* g, double* v, int) {
+    amr_sample_t<AMR_PREDICT_DEPTH>(A, l, g, v);
 }
 
 // ------------------------------------------------------------------ box pipelines

@@ -86,6 +86,22 @@ struct SweepParams {
     double* face;           // boundary face fluxes [slot][d][side][q][pencil]
     int npen;               // pencils per block face (padded)
     int pen_lane_major;     // pencil index = lane*no + other (lane axis is the lower of the two others)
+    // ---- batched independent 1-D lines (batch != 0): every lane is one
+    // segment of one instance with its own length, dx and dt
+    const struct BatchSeg* segs;
+    int nseg;
+    const double* inst_dx;
+    const double* inst_dt;  // 0: instance finished, its segments are skipped
+};
+
+// A segment of an instance line: `base` is the flat index of the cell five
+// rows before its first cell, `len` its cell count.
+struct BatchSeg {
+    int64_t base;
+    int len;
+    int inst;
+    int tail;  // the instance's last segment (owns the shared boundary midpoints/faces)
+    int pad;
 };
 
 // Flux modes (C/scheme.rs:39-47), a compile-time parameter of the sweep.
@@ -127,8 +143,12 @@ template <typename RF, int P, int MODE> struct SweepSmem {
     }
 };
 
-template <typename RF, int P, int D, int MODE, bool AMR = false>
+enum SweepKind { KIND_GRID = 0, KIND_AMR = 1, KIND_BATCH = 2 };
+
+template <typename RF, int P, int D, int MODE, int KIND = KIND_GRID>
 struct Sweep {
+    static constexpr bool AMR = KIND == KIND_AMR;
+    static constexpr bool BATCH = KIND == KIND_BATCH;
     using SM = SweepSmem<RF, P, MODE>;
     static constexpr int T = SWEEP_THREADS;
     static constexpr int RM = T / P;
@@ -331,7 +351,29 @@ struct Sweep {
         __shared__ int64_t s_loff[P];
         __shared__ int s_lok[P];
         __shared__ int s_pen[P];
-        if (tid < P) {
+        __shared__ int s_len[BATCH ? P : 1], s_tail[BATCH ? P : 1];
+        __shared__ double s_dt[BATCH ? P : 1], s_dx[BATCH ? P : 1];
+        __shared__ int s_maxlen;
+        if constexpr (BATCH) {
+            if (tid == 0) s_maxlen = 0;
+            __syncthreads();
+            if (tid < P) {
+                const int si = blockIdx.x * P + tid;
+                int len = 0;
+                if (si < p.nseg) {
+                    const BatchSeg sg = p.segs[si];
+                    const double dti = p.inst_dt[sg.inst];
+                    s_loff[tid] = sg.base;
+                    s_dt[tid] = dti;
+                    s_dx[tid] = p.inst_dx[sg.inst];
+                    s_tail[tid] = sg.tail;
+                    len = dti > 0.0 ? sg.len : 0;
+                }
+                s_len[tid] = len;
+                s_lok[tid] = len > 0;
+                atomicMax(&s_maxlen, len);
+            }
+        } else if (tid < P) {
             const int lw = AMR ? p.lw : P;
             const int la = lane0 + tid % lw, ob = ob0 + tid / lw;
             s_lok[tid] = la < p.nl && ob < p.no;
@@ -339,7 +381,7 @@ struct Sweep {
             if constexpr (AMR) s_pen[tid] = p.pen_lane_major ? la * p.no + ob : ob * p.nl + la;
         }
         // padded offset of row 0 (lane offsets are added per lane)
-        const int64_t base0 = blk + (int64_t)(p.gd + s0 - 5) * p.sd;
+        const int64_t base0 = BATCH ? 0 : blk + (int64_t)(p.gd + s0 - 5) * p.sd;
         // neighbouring segments recompute the 5 midpoints and 1 face they
         // share; only the owner counts them in the statistics
         const bool tail = s0 + Ls == p.nd;
@@ -351,8 +393,12 @@ struct Sweep {
         const bool lim_on = p.positivity && lam > 0.0;  // C/scheme.rs:278
         const double inv = 1.0 / dx;
         __syncthreads();  // lane table
-        const int nrounds = (Ls + 5 + RM - 1) / RM;
-        const int nrows = Ls + 10;
+        const int Lmax = BATCH ? s_maxlen : Ls;
+        const int nrounds = (Lmax + 5 + RM - 1) / RM;
+        const int nrows = Lmax + 10;
+        // per-lane length (batched lines differ), time step and cell size
+        auto lane_len = [&](int l) { return BATCH ? s_len[l] : Ls; };
+        auto lane_tail = [&](int l) { return BATCH ? s_tail[l] != 0 : tail; };
         double rate_max = 0.0;
 
         for (int r = 0; r < nrounds; r++) {
@@ -370,7 +416,7 @@ struct Sweep {
                         rr = idx / P;
                         l = idx % P;
                     }
-                    if (s_lok[l]) {
+                    if (s_lok[l] && lo + rr < lane_len(l) + 10) {
                         const int row = lo + rr;
                         const int64_t g = base0 + (int64_t)row * p.sd + s_loff[l];
                         double u[5], w[5];
@@ -396,7 +442,7 @@ struct Sweep {
                 // ---- Θ: blend weights of faces [RM r, RM r + RM) (C/scheme.rs:171-182)
                 const int f = RM * r + tid / P;
                 const int l = tid % P;
-                if (f <= Ls && s_lok[l]) {
+                if (s_lok[l] && f <= lane_len(l)) {
                     const int i = f + 4;
                     double rr = 0.0;
 #pragma unroll
@@ -417,12 +463,12 @@ struct Sweep {
                 // ---- B: midpoints [RM r, RM r + RM)
                 const int m = RM * r + tid / P;
                 const int l = tid % P;
-                if (m < Ls + 5 && s_lok[l]) {
+                if (s_lok[l] && m < lane_len(l) + 5) {
                     bool need = true;
                     if constexpr (MODE == MODE_HYBRID) {
                         // only midpoints of faces on the shock path (computed on demand, C/scheme.rs:233-238)
                         need = false;
-                        for (int ff = max(m - 4, 0); ff <= min(m, Ls); ff++) need = need || TH[slot(ff) * P + l] > 0.0;
+                        for (int ff = max(m - 4, 0); ff <= min(m, lane_len(l)); ff++) need = need || TH[slot(ff) * P + l] > 0.0;
                     }
                     if (need) {
                         RF f[5];
@@ -430,7 +476,7 @@ struct Sweep {
                         midpoint<SR>(ef, Wr, m, l, f, fb);
 #pragma unroll
                         for (int k = 0; k < 5; k++) MF[at<STR>(m, k, l)] = f[k];
-                        if (fb && (m < Ls || tail)) atomicAdd(&s_fallback, 1u);
+                        if (fb && (m < lane_len(l) || lane_tail(l))) atomicAdd(&s_fallback, 1u);
                     }
                 }
                 __syncthreads();
@@ -439,7 +485,7 @@ struct Sweep {
             {
                 const int fidx = RM * r - 4 + tid / P;
                 const int l = tid % P;
-                if (fidx >= 0 && fidx <= Ls && s_lok[l]) {
+                if (s_lok[l] && fidx >= 0 && fidx <= lane_len(l)) {
                     const int i = fidx + 4;
                     double theta = MODE == MODE_WENO ? 1.0 : 0.0;
                     if constexpr (MODE == MODE_HYBRID) theta = TH[slot(fidx) * P + l];
@@ -453,7 +499,7 @@ struct Sweep {
                     } else {
                         if constexpr (MID) {
                             if constexpr (MODE == MODE_HYBRID) {
-                                if (fidx < Ls || tail) atomicAdd(&s_weno, 1u);
+                                if (fidx < lane_len(l) || lane_tail(l)) atomicAdd(&s_weno, 1u);
                             }
                             // F̃ = Σ_s S6[s] (F̂_{+s} + F̂_{−s}), order as C/scheme.rs:230-246
 #pragma unroll
@@ -472,7 +518,14 @@ struct Sweep {
                             }
                         }
                     }
-                    if (lim_on) {
+                    double lam2_l = lam2;
+                    bool lim_l = lim_on;
+                    if constexpr (BATCH) {
+                        const double lm = (p.ndim * s_dt[l]) / s_dx[l];
+                        lam2_l = 2.0 * lm;
+                        lim_l = p.positivity && lm > 0.0;
+                    }
+                    if (lim_l) {
                         // Hu–Adams–Shu limiter (C/scheme.rs:395-464) between rows i and i+1
                         double wi[5], wj[5], ul[5], ur[5], flp[5], frp[5];
 #pragma unroll
@@ -487,7 +540,7 @@ struct Sweep {
                         bool finite = true;
 #pragma unroll
                         for (int k = 0; k < 5; k++) finite = finite && isfinite(fh[k]);
-                        if (!(finite && lim_ok(ed, fh, ul, flp, ur, frp, lam2))) {
+                        if (!(finite && lim_ok(ed, fh, ul, flp, ur, frp, lam2_l))) {
                             const double alpha = fmax(fabs(wi[un]) + sound_speed(ed, wi[0], wi[4]),
                                                       fabs(wj[un]) + sound_speed(ed, wj[0], wj[4]));
                             double flf[5], bl[5];
@@ -499,14 +552,14 @@ struct Sweep {
 #pragma unroll
                                 for (int k = 0; k < 5; k++)
                                     bl[k] = isfinite(fh[k]) ? mid * fh[k] + (1.0 - mid) * flf[k] : flf[k];
-                                if (lim_ok(ed, bl, ul, flp, ur, frp, lam2))
+                                if (lim_ok(ed, bl, ul, flp, ur, frp, lam2_l))
                                     lo = mid;
                                 else
                                     hi = mid;
                             }
 #pragma unroll
                             for (int k = 0; k < 5; k++) fh[k] = isfinite(fh[k]) ? lo * fh[k] + (1.0 - lo) * flf[k] : flf[k];
-                            if (fidx < Ls || tail) atomicAdd(&s_limited, 1u);
+                            if (fidx < lane_len(l) || lane_tail(l)) atomicAdd(&s_limited, 1u);
                         }
                     }
 #pragma unroll
@@ -531,14 +584,16 @@ struct Sweep {
                     c = RM * r - 5 + tid / P;
                     l = tid % P;
                 }
-                if (c >= 0 && c < Ls && s_lok[l]) {
+                if (s_lok[l] && c >= 0 && c < lane_len(l)) {
                     const int64_t g = base0 + (int64_t)(c + 5) * p.sd + s_loff[l];
+                    const double inv_l = BATCH ? 1.0 / s_dx[l] : inv;
+                    const double dt_l = BATCH ? s_dt[l] : dt;
                     double res[5];
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
                         // the block solver divides by dx (C/amr.rs:1263), the uniform one multiplies by 1/dx
                         const double df = F[at<STR>(c + 1, k, l)] - F[at<STR>(c, k, l)];
-                        const double x = AMR ? df / dx : df * inv;
+                        const double x = AMR ? df / dx : df * inv_l;
                         const double prev = p.first ? 0.0 : p.rhs[k * p.ncell + g];
                         res[k] = prev - x;
                     }
@@ -552,16 +607,16 @@ struct Sweep {
                             const double o = p.base[k * p.ncell + g];
                             double v;
                             if (p.stage == 1) {
-                                v = o + dt * res[k];
+                                v = o + dt_l * res[k];
                             } else if (p.stage == 2) {
-                                v = 0.75 * o + 0.25 * (p.cur[k * p.ncell + g] + dt * res[k]);
+                                v = 0.75 * o + 0.25 * (p.cur[k * p.ncell + g] + dt_l * res[k]);
                             } else {
-                                v = p.cur[k * p.ncell + g] / 3.0 + (2.0 / 3.0) * (o + dt * res[k]);
+                                v = p.cur[k * p.ncell + g] / 3.0 + (2.0 / 3.0) * (o + dt_l * res[k]);
                             }
                             p.dest[k * p.ncell + g] = v;
                             un_[k] = v;
                         }
-                        if (p.cfl_fuse) {
+                        if (!BATCH && p.cfl_fuse) {
                             // CFL rate Σ_d (|u_d| + c)/dx_d of the new state (C/solver.rs:485-497)
                             double w[5];
                             to_prim(ed, un_, w);
@@ -578,7 +633,7 @@ struct Sweep {
             // the next round's loads only touch W slots whose rows C has finished
             // with (barrier above), and its C writes F slots after two more barriers
         }
-        if (!AMR && p.cfl_fuse) {
+        if (!AMR && !BATCH && p.cfl_fuse) {
             double v = rate_max;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -589,7 +644,7 @@ struct Sweep {
             if (s_weno) atomicAdd(&p.ctl->counters[1], (unsigned long long)s_weno);
             if (s_fallback) atomicAdd(&p.ctl->counters[2], (unsigned long long)s_fallback);
             if (s_limited) atomicAdd(&p.ctl->counters[3], (unsigned long long)s_limited);
-            if (!AMR && p.cfl_fuse) {
+            if (!AMR && !BATCH && p.cfl_fuse) {
                 double v = s_rate[0];
                 for (int w = 1; w < T / 32; w++) v = fmax(v, s_rate[w]);
                 if (!isnan(v) && v > 0.0) atomicMax(&p.ctl->rate_bits, (unsigned long long)__double_as_longlong(v));

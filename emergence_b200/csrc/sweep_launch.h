@@ -11,6 +11,9 @@ cudaError_t sweep_launch_mixed(int P, int mode, const SweepParams& p, dim3 grid,
 // Batched block-AMR leaves (SweepParams::amr set), P = 16 or 32.
 cudaError_t sweep_launch_amr_f64(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 cudaError_t sweep_launch_amr_mixed(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
+// Batched independent 1-D lines (SweepParams::segs), 32 segments per CTA.
+cudaError_t sweep_launch_batch_f64(int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
+cudaError_t sweep_launch_batch_mixed(int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 // Opt the kernels into their dynamic shared memory size (once per device).
 cudaError_t sweep_prepare_f64();
 cudaError_t sweep_prepare_mixed();

@@ -4,14 +4,14 @@
 
 namespace emg {
 
-template <int P, int D, int MODE, bool AMR = false>
+template <int P, int D, int MODE, int KIND = KIND_GRID>
 __global__ void __launch_bounds__(SWEEP_THREADS, 2) sweep_mixed_kernel(const SweepParams p) {
-    Sweep<float, P, D, MODE, AMR>::run(p);
+    Sweep<float, P, D, MODE, KIND>::run(p);
 }
 
 // batched block-AMR leaves: P = 16 or 32 pencils, one block per lane set
 template <int P, int D, int MODE> static cudaError_t launch_amr(const SweepParams& p, dim3 grid, cudaStream_t s) {
-    sweep_mixed_kernel<P, D, MODE, true><<<grid, SWEEP_THREADS, SweepSmem<float, P, MODE>::bytes(), s>>>(p);
+    sweep_mixed_kernel<P, D, MODE, KIND_AMR><<<grid, SWEEP_THREADS, SweepSmem<float, P, MODE>::bytes(), s>>>(p);
     return cudaGetLastError();
 }
 template <int P, int MODE> static cudaError_t launch_amr_d(const SweepParams& p, dim3 grid, cudaStream_t s) {
@@ -63,9 +63,9 @@ template <int P, int MODE> static cudaError_t attr_d() {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_mixed_kernel<P, 1, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_mixed_kernel<P, 2, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     if constexpr (P >= 16) {
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_mixed_kernel<P, 0, MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_mixed_kernel<P, 1, MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_mixed_kernel<P, 2, MODE, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_mixed_kernel<P, 0, MODE, KIND_AMR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_mixed_kernel<P, 1, MODE, KIND_AMR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_mixed_kernel<P, 2, MODE, KIND_AMR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     }
     return e;
 }
@@ -77,10 +77,33 @@ template <int MODE> static cudaError_t attr_p() {
     return e;
 }
 
+// batched independent 1-D lines along axis 0, P = 32 segments per CTA
+template <int MODE> static cudaError_t launch_batch(const SweepParams& p, dim3 grid, cudaStream_t s) {
+    sweep_mixed_kernel<32, 0, MODE, KIND_BATCH><<<grid, SWEEP_THREADS, SweepSmem<float, 32, MODE>::bytes(), s>>>(p);
+    return cudaGetLastError();
+}
+cudaError_t sweep_launch_batch_mixed(int mode, const SweepParams& p, dim3 grid, cudaStream_t s) {
+    switch (mode) {
+        case MODE_WENO: return launch_batch<MODE_WENO>(p, grid, s);
+        case MODE_HYBRID: return launch_batch<MODE_HYBRID>(p, grid, s);
+        case MODE_CENTRAL: return launch_batch<MODE_CENTRAL>(p, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t sweep_prepare_mixed() {
     cudaError_t e = attr_p<MODE_WENO>();
     if (e == cudaSuccess) e = attr_p<MODE_HYBRID>();
     if (e == cudaSuccess) e = attr_p<MODE_CENTRAL>();
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(sweep_mixed_kernel<32, 0, MODE_WENO, KIND_BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SweepSmem<float, 32, MODE_WENO>::bytes());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(sweep_mixed_kernel<32, 0, MODE_HYBRID, KIND_BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SweepSmem<float, 32, MODE_HYBRID>::bytes());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(sweep_mixed_kernel<32, 0, MODE_CENTRAL, KIND_BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SweepSmem<float, 32, MODE_CENTRAL>::bytes());
     return e;
 }
 

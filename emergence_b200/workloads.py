@@ -149,3 +149,27 @@ def amr_explosion(dim=2, base=4, b=16, levels=3, eps=1e-3, regrid_every=4, radiu
 
     bc = [[Bc.Outflow, Bc.Outflow] for _ in range(3)]
     return sys_, cfg, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), bc, init
+
+
+# ---------------------------------------------------------------- batched 1-D Riemann problems
+def riemann_batch(ninst=4096, nmin=64, nmax=2048, seed=SEED, gamma=1.4, x0=0.5):
+    """Independent 1-D Riemann problems on [0,1]: cells log-uniform in
+    [nmin, nmax], left/right states ρ ∈ U[0.1,2], u ∈ U[−1,1], p ∈ U[0.1,2],
+    interface at x0. Returns (sys, n, dx, u, states) with u the concatenated
+    interior conserved data and states[i] = (ρL, uL, pL, ρR, uR, pR)."""
+    from .physics import Euler, Nasg
+    sys_ = Euler(Nasg.ideal(gamma))
+    rng = np.random.default_rng(seed)
+    n = np.floor(np.exp(rng.uniform(np.log(nmin), np.log(nmax + 1), ninst))).astype(np.int64).clip(nmin, nmax)
+    st = np.stack([rng.uniform(0.1, 2.0, ninst), rng.uniform(-1.0, 1.0, ninst), rng.uniform(0.1, 2.0, ninst),
+                   rng.uniform(0.1, 2.0, ninst), rng.uniform(-1.0, 1.0, ninst), rng.uniform(0.1, 2.0, ninst)], axis=1)
+    parts = []
+    for i in range(ninst):
+        x = (np.arange(n[i]) + 0.5) / n[i]
+        left = x < x0
+        w = np.zeros((n[i], 5))
+        w[:, 0] = np.where(left, st[i, 0], st[i, 3])
+        w[:, 1] = np.where(left, st[i, 1], st[i, 4])
+        w[:, 4] = np.where(left, st[i, 2], st[i, 5])
+        parts.append(sys_.to_cons(w))
+    return sys_, n, 1.0 / n.astype(np.float64), np.concatenate(parts), st

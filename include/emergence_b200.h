@@ -211,6 +211,37 @@ int emg_uniform_launch_count(emg_uniform* h, uint64_t* launches);
 int emg_uniform_step_noalloc(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
                              const double* u_in, double* u_out, double dt, void* stream);
 
+/* ------------------------------------------------------------------ batched 1-D lines */
+/* Many independent 1-D problems advanced together: every RK stage is one
+ * fused-sweep launch over all instances, each instance with its own cell size
+ * and its own CFL time step. No counterpart in the reference, which solves one
+ * Solver at a time (each instance here follows Solver::run_to,
+ * C/solver.rs:758-768, on a 1-D mesh). */
+typedef struct emg_batch1d emg_batch1d;
+
+/* ninst instances; instance i has n[i] cells of size dx[i] and interior
+ * conserved data u[(off_i + c)*5 + q] with off_i = Σ_{j<i} n[j]. The two
+ * boundary conditions (low, high) are shared by all instances (periodic,
+ * outflow, reflect or Dirichlet). ng = 6 ghost layers are added internally. */
+int emg_batch1d_create(const emg_eos* eos, const emg_opts* opts, const emg_bc bc[2], size_t ninst, const int64_t* n,
+                       const double* dx, const double* u, emg_batch1d** out);
+int emg_batch1d_destroy(emg_batch1d* h);
+
+/* Advance every instance to t_end with its own CFL steps (stopping rule and
+ * collapse check of Solver::run_to). Steps run without host round trips;
+ * *launched receives the number of batch steps issued (the step count of the
+ * slowest instance). */
+int emg_batch1d_run_to(emg_batch1d* h, double t_end, uint64_t* launched);
+
+/* Interior conserved data of all instances (same layout as create). */
+int emg_batch1d_download(emg_batch1d* h, double* u);
+
+/* Per-instance time and step count. */
+int emg_batch1d_status(emg_batch1d* h, double* t, uint64_t* steps);
+
+/* The handle's CUDA stream (cudaStream_t) as an opaque pointer. */
+int emg_batch1d_stream(emg_batch1d* h, void** stream);
+
 /* ------------------------------------------------------------------ block AMR */
 
 /* Block-AMR configuration (C/amr.rs:49-63). Blocks are b cells per active
