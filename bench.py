@@ -214,6 +214,13 @@ def run_ours(args, world, rank, local):
     except Exception:
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
+    traffic = None
+    try:  # DRAM bytes per cell and launch of the FP64 sweep from the committed ncu capture
+        tr = json.load(open(os.path.join(ROOT, "profiles", "sweep_traffic.json")))
+        if prec == Precision.F64:
+            traffic = tr["bytes_per_cell_per_launch"] * cells
+    except Exception:
+        pass
     u_main = g.download() if not args.no_mixed else None
     g.close()
 
@@ -278,7 +285,7 @@ def run_ours(args, world, rank, local):
                        "parallelism": f"{world} independent replica(s), one GPU each",
                        "l2": "inputs larger than L2 (state 0.77 GB per array)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "kernel": "fused sweep (3 per stage)",
+                         "traffic": traffic, "traffic_source": "ncu capture on 160^3 scaled by cells (profiles/)", "kernel": "fused sweep (3 per stage)",
                          "alg_bytes_per_launch": alg_bytes_per_launch, "avg_launch_ms": per_launch_ms,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"},
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()},
