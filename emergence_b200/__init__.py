@@ -9,7 +9,8 @@ from .physics import Bc, Euler, FluxMode, Mesh, Nasg, Precision, initial_state
 from .solver import GpuSolver, device_count
 from .amr import GpuAmr
 from .batch import GpuBatch1D
+from .adjoint import DifferentiableSolver
 from ._abi import EmgError, LIB_PATH
 
-__all__ = ["Bc", "Euler", "FluxMode", "Mesh", "Nasg", "Precision", "initial_state", "GpuSolver", "GpuAmr", "GpuBatch1D", "device_count",
+__all__ = ["Bc", "Euler", "FluxMode", "Mesh", "Nasg", "Precision", "initial_state", "GpuSolver", "GpuAmr", "GpuBatch1D", "DifferentiableSolver", "device_count",
            "EmgError", "LIB_PATH"]

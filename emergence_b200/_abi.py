@@ -107,6 +107,20 @@ SIGNATURES = {
     "emg_amr_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "emg_amr_phase_times": (C.c_int, [_P, _D]),
     "emg_amr_launch_count": (C.c_int, [_P, _U64]),
+    "emg_adjoint_create": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc), C.POINTER(EmgOpts), _D,
+                                     C.c_size_t, C.POINTER(_P)]),
+    "emg_adjoint_destroy": (C.c_int, [_P]),
+    "emg_adjoint_set_initial": (C.c_int, [_P, _D, C.c_size_t]),
+    "emg_adjoint_forward": (C.c_int, [_P, C.c_uint64, C.c_double, C.c_uint64, _U64]),
+    "emg_adjoint_forward_dts": (C.c_int, [_P, _D, C.c_uint64, C.c_uint64]),
+    "emg_adjoint_dts": (C.c_int, [_P, _D, C.c_size_t, _U64]),
+    "emg_adjoint_download": (C.c_int, [_P, _D, C.c_size_t]),
+    "emg_adjoint_objective": (C.c_int, [_P, C.c_int, _D, _D, _D]),
+    "emg_adjoint_seed": (C.c_int, [_P, _D, C.c_size_t]),
+    "emg_adjoint_backward": (C.c_int, [_P, _D, _D, _D]),
+    "emg_adjoint_step_vjp": (C.c_int, [_P, _D, C.c_size_t, C.c_double, _D, _D, _D]),
+    "emg_adjoint_times": (C.c_int, [_P, _D]),
+    "emg_adjoint_stream": (C.c_int, [_P, C.POINTER(_P)]),
 }
 
 _lib = None

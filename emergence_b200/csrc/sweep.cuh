@@ -92,6 +92,10 @@ struct SweepParams {
     int nseg;
     const double* inst_dx;
     const double* inst_dt;  // 0: instance finished, its segments are skipped
+    // optional (uniform grids and batched lines): the limiter's blend weight θ
+    // of every face, stored at the index of the face's left cell (1 where the
+    // high-order flux was kept); read back by the discrete adjoint
+    double* theta_rec;
 };
 
 // A segment of an instance line: `base` is the flat index of the cell five
@@ -525,6 +529,7 @@ struct Sweep {
                         lam2_l = 2.0 * lm;
                         lim_l = p.positivity && lm > 0.0;
                     }
+                    double th_rec = 1.0;  // blend weight kept by the limiter (1: untouched)
                     if (lim_l) {
                         // Hu–Adams–Shu limiter (C/scheme.rs:395-464) between rows i and i+1
                         double wi[5], wj[5], ul[5], ur[5], flp[5], frp[5];
@@ -560,10 +565,15 @@ struct Sweep {
 #pragma unroll
                             for (int k = 0; k < 5; k++) fh[k] = isfinite(fh[k]) ? lo * fh[k] + (1.0 - lo) * flf[k] : flf[k];
                             if (fidx < lane_len(l) || lane_tail(l)) atomicAdd(&s_limited, 1u);
+                            th_rec = lo;
                         }
                     }
 #pragma unroll
                     for (int k = 0; k < 5; k++) F[at<STR>(fidx, k, l)] = fh[k];
+                    if (!AMR && p.theta_rec) {
+                        // recorded for the discrete adjoint, at the face's left cell
+                        p.theta_rec[base0 + (int64_t)i * p.sd + s_loff[l]] = th_rec;
+                    }
                     if (AMR && (fidx == 0 || fidx == Ls)) {
                         // block boundary faces for refluxing (C/amr.rs:1291-1295)
                         const int side = fidx == 0 ? 0 : 1;

@@ -12,8 +12,7 @@
 //
 // Built with -fmad=false: the ghost, CFL and control arithmetic must round as
 // the reference CPU solver does.
-#include "../../include/emergence_b200.h"
-#include "sweep_launch.h"
+#include "uniform_internal.h"
 
 #include <cmath>
 #include <cstdio>
@@ -29,13 +28,6 @@ int set_error(int code, const std::string& msg) {
     g_last_error = msg;
     return code;
 }
-
-#define EMG_CUDA(call)                                                                                 \
-    do {                                                                                               \
-        cudaError_t _e = (call);                                                                       \
-        if (_e != cudaSuccess)                                                                         \
-            return set_error(EMG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e));      \
-    } while (0)
 
 // ------------------------------------------------------------------ auxiliary kernels
 
@@ -227,16 +219,6 @@ __global__ void ghost_kernel(const GhostParams p) {
     }
 }
 
-struct CellRange {
-    int64_t n[3], g[3], stride[3];
-    int64_t cells;
-    __device__ int64_t index(int64_t t) const {
-        const int64_t k = t % n[2];
-        const int64_t j = (t / n[2]) % n[1];
-        const int64_t i = t / (n[1] * n[2]);
-        return (i + g[0]) * stride[0] + (j + g[1]) * stride[1] + (k + g[2]) * stride[2];
-    }
-};
 
 // CFL rate max over interior cells of Σ_d (|u_d| + c)/dx_d (C/solver.rs:478-516).
 __global__ void cfl_kernel(const double* __restrict__ u, int64_t ncell, CellRange cr, int a0, int a1, int a2, double dx0,
@@ -360,48 +342,9 @@ __global__ void totals_final(const double* partial, int nblocks, double* out) {
 
 using namespace emg;
 
-// ------------------------------------------------------------------ solver object
+// ------------------------------------------------------------------ solver object (uniform_internal.h)
 
-struct emg_uniform {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    emg_mesh mesh{};
-    emg_eos eos{};
-    emg_bc bc[6]{};
-    emg_opts opts{};
-    int64_t m[3]{}, stride[3]{}, ncell = 0, cells = 0;
-    int active[3]{};
-    int ndim = 0;
-    bool deep = false;
-    double* u = nullptr;
-    double* sa = nullptr;
-    double* sb = nullptr;
-    double* rhs = nullptr;
-    double* staging = nullptr;
-    double* partial = nullptr;
-    StepCtl* ctl = nullptr;
-    StepCtl* ctl_host = nullptr;  // pinned mirror
-    bool rate_valid = false;
-    double t_host = 0.0;          // mirror of ctl->t when the device is idle
-    uint64_t faces = 0, weno_faces = 0;  // host-side face counts
-    uint64_t launches = 0;
-    // profiling
-    bool profiling = false;
-    struct Rec {
-        int kind;
-        cudaEvent_t a, b;
-    };
-    std::vector<Rec> recs;
-    std::vector<cudaEvent_t> pool;
-    double prof_ms[EMG_K_COUNT]{};
-    uint64_t prof_n[EMG_K_COUNT]{};
-    // sweep shapes per axis
-    int sweepP[3]{}, sweepSeg[3]{};
-    dim3 sweepGrid[3];
-    int lane_axis[3]{}, other_axis[3]{};
-};
-
-namespace {
+namespace emg {
 
 int kernel_grid(int64_t work, int threads) {
     int64_t b = (work + threads - 1) / threads;
@@ -563,6 +506,7 @@ int launch_stage(emg_uniform* h, int stage) {
         }
         ProfScope ps(h, EMG_K_AXIS_0 + d);
         p.tol = h->opts.tol;
+        p.theta_rec = h->theta_rec[stage - 1][d];
         cudaError_t e = h->opts.precision == EMG_PRECISION_MIXED
                             ? sweep_launch_mixed(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream)
                             : sweep_launch_f64(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream);
@@ -632,7 +576,7 @@ int check_handle(emg_uniform* h) {
     return EMG_OK;
 }
 
-}  // namespace
+}  // namespace emg
 
 extern "C" {
 

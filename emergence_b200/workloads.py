@@ -34,6 +34,13 @@ def explosion(n, radius, seed=SEED, gamma=1.4, noise=0.01, ng=6):
     """Circular/spherical explosion on [0,1]^D: ρ = 1, p = 1 for r < radius
     about the centre, ρ = 0.125, p = 0.1 outside, u = 0, with ρ ← ρ(1 + noise·ξ).
     Returns (sys, mesh, u_padded, bc) with transmissive (Outflow) boundaries."""
+    sys, mesh, w, bc = explosion_prim(n, radius, seed, gamma, noise, ng)
+    return sys, mesh, initial_state(sys, mesh, w), bc
+
+
+def explosion_prim(n, radius, seed=SEED, gamma=1.4, noise=0.01, ng=6):
+    """The explosion of ``explosion`` as interior primitives: (sys, mesh, w, bc)
+    with w of shape n + (5,)."""
     n = tuple(list(n) + [1] * (3 - len(n)))
     sys = Euler(Nasg.ideal(gamma))
     lo = (0.0, 0.0, 0.0)
@@ -50,9 +57,8 @@ def explosion(n, radius, seed=SEED, gamma=1.4, noise=0.01, ng=6):
     w = np.zeros(n + (5,))
     w[..., 0] = np.where(inside, 1.0, 0.125) * (1.0 + noise * xi)
     w[..., 4] = np.where(inside, 1.0, 0.1)
-    u = initial_state(sys, mesh, w)
     bc = [[Bc.Outflow, Bc.Outflow] for _ in range(3)]
-    return sys, mesh, u, bc
+    return sys, mesh, w, bc
 
 
 def explosion_2d(n=256, seed=SEED):

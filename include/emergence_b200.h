@@ -324,6 +324,76 @@ int emg_amr_phase_times(emg_amr* h, double out[5]);
 /* Kernel launches issued by the handle since creation. */
 int emg_amr_launch_count(emg_amr* h, uint64_t* launches);
 
+/* ------------------------------------------------------------------ discrete adjoint
+ * Reverse-mode derivative of the uniform-grid FP64 step (WENO flux mode):
+ * SSP-RK3, the WCNS/HLLC/positivity-limited flux divergence and the ghost
+ * fill, with √N checkpointing of the forward run. No counterpart in the
+ * reference, which only runs forward (its Solver::step, C/solver.rs:659-738,
+ * is the map differentiated here). The recorded run's time steps, the
+ * positivity limiter's blend weights and the admissibility fallbacks are held
+ * fixed: the result is the gradient of the discrete map the forward run
+ * applied. Host arrays use the AoS padded layout of emg_uniform_create. */
+typedef struct emg_adjoint emg_adjoint;
+
+/* Box objectives over interior cells whose centre lo + (i+½)dx lies in
+ * [box_lo, box_hi] on every active axis. */
+enum emg_objective {
+    EMG_OBJ_PRESSURE = 0, /* J = Σ p·vol */
+    EMG_OBJ_ENERGY = 1    /* J = Σ E·vol */
+};
+
+/* Differentiable solver from an initial conserved state (opts: FP64, WENO
+ * mode; boundaries periodic, outflow, reflect or Dirichlet; n ≥ ng on every
+ * active axis). */
+int emg_adjoint_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
+                       const double* u_aos, size_t len, emg_adjoint** out);
+int emg_adjoint_destroy(emg_adjoint* h);
+
+/* Replace the initial state (drops a recorded run). */
+int emg_adjoint_set_initial(emg_adjoint* h, const double* u_aos, size_t len);
+
+/* Record a forward run from the initial state: up to nsteps steps with the
+ * CFL time step (as Solver::run_to, stopping at t_end; +inf for a fixed step
+ * count), keeping the state every `checkpoint_every` steps (0: ⌈√nsteps⌉).
+ * *taken receives the steps run. */
+int emg_adjoint_forward(emg_adjoint* h, uint64_t nsteps, double t_end, uint64_t checkpoint_every, uint64_t* taken);
+
+/* Record a forward run with the given time steps (frozen-dt runs, e.g. for
+ * finite-difference checks). */
+int emg_adjoint_forward_dts(emg_adjoint* h, const double* dts, uint64_t nsteps, uint64_t checkpoint_every);
+
+/* Time steps of the recorded run (`cap` entries of room; out may be NULL to
+ * query the count). */
+int emg_adjoint_dts(emg_adjoint* h, double* out, size_t cap, uint64_t* nsteps);
+
+/* Final state of the recorded run (the initial state if none). */
+int emg_adjoint_download(emg_adjoint* h, double* u_aos, size_t len);
+
+/* J of the recorded run's final state; seeds the backward pass with ∂J/∂U
+ * and the direct ∂J/∂γ. */
+int emg_adjoint_objective(emg_adjoint* h, int kind, const double box_lo[3], const double box_hi[3], double* J);
+
+/* Seed the backward pass with a caller cotangent of the final conserved state. */
+int emg_adjoint_seed(emg_adjoint* h, const double* ubar_aos, size_t len);
+
+/* Backward pass (recomputing each checkpoint segment). Outputs, each optional:
+ * ubar0 = ∂J/∂U⁰ (conserved initial state), wbar0 = ∂J/∂W⁰ (primitive initial
+ * state, through U⁰ = to_cons(W⁰)), gamma_bar = [∂J/∂γ with U⁰ fixed, with W⁰
+ * fixed]. Ghost entries of the arrays are zero. */
+int emg_adjoint_backward(emg_adjoint* h, double* ubar0_aos, double* wbar0_aos, double gamma_bar[2]);
+
+/* One step's vector–Jacobian product: for U' = step(U, dt), ubar = (∂U'/∂U)ᵀ·ubar_next
+ * and *gamma_bar = (∂U'/∂γ)ᵀ·ubar_next. The differentiable-step primitive. */
+int emg_adjoint_step_vjp(emg_adjoint* h, const double* u_aos, size_t len, double dt, const double* ubar_next_aos,
+                         double* ubar_aos, double* gamma_bar);
+
+/* Device milliseconds of the last forward run, and of the last backward pass
+ * split into checkpoint recompute and reverse sweeps. */
+int emg_adjoint_times(emg_adjoint* h, double ms[3]);
+
+/* The handle's CUDA stream (cudaStream_t) as an opaque pointer. */
+int emg_adjoint_stream(emg_adjoint* h, void** stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,6 +6,7 @@
 // Loaded only by tests/, __graft_entry__.smoke() and bench.py's CPU leg.
 #include "oracle.hpp"
 #include "amr_oracle.hpp"
+#include "dual.hpp"
 #include "../include/emergence_b200.h"
 
 #include <cstdio>
@@ -386,4 +387,118 @@ int emgo_amr_details(void* h, double* out, size_t cap) {
     return EMG_OK;
 }
 
+}  // extern "C"
+
+// ---- forward-mode derivative of a frozen-dt run (dual-number instantiation)
+
+namespace {
+// Objective over the interior cells whose centre lo + (i+½)dx lies in
+// [box_lo, box_hi] on every active axis: kind 0 = Σ p·vol, kind 1 = Σ E·vol.
+template <class T>
+T box_objective(const Solver<T>& s, int kind, const double* box_lo, const double* box_hi) {
+    const Mesh& m = s.mesh;
+    T vol = T(1.0);
+    for (int d = 0; d < 3; d++)
+        if (m.active(d)) vol = vol * T(m.dx[d]);
+    T acc = T(0.0);
+    for (int64_t i = 0; i < m.n[0]; i++)
+        for (int64_t j = 0; j < m.n[1]; j++)
+            for (int64_t k = 0; k < m.n[2]; k++) {
+                const int64_t ijk[3] = {i, j, k};
+                bool in = true;
+                for (int d = 0; d < 3; d++) {
+                    if (!m.active(d)) continue;
+                    const double x = m.lo[d] + ((double)ijk[d] + 0.5) * m.dx[d];
+                    in = in && x >= box_lo[d] && x <= box_hi[d];
+                }
+                if (!in) continue;
+                const V5<T>& u = s.u[m.idx(i + m.g(0), j + m.g(1), k + m.g(2))];
+                T v = kind == 0 ? s.sys.to_prim(u)[4] : u[4];
+                acc = acc + v * vol;
+            }
+    return acc;
+}
+}  // namespace
+
+extern "C" {
+
+// Runs `nsteps` SSP-RK3 steps with the given time steps from the initial
+// primitive state w0 (padded AoS, ghosts ignored) in dual numbers, with the
+// tangent dw0 on the initial primitives and dgamma on γ; returns the box
+// objective J and its directional derivative dJ. Optional u_out / du_out
+// receive the final conserved state and its tangent (padded AoS).
+int emgo_dual_run(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
+                  const double* w0, const double* dw0, size_t len, double dgamma, const double* dts, size_t nsteps,
+                  int objective, const double box_lo[3], const double box_hi[3], double* J, double* dJ,
+                  double* u_out, double* du_out) {
+    if (!mesh || !eos || !bc || !opts || !w0 || !dw0 || (nsteps && !dts) || !J || !dJ)
+        return fail(EMG_ERR_INVALID, "null argument");
+    Mesh m = to_mesh(mesh);
+    if ((size_t)m.len() != len) return fail(EMG_ERR_INVALID, "state length does not match the padded mesh");
+    Euler<Dual> sys{Nasg<Dual>{Dual(eos->gamma, dgamma), Dual(eos->p_inf), Dual(eos->b), Dual(eos->q), Dual(eos->cv)}};
+    Solver<Dual> s(sys, m);
+    for (int d = 0; d < 3; d++)
+        for (int q = 0; q < 2; q++) {
+            s.bc[d][q].kind = bc[2 * d + q].kind;
+            for (int k = 0; k < 5; k++) s.bc[d][q].state[k] = Dual(bc[2 * d + q].state[k]);
+        }
+    s.cfl = opts->cfl;
+    s.tol = opts->tol;
+    s.mode = opts->mode;
+    s.positivity = opts->positivity != 0;
+    for (size_t c = 0; c < len; c++) {
+        V5<Dual> w;
+        for (int k = 0; k < 5; k++) w[k] = Dual(w0[5 * c + k], dw0[5 * c + k]);
+        s.u[c] = sys.to_cons(w);
+    }
+    for (size_t n = 0; n < nsteps; n++) s.step(dts[n]);
+    Dual j = box_objective(s, objective, box_lo, box_hi);
+    *J = j.v;
+    *dJ = j.d;
+    if (u_out)
+        for (size_t c = 0; c < len; c++)
+            for (int k = 0; k < 5; k++) u_out[5 * c + k] = s.u[c][k].v;
+    if (du_out)
+        for (size_t c = 0; c < len; c++)
+            for (int k = 0; k < 5; k++) du_out[5 * c + k] = s.u[c][k].d;
+    return EMG_OK;
+}
+
+// The same objective of a plain f64 state held by a uniform oracle handle.
+int emgo_box_objective(void* h, int objective, const double box_lo[3], const double box_hi[3], double* J) {
+    Handle* hh = (Handle*)h;
+    *J = box_objective(hh->s, objective, box_lo, box_hi);
+    return EMG_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+// One SSP-RK3 step of size dt in dual numbers from the padded conserved state
+// u with tangent du (and dgamma on γ); writes the new state and its tangent.
+int emgo_dual_step_cons(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
+                        const double* u, const double* du, size_t len, double dgamma, double dt, double* u_out,
+                        double* du_out) {
+    Mesh m = to_mesh(mesh);
+    if ((size_t)m.len() != len) return fail(EMG_ERR_INVALID, "state length does not match the padded mesh");
+    Euler<Dual> sys{Nasg<Dual>{Dual(eos->gamma, dgamma), Dual(eos->p_inf), Dual(eos->b), Dual(eos->q), Dual(eos->cv)}};
+    Solver<Dual> s(sys, m);
+    for (int d = 0; d < 3; d++)
+        for (int q = 0; q < 2; q++) {
+            s.bc[d][q].kind = bc[2 * d + q].kind;
+            for (int k = 0; k < 5; k++) s.bc[d][q].state[k] = Dual(bc[2 * d + q].state[k]);
+        }
+    s.tol = opts->tol;
+    s.mode = opts->mode;
+    s.positivity = opts->positivity != 0;
+    for (size_t c = 0; c < len; c++)
+        for (int k = 0; k < 5; k++) s.u[c][k] = Dual(u[5 * c + k], du[5 * c + k]);
+    s.step(dt);
+    for (size_t c = 0; c < len; c++)
+        for (int k = 0; k < 5; k++) {
+            u_out[5 * c + k] = s.u[c][k].v;
+            du_out[5 * c + k] = s.u[c][k].d;
+        }
+    return EMG_OK;
+}
 }  // extern "C"

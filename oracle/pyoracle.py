@@ -56,6 +56,11 @@ SIGS = {
     "emgo_characteristic_ghost_layer": (C.c_int, [C.POINTER(EmgEos), _D, _D, _D, C.c_int, C.c_int, C.c_double, _D]),
     "emgo_exact_star": (C.c_int, [_D, _D, C.POINTER(EmgEos), C.POINTER(EmgEos), _D]),
     "emgo_exact_sample": (C.c_int, [_D, _D, C.POINTER(EmgEos), C.POINTER(EmgEos), _D, C.c_size_t, _D]),
+    "emgo_dual_run": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc), C.POINTER(EmgOpts), _D, _D,
+                                C.c_size_t, C.c_double, _D, C.c_size_t, C.c_int, _D, _D, _D, _D, _D, _D]),
+    "emgo_box_objective": (C.c_int, [_P, C.c_int, _D, _D, _D]),
+    "emgo_dual_step_cons": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc), C.POINTER(EmgOpts), _D,
+                                      _D, C.c_size_t, C.c_double, C.c_double, _D, _D]),
 }
 
 _lib = None
@@ -207,6 +212,54 @@ class OracleSolver:
 
 
 # ---- unit-level helpers
+
+OBJ_PRESSURE, OBJ_ENERGY = 0, 1
+
+
+def dual_run(sys, mesh, w0, dw0, dgamma, dts, objective, box_lo, box_hi, bc, mode=FluxMode.Weno, positivity=True,
+             tol=1e-3, want_state=False):
+    """Forward-mode derivative of a frozen-dt run on the CPU: starts from the
+    padded primitive state ``w0`` with tangent ``dw0`` (and ``dgamma`` on γ),
+    takes one SSP-RK3 step per entry of ``dts`` and returns (J, dJ) of the box
+    objective (OBJ_PRESSURE: Σ p·vol, OBJ_ENERGY: Σ E·vol over interior cells
+    whose centre lies in [box_lo, box_hi]); with want_state also the final
+    conserved state and its tangent (padded AoS)."""
+    from emergence_b200.solver import _c_bcs, _c_mesh
+    w0, dw0 = arr(w0).reshape(-1, 5), arr(dw0).reshape(-1, 5)
+    dts = arr(dts).reshape(-1)
+    m, e, b = _c_mesh(mesh), c_eos(sys.eos), _c_bcs(bc)
+    o = EmgOpts(0.5, tol, mode, 1 if positivity else 0, 0, 0)
+    J, dJ = C.c_double(), C.c_double()
+    blo, bhi = arr(box_lo), arr(box_hi)
+    uo = np.zeros_like(w0) if want_state else None
+    duo = np.zeros_like(w0) if want_state else None
+    _chk(lib().emgo_dual_run(C.byref(m), C.byref(e), b, C.byref(o), dptr(w0), dptr(dw0), w0.shape[0], float(dgamma),
+                             dptr(dts), dts.shape[0], int(objective), dptr(blo), dptr(bhi), C.byref(J), C.byref(dJ),
+                             dptr(uo) if want_state else None, dptr(duo) if want_state else None))
+    if want_state:
+        return J.value, dJ.value, uo, duo
+    return J.value, dJ.value
+
+
+def dual_step(sys, mesh, u, du, dgamma, dt, bc, mode=FluxMode.Weno, positivity=True, tol=1e-3):
+    """One SSP-RK3 step of size dt in dual numbers from the padded conserved
+    state u with tangent du (dgamma on γ): returns (u', du')."""
+    from emergence_b200.solver import _c_bcs, _c_mesh
+    u, du = arr(u).reshape(-1, 5), arr(du).reshape(-1, 5)
+    m, e, b = _c_mesh(mesh), c_eos(sys.eos), _c_bcs(bc)
+    o = EmgOpts(0.5, tol, mode, 1 if positivity else 0, 0, 0)
+    u1, du1 = np.zeros_like(u), np.zeros_like(u)
+    _chk(lib().emgo_dual_step_cons(C.byref(m), C.byref(e), b, C.byref(o), dptr(u), dptr(du), u.shape[0],
+                                   float(dgamma), float(dt), dptr(u1), dptr(du1)))
+    return u1, du1
+
+
+def box_objective(solver, objective, box_lo, box_hi):
+    """The box objective of an OracleSolver's current state."""
+    J = C.c_double()
+    _chk(lib().emgo_box_objective(solver._h, int(objective), dptr(arr(box_lo)), dptr(arr(box_hi)), C.byref(J)))
+    return J.value
+
 
 def line_fluxes(eos, w, d, ng, mode, tol=1e-3, lam=0.0):
     w = arr(w)
