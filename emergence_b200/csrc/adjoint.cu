@@ -38,6 +38,9 @@ constexpr int ADJ_P = 4;                   // pencils per CTA
 constexpr int ADJ_L = ADJ_T / ADJ_P - 5;   // owned rows per pencil (one midpoint per thread: L + 5 = 64)
 constexpr int ADJ_ROWS = ADJ_L + 10;       // staged rows per pencil
 constexpr int ADJ_FACES = ADJ_L + 9;       // faces whose cotangents a CTA forms
+// 2 CTAs per SM (128 registers, some spills) measured 10 % faster than 1 CTA
+// per SM without spills on the 2-D explosion 512^2
+constexpr int ADJ_MINB = 2;
 
 struct AdjSweepParams {
     const double* __restrict__ u;      // stage input X_s, ghost-filled, SoA with field stride ncell
@@ -55,14 +58,34 @@ struct AdjSweepParams {
     EosD eos;
 };
 
+// Shared-memory layout of the adjoint sweep (dynamic, ≈94 KB): primitives and
+// their cotangents of ADJ_ROWS rows, face-flux cotangents of ADJ_FACES faces
+// (all [row][field][pencil]), and one 30-value slot per thread for the
+// stencil cotangents of its midpoint ([s·5 + k][thread]).
+constexpr size_t ADJ_SMEM = (size_t)(2 * ADJ_ROWS * 5 * ADJ_P + ADJ_FACES * 5 * ADJ_P + 30 * ADJ_T) * sizeof(double);
+
+struct SmemRows {
+    const double* W;
+    int row0, l;
+    __device__ __forceinline__ double operator()(int s, int k) const { return W[((row0 + s) * 5 + k) * ADJ_P + l]; }
+};
+struct SlotAcc {
+    double* slot;
+    int t;
+    __device__ __forceinline__ void add(int s, int k, double v) const { slot[(s * 5 + k) * ADJ_T + t] += v; }
+};
+
 // Reverse of one axis' contribution −(F_{i+½} − F_{i−½})/dx to the stage
 // residual (the forward sweep of sweep.cuh, FP64, WENO flux mode).
 template <int D>
-__global__ void __launch_bounds__(ADJ_T) adj_sweep_kernel(const AdjSweepParams p) {
-    __shared__ double W[ADJ_ROWS][5][ADJ_P];   // primitives
-    __shared__ double AW[ADJ_ROWS][5][ADJ_P];  // primitive cotangents
-    __shared__ double AF[ADJ_FACES][5][ADJ_P]; // cotangents of the high-order face fluxes F̃
+__global__ void __launch_bounds__(ADJ_T, ADJ_MINB) adj_sweep_kernel(const AdjSweepParams p) {
+    extern __shared__ __align__(16) double adj_smem[];
+    double* W = adj_smem;                             // [ADJ_ROWS][5][ADJ_P] primitives
+    double* AW = W + ADJ_ROWS * 5 * ADJ_P;            // [ADJ_ROWS][5][ADJ_P] primitive cotangents
+    double* AF = AW + ADJ_ROWS * 5 * ADJ_P;           // [ADJ_FACES][5][ADJ_P] cotangents of F̃
+    double* SLOT = AF + ADJ_FACES * 5 * ADJ_P;        // [30][ADJ_T] midpoint stencil cotangents
     __shared__ double s_g[ADJ_T / 32];
+    auto at = [](int x, int k, int l) { return (x * 5 + k) * ADJ_P + l; };
     const Eos<double> e = Eos<double>::from(p.eos);
     const int tid = threadIdx.x;
     const int nrow = p.nd + 2 * p.ng;
@@ -89,8 +112,8 @@ __global__ void __launch_bounds__(ADJ_T) adj_sweep_kernel(const AdjSweepParams p
         }
 #pragma unroll
         for (int k = 0; k < 5; k++) {
-            W[x][k][l] = w[k];
-            AW[x][k][l] = 0.0;
+            W[at(x, k, l)] = w[k];
+            AW[at(x, k, l)] = 0.0;
         }
     }
     // B: face-flux cotangents. R_c = −(F_{c,c+1} − F_{c−1,c})·inv on interior
@@ -118,7 +141,7 @@ __global__ void __launch_bounds__(ADJ_T) adj_sweep_kernel(const AdjSweepParams p
             }
         }
 #pragma unroll
-        for (int k = 0; k < 5; k++) AF[x][k][l] = fb[k];
+        for (int k = 0; k < 5; k++) AF[at(x, k, l)] = fb[k];
     }
     __syncthreads();
     // B': Lax–Friedrichs part (1 − θ)·F_LF of limited faces touching owned
@@ -136,16 +159,16 @@ __global__ void __launch_bounds__(ADJ_T) adj_sweep_kernel(const AdjSweepParams p
                 face_bar(i, l, fb);
 #pragma unroll
                 for (int k = 0; k < 5; k++) {
-                    wi[k] = W[x][k][l];
-                    wj[k] = W[x + 1][k][l];
+                    wi[k] = W[at(x, k, l)];
+                    wj[k] = W[at(x + 1, k, l)];
                 }
                 double glf = 0.0;
                 adj::lf_vjp<D>(e, wi, wj, th, fb, wib, wjb, glf);
                 if (i >= c0) gacc += glf;  // face c0 − 1 belongs to the previous segment
 #pragma unroll
                 for (int k = 0; k < 5; k++) {
-                    AW[x][k][l] += wib[k];
-                    AW[x + 1][k][l] += wjb[k];
+                    AW[at(x, k, l)] += wib[k];
+                    AW[at(x + 1, k, l)] += wjb[k];
                 }
             }
             __syncthreads();
@@ -157,45 +180,36 @@ __global__ void __launch_bounds__(ADJ_T) adj_sweep_kernel(const AdjSweepParams p
     {
         const int l = tid % ADJ_P, mj = tid / ADJ_P;  // mj < L + 5
         const int j = c0 - 3 + mj;
-        double wb6[6][5];
 #pragma unroll
-        for (int s = 0; s < 6; s++)
-#pragma unroll
-            for (int k = 0; k < 5; k++) wb6[s][k] = 0.0;
-        const bool act = lane_ok(l) && j >= p.ng - 3 && j <= p.ng + p.nd + 1;
-        if (act) {
+        for (int q = 0; q < 30; q++) SLOT[q * ADJ_T + tid] = 0.0;
+        if (lane_ok(l) && j >= p.ng - 3 && j <= p.ng + p.nd + 1) {
             double fb[5];
             bool any = false;
 #pragma unroll
             for (int k = 0; k < 5; k++) {
-                fb[k] = s6(0) * AF[mj + 2][k][l] + s6(1) * (AF[mj + 1][k][l] + AF[mj + 3][k][l]) +
-                        s6(2) * (AF[mj][k][l] + AF[mj + 4][k][l]);
+                fb[k] = s6(0) * AF[at(mj + 2, k, l)] + s6(1) * (AF[at(mj + 1, k, l)] + AF[at(mj + 3, k, l)]) +
+                        s6(2) * (AF[at(mj, k, l)] + AF[at(mj + 4, k, l)]);
                 any = any || fb[k] != 0.0;
             }
             if (any) {
-                double w6[6][5];
-#pragma unroll
-                for (int s = 0; s < 6; s++)
-#pragma unroll
-                    for (int k = 0; k < 5; k++) w6[s][k] = W[mj + s][k][l];
                 double gm = 0.0;
-                adj::midpoint_vjp<D>(e, w6, fb, wb6, gm);
+                adj::midpoint_vjp_acc<D>(e, SmemRows{W, mj, l}, fb, SlotAcc{SLOT, tid}, gm);
                 // neighbouring segments recompute the halo midpoints; only
                 // the segment owning row j counts its γ cotangent
                 if (j >= c0 && j < cend) gacc += gm;
             }
         }
-        // gather: midpoints of one residue class mod 6 touch disjoint rows
-        for (int ph = 0; ph < 6; ph++) {
-            if (act && mj % 6 == ph) {
-#pragma unroll
-                for (int s = 0; s < 6; s++)
-#pragma unroll
-                    for (int k = 0; k < 5; k++) AW[mj + s][k][l] += wb6[s][k];
-            }
-            __syncthreads();
-        }
     }
+    __syncthreads();
+    // gather: row x collects from the midpoints mj = x−5..x in a fixed order
+    for (int idx = tid; idx < ADJ_ROWS * 5 * ADJ_P; idx += ADJ_T) {
+        const int x = idx / (5 * ADJ_P), k = (idx / ADJ_P) % 5, l = idx % ADJ_P;
+        double acc = AW[at(x, k, l)];
+        for (int mj = max(0, x - 5); mj <= min(x, ADJ_L + 4); mj++)
+            acc += SLOT[((x - mj) * 5 + k) * ADJ_T + mj * ADJ_P + l];
+        AW[at(x, k, l)] = acc;
+    }
+    __syncthreads();
     // D: owned rows: primitive cotangent → conserved cotangent
     for (int idx = tid; idx < ADJ_L * ADJ_P; idx += ADJ_T) {
         const int x = idx / ADJ_P, l = idx % ADJ_P;
@@ -207,7 +221,7 @@ __global__ void __launch_bounds__(ADJ_T) adj_sweep_kernel(const AdjSweepParams p
 #pragma unroll
         for (int k = 0; k < 5; k++) {
             u[k] = p.u[k * p.ncell + g];
-            wb[k] = AW[x + 5][k][l];
+            wb[k] = AW[at(x + 5, k, l)];
             any = any || wb[k] != 0.0;
         }
         if (!any) continue;
@@ -406,12 +420,25 @@ __global__ void adj_set_dt(StepCtl* ctl, const double* dt) {
 }
 
 cudaError_t adj_sweep_launch(int d, const AdjSweepParams& p, dim3 grid, cudaStream_t s) {
+    static bool prepared[64] = {};  // dynamic shared-memory opt-in, once per device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!prepared[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(adj_sweep_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ADJ_SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(adj_sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ADJ_SMEM);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(adj_sweep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ADJ_SMEM);
+        if (e != cudaSuccess) return e;
+        prepared[dev] = true;
+    }
     if (d == 0)
-        adj_sweep_kernel<0><<<grid, ADJ_T, 0, s>>>(p);
+        adj_sweep_kernel<0><<<grid, ADJ_T, ADJ_SMEM, s>>>(p);
     else if (d == 1)
-        adj_sweep_kernel<1><<<grid, ADJ_T, 0, s>>>(p);
+        adj_sweep_kernel<1><<<grid, ADJ_T, ADJ_SMEM, s>>>(p);
     else
-        adj_sweep_kernel<2><<<grid, ADJ_T, 0, s>>>(p);
+        adj_sweep_kernel<2><<<grid, ADJ_T, ADJ_SMEM, s>>>(p);
     return cudaGetLastError();
 }
 

@@ -115,15 +115,25 @@ __device__ __forceinline__ void hllc_vjp(const Eos<double>& e, const double* wl,
     double ql[5], qr[5];
     to_cons(e, wl, ql);
     to_cons(e, wr, qr);
+    // the side whose state enters the flux is copied element-wise (selecting
+    // a whole array by pointer would force the arrays into local memory)
+    double w[5], q[5], wb[5] = {0, 0, 0, 0, 0};
     if (sl >= 0.0 || sr <= 0.0) {
         // supersonic: f = flux(w, q) of one side; sl, sr only chose the branch
         const bool L = sl >= 0.0;
-        const double* w = L ? wl : wr;
-        const double* q = L ? ql : qr;
-        double* wb = L ? wlb : wrb;
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            w[k] = L ? wl[k] : wr[k];
+            q[k] = L ? ql[k] : qr[k];
+        }
         double qb[5] = {0, 0, 0, 0, 0};
         flux_wq_vjp<UN>(w, q, fb, wb, qb);
         to_cons_vjp(e, w, qb, wb, gb);
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            wlb[k] += L ? wb[k] : 0.0;
+            wrb[k] += L ? 0.0 : wb[k];
+        }
         return;
     }
     const double rl = wl[0], rr = wr[0], pl = wl[4], pr = wr[4];
@@ -131,9 +141,11 @@ __device__ __forceinline__ void hllc_vjp(const Eos<double>& e, const double* wl,
     const double den = rl * (sl - ul) - rr * (sr - ur);
     const double ss = num / den;
     const bool L = ss >= 0.0;
-    const double* w = L ? wl : wr;
-    const double* q = L ? ql : qr;
-    double* wb = L ? wlb : wrb;
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        w[k] = L ? wl[k] : wr[k];
+        q[k] = L ? ql[k] : qr[k];
+    }
     const double s = L ? sl : sr;
     const double rho = w[0], u = w[UN], p = w[4];
     const double sm = s - u;
@@ -191,6 +203,11 @@ __device__ __forceinline__ void hllc_vjp(const Eos<double>& e, const double* wl,
     wb[UN] += ub;
     wb[4] += pb;
     to_cons_vjp(e, w, qb, wb, gb);
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        wlb[k] += L ? wb[k] : 0.0;
+        wrb[k] += L ? 0.0 : wb[k];
+    }
     // ss = num / den
     const double numb = ssb / den, denb = -ssb * ss / den;
     double rlb = numb * ul * (sl - ul) + denb * (sl - ul);
@@ -251,28 +268,30 @@ __device__ __forceinline__ void weno5z_grad(double v0, double v1, double v2, dou
                          13.0 / 12.0 * (A2 * A2) + 0.25 * (B2 * B2)};
     const double dw[3] = {1.0 / 16.0, 10.0 / 16.0, 5.0 / 16.0};
     const double tau = fabs(b[0] - b[2]);
-    double r[3], a[3];
+    // derivative arithmetic only: reciprocals instead of the reference's
+    // divisions (the interpolated value itself comes from weno5z_interp)
+    double ib[3], r[3], a[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        r[k] = tau / (b[k] + eps);
+        ib[k] = 1.0 / (b[k] + eps);
+        r[k] = tau * ib[k];
         a[k] = dw[k] * (1.0 + r[k] * r[k]);
     }
-    const double S = a[0] + a[1] + a[2];
+    const double iS = 1.0 / (a[0] + a[1] + a[2]);
     // q_k − y = Σ_m a_m (q_k − q_m) / S, formed from differences of the
     // candidate values: subtracting the rounded y would leave a rounding
     // residue that the large weight derivatives of near-flat stencils
     // (∝ 1/(β + 1e-40)) amplify into spurious gradient terms
-    const double dq[3] = {(a[1] * (q[0] - q[1]) + a[2] * (q[0] - q[2])) / S,
-                          (a[0] * (q[1] - q[0]) + a[2] * (q[1] - q[2])) / S,
-                          (a[0] * (q[2] - q[0]) + a[1] * (q[2] - q[1])) / S};
+    const double dq[3] = {(a[1] * (q[0] - q[1]) + a[2] * (q[0] - q[2])) * iS,
+                          (a[0] * (q[1] - q[0]) + a[2] * (q[1] - q[2])) * iS,
+                          (a[0] * (q[2] - q[0]) + a[1] * (q[2] - q[1])) * iS};
     double qb[3], bb[3], taub = 0.0;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        qb[k] = a[k] / S;
-        const double ab = dq[k] / S;
-        const double rb = ab * dw[k] * 2.0 * r[k];
-        taub += rb / (b[k] + eps);
-        bb[k] = -rb * r[k] / (b[k] + eps);
+        qb[k] = a[k] * iS;
+        const double rb = (dq[k] * iS) * dw[k] * 2.0 * r[k];
+        taub += rb * ib[k];
+        bb[k] = -rb * r[k] * ib[k];
     }
     const double sgn = (b[0] - b[2]) < 0.0 ? -1.0 : 1.0;
     bb[0] += sgn * taub;
@@ -291,19 +310,32 @@ __device__ __forceinline__ void weno5z_grad(double v0, double v1, double v2, dou
 
 // ---- characteristic WCNS midpoint flux (scheme.rs:286-333) ---------------
 
-// Midpoint between stencil rows 2 and 3 of the six primitive rows w6[s][k]
-// (s = 0..5); given the cotangent fb of its HLLC flux, add wb6[s][k] and gb.
-// Sparse form of the dense eigenvector products, as in the forward sweep.
-template <int D>
-__device__ __forceinline__ void midpoint_vjp(const Eos<double>& e, const double (*w6)[5], const double* fb,
-                                             double (*wb6)[5], double& gb) {
+// Stencil accessors: W(s, k) reads primitive k of stencil row s (0..5);
+// B.add(s, k, v) accumulates a cotangent. Plain arrays on the host; the
+// device kernel reads shared memory and writes a per-thread slot, which keeps
+// the 2×30 stencil values out of registers.
+struct RowsIn {
+    const double (*w)[5];
+    __device__ __forceinline__ double operator()(int s, int k) const { return w[s][k]; }
+};
+struct RowsOut {
+    double (*b)[5];
+    __device__ __forceinline__ void add(int s, int k, double v) const { b[s][k] += v; }
+};
+
+// Midpoint between stencil rows 2 and 3 of the six primitive rows W(s, k);
+// given the cotangent fb of its HLLC flux, accumulate the stencil cotangents
+// and gb. Sparse form of the dense eigenvector products, as in the forward
+// sweep; the characteristic fields are reversed one at a time.
+template <int D, class WIn, class WOut>
+__device__ __forceinline__ void midpoint_vjp_acc(const Eos<double>& e, const WIn& W, const double* fb, const WOut& B,
+                                                 double& gb) {
     constexpr int un = 1 + D;
     constexpr int t1 = 1 + (D + 1) % 3, t2 = 1 + (D + 2) % 3;
-    double avg[5];
-#pragma unroll
-    for (int k = 0; k < 5; k++) avg[k] = 0.5 * (w6[2][k] + w6[3][k]);
-    const double rho = avg[0];
-    const double c = sound_speed(e, avg[0], avg[4]);
+    const double avg0 = 0.5 * (W(2, 0) + W(3, 0));
+    const double avg4 = 0.5 * (W(2, 4) + W(3, 4));
+    const double rho = avg0;
+    const double c = sound_speed(e, avg0, avg4);
     const double l4un = rho / (2.0 * c);
     const double l0un = -l4un;
     const double l04 = 1.0 / (2.0 * c * c);
@@ -311,21 +343,22 @@ __device__ __forceinline__ void midpoint_vjp(const Eos<double>& e, const double 
     const double run4 = c / rho;
     const double run0 = -run4;
     const double r40 = c * c;
-    double ch[5][6];
-#pragma unroll
-    for (int s = 0; s < 6; s++) {
-        const double wn = w6[s][un], w4 = w6[s][4];
-        ch[0][s] = l0un * wn + l04 * w4;
-        ch[1][s] = w6[s][0] + l14 * w4;
-        ch[2][s] = w6[s][t1];
-        ch[3][s] = w6[s][t2];
-        ch[4][s] = l4un * wn + l04 * w4;
-    }
+    // characteristic values of field a at stencil row s (exact forward order)
+    auto chv = [&](int a, int s) -> double {
+        switch (a) {
+            case 0: return l0un * W(s, un) + l04 * W(s, 4);
+            case 1: return W(s, 0) + l14 * W(s, 4);
+            case 2: return W(s, t1);
+            case 3: return W(s, t2);
+            default: return l4un * W(s, un) + l04 * W(s, 4);
+        }
+    };
     double cl[5], cr[5];
 #pragma unroll
     for (int a = 0; a < 5; a++) {
-        cl[a] = weno5z_interp(ch[a][0], ch[a][1], ch[a][2], ch[a][3], ch[a][4]);
-        cr[a] = weno5z_interp(ch[a][5], ch[a][4], ch[a][3], ch[a][2], ch[a][1]);
+        const double v0 = chv(a, 0), v1 = chv(a, 1), v2 = chv(a, 2), v3 = chv(a, 3), v4 = chv(a, 4), v5 = chv(a, 5);
+        cl[a] = weno5z_interp(v0, v1, v2, v3, v4);
+        cr[a] = weno5z_interp(v5, v4, v3, v2, v1);
     }
     double wl[5], wr[5];
     wl[0] = (cl[0] + cl[1]) + cl[4];
@@ -341,11 +374,17 @@ __device__ __forceinline__ void midpoint_vjp(const Eos<double>& e, const double 
     double wlb[5] = {0, 0, 0, 0, 0}, wrb[5] = {0, 0, 0, 0, 0};
     if (!admissible(e, wl[0], wl[4]) || !admissible(e, wr[0], wr[4])) {
         // first-order fallback: the flux of the two adjacent cells
-        hllc_vjp<un>(e, w6[2], w6[3], fb, wlb, wrb, gb);
+        double w2[5], w3[5];
 #pragma unroll
         for (int k = 0; k < 5; k++) {
-            wb6[2][k] += wlb[k];
-            wb6[3][k] += wrb[k];
+            w2[k] = W(2, k);
+            w3[k] = W(3, k);
+        }
+        hllc_vjp<un>(e, w2, w3, fb, wlb, wrb, gb);
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            B.add(2, k, wlb[k]);
+            B.add(3, k, wrb[k]);
         }
         return;
     }
@@ -365,33 +404,46 @@ __device__ __forceinline__ void midpoint_vjp(const Eos<double>& e, const double 
     const double run0b = wlb[un] * cl[0] + wrb[un] * cr[0];
     const double run4b = wlb[un] * cl[4] + wrb[un] * cr[4];
     const double r40b = wlb[4] * (cl[0] + cl[4]) + wrb[4] * (cr[0] + cr[4]);
-    // WENO-Z interpolations
-    double chb[5][6];
-#pragma unroll
-    for (int a = 0; a < 5; a++) {
-        double g[5];
-        weno5z_grad(ch[a][0], ch[a][1], ch[a][2], ch[a][3], ch[a][4], g);
-#pragma unroll
-        for (int s = 0; s < 5; s++) chb[a][s] = clb[a] * g[s];
-        chb[a][5] = 0.0;
-        weno5z_grad(ch[a][5], ch[a][4], ch[a][3], ch[a][2], ch[a][1], g);
-#pragma unroll
-        for (int s = 0; s < 5; s++) chb[a][5 - s] += crb[a] * g[s];
-    }
-    // characteristic projection c = L·w
+    // WENO-Z interpolations and the projection c = L·w, one field at a time
     double l0unb = 0.0, l4unb = 0.0, l04b = 0.0, l14b = 0.0;
+    // not unrolled: keeps one field's stencil, gradients and cotangents live at a time
+#pragma unroll 1
+    for (int a = 0; a < 5; a++) {
+        if (clb[a] == 0.0 && crb[a] == 0.0) continue;
+        double v[6], chb[6], g[5];
 #pragma unroll
-    for (int s = 0; s < 6; s++) {
-        const double wn = w6[s][un], w4 = w6[s][4];
-        wb6[s][un] += l0un * chb[0][s] + l4un * chb[4][s];
-        wb6[s][4] += l04 * (chb[0][s] + chb[4][s]) + l14 * chb[1][s];
-        wb6[s][0] += chb[1][s];
-        wb6[s][t1] += chb[2][s];
-        wb6[s][t2] += chb[3][s];
-        l0unb += wn * chb[0][s];
-        l4unb += wn * chb[4][s];
-        l04b += w4 * (chb[0][s] + chb[4][s]);
-        l14b += w4 * chb[1][s];
+        for (int s2 = 0; s2 < 6; s2++) v[s2] = chv(a, s2);
+        weno5z_grad(v[0], v[1], v[2], v[3], v[4], g);
+#pragma unroll
+        for (int s2 = 0; s2 < 5; s2++) chb[s2] = clb[a] * g[s2];
+        chb[5] = 0.0;
+        weno5z_grad(v[5], v[4], v[3], v[2], v[1], g);
+#pragma unroll
+        for (int s2 = 0; s2 < 5; s2++) chb[5 - s2] += crb[a] * g[s2];
+#pragma unroll
+        for (int s2 = 0; s2 < 6; s2++) {
+            const double cb = chb[s2];
+            switch (a) {
+                case 0:
+                    B.add(s2, un, l0un * cb);
+                    B.add(s2, 4, l04 * cb);
+                    l0unb += W(s2, un) * cb;
+                    l04b += W(s2, 4) * cb;
+                    break;
+                case 1:
+                    B.add(s2, 0, cb);
+                    B.add(s2, 4, l14 * cb);
+                    l14b += W(s2, 4) * cb;
+                    break;
+                case 2: B.add(s2, t1, cb); break;
+                case 3: B.add(s2, t2, cb); break;
+                default:
+                    B.add(s2, un, l4un * cb);
+                    B.add(s2, 4, l04 * cb);
+                    l4unb += W(s2, un) * cb;
+                    l04b += W(s2, 4) * cb;
+            }
+        }
     }
     // eigenvector entries as functions of (ρ, c) at the midpoint average
     const double l4unt = l4unb - l0unb;
@@ -400,11 +452,18 @@ __device__ __forceinline__ void midpoint_vjp(const Eos<double>& e, const double 
                       r40b * (2.0 * c);
     double avgb0 = l4unt / (2.0 * c) - run4t * run4 / rho;
     double avgb4 = 0.0;
-    sound_speed_vjp(e, avg[0], avg[4], cb, avgb0, avgb4, gb);
-    wb6[2][0] += 0.5 * avgb0;
-    wb6[3][0] += 0.5 * avgb0;
-    wb6[2][4] += 0.5 * avgb4;
-    wb6[3][4] += 0.5 * avgb4;
+    sound_speed_vjp(e, avg0, avg4, cb, avgb0, avgb4, gb);
+    B.add(2, 0, 0.5 * avgb0);
+    B.add(3, 0, 0.5 * avgb0);
+    B.add(2, 4, 0.5 * avgb4);
+    B.add(3, 4, 0.5 * avgb4);
+}
+
+// Array form of midpoint_vjp: w6[s][k] in, wb6[s][k] accumulated.
+template <int D>
+__device__ __forceinline__ void midpoint_vjp(const Eos<double>& e, const double (*w6)[5], const double* fb,
+                                             double (*wb6)[5], double& gb) {
+    midpoint_vjp_acc<D>(e, RowsIn{w6}, fb, RowsOut{wb6}, gb);
 }
 
 // ---- positivity limiter with the blend weight θ held fixed (scheme.rs:395-464)
@@ -434,13 +493,17 @@ __device__ __forceinline__ void lf_vjp(const Eos<double>& e, const double* wi, c
         urb[k] = -0.5 * alpha * flfb[k];
         ulb[k] = 0.5 * alpha * flfb[k];
     }
-    double* wb = ai >= aj ? wib : wjb;
-    const double* w = ai >= aj ? wi : wj;
-    wb[un] += (w[un] < 0.0 ? -1.0 : 1.0) * alphab;
+    const bool I = ai >= aj;  // Davis-style max: first argument on ties
+    const double wun = I ? wi[un] : wj[un], w0 = I ? wi[0] : wj[0], w4 = I ? wi[4] : wj[4];
     double rb = 0.0, pb = 0.0;
-    sound_speed_vjp(e, w[0], w[4], alphab, rb, pb, gb);
-    wb[0] += rb;
-    wb[4] += pb;
+    sound_speed_vjp(e, w0, w4, alphab, rb, pb, gb);
+    const double unb = (wun < 0.0 ? -1.0 : 1.0) * alphab;
+    wib[0] += I ? rb : 0.0;
+    wib[un] += I ? unb : 0.0;
+    wib[4] += I ? pb : 0.0;
+    wjb[0] += I ? 0.0 : rb;
+    wjb[un] += I ? 0.0 : unb;
+    wjb[4] += I ? 0.0 : pb;
     flux_wq_vjp<un>(wi, ul, flpb, wib, ulb);
     flux_wq_vjp<un>(wj, ur, frpb, wjb, urb);
     to_cons_vjp(e, wi, ulb, wib, gb);
