@@ -87,6 +87,10 @@ SIGNATURES = {
     "emg_batch1d_download": (C.c_int, [_P, _D]),
     "emg_batch1d_status": (C.c_int, [_P, _D, _U64]),
     "emg_batch1d_stream": (C.c_int, [_P, C.POINTER(_P)]),
+    "emg_batch1d_record": (C.c_int, [_P, C.c_double, C.c_uint64, _U64]),
+    "emg_batch1d_objective": (C.c_int, [_P, C.c_int, C.c_double, C.c_double, _D]),
+    "emg_batch1d_backward": (C.c_int, [_P, C.c_double, _D, _D]),
+    "emg_batch1d_adjoint_times": (C.c_int, [_P, _D]),
     "emg_amr_create": (C.c_int, [C.POINTER(EmgAmrConfig), C.POINTER(EmgEos), _D, _D, C.POINTER(EmgBc),
                                  C.POINTER(EmgOpts), INIT_FN, C.c_void_p, C.POINTER(_P)]),
     "emg_amr_create_from_blocks": (C.c_int, [C.POINTER(EmgAmrConfig), C.POINTER(EmgEos), _D, _D, C.POINTER(EmgBc),

@@ -72,3 +72,33 @@ class GpuBatch1D:
     def split(self, u):
         """Per-instance views of a concatenated [Σn, 5] array."""
         return np.split(u, np.cumsum(self.n)[:-1])
+
+    # ---- discrete adjoint of a batched run (FP64 batches, WENO mode)
+    def record(self, t_end, checkpoint_every=0):
+        """Record an FP64 run of every instance from the initial state to
+        t_end; returns the number of batch steps."""
+        n = C.c_uint64()
+        check(lib().emg_batch1d_record(self._h, float(t_end), int(checkpoint_every), C.byref(n)))
+        return n.value
+
+    def objective(self, kind, x_lo, x_hi):
+        """Per-instance J over cells with centre in [x_lo, x_hi] (kind 0: Σ p·dx,
+        1: Σ E·dx) on the recorded final state; seeds the backward pass."""
+        J = np.zeros(len(self.n))
+        check(lib().emg_batch1d_objective(self._h, int(kind), float(x_lo), float(x_hi), _dptr(J)))
+        return J
+
+    def backward(self, x_split, want_wbar=False):
+        """∂J_i/∂(ρ_L, u_L, p_L, ρ_R, u_R, p_R) per instance ([ninst, 6]) for
+        initial data constant on either side of x_split; with want_wbar also
+        ∂J/∂W⁰ per cell ([Σn, 5])."""
+        g = np.zeros((len(self.n), 6))
+        wb = np.zeros((int(self.n.sum()), 5)) if want_wbar else None
+        check(lib().emg_batch1d_backward(self._h, float(x_split), _dptr(g), _dptr(wb) if want_wbar else None))
+        return (g, wb) if want_wbar else g
+
+    def adjoint_times(self):
+        """Device ms of [last recorded run, checkpoint recompute, reverse sweeps]."""
+        ms = np.zeros(3)
+        check(lib().emg_batch1d_adjoint_times(self._h, _dptr(ms)))
+        return ms

@@ -24,6 +24,7 @@
 // quantities (fallback tests, HLLC wave cases) equal the forward run's.
 #include "uniform_internal.h"
 #include "adjoint.cuh"
+#include "adjoint_launch.h"
 
 #include <cmath>
 #include <cstring>
@@ -32,31 +33,6 @@ namespace emg {
 
 __global__ void aos_to_soa(const double* __restrict__ aos, double* __restrict__ soa, int64_t ncell);
 __global__ void soa_to_aos(const double* __restrict__ soa, double* __restrict__ aos, int64_t ncell);
-
-constexpr int ADJ_T = 256;                 // threads per CTA
-constexpr int ADJ_P = 4;                   // pencils per CTA
-constexpr int ADJ_L = ADJ_T / ADJ_P - 5;   // owned rows per pencil (one midpoint per thread: L + 5 = 64)
-constexpr int ADJ_ROWS = ADJ_L + 10;       // staged rows per pencil
-constexpr int ADJ_FACES = ADJ_L + 9;       // faces whose cotangents a CTA forms
-// 2 CTAs per SM (128 registers, some spills) measured 10 % faster than 1 CTA
-// per SM without spills on the 2-D explosion 512^2
-constexpr int ADJ_MINB = 2;
-
-struct AdjSweepParams {
-    const double* __restrict__ u;      // stage input X_s, ghost-filled, SoA with field stride ncell
-    const double* __restrict__ theta;  // recorded limiter blend weights of this stage and axis (null: none)
-    const double* __restrict__ ybar;   // cotangent of the stage output (interior cells)
-    double coef;                       // β_s·dt: ∂(stage output)/∂(residual)
-    double* xbar;                      // cotangent of X_s, accumulated (ghost cells included)
-    double* gpart;                     // per-CTA partial sums of the γ cotangent
-    int64_t ncell;
-    int64_t sd, sl, so;                // strides of the sweep, lane and other axes
-    int nd, nl, no;                    // interior extents
-    int gl, go;                        // ghost offsets of the lane and other axes
-    int ng;
-    double inv;                        // 1/dx along the sweep axis (the forward multiplies by it)
-    EosD eos;
-};
 
 // Shared-memory layout of the adjoint sweep (dynamic, ≈94 KB): primitives and
 // their cotangents of ADJ_ROWS rows, face-flux cotangents of ADJ_FACES faces
@@ -77,7 +53,7 @@ struct SlotAcc {
 
 // Reverse of one axis' contribution −(F_{i+½} − F_{i−½})/dx to the stage
 // residual (the forward sweep of sweep.cuh, FP64, WENO flux mode).
-template <int D>
+template <int D, int KIND>
 __global__ void __launch_bounds__(ADJ_T, ADJ_MINB) adj_sweep_kernel(const AdjSweepParams p) {
     extern __shared__ __align__(16) double adj_smem[];
     double* W = adj_smem;                             // [ADJ_ROWS][5][ADJ_P] primitives
@@ -85,25 +61,60 @@ __global__ void __launch_bounds__(ADJ_T, ADJ_MINB) adj_sweep_kernel(const AdjSwe
     double* AF = AW + ADJ_ROWS * 5 * ADJ_P;           // [ADJ_FACES][5][ADJ_P] cotangents of F̃
     double* SLOT = AF + ADJ_FACES * 5 * ADJ_P;        // [30][ADJ_T] midpoint stencil cotangents
     __shared__ double s_g[ADJ_T / 32];
+    // per-pencil line geometry: offset of padded row 0, interior cells, owned
+    // rows [c0, cend), 1/dx and the residual coefficient β·dt
+    __shared__ int64_t s_base[ADJ_P];
+    __shared__ int s_n[ADJ_P], s_c0[ADJ_P], s_cend[ADJ_P], s_ok[ADJ_P];
+    __shared__ double s_inv[ADJ_P], s_coef[ADJ_P];
     auto at = [](int x, int k, int l) { return (x * 5 + k) * ADJ_P + l; };
     const Eos<double> e = Eos<double>::from(p.eos);
     const int tid = threadIdx.x;
-    const int nrow = p.nd + 2 * p.ng;
-    const int c0 = p.ng - 5 + (int)blockIdx.y * ADJ_L;     // first owned row
-    const int cend = min(c0 + ADJ_L, p.ng + p.nd + 5);    // rows beyond receive nothing
-    const int lane0 = blockIdx.x * ADJ_P;
-    const int ob = blockIdx.z;
-    const int ifirst = p.ng - 1, ilast = p.ng + p.nd - 1;  // faces f = 0..n sit right of rows ifirst..ilast
-    auto lane_ok = [&](int l) { return lane0 + l < p.nl; };
-    auto loff = [&](int l) { return (int64_t)(p.gl + lane0 + l) * p.sl + (int64_t)(p.go + ob) * p.so; };
+    const int ng = p.ng;
+    if (tid < ADJ_P) {
+        const int l = tid;
+        if constexpr (KIND == 0) {
+            const int la = blockIdx.x * ADJ_P + l;
+            s_ok[l] = la < p.nl;
+            s_base[l] = (int64_t)(p.gl + la) * p.sl + (int64_t)(p.go + blockIdx.z) * p.so;
+            s_n[l] = p.nd;
+            s_c0[l] = ng - 5 + (int)blockIdx.y * ADJ_L;
+            s_inv[l] = p.inv;
+            s_coef[l] = p.coef;
+        } else {
+            const int z = blockIdx.x * ADJ_P + l;
+            int ok = 0;
+            if (z < p.nlanes) {
+                const AdjLane ln = p.lanes[z];
+                const double dt = p.inst_dt[ln.inst];
+                ok = dt > 0.0;
+                s_base[l] = ln.base;
+                s_n[l] = ln.n;
+                s_c0[l] = ln.c0;
+                s_inv[l] = 1.0 / p.inst_dx[ln.inst];
+                s_coef[l] = p.beta * dt;
+            } else {
+                s_base[l] = 0;
+                s_n[l] = 0;
+                s_c0[l] = 0;
+                s_inv[l] = 0.0;
+                s_coef[l] = 0.0;
+            }
+            s_ok[l] = ok;
+        }
+        s_cend[l] = min(s_c0[l] + ADJ_L, ng + s_n[l] + 5);  // rows beyond receive nothing
+    }
+    __syncthreads();
+    // faces f = 0..n sit right of rows ng−1 .. ng+n−1
+    auto lane_ok = [&](int l) { return s_ok[l] != 0; };
+    auto loff = [&](int l) { return s_base[l]; };
     double gacc = 0.0;
 
     // A: primitives of rows [c0 − 5, c0 + L + 5)
     for (int idx = tid; idx < ADJ_ROWS * ADJ_P; idx += ADJ_T) {
         const int x = idx / ADJ_P, l = idx % ADJ_P;
-        const int c = c0 - 5 + x;
+        const int c = s_c0[l] - 5 + x;
         double w[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        if (lane_ok(l) && c >= 0 && c < nrow) {
+        if (lane_ok(l) && c >= 0 && c < s_n[l] + 2 * ng) {
             const int64_t g = loff(l) + (int64_t)c * p.sd;
             double u[5];
 #pragma unroll
@@ -120,19 +131,19 @@ __global__ void __launch_bounds__(ADJ_T, ADJ_MINB) adj_sweep_kernel(const AdjSwe
     // cells, so F̄_i = (R̄_{i+1} − R̄_i)·inv with R̄ = coef·Ȳ; F̃̄ = θ·F̄.
     auto face_bar = [&](int i, int l, double* fb) {
         const int64_t g = loff(l) + (int64_t)i * p.sd;
-        const bool in_l = i >= p.ng, in_r = i + 1 <= ilast;
+        const bool in_l = i >= ng, in_r = i + 1 <= ng + s_n[l] - 1;
 #pragma unroll
         for (int k = 0; k < 5; k++) {
-            const double rl = in_l ? p.coef * p.ybar[k * p.ncell + g] : 0.0;
-            const double rr = in_r ? p.coef * p.ybar[k * p.ncell + g + p.sd] : 0.0;
-            fb[k] = (rr - rl) * p.inv;
+            const double rl = in_l ? s_coef[l] * p.ybar[k * p.ncell + g] : 0.0;
+            const double rr = in_r ? s_coef[l] * p.ybar[k * p.ncell + g + p.sd] : 0.0;
+            fb[k] = (rr - rl) * s_inv[l];
         }
     };
     for (int idx = tid; idx < ADJ_FACES * ADJ_P; idx += ADJ_T) {
         const int x = idx / ADJ_P, l = idx % ADJ_P;
-        const int i = c0 - 5 + x;
+        const int i = s_c0[l] - 5 + x;
         double fb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-        if (lane_ok(l) && i >= ifirst && i <= ilast) {
+        if (lane_ok(l) && i >= ng - 1 && i <= ng + s_n[l] - 1) {
             face_bar(i, l, fb);
             if (p.theta) {
                 const double th = p.theta[loff(l) + (int64_t)i * p.sd];
@@ -151,8 +162,10 @@ __global__ void __launch_bounds__(ADJ_T, ADJ_MINB) adj_sweep_kernel(const AdjSwe
         for (int par = 0; par < 2; par++) {
             for (int idx = tid; idx < ADJ_FACES * ADJ_P; idx += ADJ_T) {
                 const int x = idx / ADJ_P, l = idx % ADJ_P;
-                const int i = c0 - 5 + x;
-                if (!lane_ok(l) || i < ifirst || i > ilast || (i & 1) != par || i < c0 - 1 || i >= cend) continue;
+                const int i = s_c0[l] - 5 + x;
+                if (!lane_ok(l) || i < ng - 1 || i > ng + s_n[l] - 1 || (i & 1) != par || i < s_c0[l] - 1 ||
+                    i >= s_cend[l])
+                    continue;
                 const double th = p.theta[loff(l) + (int64_t)i * p.sd];
                 if (!(th < 1.0)) continue;
                 double fb[5], wi[5], wj[5], wib[5] = {0, 0, 0, 0, 0}, wjb[5] = {0, 0, 0, 0, 0};
@@ -164,7 +177,7 @@ __global__ void __launch_bounds__(ADJ_T, ADJ_MINB) adj_sweep_kernel(const AdjSwe
                 }
                 double glf = 0.0;
                 adj::lf_vjp<D>(e, wi, wj, th, fb, wib, wjb, glf);
-                if (i >= c0) gacc += glf;  // face c0 − 1 belongs to the previous segment
+                if (i >= s_c0[l]) gacc += glf;  // face c0 − 1 belongs to the previous segment
 #pragma unroll
                 for (int k = 0; k < 5; k++) {
                     AW[at(x, k, l)] += wib[k];
@@ -179,10 +192,10 @@ __global__ void __launch_bounds__(ADJ_T, ADJ_MINB) adj_sweep_kernel(const AdjSwe
     // cotangent is the S6-weighted sum of theirs.
     {
         const int l = tid % ADJ_P, mj = tid / ADJ_P;  // mj < L + 5
-        const int j = c0 - 3 + mj;
+        const int j = s_c0[l] - 3 + mj;
 #pragma unroll
         for (int q = 0; q < 30; q++) SLOT[q * ADJ_T + tid] = 0.0;
-        if (lane_ok(l) && j >= p.ng - 3 && j <= p.ng + p.nd + 1) {
+        if (lane_ok(l) && j >= ng - 3 && j <= ng + s_n[l] + 1) {
             double fb[5];
             bool any = false;
 #pragma unroll
@@ -196,7 +209,7 @@ __global__ void __launch_bounds__(ADJ_T, ADJ_MINB) adj_sweep_kernel(const AdjSwe
                 adj::midpoint_vjp_acc<D>(e, SmemRows{W, mj, l}, fb, SlotAcc{SLOT, tid}, gm);
                 // neighbouring segments recompute the halo midpoints; only
                 // the segment owning row j counts its γ cotangent
-                if (j >= c0 && j < cend) gacc += gm;
+                if (j >= s_c0[l] && j < s_cend[l]) gacc += gm;
             }
         }
     }
@@ -213,8 +226,8 @@ __global__ void __launch_bounds__(ADJ_T, ADJ_MINB) adj_sweep_kernel(const AdjSwe
     // D: owned rows: primitive cotangent → conserved cotangent
     for (int idx = tid; idx < ADJ_L * ADJ_P; idx += ADJ_T) {
         const int x = idx / ADJ_P, l = idx % ADJ_P;
-        const int c = c0 + x;
-        if (!lane_ok(l) || c >= cend) continue;
+        const int c = s_c0[l] + x;
+        if (!lane_ok(l) || c >= s_cend[l]) continue;
         const int64_t g = loff(l) + (int64_t)c * p.sd;
         double u[5], wb[5], ub[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
         bool any = false;
@@ -234,7 +247,7 @@ __global__ void __launch_bounds__(ADJ_T, ADJ_MINB) adj_sweep_kernel(const AdjSwe
     for (int o = 16; o > 0; o >>= 1) gacc += __shfl_xor_sync(0xffffffffu, gacc, o);
     if ((tid & 31) == 0) s_g[tid >> 5] = gacc;
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 0 && p.gpart) {
         double s = 0.0;
         for (int w = 0; w < ADJ_T / 32; w++) s += s_g[w];
         p.gpart[((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = s;
@@ -419,27 +432,44 @@ __global__ void adj_set_dt(StepCtl* ctl, const double* dt) {
     ctl->rate_bits = 0ull;
 }
 
-cudaError_t adj_sweep_launch(int d, const AdjSweepParams& p, dim3 grid, cudaStream_t s) {
+template <int KIND>
+cudaError_t adj_sweep_launch_kind(int d, const AdjSweepParams& p, dim3 grid, cudaStream_t s) {
     static bool prepared[64] = {};  // dynamic shared-memory opt-in, once per device
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (!prepared[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(adj_sweep_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ADJ_SMEM);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(adj_sweep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ADJ_SMEM);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(adj_sweep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ADJ_SMEM);
+        cudaError_t e = cudaFuncSetAttribute(adj_sweep_kernel<0, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)ADJ_SMEM);
+        if constexpr (KIND == 0) {
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(adj_sweep_kernel<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ADJ_SMEM);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(adj_sweep_kernel<2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ADJ_SMEM);
+        }
         if (e != cudaSuccess) return e;
         prepared[dev] = true;
     }
-    if (d == 0)
-        adj_sweep_kernel<0><<<grid, ADJ_T, ADJ_SMEM, s>>>(p);
-    else if (d == 1)
-        adj_sweep_kernel<1><<<grid, ADJ_T, ADJ_SMEM, s>>>(p);
-    else
-        adj_sweep_kernel<2><<<grid, ADJ_T, ADJ_SMEM, s>>>(p);
+    if constexpr (KIND == 0) {
+        if (d == 0)
+            adj_sweep_kernel<0, 0><<<grid, ADJ_T, ADJ_SMEM, s>>>(p);
+        else if (d == 1)
+            adj_sweep_kernel<1, 0><<<grid, ADJ_T, ADJ_SMEM, s>>>(p);
+        else
+            adj_sweep_kernel<2, 0><<<grid, ADJ_T, ADJ_SMEM, s>>>(p);
+    } else {
+        adj_sweep_kernel<0, KIND><<<grid, ADJ_T, ADJ_SMEM, s>>>(p);
+    }
     return cudaGetLastError();
+}
+
+cudaError_t adj_sweep_launch(int d, const AdjSweepParams& p, dim3 grid, cudaStream_t s) {
+    return adj_sweep_launch_kind<0>(d, p, grid, s);
+}
+
+cudaError_t adj_sweep_launch_batch(const AdjSweepParams& p, cudaStream_t s) {
+    const dim3 grid((unsigned)((p.nlanes + ADJ_P - 1) / ADJ_P), 1, 1);
+    return adj_sweep_launch_kind<1>(0, p, grid, s);
 }
 
 }  // namespace emg

@@ -170,12 +170,13 @@ def riemann_batch(ninst=4096, nmin=64, nmax=2048, seed=SEED, gamma=1.4, x0=0.5):
     st = np.stack([rng.uniform(0.1, 2.0, ninst), rng.uniform(-1.0, 1.0, ninst), rng.uniform(0.1, 2.0, ninst),
                    rng.uniform(0.1, 2.0, ninst), rng.uniform(-1.0, 1.0, ninst), rng.uniform(0.1, 2.0, ninst)], axis=1)
     parts = []
+    dx = 1.0 / n.astype(np.float64)
     for i in range(ninst):
-        x = (np.arange(n[i]) + 0.5) / n[i]
+        x = (np.arange(n[i]) + 0.5) * dx[i]  # cell centres as the device forms them, (c + ½)·dx
         left = x < x0
         w = np.zeros((n[i], 5))
         w[:, 0] = np.where(left, st[i, 0], st[i, 3])
         w[:, 1] = np.where(left, st[i, 1], st[i, 4])
         w[:, 4] = np.where(left, st[i, 2], st[i, 5])
         parts.append(sys_.to_cons(w))
-    return sys_, n, 1.0 / n.astype(np.float64), np.concatenate(parts), st
+    return sys_, n, dx, np.concatenate(parts), st

@@ -242,6 +242,29 @@ int emg_batch1d_status(emg_batch1d* h, double* t, uint64_t* steps);
 /* The handle's CUDA stream (cudaStream_t) as an opaque pointer. */
 int emg_batch1d_stream(emg_batch1d* h, void** stream);
 
+/* Discrete adjoint of a batched run (no counterpart in the reference, which
+ * has no adjoint; each instance is the 1-D Solver::step map, C/solver.rs:659-738).
+ * Records an FP64 run of every instance to t_end from the initial state given
+ * at creation (WENO mode; FP64 batch), keeping the batch state every
+ * `checkpoint_every` batch steps (0: 64); *batch_steps receives the number of
+ * batch steps. Time steps and limiter blend weights are held fixed. */
+int emg_batch1d_record(emg_batch1d* h, double t_end, uint64_t checkpoint_every, uint64_t* batch_steps);
+
+/* Per-instance box objective J_i on the recorded final state over cells with
+ * centre (c+½)·dx_i in [x_lo, x_hi] (EMG_OBJ_PRESSURE: Σ p·dx, EMG_OBJ_ENERGY:
+ * Σ E·dx); J receives ninst values. Seeds the backward pass. */
+int emg_batch1d_objective(emg_batch1d* h, int kind, double x_lo, double x_hi, double* J);
+
+/* Backward pass: grad6[6·i..] = ∂J_i/∂(ρ, u, p) of the initial primitive
+ * state summed over the cells left of x_split, then right of it (for Riemann
+ * problems, the gradient with respect to the six initial values); wbar, if
+ * not NULL, receives ∂J/∂W⁰ per cell in the layout of create's u. */
+int emg_batch1d_backward(emg_batch1d* h, double x_split, double* grad6, double* wbar);
+
+/* Device milliseconds of the last recorded run, and of the last backward pass
+ * split into checkpoint recompute and reverse sweeps. */
+int emg_batch1d_adjoint_times(emg_batch1d* h, double ms[3]);
+
 /* ------------------------------------------------------------------ block AMR */
 
 /* Block-AMR configuration (C/amr.rs:49-63). Blocks are b cells per active
