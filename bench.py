@@ -42,10 +42,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg of the uniform workload")
-    ap.add_argument("--workload", default="uniform", choices=["uniform", "amr", "batch", "adjoint"],
+    ap.add_argument("--workload", default="uniform", choices=["uniform", "amr", "batch", "adjoint", "batch_adjoint"],
                     help="uniform: 3-D explosion 256^3; amr: 3-D shock-bubble on block AMR (base 128^3, 3 levels); "
                          "batch: 4096 independent 1-D Riemann problems; adjoint: discrete adjoint of the 2-D "
-                         "explosion 512^2 over 400 steps")
+                         "explosion 512^2 over 400 steps; batch_adjoint: gradients of the 4096 Riemann problems "
+                         "with respect to their six initial values")
     ap.add_argument("--adj-n", type=int, default=512, help="adjoint workload: cells per side")
     ap.add_argument("--adj-steps", type=int, default=400, help="adjoint workload: forward steps")
     ap.add_argument("--amr-base", type=int, default=8, help="AMR base blocks per side (16^3 cells each)")
@@ -533,6 +534,93 @@ def run_adjoint(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_batch_adjoint(args, world, rank, local):
+    """Gradients of the 4096 independent 1-D Riemann problems: J_i = total
+    energy in the right half [0.5, 1] at t = 0.15, differentiated with respect
+    to the six initial values (ρ, u, p left and right of x = 0.5) of every
+    instance in one batched backward pass (FP64 forward recorded with its
+    CFL steps, checkpoints every 64 batch steps). One "step" = one recorded
+    run + one backward pass; checked against per-instance CPU dual-number
+    runs (oracle) on a sample of instances."""
+    import numpy as np
+    import torch
+    from emergence_b200 import GpuBatch1D, workloads as W
+    from emergence_b200.adjoint import OBJ_ENERGY
+    from emergence_b200.physics import Bc, FluxMode, Mesh
+
+    torch.cuda.set_device(local)
+    dev = torch.cuda.current_device()
+    sys_, n, dx, u, st = W.riemann_batch()
+    g = GpuBatch1D(sys_, n, dx, u)
+    for _ in range(max(args.warmup, 1)):
+        g.record(0.15)
+        g.objective(OBJ_ENERGY, 0.5, 1.0)
+        g.backward(0.5)
+    fwd, rec, rev = [], [], []
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            B = g.record(0.15)
+            J = g.objective(OBJ_ENERGY, 0.5, 1.0)
+            grad = g.backward(0.5)
+            ms = g.adjoint_times()
+            fwd.append(ms[0])
+            rec.append(ms[1])
+            rev.append(ms[2])
+    _, steps = g.status()
+    g.close()
+    f, r, v = float(np.median(fwd)), float(np.median(rec)), float(np.median(rev))
+    updates = int((n * steps.astype(np.int64)).sum())
+    check = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import pyoracle as O
+        bc = [[Bc.Outflow, Bc.Outflow], [Bc.Periodic, Bc.Periodic], [Bc.Periodic, Bc.Periodic]]
+        offs = np.concatenate([[0], np.cumsum(n)])
+        sample = [int(i) for i in np.argsort(n)[:4]]  # the four shortest instances
+        worst = 0.0
+        for i in sample:
+            mesh = Mesh.new((int(n[i]), 1, 1), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), ng=6)
+            uu = np.zeros((mesh.len(), 5))
+            mesh.interior(uu)[...] = u[offs[i]:offs[i + 1]].reshape(int(n[i]), 1, 1, 5)
+            o = O.OracleSolver(sys_, mesh, uu, bc=bc, mode=FluxMode.Weno)
+            dts = []
+            while o.t < 0.15 - 1e-10 * 0.15:
+                dts.append(min(o.dt_cfl(), 0.15 - o.t))
+                o.step(dts[-1])
+            x = (np.arange(n[i]) + 0.5) * dx[i]
+            left = x < 0.5
+            wp = np.zeros((mesh.len(), 5))
+            wi = mesh.interior(wp).reshape(int(n[i]), 5)
+            wi[:, 0] = np.where(left, st[i, 0], st[i, 3])
+            wi[:, 1] = np.where(left, st[i, 1], st[i, 4])
+            wi[:, 4] = np.where(left, st[i, 2], st[i, 5])
+            mesh.interior(wp)[...] = wi.reshape(int(n[i]), 1, 1, 5)
+            for q, (side, field) in enumerate([(True, 0), (True, 1), (True, 4), (False, 0), (False, 1), (False, 4)]):
+                dw = np.zeros_like(wp)
+                sel = left if side else ~left
+                mesh.interior(dw)[sel.reshape(-1, 1, 1), field] = 1.0
+                _, dJ = O.dual_run(sys_, mesh, wp, dw, 0.0, dts, OBJ_ENERGY, [0.5, 0, 0], [1.0, 0, 0], bc)
+                worst = max(worst, abs(grad[i, q] - dJ) / max(abs(dJ), 1e-12))
+        check = {"instances": sample, "max_rel_err_vs_dual": worst,
+                 "what": "CPU f64 forward-mode dual-number runs of the oracle, 6 directions per instance, same time steps"}
+    if rank == 0:
+        line = {
+            "metric": "adjoint/forward cost", "value": (r + v) / f, "unit": "ratio", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": f + r + v, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "4096 independent 1-D Riemann problems, cells log-uniform [64, 2048] (sum %d), "
+                                   "rho,p~U[0.1,2], u~U[-1,1], t_end 0.15, outflow; J_i = sum E dx over [0.5, 1]; "
+                                   "gradient w.r.t. the six initial values" % int(n.sum()),
+                       "batch_steps": int(B), "checkpoints": "every 64 batch steps",
+                       "step": "one recorded FP64 run + one backward pass"},
+            "forward_ms": f, "recompute_ms": r, "reverse_ms": v, "reverse_over_forward": v / f,
+            "forward_cell_updates_per_s": updates / (f * 1e-3),
+            "gradient_sample": {"instance0": [float(x) for x in grad[0]], "J0": float(J[0])},
+            "dual_check": check,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_init(args)
@@ -545,6 +633,8 @@ def main():
             run_batch(args, world, rank, local)
         elif args.workload == "adjoint":
             run_adjoint(args, world, rank, local)
+        elif args.workload == "batch_adjoint":
+            run_batch_adjoint(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
