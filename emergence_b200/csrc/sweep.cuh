@@ -140,8 +140,7 @@ template <typename RF, int P, int MODE> struct SweepSmem {
     static constexpr bool MID = MODE != MODE_CENTRAL;
     static constexpr size_t bytes() {
         return (size_t)RS * STRW * sizeof(double)                                    // W (f64 primitives, ρe, sensors)
-               + (RingTypes<RF>::MIXED && MID ? (size_t)RS * STR * sizeof(float) : 0)  // Wf (f32 copy of w)
-               + (MID ? (size_t)RS * STR * sizeof(RF) : 0)                             // MF (midpoint fluxes)
+               + (MID ? (size_t)RS * STR * sizeof(double) : 0)                         // MF (midpoint fluxes)
                + (size_t)RS * STR * sizeof(double)                                    // F (face fluxes)
                + (MODE == MODE_HYBRID ? (size_t)RS * P * sizeof(double) : 0);         // TH (blend weights)
     }
@@ -237,6 +236,75 @@ struct Sweep {
         hllc(e, wl, wr, un, f);
     }
 
+    // Mixed form of the midpoint flux: the characteristic projection, the
+    // back-projection, the admissibility test and the HLLC flux in FP64; the
+    // ten WENO-Z interpolations (the bulk of the arithmetic) in FP32 on the
+    // deviations of each characteristic stencil from its FP64 value at the
+    // cell beside the midpoint. WENO-Z is translation invariant (the candidate
+    // weights sum to 1, the smoothness indicators use differences only), so
+    // the deviation form is the same interpolant in exact arithmetic, and its
+    // FP32 rounding scales with the local variation of the data instead of
+    // with the state. FP32 HLLC or FP32 interpolation of the raw values leave
+    // ~5e-6 relative error in the residual per step; this form ~5e-8.
+    __device__ static __forceinline__ void midpoint_mixed(const Eos<double>& e, const double* __restrict__ Wd, int m,
+                                                          int l, double* f, bool& fb) {
+        constexpr int un = 1 + D;
+        constexpr int t1 = 1 + (D + 1) % 3, t2 = 1 + (D + 2) % 3;
+        const int j = m + 2;
+        const double rho = 0.5 * (Wd[at<STRW>(j, 0, l)] + Wd[at<STRW>(j + 1, 0, l)]);
+        const double p4 = 0.5 * (Wd[at<STRW>(j, 4, l)] + Wd[at<STRW>(j + 1, 4, l)]);
+        const double c = sound_speed(e, rho, p4);
+        const double l4un = rho / (2.0 * c);
+        const double l0un = -l4un;
+        const double l04 = 1.0 / (2.0 * c * c);
+        const double l14 = -1.0 / (c * c);
+        const double run4 = c / rho;
+        const double run0 = -run4;
+        const double r40 = c * c;
+        double cl[5], cr[5];
+#pragma unroll
+        for (int a = 0; a < 5; a++) {
+            double ch[6];
+#pragma unroll
+            for (int s2 = 0; s2 < 6; s2++) {
+                const int row = m + s2;
+                switch (a) {
+                    case 0: ch[s2] = l0un * Wd[at<STRW>(row, un, l)] + l04 * Wd[at<STRW>(row, 4, l)]; break;
+                    case 1: ch[s2] = Wd[at<STRW>(row, 0, l)] + l14 * Wd[at<STRW>(row, 4, l)]; break;
+                    case 2: ch[s2] = Wd[at<STRW>(row, t1, l)]; break;
+                    case 3: ch[s2] = Wd[at<STRW>(row, t2, l)]; break;
+                    default: ch[s2] = l4un * Wd[at<STRW>(row, un, l)] + l04 * Wd[at<STRW>(row, 4, l)];
+                }
+            }
+            const double bl = ch[2], br = ch[3];
+            cl[a] = bl + (double)weno5z_interp<float>((float)(ch[0] - bl), (float)(ch[1] - bl), 0.0f, (float)(ch[3] - bl),
+                                                      (float)(ch[4] - bl));
+            cr[a] = br + (double)weno5z_interp<float>((float)(ch[5] - br), (float)(ch[4] - br), 0.0f, (float)(ch[2] - br),
+                                                      (float)(ch[1] - br));
+        }
+        double wl[5], wr[5];
+        wl[0] = (cl[0] + cl[1]) + cl[4];
+        wr[0] = (cr[0] + cr[1]) + cr[4];
+        wl[un] = run0 * cl[0] + run4 * cl[4];
+        wr[un] = run0 * cr[0] + run4 * cr[4];
+        wl[t1] = cl[2];
+        wr[t1] = cr[2];
+        wl[t2] = cl[3];
+        wr[t2] = cr[3];
+        wl[4] = r40 * cl[0] + r40 * cl[4];
+        wr[4] = r40 * cr[0] + r40 * cr[4];
+        fb = false;
+        if (!admissible(e, wl[0], wl[4]) || !admissible(e, wr[0], wr[4])) {
+            fb = true;
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                wl[k] = Wd[at<STRW>(j, k, l)];
+                wr[k] = Wd[at<STRW>(j + 1, k, l)];
+            }
+        }
+        hllc(e, wl, wr, un, f);
+    }
+
     // KEEP-PE two-point flux with cached ρe (C/system.rs:317-334).
     __device__ static __forceinline__ void split_flux(const double* __restrict__ W, int ra, int rb, int l, double* f) {
         constexpr int un = 1 + D;
@@ -302,26 +370,14 @@ struct Sweep {
         unsigned char* sp = smem_raw;
         double* W = reinterpret_cast<double*>(sp);
         sp += (size_t)RS * STRW * sizeof(double);
-        const RF* Wr;  // primitives read by the midpoint code
-        RF* Wf = nullptr;
-        if constexpr (MIXED && MID) {
-            Wf = reinterpret_cast<RF*>(sp);
-            sp += (size_t)RS * STR * sizeof(float);
-        }
-        RF* MF = nullptr;
+        double* MF = nullptr;  // midpoint fluxes (FP64 in both forms)
         if constexpr (MID) {
-            MF = reinterpret_cast<RF*>(sp);
-            sp += (size_t)RS * STR * sizeof(RF);
+            MF = reinterpret_cast<double*>(sp);
+            sp += (size_t)RS * STR * sizeof(double);
         }
         double* F = reinterpret_cast<double*>(sp);
         sp += (size_t)RS * STR * sizeof(double);
         double* TH = reinterpret_cast<double*>(sp);
-        if constexpr (MIXED) {
-            Wr = Wf;
-        } else {
-            Wr = reinterpret_cast<const RF*>(W);
-        }
-        constexpr int SR = MIXED ? STR : STRW;  // row stride of the ring the midpoint code reads
 
         __shared__ unsigned int s_fallback, s_limited, s_weno;
         __shared__ double s_rate[T / 32];
@@ -390,7 +446,6 @@ struct Sweep {
         // share; only the owner counts them in the statistics
         const bool tail = s0 + Ls == p.nd;
         const Eos<double> ed = Eos<double>::from(p.eos);
-        const Eos<RF> ef = Eos<RF>::from(p.eos);
         constexpr int un = 1 + D;
         const double lam = (p.ndim * dt) / dx;  // λ = ndim·dt/dx (C/solver.rs:393, C/amr.rs:1246)
         const double lam2 = 2.0 * lam;
@@ -430,7 +485,6 @@ struct Sweep {
 #pragma unroll
                         for (int k = 0; k < 5; k++) {
                             W[at<STRW>(row, k, l)] = w[k];
-                            if constexpr (MIXED && MID) Wf[at<STR>(row, k, l)] = RF(w[k]);
                         }
                         if constexpr (MODE != MODE_WENO) W[at<STRW>(row, 5, l)] = ed.rho_e(w[0], w[4]);
                         if constexpr (MODE == MODE_HYBRID) {
@@ -475,9 +529,12 @@ struct Sweep {
                         for (int ff = max(m - 4, 0); ff <= min(m, lane_len(l)); ff++) need = need || TH[slot(ff) * P + l] > 0.0;
                     }
                     if (need) {
-                        RF f[5];
+                        double f[5];
                         bool fb;
-                        midpoint<SR>(ef, Wr, m, l, f, fb);
+                        if constexpr (MIXED)
+                            midpoint_mixed(ed, W, m, l, f, fb);
+                        else
+                            midpoint<STRW>(ed, W, m, l, f, fb);
 #pragma unroll
                         for (int k = 0; k < 5; k++) MF[at<STR>(m, k, l)] = f[k];
                         if (fb && (m < lane_len(l) || lane_tail(l))) atomicAdd(&s_fallback, 1u);

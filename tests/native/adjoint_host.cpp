@@ -472,3 +472,132 @@ int adjh_line_vjp(const emg_eos* eos, const double* w, int len, int d, int ng, c
     return 0;
 }
 }  // extern "C"
+
+// ---- (study aid) the mixed form's midpoint flux on the host, variants ----
+namespace {
+// variant 0: as the device mixed sweep (FP32 avg, eigenvectors, projection,
+// WENO-Z, back-projection, HLLC); variant 1: characteristic deviations from
+// the FP64 value at row j (WENO is translation invariant), FP32 WENO on the
+// deviations, back-projection + HLLC in FP32; variant 2: as 1 with the
+// back-projection and HLLC in FP64.
+template <int D>
+void mixed_midpoint(const emg::Eos<double>& ed, const double (*w6)[5], int variant, double* f) {
+    using emg::Eos;
+    const Eos<float> ef = Eos<float>::from(emg::EosD{ed.gamma, ed.p_inf, ed.b, ed.q});
+    constexpr int un = 1 + D, t1 = 1 + (D + 1) % 3, t2 = 1 + (D + 2) % 3;
+    if (variant == 0) {
+        float w[6][5];
+        for (int s = 0; s < 6; s++)
+            for (int k = 0; k < 5; k++) w[s][k] = (float)w6[s][k];
+        float avg0 = 0.5f * (w[2][0] + w[3][0]), avg4 = 0.5f * (w[2][4] + w[3][4]);
+        float rho = avg0, c = emg::sound_speed(ef, avg0, avg4);
+        float l4un = rho / (2.f * c), l0un = -l4un, l04 = 1.f / (2.f * c * c), l14 = -1.f / (c * c);
+        float run4 = c / rho, run0 = -run4, r40 = c * c;
+        float ch[5][6];
+        for (int s = 0; s < 6; s++) {
+            ch[0][s] = l0un * w[s][un] + l04 * w[s][4];
+            ch[1][s] = w[s][0] + l14 * w[s][4];
+            ch[2][s] = w[s][t1];
+            ch[3][s] = w[s][t2];
+            ch[4][s] = l4un * w[s][un] + l04 * w[s][4];
+        }
+        float cl[5], cr[5];
+        for (int a = 0; a < 5; a++) {
+            cl[a] = emg::weno5z_interp(ch[a][0], ch[a][1], ch[a][2], ch[a][3], ch[a][4]);
+            cr[a] = emg::weno5z_interp(ch[a][5], ch[a][4], ch[a][3], ch[a][2], ch[a][1]);
+        }
+        float wl[5], wr[5];
+        wl[0] = (cl[0] + cl[1]) + cl[4];
+        wr[0] = (cr[0] + cr[1]) + cr[4];
+        wl[un] = run0 * cl[0] + run4 * cl[4];
+        wr[un] = run0 * cr[0] + run4 * cr[4];
+        wl[t1] = cl[2]; wr[t1] = cr[2]; wl[t2] = cl[3]; wr[t2] = cr[3];
+        wl[4] = r40 * cl[0] + r40 * cl[4];
+        wr[4] = r40 * cr[0] + r40 * cr[4];
+        if (!emg::admissible(ef, wl[0], wl[4]) || !emg::admissible(ef, wr[0], wr[4]))
+            for (int k = 0; k < 5; k++) { wl[k] = w[2][k]; wr[k] = w[3][k]; }
+        float ff[5];
+        emg::hllc(ef, wl, wr, un, ff);
+        for (int k = 0; k < 5; k++) f[k] = ff[k];
+        return;
+    }
+    // characteristic projection in FP64, deviations from row 2 (left) / row 3 (right)
+    double avg0 = 0.5 * (w6[2][0] + w6[3][0]), avg4 = 0.5 * (w6[2][4] + w6[3][4]);
+    double rho = avg0, c = emg::sound_speed(ed, avg0, avg4);
+    double l4un = rho / (2.0 * c), l0un = -l4un, l04 = 1.0 / (2.0 * c * c), l14 = -1.0 / (c * c);
+    double run4 = c / rho, run0 = -run4, r40 = c * c;
+    double ch[5][6];
+    for (int s = 0; s < 6; s++) {
+        ch[0][s] = l0un * w6[s][un] + l04 * w6[s][4];
+        ch[1][s] = w6[s][0] + l14 * w6[s][4];
+        ch[2][s] = w6[s][t1];
+        ch[3][s] = w6[s][t2];
+        ch[4][s] = l4un * w6[s][un] + l04 * w6[s][4];
+    }
+    double cl[5], cr[5];
+    for (int a = 0; a < 5; a++) {
+        const double bl = variant == 3 ? 0.0 : ch[a][2], br = variant == 3 ? 0.0 : ch[a][3];
+        float v[6];
+        for (int s = 0; s < 6; s++) v[s] = (float)(ch[a][s] - bl);
+        cl[a] = bl + (double)emg::weno5z_interp(v[0], v[1], v[2], v[3], v[4]);
+        for (int s = 0; s < 6; s++) v[s] = (float)(ch[a][s] - br);
+        cr[a] = br + (double)emg::weno5z_interp(v[5], v[4], v[3], v[2], v[1]);
+    }
+    double wl[5], wr[5];
+    wl[0] = (cl[0] + cl[1]) + cl[4];
+    wr[0] = (cr[0] + cr[1]) + cr[4];
+    wl[un] = run0 * cl[0] + run4 * cl[4];
+    wr[un] = run0 * cr[0] + run4 * cr[4];
+    wl[t1] = cl[2]; wr[t1] = cr[2]; wl[t2] = cl[3]; wr[t2] = cr[3];
+    wl[4] = r40 * cl[0] + r40 * cl[4];
+    wr[4] = r40 * cr[0] + r40 * cr[4];
+    if (!emg::admissible(ed, wl[0], wl[4]) || !emg::admissible(ed, wr[0], wr[4]))
+        for (int k = 0; k < 5; k++) { wl[k] = w6[2][k]; wr[k] = w6[3][k]; }
+    if (variant == 2 || variant == 3) {
+        emg::hllc(ed, wl, wr, un, f);
+        return;
+    }
+    float wlf[5], wrf[5], ff[5];
+    for (int k = 0; k < 5; k++) { wlf[k] = (float)wl[k]; wrf[k] = (float)wr[k]; }
+    emg::hllc(ef, wlf, wrf, un, ff);
+    for (int k = 0; k < 5; k++) f[k] = ff[k];
+}
+}  // namespace
+
+extern "C" {
+// Face fluxes (S6 of midpoint fluxes, no limiter) of a primitive line with the
+// midpoint flux in a mixed-precision variant (variant < 0: plain FP64).
+int adjh_mixed_line_fluxes(const emg_eos* eos, const double* w, int len, int d, int ng, int variant, double* out) {
+    emg::Eos<double> e = deos(eos);
+    const int n = len - 2 * ng;
+    std::vector<double> mf(5 * len, 0.0);
+    for (int j = ng - 3; j <= ng + n + 1; j++) {
+        const double(*w6)[5] = reinterpret_cast<const double(*)[5]>(w + 5 * (j - 2));
+        double f[5];
+        if (variant < 0) {
+            oracle::Euler<double> sys{oracle::Nasg<double>{eos->gamma, eos->p_inf, eos->b, eos->q, eos->cv}};
+            std::vector<oracle::V5<double>> wl(len);
+            for (int c = 0; c < len; c++)
+                for (int k = 0; k < 5; k++) wl[c][k] = w[5 * c + k];
+            auto m = oracle::midpoint_flux(sys, wl.data(), j, d);
+            for (int k = 0; k < 5; k++) f[k] = m.f[k];
+        } else if (d == 0) mixed_midpoint<0>(e, w6, variant, f);
+        else if (d == 1) mixed_midpoint<1>(e, w6, variant, f);
+        else mixed_midpoint<2>(e, w6, variant, f);
+        for (int k = 0; k < 5; k++) mf[5 * j + k] = f[k];
+    }
+    for (int fc = 0; fc <= n; fc++) {
+        const int i = ng - 1 + fc;
+        for (int k = 0; k < 5; k++) {
+            double acc = 0.0;
+            acc = acc + oracle::S6[0] * mf[5 * i + k];
+            acc = acc + oracle::S6[1] * mf[5 * (i + 1) + k];
+            acc = acc + oracle::S6[1] * mf[5 * (i - 1) + k];
+            acc = acc + oracle::S6[2] * mf[5 * (i + 2) + k];
+            acc = acc + oracle::S6[2] * mf[5 * (i - 2) + k];
+            out[5 * fc + k] = acc;
+        }
+    }
+    return 0;
+}
+}  // extern "C"
