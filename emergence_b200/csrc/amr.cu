@@ -134,18 +134,19 @@ struct emg_amr {
     int64_t scr_cap = 0;
     unsigned long long* det = nullptr;
     int64_t det_cap = 0;
-    DevVec<int> dmap, dleaves, dlevel, dbcleaves, dcell_slot, dtask_start;
-    DevVec<int64_t> didx, dcell_ext;
+    DevVec<int> dmap, dleaves, dlevel, dbcleaves;
+    DevVec<int64_t> didx;
     DevVec<double> ddxl;
     DevVec<CopyTask> dcopy;
     DevVec<PBox> dpbox;
     std::vector<DevVec<RBox>> drbox;  // per level
-    DevVec<RefluxTask> dreflux;
+    DevVec<RefluxFace> dreflux;
+    int rface_start[7]{};  // refluxing faces of bucket (d, side) = 2d + side: [rface_start[b], rface_start[b+1])
     DevVec<PBox> dtmp_pbox;    // one-off prediction boxes (refined children)
     DevVec<RBox> dtmp_rbox;    // one-off restriction boxes (coarsened parents)
     DevVec<double> dstage;     // host initial data of new blocks
     std::vector<int> rbox_count;
-    int ncopy = 0, npbox = 0, nbcleaves = 0, nrefcells = 0, nleaves = 0;
+    int ncopy = 0, npbox = 0, nbcleaves = 0, nleaves = 0;
     bool layout_valid = false, map_dirty = true;
     uint64_t launches = 0;
     double phase_ms[5]{};
@@ -174,16 +175,24 @@ struct emg_amr {
     }
     void insert(int l, const Key& k, int id) {
         int64_t s = slot_of(l, k);
-        if (s >= 0) map[l][s] = id;
+        if (s >= 0) {
+            map[l][s] = id;
+            map_changed.push_back(mapoff[l] + s);
+        }
         map_dirty = true;
         layout_valid = false;
     }
     void remove(int l, const Key& k) {
         int64_t s = slot_of(l, k);
-        if (s >= 0) map[l][s] = -1;
+        if (s >= 0) {
+            map[l][s] = -1;
+            map_changed.push_back(mapoff[l] + s);
+        }
         map_dirty = true;
         layout_valid = false;
     }
+    std::vector<int64_t> map_changed;  // flat map entries changed since the last upload
+    bool map_uploaded = false;
 
     // same-level neighbour keys with periodic wrap (C/amr.rs:918-947)
     std::vector<Key> neighbours(int l, const Key& idx) const {
@@ -272,15 +281,42 @@ struct emg_amr {
         return A;
     }
 
+    // Device copy of the block map: the whole map on first use, afterwards only
+    // the entries changed since (a regrid edits a few entries per refinement).
     int upload_map() {
         if (!map_dirty) return EMG_OK;
-        std::vector<int> flat;
-        for (auto& m : map) flat.insert(flat.end(), m.begin(), m.end());
-        int rc = dmap.put(flat, stream);
-        if (rc) return rc;
+        size_t total = 0;
+        for (auto& m : map) total += m.size();
+        if (!map_uploaded || map_changed.size() * 8 > total) {
+            std::vector<int> flat;
+            flat.reserve(total);
+            for (auto& m : map) flat.insert(flat.end(), m.begin(), m.end());
+            int rc = dmap.put(flat, stream);
+            if (rc) return rc;
+            map_uploaded = true;
+        } else if (!map_changed.empty()) {
+            std::sort(map_changed.begin(), map_changed.end());
+            map_changed.erase(std::unique(map_changed.begin(), map_changed.end()), map_changed.end());
+            std::vector<int64_t> pairs;
+            pairs.reserve(2 * map_changed.size());
+            for (int64_t f : map_changed) {
+                int l = 0;
+                while (l + 1 < levels && mapoff[l + 1] <= f) l++;
+                pairs.push_back(f);
+                pairs.push_back(map[l][f - mapoff[l]]);
+            }
+            int rc = dmap_edits.put(pairs, stream);
+            if (rc) return rc;
+            const int n = (int)map_changed.size();
+            map_scatter<<<(n + 255) / 256, 256, 0, stream>>>(dmap.p, dmap_edits.p, n);
+            launches++;
+            AMR_CUDA(cudaGetLastError());
+        }
+        map_changed.clear();
         map_dirty = false;
         return EMG_OK;
     }
+    DevVec<int64_t> dmap_edits;
 
     // grow the pool to hold at least n blocks, preserving block data
     int reserve(int64_t n) {
@@ -374,6 +410,18 @@ struct emg_amr {
     int run_pboxes(const PBox* dboxes, int nbox, int64_t maxcells) {
         if (!nbox) return EMG_OK;
         AmrDev A = view();
+        // one CTA per box in shared memory when the largest box stage fits
+        const size_t fused_smem = (size_t)maxcells * (2 * 5 * sizeof(double) + 1);
+        if (fused_smem <= 227 * 1024) {
+            if (!pbox_fused_ready) {
+                AMR_CUDA(cudaFuncSetAttribute(pbox_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+                pbox_fused_ready = true;
+            }
+            pbox_fused<<<nbox, 256, fused_smem, stream>>>(A, dboxes, (int)maxcells);
+            launches++;
+            AMR_CUDA(cudaGetLastError());
+            return EMG_OK;
+        }
         const dim3 gr = box_grid(maxcells, nbox);
         pbox_gather<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0]);
         for (int di = 0; di < (int)dims.size(); di++) pbox_bc<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], di);
@@ -593,79 +641,49 @@ struct emg_amr {
             rbox_count[l] = (int)rb.size();
             if ((rc = drbox[l].put(rb, stream))) return rc;
         }
-        // refluxing tasks (C/amr.rs:1327-1406), grouped by target cell in CPU order
-        std::vector<std::tuple<int, int64_t, RefluxTask>> corr;
-        for (size_t id = 0; id < blocks.size(); id++) {
-            const HBlock& b = blocks[id];
-            const int l = b.level;
-            if (!b.leaf || l + 1 >= levels) continue;
-            for (int d : dims) {
-                const int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
+        // refluxing faces (C/amr.rs:1327-1406), bucketed by (d, side) in the reference's order
+        std::vector<RefluxFace> rfaces;
+        for (int bucket = 0; bucket < 6; bucket++) {
+            rface_start[bucket] = (int)rfaces.size();
+            const int d = bucket / 2, side = bucket % 2;
+            if (!act[d]) continue;
+            const int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
+            for (size_t id = 0; id < blocks.size(); id++) {
+                const HBlock& b = blocks[id];
+                const int l = b.level;
+                if (!b.leaf || l + 1 >= levels) continue;
                 const int64_t nbk = nb0[d] << l;
-                for (int side = 0; side < 2; side++) {
-                    Key nk = b.idx;
-                    nk[d] += side == 1 ? 1 : -1;
-                    if (nk[d] < 0 || nk[d] >= nbk) {
-                        if (bckind(d, side) != EMG_BC_PERIODIC) continue;
-                        nk[d] = erem(nk[d], nbk);
-                    }
-                    const int nj = get(l, nk);
-                    if (!(nj >= 0 && !blocks[nj].leaf)) continue;
-                    for (int a = 0; a < bd[e0]; a++)
-                        for (int bb = 0; bb < bd[e1]; bb++) {
-                            RefluxTask tk{};
-                            tk.slot = (int)id;
-                            tk.d = d;
-                            tk.side = side;
-                            tk.pen = a * bd[e1] + bb;
-                            tk.dx = dxl[3 * l + d];
-                            for (int fa = 0; fa < (act[e0] ? 2 : 1); fa++)
-                                for (int fb = 0; fb < (act[e1] ? 2 : 1); fb++) {
-                                    const int64_t ga = 2 * (b.idx[e0] * bd[e0] + a) + fa;
-                                    const int64_t gb = 2 * (b.idx[e1] * bd[e1] + bb) + fb;
-                                    Key ck = nk;
-                                    ck[d] = 2 * nk[d] + (side == 1 ? 0 : 1);
-                                    ck[e0] = act[e0] ? ediv(ga, bd[e0]) : 0;
-                                    ck[e1] = act[e1] ? ediv(gb, bd[e1]) : 0;
-                                    const int cid = get(l + 1, ck);
-                                    if (cid < 0 || !blocks[cid].leaf) continue;
-                                    const int la = act[e0] ? (int)erem(ga, bd[e0]) : 0;
-                                    const int lb = act[e1] ? (int)erem(gb, bd[e1]) : 0;
-                                    tk.fslot[tk.nfine] = cid;
-                                    tk.fpen[tk.nfine] = la * bd[e1] + lb;
-                                    tk.nfine++;
-                                }
-                            if (!tk.nfine) continue;
-                            int64_t c[3];
-                            c[d] = side == 1 ? bd[d] - 1 : 0;
-                            c[e0] = a;
-                            c[e1] = bb;
-                            const int64_t ce = ((c[0] + gof[0]) * ext[1] + (c[1] + gof[1])) * ext[2] + (c[2] + gof[2]);
-                            corr.push_back({(int)id, ce, tk});
-                        }
+                Key nk = b.idx;
+                nk[d] += side == 1 ? 1 : -1;
+                if (nk[d] < 0 || nk[d] >= nbk) {
+                    if (bckind(d, side) != EMG_BC_PERIODIC) continue;
+                    nk[d] = erem(nk[d], nbk);
                 }
+                const int nj = get(l, nk);
+                if (!(nj >= 0 && !blocks[nj].leaf)) continue;
+                RefluxFace rf{};
+                rf.slot = (int)id;
+                rf.d = d;
+                rf.side = side;
+                rf.dx = dxl[3 * l + d];
+                for (int qa = 0; qa < 2; qa++)
+                    for (int qb = 0; qb < 2; qb++) {
+                        rf.fine[qa][qb] = -1;
+                        if ((qa && !act[e0]) || (qb && !act[e1])) continue;
+                        Key ck = nk;
+                        ck[d] = 2 * nk[d] + (side == 1 ? 0 : 1);
+                        ck[e0] = act[e0] ? 2 * b.idx[e0] + qa : 0;
+                        ck[e1] = act[e1] ? 2 * b.idx[e1] + qb : 0;
+                        const int cid = get(l + 1, ck);
+                        if (cid >= 0 && blocks[cid].leaf) rf.fine[qa][qb] = cid;
+                    }
+                rfaces.push_back(rf);
             }
         }
-        std::stable_sort(corr.begin(), corr.end(), [](const auto& x, const auto& y) {
-            return std::get<0>(x) != std::get<0>(y) ? std::get<0>(x) < std::get<0>(y) : std::get<1>(x) < std::get<1>(y);
-        });
-        std::vector<int> cslot, tstart;
-        std::vector<int64_t> cext;
-        std::vector<RefluxTask> tasks;
-        for (size_t i = 0; i < corr.size(); i++) {
-            if (i == 0 || std::get<0>(corr[i]) != std::get<0>(corr[i - 1]) || std::get<1>(corr[i]) != std::get<1>(corr[i - 1])) {
-                cslot.push_back(std::get<0>(corr[i]));
-                cext.push_back(std::get<1>(corr[i]));
-                tstart.push_back((int)tasks.size());
-            }
-            tasks.push_back(std::get<2>(corr[i]));
-        }
-        tstart.push_back((int)tasks.size());
-        nrefcells = (int)cslot.size();
+        rface_start[6] = (int)rfaces.size();
         if ((rc = dleaves.put(leaves, stream)) || (rc = dlevel.put(lvl, stream)) || (rc = didx.put(idx, stream)) ||
             (rc = dbcleaves.put(bcl, stream)) || (rc = dcopy.put(copies, stream)) || (rc = dpbox.put(pboxes, stream)) ||
-            (rc = dcell_slot.put(cslot, stream)) || (rc = dcell_ext.put(cext, stream)) ||
-            (rc = dtask_start.put(tstart, stream)) || (rc = dreflux.put(tasks, stream)))
+            (rc = dreflux.put(rfaces, stream)))
             return rc;
         ncopy = (int)copies.size();
         npbox = (int)pboxes.size();
@@ -676,6 +694,7 @@ struct emg_amr {
         return EMG_OK;
     }
     int64_t pbox_max = 0;
+    bool pbox_fused_ready = false;  // dynamic shared-memory opt-in of pbox_fused (per handle and device)
 
     // ghost-extended boxes of every leaf (fill_scratch, C/amr.rs:1113-1221)
     int fill_ghosts() {
@@ -766,11 +785,14 @@ struct emg_amr {
         cudaEventRecord(ev[2], stream);
         if ((rc = sweeps(stage))) return rc;
         cudaEventRecord(ev[3], stream);
-        if (nrefcells) {
+        {
             AmrDev A = view();
-            reflux_kernel<<<(nrefcells + 255) / 256, 256, 0, stream>>>(A, rhs, face, npen, dcell_slot.p, dcell_ext.p,
-                                                                      dtask_start.p, dreflux.p, nrefcells);
-            launches++;
+            for (int bucket = 0; bucket < 6; bucket++) {
+                const int nf = rface_start[bucket + 1] - rface_start[bucket];
+                if (!nf) continue;
+                reflux_faces<<<nf, 256, 0, stream>>>(A, rhs, face, npen, dreflux.p + rface_start[bucket]);
+                launches++;
+            }
             AMR_CUDA(cudaGetLastError());
         }
         cudaEventRecord(ev[4], stream);
@@ -1234,13 +1256,13 @@ struct emg_amr {
         }
         cudaFree(det);
         dmap.release();
+        dmap_edits.release();
         dleaves.release();
         dlevel.release();
         dbcleaves.release();
-        dcell_slot.release();
-        dtask_start.release();
+
         didx.release();
-        dcell_ext.release();
+
         ddxl.release();
         dcopy.release();
         dpbox.release();

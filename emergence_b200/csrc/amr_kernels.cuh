@@ -28,29 +28,33 @@ __device__ __forceinline__ void rbox_size(const AmrDev& A, const RBox& b, int np
 }
 
 // gather_box(l−1) inner cells by sampling; cells beyond a non-periodic
-// boundary are left invalid for bc_box (amr.rs:508-530)
+// boundary are left invalid for bc_box (amr.rs:508-530). `off` is the box's
+// cell offset in buf/ok.
+__device__ __forceinline__ void pbox_gather_cell(const AmrDev& A, const PBox& b, int64_t q, double* buf,
+                                                 unsigned char* ok, int64_t off) {
+    const int l = b.l - 1;
+    int64_t c[3];
+    box_coord(q, b.csz, c);
+    int64_t g[3] = {b.cmin[0] + c[0], b.cmin[1] + c[1], b.cmin[2] + c[2]};
+    bool out = false;
+    for (int i = 0; i < A.ndims; i++) {
+        const int d = A.dims[i];
+        const int64_t nn = amr_nlevel(A, l, d);
+        if ((g[d] < 0 || g[d] >= nn) && A.bc[d][g[d] >= nn ? 1 : 0] != EMG_BC_PERIODIC) out = true;
+    }
+    double* v = buf + (off + q) * 5;
+    if (out) {
+        ok[off + q] = 0;
+    } else {
+        amr_sample(A, l, g, v, 0);
+        ok[off + q] = 1;
+    }
+}
 __global__ void pbox_gather(const AmrDev A, const PBox* __restrict__ boxes, double* buf, unsigned char* ok) {
     const PBox b = boxes[blockIdx.x];
-    const int l = b.l - 1;
     const int64_t n = (int64_t)b.csz[0] * b.csz[1] * b.csz[2];
-    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
-        int64_t c[3];
-        box_coord(q, b.csz, c);
-        int64_t g[3] = {b.cmin[0] + c[0], b.cmin[1] + c[1], b.cmin[2] + c[2]};
-        bool out = false;
-        for (int i = 0; i < A.ndims; i++) {
-            const int d = A.dims[i];
-            const int64_t nn = amr_nlevel(A, l, d);
-            if ((g[d] < 0 || g[d] >= nn) && A.bc[d][g[d] >= nn ? 1 : 0] != EMG_BC_PERIODIC) out = true;
-        }
-        double* v = buf + (b.off + q) * 5;
-        if (out) {
-            ok[b.off + q] = 0;
-        } else {
-            amr_sample(A, l, g, v, 0);
-            ok[b.off + q] = 1;
-        }
-    }
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
+        pbox_gather_cell(A, b, q, buf, ok, b.off);
 }
 
 // bc_box sweep along active axis dims[di] over a box at level l with global
@@ -103,58 +107,101 @@ __global__ void pbox_bc(const AmrDev A, const PBox* __restrict__ boxes, double* 
 }
 
 // cells still invalid after bc_box are sampled (amr.rs:531-542)
+__device__ __forceinline__ void pbox_fallback_cell(const AmrDev& A, const PBox& b, int64_t q, double* buf,
+                                                   unsigned char* ok, int64_t off) {
+    if (ok[off + q]) return;
+    int64_t c[3];
+    box_coord(q, b.csz, c);
+    const int64_t g[3] = {b.cmin[0] + c[0], b.cmin[1] + c[1], b.cmin[2] + c[2]};
+    amr_sample(A, b.l - 1, g, buf + (off + q) * 5, 0);
+    ok[off + q] = 1;
+}
 __global__ void pbox_fallback(const AmrDev A, const PBox* __restrict__ boxes, double* buf, unsigned char* ok) {
     const PBox b = boxes[blockIdx.x];
     const int64_t n = (int64_t)b.csz[0] * b.csz[1] * b.csz[2];
-    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
-        if (ok[b.off + q]) continue;
-        int64_t c[3];
-        box_coord(q, b.csz, c);
-        const int64_t g[3] = {b.cmin[0] + c[0], b.cmin[1] + c[1], b.cmin[2] + c[2]};
-        amr_sample(A, b.l - 1, g, buf + (b.off + q) * 5, 0);
-        ok[b.off + q] = 1;
-    }
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
+        pbox_fallback_cell(A, b, q, buf, ok, b.off);
 }
 
-// one separable 6-point prediction pass along dims[di] (amr.rs:560-583)
+// one separable 6-point prediction pass along dims[di] (amr.rs:560-583): output
+// cell q of the box after di+1 passes from the box after di passes
+__device__ __forceinline__ void pbox_pass_cell(const AmrDev& A, const PBox& b, int di, const int* si, const int* so,
+                                               int64_t q, const double* in, double* outb, int64_t off) {
+    const int d = A.dims[di];
+    int64_t c[3];
+    box_coord(q, so, c);
+    const int64_t f = b.fmin[d] + c[d];
+    const int par = (int)amr_erem(f, 2);
+    const int64_t base = amr_ediv(f, 2) + (par == 1 ? -2 : -3) - b.cmin[d];
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int kk = 0; kk < 6; kk++) {
+        int64_t sc[3] = {c[0], c[1], c[2]};
+        sc[d] = base + kk;
+        const double* v = in + (off + box_index(sc, si)) * 5;
+        const double w = A.wp[par][kk];
+        for (int k = 0; k < 5; k++) acc[k] = acc[k] + w * v[k];
+    }
+    double* o = outb + (off + q) * 5;
+    for (int k = 0; k < 5; k++) o[k] = acc[k];
+}
 __global__ void pbox_pass(const AmrDev A, const PBox* __restrict__ boxes, const double* in, double* outb, int di) {
     const PBox b = boxes[blockIdx.x];
-    const int d = A.dims[di];
     int si[3], so[3];
     pbox_size(A, b, di, si);
     pbox_size(A, b, di + 1, so);
     const int64_t n = (int64_t)so[0] * so[1] * so[2];
-    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
-        int64_t c[3];
-        box_coord(q, so, c);
-        const int64_t f = b.fmin[d] + c[d];
-        const int par = (int)amr_erem(f, 2);
-        const int64_t base = amr_ediv(f, 2) + (par == 1 ? -2 : -3) - b.cmin[d];
-        double acc[5] = {0, 0, 0, 0, 0};
-        for (int kk = 0; kk < 6; kk++) {
-            int64_t sc[3] = {c[0], c[1], c[2]};
-            sc[d] = base + kk;
-            const double* v = in + (b.off + box_index(sc, si)) * 5;
-            const double w = A.wp[par][kk];
-            for (int k = 0; k < 5; k++) acc[k] = acc[k] + w * v[k];
-        }
-        double* o = outb + (b.off + q) * 5;
-        for (int k = 0; k < 5; k++) o[k] = acc[k];
-    }
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
+        pbox_pass_cell(A, b, di, si, so, q, in, outb, b.off);
 }
 
 // write the predicted fine box into its target block
+__device__ __forceinline__ void pbox_scatter_cell(const AmrDev& A, const PBox& b, int64_t q, const double* in,
+                                                  int64_t off) {
+    double* u = A.u + (int64_t)b.slot * A.bcell;
+    int64_t c[3];
+    box_coord(q, b.fsz, c);
+    const int64_t cell = ((b.t0[0] + c[0]) * A.ext[1] + (b.t0[1] + c[1])) * A.ext[2] + (b.t0[2] + c[2]);
+    const double* v = in + (off + q) * 5;
+    for (int k = 0; k < 5; k++) u[(int64_t)k * A.ntot + cell] = v[k];
+}
 __global__ void pbox_scatter(const AmrDev A, const PBox* __restrict__ boxes, const double* in) {
     const PBox b = boxes[blockIdx.x];
     const int64_t n = (int64_t)b.fsz[0] * b.fsz[1] * b.fsz[2];
-    double* u = A.u + (int64_t)b.slot * A.bcell;
-    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
-        int64_t c[3];
-        box_coord(q, b.fsz, c);
-        const int64_t cell = ((b.t0[0] + c[0]) * A.ext[1] + (b.t0[1] + c[1])) * A.ext[2] + (b.t0[2] + c[2]);
-        const double* v = in + (b.off + q) * 5;
-        for (int k = 0; k < 5; k++) u[(int64_t)k * A.ntot + cell] = v[k];
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
+        pbox_scatter_cell(A, b, q, in, b.off);
+}
+
+// The whole prediction pipeline of one box in shared memory (one CTA per
+// box): gather, boundary fill per active axis, fallback sampling, one
+// separable pass per active axis (ping-pong) and the scatter, with the same
+// per-cell arithmetic as the multi-launch pipeline above. `cap` is the
+// largest box stage in cells; dynamic shared memory 2·cap·5 doubles + cap bytes.
+__global__ void __launch_bounds__(256) pbox_fused(const AmrDev A, const PBox* __restrict__ boxes, int cap) {
+    extern __shared__ __align__(16) double pb_smem[];
+    double* bufs[2] = {pb_smem, pb_smem + (size_t)cap * 5};
+    unsigned char* ok = reinterpret_cast<unsigned char*>(pb_smem + (size_t)2 * cap * 5);
+    const PBox b = boxes[blockIdx.x];
+    const int64_t nc = (int64_t)b.csz[0] * b.csz[1] * b.csz[2];
+    for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) pbox_gather_cell(A, b, q, bufs[0], ok, 0);
+    __syncthreads();
+    for (int di = 0; di < A.ndims; di++) {
+        for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) bc_cell(A, b.l - 1, b.cmin, b.csz, q, di, bufs[0], ok, 0);
+        __syncthreads();
     }
+    for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) pbox_fallback_cell(A, b, q, bufs[0], ok, 0);
+    __syncthreads();
+    int cur = 0;
+    for (int di = 0; di < A.ndims; di++) {
+        int si[3], so[3];
+        pbox_size(A, b, di, si);
+        pbox_size(A, b, di + 1, so);
+        const int64_t n = (int64_t)so[0] * so[1] * so[2];
+        for (int64_t q = threadIdx.x; q < n; q += blockDim.x) pbox_pass_cell(A, b, di, si, so, q, bufs[cur], bufs[1 - cur], 0);
+        __syncthreads();
+        cur = 1 - cur;
+    }
+    const int64_t nf = (int64_t)b.fsz[0] * b.fsz[1] * b.fsz[2];
+    for (int64_t q = threadIdx.x; q < nf; q += blockDim.x) pbox_scatter_cell(A, b, q, bufs[cur], 0);
 }
 
 // fine patch of a restriction box with validity (amr.rs:632-663)
@@ -365,37 +412,57 @@ __global__ void ghost_bc(const AmrDev A, const int* __restrict__ leaves, const i
 // Refluxing (amr.rs:1327-1406): one thread per corrected coarse cell applies
 // its corrections in the CPU's order. A task names the coarse face (slot, d,
 // side, pencil) and up to four fine faces.
-struct RefluxTask {
-    int slot, d, side, pen;
-    int nfine;
-    int fslot[4], fpen[4];
+// (flat index, block id) edits of the device block map
+__global__ void map_scatter(int* map, const int64_t* __restrict__ pairs, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) map[pairs[2 * i]] = (int)pairs[2 * i + 1];
+}
+
+// One coarse face of a leaf whose same-level neighbour is refined
+// (reflux, amr.rs:1327-1406): fine[qa][qb] are the leaf children of that
+// neighbour covering quadrant (qa, qb) of the face (−1: none).
+struct RefluxFace {
+    int slot, d, side;
+    int fine[2][2];
     double dx;
 };
-__global__ void reflux_kernel(const AmrDev A, double* rhs, const double* __restrict__ face, int npen,
-                              const int* __restrict__ cell_slot, const int64_t* __restrict__ cell_ext,
-                              const int* __restrict__ task_start, const RefluxTask* __restrict__ tasks, int ncells) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ncells) return;
-    double* r = rhs + (int64_t)cell_slot[i] * A.bcell + cell_ext[i];
-    double acc[5];
-    for (int k = 0; k < 5; k++) acc[k] = r[(int64_t)k * A.ntot];
-    for (int t = task_start[i]; t < task_start[i + 1]; t++) {
-        const RefluxTask tk = tasks[t];
+// Corrections of every face of one (d, side) bucket: one CTA per face, one
+// thread per face pen. Each cell receives at most one correction per bucket,
+// and the buckets run in the reference's (d, side) order, so every cell sums
+// its corrections in the reference's order.
+__global__ void reflux_faces(const AmrDev A, double* rhs, const double* __restrict__ face, int npen,
+                             const RefluxFace* __restrict__ tasks) {
+    const RefluxFace tk = tasks[blockIdx.x];
+    const int d = tk.d;
+    const int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
+    const int b0 = A.bd[e0], b1 = A.bd[e1];
+    for (int pen = threadIdx.x; pen < b0 * b1; pen += blockDim.x) {
+        const int a = pen / b1, bb = pen % b1;
         double sum[5] = {0, 0, 0, 0, 0};
         double cnt = 0.0;
-        for (int f = 0; f < tk.nfine; f++) {
-            const double* fv = face + ((((int64_t)tk.fslot[f] * 3 + tk.d) * 2 + (1 - tk.side)) * 5) * npen + tk.fpen[f];
-            for (int k = 0; k < 5; k++) sum[k] = sum[k] + fv[(int64_t)k * npen];
-            cnt = cnt + 1.0;
-        }
-        const double* fc = face + ((((int64_t)tk.slot * 3 + tk.d) * 2 + tk.side) * 5) * npen + tk.pen;
+        for (int fa = 0; fa < (A.act[e0] ? 2 : 1); fa++)
+            for (int fb = 0; fb < (A.act[e1] ? 2 : 1); fb++) {
+                const int qa = A.act[e0] ? (2 * a + fa) / b0 : 0, qb = A.act[e1] ? (2 * bb + fb) / b1 : 0;
+                const int cid = tk.fine[qa][qb];
+                if (cid < 0) continue;
+                const int la = A.act[e0] ? (2 * a + fa) % b0 : 0, lb = A.act[e1] ? (2 * bb + fb) % b1 : 0;
+                const double* fv = face + ((((int64_t)cid * 3 + d) * 2 + (1 - tk.side)) * 5) * npen + la * b1 + lb;
+                for (int k = 0; k < 5; k++) sum[k] = sum[k] + fv[(int64_t)k * npen];
+                cnt = cnt + 1.0;
+            }
+        if (cnt == 0.0) continue;
+        const double* fc = face + ((((int64_t)tk.slot * 3 + d) * 2 + tk.side) * 5) * npen + pen;
+        int64_t c[3];
+        c[d] = tk.side == 1 ? A.bd[d] - 1 : 0;
+        c[e0] = a;
+        c[e1] = bb;
+        double* r = rhs + (int64_t)tk.slot * A.bcell + amr_cell(A, c);
         for (int k = 0; k < 5; k++) {
             const double df = sum[k] / cnt - fc[(int64_t)k * npen];
             const double dr = tk.side == 1 ? -df / tk.dx : df / tk.dx;
-            acc[k] = acc[k] + dr;
+            r[(int64_t)k * A.ntot] = r[(int64_t)k * A.ntot] + dr;
         }
     }
-    for (int k = 0; k < 5; k++) r[(int64_t)k * A.ntot] = acc[k];
 }
 
 // SSP-RK3 stage update of the leaves (amr.rs:1476-1498) and, after the third
