@@ -691,6 +691,7 @@ struct emg_amr {
         pbox_max = pmax;
         if ((rc = scratch(std::max(poff, rneed)))) return rc;
         layout_valid = true;
+        layout_gen++;
         return EMG_OK;
     }
     int64_t pbox_max = 0;
@@ -775,16 +776,15 @@ struct emg_amr {
     }
 
     int compute_rhs(int stage) {
-        cudaEvent_t ev[5];
-        for (auto& e : ev) cudaEventCreate(&e);
-        cudaEventRecord(ev[0], stream);
+        cudaEvent_t* ev = stage_ev[stage - 1];
+        record_ev(ev[0]);
         int rc = restrict_all();
         if (rc) return rc;
-        cudaEventRecord(ev[1], stream);
+        record_ev(ev[1]);
         if ((rc = fill_ghosts())) return rc;
-        cudaEventRecord(ev[2], stream);
+        record_ev(ev[2]);
         if ((rc = sweeps(stage))) return rc;
-        cudaEventRecord(ev[3], stream);
+        record_ev(ev[3]);
         {
             AmrDev A = view();
             for (int bucket = 0; bucket < 6; bucket++) {
@@ -795,25 +795,41 @@ struct emg_amr {
             }
             AMR_CUDA(cudaGetLastError());
         }
-        cudaEventRecord(ev[4], stream);
-        pending.push_back({ev[0], ev[1], ev[2], ev[3], ev[4]});
+        record_ev(ev[4]);
+        record_ev(ev[5]);  // start of the RK update (rk follows)
         return EMG_OK;
     }
-    std::vector<std::array<cudaEvent_t, 5>> pending;
+    // per stage: [restrict, ghosts, fluxes, reflux, rk start, rk end] events,
+    // created once (a captured step graph records into the same events)
+    cudaEvent_t stage_ev[3][7]{};
+    bool stage_pending = false;
+    // external records: inside a step capture they become event-record nodes
+    // of the graph, so replays record the events too
+    bool capturing = false;
+    void record_ev(cudaEvent_t e) {
+        if (capturing)
+            cudaEventRecordWithFlags(e, stream, cudaEventRecordExternal);
+        else
+            cudaEventRecord(e, stream);
+    }
+    int make_events() {
+        for (auto& st : stage_ev)
+            for (auto& e : st)
+                if (!e) AMR_CUDA(cudaEventCreate(&e));
+        return EMG_OK;
+    }
     void collect_times() {
-        for (auto& e : pending) {
-            float a = 0, b = 0, c = 0, d = 0;
-            cudaEventElapsedTime(&a, e[0], e[1]);
-            cudaEventElapsedTime(&b, e[1], e[2]);
-            cudaEventElapsedTime(&c, e[2], e[3]);
-            cudaEventElapsedTime(&d, e[3], e[4]);
-            phase_ms[0] += a;
-            phase_ms[1] += b;
-            phase_ms[2] += c;
-            phase_ms[3] += d;
-            for (auto x : e) cudaEventDestroy(x);
+        if (!stage_pending) return;
+        for (auto& e : stage_ev) {
+            float t[6] = {0, 0, 0, 0, 0, 0};
+            for (int i = 0; i < 6; i++) cudaEventElapsedTime(&t[i], e[i], e[i + 1]);
+            phase_ms[0] += t[0];
+            phase_ms[1] += t[1];
+            phase_ms[2] += t[2];
+            phase_ms[3] += t[3] + t[5];  // reflux + RK update
         }
-        pending.clear();
+        cudaGetLastError();  // timing queries never leave an error behind
+        stage_pending = false;
     }
 
     int rk(int stage) {
@@ -822,6 +838,68 @@ struct emg_amr {
             A, u0, rhs, dleaves.p, dlevel.p, ddxl.p, stage, ctl);
         launches++;
         AMR_CUDA(cudaGetLastError());
+        record_ev(stage_ev[stage - 1][6]);
+        return EMG_OK;
+    }
+
+    // the three stages of one step (the work a step graph holds)
+    int step_body() {
+        for (int s = 1; s <= 3; s++) {
+            int rc = compute_rhs(s);
+            if (rc) return rc;
+            if ((rc = rk(s))) return rc;
+        }
+        return EMG_OK;
+    }
+
+    // ---- CUDA graph of a step: between regrids the launch sequence of a step
+    // (every kernel, its grid and its arguments) is fixed, so the first step
+    // after a layout change runs eagerly, the second is captured into a graph
+    // and later steps replay it; dt reaches the kernels through the control
+    // block, copied in before each launch.
+    cudaGraphExec_t step_exec = nullptr;
+    uint64_t layout_gen = 0, graph_gen = 0, eager_gen = 0;
+    uint64_t graph_launches = 0;
+    bool use_graph = true;
+    void drop_graph() {
+        if (step_exec) cudaGraphExecDestroy(step_exec);
+        step_exec = nullptr;
+    }
+    int run_step_body() {
+        if (!use_graph) return step_body();
+        if (step_exec && graph_gen == layout_gen) {
+            AMR_CUDA(cudaGraphLaunch(step_exec, stream));
+            launches += graph_launches;
+            return EMG_OK;
+        }
+        drop_graph();
+        if (eager_gen != layout_gen) {  // first step with this layout: eager (sets up kernels)
+            eager_gen = layout_gen;
+            return step_body();
+        }
+        AMR_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        const uint64_t l0 = launches;
+        capturing = true;
+        int rc = step_body();
+        capturing = false;
+        cudaGraph_t gph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(stream, &gph);
+        graph_launches = launches - l0;
+        launches = l0;
+        if (rc) {
+            if (gph) cudaGraphDestroy(gph);
+            return rc;
+        }
+        if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("step capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&step_exec, gph, 0);
+        cudaGraphDestroy(gph);
+        if (e != cudaSuccess) {
+            step_exec = nullptr;
+            return set_error(EMG_ERR_CUDA, std::string("step graph: ") + cudaGetErrorString(e));
+        }
+        graph_gen = layout_gen;
+        AMR_CUDA(cudaGraphLaunch(step_exec, stream));
+        launches += graph_launches;
         return EMG_OK;
     }
 
@@ -1073,16 +1151,9 @@ struct emg_amr {
         ctl_host->done = 0;
         ctl_host->rate_bits = 0;
         AMR_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice, stream));
-        for (int s = 1; s <= 3; s++) {
-            if ((rc = compute_rhs(s))) return rc;
-            cudaEvent_t a, b;
-            cudaEventCreate(&a);
-            cudaEventCreate(&b);
-            cudaEventRecord(a, stream);
-            if ((rc = rk(s))) return rc;
-            cudaEventRecord(b, stream);
-            rk_events.push_back({a, b});
-        }
+        if ((rc = make_events())) return rc;
+        if ((rc = run_step_body())) return rc;
+        stage_pending = true;
         uint64_t f = 0;
         for (int d : dims) f += (uint64_t)nleaves * (bcells() / bd[d]) * (bd[d] + 1);
         faces += 3 * f;
@@ -1090,14 +1161,6 @@ struct emg_amr {
         AMR_CUDA(cudaMemcpyAsync(ctl_host, ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, stream));
         AMR_CUDA(cudaStreamSynchronize(stream));
         collect_times();
-        for (auto& e : rk_events) {
-            float ms = 0;
-            cudaEventElapsedTime(&ms, e.first, e.second);
-            phase_ms[3] += ms;
-            cudaEventDestroy(e.first);
-            cudaEventDestroy(e.second);
-        }
-        rk_events.clear();
         rate_valid = true;
         t += dt;
         steps += 1;
@@ -1124,7 +1187,6 @@ struct emg_amr {
         if (e) return set_error(EMG_ERR_UNFILLABLE, "AMR ghost cell without a source (prediction depth or box)");
         return EMG_OK;
     }
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> rk_events;
 
     int dt_cfl(double* dt) {
         if (!rate_valid) {
@@ -1243,6 +1305,10 @@ struct emg_amr {
     void release() {
         if (stream) cudaStreamSynchronize(stream);
         collect_times();
+        drop_graph();
+        for (auto& st : stage_ev)
+            for (auto& e : st)
+                if (e) cudaEventDestroy(e);
         cudaFree(u);
         cudaFree(u0);
         cudaFree(rhs);
