@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg of the uniform workload")
+    ap.add_argument("--no-autotune", action="store_true", help="uniform workload: use the planned sweep shapes")
     ap.add_argument("--workload", default="uniform", choices=["uniform", "amr", "batch", "adjoint", "batch_adjoint"],
                     help="uniform: 3-D explosion 256^3; amr: 3-D shock-bubble on block AMR (base 128^3, 3 levels); "
                          "batch: 4096 independent 1-D Riemann problems; adjoint: discrete adjoint of the 2-D "
@@ -173,7 +174,8 @@ def run_ours(args, world, rank, local):
     state_bytes = u.nbytes
 
     # ---- device-resident timing (value)
-    g = GpuSolver(sys_, mesh, u, bc=bc, mode=FluxMode.Weno, cfl=0.5, precision=prec)
+    tune = not args.no_autotune
+    g = GpuSolver(sys_, mesh, u, bc=bc, mode=FluxMode.Weno, cfl=0.5, precision=prec, autotune=tune)
     g.advance(args.warmup)
     g.synchronize()
     stream = torch.cuda.ExternalStream(g.stream())
@@ -231,7 +233,7 @@ def run_ours(args, world, rank, local):
     # ---- mixed-precision form (FP32 flux, FP64 state): same workload and steps
     mixed = None
     if not args.no_mixed and prec == Precision.F64:
-        gm = GpuSolver(sys_, mesh, u, bc=bc, mode=FluxMode.Weno, cfl=0.5, precision=Precision.Mixed)
+        gm = GpuSolver(sys_, mesh, u, bc=bc, mode=FluxMode.Weno, cfl=0.5, precision=Precision.Mixed, autotune=tune)
         gm.advance(args.warmup)
         gm.synchronize()
         sm = torch.cuda.ExternalStream(gm.stream())
@@ -260,7 +262,7 @@ def run_ours(args, world, rank, local):
         host = np.ascontiguousarray(u)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        h = GpuSolver(sys_, mesh, host, bc=bc, mode=FluxMode.Weno, cfl=0.5, precision=prec)
+        h = GpuSolver(sys_, mesh, host, bc=bc, mode=FluxMode.Weno, cfl=0.5, precision=prec, autotune=tune)
         h.advance(args.steps)
         out = h.download()
         el = time.perf_counter() - t0

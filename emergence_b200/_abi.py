@@ -45,7 +45,7 @@ INIT_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.c_int64, C.POIN
 
 class EmgOpts(C.Structure):
     _fields_ = [("cfl", C.c_double), ("tol", C.c_double), ("mode", C.c_int32), ("positivity", C.c_int32),
-                ("precision", C.c_int32), ("reserved", C.c_int32)]
+                ("precision", C.c_int32), ("flags", C.c_int32)]
 
 
 EMG_K_COUNT = 5

@@ -17,6 +17,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -384,6 +386,12 @@ struct ProfScope {
     }
 };
 
+// launch grid of the sweep along d for P pencils per CTA and segments of seg cells
+dim3 sweep_grid(const emg_uniform* h, int d, int P, int64_t seg) {
+    const int64_t nd = h->mesh.n[d], nl = h->mesh.n[h->lane_axis[d]], nother = h->mesh.n[h->other_axis[d]];
+    return dim3((unsigned)((nl + P - 1) / P), (unsigned)((nd + seg - 1) / seg), (unsigned)nother);
+}
+
 void plan_sweeps(emg_uniform* h) {
     for (int d = 0; d < 3; d++) {
         if (!h->active[d]) continue;
@@ -446,6 +454,8 @@ int launch_ghosts(emg_uniform* h, double* arr) {
     return EMG_OK;
 }
 
+int launch_axis(emg_uniform* h, int stage, int d, double* in, bool first, bool last);
+
 int launch_stage(emg_uniform* h, int stage) {
     double* in = stage == 1 ? h->u : (stage == 2 ? h->sa : h->sb);
     int rc = launch_ghosts(h, in);
@@ -458,6 +468,14 @@ int launch_stage(emg_uniform* h, int stage) {
         }
     for (int d = 0; d < 3; d++) {
         if (!h->active[d]) continue;
+        if ((rc = launch_axis(h, stage, d, in, d == first_axis, d == last_axis))) return rc;
+    }
+    return EMG_OK;
+}
+
+// one fused sweep of stage `stage` along d with the planned launch shape
+int launch_axis(emg_uniform* h, int stage, int d, double* in, bool first, bool last) {
+    {
         SweepParams p{};
         p.uin = in;
         p.rhs = h->rhs;
@@ -476,8 +494,8 @@ int launch_stage(emg_uniform* h, int stage) {
         p.d = d;
         p.seg = h->sweepSeg[d];
         p.lw = h->sweepP[d];
-        p.first = d == first_axis;
-        p.last = d == last_axis;
+        p.first = first;
+        p.last = last;
         p.stage = stage;
         p.rows_contig = p.sd == 1;
         p.dx = h->mesh.dx[d];
@@ -512,6 +530,99 @@ int launch_stage(emg_uniform* h, int stage) {
                             : sweep_launch_f64(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream);
         if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("sweep launch: ") + cudaGetErrorString(e));
     }
+    return EMG_OK;
+}
+
+// Project-written autotuner of the sweep launch shape: per active axis, every
+// candidate (pencils per CTA P ∈ {8, 16, 32}, segment length nd, nd/2, nd/4)
+// sweeps the current state once untimed and three times timed (residual only:
+// no RK epilogue), and the fastest is kept. A sweep's results do not depend on
+// its launch shape (each cell's arithmetic is the same), so tuning changes
+// speed only. Shapes are cached per (mesh extents, flux mode, precision).
+struct TuneKey {
+    int64_t n[3];
+    int mode, precision;
+    bool operator<(const TuneKey& o) const {
+        for (int d = 0; d < 3; d++)
+            if (n[d] != o.n[d]) return n[d] < o.n[d];
+        return mode != o.mode ? mode < o.mode : precision < o.precision;
+    }
+};
+struct TuneVal {
+    int P[3];
+    int seg[3];
+};
+
+int autotune_sweeps(emg_uniform* h) {
+    static std::mutex mu;
+    static std::map<TuneKey, TuneVal> cache;
+    TuneKey key{{h->mesh.n[0], h->mesh.n[1], h->mesh.n[2]}, h->opts.mode, h->opts.precision};
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            for (int d = 0; d < 3; d++)
+                if (h->active[d]) {
+                    h->sweepP[d] = it->second.P[d];
+                    h->sweepSeg[d] = it->second.seg[d];
+                    h->sweepGrid[d] = sweep_grid(h, d, h->sweepP[d], h->sweepSeg[d]);
+                }
+            return EMG_OK;
+        }
+    }
+    int rc = launch_ghosts(h, h->u);
+    if (rc) return rc;
+    ctl_begin_host<<<1, 1, 0, h->stream>>>(h->ctl, 1e-12);
+    EMG_CUDA(cudaGetLastError());
+    cudaEvent_t a, b;
+    EMG_CUDA(cudaEventCreate(&a));
+    EMG_CUDA(cudaEventCreate(&b));
+    TuneVal best{};
+    for (int d = 0; d < 3; d++) {
+        if (!h->active[d]) continue;
+        const int64_t nd = h->mesh.n[d], nl = h->mesh.n[h->lane_axis[d]];
+        float best_ms = 1e30f;
+        best.P[d] = h->sweepP[d];
+        best.seg[d] = h->sweepSeg[d];
+        for (int P : {8, 16, 32}) {
+            if (P > 8 && nl <= P / 2) continue;                         // lanes mostly idle
+            if (P == 32 && h->opts.mode == EMG_MODE_HYBRID) continue;  // hybrid rings: one CTA per SM at P = 32
+            for (int64_t seg : {nd, (nd + 1) / 2, (nd + 3) / 4}) {
+                if (seg < 16 && seg != nd) continue;
+                const dim3 g = sweep_grid(h, d, P, seg);
+                if (g.y > 65535u || g.z > 65535u) continue;
+                h->sweepP[d] = P;
+                h->sweepSeg[d] = (int)seg;
+                h->sweepGrid[d] = g;
+                if ((rc = launch_axis(h, 1, d, h->u, true, false))) return rc;
+                cudaEventRecord(a, h->stream);
+                for (int r = 0; r < 3; r++)
+                    if ((rc = launch_axis(h, 1, d, h->u, true, false))) return rc;
+                cudaEventRecord(b, h->stream);
+                EMG_CUDA(cudaEventSynchronize(b));
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, a, b);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best.P[d] = P;
+                    best.seg[d] = (int)seg;
+                }
+            }
+        }
+        h->sweepP[d] = best.P[d];
+        h->sweepSeg[d] = best.seg[d];
+        h->sweepGrid[d] = sweep_grid(h, d, best.P[d], best.seg[d]);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    // the timing sweeps touched the residual and the counters: reset the control block
+    std::memset(h->ctl_host, 0, sizeof(StepCtl));
+    h->ctl_host->t_end = INFINITY;
+    EMG_CUDA(cudaMemcpyAsync(h->ctl, h->ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice, h->stream));
+    EMG_CUDA(cudaStreamSynchronize(h->stream));
+    h->launches = 0;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = best;
     return EMG_OK;
 }
 
@@ -701,6 +812,7 @@ int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc
             return bail(set_error(EMG_ERR_INVALID, "mesh too large for the sweep grid (an axis above 65535 pencils)"));
     int rc = emg_uniform_upload(h, u_aos, len);
     if (rc) return bail(rc);
+    if ((opts->flags & EMG_OPT_AUTOTUNE) && (rc = autotune_sweeps(h))) return bail(rc);
     *out = h;
     return EMG_OK;
 }

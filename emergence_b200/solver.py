@@ -49,12 +49,13 @@ class GpuSolver:
     """Device solver of a ghost-padded conserved state.
 
     ``GpuSolver(sys, mesh, u, bc=..., cfl=0.5, mode=FluxMode.Weno, tol=1e-3,
-    positivity=True, precision=Precision.F64)`` uploads ``u`` (float64
-    ``[mesh.len(), 5]``) like ``GpuSolver::from_cpu``.
+    positivity=True, precision=Precision.F64, autotune=False)`` uploads ``u``
+    (float64 ``[mesh.len(), 5]``) like ``GpuSolver::from_cpu``; ``autotune``
+    times the sweep launch shapes on ``u`` at creation (EMG_OPT_AUTOTUNE).
     """
 
     def __init__(self, sys, mesh, u, bc=None, cfl=0.5, mode=FluxMode.Weno, tol=1e-3, positivity=True,
-                 precision=Precision.F64):
+                 precision=Precision.F64, autotune=False):
         self.sys = sys
         self.mesh = mesh
         self.bc = bc if bc is not None else [[Bc.Periodic, Bc.Periodic] for _ in range(3)]
@@ -69,7 +70,7 @@ class GpuSolver:
         self._m = _c_mesh(mesh)
         self._e = _c_eos(sys.eos)
         self._b = _c_bcs(self.bc)
-        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, precision, 0)
+        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, precision, 1 if autotune else 0)
         h = C.c_void_p()
         check(lib().emg_uniform_create(C.byref(self._m), C.byref(self._e), self._b, C.byref(self._o), _dptr(u),
                                        mesh.len(), C.byref(h)))

@@ -98,8 +98,14 @@ typedef struct emg_opts {
     int32_t mode;       /* emg_flux_mode */
     int32_t positivity; /* Hu–Adams–Shu limiter on/off (1) */
     int32_t precision;  /* emg_precision */
-    int32_t reserved;
+    int32_t flags;      /* EMG_OPT_* bits (0: none) */
 } emg_opts;
+
+/* emg_opts.flags: time the fused-sweep launch shapes (pencils per CTA, segment
+ * length) of each axis on the initial state at creation and keep the fastest
+ * (uniform grids; cached per mesh extents, flux mode and precision). Results
+ * are the same for every shape. */
+#define EMG_OPT_AUTOTUNE 1
 
 /* ------------------------------------------------------------------ misc */
 
