@@ -270,29 +270,31 @@ struct AdjGhostParams {
 };
 
 __global__ void adj_ghost_kernel(const AdjGhostParams p) {
+    // one thread per (line, field): ghost layers of one line may share source
+    // cells (outflow; both sides of a short periodic or reflecting axis), so a
+    // line is folded in sequence
     const int64_t lines = p.m[p.e0] * p.m[p.e1];
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < lines; t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t a = t / p.m[p.e1], b = t % p.m[p.e1];
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < lines * 5; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t line = t / 5;
+        const int k = (int)(t % 5);
+        const int64_t a = line / p.m[p.e1], b = line % p.m[p.e1];
         const int64_t base = a * p.stride[p.e0] + b * p.stride[p.e1];
         auto at = [&](int64_t c) { return base + c * p.stride[p.d]; };
+        double* x = p.xbar + k * p.ncell;
         for (int gi = 0; gi < p.ng; gi++) {
             for (int side = 0; side < 2; side++) {
+                const int kind = p.kind[side];
                 const int64_t dst = side == 0 ? at(gi) : at(p.n + p.ng + gi);
                 int64_t src = -1;
-                const int kind = p.kind[side];
                 if (kind == EMG_BC_OUTFLOW)
                     src = side == 0 ? at(p.ng) : at(p.n + p.ng - 1);
                 else if (kind == EMG_BC_PERIODIC)
                     src = side == 0 ? at(p.n + gi) : at(p.ng + gi);
                 else if (kind == EMG_BC_REFLECT)
                     src = side == 0 ? at(2 * p.ng - 1 - gi) : at(p.n + p.ng - 1 - gi);
-#pragma unroll
-                for (int k = 0; k < 5; k++) {
-                    const double v = p.xbar[k * p.ncell + dst];
-                    p.xbar[k * p.ncell + dst] = 0.0;
-                    if (src >= 0 && v != 0.0)
-                        p.xbar[k * p.ncell + src] += (kind == EMG_BC_REFLECT && k == 1 + p.d) ? -v : v;
-                }
+                const double v = x[dst];
+                x[dst] = 0.0;
+                if (src >= 0 && v != 0.0) x[src] += (kind == EMG_BC_REFLECT && k == 1 + p.d) ? -v : v;
             }
         }
     }
@@ -593,7 +595,7 @@ int adj_ghosts(emg_adjoint* h, double* xbar) {
         p.e1 = d == 2 ? 1 : 2;
         p.kind[0] = f->bc[2 * d].kind;
         p.kind[1] = f->bc[2 * d + 1].kind;
-        adj_ghost_kernel<<<grid_for(f->m[p.e0] * f->m[p.e1]), ADJ_T, 0, f->stream>>>(p);
+        adj_ghost_kernel<<<grid_for(f->m[p.e0] * f->m[p.e1] * 5), ADJ_T, 0, f->stream>>>(p);
         EMG_CUDA(cudaGetLastError());
         f->launches++;
     }
