@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(ADJ_T, ADJ_MINB) adj_sweep_kernel(const AdjSwe
 // each ghost cell's cotangent moves to the interior cell it was copied from
 // (with the normal momentum negated for reflecting walls; dropped for a
 // Dirichlet state) and the ghost's own cotangent is cleared. One thread per
-// line, over the padded extents of the two other axes like the forward fill;
+// (line, field), over the padded extents of the two other axes like the forward fill;
 // axes run in reverse order (2, 1, 0).
 struct AdjGhostParams {
     double* xbar;
@@ -269,32 +269,75 @@ struct AdjGhostParams {
     int kind[2];
 };
 
+// Source cell of ghost layer gi on one side (-1: Dirichlet, no source).
+__device__ __forceinline__ int64_t adj_ghost_src(const AdjGhostParams& p, int side, int gi) {
+    const int kind = p.kind[side];
+    if (kind == EMG_BC_OUTFLOW) return side == 0 ? p.ng : p.n + p.ng - 1;
+    if (kind == EMG_BC_PERIODIC) return side == 0 ? p.n + gi : p.ng + gi;
+    if (kind == EMG_BC_REFLECT) return side == 0 ? 2 * p.ng - 1 - gi : p.n + p.ng - 1 - gi;
+    return -1;
+}
+
+constexpr int ADJ_GHOST_MAX = 8;
+
 __global__ void adj_ghost_kernel(const AdjGhostParams p) {
-    // one thread per (line, field): ghost layers of one line may share source
-    // cells (outflow; both sides of a short periodic or reflecting axis), so a
-    // line is folded in sequence
+    // one thread per (line, field). The ghost values of a line are gathered
+    // first (independent loads), then each side adds its gathered values into
+    // its sources: an outflow side folds its layers (gi ascending) into its one
+    // source; periodic and reflecting sources of one side are distinct cells
+    // for n >= ng. The two sides go one after the other, as their sources may
+    // coincide on a short axis.
     const int64_t lines = p.m[p.e0] * p.m[p.e1];
+    const int ng = p.ng;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < lines * 5; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t line = t / 5;
         const int k = (int)(t % 5);
         const int64_t a = line / p.m[p.e1], b = line % p.m[p.e1];
         const int64_t base = a * p.stride[p.e0] + b * p.stride[p.e1];
-        auto at = [&](int64_t c) { return base + c * p.stride[p.d]; };
-        double* x = p.xbar + k * p.ncell;
-        for (int gi = 0; gi < p.ng; gi++) {
-            for (int side = 0; side < 2; side++) {
-                const int kind = p.kind[side];
-                const int64_t dst = side == 0 ? at(gi) : at(p.n + p.ng + gi);
-                int64_t src = -1;
-                if (kind == EMG_BC_OUTFLOW)
-                    src = side == 0 ? at(p.ng) : at(p.n + p.ng - 1);
-                else if (kind == EMG_BC_PERIODIC)
-                    src = side == 0 ? at(p.n + gi) : at(p.ng + gi);
-                else if (kind == EMG_BC_REFLECT)
-                    src = side == 0 ? at(2 * p.ng - 1 - gi) : at(p.n + p.ng - 1 - gi);
-                const double v = x[dst];
-                x[dst] = 0.0;
-                if (src >= 0 && v != 0.0) x[src] += (kind == EMG_BC_REFLECT && k == 1 + p.d) ? -v : v;
+        const int64_t sd = p.stride[p.d];
+        double* x = p.xbar + k * p.ncell + base;
+        if (ng > ADJ_GHOST_MAX) {
+            for (int gi = 0; gi < ng; gi++)
+                for (int side = 0; side < 2; side++) {
+                    const int64_t dst = (side == 0 ? gi : p.n + ng + gi) * sd;
+                    const int64_t src = adj_ghost_src(p, side, gi);
+                    const double v = x[dst];
+                    x[dst] = 0.0;
+                    if (src >= 0 && v != 0.0) x[src * sd] += (p.kind[side] == EMG_BC_REFLECT && k == 1 + p.d) ? -v : v;
+                }
+            continue;
+        }
+        double g[2][ADJ_GHOST_MAX];
+#pragma unroll
+        for (int gi = 0; gi < ADJ_GHOST_MAX; gi++)
+            if (gi < ng) {
+                g[0][gi] = x[gi * sd];
+                g[1][gi] = x[(p.n + ng + gi) * sd];
+            }
+#pragma unroll
+        for (int gi = 0; gi < ADJ_GHOST_MAX; gi++)
+            if (gi < ng) {
+                x[gi * sd] = 0.0;
+                x[(p.n + ng + gi) * sd] = 0.0;
+            }
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            const int kind = p.kind[side];
+            if (kind == EMG_BC_OUTFLOW) {
+                double acc = 0.0;
+#pragma unroll
+                for (int gi = 0; gi < ADJ_GHOST_MAX; gi++)
+                    if (gi < ng) acc += g[side][gi];
+                if (acc != 0.0) x[adj_ghost_src(p, side, 0) * sd] += acc;
+            } else if (kind == EMG_BC_PERIODIC || kind == EMG_BC_REFLECT) {
+                const double sg = (kind == EMG_BC_REFLECT && k == 1 + p.d) ? -1.0 : 1.0;
+                double s[ADJ_GHOST_MAX];
+#pragma unroll
+                for (int gi = 0; gi < ADJ_GHOST_MAX; gi++)
+                    if (gi < ng) s[gi] = x[adj_ghost_src(p, side, gi) * sd];
+#pragma unroll
+                for (int gi = 0; gi < ADJ_GHOST_MAX; gi++)
+                    if (gi < ng) x[adj_ghost_src(p, side, gi) * sd] = s[gi] + sg * g[side][gi];
             }
         }
     }

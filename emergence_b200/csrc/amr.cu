@@ -75,16 +75,21 @@ struct HBlock {
 template <class T> struct DevVec {
     T* p = nullptr;
     size_t n = 0, cap = 0;
-    int put(const std::vector<T>& v, cudaStream_t s) {
-        if (v.size() > cap) {
-            if (p) cudaFree(p);
-            cap = std::max<size_t>(v.size(), 2 * cap);
-            if (cudaMalloc(&p, cap * sizeof(T)) != cudaSuccess) {
-                p = nullptr;
-                cap = 0;
-                return set_error(EMG_ERR_CUDA, "device allocation failed");
-            }
+    // capacity for at least m elements (contents not kept)
+    int grow(size_t m) {
+        if (m <= cap) return EMG_OK;
+        if (p) cudaFree(p);
+        cap = std::max<size_t>(m, 2 * cap);
+        if (cudaMalloc(&p, cap * sizeof(T)) != cudaSuccess) {
+            p = nullptr;
+            cap = n = 0;
+            return set_error(EMG_ERR_CUDA, "device allocation failed");
         }
+        return EMG_OK;
+    }
+    int put(const std::vector<T>& v, cudaStream_t s) {
+        int rc = grow(v.size());
+        if (rc) return rc;
         n = v.size();
         if (n && cudaMemcpyAsync(p, v.data(), n * sizeof(T), cudaMemcpyHostToDevice, s) != cudaSuccess)
             return set_error(EMG_ERR_CUDA, "upload failed");
@@ -144,6 +149,9 @@ struct emg_amr {
     int rface_start[7]{};  // refluxing faces of bucket (d, side) = 2d + side: [rface_start[b], rface_start[b+1])
     DevVec<PBox> dtmp_pbox;    // one-off prediction boxes (refined children)
     DevVec<RBox> dtmp_rbox;    // one-off restriction boxes (coarsened parents)
+    DevVec<int> drem, dmoves;  // batch of coarsenings: removal order of fine blocks, block moves
+    std::vector<PBox> pend_pbox;  // prediction boxes of refinements not yet launched
+    int pend_level = -1;          // their parent level
     DevVec<double> dstage;     // host initial data of new blocks
     std::vector<int> rbox_count;
     int ncopy = 0, npbox = 0, nbcleaves = 0, nleaves = 0;
@@ -356,6 +364,43 @@ struct emg_amr {
         return EMG_OK;
     }
 
+    // Growing the pool reallocates and copies it (hundreds of ms for a pool of
+    // 10 GB), and every regrid that refines holds the new children before the
+    // coarsened blocks are removed. The pool therefore starts with room for
+    // twice the initial hierarchy, when old and new pool fit in half of the
+    // free device memory.
+    int reserve_headroom() {
+        int rc = EMG_OK;
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+            cudaGetLastError();
+            fr = 0;
+        }
+        const int64_t want = 2 * (int64_t)blocks.size();
+        const size_t per_block = (size_t)bcell * 5 * sizeof(double) * 3 + (size_t)3 * 2 * 5 * npen * sizeof(double);
+        if (want > cap && (size_t)(want + cap) * per_block <= fr / 2 && (rc = reserve(want))) return rc;
+        // the block lists of the layout and of regrids likewise, so that a
+        // regrid allocates nothing (an allocation or free in the middle of a
+        // run stalls the host for milliseconds, at times for hundreds)
+        if ((rc = ensure_layout())) return rc;
+        const size_t nb = blocks.size();
+        if ((rc = dleaves.grow(2 * nb)) || (rc = dlevel.grow(2 * nb)) || (rc = didx.grow(6 * nb)) ||
+            (rc = dbcleaves.grow(2 * nb)) || (rc = dcopy.grow(2 * dcopy.n)) || (rc = dpbox.grow(2 * dpbox.n)) ||
+            (rc = dreflux.grow(2 * dreflux.n)) || (rc = dtmp_pbox.grow(8 * nb)) || (rc = drem.grow(2 * nb)) ||
+            (rc = dmoves.grow(4 * nb)) || (rc = dtmp_rbox.grow(4 * nb)) || (rc = dmap_edits.grow(2 * map_size())))
+            return rc;
+        for (auto& r : drbox)
+            if ((rc = r.grow(2 * r.n))) return rc;
+        if ((rc = grow_det(2 * (int64_t)nb))) return rc;
+        layout_valid = false;  // grown lists do not keep their contents
+        return EMG_OK;
+    }
+    size_t map_size() const {
+        size_t t = 0;
+        for (auto& m : map) t += m.size();
+        return t;
+    }
+
     int scratch(int64_t cells) {
         if (cells <= scr_cap) return EMG_OK;
         int64_t nc = std::max<int64_t>(cells, scr_cap * 2);
@@ -407,12 +452,16 @@ struct emg_amr {
         return b;
     }
 
+    // one CTA per box in shared memory when the largest box stage fits; the
+    // multi-launch pipeline (global scratch) otherwise
+    static size_t pbox_smem(int64_t maxcells) { return (size_t)maxcells * (2 * 5 * sizeof(double) + 1); }
+    static bool pbox_fused_fits(int64_t maxcells) { return pbox_smem(maxcells) <= 227 * 1024; }
+
     int run_pboxes(const PBox* dboxes, int nbox, int64_t maxcells) {
         if (!nbox) return EMG_OK;
         AmrDev A = view();
-        // one CTA per box in shared memory when the largest box stage fits
-        const size_t fused_smem = (size_t)maxcells * (2 * 5 * sizeof(double) + 1);
-        if (fused_smem <= 227 * 1024) {
+        const size_t fused_smem = pbox_smem(maxcells);
+        if (pbox_fused_fits(maxcells)) {
             if (!pbox_fused_ready) {
                 AMR_CUDA(cudaFuncSetAttribute(pbox_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
                 pbox_fused_ready = true;
@@ -447,7 +496,7 @@ struct emg_amr {
             off += b.cap;
             mx = std::max(mx, b.cap);
         }
-        if ((rc = scratch(off))) return rc;
+        if (!pbox_fused_fits(mx) && (rc = scratch(off))) return rc;
         if ((rc = dtmp_pbox.put(boxes, stream))) return rc;
         return run_pboxes(dtmp_pbox.p, (int)boxes.size(), mx);
     }
@@ -509,14 +558,15 @@ struct emg_amr {
             b.sz[d] = act[d] ? 2 * (hi_[d] - lo_[d]) + 8 : 1;
         }
         b.cap = (int64_t)b.sz[0] * b.sz[1] * b.sz[2];
+        b.seq = -1;
         return b;
     }
 
-    int run_rboxes(const RBox* dboxes, int nbox, int64_t maxcells) {
+    int run_rboxes(const RBox* dboxes, int nbox, int64_t maxcells, const int* rem = nullptr) {
         if (!nbox) return EMG_OK;
         AmrDev A = view();
         const dim3 gr = box_grid(maxcells, nbox);
-        rbox_gather<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0]);
+        rbox_gather<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], rem);
         for (int di = 0; di < (int)dims.size(); di++) rbox_bc<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], di);
         int cur = 0;
         for (int di = 0; di < (int)dims.size(); di++) {
@@ -689,7 +739,7 @@ struct emg_amr {
         npbox = (int)pboxes.size();
         nbcleaves = (int)bcl.size();
         pbox_max = pmax;
-        if ((rc = scratch(std::max(poff, rneed)))) return rc;
+        if ((rc = scratch(std::max(pbox_fused_fits(pmax) ? 0 : poff, rneed)))) return rc;
         layout_valid = true;
         layout_gen++;
         return EMG_OK;
@@ -950,6 +1000,28 @@ struct emg_amr {
         return EMG_OK;
     }
 
+    // Refinements are predicted in batches: the children of a parent at level l
+    // read levels <= l only and write level l + 1, so refinements of parents of
+    // one level are independent and run as one launch; a refinement of another
+    // level first flushes the batch, which keeps the sequential order's data
+    // and block map for every box.
+    int queue_pboxes(int l, std::vector<PBox>& boxes) {
+        if (l != pend_level) {
+            int rc = flush_pboxes();
+            if (rc) return rc;
+        }
+        pend_level = l;
+        pend_pbox.insert(pend_pbox.end(), boxes.begin(), boxes.end());
+        return EMG_OK;
+    }
+    int flush_pboxes() {
+        if (pend_pbox.empty()) return EMG_OK;
+        std::vector<PBox> boxes;
+        boxes.swap(pend_pbox);
+        pend_level = -1;
+        return predict_now(std::move(boxes));
+    }
+
     // C/amr.rs:952-1011
     int refine_block(int id, emg_init_fn init, void* ictx) {
         const int l = blocks[id].level;
@@ -993,7 +1065,7 @@ struct emg_amr {
         if (init) {
             for (size_t n = 0; n < kids.size(); n++)
                 if ((rc = init_block_data(first + (int)n, init, ictx))) return rc;
-        } else if ((rc = predict_now(boxes))) {
+        } else if ((rc = queue_pboxes(l, boxes))) {
             return rc;
         }
         blocks[id].leaf = false;
@@ -1002,51 +1074,95 @@ struct emg_amr {
         return EMG_OK;
     }
 
-    // C/amr.rs:1014-1032
-    int coarsen(int l, const Key& idx) {
-        std::vector<Key> kids = children(idx);
-        const int pid = get(l, idx);
-        // restriction of the whole parent from its children
-        {
-            int rc = upload_map();
-            if (rc) return rc;
-            RBox b = make_rbox(l, pid, idx, {0, 0, 0}, {bd[0], bd[1], bd[2]});
-            b.off = 0;
-            if ((rc = scratch(b.cap))) return rc;
-            if ((rc = dtmp_rbox.put(std::vector<RBox>{b}, stream))) return rc;
-            if ((rc = run_rboxes(dtmp_rbox.p, 1, b.cap))) return rc;
-        }
-        blocks[pid].leaf = true;
-        std::vector<int> ids;
-        for (auto& c : kids) ids.push_back(get(l + 1, c));
-        std::sort(ids.begin(), ids.end(), [](int x, int y) { return x > y; });
-        for (int i : ids) {
-            remove(blocks[i].level, blocks[i].idx);
-            const int last = (int)blocks.size() - 1;
-            if (i != last) {
-                AmrDev A = view();
-                pool_move<<<64, 256, 0, stream>>>(A, last, i);
-                launches++;
-                blocks[i] = blocks[last];
+    // Coarsenings of parents at level l (C/amr.rs:1014-1032, in candidate
+    // order). The hierarchy edits (parent becomes a leaf, children removed by
+    // swap-remove) run in sequence on the host; the restrictions of the whole
+    // batch then run as one set of launches on the pool as it was at the batch
+    // start, each box seeing the fine blocks removed by earlier coarsenings of
+    // the batch as absent (`rem`), and the block moves of the compaction follow
+    // in one launch. Parents of one level neither read nor write each other's
+    // data (a box reads level l + 1 only), so this equals the sequential order.
+    int coarsen_batch(int l, const std::vector<Key>& parents) {
+        int rc = upload_map();  // the device map as at the batch start
+        if (rc) return rc;
+        const int n0 = (int)blocks.size();
+        std::vector<int> orig(n0), rem(n0, INT32_MAX);
+        for (int i = 0; i < n0; i++) orig[i] = i;
+        std::vector<RBox> boxes;
+        for (const Key& idx : parents) {
+            const int pid = get(l, idx);
+            if (pid < 0) continue;
+            RBox b = make_rbox(l, orig[pid], idx, {0, 0, 0}, {bd[0], bd[1], bd[2]});
+            b.seq = (int)boxes.size();
+            boxes.push_back(b);
+            blocks[pid].leaf = true;
+            std::vector<int> ids;
+            for (auto& c : children(idx)) ids.push_back(get(l + 1, c));
+            std::sort(ids.begin(), ids.end(), [](int x, int y) { return x > y; });
+            for (int i : ids) {
+                rem[orig[i]] = b.seq;
+                remove(blocks[i].level, blocks[i].idx);
+                const int last = (int)blocks.size() - 1;
+                if (i != last) {
+                    blocks[i] = blocks[last];
+                    orig[i] = orig[last];
+                }
+                blocks.pop_back();
+                orig.pop_back();
+                if (i < (int)blocks.size()) insert(blocks[i].level, blocks[i].idx, i);
             }
-            blocks.pop_back();
-            if (i < (int)blocks.size()) insert(blocks[i].level, blocks[i].idx, i);
+            layout_valid = false;
         }
-        layout_valid = false;
+        if (boxes.empty()) return EMG_OK;
+        if ((rc = drem.put(rem, stream))) return rc;
+        if ((rc = dtmp_rbox.put(boxes, stream))) return rc;
+        // restrictions in chunks of up to 64 boxes (scratch of 64 whole-parent boxes)
+        const int chunk = 64;
+        for (int c0 = 0; c0 < (int)boxes.size(); c0 += chunk) {
+            const int nb = std::min<int>(chunk, (int)boxes.size() - c0);
+            int64_t off = 0, mx = 0;
+            std::vector<RBox> part(boxes.begin() + c0, boxes.begin() + c0 + nb);
+            for (auto& b : part) {
+                b.off = off;
+                off += b.cap;
+                mx = std::max(mx, b.cap);
+            }
+            if ((rc = scratch(off))) return rc;
+            if ((rc = dtmp_rbox.put(part, stream))) return rc;
+            if ((rc = run_rboxes(dtmp_rbox.p, nb, mx, drem.p))) return rc;
+        }
+        // moves of the compaction: slot s < size now holds the block that was at orig[s]
+        std::vector<int> moves;
+        for (int s2 = 0; s2 < (int)blocks.size(); s2++)
+            if (orig[s2] != s2) {
+                moves.push_back(s2);
+                moves.push_back(orig[s2]);
+            }
+        if (!moves.empty()) {
+            if ((rc = dmoves.put(moves, stream))) return rc;
+            AmrDev A = view();
+            const int nm = (int)moves.size() / 2;
+            const unsigned cy = (unsigned)std::max(1, std::min(16, 296 / nm));
+            pool_move_list<<<dim3((unsigned)nm, cy), 256, 0, stream>>>(A, dmoves.p);
+            launches++;
+        }
         AMR_CUDA(cudaGetLastError());
         return EMG_OK;
     }
 
+    int grow_det(int64_t n) {
+        if (n <= det_cap) return EMG_OK;
+        cudaFree(det);
+        det_cap = std::max<int64_t>(n, 2 * det_cap);
+        AMR_CUDA(cudaMalloc(&det, det_cap * sizeof(unsigned long long)));
+        return EMG_OK;
+    }
     // details of all leaves (C/amr.rs:823-867), ancestors 0
     int details(std::vector<double>& out) {
         int rc = ensure_layout();
         if (rc) return rc;
         if ((rc = fill_ghosts())) return rc;
-        if ((int64_t)blocks.size() > det_cap) {
-            cudaFree(det);
-            det_cap = std::max<int64_t>(blocks.size(), 2 * det_cap);
-            AMR_CUDA(cudaMalloc(&det, det_cap * sizeof(unsigned long long)));
-        }
+        if ((rc = grow_det((int64_t)blocks.size()))) return rc;
         AMR_CUDA(cudaMemsetAsync(det, 0, blocks.size() * sizeof(unsigned long long), stream));
         AmrDev A = view();
         amr_detail<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
@@ -1101,12 +1217,16 @@ struct emg_amr {
         std::sort(want.begin(), want.end());
         want.erase(std::unique(want.begin(), want.end()), want.end());
         std::set<std::pair<int, Key>> prot(want.begin(), want.end());
+        const size_t nb_before = blocks.size();
         for (auto& k : want) {
             int id = get(k.first, k.second);
             if (id >= 0 && k.first + 1 < levels)
                 if ((rc = refine_block(id, nullptr, nullptr))) return rc;
         }
-        if ((rc = flags(f))) return rc;
+        if ((rc = flush_pboxes())) return rc;
+        // flags of the refined hierarchy; without a refinement they are the
+        // ones just computed (same leaves, same restriction and ghosts)
+        if (blocks.size() != nb_before && (rc = flags(f))) return rc;
         const size_t nkids = (size_t)1 << dims.size();
         std::vector<std::pair<int, Key>> cand;
         for (size_t bi = 0; bi < blocks.size(); bi++) {
@@ -1122,16 +1242,23 @@ struct emg_amr {
             if (ok) cand.push_back({b.level, b.idx});
         }
         std::stable_sort(cand.begin(), cand.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
-        for (auto& c : cand) {
-            const int l = c.first;
-            bool ok = true;
-            for (auto& nk : neighbours(l, c.second))
-                for (auto& ch : children(nk)) {
-                    int j = get(l + 1, ch);
-                    if (j >= 0 && !blocks[j].leaf) ok = false;
-                }
-            if (ok && get(l, c.second) >= 0)
-                if ((rc = coarsen(l, c.second))) return rc;
+        // the decisions of one level do not depend on that level's coarsenings
+        // (they look at level l + 1 blocks that are not children of a candidate
+        // of the level), so they are taken before the level's batch runs
+        for (size_t ci = 0; ci < cand.size();) {
+            const int l = cand[ci].first;
+            std::vector<Key> batch;
+            for (; ci < cand.size() && cand[ci].first == l; ci++) {
+                const Key& key = cand[ci].second;
+                bool ok = true;
+                for (auto& nk : neighbours(l, key))
+                    for (auto& ch : children(nk)) {
+                        int j = get(l + 1, ch);
+                        if (j >= 0 && !blocks[j].leaf) ok = false;
+                    }
+                if (ok && get(l, key) >= 0) batch.push_back(key);
+            }
+            if ((rc = coarsen_batch(l, batch))) return rc;
         }
         rate_valid = false;
         return EMG_OK;
@@ -1336,6 +1463,8 @@ struct emg_amr {
         dreflux.release();
         dtmp_pbox.release();
         dtmp_rbox.release();
+        drem.release();
+        dmoves.release();
         dstage.release();
         if (stream) cudaStreamDestroy(stream);
     }
@@ -1375,6 +1504,7 @@ int emg_amr_create(const emg_amr_config* cfg, const emg_eos* eos, const double l
             if (id >= 0 && (rc = h->refine_block(id, init, ctx))) return bail(rc);
         }
     }
+    if ((rc = h->reserve_headroom())) return bail(rc);
     *out = h;
     return EMG_OK;
 }
@@ -1410,6 +1540,7 @@ int emg_amr_create_from_blocks(const emg_amr_config* cfg, const emg_eos* eos, co
     }
     cudaStreamSynchronize(h->stream);
     cudaFree(tmp);
+    if ((rc = h->reserve_headroom())) return bail(rc);
     *out = h;
     return EMG_OK;
 }

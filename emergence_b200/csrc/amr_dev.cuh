@@ -196,6 +196,7 @@ struct RBox {
     int sz[3];           // fine patch size
     int64_t off;         // scratch offset (cells)
     int64_t cap;         // cells per buffer
+    int seq;             // position in a batch of coarsenings (-1: none)
 };
 
 // thread → (box, cell) over a prefix-sum of box sizes

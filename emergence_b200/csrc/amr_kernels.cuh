@@ -204,8 +204,12 @@ __global__ void __launch_bounds__(256) pbox_fused(const AmrDev A, const PBox* __
     for (int64_t q = threadIdx.x; q < nf; q += blockDim.x) pbox_scatter_cell(A, b, q, bufs[cur], 0);
 }
 
-// fine patch of a restriction box with validity (amr.rs:632-663)
-__global__ void rbox_gather(const AmrDev A, const RBox* __restrict__ boxes, double* buf, unsigned char* ok) {
+// fine patch of a restriction box with validity (amr.rs:632-663). `rem`
+// (optional) replays a batch of coarsenings in their sequential order: fine
+// block id is absent for box seq when rem[id] < seq, i.e. it was removed by an
+// earlier coarsening of the batch.
+__global__ void rbox_gather(const AmrDev A, const RBox* __restrict__ boxes, double* buf, unsigned char* ok,
+                            const int* __restrict__ rem) {
     const RBox b = boxes[blockIdx.x];
     const int lf = b.l + 1;
     const int64_t n = (int64_t)b.sz[0] * b.sz[1] * b.sz[2];
@@ -235,7 +239,8 @@ __global__ void rbox_gather(const AmrDev A, const RBox* __restrict__ boxes, doub
                 key[d] = A.act[d] ? amr_ediv(gw[d], A.bd[d]) : 0;
                 lc[d] = A.act[d] ? amr_erem(gw[d], A.bd[d]) : 0;
             }
-            const int id = amr_get(A, lf, key);
+            int id = amr_get(A, lf, key);
+            if (id >= 0 && rem != nullptr && b.seq >= 0 && rem[id] < b.seq) id = -1;
             if (id >= 0) {
                 amr_load(A, id, amr_cell(A, lc), v);
                 o = 1;
@@ -608,9 +613,12 @@ __global__ void amr_detail(const AmrDev A, const int* __restrict__ leaves, unsig
     }
 }
 
-// copy one pool block's state (swap_remove of a coarsened child, amr.rs:1024-1031)
-__global__ void pool_move(const AmrDev A, int from, int to) {
-    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < A.bcell; q += (int64_t)gridDim.x * blockDim.x)
+// block moves (to, from) of the swap-removes of a batch of coarsenings
+// (amr.rs:1024-1031): every source lies above every
+// destination, so the moves are independent. grid = (moves, chunks of cells)
+__global__ void pool_move_list(const AmrDev A, const int* __restrict__ moves) {
+    const int to = moves[2 * blockIdx.x], from = moves[2 * blockIdx.x + 1];
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < A.bcell; q += (int64_t)gridDim.y * blockDim.x)
         for (int k = 0; k < 5; k++)
             A.u[(int64_t)k * A.ntot + (int64_t)to * A.bcell + q] = A.u[(int64_t)k * A.ntot + (int64_t)from * A.bcell + q];
 }
