@@ -189,30 +189,26 @@ struct Sweep {
         const RF run4 = c / rho;
         const RF run0 = -run4;
         const RF r40 = c * c;
-        RF ch0[6], ch1[6], ch2[6], ch3[6], ch4[6];
-#pragma unroll
-        for (int s = 0; s < 6; s++) {
-            const int row = m + s;
-            const RF w0 = Wr[at<S>(row, 0, l)];
-            const RF wn = Wr[at<S>(row, un, l)];
-            const RF w4 = Wr[at<S>(row, 4, l)];
-            ch0[s] = l0un * wn + l04 * w4;
-            ch1[s] = w0 + l14 * w4;
-            ch2[s] = Wr[at<S>(row, t1, l)];
-            ch3[s] = Wr[at<S>(row, t2, l)];
-            ch4[s] = l4un * wn + l04 * w4;
-        }
+        // one characteristic field at a time: six live stencil values instead
+        // of thirty keep the kernel within 80 registers (3 CTAs per SM)
         RF cl[5], cr[5];
-        cl[0] = weno5z_interp(ch0[0], ch0[1], ch0[2], ch0[3], ch0[4]);
-        cr[0] = weno5z_interp(ch0[5], ch0[4], ch0[3], ch0[2], ch0[1]);
-        cl[1] = weno5z_interp(ch1[0], ch1[1], ch1[2], ch1[3], ch1[4]);
-        cr[1] = weno5z_interp(ch1[5], ch1[4], ch1[3], ch1[2], ch1[1]);
-        cl[2] = weno5z_interp(ch2[0], ch2[1], ch2[2], ch2[3], ch2[4]);
-        cr[2] = weno5z_interp(ch2[5], ch2[4], ch2[3], ch2[2], ch2[1]);
-        cl[3] = weno5z_interp(ch3[0], ch3[1], ch3[2], ch3[3], ch3[4]);
-        cr[3] = weno5z_interp(ch3[5], ch3[4], ch3[3], ch3[2], ch3[1]);
-        cl[4] = weno5z_interp(ch4[0], ch4[1], ch4[2], ch4[3], ch4[4]);
-        cr[4] = weno5z_interp(ch4[5], ch4[4], ch4[3], ch4[2], ch4[1]);
+#pragma unroll
+        for (int a = 0; a < 5; a++) {
+            RF ch[6];
+#pragma unroll
+            for (int s = 0; s < 6; s++) {
+                const int row = m + s;
+                switch (a) {
+                    case 0: ch[s] = l0un * Wr[at<S>(row, un, l)] + l04 * Wr[at<S>(row, 4, l)]; break;
+                    case 1: ch[s] = Wr[at<S>(row, 0, l)] + l14 * Wr[at<S>(row, 4, l)]; break;
+                    case 2: ch[s] = Wr[at<S>(row, t1, l)]; break;
+                    case 3: ch[s] = Wr[at<S>(row, t2, l)]; break;
+                    default: ch[s] = l4un * Wr[at<S>(row, un, l)] + l04 * Wr[at<S>(row, 4, l)];
+                }
+            }
+            cl[a] = weno5z_interp(ch[0], ch[1], ch[2], ch[3], ch[4]);
+            cr[a] = weno5z_interp(ch[5], ch[4], ch[3], ch[2], ch[1]);
+        }
         RF wl[5], wr[5];
         wl[0] = (cl[0] + cl[1]) + cl[4];
         wr[0] = (cr[0] + cr[1]) + cr[4];
