@@ -466,7 +466,7 @@ struct emg_amr {
                 AMR_CUDA(cudaFuncSetAttribute(pbox_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
                 pbox_fused_ready = true;
             }
-            pbox_fused<<<nbox, 256, fused_smem, stream>>>(A, dboxes, (int)maxcells);
+            pbox_fused<<<nbox, PBOX_THREADS, fused_smem, stream>>>(A, dboxes, (int)maxcells);
             launches++;
             AMR_CUDA(cudaGetLastError());
             return EMG_OK;
@@ -751,7 +751,7 @@ struct emg_amr {
     int fill_ghosts() {
         AmrDev A = view();
         if (ncopy) {
-            ghost_copy<<<box_grid((int64_t)ng * std::max(bd[0], 1) * std::max(bd[1], 1), ncopy), 256, 0, stream>>>(A, dcopy.p);
+            ghost_copy<<<ncopy, COPY_THREADS, 0, stream>>>(A, dcopy.p);
             launches++;
         }
         int rc = run_pboxes(dpbox.p, npbox, pbox_max);

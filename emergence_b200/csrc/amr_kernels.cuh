@@ -10,10 +10,14 @@
 namespace emg {
 
 // row-major cell index within a box of size s
+// (box cells stay far below 2^31: 32-bit division, several times cheaper
+// than the 64-bit one in these index-bound kernels)
 __device__ __forceinline__ void box_coord(int64_t q, const int* s, int64_t* c) {
-    c[2] = q % s[2];
-    c[1] = (q / s[2]) % s[1];
-    c[0] = q / ((int64_t)s[1] * s[2]);
+    const int qi = (int)q;
+    const int a = qi / s[2];
+    c[2] = qi - a * s[2];
+    c[1] = a % s[1];
+    c[0] = a / s[1];
 }
 __device__ __forceinline__ int64_t box_index(const int64_t* c, const int* s) { return (c[0] * s[1] + c[1]) * s[2] + c[2]; }
 
@@ -176,7 +180,10 @@ __global__ void pbox_scatter(const AmrDev A, const PBox* __restrict__ boxes, con
 // separable pass per active axis (ping-pong) and the scatter, with the same
 // per-cell arithmetic as the multi-launch pipeline above. `cap` is the
 // largest box stage in cells; dynamic shared memory 2·cap·5 doubles + cap bytes.
-__global__ void __launch_bounds__(256) pbox_fused(const AmrDev A, const PBox* __restrict__ boxes, int cap) {
+// 512 threads: one CTA per box fills an SM's shared memory, so the CTA's own
+// warps are all the latency hiding the gathers get
+constexpr int PBOX_THREADS = 512;
+__global__ void __launch_bounds__(PBOX_THREADS) pbox_fused(const AmrDev A, const PBox* __restrict__ boxes, int cap) {
     extern __shared__ __align__(16) double pb_smem[];
     double* bufs[2] = {pb_smem, pb_smem + (size_t)cap * 5};
     unsigned char* ok = reinterpret_cast<unsigned char*>(pb_smem + (size_t)2 * cap * 5);
@@ -331,7 +338,10 @@ struct CopyTask {
     int slot, src;
     int o[3];
 };
-__global__ void ghost_copy(const AmrDev A, const CopyTask* __restrict__ tasks) {
+// one CTA per task; the source cell is the destination cell shifted by one
+// block along the task's direction (o = 0 on inactive axes)
+constexpr int COPY_THREADS = 128;
+__global__ void __launch_bounds__(COPY_THREADS) ghost_copy(const AmrDev A, const CopyTask* __restrict__ tasks) {
     const CopyTask t = tasks[blockIdx.x];
     int rs[3], sz[3];
     for (int d = 0; d < 3; d++) {
@@ -349,19 +359,17 @@ __global__ void ghost_copy(const AmrDev A, const CopyTask* __restrict__ tasks) {
             sz[d] = A.ng;
         }
     }
-    const int64_t n = (int64_t)sz[0] * sz[1] * sz[2];
+    const int e1 = A.ext[1], e2 = A.ext[2];
+    const int shift = ((t.o[0] * A.bd[0]) * e1 + t.o[1] * A.bd[1]) * e2 + t.o[2] * A.bd[2];
+    const int n = sz[0] * sz[1] * sz[2];
     double* dst = A.u + (int64_t)t.slot * A.bcell;
     const double* src = A.u + (int64_t)t.src * A.bcell;
-    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
-        int64_t c[3];
-        box_coord(q, sz, c);
-        int64_t e[3], s[3];
-        for (int d = 0; d < 3; d++) {
-            e[d] = rs[d] + c[d];
-            s[d] = A.act[d] ? e[d] - t.o[d] * A.bd[d] : 0;  // ext index of the neighbour's interior cell
-        }
-        const int64_t de = (e[0] * A.ext[1] + e[1]) * A.ext[2] + e[2];
-        const int64_t se = (s[0] * A.ext[1] + s[1]) * A.ext[2] + s[2];
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        const int a = q / sz[2];
+        const int c2 = q - a * sz[2], c1 = a % sz[1], c0 = a / sz[1];
+        const int de = ((rs[0] + c0) * e1 + rs[1] + c1) * e2 + rs[2] + c2;
+        const int se = de - shift;
+#pragma unroll
         for (int k = 0; k < 5; k++) dst[(int64_t)k * A.ntot + de] = src[(int64_t)k * A.ntot + se];
     }
 }
