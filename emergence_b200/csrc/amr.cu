@@ -391,6 +391,9 @@ struct emg_amr {
             return rc;
         for (auto& r : drbox)
             if ((rc = r.grow(2 * r.n))) return rc;
+        for (auto& a : drbsel)
+            for (auto& v : a)
+                if ((rc = v.grow(2 * v.n + 64))) return rc;
         if ((rc = grow_det(2 * (int64_t)nb))) return rc;
         layout_valid = false;  // grown lists do not keep their contents
         return EMG_OK;
@@ -562,19 +565,28 @@ struct emg_amr {
         return b;
     }
 
-    int run_rboxes(const RBox* dboxes, int nbox, int64_t maxcells, const int* rem = nullptr) {
+    // `bsel[di]` (optional): the boxes whose fine patch crosses a non-periodic
+    // domain side along dims[di], the only ones the boundary pass of that axis
+    // changes (all boxes when null)
+    int run_rboxes(const RBox* dboxes, int nbox, int64_t maxcells, const int* rem = nullptr,
+                   const int* const* bsel = nullptr, const int* nbsel = nullptr) {
         if (!nbox) return EMG_OK;
         AmrDev A = view();
         const dim3 gr = box_grid(maxcells, nbox);
         rbox_gather<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], rem);
-        for (int di = 0; di < (int)dims.size(); di++) rbox_bc<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], di);
+        for (int di = 0; di < (int)dims.size(); di++) {
+            if (bsel && !nbsel[di]) continue;
+            const dim3 gb(bsel ? (unsigned)nbsel[di] : gr.x, gr.y, 1);
+            rbox_bc<<<gb, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], di, bsel ? bsel[di] : nullptr);
+            launches++;
+        }
         int cur = 0;
         for (int di = 0; di < (int)dims.size(); di++) {
             rbox_pass<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur], sok[cur], scr[1 - cur], sok[1 - cur], di);
             cur = 1 - cur;
         }
         rbox_scatter<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur]);
-        launches += 2 + 2 * dims.size();
+        launches += 2 + dims.size();
         AMR_CUDA(cudaGetLastError());
         return EMG_OK;
     }
@@ -585,11 +597,14 @@ struct emg_amr {
         if (rc) return rc;
         for (int l = levels - 2; l >= 0; l--) {
             if (!rbox_count[l]) continue;
-            if ((rc = run_rboxes(drbox[l].p, rbox_count[l], rbox_max[l]))) return rc;
+            const int* sel[3] = {drbsel[l][0].p, drbsel[l][1].p, drbsel[l][2].p};
+            if ((rc = run_rboxes(drbox[l].p, rbox_count[l], rbox_max[l], nullptr, sel, rbsel_count[l].data()))) return rc;
         }
         return EMG_OK;
     }
     std::vector<int64_t> rbox_max;
+    std::vector<std::array<DevVec<int>, 3>> drbsel;  // per level and axis: boxes the boundary pass changes
+    std::vector<std::array<int, 3>> rbsel_count;
 
     // ---------------------------------------------------------------- layout
     int ensure_layout() {
@@ -673,9 +688,12 @@ struct emg_amr {
         rbox_count.assign(levels, 0);
         rbox_max.assign(levels, 0);
         if ((int)drbox.size() < levels) drbox.resize(levels);
+        if ((int)drbsel.size() < levels) drbsel.resize(levels);
+        rbsel_count.assign(levels, {0, 0, 0});
         int64_t rneed = 0;
         for (int l = levels - 2; l >= 0; l--) {
             std::vector<RBox> rb;
+            std::vector<int> bsel[3];
             int64_t off = 0;
             for (size_t i = 0; i < blocks.size(); i++) {
                 if (blocks[i].level != l || !is_edge_ancestor((int)i)) continue;
@@ -684,12 +702,23 @@ struct emg_amr {
                     r.off = off;
                     off += r.cap;
                     rbox_max[l] = std::max(rbox_max[l], r.cap);
+                    for (int di = 0; di < (int)dims.size(); di++) {
+                        const int d = dims[di];
+                        const int64_t nf = n_level(l + 1, d);
+                        if ((r.f0[d] < 0 && bckind(d, 0) != EMG_BC_PERIODIC) ||
+                            (r.f0[d] + r.sz[d] > nf && bckind(d, 1) != EMG_BC_PERIODIC))
+                            bsel[di].push_back((int)rb.size());
+                    }
                     rb.push_back(r);
                 }
             }
             rneed = std::max(rneed, off);
             rbox_count[l] = (int)rb.size();
             if ((rc = drbox[l].put(rb, stream))) return rc;
+            for (int di = 0; di < 3; di++) {
+                rbsel_count[l][di] = (int)bsel[di].size();
+                if ((rc = drbsel[l][di].put(bsel[di], stream))) return rc;
+            }
         }
         // refluxing faces (C/amr.rs:1327-1406), bucketed by (d, side) in the reference's order
         std::vector<RefluxFace> rfaces;
@@ -1460,6 +1489,8 @@ struct emg_amr {
         dcopy.release();
         dpbox.release();
         for (auto& r : drbox) r.release();
+        for (auto& a : drbsel)
+            for (auto& v : a) v.release();
         dreflux.release();
         dtmp_pbox.release();
         dtmp_rbox.release();

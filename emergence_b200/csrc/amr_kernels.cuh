@@ -259,8 +259,9 @@ __global__ void rbox_gather(const AmrDev A, const RBox* __restrict__ boxes, doub
     }
 }
 
-__global__ void rbox_bc(const AmrDev A, const RBox* __restrict__ boxes, double* buf, unsigned char* ok, int di) {
-    const RBox b = boxes[blockIdx.x];
+__global__ void rbox_bc(const AmrDev A, const RBox* __restrict__ boxes, double* buf, unsigned char* ok, int di,
+                        const int* __restrict__ sel) {
+    const RBox b = boxes[sel ? sel[blockIdx.x] : blockIdx.x];
     const int64_t n = (int64_t)b.sz[0] * b.sz[1] * b.sz[2];
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
         bc_cell(A, b.l + 1, b.f0, b.sz, q, di, buf, ok, b.off);
