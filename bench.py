@@ -350,6 +350,10 @@ def run_amr(args, world, rank, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = leaf_cells * world / (ms * 1e-3)
+    eff_cells = 1
+    for d in range(3):
+        if cfg["base_blocks"][d] > 0:
+            eff_cells *= cfg["base_blocks"][d] * cfg["b"] * 2 ** (cfg["levels"] - 1)
     nb, nl = g.block_count()
     st = g.structure()
     per_level = [int(((st[:, 0] == l) & (st[:, 4] == 1)).sum()) for l in range(cfg["levels"])]
@@ -378,6 +382,10 @@ def run_amr(args, world, rank, local):
                        "blocks": nb, "leaves": nl, "leaves_per_level": per_level, "build_s": build_s,
                        "precision": args.precision},
             "phase_ms_per_step": {k: v / args.steps for k, v in phases.items()},
+            # the same steps counted at the finest level's resolution over the whole
+            # domain (what a uniform grid of the finest spacing would update per step)
+            "effective_cell_updates_per_s": eff_cells * args.steps * world / (ms * 1e-3),
+            "effective_cells": eff_cells,
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,

@@ -14,6 +14,9 @@ cudaError_t sweep_launch_amr_mixed(int P, int mode, const SweepParams& p, dim3 g
 // Batched independent 1-D lines (SweepParams::segs), 32 segments per CTA.
 cudaError_t sweep_launch_batch_f64(int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 cudaError_t sweep_launch_batch_mixed(int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
+// Resident CTAs per SM of the uniform-grid sweep kernel (after the prepare call).
+int sweep_ctas_per_sm_f64(int P, int mode);
+int sweep_ctas_per_sm_mixed(int P, int mode);
 // Opt the kernels into their dynamic shared memory size (once per device).
 cudaError_t sweep_prepare_f64();
 cudaError_t sweep_prepare_mixed();

@@ -107,4 +107,22 @@ cudaError_t sweep_prepare_mixed() {
     return e;
 }
 
+// resident CTAs per SM of the uniform-grid sweep (the three axes share registers and shared memory)
+template <int P, int MODE> static int occupancy() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_mixed_kernel<P, 0, MODE>, SWEEP_THREADS,
+                                                      SweepSmem<float, P, MODE>::bytes()) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return n > 0 ? n : 1;
+}
+template <int MODE> static int occupancy_p(int P) {
+    return P == 8 ? occupancy<8, MODE>() : (P == 16 ? occupancy<16, MODE>() : occupancy<32, MODE>());
+}
+int sweep_ctas_per_sm_mixed(int P, int mode) {
+    return mode == MODE_HYBRID ? occupancy_p<MODE_HYBRID>(P)
+                               : (mode == MODE_CENTRAL ? occupancy_p<MODE_CENTRAL>(P) : occupancy_p<MODE_WENO>(P));
+}
+
 }  // namespace emg

@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <set>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -392,6 +393,39 @@ dim3 sweep_grid(const emg_uniform* h, int d, int P, int64_t seg) {
     return dim3((unsigned)((nl + P - 1) / P), (unsigned)((nd + seg - 1) / seg), (unsigned)nother);
 }
 
+// Segment length of the sweep along d: the fewest (waves of CTAs) × (rows a
+// CTA streams, seg + 6 with the halo) over the slots of resident CTAs of the
+// whole GPU; a shorter segment only when it is 5 % cheaper. Short segments
+// fill the SMs on small grids, and a wave count just above a whole number is
+// avoided.
+int64_t plan_seg(const emg_uniform* h, int d, int P) {
+    const int64_t nd = h->mesh.n[d], nl = h->mesh.n[h->lane_axis[d]], nother = h->mesh.n[h->other_axis[d]];
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        sms = 148;
+    }
+    const int per_sm = h->opts.precision == EMG_PRECISION_MIXED ? sweep_ctas_per_sm_mixed(P, h->opts.mode)
+                                                                 : sweep_ctas_per_sm_f64(P, h->opts.mode);
+    const int64_t slots = (int64_t)sms * per_sm;
+    const int64_t lane_tiles = (nl + P - 1) / P;
+    int64_t best = nd;
+    double best_cost = 1e300;
+    for (int64_t k = 1; k <= nd; k++) {
+        const int64_t seg = (nd + k - 1) / k;
+        if (k > 1 && seg < 16) break;
+        if ((nd + seg - 1) / seg != k) continue;  // same seg as a smaller k
+        const int64_t ctas = lane_tiles * k * nother;
+        if (k > 65535) break;
+        const double cost = (double)((ctas + slots - 1) / slots) * (double)(seg + 6);
+        if (cost < best_cost * 0.95) {  // shorter segments only for a clear gain
+            best_cost = cost;
+            best = seg;
+        }
+    }
+    return best;
+}
+
 void plan_sweeps(emg_uniform* h) {
     for (int d = 0; d < 3; d++) {
         if (!h->active[d]) continue;
@@ -414,10 +448,7 @@ void plan_sweeps(emg_uniform* h) {
         else if (nl <= 16)
             P = 16;
         const int64_t lane_tiles = (nl + P - 1) / P;
-        // segment length: whole pencils when that already gives enough CTAs
-        int64_t seg = nd;
-        const int64_t target = 4 * 148;
-        while (seg > 16 && lane_tiles * ((nd + seg - 1) / seg) * nother < target) seg = (seg + 1) / 2;
+        const int64_t seg = plan_seg(h, d, P);
         h->sweepP[d] = P;
         h->sweepSeg[d] = (int)seg;
         h->sweepGrid[d] = dim3((unsigned)lane_tiles, (unsigned)((nd + seg - 1) / seg), (unsigned)nother);
@@ -587,7 +618,9 @@ int autotune_sweeps(emg_uniform* h) {
         for (int P : {8, 16, 32}) {
             if (P > 8 && nl <= P / 2) continue;                         // lanes mostly idle
             if (P == 32 && h->opts.mode == EMG_MODE_HYBRID) continue;  // hybrid rings: one CTA per SM at P = 32
-            for (int64_t seg : {nd, (nd + 1) / 2, (nd + 3) / 4}) {
+            const int64_t planned = plan_seg(h, d, P);
+            std::set<int64_t> segs = {nd, (nd + 1) / 2, (nd + 3) / 4, planned, std::min(nd, 2 * planned), (planned + 1) / 2};
+            for (int64_t seg : segs) {
                 if (seg < 16 && seg != nd) continue;
                 const dim3 g = sweep_grid(h, d, P, seg);
                 if (g.y > 65535u || g.z > 65535u) continue;
