@@ -125,8 +125,14 @@ class GpuSolver:
         return n.value
 
     # ---- state
-    def download(self):
-        out = np.empty((self.mesh.len(), 5), dtype=np.float64)
+    def download(self, out=None):
+        """The conserved state as host AoS [cell][q]. ``out`` (optional): a
+        C-contiguous float64 array of that shape to fill, e.g. a view of pinned
+        (page-locked) host memory, which the copy reaches at full link speed."""
+        if out is None:
+            out = np.empty((self.mesh.len(), 5), dtype=np.float64)
+        elif out.shape != (self.mesh.len(), 5) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float64 array of shape {(self.mesh.len(), 5)}")
         check(lib().emg_uniform_download(self._h, _dptr(out), self.mesh.len()))
         return out
 

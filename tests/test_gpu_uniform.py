@@ -290,3 +290,18 @@ def test_autotuned_launch_shapes_give_identical_results():
     assert g0.counters() == g1.counters()
     g0.close()
     g1.close()
+
+
+def test_download_into_a_pinned_host_buffer():
+    """download(out=...) fills a caller's buffer (here page-locked memory from
+    torch) with the same bytes as a fresh download; wrong shapes are refused."""
+    import torch
+    sys, mesh, u, bc = W.explosion((24, 20, 16), 0.3)
+    g = gpu_solver(sys, mesh, u, bc=bc, mode=FluxMode.Weno)
+    g.advance(3)
+    ref = g.download()
+    pinned = torch.empty(tuple(ref.shape), dtype=torch.float64, pin_memory=True).numpy()
+    assert g.download(out=pinned) is pinned
+    assert np.array_equal(pinned, ref)
+    with pytest.raises(ValueError):
+        g.download(out=np.empty((3, 5)))
