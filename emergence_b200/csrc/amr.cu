@@ -445,6 +445,14 @@ struct emg_amr {
             b.csz[d] = (int)(cmax - b.cmin[d] + 1);
             b.t0[d] = t0[d];
         }
+        b.bcmask = 0;
+        for (int di = 0; di < (int)dims.size(); di++) {
+            const int d = dims[di];
+            const int64_t nc = n_level(l - 1, d);
+            if ((b.cmin[d] < 0 && bckind(d, 0) != EMG_BC_PERIODIC) ||
+                (b.cmin[d] + b.csz[d] > nc && bckind(d, 1) != EMG_BC_PERIODIC))
+                b.bcmask |= 1 << di;
+        }
         int64_t c = (int64_t)b.csz[0] * b.csz[1] * b.csz[2], mx = c;
         int s[3] = {b.csz[0], b.csz[1], b.csz[2]};
         for (int d : dims) {

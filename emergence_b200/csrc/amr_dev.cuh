@@ -184,6 +184,7 @@ struct PBox {
     int t0[3];           // ext-local coordinates of fmin in the target block
     int64_t off;         // scratch offset (cells) of this box's buffers
     int64_t cap;         // cells per buffer
+    int bcmask;          // bit di: the coarse patch crosses a non-periodic side along dims[di]
 };
 
 // Restriction of ancestor (l, idx) cells [lo, hi) from level l + 1

@@ -105,6 +105,7 @@ __device__ __forceinline__ void bc_cell(const AmrDev& A, int l, const int64_t* g
 
 __global__ void pbox_bc(const AmrDev A, const PBox* __restrict__ boxes, double* buf, unsigned char* ok, int di) {
     const PBox b = boxes[blockIdx.x];
+    if (!((b.bcmask >> di) & 1)) return;  // nothing of this box lies outside along dims[di]
     const int64_t n = (int64_t)b.csz[0] * b.csz[1] * b.csz[2];
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
         bc_cell(A, b.l - 1, b.cmin, b.csz, q, di, buf, ok, b.off);
@@ -192,6 +193,7 @@ __global__ void __launch_bounds__(PBOX_THREADS) pbox_fused(const AmrDev A, const
     for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) pbox_gather_cell(A, b, q, bufs[0], ok, 0);
     __syncthreads();
     for (int di = 0; di < A.ndims; di++) {
+        if (!((b.bcmask >> di) & 1)) continue;  // the same for the whole CTA
         for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) bc_cell(A, b.l - 1, b.cmin, b.csz, q, di, bufs[0], ok, 0);
         __syncthreads();
     }
