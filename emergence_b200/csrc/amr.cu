@@ -466,7 +466,8 @@ struct emg_amr {
     // one CTA per box in shared memory when the largest box stage fits; the
     // multi-launch pipeline (global scratch) otherwise
     static size_t pbox_smem(int64_t maxcells) { return (size_t)maxcells * (2 * 5 * sizeof(double) + 1); }
-    static bool pbox_fused_fits(int64_t maxcells) { return pbox_smem(maxcells) <= 227 * 1024; }
+    // (227 KB per CTA, less 1 KB for the kernel's static shared memory)
+    static bool pbox_fused_fits(int64_t maxcells) { return pbox_smem(maxcells) <= 226 * 1024; }
 
     int run_pboxes(const PBox* dboxes, int nbox, int64_t maxcells) {
         if (!nbox) return EMG_OK;
@@ -474,7 +475,7 @@ struct emg_amr {
         const size_t fused_smem = pbox_smem(maxcells);
         if (pbox_fused_fits(maxcells)) {
             if (!pbox_fused_ready) {
-                AMR_CUDA(cudaFuncSetAttribute(pbox_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+                AMR_CUDA(cudaFuncSetAttribute(pbox_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, 226 * 1024));
                 pbox_fused_ready = true;
             }
             pbox_fused<<<nbox, PBOX_THREADS, fused_smem, stream>>>(A, dboxes, (int)maxcells);

@@ -190,7 +190,66 @@ __global__ void __launch_bounds__(PBOX_THREADS) pbox_fused(const AmrDev A, const
     unsigned char* ok = reinterpret_cast<unsigned char*>(pb_smem + (size_t)2 * cap * 5);
     const PBox b = boxes[blockIdx.x];
     const int64_t nc = (int64_t)b.csz[0] * b.csz[1] * b.csz[2];
-    for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) pbox_gather_cell(A, b, q, bufs[0], ok, 0);
+    // A coarse patch inside the domain that spans at most three blocks per
+    // axis reads its blocks through a table of their pool slots, filled once
+    // per box: no per-cell key division or block-map load. Cells of absent
+    // blocks (and every other patch) take the general sample, which gives the
+    // same value for cells inside the domain.
+    __shared__ int s_slot[27];
+    __shared__ int s_fast;
+    __shared__ int64_t s_kmin[3];
+    __shared__ int s_nk[3];
+    const int L = b.l - 1;
+    if (threadIdx.x == 0) {
+        int fast = 1;
+        for (int d = 0; d < 3; d++) {
+            s_kmin[d] = 0;
+            s_nk[d] = 1;
+            if (!A.act[d]) continue;
+            const int64_t n = amr_nlevel(A, L, d);
+            if (b.cmin[d] < 0 || b.cmin[d] + b.csz[d] > n || b.csz[d] > 2 * A.bd[d] + 1) fast = 0;
+            s_kmin[d] = amr_ediv(b.cmin[d], A.bd[d]);
+            s_nk[d] = (int)(amr_ediv(b.cmin[d] + b.csz[d] - 1, A.bd[d]) - s_kmin[d] + 1);
+        }
+        s_fast = fast;
+    }
+    __syncthreads();
+    if (s_fast) {
+        const int nt = s_nk[0] * s_nk[1] * s_nk[2];
+        if (threadIdx.x < nt) {
+            const int t = threadIdx.x;
+            const int64_t key[3] = {s_kmin[0] + t / (s_nk[1] * s_nk[2]), s_kmin[1] + (t / s_nk[2]) % s_nk[1], s_kmin[2] + t % s_nk[2]};
+            s_slot[t] = amr_get(A, L, key);
+        }
+        __syncthreads();
+        for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) {
+            int64_t c[3];
+            box_coord(q, b.csz, c);
+            int j[3];
+            int64_t lc[3];
+            for (int d = 0; d < 3; d++) {
+                if (!A.act[d]) {
+                    j[d] = 0;
+                    lc[d] = 0;
+                    continue;
+                }
+                const int o = (int)(b.cmin[d] - s_kmin[d] * A.bd[d] + c[d]);  // 0 <= o < 3·bd
+                j[d] = o >= A.bd[d] ? (o >= 2 * A.bd[d] ? 2 : 1) : 0;
+                lc[d] = o - j[d] * A.bd[d];
+            }
+            const int slot = s_slot[(j[0] * s_nk[1] + j[1]) * s_nk[2] + j[2]];
+            double* v = bufs[0] + q * 5;
+            if (slot >= 0) {
+                amr_load(A, slot, amr_cell(A, lc), v);
+            } else {
+                const int64_t g[3] = {b.cmin[0] + c[0], b.cmin[1] + c[1], b.cmin[2] + c[2]};
+                amr_sample(A, L, g, v, 0);
+            }
+            ok[q] = 1;
+        }
+    } else {
+        for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) pbox_gather_cell(A, b, q, bufs[0], ok, 0);
+    }
     __syncthreads();
     for (int di = 0; di < A.ndims; di++) {
         if (!((b.bcmask >> di) & 1)) continue;  // the same for the whole CTA
