@@ -281,6 +281,63 @@ __global__ void rbox_gather(const AmrDev A, const RBox* __restrict__ boxes, doub
     const RBox b = boxes[blockIdx.x];
     const int lf = b.l + 1;
     const int64_t n = (int64_t)b.sz[0] * b.sz[1] * b.sz[2];
+    // fine patch inside the domain spanning at most four blocks per axis: the
+    // pool slots of its blocks (after the removal mask) from a table built by
+    // each CTA, instead of a key division and a block-map load per cell
+    __shared__ int s_slot[64];
+    __shared__ int s_fast;
+    __shared__ int64_t s_kmin[3];
+    __shared__ int s_nk[3];
+    if (threadIdx.x == 0) {
+        int fast = 1;
+        for (int d = 0; d < 3; d++) {
+            s_kmin[d] = 0;
+            s_nk[d] = 1;
+            if (!A.act[d]) continue;
+            const int64_t nf = amr_nlevel(A, lf, d);
+            if (b.f0[d] < 0 || b.f0[d] + b.sz[d] > nf || b.sz[d] > 3 * A.bd[d] + 1) fast = 0;
+            s_kmin[d] = amr_ediv(b.f0[d], A.bd[d]);
+            s_nk[d] = (int)(amr_ediv(b.f0[d] + b.sz[d] - 1, A.bd[d]) - s_kmin[d] + 1);
+        }
+        s_fast = fast;
+    }
+    __syncthreads();
+    if (s_fast) {
+        const int nt = s_nk[0] * s_nk[1] * s_nk[2];
+        if (threadIdx.x < nt) {
+            const int t = threadIdx.x;
+            const int64_t key[3] = {s_kmin[0] + t / (s_nk[1] * s_nk[2]), s_kmin[1] + (t / s_nk[2]) % s_nk[1], s_kmin[2] + t % s_nk[2]};
+            int id = amr_get(A, lf, key);
+            if (id >= 0 && rem != nullptr && b.seq >= 0 && rem[id] < b.seq) id = -1;
+            s_slot[t] = id;
+        }
+        __syncthreads();
+        for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+            int64_t c[3];
+            box_coord(q, b.sz, c);
+            int j[3];
+            int64_t lc[3];
+            for (int d = 0; d < 3; d++) {
+                if (!A.act[d]) {
+                    j[d] = 0;
+                    lc[d] = 0;
+                    continue;
+                }
+                const int o = (int)(b.f0[d] - s_kmin[d] * A.bd[d] + c[d]);  // 0 <= o < 4·bd
+                j[d] = o / A.bd[d];
+                lc[d] = o - j[d] * A.bd[d];
+            }
+            const int id = s_slot[(j[0] * s_nk[1] + j[1]) * s_nk[2] + j[2]];
+            double* v = buf + (b.off + q) * 5;
+            if (id >= 0) {
+                amr_load(A, id, amr_cell(A, lc), v);
+            } else {
+                for (int k = 0; k < 5; k++) v[k] = 0.0;
+            }
+            ok[b.off + q] = id >= 0 ? 1 : 0;
+        }
+        return;
+    }
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
         int64_t c[3];
         box_coord(q, b.sz, c);
