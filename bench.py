@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg of the uniform workload")
-    ap.add_argument("--no-autotune", action="store_true", help="uniform workload: use the planned sweep shapes")
+    ap.add_argument("--no-autotune", action="store_true", help="uniform and AMR workloads: use the planned sweep shapes")
     ap.add_argument("--workload", default="uniform", choices=["uniform", "amr", "batch", "adjoint", "batch_adjoint"],
                     help="uniform: 3-D explosion 256^3; amr: 3-D shock-bubble on block AMR (base 128^3, 3 levels); "
                          "batch: 4096 independent 1-D Riemann problems; adjoint: discrete adjoint of the 2-D "
@@ -323,7 +323,7 @@ def run_amr(args, world, rank, local):
     prec = Precision.Mixed if args.precision == "mixed" else Precision.F64
     s, cfg, lo, hi, bc, init = W.shock_bubble(dim=3, base=args.amr_base, levels=3)
     t0 = time.perf_counter()
-    g = GpuAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno, cfl=0.4, precision=prec)
+    g = GpuAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno, cfl=0.4, precision=prec, autotune=not args.no_autotune)
     build_s = time.perf_counter() - t0
     for _ in range(args.warmup):
         g.step(g.dt_cfl())
@@ -383,6 +383,7 @@ def run_amr(args, world, rank, local):
                                    "seeded interface perturbation), base 128^3 = 8^3 blocks of 16^3, 3 levels (eff. 512^3), "
                                    "ng=5, WCNS WENO5-Z + HLLC + positivity, CFL 0.4, regrid every 4 steps",
                        "blocks": nb, "leaves": nl, "leaves_per_level": per_level, "build_s": build_s,
+                       "autotune": not args.no_autotune,
                        "precision": args.precision},
             "phase_ms_per_step": {k: v / args.steps for k, v in phases.items()},
             # the same steps counted at the finest level's resolution over the whole

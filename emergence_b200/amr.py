@@ -33,15 +33,17 @@ def init_callback(fn):
 
 class GpuAmr:
     """Device block-AMR solver. ``cfg`` holds the fields of AmrConfig
-    (b, levels, eps, regrid_every, base_blocks, ghosts)."""
+    (b, levels, eps, regrid_every, base_blocks, ghosts). ``autotune``: on the
+    first step, time the batched sweeps with one and two block rows per CTA
+    and keep the faster per axis (results are the same either way)."""
 
     def __init__(self, sys, cfg, lo, hi, bc, init=None, cfl=0.4, mode=FluxMode.Weno, tol=1e-3, positivity=True,
-                 precision=Precision.F64, blocks=None):
+                 precision=Precision.F64, blocks=None, autotune=False):
         self.cfg = dict(cfg)
         self._c = _cfg(cfg)
         self._e = EmgEos(sys.eos.gamma, sys.eos.p_inf, sys.eos.b, sys.eos.q, sys.eos.cv)
         self._b = _c_bcs(bc)
-        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, precision, 0)
+        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, precision, 1 if autotune else 0)
         self._lo = np.ascontiguousarray(lo, dtype=np.float64)
         self._hi = np.ascontiguousarray(hi, dtype=np.float64)
         self.bcells = 1

@@ -150,6 +150,8 @@ struct emg_amr {
     DevVec<PBox> dtmp_pbox;    // one-off prediction boxes (refined children)
     DevVec<RBox> dtmp_rbox;    // one-off restriction boxes (coarsened parents)
     DevVec<int> drem, dmoves;  // batch of coarsenings: removal order of fine blocks, block moves
+    int amrP[3] = {0, 0, 0};      // tuned pencils per CTA of the sweeps (0: default)
+    bool tuned = false;
     std::vector<PBox> pend_pbox;  // prediction boxes of refinements not yet launched
     int pend_level = -1;          // their parent level
     DevVec<double> dstage;     // host initial data of new blocks
@@ -803,11 +805,22 @@ struct emg_amr {
         return EMG_OK;
     }
 
+    // pencils per CTA of the sweep along d: the tuned value, else 32 (two
+    // rows of a 16-wide block per CTA) unless the block face has fewer cells
+    int amr_sweep_P(int d, int lane, int other) const {
+        if (amrP[d]) return amrP[d];
+        return bd[lane] > 16 ? 32 : (bd[lane] * bd[other] >= 32 ? 32 : 16);
+    }
     int sweeps(int stage) {
-        AmrDev A = view();
-        int first = -1;
         for (int d : dims) {
-            if (first < 0) first = d;
+            int rc = sweep_axis(stage, d, dims[0]);
+            if (rc) return rc;
+        }
+        return EMG_OK;
+    }
+    int sweep_axis(int stage, int d, int first) {
+        AmrDev A = view();
+        {
             int o[2], no_ = 0;
             for (int e = 0; e < 3; e++)
                 if (e != d) o[no_++] = e;
@@ -841,7 +854,7 @@ struct emg_amr {
             p.positivity = opts.positivity ? 1 : 0;
             p.tol = opts.tol;
             p.eos = A.eos;
-            const int P = bd[lane] > 16 ? 32 : (bd[lane] * bd[other] >= 32 ? 32 : 16);
+            const int P = amr_sweep_P(d, lane, other);
             p.lw = std::min(P, bd[lane]);
             p.amr = 1;
             p.leaf_slot = dleaves.p;
@@ -861,6 +874,58 @@ struct emg_amr {
             if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("AMR sweep: ") + cudaGetErrorString(e));
         }
         return EMG_OK;
+    }
+
+    // Launch shape of the batched sweeps (EMG_OPT_AUTOTUNE): per axis, time
+    // the sweep over all leaves with 16 and 32 pencils per CTA (one or two rows
+    // of the block face) on the current state and keep the faster. The sweeps
+    // only write the residual and the face-flux record, which the step then
+    // overwrites; results do not depend on the shape.
+    int autotune_sweeps() {
+        int rc = restrict_all();
+        if (rc) return rc;
+        if ((rc = fill_ghosts())) return rc;
+        cudaEvent_t a, b;
+        AMR_CUDA(cudaEventCreate(&a));
+        AMR_CUDA(cudaEventCreate(&b));
+        for (int d : dims) {
+            int o[2], no_ = 0;
+            for (int e = 0; e < 3; e++)
+                if (e != d) o[no_++] = e;
+            int lane = o[1], other = o[0];
+            if (!act[o[1]] && act[o[0]]) {
+                lane = o[0];
+                other = o[1];
+            }
+            std::vector<int> cands;
+            if (bd[lane] <= 16) cands.push_back(16);
+            if (bd[lane] > 16 || bd[lane] * bd[other] >= 32) cands.push_back(32);
+            float best_ms = 1e30f;
+            int best = 0;
+            for (int P : cands) {
+                amrP[d] = P;
+                if ((rc = sweep_axis(1, d, dims[0]))) break;
+                cudaEventRecord(a, stream);
+                for (int r = 0; r < 3 && !rc; r++) rc = sweep_axis(1, d, dims[0]);
+                cudaEventRecord(b, stream);
+                if (rc) break;
+                if (cudaEventSynchronize(b) != cudaSuccess) {
+                    rc = set_error(EMG_ERR_CUDA, "AMR autotune timing failed");
+                    break;
+                }
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, a, b);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = P;
+                }
+            }
+            amrP[d] = best;
+            if (rc) break;
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        return rc;
     }
 
     int compute_rhs(int stage) {
@@ -1316,6 +1381,12 @@ struct emg_amr {
         ctl_host->done = 0;
         ctl_host->rate_bits = 0;
         AMR_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice, stream));
+        if ((opts.flags & EMG_OPT_AUTOTUNE) && !tuned) {
+            tuned = true;
+            if ((rc = autotune_sweeps())) return rc;
+            // the timing launches counted faces and fallbacks: restore the control block
+            AMR_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice, stream));
+        }
         if ((rc = make_events())) return rc;
         if ((rc = run_step_body())) return rc;
         stage_pending = true;

@@ -173,3 +173,19 @@ def test_batched_regrids_match_the_sequential_oracle():
         multi_level |= len({k[0] for k in before - after}) > 1
     print("batched regrids: blocks added", added, "removed", removed)
     assert added >= 40 and removed >= 80 and multi_level
+
+
+def test_autotuned_amr_sweeps_give_identical_results():
+    """The AMR autotuner only changes the batched sweeps' CTA shape; hierarchy
+    and data after steps with a regrid equal the untuned run bit for bit."""
+    s, cfg, lo, hi, bc, init = W.shock_bubble(dim=3, base=2, levels=2)
+    g0 = gpu_amr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno)
+    g1 = gpu_amr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno, autotune=True)
+    for _ in range(5):
+        dt = g0.dt_cfl()
+        assert g1.dt_cfl() == dt
+        g0.step(dt)
+        g1.step(dt)
+    assert np.array_equal(g0.structure(), g1.structure())
+    assert np.array_equal(g0.download(), g1.download())
+    assert g0.counters() == g1.counters()
