@@ -664,9 +664,7 @@ __global__ void amr_cfl(const AmrDev A, const int* __restrict__ leaves, const in
     double rate = 0.0;
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
         int64_t c[3];
-        c[2] = q % A.bd[2];
-        c[1] = (q / A.bd[2]) % A.bd[1];
-        c[0] = q / ((int64_t)A.bd[1] * A.bd[2]);
+        box_coord(q, A.bd, c);
         double uu[5], w[5];
         amr_load(A, slot, amr_cell(A, c), uu);
         to_prim(e, uu, w);
@@ -707,9 +705,7 @@ __global__ void amr_detail(const AmrDev A, const int* __restrict__ leaves, unsig
     double mx = 0.0;
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
         int64_t c[3];
-        c[2] = q % A.bd[2];
-        c[1] = (q / A.bd[2]) % A.bd[1];
-        c[0] = q / ((int64_t)A.bd[1] * A.bd[2]);
+        box_coord(q, A.bd, c);
         const int64_t cell = amr_cell(A, c);
         double s0[2];
         amr_sensor(A, e, u, cell, s0);
@@ -755,9 +751,7 @@ __global__ void pool_put_interior(const AmrDev A, int slot, const double* __rest
     const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
         int64_t c[3];
-        c[2] = q % A.bd[2];
-        c[1] = (q / A.bd[2]) % A.bd[1];
-        c[0] = q / ((int64_t)A.bd[1] * A.bd[2]);
+        box_coord(q, A.bd, c);
         const int64_t cell = (int64_t)slot * A.bcell + amr_cell(A, c);
         for (int k = 0; k < 5; k++) A.u[(int64_t)k * A.ntot + cell] = aos[5 * q + k];
     }
@@ -770,9 +764,7 @@ __global__ void pool_get_interior(const AmrDev A, int nblocks, double* __restric
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t slot = t / nb, q = t % nb;
         int64_t c[3];
-        c[2] = q % A.bd[2];
-        c[1] = (q / A.bd[2]) % A.bd[1];
-        c[0] = q / ((int64_t)A.bd[1] * A.bd[2]);
+        box_coord(q, A.bd, c);
         const int64_t cell = slot * A.bcell + amr_cell(A, c);
         for (int k = 0; k < 5; k++) aos[5 * t + k] = A.u[(int64_t)k * A.ntot + cell];
     }
