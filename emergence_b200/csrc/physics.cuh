@@ -126,6 +126,51 @@ __device__ __forceinline__ R hllc(const Eos<R>& e, const R* wl, const R* wr, int
     return ss;
 }
 
+// HLLC of the mixed form: the Davis wave-speed bounds from FP32 sound speeds,
+// everything else (conserved states, physical fluxes, contact speed, star
+// states) in FP64. An error in a wave speed enters the flux multiplied by a
+// jump of the state across the midpoint, so it vanishes where the data are
+// smooth.
+__device__ __forceinline__ double hllc_fs(const Eos<double>& e, const double* wl, const double* wr, int un, double* f) {
+    const Eos<float> ef{(float)e.gamma, (float)e.p_inf, (float)e.b, (float)e.q};
+    const double cl = (double)sound_speed(ef, (float)wl[0], (float)wl[4]);
+    const double cr = (double)sound_speed(ef, (float)wr[0], (float)wr[4]);
+    double ul = wl[un], ur = wr[un];
+    double sl = fmin(ul - cl, ur - cr);
+    double sr = fmax(ul + cl, ur + cr);
+    double ql[5], qr[5];
+    to_cons(e, wl, ql);
+    to_cons(e, wr, qr);
+    if (sl >= 0.0) {
+        flux_wq(wl, ql, un, f);
+        return ul;
+    }
+    if (sr <= 0.0) {
+        flux_wq(wr, qr, un, f);
+        return ur;
+    }
+    double rl = wl[0], rr = wr[0], pl = wl[4], pr = wr[4];
+    double ss = (pr - pl + rl * ul * (sl - ul) - rr * ur * (sr - ur)) / (rl * (sl - ul) - rr * (sr - ur));
+    const bool left = ss >= 0.0;
+    const double* w = left ? wl : wr;
+    const double* q = left ? ql : qr;
+    double s = left ? sl : sr;
+    double fx[5];
+    flux_wq(w, q, un, fx);
+    double rho = w[0], u = w[un];
+    double fac = rho * (s - u) / (s - ss);
+    double qs[5];
+    qs[0] = fac;
+    qs[1] = fac * w[1];
+    qs[2] = fac * w[2];
+    qs[3] = fac * w[3];
+    qs[un] = fac * ss;
+    qs[4] = fac * (q[4] / rho + (ss - u) * (ss + w[4] / (rho * (s - u))));
+#pragma unroll
+    for (int k = 0; k < 5; k++) f[k] = fx[k] + s * (qs[k] - q[k]);
+    return ss;
+}
+
 // WENO-Z combination (scheme.rs:76-86); eps 1e-40 in f64 (scheme.rs:55), 1e-30 in f32.
 template <typename R> struct WenoEps;
 template <> struct WenoEps<double> { static constexpr double v = 1e-40; };

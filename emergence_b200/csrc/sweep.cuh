@@ -233,7 +233,8 @@ struct Sweep {
     }
 
     // Mixed form of the midpoint flux: the characteristic projection, the
-    // back-projection, the admissibility test and the HLLC flux in FP64; the
+    // back-projection, the admissibility test and the HLLC flux in FP64 (its
+    // wave-speed bounds from FP32 sound speeds, hllc_fs); the
     // ten WENO-Z interpolations (the bulk of the arithmetic) in FP32 on the
     // deviations of each characteristic stencil from its FP64 value at the
     // cell beside the midpoint. WENO-Z is translation invariant (the candidate
@@ -298,7 +299,7 @@ struct Sweep {
                 wr[k] = Wd[at<STRW>(j + 1, k, l)];
             }
         }
-        hllc(e, wl, wr, un, f);
+        hllc_fs(e, wl, wr, un, f);
     }
 
     // KEEP-PE two-point flux with cached ρe (C/system.rs:317-334).
