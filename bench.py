@@ -27,6 +27,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from emergence_b200 import replicas  # noqa: E402  (one process per GPU: barrier, max over ranks)
+
 N_CELLS = 256
 CELL_BYTES_3D = 320  # algorithmic bytes per 3-D cell-update (64·F, F = 5)
 
@@ -111,15 +113,7 @@ class ClockSampler:
 
 
 def dist_init(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import torch.distributed as dist
-        import datetime
-        backend = "gloo" if args.impl == "reference" else "nccl"
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
-    return world, rank, local
+    return replicas.init_from_env("gloo" if args.impl == "reference" else "nccl")
 
 
 def cpu_reference_steps(n, steps, warmup):
@@ -182,9 +176,7 @@ def run_ours(args, world, rank, local):
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     g.set_profiling(True)
     g.kernel_times()  # reset
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    replicas.barrier(world)
     torch.cuda.synchronize()
     l0 = g.launch_count()
     with ClockSampler(dev) as clk:
@@ -197,12 +189,8 @@ def run_ours(args, world, rank, local):
     ms = start.elapsed_time(end)
     kt = g.kernel_times()
     g.set_profiling(False)
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+    ms = replicas.max_over_ranks(ms, world)
+    replicas.barrier(world)
     assert taken == args.steps, taken
     value = cells * args.steps * world / (ms * 1e-3)
 
@@ -332,9 +320,7 @@ def run_amr(args, world, rank, local):
     stream = torch.cuda.ExternalStream(g.stream())
     leaf_cells = 0
     l0 = g.launch_count()
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    replicas.barrier(world)
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev) as clk:
@@ -347,11 +333,7 @@ def run_amr(args, world, rank, local):
     ms = a.elapsed_time(b)
     phases = g.phase_times()
     launches = g.launch_count() - l0
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(ms, world)
     value = leaf_cells * world / (ms * 1e-3)
     eff_cells = 1
     for d in range(3):
@@ -417,6 +399,7 @@ def run_batch(args, world, rank, local):
         g.run_to(0.15)
         g.close()
     total_ms, updates = 0.0, 0
+    replicas.barrier(world)
     with ClockSampler(dev) as clk:
         for _ in range(args.steps):
             g = GpuBatch1D(sys_, n, dx, u, precision=prec)
@@ -431,6 +414,7 @@ def run_batch(args, world, rank, local):
             t, steps = g.status()
             updates += int((n * steps.astype(np.int64)).sum())
             g.close()
+    total_ms = replicas.max_over_ranks(total_ms, world)
     value = updates * world / (total_ms * 1e-3)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -525,6 +509,8 @@ def run_adjoint(args, world, rank, local):
     fd7 = (J_of(h7) - J_of(-h7)) / (2 * h7)
     g.close()
     f, r, v = float(np.median(fwd_ms)), float(np.median(rec_ms)), float(np.median(rev_ms))
+    # the slowest replica's phases (a ratio of device times; every rank takes the same steps)
+    f, r, v = (replicas.max_over_ranks(x, world) for x in (f, r, v))
     cells = mesh.cells()
     if rank == 0:
         line = {
@@ -583,6 +569,7 @@ def run_batch_adjoint(args, world, rank, local):
     _, steps = g.status()
     g.close()
     f, r, v = float(np.median(fwd)), float(np.median(rec)), float(np.median(rev))
+    f, r, v = (replicas.max_over_ranks(x, world) for x in (f, r, v))
     updates = int((n * steps.astype(np.int64)).sum())
     check = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -652,9 +639,7 @@ def main():
         else:
             run_ours(args, world, rank, local)
     finally:
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        replicas.finish(world)
 
 
 if __name__ == "__main__":
