@@ -284,7 +284,10 @@ def run_ours(args, world, rank, local):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "traffic_source": "ncu capture on 160^3 scaled by cells (profiles/)", "kernel": "fused sweep (3 per stage)",
                          "alg_bytes_per_launch": alg_bytes_per_launch, "avg_launch_ms": per_launch_ms,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"},
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback",
+                         "compute_note": "the sweep is FP64-ALU bound (about 38 flop per algorithmic byte): FP64 pipe "
+                                         "48-52 % active, issue 54-57 % (ncu, profiles/sweep_f64_uniform_160.md); "
+                                         "the HBM fraction is small by construction"},
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()},
             "kernel_share": {k: (v[0] / total_kernel_ms if total_kernel_ms else None) for k, v in kt.items()},
             "gpu_launches": launches,
