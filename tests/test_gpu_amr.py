@@ -2,7 +2,7 @@
 
 The device keeps the reference's block ids, so hierarchies are compared block
 by block: structure (level, coordinates, leaf flag) exactly, block data to the
-north-star 1e-12 relative L1 (and, where the arithmetic order is the same,
+parity bound of 1e-12 relative L1 (and, where the arithmetic order is the same,
 bit for bit)."""
 import numpy as np
 import pytest

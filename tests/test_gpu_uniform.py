@@ -2,7 +2,7 @@
 
 Every test drives the CUDA library through its C ABI (GpuSolver) and the
 oracle through the same calls, on bit-identical inputs. The plain FP64 form
-is held to the north-star tolerance of 1e-12 relative L1 per conserved field
+is held to the parity tolerance of 1e-12 relative L1 per conserved field
 (it is built without FMA contraction and is expected to be bit-exact); the
 mixed form to its stated error bound.
 """
