@@ -36,7 +36,9 @@ CELL_BYTES_3D = 320  # algorithmic bytes per 3-D cell-update (64·F, F = 5)
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 100 for the uniform workload, the 3-D explosion's run length; "
+                         "20 AMR steps; 3 whole runs or gradients for the batch and adjoint workloads)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed"])
@@ -53,7 +55,12 @@ def parse():
     ap.add_argument("--adj-n", type=int, default=512, help="adjoint workload: cells per side")
     ap.add_argument("--adj-steps", type=int, default=400, help="adjoint workload: forward steps")
     ap.add_argument("--amr-base", type=int, default=8, help="AMR base blocks per side (16^3 cells each)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.steps is None:
+        args.steps = {"uniform": 100, "amr": 20}.get(args.workload, 3)
+        if args.impl == "reference":
+            args.steps = 3
+    return args
 
 
 class ClockSampler:
