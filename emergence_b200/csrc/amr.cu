@@ -573,6 +573,9 @@ struct emg_amr {
         }
         b.cap = (int64_t)b.sz[0] * b.sz[1] * b.sz[2];
         b.seq = -1;
+        b.fast = 1;
+        for (int d = 0; d < 3; d++)
+            if (act[d] && (b.f0[d] < 0 || b.f0[d] + b.sz[d] > n_level(l + 1, d) || b.sz[d] > 3 * bd[d] + 1)) b.fast = 0;
         return b;
     }
 
@@ -584,7 +587,9 @@ struct emg_amr {
         if (!nbox) return EMG_OK;
         AmrDev A = view();
         const dim3 gr = box_grid(maxcells, nbox);
-        rbox_gather<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], rem);
+        // boxes inside the domain: gather and first pass fused, straight into the first pass's output
+        rbox_gather_pass0<<<gr, 256, 0, stream>>>(A, dboxes, scr[1], sok[1], rem);
+        rbox_gather<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], rem, 1);
         for (int di = 0; di < (int)dims.size(); di++) {
             if (bsel && !nbsel[di]) continue;
             const dim3 gb(bsel ? (unsigned)nbsel[di] : gr.x, gr.y, 1);
@@ -593,11 +598,11 @@ struct emg_amr {
         }
         int cur = 0;
         for (int di = 0; di < (int)dims.size(); di++) {
-            rbox_pass<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur], sok[cur], scr[1 - cur], sok[1 - cur], di);
+            rbox_pass<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur], sok[cur], scr[1 - cur], sok[1 - cur], di, di == 0 ? 1 : 0);
             cur = 1 - cur;
         }
         rbox_scatter<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur]);
-        launches += 2 + dims.size();
+        launches += 3 + dims.size();
         AMR_CUDA(cudaGetLastError());
         return EMG_OK;
     }

@@ -198,6 +198,7 @@ struct RBox {
     int64_t off;         // scratch offset (cells)
     int64_t cap;         // cells per buffer
     int seq;             // position in a batch of coarsenings (-1: none)
+    int fast;            // fine patch inside the domain over at most four blocks per axis
 };
 
 // thread → (box, cell) over a prefix-sum of box sizes

@@ -277,8 +277,9 @@ __global__ void __launch_bounds__(PBOX_THREADS) pbox_fused(const AmrDev A, const
 // block id is absent for box seq when rem[id] < seq, i.e. it was removed by an
 // earlier coarsening of the batch.
 __global__ void rbox_gather(const AmrDev A, const RBox* __restrict__ boxes, double* buf, unsigned char* ok,
-                            const int* __restrict__ rem) {
+                            const int* __restrict__ rem, int skip_fast) {
     const RBox b = boxes[blockIdx.x];
+    if (skip_fast && b.fast) return;  // gathered inside rbox_gather_pass0
     const int lf = b.l + 1;
     const int64_t n = (int64_t)b.sz[0] * b.sz[1] * b.sz[2];
     // fine patch inside the domain spanning at most four blocks per axis: the
@@ -388,8 +389,9 @@ __global__ void rbox_bc(const AmrDev A, const RBox* __restrict__ boxes, double* 
 // one restriction pass along dims[di] with the shifted stencils and the
 // child-average fallback (amr.rs:674-727)
 __global__ void rbox_pass(const AmrDev A, const RBox* __restrict__ boxes, const double* in, const unsigned char* okin,
-                          double* outb, unsigned char* okout, int di) {
+                          double* outb, unsigned char* okout, int di, int skip_fast) {
     const RBox b = boxes[blockIdx.x];
+    if (skip_fast && b.fast) return;  // first pass done by rbox_gather_pass0
     const int d = A.dims[di];
     int si[3], so[3];
     rbox_size(A, b, di, si);
@@ -427,6 +429,100 @@ __global__ void rbox_pass(const AmrDev A, const RBox* __restrict__ boxes, const 
                 for (int k = 0; k < 5; k++) acc[k] = 0.5 * (in[pa * 5 + k] + in[pb * 5 + k]);
                 o = 1;
             }
+        }
+        double* ov = outb + (b.off + q) * 5;
+        for (int k = 0; k < 5; k++) ov[k] = acc[k];
+        okout[b.off + q] = o;
+    }
+}
+
+// Gather and first restriction pass (along dims[0]) in one kernel for boxes
+// whose fine patch lies inside the domain (RBox::fast): the fine values come
+// straight from the pool through a per-CTA table of the patch's block slots,
+// so the gathered patch never goes through global scratch. Same stencil
+// choice, validity and summation order as rbox_gather + rbox_pass.
+__global__ void rbox_gather_pass0(const AmrDev A, const RBox* __restrict__ boxes, double* outb, unsigned char* okout,
+                                  const int* __restrict__ rem) {
+    const RBox b = boxes[blockIdx.x];
+    if (!b.fast) return;
+    const int lf = b.l + 1;
+    __shared__ int s_slot[64];
+    __shared__ int64_t s_kmin[3];
+    __shared__ int s_nk[3];
+    if (threadIdx.x == 0) {
+        for (int d = 0; d < 3; d++) {
+            s_kmin[d] = A.act[d] ? amr_ediv(b.f0[d], A.bd[d]) : 0;
+            s_nk[d] = A.act[d] ? (int)(amr_ediv(b.f0[d] + b.sz[d] - 1, A.bd[d]) - s_kmin[d] + 1) : 1;
+        }
+    }
+    __syncthreads();
+    const int nt = s_nk[0] * s_nk[1] * s_nk[2];
+    if (threadIdx.x < nt) {
+        const int t = threadIdx.x;
+        const int64_t key[3] = {s_kmin[0] + t / (s_nk[1] * s_nk[2]), s_kmin[1] + (t / s_nk[2]) % s_nk[1], s_kmin[2] + t % s_nk[2]};
+        int id = amr_get(A, lf, key);
+        if (id >= 0 && rem != nullptr && b.seq >= 0 && rem[id] < b.seq) id = -1;
+        s_slot[t] = id;
+    }
+    __syncthreads();
+    const int d = A.dims[0];
+    int so[3];
+    rbox_size(A, b, 1, so);
+    const int sid = b.sz[d];
+    const int shifts[5] = {0, -1, 1, -2, 2};
+    const int64_t n = (int64_t)so[0] * so[1] * so[2];
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        box_coord(q, so, c);
+        const int base = 2 * (int)c[d] + 2;
+        // slot and local cell of the fine cell at position x along d
+        auto locate = [&](int x, int64_t* lc) -> int {
+            int j[3];
+            for (int e = 0; e < 3; e++) {
+                if (!A.act[e]) {
+                    j[e] = 0;
+                    lc[e] = 0;
+                    continue;
+                }
+                const int o = (int)(b.f0[e] - s_kmin[e] * A.bd[e] + (e == d ? x : c[e]));
+                j[e] = o / A.bd[e];
+                lc[e] = o - j[e] * A.bd[e];
+            }
+            return s_slot[(j[0] * s_nk[1] + j[1]) * s_nk[2] + j[2]];
+        };
+        // validity of positions base − 2 .. base + 7 (every stencil the shifts can reach)
+        bool okp[10];
+        for (int i = 0; i < 10; i++) {
+            const int x = base - 2 + i;
+            int64_t lc[3];
+            okp[i] = x >= 0 && x < sid && locate(x, lc) >= 0;
+        }
+        double acc[5] = {0, 0, 0, 0, 0};
+        bool done = false;
+        for (int m = 0; m < 5 && !done; m++) {
+            const int st = base + shifts[m];
+            if (st < 0 || st + 5 >= sid) continue;
+            bool all = true;
+            for (int kk = 0; kk < 6; kk++) all = all && okp[st + kk - (base - 2)];
+            if (all) {
+                for (int kk = 0; kk < 6; kk++) {
+                    int64_t lc[3];
+                    const int slot = locate(st + kk, lc);
+                    double v[5];
+                    amr_load(A, slot, amr_cell(A, lc), v);
+                    for (int k = 0; k < 5; k++) acc[k] = acc[k] + A.wrs[m][kk] * v[k];
+                }
+                done = true;
+            }
+        }
+        unsigned char o = done ? 1 : 0;
+        if (!done && okp[4] && okp[5]) {  // positions base + 2, base + 3: the child average
+            double va[5], vb[5];
+            int64_t lc[3];
+            amr_load(A, locate(base + 2, lc), amr_cell(A, lc), va);
+            amr_load(A, locate(base + 3, lc), amr_cell(A, lc), vb);
+            for (int k = 0; k < 5; k++) acc[k] = 0.5 * (va[k] + vb[k]);
+            o = 1;
         }
         double* ov = outb + (b.off + q) * 5;
         for (int k = 0; k < 5; k++) ov[k] = acc[k];
