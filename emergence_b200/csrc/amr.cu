@@ -650,6 +650,11 @@ struct emg_amr {
                     for (int o2 = -r[2]; o2 <= r[2]; o2++) {
                         int o[3] = {o0, o1, o2};
                         if (!o0 && !o1 && !o2) continue;
+                        // only the six face slabs: the sweeps read ghost rows along
+                        // their own axis within the block's interior lanes, and every
+                        // gather (prediction, restriction, details) reads block
+                        // interiors, so edge and corner ghost regions are never read
+                        if ((o0 != 0) + (o1 != 0) + (o2 != 0) > 1) continue;
                         Key nk;
                         bool inside = true;
                         for (int d = 0; d < 3; d++) {
