@@ -808,7 +808,8 @@ struct emg_amr {
         if (rc) return rc;
         if (nbcleaves)
             for (int di = 0; di < (int)dims.size(); di++) {
-                ghost_bc<<<box_grid(bcell, nbcleaves), 256, 0, stream>>>(A, dbcleaves.p, dlevel.p, didx.p, di);
+                ghost_bc<<<box_grid(2 * (int64_t)ng * std::max(bd[0], 1) * std::max(bd[1], 1), nbcleaves), 256, 0, stream>>>(
+                    A, dbcleaves.p, dlevel.p, didx.p, di);
                 launches++;
             }
         AMR_CUDA(cudaGetLastError());

@@ -590,7 +590,8 @@ __global__ void __launch_bounds__(COPY_THREADS) ghost_copy(const AmrDev A, const
 }
 
 // bc_box over the ghost-extended box of a leaf touching the domain boundary
-// (fill_scratch → bc_box, amr.rs:1205-1217), one active axis per launch.
+// (fill_scratch → bc_box, amr.rs:1205-1217), one active axis per launch,
+// restricted to the face slabs along that axis.
 __global__ void ghost_bc(const AmrDev A, const int* __restrict__ leaves, const int* __restrict__ level,
                          const int64_t* __restrict__ idx, int di) {
     const int slot = leaves[blockIdx.x];
@@ -602,11 +603,22 @@ __global__ void ghost_bc(const AmrDev A, const int* __restrict__ leaves, const i
     for (int e = 0; e < 3; e++) nl[e] = amr_nlevel(A, l, e);
     const int d = A.dims[di];
     double* u = A.u + (int64_t)slot * A.bcell;
-    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+    // the two face slabs along d over the interior lanes (the only ghost cells
+    // that are read); other ghost cells are left as they are
+    int span[3];
+    for (int e = 0; e < 3; e++) span[e] = e == d ? 2 * A.gof[d] : (A.act[e] ? A.bd[e] : 1);
+    const int64_t ns = (int64_t)span[0] * span[1] * span[2];
+    (void)n;
+    for (int64_t t = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; t < ns; t += (int64_t)gridDim.y * blockDim.x) {
         int64_t c[3];
-        c[2] = q % A.ext[2];
-        c[1] = (q / A.ext[2]) % A.ext[1];
-        c[0] = q / ((int64_t)A.ext[1] * A.ext[2]);
+        box_coord(t, span, c);
+        for (int e = 0; e < 3; e++) {
+            if (e == d)
+                c[e] = c[e] < A.gof[d] ? c[e] : c[e] + A.bd[d];
+            else if (A.act[e])
+                c[e] += A.gof[e];
+        }
+        const int64_t q = (c[0] * A.ext[1] + c[1]) * A.ext[2] + c[2];
         const int64_t g[3] = {g0[0] + c[0], g0[1] + c[1], g0[2] + c[2]};
         auto outside = [&](int e) {
             return (g[e] < 0 || g[e] >= nl[e]) && A.bc[e][g[e] >= nl[e] ? 1 : 0] != EMG_BC_PERIODIC;
