@@ -6,8 +6,9 @@
 // refine/coarsen decisions) runs on the host and keeps the block ids of the
 // reference CPU solver (fluid/crates/compressible/src/amr.rs), so the device
 // pool, indexed by block id, mirrors `Amr::blocks`. All numerical work —
-// restriction of edge ancestors, ghost slabs (same-level copies, 6th-order
-// prediction from the coarser level, boundary conditions), the fused WCNS
+// restriction of edge ancestors, the six face ghost slabs of every leaf
+// (same-level copies, 6th-order prediction from the coarser level, boundary
+// conditions; edge and corner ghost regions are never read), the fused WCNS
 // sweeps of every leaf, refluxing, SSP-RK3, the CFL reduction, wavelet details
 // and the data of refined / coarsened blocks — runs on the device; unlike the
 // reference GPU path, a regrid never downloads the solution (only one detail
