@@ -37,7 +37,12 @@ using namespace emg;
 namespace {
 
 constexpr int NG = 6;
-constexpr int SEG = 64;
+// cells per segment (one lane of a sweep CTA): short segments keep the CTAs
+// of unfinished instances evenly spread as instances finish at different
+// batch steps (4096 Riemann problems: 24 cells 2.8 s, 32 cells 2.9 s, 64 cells
+// 3.7 s per run, FP64; the 5 halo midpoints per segment cost less than the
+// imbalance of long ones)
+constexpr int SEG = 24;
 
 struct Inst {
     int64_t off;   // flat index of the instance's first padded cell
@@ -205,25 +210,49 @@ __global__ void batch_adj_rk1(const double* __restrict__ ay, double* an, int64_t
 // Reverse of batch_ghosts: each ghost's cotangent moves to its source cell
 // (normal momentum negated for reflecting walls, dropped for Dirichlet).
 __global__ void batch_adj_ghosts(double* xb, int64_t ntot, const Inst* inst, int ninst, int kind_lo, int kind_hi) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ninst) return;
-    const int64_t off = inst[i].off, n = inst[i].n;
+    // one thread per (instance, field): the ghost cotangents of both sides are
+    // loaded together and cleared, then each side adds them into its source
+    // cells (an outflow side sums its layers first; periodic and reflecting
+    // sources of one side are distinct cells when n >= NG); the sides go one
+    // after the other, as their sources may coincide on a short line
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ninst * 5) return;
+    const int i = t / 5, k = t % 5;
+    const int64_t n = inst[i].n;
+    double* x = xb + k * ntot + inst[i].off;
+    double g[2][NG];
+#pragma unroll
+    for (int gi = 0; gi < NG; gi++) {
+        g[0][gi] = x[gi];
+        g[1][gi] = x[n + NG + gi];
+    }
+#pragma unroll
+    for (int gi = 0; gi < NG; gi++) {
+        x[gi] = 0.0;
+        x[n + NG + gi] = 0.0;
+    }
     for (int side = 0; side < 2; side++) {
         const int kind = side ? kind_hi : kind_lo;
-        for (int gi = 0; gi < NG; gi++) {
-            int64_t src = -1;
-            if (kind == EMG_BC_PERIODIC)
-                src = side ? NG + gi : n + gi;
-            else if (kind == EMG_BC_OUTFLOW)
-                src = side ? n + NG - 1 : NG;
-            else if (kind == EMG_BC_REFLECT)
-                src = side ? n + NG - 1 - gi : 2 * NG - 1 - gi;
-            const int64_t dst = off + (side ? n + NG + gi : gi);
-            for (int k = 0; k < 5; k++) {
-                const double v = xb[k * ntot + dst];
-                xb[k * ntot + dst] = 0.0;
-                if (src >= 0) xb[k * ntot + off + src] += (kind == EMG_BC_REFLECT && k == 1) ? -v : v;
-            }
+        auto src = [&](int gi) -> int64_t {
+            if (kind == EMG_BC_PERIODIC) return side ? NG + gi : n + gi;
+            if (kind == EMG_BC_OUTFLOW) return side ? n + NG - 1 : NG;
+            if (kind == EMG_BC_REFLECT) return side ? n + NG - 1 - gi : 2 * NG - 1 - gi;
+            return -1;
+        };
+        const double sg = (kind == EMG_BC_REFLECT && k == 1) ? -1.0 : 1.0;
+        if (kind == EMG_BC_OUTFLOW) {
+            double acc = 0.0;
+#pragma unroll
+            for (int gi = 0; gi < NG; gi++) acc += g[side][gi];
+            x[src(0)] += acc;
+        } else if ((kind == EMG_BC_PERIODIC || kind == EMG_BC_REFLECT) && n >= NG) {
+            double sv[NG];
+#pragma unroll
+            for (int gi = 0; gi < NG; gi++) sv[gi] = x[src(gi)];
+#pragma unroll
+            for (int gi = 0; gi < NG; gi++) x[src(gi)] = sv[gi] + sg * g[side][gi];
+        } else if (kind == EMG_BC_PERIODIC || kind == EMG_BC_REFLECT) {
+            for (int gi = 0; gi < NG; gi++) x[src(gi)] += sg * g[side][gi];
         }
     }
 }
@@ -484,22 +513,22 @@ struct emg_batch1d {
     int reverse_step(uint64_t b, uint64_t slot) {
         const double* dtb = rec_dt + b * ninst;
         const int kl = bc[0].kind, kh = bc[1].kind;
-        const int gg = (ninst + 127) / 128;
+        const int gg5 = (ninst * 5 + 127) / 128;  // reverse ghost fill: one thread per (instance, field)
         for (double* x : {a_n, a_x, a_y}) B_CUDA(cudaMemsetAsync(x, 0, state_bytes(), stream));
         batch_adj_rk3<<<ninst, 256, 0, stream>>>(a_next, a_n, a_x, ntot, inst, dtb, ninst);
         int rc = adj_sweep(seg_x(slot, 3), seg_theta(slot, 3), a_next, 2.0 / 3.0, a_x, dtb);
         if (rc) return rc;
-        batch_adj_ghosts<<<gg, 128, 0, stream>>>(a_x, ntot, inst, ninst, kl, kh);
+        batch_adj_ghosts<<<gg5, 128, 0, stream>>>(a_x, ntot, inst, ninst, kl, kh);
         batch_adj_rk2<<<ninst, 256, 0, stream>>>(a_x, a_y, a_n, ntot, inst, ninst);
         if ((rc = adj_sweep(seg_x(slot, 2), seg_theta(slot, 2), a_x, 0.25, a_y, dtb))) return rc;
-        batch_adj_ghosts<<<gg, 128, 0, stream>>>(a_y, ntot, inst, ninst, kl, kh);
+        batch_adj_ghosts<<<gg5, 128, 0, stream>>>(a_y, ntot, inst, ninst, kl, kh);
         batch_adj_rk1<<<ninst, 256, 0, stream>>>(a_y, a_n, ntot, inst, ninst);
         // the slot holds Uⁿ as it was before its ghost fill
         batch_set_done<<<(ninst + 255) / 256, 256, 0, stream>>>(inst, dtb, ninst);
         batch_ghosts<<<ninst, 32, 0, stream>>>(seg_x(slot, 1), ntot, inst, ninst, kl, kh,
                                                 EosD{eos.gamma, eos.p_inf, eos.b, eos.q}, dstate, dstate + 5);
         if ((rc = adj_sweep(seg_x(slot, 1), seg_theta(slot, 1), a_y, 1.0, a_n, dtb))) return rc;
-        batch_adj_ghosts<<<gg, 128, 0, stream>>>(a_n, ntot, inst, ninst, kl, kh);
+        batch_adj_ghosts<<<gg5, 128, 0, stream>>>(a_n, ntot, inst, ninst, kl, kh);
         B_CUDA(cudaGetLastError());
         std::swap(a_next, a_n);
         return EMG_OK;
