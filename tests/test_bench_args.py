@@ -1,0 +1,33 @@
+"""bench.py's command line: the default step counts per workload and the
+reference arm (host only; no GPU call)."""
+import importlib.util
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _bench():
+    spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _parse(argv, monkeypatch):
+    monkeypatch.setattr(sys, "argv", ["bench.py"] + argv)
+    return _bench().parse()
+
+
+def test_default_steps_per_workload(monkeypatch):
+    assert _parse([], monkeypatch).steps == 100  # the 3-D explosion's run length
+    assert _parse(["--workload", "amr"], monkeypatch).steps == 20
+    for w in ("batch", "adjoint", "batch_adjoint"):
+        assert _parse(["--workload", w], monkeypatch).steps == 3
+    assert _parse(["--impl", "reference"], monkeypatch).steps == 3
+
+
+def test_driver_flags_override_the_defaults(monkeypatch):
+    a = _parse(["--gpus", "4", "--steps", "7", "--warmup", "5"], monkeypatch)
+    assert (a.gpus, a.steps, a.warmup, a.impl, a.workload) == (4, 7, 5, "ours", "uniform")
+    assert _parse([], monkeypatch).warmup >= 3  # at least 3 untimed warm-up steps
