@@ -126,11 +126,53 @@ __device__ __forceinline__ R hllc(const Eos<R>& e, const R* wl, const R* wr, int
     return ss;
 }
 
+// Reciprocal and reciprocal square root of the mixed form, FP64 to about
+// 1e-12 relative instead of correctly rounded: the PTX estimate
+// (rcp.approx.ftz.f64 / rsqrt.approx.ftz.f64, good to about 2^-20) refined by
+// one Newton–Raphson step, which squares the estimate's relative error
+// (measured on a B200: at most 9.7e-13 and 1.24e-12 over 2^20 inputs). For 1/y, Newton's method
+// on g(r) = 1/r − y gives r ← r + r·(1 − y·r); for 1/√x, on g(r) = 1/r² − x it
+// gives r ← r + (r/2)·(1 − x·r²). Zero, infinite and NaN inputs give
+// non-finite results, which the admissibility tests and the limiter treat as
+// they treat the correctly rounded quotients' infinities. Subnormal inputs are
+// flushed to zero. Only the mixed form uses these: the plain FP64 form keeps
+// IEEE division and square root for bitwise parity with the CPU solver.
+__device__ __forceinline__ double rcp_nr(double y) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(y));
+    const double h = fma(-y, r, 1.0);
+    return fma(r, h, r);
+}
+__device__ __forceinline__ double rsqrt_nr(double x) {
+    double r;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    const double xr = x * r;
+    const double h = fma(-xr, r, 1.0);
+    return fma(0.5 * r, h, r);
+}
+
+// Conserved state of the mixed form with 1/ρ and 1/(γ−1) given (eos.rs:44-54).
+__device__ __forceinline__ void to_cons_nr(const Eos<double>& e, const double* w, double irho, double igm1, double* u) {
+    const double rho = w[0];
+    const double ke = 0.5 * rho * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+    u[0] = rho;
+    u[1] = rho * w[1];
+    u[2] = rho * w[2];
+    u[3] = rho * w[3];
+    u[4] = rho * ((w[4] + e.gamma * e.p_inf) * (irho - e.b) * igm1 + e.q) + ke;
+}
+
+// Admissibility of the mixed form (system.rs:404-407 with eos.rs:75-79).
+__device__ __forceinline__ bool admissible_nr(const Eos<double>& e, double rho, double p) {
+    return isfinite(rho) && isfinite(p) && rho > 0.0 && rcp_nr(rho) > e.b && p + e.p_inf > 0.0;
+}
+
 // HLLC of the mixed form: the Davis wave-speed bounds from FP32 sound speeds,
-// everything else (conserved states, physical fluxes, contact speed, star
-// states) in FP64. An error in a wave speed enters the flux multiplied by a
-// jump of the state across the midpoint, so it vanishes where the data are
-// smooth.
+// the conserved states, physical fluxes, contact speed and star states in
+// FP64 with the Newton-refined reciprocals above in place of divisions. An
+// error in a wave speed enters the flux multiplied by a jump of the state
+// across the midpoint, so it vanishes where the data are smooth; the
+// reciprocals' 1e-12 stays far below the FP32 interpolation error.
 __device__ __forceinline__ double hllc_fs(const Eos<double>& e, const double* wl, const double* wr, int un, double* f) {
     const Eos<float> ef{(float)e.gamma, (float)e.p_inf, (float)e.b, (float)e.q};
     const double cl = (double)sound_speed(ef, (float)wl[0], (float)wl[4]);
@@ -138,9 +180,11 @@ __device__ __forceinline__ double hllc_fs(const Eos<double>& e, const double* wl
     double ul = wl[un], ur = wr[un];
     double sl = fmin(ul - cl, ur - cr);
     double sr = fmax(ul + cl, ur + cr);
+    const double igm1 = rcp_nr(e.gamma - 1.0);
+    const double irl = rcp_nr(wl[0]), irr = rcp_nr(wr[0]);
     double ql[5], qr[5];
-    to_cons(e, wl, ql);
-    to_cons(e, wr, qr);
+    to_cons_nr(e, wl, irl, igm1, ql);
+    to_cons_nr(e, wr, irr, igm1, qr);
     if (sl >= 0.0) {
         flux_wq(wl, ql, un, f);
         return ul;
@@ -150,22 +194,24 @@ __device__ __forceinline__ double hllc_fs(const Eos<double>& e, const double* wl
         return ur;
     }
     double rl = wl[0], rr = wr[0], pl = wl[4], pr = wr[4];
-    double ss = (pr - pl + rl * ul * (sl - ul) - rr * ur * (sr - ur)) / (rl * (sl - ul) - rr * (sr - ur));
+    double ss = (pr - pl + rl * ul * (sl - ul) - rr * ur * (sr - ur)) * rcp_nr(rl * (sl - ul) - rr * (sr - ur));
     const bool left = ss >= 0.0;
     const double* w = left ? wl : wr;
     const double* q = left ? ql : qr;
+    const double irho = left ? irl : irr;
     double s = left ? sl : sr;
     double fx[5];
     flux_wq(w, q, un, fx);
     double rho = w[0], u = w[un];
-    double fac = rho * (s - u) / (s - ss);
+    const double smu = s - u;
+    double fac = rho * smu * rcp_nr(s - ss);
     double qs[5];
     qs[0] = fac;
     qs[1] = fac * w[1];
     qs[2] = fac * w[2];
     qs[3] = fac * w[3];
     qs[un] = fac * ss;
-    qs[4] = fac * (q[4] / rho + (ss - u) * (ss + w[4] / (rho * (s - u))));
+    qs[4] = fac * (q[4] * irho + (ss - u) * (ss + w[4] * irho * rcp_nr(smu)));
 #pragma unroll
     for (int k = 0; k < 5; k++) f[k] = fx[k] + s * (qs[k] - q[k]);
     return ss;

@@ -234,7 +234,9 @@ struct Sweep {
 
     // Mixed form of the midpoint flux: the characteristic projection, the
     // back-projection, the admissibility test and the HLLC flux in FP64 (its
-    // wave-speed bounds from FP32 sound speeds, hllc_fs); the
+    // wave-speed bounds from FP32 sound speeds, hllc_fs), with Newton-refined
+    // reciprocals (rcp_nr, rsqrt_nr: ~1e-12 relative) in place of the
+    // correctly rounded divisions and square root; the
     // ten WENO-Z interpolations (the bulk of the arithmetic) in FP32 on the
     // deviations of each characteristic stencil from its FP64 value at the
     // cell beside the midpoint. WENO-Z is translation invariant (the candidate
@@ -250,14 +252,19 @@ struct Sweep {
         const int j = m + 2;
         const double rho = 0.5 * (Wd[at<STRW>(j, 0, l)] + Wd[at<STRW>(j + 1, 0, l)]);
         const double p4 = 0.5 * (Wd[at<STRW>(j, 4, l)] + Wd[at<STRW>(j + 1, 4, l)]);
-        const double c = sound_speed(e, rho, p4);
-        const double l4un = rho / (2.0 * c);
+        // c² (eos.rs:56-60), 1/c and 1/ρ from three Newton-refined estimates
+        // instead of six correctly rounded divisions and a square root
+        const double irho = rcp_nr(rho);
+        const double c2 = fmax(e.gamma * (p4 + e.p_inf) * irho * irho * rcp_nr(irho - e.b), 0.0);
+        const double ic = rsqrt_nr(c2);
+        const double c = c2 * ic;
+        const double l4un = 0.5 * rho * ic;
         const double l0un = -l4un;
-        const double l04 = 1.0 / (2.0 * c * c);
-        const double l14 = -1.0 / (c * c);
-        const double run4 = c / rho;
+        const double l04 = 0.5 * (ic * ic);
+        const double l14 = -(ic * ic);
+        const double run4 = c * irho;
         const double run0 = -run4;
-        const double r40 = c * c;
+        const double r40 = c2;
         double cl[5], cr[5];
 #pragma unroll
         for (int a = 0; a < 5; a++) {
@@ -291,7 +298,7 @@ struct Sweep {
         wl[4] = r40 * cl[0] + r40 * cl[4];
         wr[4] = r40 * cr[0] + r40 * cr[4];
         fb = false;
-        if (!admissible(e, wl[0], wl[4]) || !admissible(e, wr[0], wr[4])) {
+        if (!admissible_nr(e, wl[0], wl[4]) || !admissible_nr(e, wr[0], wr[4])) {
             fb = true;
 #pragma unroll
             for (int k = 0; k < 5; k++) {

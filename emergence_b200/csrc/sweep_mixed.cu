@@ -1,5 +1,6 @@
-// Mixed-precision form of the fused sweep: midpoint reconstruction and HLLC
-// in FP32; primitives, limiter, divergence and RK accumulation in FP64.
+// Mixed-precision form of the fused sweep: WENO-Z interpolation and the HLLC
+// wave-speed bounds in FP32; primitives, projections, HLLC fluxes, limiter,
+// divergence and RK accumulation in FP64.
 #include "sweep_launch.h"
 
 namespace emg {
