@@ -28,6 +28,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 namespace emg {
 
@@ -479,10 +480,12 @@ __global__ void adj_set_dt(StepCtl* ctl, const double* dt) {
 
 template <int KIND>
 cudaError_t adj_sweep_launch_kind(int d, const AdjSweepParams& p, dim3 grid, cudaStream_t s) {
+    static std::mutex mu;
     static bool prepared[64] = {};  // dynamic shared-memory opt-in, once per device
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
     if (!prepared[dev]) {
         cudaError_t e = cudaFuncSetAttribute(adj_sweep_kernel<0, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)ADJ_SMEM);

@@ -1540,13 +1540,7 @@ struct emg_amr {
         AMR_CUDA(cudaMemcpy(ctl, ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice));
         int rc = ddxl.put(dxl, stream);
         if (rc) return rc;
-        static bool prepared = false;
-        if (!prepared) {
-            cudaError_t e2 = sweep_prepare_f64();
-            if (e2 == cudaSuccess) e2 = sweep_prepare_mixed();
-            if (e2 != cudaSuccess) return set_error(EMG_ERR_CUDA, "sweep setup failed");
-            prepared = true;
-        }
+        if (sweep_prepare_device() != cudaSuccess) return set_error(EMG_ERR_CUDA, "sweep setup failed");
         return EMG_OK;
     }
 

@@ -608,13 +608,7 @@ int emg_batch1d_create(const emg_eos* eos, const emg_opts* opts, const emg_bc bc
         cudaGetLastError();
         return bail(set_error(EMG_ERR_CUDA, "device allocation failed"));
     }
-    static bool prepared = false;
-    if (!prepared) {
-        cudaError_t e = sweep_prepare_f64();
-        if (e == cudaSuccess) e = sweep_prepare_mixed();
-        if (e != cudaSuccess) return bail(set_error(EMG_ERR_CUDA, "sweep setup failed"));
-        prepared = true;
-    }
+    if (sweep_prepare_device() != cudaSuccess) return bail(set_error(EMG_ERR_CUDA, "sweep setup failed"));
     StepCtl c{};
     c.dt = 1.0;  // the batched sweep reads per-instance dt; the control block only gates it
     double st[10];

@@ -20,4 +20,7 @@ int sweep_ctas_per_sm_mixed(int P, int mode);
 // Opt the kernels into their dynamic shared memory size (once per device).
 cudaError_t sweep_prepare_f64();
 cudaError_t sweep_prepare_mixed();
+// Both forms' opt-ins for the current device, done once per device; safe to
+// call from several host threads.
+cudaError_t sweep_prepare_device();
 }  // namespace emg

@@ -349,6 +349,20 @@ using namespace emg;
 
 namespace emg {
 
+cudaError_t sweep_prepare_device() {
+    static std::mutex mu;
+    static bool prepared[64] = {false};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < 64 && prepared[dev]) return cudaSuccess;
+    e = sweep_prepare_f64();
+    if (e == cudaSuccess) e = sweep_prepare_mixed();
+    if (e == cudaSuccess && dev >= 0 && dev < 64) prepared[dev] = true;
+    return e;
+}
+
 int kernel_grid(int64_t work, int threads) {
     int64_t b = (work + threads - 1) / threads;
     if (b < 1) b = 1;
@@ -813,12 +827,9 @@ int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc
         emg_uniform_destroy(h);
         return rc;
     };
-    static bool prepared[64] = {false};
-    if (dev < 64 && !prepared[dev]) {
-        cudaError_t e = sweep_prepare_f64();
-        if (e == cudaSuccess) e = sweep_prepare_mixed();
+    {
+        cudaError_t e = sweep_prepare_device();
         if (e != cudaSuccess) return bail(set_error(EMG_ERR_CUDA, std::string("sweep setup: ") + cudaGetErrorString(e)));
-        prepared[dev] = true;
     }
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(set_error(EMG_ERR_CUDA, "cudaStreamCreate failed"));
@@ -1121,18 +1132,22 @@ int emg_uniform_step_noalloc(const emg_mesh* mesh, const emg_eos* eos, const emg
     if (dev < 0 || dev >= 64) return set_error(EMG_ERR_INVALID, "device index out of range");
     // once per device, with that device current: the scratch address and the
     // sweep kernels' shared-memory attribute
+    static std::mutex scratch_mu;
     static double* scratch_ptr[64] = {nullptr};
-    if (!scratch_ptr[dev]) {
-        double* ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess || !ptr)
-            return set_error(EMG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        e = sweep_prepare_f64();
-        if (e == cudaSuccess) e = sweep_prepare_mixed();
-        if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("sweep setup: ") + cudaGetErrorString(e));
-        scratch_ptr[dev] = ptr;
+    double* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(scratch_mu);
+        if (!scratch_ptr[dev]) {
+            double* ptr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
+            if (e != cudaSuccess || !ptr)
+                return set_error(EMG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            e = sweep_prepare_device();
+            if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("sweep setup: ") + cudaGetErrorString(e));
+            scratch_ptr[dev] = ptr;
+        }
+        base = scratch_ptr[dev];
     }
-    double* base = scratch_ptr[dev];
     emg_uniform h;
     h.device = dev;
     h.stream = (cudaStream_t)stream;
