@@ -1469,11 +1469,17 @@ struct emg_amr {
         for (int i = 0; i < 6; i++) bc[i] = b[i];
         if (cfg.b < 6 || cfg.levels < 1 || cfg.levels > AMR_MAX_LEVELS || cfg.regrid_every < 1)
             return set_error(EMG_ERR_INVALID, "invalid AMR configuration (b >= 6, 1 <= levels <= 12, regrid_every >= 1)");
-        for (int i = 0; i < 6; i++)
+        for (int i = 0; i < 6; i++) {
             if (bc[i].kind == EMG_BC_CHARACTERISTIC)
                 return set_error(EMG_ERR_INVALID, "characteristic boundaries are not available on the AMR path");
+            if (bc[i].kind < 0 || bc[i].kind > 4) return set_error(EMG_ERR_INVALID, "unknown boundary condition");
+        }
         if (opts.mode != EMG_MODE_WENO && opts.mode != EMG_MODE_HYBRID && opts.mode != EMG_MODE_CENTRAL)
             return set_error(EMG_ERR_INVALID, "unknown flux mode");
+        if (opts.mode == EMG_MODE_HYBRID && !(opts.tol > 0.0))
+            return set_error(EMG_ERR_INVALID, "hybrid mode needs tol > 0");
+        if (opts.precision != EMG_PRECISION_F64 && opts.precision != EMG_PRECISION_MIXED)
+            return set_error(EMG_ERR_INVALID, "unknown precision");
         ng = (int)std::max<int64_t>(cfg.ghosts, 5);
         for (int d = 0; d < 3; d++) {
             bd[d] = cfg.base_blocks[d] == 0 ? 1 : (int)cfg.b;
@@ -1485,6 +1491,9 @@ struct emg_amr {
             if (act[d]) dims.push_back(d);
         }
         if (dims.empty()) return set_error(EMG_ERR_INVALID, "no active axis");
+        for (int d : dims)
+            if ((bc[2 * d].kind == EMG_BC_PERIODIC) != (bc[2 * d + 1].kind == EMG_BC_PERIODIC))
+                return set_error(EMG_ERR_INVALID, "periodic boundaries must be paired");
         if (cfg.b > 32) return set_error(EMG_ERR_INVALID, "block side above 32");
         levels = (int)cfg.levels;
         dxl.assign(3 * levels, 0.0);

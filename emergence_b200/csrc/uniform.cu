@@ -764,18 +764,7 @@ int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc
                        const double* u_aos, size_t len, emg_uniform** out) {
     if (!mesh || !eos || !bc || !opts || !u_aos || !out) return set_error(EMG_ERR_INVALID, "null argument");
     *out = nullptr;
-    int dev = 0;
-    {
-        int n = 0;
-        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
-            cudaGetLastError();
-            return set_error(EMG_ERR_NO_DEVICE, "no CUDA device visible");
-        }
-        EMG_CUDA(cudaGetDevice(&dev));
-        cudaDeviceProp pr;
-        EMG_CUDA(cudaGetDeviceProperties(&pr, dev));
-        if (pr.major != 10) return set_error(EMG_ERR_NO_DEVICE, "device is not sm_100 (B200)");
-    }
+    // arguments first, so that a bad call is reported as such on any host
     if (mesh->ng < 5) return set_error(EMG_ERR_INVALID, "the WCNS stencil needs ng >= 5 ghost layers");
     int ndim = 0;
     for (int d = 0; d < 3; d++) {
@@ -798,6 +787,23 @@ int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc
     for (int d = 0; d < 3; d++) {
         const bool per0 = bc[2 * d].kind == EMG_BC_PERIODIC, per1 = bc[2 * d + 1].kind == EMG_BC_PERIODIC;
         if (mesh->n[d] > 1 && per0 != per1) return set_error(EMG_ERR_INVALID, "periodic boundaries must be paired");
+    }
+    {
+        size_t padded = 1;
+        for (int d = 0; d < 3; d++) padded *= (size_t)(mesh->n[d] > 1 ? mesh->n[d] + 2 * mesh->ng : 1);
+        if (padded != len) return set_error(EMG_ERR_INVALID, "state length does not match the padded mesh");
+    }
+    int dev = 0;
+    {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+            cudaGetLastError();
+            return set_error(EMG_ERR_NO_DEVICE, "no CUDA device visible");
+        }
+        EMG_CUDA(cudaGetDevice(&dev));
+        cudaDeviceProp pr;
+        EMG_CUDA(cudaGetDeviceProperties(&pr, dev));
+        if (pr.major != 10) return set_error(EMG_ERR_NO_DEVICE, "device is not sm_100 (B200)");
     }
     emg_uniform* h = new emg_uniform();
     h->device = dev;
