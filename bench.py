@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg of the uniform workload")
     ap.add_argument("--no-autotune", action="store_true", help="uniform and AMR workloads: use the planned sweep shapes")
+    ap.add_argument("--reference-gpu", action="store_true",
+                    help="uniform workload: also time the reference's own GPU kernels on the same grid "
+                         "(oracle/_ref/librefgpu.so, built from the reference tree by `make -C oracle refgpu`)")
     ap.add_argument("--workload", default="uniform", choices=["uniform", "amr", "batch", "adjoint", "batch_adjoint"],
                     help="uniform: 3-D explosion 256^3; amr: 3-D shock-bubble on block AMR (base 128^3, 3 levels); "
                          "batch: 4096 independent 1-D Riemann problems; adjoint: discrete adjoint of the 2-D "
@@ -222,8 +225,13 @@ def run_ours(args, world, rank, local):
             traffic = tr["bytes_per_cell_per_launch"] * cells
     except Exception:
         pass
-    u_main = g.download() if not args.no_mixed else None
+    u_main = g.download() if not (args.no_mixed and not args.reference_gpu) else None
     g.close()
+
+    # ---- the reference's own GPU kernels on the same workload (same-box baseline)
+    ref_gpu = None
+    if args.reference_gpu and prec == Precision.F64 and rank == 0:
+        ref_gpu = reference_gpu_leg(args, sys_, mesh, u, bc, cells, ms / args.steps, u_main)
 
     # ---- mixed-precision form (FP32 flux, FP64 state): same workload and steps
     mixed = None
@@ -303,7 +311,73 @@ def run_ours(args, world, rank, local):
             "cpu_baseline": cpu,
             "mixed": mixed,
         }
+        if ref_gpu is not None:
+            line["reference_gpu"] = ref_gpu
         print(json.dumps(line), flush=True)
+
+
+def reference_gpu_leg(args, sys_, mesh, u, bc, cells, ours_ms_per_step, u_ours):
+    """The reference's uniform-solver kernels (fluid/crates/compressible-cuda/
+    src/kernels.cu, compiled unmodified for sm_100a) driven in the order of its
+    GpuSolver<f64> (oracle/ref_gpu.cu) over warmup + steps steps of the same
+    explosion, each step's dt from its own rate kernel and host max as in its
+    run_to loop. Timed with CUDA events on its stream; the per-step device→host
+    copy of the rates is part of that design and inside the timed region."""
+    import ctypes as C
+    import numpy as np
+    import torch
+    from emergence_b200._abi import EmgOpts
+    from emergence_b200.physics import FluxMode
+    from emergence_b200.solver import _c_bcs, _c_eos, _c_mesh
+
+    path = os.path.join(ROOT, "oracle", "_ref", "librefgpu.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/librefgpu.so is not built (make -C oracle refgpu needs the reference tree)"}
+    L = C.CDLL(path)
+    L.refgpu_last_error.restype = C.c_char_p
+    L.refgpu_stream.restype = C.c_void_p
+    L.refgpu_stream.argtypes = [C.c_void_p]
+    for name in ("refgpu_advance", "refgpu_download", "refgpu_synchronize", "refgpu_destroy"):
+        getattr(L, name).restype = C.c_int
+    L.refgpu_advance.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]
+    L.refgpu_download.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_size_t]
+    L.refgpu_synchronize.argtypes = [C.c_void_p]
+    L.refgpu_destroy.argtypes = [C.c_void_p]
+    m, e, b = _c_mesh(mesh), _c_eos(sys_.eos), _c_bcs(bc)
+    o = EmgOpts(0.5, 1e-3, FluxMode.Weno, 1, 0, 0)
+    ua = np.ascontiguousarray(u, dtype=np.float64)
+    h = C.c_void_p()
+    if L.refgpu_create(C.byref(m), C.byref(e), b, C.byref(o), ua.ctypes.data_as(C.POINTER(C.c_double)),
+                       C.c_size_t(mesh.len()), C.byref(h)):
+        return {"error": L.refgpu_last_error().decode()}
+    taken = C.c_uint64()
+    try:
+        if L.refgpu_advance(h, args.warmup, C.byref(taken)) or L.refgpu_synchronize(h):
+            return {"error": L.refgpu_last_error().decode()}
+        s = torch.cuda.ExternalStream(L.refgpu_stream(h))
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(s)
+        rc = L.refgpu_advance(h, args.steps, C.byref(taken))
+        z.record(s)
+        z.synchronize()
+        if rc:
+            return {"error": L.refgpu_last_error().decode()}
+        rms = a.elapsed_time(z)
+        out = np.empty_like(ua)
+        if L.refgpu_download(h, out.ctypes.data_as(C.POINTER(C.c_double)), C.c_size_t(mesh.len())):
+            return {"error": L.refgpu_last_error().decode()}
+    finally:
+        L.refgpu_destroy(h)
+    res = {"value": cells * args.steps / (rms * 1e-3), "unit": "cell-updates/s", "ms_per_step": rms / args.steps,
+           "ours_speedup": (rms / args.steps) / ours_ms_per_step,
+           "what": "the reference's compressible-cuda kernels (unmodified source, nvcc sm_100a) in GpuSolver<f64> "
+                   "launch order: ghost, prim, theta/midflux/flux/accum per axis, rk per stage; dt_cfl each step"}
+    if u_ours is not None:
+        ia, ib = mesh.interior(out).reshape(-1, 5), mesh.interior(u_ours).reshape(-1, 5)
+        num, den = np.abs(ia - ib).sum(axis=0), np.abs(ib).sum(axis=0)
+        res["rel_l1_vs_ours"] = [float(x) for x in num / np.maximum(den, 1e-3 * den[0])]
+    return res
 
 
 def run_amr(args, world, rank, local):
