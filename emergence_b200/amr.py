@@ -96,6 +96,11 @@ class GpuAmr:
         check(lib().emg_amr_block_count(self._h, C.byref(b), C.byref(l)))
         return b.value, l.value
 
+    def leaf_count(self):
+        """Leaf blocks of the hierarchy (GpuAmr::leaf_count,
+        fluid/crates/compressible-cuda/src/amr.rs:855-857)."""
+        return self.block_count()[1]
+
     def structure(self):
         nb, _ = self.block_count()
         out = np.zeros((nb, 5), dtype=np.int64)

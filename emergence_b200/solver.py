@@ -145,6 +145,12 @@ class GpuSolver:
         check(lib().emg_uniform_totals(self._h, _dptr(out)))
         return out
 
+    @staticmethod
+    def nv():
+        """Conserved variables per cell: 5 for the Euler system (GpuSolver::nv,
+        fluid/crates/compressible-cuda/src/lib.rs:474-476)."""
+        return 5
+
     def counters(self):
         """[faces, shock-path faces, first-order fallbacks, limited faces]."""
         out = (C.c_uint64 * 4)()
