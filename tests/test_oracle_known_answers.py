@@ -291,3 +291,46 @@ def test_weno_interpolation_is_exact_for_constants_and_bounded_at_jumps():
     # quadratic data: each candidate stencil is exact, so the result is too
     f = lambda x: 1.0 + 0.5 * x - 0.25 * x * x
     assert abs(O.weno5z_interp(f(0), f(1), f(2), f(3), f(4)) - f(2.5)) < 1e-12
+
+
+# examples/validate.rs:24-65 and :155-159: Sod, Lax, Toro test 3 (pressure
+# ratio 1e5) and the stiffened-gas water shock tube (eos.rs:88, 1 GPa : 1 bar),
+# each in WENO and Hybrid mode against the exact Riemann solution (exact.rs).
+# The reference prints L1(ρ)/|ρ| and its rate for N = 100…1600; here the
+# error must fall with N at about first order (discontinuous solutions) and
+# stay under a bound of about twice the value the oracle reaches at N = 400.
+RIEMANN_CASES = {
+    "sod": (Nasg.ideal(1.4), (1.0, 0.0, 1.0), (0.125, 0.0, 0.1), 0.2, 4e-3),
+    "lax": (Nasg.ideal(1.4), (0.445, 0.698, 3.528), (0.5, 0.0, 0.571), 0.14, 1.5e-2),
+    "toro3": (Nasg.ideal(1.4), (1.0, 0.0, 1000.0), (1.0, 0.0, 0.01), 0.012, 5e-2),
+    "water": (Nasg.stiffened(4.4, 6.0e8), (1000.0, 0.0, 1e9), (1000.0, 0.0, 1e5), 1.2e-4, 2e-3),
+}
+
+
+@pytest.mark.parametrize("mode", [FluxMode.Weno, FluxMode.Hybrid])
+@pytest.mark.parametrize("case", list(RIEMANN_CASES))
+def test_riemann_problems_converge_to_the_exact_solution(case, mode):
+    eos, left, right, t_end, bound = RIEMANN_CASES[case]
+    sys_ = Euler(eos)
+    errs = []
+    for n in (100, 200, 400):
+        mesh = Mesh.new((n, 1, 1), (0, 0, 0), (1, 1, 1), ng=6)
+        x = mesh.centres()
+        w = np.zeros(x[0].shape + (5,))
+        on_left = x[0] < 0.5
+        for k, q in ((0, 0), (1, 1), (4, 2)):
+            w[..., k] = np.where(on_left, left[q], right[q])
+        u = initial_state(sys_, mesh, w)
+        bc = [[Bc.Outflow, Bc.Outflow], [Bc.Periodic] * 2, [Bc.Periodic] * 2]
+        s = O.OracleSolver(sys_, mesh, u, bc=bc, cfl=0.4, mode=mode)
+        s.run_to(t_end)
+        wf = sys_.to_prim(mesh.interior(s.download()))[:, 0, 0]
+        assert np.all(wf[:, 0] > 0) and np.all(wf[:, 4] + eos.p_inf > 0)  # admissible throughout
+        xc = mesh.centres()[0][:, 0, 0]
+        exact = O.exact_sample(left, right, (xc - 0.5) / t_end, eos)[:, 0]
+        errs.append(np.mean(np.abs(wf[:, 0] - exact)) / np.mean(np.abs(exact)))
+    assert errs[0] > errs[1] > errs[2], errs
+    assert math.log2(errs[0] / errs[2]) / 2 >= 0.6, errs
+    assert errs[2] < bound, errs
+    if case == "toro3":
+        assert s.counters()[3] > 0  # the 1e5 pressure jump needs the positivity limiter
