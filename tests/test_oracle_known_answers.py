@@ -334,3 +334,40 @@ def test_riemann_problems_converge_to_the_exact_solution(case, mode):
     assert errs[2] < bound, errs
     if case == "toro3":
         assert s.counters()[3] > 0  # the 1e5 pressure jump needs the positivity limiter
+
+
+# examples/validate.rs:66-116: Shu's isentropic vortex (γ = 1.4, β = 5, mean
+# flow (1, 1), periodic [−5, 5]², t = 2), a smooth exact solution, with the
+# reference's fixed dt ∝ dx·(20/N)^(2/3) so that the time error stays below the
+# space error. The split-form central flux is 6th order; the WCNS WENO-Z path
+# is high order but pre-asymptotic at N ≤ 80 (the oracle: rates 4.3 then 3.3).
+def _vortex(x, y, t, g=1.4, beta=5.0):
+    wrap = lambda a: np.mod(a + 5.0, 10.0) - 5.0
+    xr, yr = wrap(x - t), wrap(y - t)
+    r2 = xr * xr + yr * yr
+    f = beta / (2 * math.pi) * np.exp(0.5 * (1 - r2))
+    tt = 1 - (g - 1) * beta * beta / (8 * g * math.pi ** 2) * np.exp(1 - r2)
+    rho = tt ** (1 / (g - 1))
+    w = np.zeros(x.shape + (5,))
+    w[..., 0], w[..., 1], w[..., 2], w[..., 4] = rho, 1 - f * yr, 1 + f * xr, rho * tt
+    return w
+
+
+@pytest.mark.parametrize("mode, min_rate, bound", [(FluxMode.Central, 5.0, 1e-6), (FluxMode.Hybrid, 3.0, 2e-5),
+                                                   (FluxMode.Weno, 3.0, 2e-5)])
+def test_isentropic_vortex_converges_at_high_order(mode, min_rate, bound):
+    errs = []
+    for n in (20, 40, 80):
+        mesh = Mesh.new((n, n, 1), (-5, -5, 0), (5, 5, 1), ng=6)
+        x = mesh.centres()
+        u = initial_state(SYS, mesh, _vortex(x[0], x[1], 0.0))
+        s = O.OracleSolver(SYS, mesh, u, bc=[[Bc.Periodic] * 2] * 3, cfl=0.4, mode=mode)
+        dt = 0.4 * mesh.dx[0] / 3.0 * min((20.0 / n) ** (2.0 / 3.0), 1.0)
+        steps = math.ceil(2.0 / dt)
+        for _ in range(steps):
+            s.step(2.0 / steps)
+        rho = SYS.to_prim(mesh.interior(s.download()))[..., 0]
+        errs.append(float(np.mean(np.abs(rho - _vortex(x[0], x[1], 2.0)[..., 0]))))
+    rates = [math.log2(errs[i] / errs[i + 1]) for i in range(2)]
+    assert min(rates) >= min_rate, (errs, rates)
+    assert errs[2] < bound, errs
