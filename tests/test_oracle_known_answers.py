@@ -371,3 +371,38 @@ def test_isentropic_vortex_converges_at_high_order(mode, min_rate, bound):
     rates = [math.log2(errs[i] / errs[i + 1]) for i in range(2)]
     assert min(rates) >= min_rate, (errs, rates)
     assert errs[2] < bound, errs
+
+
+# examples/validate.rs:119-150: Shu–Osher (Mach-3 shock into an entropy wave,
+# t = 1.8) against a finer run of the same solver, cell averages compared.
+# The reference uses 6400 cells; 800 keep the CPU suite short. The hybrid
+# sensor keeps most faces on the central flux (the reference prints the
+# share of shock-path faces) at the accuracy of the all-WENO run.
+def _shu_osher(n, mode):
+    mesh = Mesh.new((n, 1, 1), (-5, 0, 0), (5, 1, 1), ng=6)
+    x = mesh.centres()[0]
+    w = np.zeros(x.shape + (5,))
+    pre = x < -4.0
+    w[..., 0] = np.where(pre, 3.857143, 1.0 + 0.2 * np.sin(5.0 * x))
+    w[..., 1] = np.where(pre, 2.629369, 0.0)
+    w[..., 4] = np.where(pre, 10.33333, 1.0)
+    bc = [[Bc.Outflow, Bc.Outflow], [Bc.Periodic] * 2, [Bc.Periodic] * 2]
+    s = O.OracleSolver(SYS, mesh, initial_state(SYS, mesh, w), bc=bc, cfl=0.4, mode=mode)
+    s.run_to(1.8)
+    return SYS.to_prim(mesh.interior(s.download()))[:, 0, 0, 0], s.counters()
+
+
+def test_shu_osher_converges_and_the_hybrid_sensor_limits_the_shock_path():
+    ref, _ = _shu_osher(800, FluxMode.Weno)
+    errs = {}
+    for mode in (FluxMode.Weno, FluxMode.Hybrid):
+        for n in (100, 200):
+            rho, c = _shu_osher(n, mode)
+            errs[mode, n] = float(np.mean(np.abs(rho - ref.reshape(n, 800 // n).mean(axis=1))))
+            if mode == FluxMode.Hybrid:
+                assert 0 < c[1] < c[0]  # shock-path faces are a strict subset
+            else:
+                assert c[1] == c[0]
+    for mode in (FluxMode.Weno, FluxMode.Hybrid):
+        assert errs[mode, 200] < 0.75 * errs[mode, 100], errs
+    assert abs(errs[FluxMode.Hybrid, 200] / errs[FluxMode.Weno, 200] - 1.0) < 0.05, errs
