@@ -128,7 +128,8 @@ def dist_init(args):
 
 def cpu_reference_steps(n, steps, warmup):
     """Time the reference CPU solver (C++ restatement, all host threads) on an
-    n^3 instance of the same explosion; returns (cell-updates/s, seconds/step, threads)."""
+    n^3 instance of the same explosion; returns (cell-updates/s, seconds/step,
+    threads, the hash of the final state as cpu_validate.rs:7-22 prints it)."""
     from emergence_b200 import workloads as W
     from emergence_b200.physics import FluxMode
     from oracle import pyoracle as O
@@ -140,7 +141,7 @@ def cpu_reference_steps(n, steps, warmup):
     for _ in range(steps):
         o.step(o.dt_cfl())
     el = time.perf_counter() - t0
-    return mesh.cells() * steps / el, el / max(steps, 1), O.num_threads()
+    return mesh.cells() * steps / el, el / max(steps, 1), O.num_threads(), f"{O.state_hash(mesh, o.download()):016x}"
 
 
 def run_reference(args, world, rank):
@@ -149,7 +150,7 @@ def run_reference(args, world, rank):
         return
     # bounded sample of the workload: a 96^3 instance of the same explosion
     n = 96
-    value, sps, threads = cpu_reference_steps(n, args.steps, args.warmup)
+    value, sps, threads, fnv = cpu_reference_steps(n, args.steps, args.warmup)
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sps * 1e3,
@@ -157,7 +158,8 @@ def run_reference(args, world, rank):
         "config": {"workload": f"3-D spherical explosion {args.n}^3, WCNS WENO5-Z + HLLC + positivity, SSP-RK3, CFL 0.5",
                    "sample": f"{n}^3 instance of the same explosion per step"},
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-                         "sample": f"SSP-RK3 steps of a {n}^3 instance, C++ restatement of the reference CPU f64 solver"},
+                         "sample": f"SSP-RK3 steps of a {n}^3 instance, C++ restatement of the reference CPU f64 solver",
+                         "state_fnv": fnv},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -280,10 +282,11 @@ def run_ours(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nb = 64
-        v, sps, threads = cpu_reference_steps(nb, 2, 1)
+        v, sps, threads, fnv = cpu_reference_steps(nb, 2, 1)
         cpu = {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
                "sample": f"2 SSP-RK3 steps of a {nb}^3 instance of the same explosion, "
-                         "C++ restatement of the reference CPU f64 solver (OpenMP over pencils)"}
+                         "C++ restatement of the reference CPU f64 solver (OpenMP over pencils)",
+               "state_fnv": fnv}
 
     if rank == 0:
         line = {

@@ -6,11 +6,11 @@ limiter, SSP-RK3, ghost fill, CFL reduction), behind the C ABI of
 ``include/emergence_b200.h``.
 """
 from .physics import Bc, Euler, FluxMode, Mesh, Nasg, Precision, initial_state
-from .solver import GpuSolver, device_count
+from .solver import GpuSolver, device_count, state_hash
 from .amr import GpuAmr
 from .batch import GpuBatch1D
 from .adjoint import DifferentiableSolver
 from ._abi import EmgError, LIB_PATH
 
-__all__ = ["Bc", "Euler", "FluxMode", "Mesh", "Nasg", "Precision", "initial_state", "GpuSolver", "GpuAmr", "GpuBatch1D", "DifferentiableSolver", "device_count",
+__all__ = ["Bc", "Euler", "FluxMode", "Mesh", "Nasg", "Precision", "initial_state", "GpuSolver", "GpuAmr", "GpuBatch1D", "DifferentiableSolver", "device_count", "state_hash",
            "EmgError", "LIB_PATH"]

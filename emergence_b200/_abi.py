@@ -60,6 +60,7 @@ SIGNATURES = {
     "emg_last_error": (C.c_char_p, []),
     "emg_version": (C.c_char_p, []),
     "emg_device_count": (C.c_int, [C.POINTER(C.c_int)]),
+    "emg_state_hash": (C.c_int, [C.POINTER(EmgMesh), _D, C.c_size_t, _U64]),
     "emg_uniform_create": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc), C.POINTER(EmgOpts),
                                      _D, C.c_size_t, C.POINTER(_P)]),
     "emg_uniform_destroy": (C.c_int, [_P]),

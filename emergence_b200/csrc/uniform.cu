@@ -760,6 +760,32 @@ int emg_device_count(int* count) {
     return EMG_OK;
 }
 
+int emg_state_hash(const emg_mesh* mesh, const double* u_aos, size_t len, uint64_t* out) {
+    if (!mesh || !u_aos || !out) return set_error(EMG_ERR_INVALID, "null argument");
+    int64_t m[3], g[3];
+    size_t padded = 1;
+    for (int d = 0; d < 3; d++) {
+        if (mesh->n[d] < 1 || mesh->ng < 0) return set_error(EMG_ERR_INVALID, "mesh extents must be >= 1");
+        g[d] = mesh->n[d] > 1 ? mesh->ng : 0;
+        m[d] = mesh->n[d] + 2 * g[d];
+        padded *= (size_t)m[d];
+    }
+    if (padded != len) return set_error(EMG_ERR_INVALID, "state length does not match the padded mesh");
+    uint64_t h = 0xcbf29ce484222325ull;
+    for (int64_t i = 0; i < mesh->n[0]; i++)
+        for (int64_t j = 0; j < mesh->n[1]; j++)
+            for (int64_t k = 0; k < mesh->n[2]; k++) {
+                const double* v = u_aos + 5 * (((i + g[0]) * m[1] + (j + g[1])) * m[2] + (k + g[2]));
+                for (int q = 0; q < 5; q++) {
+                    uint64_t bits;
+                    std::memcpy(&bits, v + q, sizeof bits);
+                    h = (h ^ bits) * 0x100000001b3ull;
+                }
+            }
+    *out = h;
+    return EMG_OK;
+}
+
 int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
                        const double* u_aos, size_t len, emg_uniform** out) {
     if (!mesh || !eos || !bc || !opts || !u_aos || !out) return set_error(EMG_ERR_INVALID, "null argument");

@@ -191,6 +191,16 @@ class GpuSolver:
         return n.value
 
 
+def state_hash(mesh, u):
+    """64-bit fingerprint of a ghost-padded AoS conserved state (host code, no
+    device): the hash of fluid/crates/compressible/examples/cpu_validate.rs:7-22
+    over the interior cells. Equal states, bit for bit, give equal hashes."""
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    out = C.c_uint64()
+    check(lib().emg_state_hash(C.byref(_c_mesh(mesh)), _dptr(u), mesh.len(), C.byref(out)))
+    return out.value
+
+
 def device_count():
     n = C.c_int()
     check(lib().emg_device_count(C.byref(n)))

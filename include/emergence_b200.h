@@ -119,6 +119,16 @@ const char* emg_version(void);
 /* Number of visible sm_100 devices. */
 int emg_device_count(int* count);
 
+/* Fingerprint of a ghost-padded AoS conserved state (host memory, host code:
+ * no device needed): over the interior cells in (i, j, k) order and their 5
+ * fields in order, h ← (h XOR bits(v))·0x100000001b3 from h = 0xcbf29ce484222325,
+ * each value's IEEE-754 bits folded in whole. Equal states give equal
+ * hashes; ghost layers do not enter. Replaces the `hash` of
+ * fluid/crates/compressible/examples/cpu_validate.rs:7-22, which the
+ * reference's CPU benchmark script uses to show that two builds agree bit for
+ * bit. `len` counts cells and must equal the padded mesh. */
+int emg_state_hash(const emg_mesh* mesh, const double* u_aos, size_t len, uint64_t* out);
+
 /* ------------------------------------------------------------------ uniform grids */
 typedef struct emg_uniform emg_uniform;
 

@@ -10,6 +10,7 @@
 #include "../include/emergence_b200.h"
 
 #include <cstdio>
+#include <cstring>
 #include <string>
 
 using namespace oracle;
@@ -40,6 +41,28 @@ Euler<double> to_sys(const emg_eos* e) { return Euler<double>{Nasg<double>{e->ga
 extern "C" {
 
 const char* emgo_last_error(void) { return g_err.c_str(); }
+
+// fluid/crates/compressible/examples/cpu_validate.rs:7-22: FNV-style hash of
+// the interior conserved state, cells in (i, j, k) order, each value's bits
+// folded in whole.
+int emgo_state_hash(const emg_mesh* mesh, const double* u_aos, size_t len, uint64_t* out) {
+    if (!mesh || !u_aos || !out) return fail(1, "null argument");
+    const Mesh m = to_mesh(mesh);
+    if ((size_t)m.len() != len) return fail(1, "state length does not match the padded mesh");
+    uint64_t h = 0xcbf29ce484222325ull;
+    for (int64_t i = 0; i < m.n[0]; i++)
+        for (int64_t j = 0; j < m.n[1]; j++)
+            for (int64_t k = 0; k < m.n[2]; k++) {
+                const size_t q = (size_t)m.idx(i + m.g(0), j + m.g(1), k + m.g(2));
+                for (int f = 0; f < 5; f++) {
+                    uint64_t bits;
+                    std::memcpy(&bits, u_aos + 5 * q + f, sizeof bits);
+                    h = (h ^ bits) * 0x100000001b3ull;
+                }
+            }
+    *out = h;
+    return 0;
+}
 
 int emgo_num_threads(void) {
 #ifdef _OPENMP

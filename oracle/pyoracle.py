@@ -28,6 +28,7 @@ SIGS = {
     "emgo_last_error": (C.c_char_p, []),
     "emgo_num_threads": (C.c_int, []),
     "emgo_set_num_threads": (None, [C.c_int]),
+    "emgo_state_hash": (C.c_int, [C.POINTER(EmgMesh), _D, C.c_size_t, C.POINTER(C.c_uint64)]),
     "emgo_uniform_create": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc), C.POINTER(EmgOpts),
                                       _D, C.c_size_t, C.POINTER(_P)]),
     "emgo_uniform_destroy": (C.c_int, [_P]),
@@ -352,6 +353,16 @@ def exact_sample(left, right, xi, eos_l, eos_r=None):
     _chk(lib().emgo_exact_sample(dptr(arr(left)), dptr(arr(right)), C.byref(el), C.byref(er), dptr(xi), xi.size,
                                  dptr(out)))
     return out  # rho, u, p per xi
+
+
+def state_hash(mesh, u):
+    """The hash of fluid/crates/compressible/examples/cpu_validate.rs:7-22 over
+    the interior cells of a ghost-padded AoS state."""
+    from emergence_b200.solver import _c_mesh
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    out = C.c_uint64()
+    _chk(lib().emgo_state_hash(C.byref(_c_mesh(mesh)), dptr(u), mesh.len(), C.byref(out)))
+    return out.value
 
 
 # ---- block AMR (amr_oracle.hpp)
