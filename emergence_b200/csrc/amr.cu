@@ -1640,6 +1640,7 @@ int emg_amr_create_from_blocks(const emg_amr_config* cfg, const emg_eos* eos, co
                                const double* u, emg_amr** out) {
     if (!cfg || !eos || !lo || !hi || !bc || !opts || !desc || !u || !out) return set_error(EMG_ERR_INVALID, "null argument");
     *out = nullptr;
+    if (nblocks == 0) return set_error(EMG_ERR_INVALID, "a hierarchy needs at least one block");
     emg_amr* h = new emg_amr();
     int rc = h->setup(cfg, eos, lo, hi, bc, opts);
     auto bail = [&](int code) {

@@ -191,3 +191,14 @@ def test_adjoint_create_rejects_forms_it_does_not_differentiate():
         rc = lib().emg_adjoint_create(C.byref(m), C.byref(EOS), bcs(OUT6), C.byref(o),
                                       u.ctypes.data_as(C.POINTER(C.c_double)), padded(m), C.byref(h))
         assert rc == INVALID and want in err() and not h.value
+
+
+def test_amr_create_from_blocks_rejects_an_empty_hierarchy():
+    cfg = EmgAmrConfig(16, 2, 1e-3, 4, (4, 4, 0), 5)
+    lo_a, hi_a = (C.c_double * 3)(0.0, 0.0, 0.0), (C.c_double * 3)(1.0, 1.0, 0.0)
+    desc = (C.c_int64 * 5)()
+    u = (C.c_double * 5)()
+    h = C.c_void_p()
+    rc = lib().emg_amr_create_from_blocks(C.byref(cfg), C.byref(EOS), lo_a, hi_a, bcs(OUT6), C.byref(opts()), desc, 0,
+                                          u, C.byref(h))
+    assert rc == INVALID and "at least one block" in err() and not h.value
