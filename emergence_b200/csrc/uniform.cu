@@ -786,22 +786,23 @@ int emg_state_hash(const emg_mesh* mesh, const double* u_aos, size_t len, uint64
     return EMG_OK;
 }
 
-int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
-                       const double* u_aos, size_t len, emg_uniform** out) {
-    if (!mesh || !eos || !bc || !opts || !u_aos || !out) return set_error(EMG_ERR_INVALID, "null argument");
-    *out = nullptr;
-    // arguments first, so that a bad call is reported as such on any host
+// Argument checks shared by emg_uniform_create and emg_uniform_step_noalloc,
+// made before any device work. *ndim receives the number of active axes and
+// *padded the padded cell count m0·m1·m2.
+static int check_uniform_args(const emg_mesh* mesh, const emg_bc bc[6], const emg_opts* opts, int* ndim, size_t* padded) {
     if (mesh->ng < 5) return set_error(EMG_ERR_INVALID, "the WCNS stencil needs ng >= 5 ghost layers");
-    int ndim = 0;
+    int nd = 0;
+    size_t cells = 1;
     for (int d = 0; d < 3; d++) {
         if (mesh->n[d] < 1) return set_error(EMG_ERR_INVALID, "mesh extents must be >= 1");
         if (mesh->n[d] > 1) {
-            ndim++;
+            nd++;
             if (!(mesh->dx[d] > 0.0)) return set_error(EMG_ERR_INVALID, "dx must be > 0 on active axes");
             if (mesh->n[d] > (1 << 30)) return set_error(EMG_ERR_INVALID, "axis too long");
+            cells *= (size_t)(mesh->n[d] + 2 * mesh->ng);
         }
     }
-    if (ndim == 0) return set_error(EMG_ERR_INVALID, "mesh has no active axis");
+    if (nd == 0) return set_error(EMG_ERR_INVALID, "mesh has no active axis");
     if (opts->mode != EMG_MODE_WENO && opts->mode != EMG_MODE_HYBRID && opts->mode != EMG_MODE_CENTRAL)
         return set_error(EMG_ERR_INVALID, "unknown flux mode");
     if (opts->mode == EMG_MODE_HYBRID && !(opts->tol > 0.0))
@@ -814,11 +815,20 @@ int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc
         const bool per0 = bc[2 * d].kind == EMG_BC_PERIODIC, per1 = bc[2 * d + 1].kind == EMG_BC_PERIODIC;
         if (mesh->n[d] > 1 && per0 != per1) return set_error(EMG_ERR_INVALID, "periodic boundaries must be paired");
     }
-    {
-        size_t padded = 1;
-        for (int d = 0; d < 3; d++) padded *= (size_t)(mesh->n[d] > 1 ? mesh->n[d] + 2 * mesh->ng : 1);
-        if (padded != len) return set_error(EMG_ERR_INVALID, "state length does not match the padded mesh");
-    }
+    *ndim = nd;
+    *padded = cells;
+    return EMG_OK;
+}
+
+int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
+                       const double* u_aos, size_t len, emg_uniform** out) {
+    if (!mesh || !eos || !bc || !opts || !u_aos || !out) return set_error(EMG_ERR_INVALID, "null argument");
+    *out = nullptr;
+    // arguments first, so that a bad call is reported as such on any host
+    int ndim = 0;
+    size_t padded = 0;
+    if (int rc = check_uniform_args(mesh, bc, opts, &ndim, &padded)) return rc;
+    if (padded != len) return set_error(EMG_ERR_INVALID, "state length does not match the padded mesh");
     int dev = 0;
     {
         int n = 0;
@@ -1138,47 +1148,40 @@ int emg_uniform_launch_count(emg_uniform* h, uint64_t* launches) {
 int emg_uniform_step_noalloc(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
                              const double* u_in, double* u_out, double dt, void* stream) {
     if (!mesh || !eos || !bc || !opts || !u_in || !u_out) return set_error(EMG_ERR_INVALID, "null argument");
-    if (u_in == u_out) return set_error(EMG_ERR_INVALID, "u_in and u_out must be distinct buffers");
-    if (mesh->ng < 5) return set_error(EMG_ERR_INVALID, "the WCNS stencil needs ng >= 5 ghost layers");
-    if (opts->mode != EMG_MODE_WENO && opts->mode != EMG_MODE_HYBRID && opts->mode != EMG_MODE_CENTRAL)
-        return set_error(EMG_ERR_INVALID, "unknown flux mode");
-    if (opts->precision != EMG_PRECISION_F64 && opts->precision != EMG_PRECISION_MIXED)
-        return set_error(EMG_ERR_INVALID, "unknown precision");
     int ndim = 0;
-    int64_t ncell = 1;
-    for (int d = 0; d < 3; d++) {
-        if (mesh->n[d] < 1) return set_error(EMG_ERR_INVALID, "mesh extents must be >= 1");
-        if (mesh->n[d] > 1) {
-            ndim++;
-            if (!(mesh->dx[d] > 0.0)) return set_error(EMG_ERR_INVALID, "dx must be > 0 on active axes");
-            ncell *= mesh->n[d] + 2 * mesh->ng;
-        }
-        if (ncell > EMG_NOALLOC_MAX_CELLS)
-            return set_error(EMG_ERR_INVALID, "grid exceeds EMG_NOALLOC_MAX_CELLS padded cells (131072)");
+    size_t padded = 0;
+    if (int rc = check_uniform_args(mesh, bc, opts, &ndim, &padded)) return rc;
+    if (padded > (size_t)EMG_NOALLOC_MAX_CELLS)
+        return set_error(EMG_ERR_INVALID, "grid exceeds EMG_NOALLOC_MAX_CELLS padded cells (131072)");
+    const int64_t ncell = (int64_t)padded;
+    {
+        // u_out is written while u_in is still read: no shared byte allowed
+        const uintptr_t a0 = (uintptr_t)u_in, b0 = (uintptr_t)u_out, nb = (uintptr_t)padded * 5 * sizeof(double);
+        if (a0 < b0 + nb && b0 < a0 + nb) return set_error(EMG_ERR_INVALID, "u_in and u_out must not overlap");
     }
-    if (ndim == 0) return set_error(EMG_ERR_INVALID, "mesh has no active axis");
-    for (int i = 0; i < 6; i++)
-        if (bc[i].kind < 0 || bc[i].kind > 4) return set_error(EMG_ERR_INVALID, "unknown boundary condition");
+    if (!(std::isfinite(dt) && dt > 0.0)) return set_error(EMG_ERR_INVALID, "dt must be finite and > 0");
     int dev = 0;
     EMG_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return set_error(EMG_ERR_INVALID, "device index out of range");
-    // once per device, with that device current: the scratch address and the
-    // sweep kernels' shared-memory attribute
-    static std::mutex scratch_mu;
-    static double* scratch_ptr[64] = {nullptr};
+    // The sweep kernels' shared-memory attribute is set once per device (the
+    // first call on a device; make it before any stream capture). The scratch
+    // address is looked up on every call, with this device current: a cached
+    // address would not survive a device reset or a new primary context.
+    static std::mutex prep_mu;
+    static bool prepared[64] = {false};
+    {
+        std::lock_guard<std::mutex> lock(prep_mu);
+        if (!prepared[dev]) {
+            cudaError_t e = sweep_prepare_device();
+            if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("sweep setup: ") + cudaGetErrorString(e));
+            prepared[dev] = true;
+        }
+    }
     double* base = nullptr;
     {
-        std::lock_guard<std::mutex> lock(scratch_mu);
-        if (!scratch_ptr[dev]) {
-            double* ptr = nullptr;
-            cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
-            if (e != cudaSuccess || !ptr)
-                return set_error(EMG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            e = sweep_prepare_device();
-            if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("sweep setup: ") + cudaGetErrorString(e));
-            scratch_ptr[dev] = ptr;
-        }
-        base = scratch_ptr[dev];
+        cudaError_t e = cudaGetSymbolAddress((void**)&base, g_noalloc_scratch);
+        if (e != cudaSuccess || !base)
+            return set_error(EMG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
     }
     emg_uniform h;
     h.device = dev;

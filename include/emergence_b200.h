@@ -219,9 +219,12 @@ int emg_uniform_launch_count(emg_uniform* h, uint64_t* launches);
  * (3·5·EMG_NOALLOC_MAX_CELLS doubles plus a control block, ≈15.7 MB, held by
  * every GPU that loads the library until the process exits). u_in is read
  * only; u_out receives the new state with the ghost layers of the stage-1 fill.
- * Grids above EMG_NOALLOC_MAX_CELLS padded cells return EMG_ERR_INVALID. The
- * first call on a device resolves the scratch address and sets kernel
- * attributes (make it before any stream capture). All calls share the one
+ * The argument checks of emg_uniform_create apply; in addition grids above
+ * EMG_NOALLOC_MAX_CELLS padded cells, u_in and u_out ranges that share any
+ * byte, and a dt that is not finite and > 0 return EMG_ERR_INVALID before any
+ * device work. The first call on a device sets kernel attributes (make it
+ * before any stream capture); the scratch address is looked up again on every
+ * call, so a device reset in between is harmless. All calls share the one
  * scratch area, so calls that overlap on the GPU (other streams, other host
  * threads) race; serialize them. Work is queued on `stream` (a cudaStream_t,
  * NULL for the legacy default stream) and the call does not synchronize. */

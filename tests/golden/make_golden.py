@@ -5,7 +5,8 @@ tables are read from its test sources as text:
   toro_star.json  <- fluid/crates/compressible/src/exact.rs, test
                      `toro_star_values` (Toro Tables 4.2/4.3, Tests 1-5, γ = 1.4,
                      with the test's tolerances).
-Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_golden.py REFERENCE_ROOT
+(REFERENCE_ROOT: the root of a checkout of the reference repository.)
 """
 import json
 import os
@@ -36,7 +37,9 @@ def toro_star(ref_root):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT")
+    ref = sys.argv[1]
     data = toro_star(ref)
     assert len(data["cases"]) == 5, data
     with open(os.path.join(HERE, "toro_star.json"), "w") as f:

@@ -110,16 +110,27 @@ def test_periodic_pairing_only_matters_on_active_axes():
 
 def test_noalloc_step_rejects_bad_arguments():
     m, bc, o = mesh(), bcs(OUT6), opts()
-    buf = (C.c_double * 16)()
-    p = C.cast(buf, C.c_void_p)
+    n = padded(m) * 5 * 8  # bytes of one state
+    buf = (C.c_char * (3 * n))()
+    p = C.cast(buf, C.c_void_p).value
     f = lib().emg_uniform_step_noalloc
-    assert f(C.byref(m), C.byref(EOS), bc, C.byref(o), None, p, 1e-3, None) == INVALID and "null" in err()
-    assert f(C.byref(m), C.byref(EOS), bc, C.byref(o), p, p, 1e-3, None) == INVALID and "distinct" in err()
-    big = mesh(n=(64, 64, 40))
-    assert f(C.byref(big), C.byref(EOS), bc, C.byref(o), p, C.c_void_p(p.value + 64), 1e-3, None) == INVALID
-    assert "EMG_NOALLOC_MAX_CELLS" in err()
-    assert f(C.byref(mesh(ng=3)), C.byref(EOS), bc, C.byref(o), p, C.c_void_p(p.value + 64), 1e-3, None) == INVALID
-    assert "ng >= 5" in err()
+
+    def call(m=m, bc=bc, o=o, a=p, b=p + n, dt=1e-3):
+        return f(C.byref(m), C.byref(EOS), bc, C.byref(o), C.c_void_p(a), C.c_void_p(b), dt, None)
+
+    assert call(a=None) == INVALID and "null" in err()
+    assert call(b=p) == INVALID and "overlap" in err()
+    # partial overlaps either way round
+    assert call(b=p + n - 8) == INVALID and "overlap" in err()
+    assert call(a=p + n - 8) == INVALID and "overlap" in err()
+    assert call(m=mesh(n=(64, 64, 40))) == INVALID and "EMG_NOALLOC_MAX_CELLS" in err()
+    assert call(m=mesh(ng=3)) == INVALID and "ng >= 5" in err()
+    # the checks emg_uniform_create makes apply here too
+    assert call(o=opts(mode=HYBRID, tol=0.0)) == INVALID and "tol > 0" in err()
+    assert call(bc=bcs([PERIODIC, OUTFLOW, OUTFLOW, OUTFLOW, OUTFLOW, OUTFLOW])) == INVALID
+    assert "paired" in err()
+    for dt in (0.0, -1e-3, float("nan"), float("inf")):
+        assert call(dt=dt) == INVALID and "dt" in err(), dt
 
 
 def batch_create(n, dx, bc=(OUTFLOW, OUTFLOW), o=None):
