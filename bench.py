@@ -30,6 +30,8 @@ sys.path.insert(0, ROOT)
 from emergence_b200 import replicas  # noqa: E402  (one process per GPU: barrier, max over ranks)
 
 N_CELLS = 256
+CPU_STEPS = 5  # timed steps of the CPU baseline on the full grid (about 5 s each on 16 host threads)
+AMR_STEPS = 20
 CELL_BYTES_3D = 320  # algorithmic bytes per 3-D cell-update (64·F, F = 5)
 
 
@@ -46,10 +48,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg of the uniform workload")
+    ap.add_argument("--no-subrecords", action="store_true",
+                    help="uniform workload: skip the AMR, batched-lines and adjoint records added to the line at N=1")
     ap.add_argument("--no-autotune", action="store_true", help="uniform and AMR workloads: use the planned sweep shapes")
-    ap.add_argument("--reference-gpu", action="store_true",
-                    help="uniform workload: also time the reference's own GPU kernels on the same grid "
-                         "(oracle/_ref/librefgpu.so, built from the reference tree by `make -C oracle refgpu`)")
+    ap.add_argument("--no-reference-gpu", dest="reference_gpu", action="store_false",
+                    help="uniform workload: skip the same-box GPU baseline, the reference's own GPU kernels timed on "
+                         "the same grid (oracle/_ref/librefgpu.so, built from the reference tree by "
+                         "`make -C oracle refgpu`; reported as unavailable where it is not built)")
     ap.add_argument("--workload", default="uniform", choices=["uniform", "amr", "batch", "adjoint", "batch_adjoint"],
                     help="uniform: 3-D explosion 256^3; amr: 3-D shock-bubble on block AMR (base 128^3, 3 levels); "
                          "batch: 4096 independent 1-D Riemann problems; adjoint: discrete adjoint of the 2-D "
@@ -144,21 +149,30 @@ def cpu_reference_steps(n, steps, warmup):
     return mesh.cells() * steps / el, el / max(steps, 1), O.num_threads(), f"{O.state_hash(mesh, o.download()):016x}"
 
 
+def uniform_config(n, world, precision):
+    """The `config` of the uniform workload's line (both arms)."""
+    return {"workload": f"3-D spherical explosion {n}^3 (r<0.3: rho=1,p=1; else 0.125,0.1; +-1% rho noise),"
+                        " WCNS WENO5-Z + HLLC + positivity, SSP-RK3, CFL 0.5, outflow",
+            "cells": n ** 3, "precision": precision,
+            "parallelism": f"{world} independent replica(s), one GPU each",
+            "l2": f"inputs larger than L2 (state {(n + 12) ** 3 * 40 / 1e9:.2f} GB per array)"}
+
+
 def run_reference(args, world, rank):
     """--impl reference: the reference CPU solver on host cores (rank 0 only)."""
     if rank != 0:
         return
-    # bounded sample of the workload: a 96^3 instance of the same explosion
-    n = 96
+    # the full workload: the same 256^3 explosion, warmup + steps steps
+    n = args.n
     value, sps, threads, fnv = cpu_reference_steps(n, args.steps, args.warmup)
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"3-D spherical explosion {args.n}^3, WCNS WENO5-Z + HLLC + positivity, SSP-RK3, CFL 0.5",
-                   "sample": f"{n}^3 instance of the same explosion per step"},
+        "config": dict(uniform_config(n, world, "f64"), sample=f"the full {n}^3 grid, every step"),
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-                         "sample": f"SSP-RK3 steps of a {n}^3 instance, C++ restatement of the reference CPU f64 solver",
+                         "sample": f"{args.steps} timed SSP-RK3 steps (after {args.warmup}) of the full {n}^3 explosion, "
+                                   "C++ restatement of the reference CPU f64 solver (OpenMP over pencils)",
                          "state_fnv": fnv},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -281,12 +295,16 @@ def run_ours(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        nb = 64
-        v, sps, threads, fnv = cpu_reference_steps(nb, 2, 1)
+        # the same grid and initial state, the first CPU_STEPS steps (after one untimed step)
+        v, sps, threads, fnv = cpu_reference_steps(n, CPU_STEPS, 1)
         cpu = {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-               "sample": f"2 SSP-RK3 steps of a {nb}^3 instance of the same explosion, "
+               "sample": f"{CPU_STEPS} timed SSP-RK3 steps (after 1 untimed) of the same {n}^3 explosion, "
                          "C++ restatement of the reference CPU f64 solver (OpenMP over pencils)",
-               "state_fnv": fnv}
+               "seconds_per_step": sps, "state_fnv": fnv}
+
+    subs = {}
+    if rank == 0 and world == 1 and not args.no_subrecords:
+        subs = sub_records(args, world, rank, local)
 
     if rank == 0:
         line = {
@@ -294,11 +312,7 @@ def run_ours(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if prec == Precision.F64 else "f32-flux/f64-state", "data": "synthetic",
-            "config": {"workload": f"3-D spherical explosion {n}^3 (r<0.3: rho=1,p=1; else 0.125,0.1; +-1% rho noise),"
-                                   " WCNS WENO5-Z + HLLC + positivity, SSP-RK3, CFL 0.5, outflow",
-                       "cells": cells, "precision": args.precision,
-                       "parallelism": f"{world} independent replica(s), one GPU each",
-                       "l2": "inputs larger than L2 (state 0.77 GB per array)"},
+            "config": uniform_config(n, world, args.precision),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "traffic_source": "ncu capture on 160^3 scaled by cells (profiles/)", "kernel": "fused sweep (3 per stage)",
                          "alg_bytes_per_launch": alg_bytes_per_launch, "avg_launch_ms": per_launch_ms,
@@ -316,62 +330,100 @@ def run_ours(args, world, rank, local):
         }
         if ref_gpu is not None:
             line["reference_gpu"] = ref_gpu
+        line.update(subs)
         print(json.dumps(line), flush=True)
 
 
+def _compact(line, keys):
+    return {k: line[k] for k in keys if k in line}
+
+
+def sub_records(args, world, rank, local):
+    """The other workloads, each measured in both forms on the same box in
+    the same run (one GPU): block AMR (20 steps of the shock-bubble), the
+    4096 batched Riemann problems (one whole run), the 2-D adjoint (one
+    gradient with its finite-difference check) and the batched gradients."""
+    import numpy as np
+    out = {}
+    amr = {}
+    for prec in ("f64", "mixed"):
+        ln = measure_amr(args, world, rank, local, precision=prec, steps=AMR_STEPS, warmup=3, cpu_baseline=False,
+                         keep_state=True)
+        amr[prec] = ln
+    a64, amx = amr["f64"], amr["mixed"]
+    rec = {"workload": "3-D shock-bubble block AMR, base 128^3, 3 levels (eff. 512^3), 16^3 blocks, ng=5, CFL 0.4, "
+                       f"regrid every 4 steps; {AMR_STEPS} timed steps after 3, each form with its own CFL dt",
+           "unit": "leaf cell-updates/s"}
+    for prec in ("f64", "mixed"):
+        rec[prec] = _compact(amr[prec], ("value", "ms_per_step", "effective_cell_updates_per_s", "phase_ms_per_step",
+                                         "gpu_launches", "clocks"))
+        rec[prec]["leaves"] = amr[prec]["config"]["leaves"]
+        rec[prec]["build_s"] = amr[prec]["config"]["build_s"]
+    rec["mixed_over_f64"] = a64["ms_per_step"] / amx["ms_per_step"]
+    (s64, u64), (smx, umx) = a64.pop("_state"), amx.pop("_state")
+    if s64.shape == smx.shape and np.array_equal(s64, smx):
+        leaves = s64[:, 4] == 1
+        ia, ib = umx[leaves].reshape(-1, 5), u64[leaves].reshape(-1, 5)
+        num, den = np.abs(ia - ib).sum(axis=0), np.abs(ib).sum(axis=0)
+        rec["rel_l1_mixed_vs_f64"] = [float(x) for x in num / np.maximum(den, 1e-3 * den[0])]
+        rec["linf_mixed_vs_f64"] = [float(x) for x in np.abs(ia - ib).max(axis=0)]
+    else:
+        rec["rel_l1_mixed_vs_f64"] = "hierarchies differ after the regrids (mixed-form details moved a decision)"
+    out["amr"] = rec
+
+    bat = {}
+    for prec in ("f64", "mixed"):
+        bat[prec] = measure_batch(args, world, rank, local, precision=prec, steps=1, warmup=1, cpu_baseline=False)
+    out["batch"] = {"workload": bat["f64"]["config"]["workload"], "unit": "cell-updates/s",
+                    "f64": _compact(bat["f64"], ("value", "ms_per_step", "clocks")),
+                    "mixed": _compact(bat["mixed"], ("value", "ms_per_step", "clocks")),
+                    "mixed_over_f64": bat["f64"]["ms_per_step"] / bat["mixed"]["ms_per_step"]}
+
+    adj = measure_adjoint(args, world, rank, local, steps=1, warmup=1)
+    out["adjoint"] = _compact(adj, ("value", "unit", "forward_ms", "recompute_ms", "reverse_ms",
+                                    "forward_cell_updates_per_s", "fd_check", "clocks"))
+    out["adjoint"]["workload"] = adj["config"]["workload"]
+    badj = measure_batch_adjoint(args, world, rank, local, steps=1, warmup=1, dual_check=False)
+    out["batch_adjoint"] = _compact(badj, ("value", "unit", "forward_ms", "recompute_ms", "reverse_ms", "clocks"))
+    out["batch_adjoint"]["workload"] = badj["config"]["workload"]
+    return out
+
+
 def reference_gpu_leg(args, sys_, mesh, u, bc, cells, ours_ms_per_step, u_ours):
-    """The reference's uniform-solver kernels (fluid/crates/compressible-cuda/
-    src/kernels.cu, compiled unmodified for sm_100a) driven in the order of its
-    GpuSolver<f64> (oracle/ref_gpu.cu) over warmup + steps steps of the same
-    explosion, each step's dt from its own rate kernel and host max as in its
-    run_to loop. Timed with CUDA events on its stream; the per-step device→host
-    copy of the rates is part of that design and inside the timed region."""
-    import ctypes as C
+    """Same-box GPU baseline: the reference's uniform-solver kernels
+    (fluid/crates/compressible-cuda/src/kernels.cu, compiled unmodified for
+    sm_100a) driven in the order of its GpuSolver<f64> (oracle/ref_gpu.cu, bound
+    by oracle/pyrefgpu.py) over warmup + steps steps of the same explosion, each
+    step's dt from its own rate kernel and host max as in its run_to loop. Timed
+    with CUDA events on its stream; the per-step device→host copy of the rates
+    is part of that design and inside the timed region."""
     import numpy as np
     import torch
-    from emergence_b200._abi import EmgOpts
     from emergence_b200.physics import FluxMode
-    from emergence_b200.solver import _c_bcs, _c_eos, _c_mesh
+    from oracle import pyrefgpu
 
-    path = os.path.join(ROOT, "oracle", "_ref", "librefgpu.so")
-    if not os.path.exists(path):
+    if not pyrefgpu.available():
         return {"unavailable": "oracle/_ref/librefgpu.so is not built (make -C oracle refgpu needs the reference tree)"}
-    L = C.CDLL(path)
-    L.refgpu_last_error.restype = C.c_char_p
-    L.refgpu_stream.restype = C.c_void_p
-    L.refgpu_stream.argtypes = [C.c_void_p]
-    for name in ("refgpu_advance", "refgpu_download", "refgpu_synchronize", "refgpu_destroy"):
-        getattr(L, name).restype = C.c_int
-    L.refgpu_advance.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]
-    L.refgpu_download.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_size_t]
-    L.refgpu_synchronize.argtypes = [C.c_void_p]
-    L.refgpu_destroy.argtypes = [C.c_void_p]
-    m, e, b = _c_mesh(mesh), _c_eos(sys_.eos), _c_bcs(bc)
-    o = EmgOpts(0.5, 1e-3, FluxMode.Weno, 1, 0, 0)
-    ua = np.ascontiguousarray(u, dtype=np.float64)
-    h = C.c_void_p()
-    if L.refgpu_create(C.byref(m), C.byref(e), b, C.byref(o), ua.ctypes.data_as(C.POINTER(C.c_double)),
-                       C.c_size_t(mesh.len()), C.byref(h)):
-        return {"error": L.refgpu_last_error().decode()}
-    taken = C.c_uint64()
     try:
-        if L.refgpu_advance(h, args.warmup, C.byref(taken)) or L.refgpu_synchronize(h):
-            return {"error": L.refgpu_last_error().decode()}
-        s = torch.cuda.ExternalStream(L.refgpu_stream(h))
+        r = pyrefgpu.RefGpuSolver(sys_, mesh, u, bc=bc, cfl=0.5, mode=FluxMode.Weno)
+    except RuntimeError as ex:
+        return {"error": str(ex)}
+    try:
+        r.advance(args.warmup)
+        r.synchronize()
+        s = torch.cuda.ExternalStream(r.stream())
         a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         a.record(s)
-        rc = L.refgpu_advance(h, args.steps, C.byref(taken))
+        r.advance(args.steps)
         z.record(s)
         z.synchronize()
-        if rc:
-            return {"error": L.refgpu_last_error().decode()}
         rms = a.elapsed_time(z)
-        out = np.empty_like(ua)
-        if L.refgpu_download(h, out.ctypes.data_as(C.POINTER(C.c_double)), C.c_size_t(mesh.len())):
-            return {"error": L.refgpu_last_error().decode()}
+        out = r.download()
+    except RuntimeError as ex:
+        return {"error": str(ex)}
     finally:
-        L.refgpu_destroy(h)
+        r.close()
     res = {"value": cells * args.steps / (rms * 1e-3), "unit": "cell-updates/s", "ms_per_step": rms / args.steps,
            "ours_speedup": (rms / args.steps) / ours_ms_per_step,
            "what": "the reference's compressible-cuda kernels (unmodified source, nvcc sm_100a) in GpuSolver<f64> "
@@ -384,10 +436,19 @@ def reference_gpu_leg(args, sys_, mesh, u, bc, cells, ours_ms_per_step, u_ours):
 
 
 def run_amr(args, world, rank, local):
+    line = measure_amr(args, world, rank, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def measure_amr(args, world, rank, local, precision=None, steps=None, warmup=None, cpu_baseline=True, keep_state=False):
     """3-D shock-bubble on block AMR: Mach-2 shock into a light sphere,
     16^3-cell blocks, base 8^3 blocks (128^3 cells), 3 levels (effective
     512^3), ng = 5, regrid every 4 steps, CFL 0.4. One step = one global
-    SSP-RK3 step over all leaves (regrids included when due)."""
+    SSP-RK3 step over all leaves (regrids included when due), dt from the
+    CFL reduction over the leaves each step. Returns the JSON line (on every
+    rank; rank 0 prints it); with keep_state, also the final hierarchy and
+    leaf data under "_state"."""
     import numpy as np
     import torch
     from emergence_b200 import GpuAmr, workloads as W
@@ -395,12 +456,15 @@ def run_amr(args, world, rank, local):
 
     torch.cuda.set_device(local)
     dev = torch.cuda.current_device()
-    prec = Precision.Mixed if args.precision == "mixed" else Precision.F64
+    precision = args.precision if precision is None else precision
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    prec = Precision.Mixed if precision == "mixed" else Precision.F64
     s, cfg, lo, hi, bc, init = W.shock_bubble(dim=3, base=args.amr_base, levels=3)
     t0 = time.perf_counter()
     g = GpuAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno, cfl=0.4, precision=prec, autotune=not args.no_autotune)
     build_s = time.perf_counter() - t0
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         g.step(g.dt_cfl())
     g.synchronize()
     g.phase_times()
@@ -412,7 +476,7 @@ def run_amr(args, world, rank, local):
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev) as clk:
         a.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             leaf_cells += g.block_count()[1] * g.bcells
             g.step(g.dt_cfl())
         b.record(stream)
@@ -429,9 +493,10 @@ def run_amr(args, world, rank, local):
     nb, nl = g.block_count()
     st = g.structure()
     per_level = [int(((st[:, 0] == l) & (st[:, 4] == 1)).sum()) for l in range(cfg["levels"])]
+    state = (st, g.download()) if keep_state else None
     g.close()
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and cpu_baseline and not args.no_cpu_baseline:
         from oracle import pyoracle as O
         sc, cfgc, loc, hic, bcc, initc = W.shock_bubble(dim=3, base=2, levels=3)
         o = O.OracleAmr(sc, cfgc, loc, hic, bcc, initc, mode=FluxMode.Weno, cfl=0.4)
@@ -442,31 +507,38 @@ def run_amr(args, world, rank, local):
         cpu = {"value": cells_c / el, "unit": "cell-updates/s", "cores": O.num_threads(), "kind": "port",
                "sample": f"1 step of the shock-bubble with base 2^3 blocks (32^3), 3 levels, {o.block_count()[1]} leaves; "
                          "C++ restatement of the reference CPU AMR solver"}
-    if rank == 0:
-        line = {
-            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == Precision.F64 else "f32-flux/f64-state",
-            "data": "synthetic",
-            "config": {"workload": "3-D shock-bubble block AMR: Mach-2 shock into rho=0.138 sphere r=0.15 (+-0.5% "
-                                   "seeded interface perturbation), base 128^3 = 8^3 blocks of 16^3, 3 levels (eff. 512^3), "
-                                   "ng=5, WCNS WENO5-Z + HLLC + positivity, CFL 0.4, regrid every 4 steps",
-                       "blocks": nb, "leaves": nl, "leaves_per_level": per_level, "build_s": build_s,
-                       "autotune": not args.no_autotune,
-                       "precision": args.precision},
-            "phase_ms_per_step": {k: v / args.steps for k, v in phases.items()},
-            # the same steps counted at the finest level's resolution over the whole
-            # domain (what a uniform grid of the finest spacing would update per step)
-            "effective_cell_updates_per_s": eff_cells * args.steps * world / (ms * 1e-3),
-            "effective_cells": eff_cells,
-            "gpu_launches": launches,
-            "clocks": clk.summary(),
-            "cpu_baseline": cpu,
-        }
-        print(json.dumps(line), flush=True)
+    line = {
+        "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": steps, "warmup": warmup, "ms_per_step": ms / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == Precision.F64 else "f32-flux/f64-state",
+        "data": "synthetic",
+        "config": {"workload": "3-D shock-bubble block AMR: Mach-2 shock into rho=0.138 sphere r=0.15 (+-0.5% "
+                               "seeded interface perturbation), base 128^3 = 8^3 blocks of 16^3, 3 levels (eff. 512^3), "
+                               "ng=5, WCNS WENO5-Z + HLLC + positivity, CFL 0.4, regrid every 4 steps",
+                   "blocks": nb, "leaves": nl, "leaves_per_level": per_level, "build_s": build_s,
+                   "autotune": not args.no_autotune,
+                   "precision": precision},
+        "phase_ms_per_step": {k: v / steps for k, v in phases.items()},
+        # the same steps counted at the finest level's resolution over the whole
+        # domain (what a uniform grid of the finest spacing would update per step)
+        "effective_cell_updates_per_s": eff_cells * steps * world / (ms * 1e-3),
+        "effective_cells": eff_cells,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    if state is not None:
+        line["_state"] = state
+    return line
 
 
 def run_batch(args, world, rank, local):
+    line = measure_batch(args, world, rank, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def measure_batch(args, world, rank, local, precision=None, steps=None, warmup=None, cpu_baseline=True):
     """4096 independent 1-D Riemann problems (cells log-uniform in [64, 2048],
     ρ, p ∈ U[0.1, 2], u ∈ U[−1, 1] on each side, interface at 0.5, outflow),
     each run to t = 0.15 with its own CFL steps, all instances in one launch
@@ -479,16 +551,19 @@ def run_batch(args, world, rank, local):
 
     torch.cuda.set_device(local)
     dev = torch.cuda.current_device()
-    prec = Precision.F64 if args.precision == "f64" else Precision.Mixed
+    precision = args.precision if precision is None else precision
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    prec = Precision.F64 if precision == "f64" else Precision.Mixed
     sys_, n, dx, u, st = W.riemann_batch()
-    for _ in range(max(args.warmup, 1)):
+    for _ in range(max(warmup, 1)):
         g = GpuBatch1D(sys_, n, dx, u, precision=prec)
         g.run_to(0.15)
         g.close()
     total_ms, updates = 0.0, 0
     replicas.barrier(world)
     with ClockSampler(dev) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             g = GpuBatch1D(sys_, n, dx, u, precision=prec)
             stream = torch.cuda.ExternalStream(g.stream())
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -498,13 +573,13 @@ def run_batch(args, world, rank, local):
             b.record(stream)
             b.synchronize()
             total_ms += a.elapsed_time(b)
-            t, steps = g.status()
-            updates += int((n * steps.astype(np.int64)).sum())
+            _, inst_steps = g.status()
+            updates += int((n * inst_steps.astype(np.int64)).sum())
             g.close()
     total_ms = replicas.max_over_ranks(total_ms, world)
     value = updates * world / (total_ms * 1e-3)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and cpu_baseline and not args.no_cpu_baseline:
         from oracle import pyoracle as O
         from emergence_b200.physics import Bc, Mesh
         sub = slice(0, 256, 8)  # 32 instances of the same batch
@@ -521,23 +596,28 @@ def run_batch(args, world, rank, local):
         cpu = {"value": cu / el, "unit": "cell-updates/s", "cores": O.num_threads(), "kind": "port",
                "sample": "32 of the 4096 instances (every 8th of the first 256), each run to t = 0.15; "
                          "C++ restatement of the reference CPU solver"}
-    if rank == 0:
-        line = {
-            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == Precision.F64 else "f32-flux/f64-state",
-            "data": "synthetic",
-            "config": {"workload": "4096 independent 1-D Riemann problems, cells log-uniform [64, 2048] (sum %d), "
-                                   "rho,p~U[0.1,2], u~U[-1,1], t_end 0.15, outflow, per-instance CFL 0.5" % int(n.sum()),
-                       "step": "one whole batched run to t_end", "batch_steps": int(launched),
-                       "precision": args.precision},
-            "clocks": clk.summary(),
-            "cpu_baseline": cpu,
-        }
-        print(json.dumps(line), flush=True)
+    line = {
+        "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": steps, "warmup": warmup, "ms_per_step": total_ms / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == Precision.F64 else "f32-flux/f64-state",
+        "data": "synthetic",
+        "config": {"workload": "4096 independent 1-D Riemann problems, cells log-uniform [64, 2048] (sum %d), "
+                               "rho,p~U[0.1,2], u~U[-1,1], t_end 0.15, outflow, per-instance CFL 0.5" % int(n.sum()),
+                   "step": "one whole batched run to t_end", "batch_steps": int(launched),
+                   "precision": precision},
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    return line
 
 
 def run_adjoint(args, world, rank, local):
+    line = measure_adjoint(args, world, rank, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def measure_adjoint(args, world, rank, local, steps=None, warmup=None):
     """Discrete adjoint of the 2-D explosion (radius 0.4, ±1 % density noise,
     outflow) on 512^2 cells over 400 CFL steps, FP64 forward and adjoint:
     J = ∫ p dA over [0.7, 0.9]^2 at the end, gradient with respect to the
@@ -553,18 +633,20 @@ def run_adjoint(args, world, rank, local):
 
     torch.cuda.set_device(local)
     dev = torch.cuda.current_device()
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     n, N = args.adj_n, args.adj_steps
     sys_, mesh, w, bc = W.explosion_prim((n, n, 1), 0.4)
     u0 = initial_state(sys_, mesh, w)
     box = ([0.7, 0.7, 0.0], [0.9, 0.9, 0.0])
     g = DifferentiableSolver(sys_, mesh, u0, bc=bc)
-    for _ in range(max(args.warmup, 1)):
+    for _ in range(max(warmup, 1)):
         g.forward(N)
         g.objective(OBJ_PRESSURE, *box)
         g.backward()
     fwd_ms, rec_ms, rev_ms, wall = [], [], [], []
     with ClockSampler(dev) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             t0 = time.perf_counter()
             g.forward(N)
             J = g.objective(OBJ_PRESSURE, *box)
@@ -599,29 +681,34 @@ def run_adjoint(args, world, rank, local):
     # the slowest replica's phases (a ratio of device times; every rank takes the same steps)
     f, r, v = (replicas.max_over_ranks(x, world) for x in (f, r, v))
     cells = mesh.cells()
-    if rank == 0:
-        line = {
-            "metric": "adjoint/forward cost", "value": (r + v) / f, "unit": "ratio", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": f + r + v, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"2-D explosion {n}^2 (r<0.4: rho=1,p=1; else 0.125,0.1; +-1% rho noise), "
-                                   f"{N} CFL steps, WCNS WENO5-Z + HLLC + positivity, SSP-RK3, CFL 0.5, outflow",
-                       "objective": "J = sum p dA over [0.7,0.9]^2 at t_end", "checkpoints": "every ceil(sqrt(N)) steps",
-                       "step": "one recorded forward run + one backward pass"},
-            "forward_ms": f, "recompute_ms": r, "reverse_ms": v,
-            "reverse_over_forward": v / f, "backward_over_forward": (r + v) / f,
-            "forward_cell_updates_per_s": cells * N / (f * 1e-3),
-            "wall_s_per_gradient": float(np.median(wall)),
-            "J": J, "t_end": float(dts.sum()), "gamma_bar": [float(gam[0]), float(gam[1])],
-            "fd_check": {"h": h, "direction": "seeded uniform(-1,1) on rho0 interior, 0.5 on gamma",
-                         "fd": fd, "adjoint": adj, "rel_err": abs(fd - adj) / abs(adj),
-                         "h_1e-7": {"fd": fd7, "rel_err": abs(fd7 - adj) / abs(adj)}},
-            "clocks": clk.summary(),
-        }
-        print(json.dumps(line), flush=True)
+    line = {
+        "metric": "adjoint/forward cost", "value": (r + v) / f, "unit": "ratio", "n_gpus": world,
+        "steps": steps, "warmup": warmup, "ms_per_step": f + r + v, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"2-D explosion {n}^2 (r<0.4: rho=1,p=1; else 0.125,0.1; +-1% rho noise), "
+                               f"{N} CFL steps, WCNS WENO5-Z + HLLC + positivity, SSP-RK3, CFL 0.5, outflow",
+                   "objective": "J = sum p dA over [0.7,0.9]^2 at t_end", "checkpoints": "every ceil(sqrt(N)) steps",
+                   "step": "one recorded forward run + one backward pass"},
+        "forward_ms": f, "recompute_ms": r, "reverse_ms": v,
+        "reverse_over_forward": v / f, "backward_over_forward": (r + v) / f,
+        "forward_cell_updates_per_s": cells * N / (f * 1e-3),
+        "wall_s_per_gradient": float(np.median(wall)),
+        "J": J, "t_end": float(dts.sum()), "gamma_bar": [float(gam[0]), float(gam[1])],
+        "fd_check": {"h": h, "direction": "seeded uniform(-1,1) on rho0 interior, 0.5 on gamma",
+                     "fd": fd, "adjoint": adj, "rel_err": abs(fd - adj) / abs(adj),
+                     "h_1e-7": {"fd": fd7, "rel_err": abs(fd7 - adj) / abs(adj)}},
+        "clocks": clk.summary(),
+    }
+    return line
 
 
 def run_batch_adjoint(args, world, rank, local):
+    line = measure_batch_adjoint(args, world, rank, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def measure_batch_adjoint(args, world, rank, local, steps=None, warmup=None, dual_check=True):
     """Gradients of the 4096 independent 1-D Riemann problems: J_i = total
     energy in the right half [0.5, 1] at t = 0.15, differentiated with respect
     to the six initial values (ρ, u, p left and right of x = 0.5) of every
@@ -637,15 +724,17 @@ def run_batch_adjoint(args, world, rank, local):
 
     torch.cuda.set_device(local)
     dev = torch.cuda.current_device()
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     sys_, n, dx, u, st = W.riemann_batch()
     g = GpuBatch1D(sys_, n, dx, u)
-    for _ in range(max(args.warmup, 1)):
+    for _ in range(max(warmup, 1)):
         g.record(0.15)
         g.objective(OBJ_ENERGY, 0.5, 1.0)
         g.backward(0.5)
     fwd, rec, rev = [], [], []
     with ClockSampler(dev) as clk:
-        for _ in range(args.steps):
+        for _ in range(steps):
             B = g.record(0.15)
             J = g.objective(OBJ_ENERGY, 0.5, 1.0)
             grad = g.backward(0.5)
@@ -653,13 +742,13 @@ def run_batch_adjoint(args, world, rank, local):
             fwd.append(ms[0])
             rec.append(ms[1])
             rev.append(ms[2])
-    _, steps = g.status()
+    _, inst_steps = g.status()
     g.close()
     f, r, v = float(np.median(fwd)), float(np.median(rec)), float(np.median(rev))
     f, r, v = (replicas.max_over_ranks(x, world) for x in (f, r, v))
-    updates = int((n * steps.astype(np.int64)).sum())
+    updates = int((n * inst_steps.astype(np.int64)).sum())
     check = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and dual_check and not args.no_cpu_baseline:
         from oracle import pyoracle as O
         bc = [[Bc.Outflow, Bc.Outflow], [Bc.Periodic, Bc.Periodic], [Bc.Periodic, Bc.Periodic]]
         offs = np.concatenate([[0], np.cumsum(n)])
@@ -690,23 +779,22 @@ def run_batch_adjoint(args, world, rank, local):
                 worst = max(worst, abs(grad[i, q] - dJ) / max(abs(dJ), 1e-12))
         check = {"instances": sample, "max_rel_err_vs_dual": worst,
                  "what": "CPU f64 forward-mode dual-number runs of the oracle, 6 directions per instance, same time steps"}
-    if rank == 0:
-        line = {
-            "metric": "adjoint/forward cost", "value": (r + v) / f, "unit": "ratio", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": f + r + v, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "4096 independent 1-D Riemann problems, cells log-uniform [64, 2048] (sum %d), "
-                                   "rho,p~U[0.1,2], u~U[-1,1], t_end 0.15, outflow; J_i = sum E dx over [0.5, 1]; "
-                                   "gradient w.r.t. the six initial values" % int(n.sum()),
-                       "batch_steps": int(B), "checkpoints": "every 64 batch steps",
-                       "step": "one recorded FP64 run + one backward pass"},
-            "forward_ms": f, "recompute_ms": r, "reverse_ms": v, "reverse_over_forward": v / f,
-            "forward_cell_updates_per_s": updates / (f * 1e-3),
-            "gradient_sample": {"instance0": [float(x) for x in grad[0]], "J0": float(J[0])},
-            "dual_check": check,
-            "clocks": clk.summary(),
-        }
-        print(json.dumps(line), flush=True)
+    line = {
+        "metric": "adjoint/forward cost", "value": (r + v) / f, "unit": "ratio", "n_gpus": world,
+        "steps": steps, "warmup": warmup, "ms_per_step": f + r + v, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "4096 independent 1-D Riemann problems, cells log-uniform [64, 2048] (sum %d), "
+                               "rho,p~U[0.1,2], u~U[-1,1], t_end 0.15, outflow; J_i = sum E dx over [0.5, 1]; "
+                               "gradient w.r.t. the six initial values" % int(n.sum()),
+                   "batch_steps": int(B), "checkpoints": "every 64 batch steps",
+                   "step": "one recorded FP64 run + one backward pass"},
+        "forward_ms": f, "recompute_ms": r, "reverse_ms": v, "reverse_over_forward": v / f,
+        "forward_cell_updates_per_s": updates / (f * 1e-3),
+        "gradient_sample": {"instance0": [float(x) for x in grad[0]], "J0": float(J[0])},
+        "dual_check": check,
+        "clocks": clk.summary(),
+    }
+    return line
 
 
 def main():

@@ -33,15 +33,21 @@ def test_driver_flags_override_the_defaults(monkeypatch):
     assert _parse([], monkeypatch).warmup >= 3  # at least 3 untimed warm-up steps
 
 
-def test_reference_gpu_leg_is_off_by_default(monkeypatch):
-    assert _parse([], monkeypatch).reference_gpu is False
-    assert _parse(["--reference-gpu"], monkeypatch).reference_gpu is True
+def test_reference_gpu_leg_is_on_by_default(monkeypatch):
+    assert _parse([], monkeypatch).reference_gpu is True
+    assert _parse(["--no-reference-gpu"], monkeypatch).reference_gpu is False
+
+
+def test_subrecords_are_on_by_default(monkeypatch):
+    assert _parse([], monkeypatch).no_subrecords is False
+    assert _parse(["--no-subrecords"], monkeypatch).no_subrecords is True
 
 
 def test_reference_gpu_leg_reports_a_missing_library(monkeypatch, tmp_path):
     """Without oracle/_ref/librefgpu.so the leg says so instead of failing
     (it returns before any device call)."""
     bench = _bench()
-    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    from oracle import pyrefgpu
+    monkeypatch.setattr(pyrefgpu, "LIB_PATH", str(tmp_path / "librefgpu.so"))
     out = bench.reference_gpu_leg(None, None, None, None, None, 0, 1.0, None)
     assert "unavailable" in out and "librefgpu.so" in out["unavailable"]
