@@ -9,6 +9,7 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libemergence_b200.so")
+LIB_PATH_BC = os.path.join(HERE, "libemergence_b200_bc.so")
 
 EMG_OK = 0
 STATUS_NAMES = {
@@ -131,15 +132,22 @@ SIGNATURES = {
 _lib = None
 
 
+def lib_path():
+    """The product library, or its bounds-check build when the environment
+    sets EMG_BOUNDS_CHECK=1 (index checks that report EMG_ERR_BOUNDS)."""
+    return LIB_PATH_BC if os.environ.get("EMG_BOUNDS_CHECK") == "1" else LIB_PATH
+
+
 def lib():
     """Load the in-tree CUDA library (raises if it has not been built)."""
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
+        path = lib_path()
+        if not os.path.exists(path):
             raise RuntimeError(
-                "libemergence_b200.so is missing: build it with `python -m emergence_b200.build` "
+                f"{os.path.basename(path)} is missing: build it with `python -m emergence_b200.build` "
                 "(there is no CPU fallback)")
-        L = C.CDLL(LIB_PATH)
+        L = C.CDLL(path)
         for name, (res, args) in SIGNATURES.items():
             f = getattr(L, name)
             f.restype = res

@@ -19,6 +19,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libemergence_b200.so")
+OUT_BC = os.path.join(HERE, "libemergence_b200_bc.so")
 BUILD = os.path.join(HERE, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -48,26 +49,40 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose=False, force=False):
-    os.makedirs(BUILD, exist_ok=True)
+def _build_one(out, objdir, extra, verbose, force):
+    os.makedirs(objdir, exist_ok=True)
     nvcc = _nvcc()
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     headers.append(os.path.join(HERE, "..", "include", "emergence_b200.h"))
-    objs = []
+    objs, jobs = [], []
     for src, flags in UNITS:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(objdir, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _stale(o, [s] + headers + [__file__]):
-            cmd = [nvcc] + ARCH + COMMON + flags + ["-c", s, "-o", o]
+            cmd = [nvcc] + ARCH + COMMON + flags + extra + ["-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
-    if force or _stale(OUT, objs):
-        cmd = [nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", OUT] + objs
+            jobs.append(subprocess.Popen(cmd))
+    if any(j.wait() != 0 for j in jobs):
+        raise subprocess.CalledProcessError(1, "nvcc")
+    if force or _stale(out, objs):
+        cmd = [nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", out] + objs
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
+    return out
+
+
+def build(verbose=False, force=False, bounds_check=True):
+    """The product library and, unless bounds_check is False, the
+    bounds-check variant libemergence_b200_bc.so (-DEMG_BOUNDS_CHECK: every
+    global index of the sweeps, the ghost fill and the AMR pool accesses is
+    checked and an out-of-range index is reported as EMG_ERR_BOUNDS; loaded
+    instead of the product library when EMG_BOUNDS_CHECK=1 is set)."""
+    _build_one(OUT, BUILD, [], verbose, force)
+    if bounds_check:
+        _build_one(OUT_BC, os.path.join(BUILD, "bc"), ["-DEMG_BOUNDS_CHECK"], verbose, force)
     return OUT
 
 

@@ -877,6 +877,7 @@ struct emg_amr {
             for (int l = 0; l < levels && l < 16; l++) p.dx_level[l] = dxl[3 * l + d];
             p.dx = dxl[d];
             p.face = face;
+            p.nface = cap * 3 * 2 * 5 * (int64_t)npen;
             p.npen = npen;
             p.pen_lane_major = lane < other ? 1 : 0;
             const dim3 grid((unsigned)(nleaves * p.ngroups), 1, 1);
@@ -1391,6 +1392,7 @@ struct emg_amr {
         if (rc) return rc;
         ctl_host->dt = dt;
         ctl_host->done = 0;
+        ctl_host->status = 0;
         ctl_host->rate_bits = 0;
         AMR_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice, stream));
         if ((opts.flags & EMG_OPT_AUTOTUNE) && !tuned) {
@@ -1412,6 +1414,7 @@ struct emg_amr {
         rate_valid = true;
         t += dt;
         steps += 1;
+        if (ctl_host->status == EMG_ERR_INADMISSIBLE) return inadmissible();
         if (steps >= next_regrid) {
             cudaEvent_t a, b;
             cudaEventCreate(&a);
@@ -1432,6 +1435,8 @@ struct emg_amr {
         }
         unsigned int e = 0;
         AMR_CUDA(cudaMemcpy(&e, err, sizeof e, cudaMemcpyDeviceToHost));
+        if ((e & 4u) || ctl_host->status == EMG_ERR_BOUNDS)
+            return set_error(EMG_ERR_BOUNDS, "device index out of range (bounds-check build)");
         if (e) return set_error(EMG_ERR_UNFILLABLE, "AMR ghost cell without a source (prediction depth or box)");
         return EMG_OK;
     }
@@ -1441,6 +1446,7 @@ struct emg_amr {
             int rc = ensure_layout();
             if (rc) return rc;
             ctl_host->rate_bits = 0;
+            ctl_host->status = 0;
             AMR_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice, stream));
             AmrDev A = view();
             amr_cfl<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
@@ -1451,14 +1457,108 @@ struct emg_amr {
         AMR_CUDA(cudaMemcpyAsync(ctl_host, ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, stream));
         AMR_CUDA(cudaStreamSynchronize(stream));
         rate_valid = true;
+        if (ctl_host->status == EMG_ERR_INADMISSIBLE) return inadmissible();
         double rate;
         std::memcpy(&rate, &ctl_host->rate_bits, sizeof rate);
         *dt = opts.cfl / rate;
         return EMG_OK;
     }
 
-    int setup(const emg_amr_config* c, const emg_eos* e, const double* lo_, const double* hi_, const emg_bc* b,
-              const emg_opts* o) {
+    static int inadmissible() {
+        return set_error(EMG_ERR_INADMISSIBLE,
+                         "non-finite or inadmissible state (density, pressure or specific volume) in a leaf cell");
+    }
+
+    // Consistency of an adopted hierarchy (create_from_blocks), on the host
+    // before any device work. Structure errors (a block outside the levels or
+    // the domain, twice, without its parent, a leaf with children, an
+    // ancestor without all 2^D children) are EMG_ERR_INVALID. A hierarchy
+    // whose ghost cells would have no source — a base block missing, or a
+    // block whose parent lacks a same-level neighbour, i.e. not 2:1 balanced
+    // as Amr::refine_block keeps it (C/amr.rs:951-972) — is
+    // EMG_ERR_UNFILLABLE: the ghost prediction reads one coarser level only.
+    int check_hierarchy(const int64_t* desc, size_t nblocks) {
+        std::vector<std::vector<int>> seen(levels);
+        for (int l = 0; l < levels; l++) seen[l].assign(map[l].size(), -1);
+        for (size_t i = 0; i < nblocks; i++) {
+            const int64_t l = desc[5 * i];
+            const Key k = {desc[5 * i + 1], desc[5 * i + 2], desc[5 * i + 3]};
+            const int64_t sl = (l >= 0 && l < levels) ? slot_of((int)l, k) : -1;
+            if (sl < 0) return set_error(EMG_ERR_INVALID, "block outside the hierarchy");
+            if (seen[l][sl] >= 0) return set_error(EMG_ERR_INVALID, "block given twice");
+            seen[l][sl] = (int)i;
+        }
+        auto has = [&](int l, Key k) -> bool {
+            if (l < 0 || l >= levels) return false;
+            for (int d = 0; d < 3; d++) {
+                if (!act[d]) {
+                    k[d] = 0;
+                    continue;
+                }
+                const int64_t nbl_ = nb0[d] << l;
+                if (k[d] < 0 || k[d] >= nbl_) {
+                    if (bc[2 * d + (k[d] >= nbl_ ? 1 : 0)].kind != EMG_BC_PERIODIC) return true;  // outside: no block needed
+                    k[d] = ((k[d] % nbl_) + nbl_) % nbl_;
+                }
+            }
+            const int64_t sl = slot_of(l, k);
+            return sl >= 0 && seen[l][sl] >= 0;
+        };
+        for (int64_t i = 0; i < nb0[0]; i++)
+            for (int64_t j = 0; j < nb0[1]; j++)
+                for (int64_t k = 0; k < nb0[2]; k++)
+                    if (!has(0, Key{i, j, k}))
+                        return set_error(EMG_ERR_UNFILLABLE, "a base block is missing: part of the domain has no source");
+        int nkids = 1;
+        for (int d = 0; d < 3; d++) nkids *= act[d] ? 2 : 1;
+        for (size_t i = 0; i < nblocks; i++) {
+            const int l = (int)desc[5 * i];
+            const Key k = {desc[5 * i + 1], desc[5 * i + 2], desc[5 * i + 3]};
+            const bool leaf = desc[5 * i + 4] != 0;
+            int kids = 0;
+            for (int c = 0; c < 8; c++) {
+                Key ck = k;
+                bool valid = true;
+                for (int d = 0; d < 3; d++) {
+                    const int bit = (c >> d) & 1;
+                    if (!act[d]) {
+                        if (bit) valid = false;
+                        continue;
+                    }
+                    ck[d] = 2 * k[d] + bit;
+                }
+                if (valid && l + 1 < levels && has(l + 1, ck)) kids++;
+            }
+            if (leaf && kids > 0) return set_error(EMG_ERR_INVALID, "a leaf block has children");
+            if (!leaf && kids != nkids) return set_error(EMG_ERR_INVALID, "an ancestor block lacks some of its children");
+            if (l == 0) continue;
+            Key pk = k;
+            for (int d = 0; d < 3; d++) pk[d] = act[d] ? k[d] >> 1 : 0;
+            if (!has(l - 1, pk)) return set_error(EMG_ERR_INVALID, "a block without its parent");
+            for (int a = -1; a <= 1; a++)
+                for (int b = -1; b <= 1; b++)
+                    for (int c = -1; c <= 1; c++) {
+                        const int o[3] = {a, b, c};
+                        bool skip = false;
+                        Key nk = pk;
+                        for (int d = 0; d < 3; d++) {
+                            if (!act[d] && o[d] != 0) skip = true;
+                            nk[d] += o[d];
+                        }
+                        if (skip || (a == 0 && b == 0 && c == 0)) continue;
+                        if (!has(l - 1, nk))
+                            return set_error(EMG_ERR_UNFILLABLE,
+                                             "ghost cells without a source: the hierarchy is not 2:1 balanced (a block's "
+                                             "parent lacks a same-level neighbour)");
+                    }
+        }
+        return EMG_OK;
+    }
+
+    // host part of the set-up (configuration checks, level geometry, block
+    // map); no device work, so a bad configuration is reported on any host
+    int setup_host(const emg_amr_config* c, const emg_eos* e, const double* lo_, const double* hi_, const emg_bc* b,
+                   const emg_opts* o) {
         cfg = *c;
         eos = *e;
         opts = *o;
@@ -1530,6 +1630,11 @@ struct emg_amr {
         }
         regrid_interval = cfg.regrid_every;
         next_regrid = cfg.regrid_every;
+        return EMG_OK;
+    }
+
+    // device part of the set-up: stream, error word, control block, per-level dx
+    int setup_device() {
         int n = 0;
         if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
             cudaGetLastError();
@@ -1551,6 +1656,12 @@ struct emg_amr {
         if (rc) return rc;
         if (sweep_prepare_device() != cudaSuccess) return set_error(EMG_ERR_CUDA, "sweep setup failed");
         return EMG_OK;
+    }
+
+    int setup(const emg_amr_config* c, const emg_eos* e, const double* lo_, const double* hi_, const emg_bc* b,
+              const emg_opts* o) {
+        int rc = setup_host(c, e, lo_, hi_, b, o);
+        return rc ? rc : setup_device();
     }
 
     void release() {
@@ -1642,18 +1753,20 @@ int emg_amr_create_from_blocks(const emg_amr_config* cfg, const emg_eos* eos, co
     *out = nullptr;
     if (nblocks == 0) return set_error(EMG_ERR_INVALID, "a hierarchy needs at least one block");
     emg_amr* h = new emg_amr();
-    int rc = h->setup(cfg, eos, lo, hi, bc, opts);
     auto bail = [&](int code) {
         h->release();
         delete h;
         return code;
     };
+    int rc = h->setup_host(cfg, eos, lo, hi, bc, opts);
     if (rc) return bail(rc);
+    // the hierarchy is checked on the host before any device work
+    if ((rc = h->check_hierarchy(desc, nblocks))) return bail(rc);
+    if ((rc = h->setup_device())) return bail(rc);
     if ((rc = h->reserve((int64_t)nblocks))) return bail(rc);
     for (size_t i = 0; i < nblocks; i++) {
         const int l = (int)desc[5 * i];
         const Key k = {desc[5 * i + 1], desc[5 * i + 2], desc[5 * i + 3]};
-        if (l < 0 || l >= h->levels || h->slot_of(l, k) < 0) return bail(set_error(EMG_ERR_INVALID, "block outside the hierarchy"));
         h->blocks.push_back(HBlock{l, k, desc[5 * i + 4] != 0});
         h->insert(l, k, (int)i);
     }

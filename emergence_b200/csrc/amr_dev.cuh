@@ -69,6 +69,16 @@ __device__ __forceinline__ int64_t amr_cell(const AmrDev& A, const int64_t* c) {
 }
 
 __device__ __forceinline__ void amr_load(const AmrDev& A, int slot, int64_t cell, double* v) {
+    if constexpr (BOUNDS_CHECK) {
+        // bounds-check build: a pool index outside the pool sets bit 4 of the error word
+        const int64_t i = (int64_t)slot * A.bcell + cell;
+        if (slot < 0 || cell < 0 || cell >= A.bcell || i >= A.ntot) {
+            atomicOr(A.err, 4u);
+#pragma unroll
+            for (int q = 0; q < 5; q++) v[q] = 0.0;
+            return;
+        }
+    }
     const double* p = A.u + (int64_t)slot * A.bcell + cell;
 #pragma unroll
     for (int q = 0; q < 5; q++) v[q] = p[(int64_t)q * A.ntot];

@@ -715,12 +715,19 @@ __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rh
     const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
     const Eos<double> e = Eos<double>::from(A.eos);
     double rate = 0.0;
+    int bad = 0;  // a non-finite or inadmissible new leaf state (stage 3)
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
         int64_t c[3];
         c[2] = q % A.bd[2];
         c[1] = (q / A.bd[2]) % A.bd[1];
         c[0] = q / ((int64_t)A.bd[1] * A.bd[2]);
         const int64_t cell = (int64_t)slot * A.bcell + amr_cell(A, c);
+        if constexpr (BOUNDS_CHECK) {
+            if (slot < 0 || cell < 0 || cell >= A.ntot) {
+                atomicOr(A.err, 4u);
+                continue;
+            }
+        }
         double un[5];
         for (int k = 0; k < 5; k++) {
             const int64_t o = (int64_t)k * A.ntot + cell;
@@ -740,6 +747,7 @@ __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rh
         if (stage == 3) {
             double w[5];
             to_prim(e, un, w);
+            if (!admissible(e, w[0], w[4])) bad = 1;
             const double cs = sound_speed(e, w[0], w[4]);
             double s = -0.0;
             for (int i = 0; i < A.ndims; i++) {
@@ -753,11 +761,12 @@ __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rh
         for (int o = 16; o > 0; o >>= 1) rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, o));
         __shared__ double sr[32];
         if ((threadIdx.x & 31) == 0) sr[threadIdx.x >> 5] = rate;
-        __syncthreads();
+        const int any_bad = __syncthreads_or(bad);
         if (threadIdx.x == 0) {
             double v = sr[0];
             for (int w = 1; w < (int)(blockDim.x >> 5); w++) v = fmax(v, sr[w]);
             if (!isnan(v) && v > 0.0) atomicMax(&ctl->rate_bits, (unsigned long long)__double_as_longlong(v));
+            if (any_bad) atomicCAS(&ctl->status, 0, (int)EMG_ERR_INADMISSIBLE);
         }
     }
 }
@@ -770,12 +779,14 @@ __global__ void amr_cfl(const AmrDev A, const int* __restrict__ leaves, const in
     const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
     const Eos<double> e = Eos<double>::from(A.eos);
     double rate = 0.0;
+    int bad = 0;  // a non-finite or inadmissible leaf cell
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
         int64_t c[3];
         box_coord(q, A.bd, c);
         double uu[5], w[5];
         amr_load(A, slot, amr_cell(A, c), uu);
         to_prim(e, uu, w);
+        if (!admissible(e, w[0], w[4])) bad = 1;
         const double cs = sound_speed(e, w[0], w[4]);
         double s = -0.0;
         for (int i = 0; i < A.ndims; i++) {
@@ -787,11 +798,12 @@ __global__ void amr_cfl(const AmrDev A, const int* __restrict__ leaves, const in
     for (int o = 16; o > 0; o >>= 1) rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, o));
     __shared__ double sr[32];
     if ((threadIdx.x & 31) == 0) sr[threadIdx.x >> 5] = rate;
-    __syncthreads();
+    const int any_bad = __syncthreads_or(bad);
     if (threadIdx.x == 0) {
         double v = sr[0];
         for (int w = 1; w < (int)(blockDim.x >> 5); w++) v = fmax(v, sr[w]);
         if (!isnan(v) && v > 0.0) atomicMax(&ctl->rate_bits, (unsigned long long)__double_as_longlong(v));
+        if (any_bad) atomicCAS(&ctl->status, 0, (int)EMG_ERR_INADMISSIBLE);
     }
 }
 

@@ -684,6 +684,11 @@ int emg_batch1d_run_to(emg_batch1d* h, double t_end, uint64_t* launched) {
         if (I.status) return set_error(I.status, "time step collapsed in an instance");
         mx = std::max<uint64_t>(mx, I.steps);
     }
+    if (BOUNDS_CHECK) {
+        StepCtl c;
+        B_CUDA(cudaMemcpy(&c, h->ctl, sizeof c, cudaMemcpyDeviceToHost));
+        if (c.status == EMG_ERR_BOUNDS) return set_error(EMG_ERR_BOUNDS, "device index out of range (bounds-check build)");
+    }
     if (launched) *launched = mx;
     return EMG_OK;
 }

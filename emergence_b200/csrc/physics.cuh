@@ -13,6 +13,20 @@
 
 namespace emg {
 
+// Bounds-check build (compiled with -DEMG_BOUNDS_CHECK into
+// libemergence_b200_bc.so): every global index of the sweeps, the uniform
+// ghost fill and the AMR pool loads and RK update is checked against its
+// array before the access; an index out of range skips the access and raises
+// EMG_ERR_BOUNDS in the control block (or bit 4 of the AMR error word),
+// which the host reports after the call. Nothing traps. In the product build
+// the checks compile to nothing.
+#ifdef EMG_BOUNDS_CHECK
+constexpr bool BOUNDS_CHECK = true;
+#else
+constexpr bool BOUNDS_CHECK = false;
+#endif
+constexpr int STATUS_BOUNDS = 6;  // EMG_ERR_BOUNDS
+
 // NASG parameters (fluid/crates/compressible/src/eos.rs:12-25).
 struct EosD {
     double gamma, p_inf, b, q;

@@ -35,6 +35,7 @@ namespace emg {
 
 constexpr int SWEEP_THREADS = 256;
 
+
 // Device control block of one solver: the time step of the stage kernels is
 // read from here so that whole steps can run without a host round trip.
 struct StepCtl {
@@ -96,7 +97,20 @@ struct SweepParams {
     // of every face, stored at the index of the face's left cell (1 where the
     // high-order flux was kept); read back by the discrete adjoint
     double* theta_rec;
+    int64_t nface;  // elements of `face` (bounds-check build)
 };
+
+// index check of the bounds-check build: true when 0 <= i < n; otherwise the
+// control block's status becomes EMG_ERR_BOUNDS (first error kept)
+__device__ __forceinline__ bool in_bounds(StepCtl* ctl, int64_t i, int64_t n) {
+    if constexpr (!BOUNDS_CHECK) {
+        return true;
+    } else {
+        if (i >= 0 && i < n) return true;
+        atomicCAS(&ctl->status, 0, STATUS_BOUNDS);
+        return false;
+    }
+}
 
 // A segment of an instance line: `base` is the flat index of the cell five
 // rows before its first cell, `len` its cell count.
@@ -463,6 +477,7 @@ struct Sweep {
         auto lane_len = [&](int l) { return BATCH ? s_len[l] : Ls; };
         auto lane_tail = [&](int l) { return BATCH ? s_tail[l] != 0 : tail; };
         double rate_max = 0.0;
+        int bad_state = 0;  // a non-finite or inadmissible new state (fused CFL only)
 
         for (int r = 0; r < nrounds; r++) {
             // ---- A: load rows [lo, hi) and recover primitives (and ρe, sensors)
@@ -479,7 +494,8 @@ struct Sweep {
                         rr = idx / P;
                         l = idx % P;
                     }
-                    if (s_lok[l] && lo + rr < lane_len(l) + 10) {
+                    if (s_lok[l] && lo + rr < lane_len(l) + 10 &&
+                        in_bounds(p.ctl, base0 + (int64_t)(lo + rr) * p.sd + s_loff[l], p.ncell)) {
                         const int row = lo + rr;
                         const int64_t g = base0 + (int64_t)row * p.sd + s_loff[l];
                         double u[5], w[5];
@@ -631,11 +647,13 @@ struct Sweep {
                     }
 #pragma unroll
                     for (int k = 0; k < 5; k++) F[at<STR>(fidx, k, l)] = fh[k];
-                    if (!AMR && p.theta_rec) {
+                    if (!AMR && p.theta_rec && in_bounds(p.ctl, base0 + (int64_t)i * p.sd + s_loff[l], p.ncell)) {
                         // recorded for the discrete adjoint, at the face's left cell
                         p.theta_rec[base0 + (int64_t)i * p.sd + s_loff[l]] = th_rec;
                     }
-                    if (AMR && (fidx == 0 || fidx == Ls)) {
+                    if (AMR && (fidx == 0 || fidx == Ls) &&
+                        in_bounds(p.ctl, ((((int64_t)slot_id * 3 + D) * 2 + (fidx == 0 ? 0 : 1)) * 5 + 4) * p.npen + s_pen[l],
+                                  p.nface)) {
                         // block boundary faces for refluxing (C/amr.rs:1291-1295)
                         const int side = fidx == 0 ? 0 : 1;
                         double* fo = p.face + ((((int64_t)slot_id * 3 + D) * 2 + side) * 5) * p.npen + s_pen[l];
@@ -655,7 +673,8 @@ struct Sweep {
                     c = RM * r - 5 + tid / P;
                     l = tid % P;
                 }
-                if (s_lok[l] && c >= 0 && c < lane_len(l)) {
+                if (s_lok[l] && c >= 0 && c < lane_len(l) &&
+                    in_bounds(p.ctl, base0 + (int64_t)(c + 5) * p.sd + s_loff[l], p.ncell)) {
                     const int64_t g = base0 + (int64_t)(c + 5) * p.sd + s_loff[l];
                     const double inv_l = BATCH ? 1.0 / s_dx[l] : inv;
                     const double dt_l = BATCH ? s_dt[l] : dt;
@@ -691,6 +710,7 @@ struct Sweep {
                             // CFL rate Σ_d (|u_d| + c)/dx_d of the new state (C/solver.rs:485-497)
                             double w[5];
                             to_prim(ed, un_, w);
+                            if (!admissible(ed, w[0], w[4])) bad_state = 1;
                             const double cs = sound_speed(ed, w[0], w[4]);
                             double acc = -0.0;
 #pragma unroll
@@ -710,7 +730,7 @@ struct Sweep {
             for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
             if ((tid & 31) == 0) s_rate[tid >> 5] = v;
         }
-        __syncthreads();
+        const int any_bad = __syncthreads_or(bad_state);
         if (tid == 0) {
             if (s_weno) atomicAdd(&p.ctl->counters[1], (unsigned long long)s_weno);
             if (s_fallback) atomicAdd(&p.ctl->counters[2], (unsigned long long)s_fallback);
@@ -719,6 +739,7 @@ struct Sweep {
                 double v = s_rate[0];
                 for (int w = 1; w < T / 32; w++) v = fmax(v, s_rate[w]);
                 if (!isnan(v) && v > 0.0) atomicMax(&p.ctl->rate_bits, (unsigned long long)__double_as_longlong(v));
+                if (any_bad) atomicCAS(&p.ctl->status, 0, 4 /* EMG_ERR_INADMISSIBLE */);
             }
         }
     }

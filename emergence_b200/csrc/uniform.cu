@@ -50,7 +50,7 @@ __global__ void soa_to_aos(const double* __restrict__ soa, double* __restrict__ 
 
 struct GhostParams {
     double* u;
-    const StepCtl* ctl;
+    StepCtl* ctl;
     int64_t ncell;
     int64_t m[3];
     int64_t stride[3];
@@ -129,6 +129,10 @@ __global__ void ghost_kernel(const GhostParams p) {
         const int64_t sd = p.stride[p.d];
         auto at = [&](int64_t c) { return off + c * sd; };
         auto load = [&](int64_t c, double* v) {
+            if (!in_bounds(p.ctl, at(c), p.ncell)) {
+                for (int k = 0; k < 5; k++) v[k] = 0.0;
+                return;
+            }
             for (int k = 0; k < 5; k++) v[k] = p.u[k * p.ncell + at(c)];
         };
         CharStencilD ch[2];
@@ -202,7 +206,8 @@ __global__ void ghost_kernel(const GhostParams p) {
                     v[1 + p.d] = -v[1 + p.d];
                 }
         }
-        for (int k = 0; k < 5; k++) p.u[k * p.ncell + at(gi)] = v[k];
+        if (in_bounds(p.ctl, at(gi), p.ncell))
+            for (int k = 0; k < 5; k++) p.u[k * p.ncell + at(gi)] = v[k];
         switch (p.kind[1]) {
             case EMG_BC_PERIODIC: load(hi_s, v); break;
             case EMG_BC_OUTFLOW: load(n + ng - 1, v); break;
@@ -218,7 +223,8 @@ __global__ void ghost_kernel(const GhostParams p) {
                     v[1 + p.d] = -v[1 + p.d];
                 }
         }
-        for (int k = 0; k < 5; k++) p.u[k * p.ncell + at(n + ng + gi)] = v[k];
+        if (in_bounds(p.ctl, at(n + ng + gi), p.ncell))
+            for (int k = 0; k < 5; k++) p.u[k * p.ncell + at(n + ng + gi)] = v[k];
     }
 }
 
@@ -230,11 +236,13 @@ __global__ void cfl_kernel(const double* __restrict__ u, int64_t ncell, CellRang
     const int act[3] = {a0, a1, a2};
     const double dx[3] = {dx0, dx1, dx2};
     double rate = 0.0;
+    int bad = 0;  // a non-finite or inadmissible interior cell
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < cr.cells; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t c = cr.index(t);
         double q[5], w[5];
         for (int k = 0; k < 5; k++) q[k] = u[k * ncell + c];
         to_prim(e, q, w);
+        if (!admissible(e, w[0], w[4])) bad = 1;
         const double cs = sound_speed(e, w[0], w[4]);
         double acc = -0.0;
         for (int d = 0; d < 3; d++)
@@ -244,20 +252,26 @@ __global__ void cfl_kernel(const double* __restrict__ u, int64_t ncell, CellRang
     for (int o = 16; o > 0; o >>= 1) rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, o));
     __shared__ double s[32];
     if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = rate;
-    __syncthreads();
+    const int any_bad = __syncthreads_or(bad);
     if (threadIdx.x == 0) {
         double v = s[0];
         for (int w = 1; w < (int)(blockDim.x >> 5); w++) v = fmax(v, s[w]);
         if (!isnan(v) && v > 0.0) atomicMax(&ctl->rate_bits, (unsigned long long)__double_as_longlong(v));
+        if (any_bad) atomicCAS(&ctl->status, 0, (int)EMG_ERR_INADMISSIBLE);
     }
 }
 
-__global__ void ctl_reset_rate(StepCtl* ctl) { ctl->rate_bits = 0ull; }
+// the rate (and the status it may raise) is recomputed from the current state
+__global__ void ctl_reset_rate(StepCtl* ctl) {
+    ctl->rate_bits = 0ull;
+    ctl->status = 0;
+}
 
 // Host-given dt (Solver::step / GpuSolver::step).
 __global__ void ctl_begin_host(StepCtl* ctl, double dt) {
     ctl->dt = dt;
     ctl->done = 0;
+    ctl->status = 0;
     ctl->rate_bits = 0ull;
 }
 
@@ -265,6 +279,10 @@ __global__ void ctl_begin_host(StepCtl* ctl, double dt) {
 // check of Solver::run_to (C/solver.rs:758-768).
 __global__ void ctl_begin_device(StepCtl* ctl, double cfl) {
     if (ctl->done) return;
+    if (ctl->status) {  // the previous step left an inadmissible state
+        ctl->done = 1;
+        return;
+    }
     const double rate = __longlong_as_double((long long)ctl->rate_bits);
     const double t = ctl->t, t_end = ctl->t_end;
     double dt = cfl / rate;
@@ -727,6 +745,17 @@ double bits_to_double(unsigned long long b) {
     return v;
 }
 
+// the status the device raised, as read by the last sync_ctl
+int check_status(emg_uniform* h) {
+    const int st = h->ctl_host->status;
+    if (st == EMG_ERR_DT_COLLAPSED) return set_error(st, "time step collapsed: the solution lost admissibility");
+    if (st == EMG_ERR_INADMISSIBLE)
+        return set_error(st, "non-finite or inadmissible state (density, pressure or specific volume) in an interior cell");
+    if (st == EMG_ERR_BOUNDS) return set_error(st, "device index out of range (bounds-check build)");
+    if (st) return set_error(st, "device error");
+    return EMG_OK;
+}
+
 int check_handle(emg_uniform* h) {
     if (!h) return set_error(EMG_ERR_INVALID, "null handle");
     cudaError_t e = cudaSetDevice(h->device);
@@ -960,7 +989,9 @@ int emg_uniform_step(emg_uniform* h, double dt) {
     rc = launch_step_body(h);
     if (rc) return rc;
     h->rate_valid = true;
-    return sync_ctl(h);
+    rc = sync_ctl(h);
+    if (rc) return rc;
+    return check_status(h);
 }
 
 int emg_uniform_dt_cfl(emg_uniform* h, double* dt) {
@@ -971,6 +1002,7 @@ int emg_uniform_dt_cfl(emg_uniform* h, double* dt) {
     if (rc) return rc;
     rc = sync_ctl(h);
     if (rc) return rc;
+    if ((rc = check_status(h))) return rc;
     const double rate = bits_to_double(h->ctl_host->rate_bits);
     *dt = h->opts.cfl / rate;
     return EMG_OK;
@@ -981,9 +1013,10 @@ int emg_uniform_advance(emg_uniform* h, uint64_t nsteps, double t_end, uint64_t*
     if (rc) return rc;
     rc = ensure_rate(h);
     if (rc) return rc;
-    // arm device-driven stepping
+    // arm device-driven stepping (not from an inadmissible state)
     rc = sync_ctl(h);
     if (rc) return rc;
+    if ((rc = check_status(h))) return rc;
     StepCtl c = *h->ctl_host;
     c.t_end = t_end;
     c.done = 0;
@@ -1022,12 +1055,7 @@ int emg_uniform_advance(emg_uniform* h, uint64_t nsteps, double t_end, uint64_t*
     }
     if (taken) *taken = done_steps;
     h->rate_valid = true;
-    if (h->ctl_host->status) {
-        const int st = h->ctl_host->status;
-        return set_error(st, st == EMG_ERR_DT_COLLAPSED ? "time step collapsed: the solution lost admissibility"
-                                                        : "device error");
-    }
-    return EMG_OK;
+    return check_status(h);
 }
 
 int emg_uniform_run_to(emg_uniform* h, double t_end, uint64_t* steps) {

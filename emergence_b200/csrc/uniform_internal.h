@@ -90,4 +90,6 @@ int ensure_rate(emg_uniform* h);
 int sync_ctl(emg_uniform* h);
 // null check and cudaSetDevice
 int check_handle(emg_uniform* h);
+// EMG_OK, or the error the device raised (status of the control block mirror)
+int check_status(emg_uniform* h);
 }  // namespace emg

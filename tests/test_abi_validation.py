@@ -213,3 +213,87 @@ def test_amr_create_from_blocks_rejects_an_empty_hierarchy():
     rc = lib().emg_amr_create_from_blocks(C.byref(cfg), C.byref(EOS), lo_a, hi_a, bcs(OUT6), C.byref(opts()), desc, 0,
                                           u, C.byref(h))
     assert rc == INVALID and "at least one block" in err() and not h.value
+
+
+UNFILLABLE = 5
+
+
+def from_blocks(blocks, levels=3, bc=None):
+    """emg_amr_create_from_blocks on a 2-D 4×4-block base (16² cells per
+    block) with the given (level, i, j, k, leaf) rows; the data are zeros
+    (the hierarchy is checked before the data are read)."""
+    cfg = EmgAmrConfig(16, levels, 1e-3, 4, (4, 4, 0), 5)
+    lo_a, hi_a = (C.c_double * 3)(0.0, 0.0, 0.0), (C.c_double * 3)(1.0, 1.0, 0.0)
+    desc = np.asarray(blocks, dtype=np.int64).reshape(-1, 5)
+    u = np.zeros((len(desc), 16 * 16, 5))
+    h = C.c_void_p()
+    rc = lib().emg_amr_create_from_blocks(C.byref(cfg), C.byref(EOS), lo_a, hi_a, bcs(OUT6) if bc is None else bc,
+                                          C.byref(opts()), desc.ctypes.data_as(C.POINTER(C.c_int64)), len(desc),
+                                          u.ctypes.data_as(C.POINTER(C.c_double)), C.byref(h))
+    if rc == 0:
+        lib().emg_amr_destroy(h)
+    else:
+        assert not h.value
+    return rc
+
+
+def base(leaf_except=()):
+    return [[0, i, j, 0, 0 if (i, j) in leaf_except else 1] for i in range(4) for j in range(4)]
+
+
+def children(l, i, j, leaf=1):
+    return [[l + 1, 2 * i + a, 2 * j + b, 0, leaf] for a in range(2) for b in range(2)]
+
+
+def balanced():
+    """Every base block refined once, and the level-1 block (3,3) once more:
+    every block's parent has all its same-level neighbours."""
+    rows = base(leaf_except=[(i, j) for i in range(4) for j in range(4)])
+    for i in range(4):
+        for j in range(4):
+            rows += children(0, i, j)
+    rows = [r if r[:3] != [1, 3, 3] else [1, 3, 3, 0, 0] for r in rows]
+    return rows + children(1, 3, 3)
+
+
+def test_create_from_blocks_accepts_a_balanced_hierarchy_before_device_work():
+    if not no_gpu():
+        pytest.skip("a GPU is visible")
+    # the hierarchy passes its checks; only then is the (absent) device asked for
+    assert from_blocks(balanced()) == NO_DEVICE
+
+
+def test_create_from_blocks_reports_ghosts_without_a_source():
+    """Hierarchies the reference's Amr never produces (it keeps 2:1 balance,
+    C/amr.rs:951-972, and every base block): their ghost cells have no source
+    within one coarser level, so they are rejected as EMG_ERR_UNFILLABLE
+    before any device work, not discovered by a kernel."""
+    rows = [r for r in base() if (r[1], r[2]) != (2, 2)]
+    assert from_blocks(rows) == UNFILLABLE and "base block" in err()
+    # a level-2 block next to a level-0 leaf: the base block (0,0) refined,
+    # its child (1, 1,1) refined again, nothing else
+    rows = base(leaf_except=[(0, 0)]) + children(0, 0, 0)
+    rows = [r if r[:3] != [1, 1, 1] else [1, 1, 1, 0, 0] for r in rows] + children(1, 1, 1)
+    assert from_blocks(rows) == UNFILLABLE and "2:1" in err()
+
+
+@pytest.mark.parametrize("case, want", [
+    ("duplicate", "twice"),
+    ("outside", "outside"),
+    ("leaf_with_children", "leaf block has children"),
+    ("ancestor_missing_child", "lacks some of its children"),
+    ("orphan", "without its parent"),
+])
+def test_create_from_blocks_rejects_inconsistent_hierarchies(case, want):
+    rows = base()
+    if case == "duplicate":
+        rows = rows + [rows[0]]
+    elif case == "outside":
+        rows = rows + [[0, 4, 0, 0, 1]]
+    elif case == "leaf_with_children":
+        rows = rows + children(0, 1, 1)
+    elif case == "ancestor_missing_child":
+        rows = base(leaf_except=[(1, 1)]) + children(0, 1, 1)[:3]
+    elif case == "orphan":
+        rows = rows + [[2, 4, 4, 0, 1]]
+    assert from_blocks(rows) == INVALID and want in err(), err()

@@ -189,3 +189,22 @@ def test_autotuned_amr_sweeps_give_identical_results():
     assert np.array_equal(g0.structure(), g1.structure())
     assert np.array_equal(g0.download(), g1.download())
     assert g0.counters() == g1.counters()
+
+
+def test_inadmissible_leaf_state_is_reported():
+    """A NaN planted in one leaf cell of an adopted hierarchy: dt_cfl and step
+    return EMG_ERR_INADMISSIBLE (no trap, no device fault)."""
+    from emergence_b200 import EmgError
+    s, cfg, lo, hi, bc, init = W.shock_bubble(dim=2, base=4, levels=3)
+    o = O.OracleAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno)
+    st, u = o.structure(), o.download()
+    leaf = int(np.flatnonzero(st[:, 4] == 1)[0])
+    u = u.copy()
+    u[leaf, 37, 0] = float("nan")
+    g = gpu_amr(s, cfg, lo, hi, bc, mode=FluxMode.Weno, blocks=(st, u))
+    with pytest.raises(EmgError) as e:
+        g.dt_cfl()
+    assert e.value.code == 4
+    with pytest.raises(EmgError) as e:
+        g.step(1e-4)
+    assert e.value.code == 4

@@ -209,6 +209,50 @@ def test_collapsed_time_step_is_reported_not_trapped():
     assert g.dt_cfl() == O.OracleSolver(sys, mesh, u, bc=bc, mode=FluxMode.Weno).dt_cfl()
 
 
+@pytest.mark.parametrize("poison", ["nan_density", "negative_density", "negative_pressure", "nan_ghost"])
+def test_inadmissible_state_is_reported_by_the_cfl_reduction(poison):
+    """A host-poisoned interior cell (NaN, ρ < 0, or an energy below the
+    kinetic energy) is reported as EMG_ERR_INADMISSIBLE by dt_cfl and by
+    advance before any step is taken, and by a host-given step whose result
+    is still inadmissible; nothing traps and the handle stays usable. NaN in a ghost layer only is not an error: ghost
+    layers are refilled before they are read (tests/cpu.rs:25-52)."""
+    from emergence_b200 import EmgError
+    sys, mesh, u, bc = W.explosion((16, 16, 1), 0.4)
+    bad = u.copy()
+    c = mesh.idx(mesh.g(0) + 5, mesh.g(1) + 7, 0)
+    if poison == "nan_density":
+        bad[c, 0] = float("nan")
+    elif poison == "negative_density":
+        bad[c, 0] = -bad[c, 0]
+    elif poison == "negative_pressure":
+        bad[c, 4] = 0.0  # E = 0 with momentum 0: p = 0, not > 0
+        bad[c, 1] = 0.1
+    else:
+        bad[mesh.idx(0, mesh.g(1) + 7, 0), 0] = float("nan")
+    g = gpu_solver(sys, mesh, bad, bc=bc, mode=FluxMode.Weno)
+    if poison == "nan_ghost":
+        o = O.OracleSolver(sys, mesh, bad, bc=bc, mode=FluxMode.Weno)
+        assert g.dt_cfl() == o.dt_cfl()
+        g.step(o.dt_cfl())
+        return
+    for call in ("dt_cfl", "advance"):
+        with pytest.raises(EmgError) as e:
+            if call == "dt_cfl":
+                g.dt_cfl()
+            else:
+                g.advance(3)
+        assert e.value.code == 4, (call, e.value)
+    if poison == "nan_density":
+        # a host-given step is checked on its result: a NaN stays in the state
+        # (a negative ρ or p may be repaired by the fluxes of one step)
+        with pytest.raises(EmgError) as e:
+            g.step(1e-4)
+        assert e.value.code == 4
+    g.upload(u)
+    assert g.dt_cfl() == O.OracleSolver(sys, mesh, u, bc=bc, mode=FluxMode.Weno).dt_cfl()
+    g.advance(2)
+
+
 def test_unsupported_options_are_rejected():
     sys, mesh, u, bc = W.explosion((16, 16, 1), 0.4)
     from emergence_b200 import EmgError
