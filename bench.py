@@ -241,6 +241,7 @@ def run_ours(args, world, rank, local):
             traffic = tr["bytes_per_cell_per_launch"] * cells
     except Exception:
         pass
+    row_staging = "TMA bulk tensor copies" if g.features() & 1 else "per-thread loads"
     u_main = g.download() if not (args.no_mixed and not args.reference_gpu) else None
     g.close()
 
@@ -312,7 +313,7 @@ def run_ours(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if prec == Precision.F64 else "f32-flux/f64-state", "data": "synthetic",
-            "config": uniform_config(n, world, args.precision),
+            "config": dict(uniform_config(n, world, args.precision), sweep_row_loads=row_staging),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "traffic_source": "ncu capture on 160^3 scaled by cells (profiles/)", "kernel": "fused sweep (3 per stage)",
                          "alg_bytes_per_launch": alg_bytes_per_launch, "avg_launch_ms": per_launch_ms,

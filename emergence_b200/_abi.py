@@ -80,6 +80,7 @@ SIGNATURES = {
     "emg_uniform_set_profiling": (C.c_int, [_P, C.c_int]),
     "emg_uniform_kernel_times": (C.c_int, [_P, _D, _U64]),
     "emg_uniform_launch_count": (C.c_int, [_P, _U64]),
+    "emg_uniform_features": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "emg_uniform_step_noalloc": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc),
                                            C.POINTER(EmgOpts), C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
     "emg_batch1d_create": (C.c_int, [C.POINTER(EmgEos), C.POINTER(EmgOpts), C.POINTER(EmgBc), C.c_size_t,

@@ -29,6 +29,7 @@
 // and c+1.
 #pragma once
 #include "physics.cuh"
+#include "tma.cuh"
 #include <stdint.h>
 
 namespace emg {
@@ -160,12 +161,19 @@ template <typename RF, int P, int MODE> struct SweepSmem {
     }
 };
 
-enum SweepKind { KIND_GRID = 0, KIND_AMR = 1, KIND_BATCH = 2 };
+// KIND_GRID_TMA: a uniform 3-D grid whose phase-A rows arrive by TMA (one
+// box of the next round's RM rows × P lanes × 5 fields per round, issued a
+// round ahead into a shared-memory staging buffer) instead of per-thread loads.
+enum SweepKind { KIND_GRID = 0, KIND_AMR = 1, KIND_BATCH = 2, KIND_GRID_TMA = 3 };
+
+// Staging buffer of KIND_GRID_TMA (bytes, plus 128 for its alignment).
+template <int P> constexpr size_t tma_stage_bytes() { return (size_t)5 * P * (SWEEP_THREADS / P) * sizeof(double) + 128; }
 
 template <typename RF, int P, int D, int MODE, int KIND = KIND_GRID>
 struct Sweep {
     static constexpr bool AMR = KIND == KIND_AMR;
     static constexpr bool BATCH = KIND == KIND_BATCH;
+    static constexpr bool TMA = KIND == KIND_GRID_TMA;
     using SM = SweepSmem<RF, P, MODE>;
     static constexpr int T = SWEEP_THREADS;
     static constexpr int RM = T / P;
@@ -383,9 +391,17 @@ struct Sweep {
         return fabs(q0 - 4.0 * q1 + 6.0 * q2 - 4.0 * q3 + q4);  // C/scheme.rs:97-99
     }
 
-    __device__ static void run(const SweepParams& p) {
+    // tm: the stage input as a 4-D tensor map (dims k, j, i, field; box of
+    // RM rows along D × P lanes × 1 × 5 fields), KIND_GRID_TMA only
+    __device__ static void run(const SweepParams& p, const CUtensorMap* tm = nullptr) {
         extern __shared__ __align__(16) unsigned char smem_raw[];
         unsigned char* sp = smem_raw;
+        double* stg = nullptr;  // TMA staging buffer [field][row][lane] (D = 2: [field][lane][row])
+        if constexpr (TMA) {
+            const uintptr_t a = reinterpret_cast<uintptr_t>(sp);
+            stg = reinterpret_cast<double*>(sp + ((128 - (a & 127)) & 127));
+            sp += tma_stage_bytes<P>();
+        }
         double* W = reinterpret_cast<double*>(sp);
         sp += (size_t)RS * STRW * sizeof(double);
         double* MF = nullptr;  // midpoint fluxes (FP64 in both forms)
@@ -408,6 +424,14 @@ struct Sweep {
             s_fallback = 0;
             s_limited = 0;
             s_weno = 0;
+        }
+        __shared__ __align__(8) uint64_t s_bar;
+        if constexpr (TMA) {
+            if (tid == 0) {
+                mbar_init(smem_u32(&s_bar), 1);
+                fence_mbar_init();
+            }
+            // published by the lane-table barrier below
         }
 
         // uniform grids: x = lane tile, y = segment, z = other-axis row;
@@ -479,9 +503,76 @@ struct Sweep {
         double rate_max = 0.0;
         int bad_state = 0;  // a non-finite or inadmissible new state (fused CFL only)
 
+        // TMA: the box of round rr's rows [RM rr + AHEAD, RM rr + AHEAD + RM)
+        // (3-D grids: D = 0 rows along i, lanes along k; D = 1 rows along j,
+        // lanes along k; D = 2 rows along k, lanes along j; the host enables
+        // this kind only where every start coordinate along k is even)
+        auto tma_issue = [&](int rr) {
+            if constexpr (TMA) {
+                const int row0 = p.gd + s0 - 5 + RM * rr + AHEAD;
+                const int lane_c = p.gl + lane0, other_c = p.go + ob0;
+                int c0, c1, c2;
+                if constexpr (D == 0) {
+                    c0 = lane_c;
+                    c1 = other_c;
+                    c2 = row0;
+                } else if constexpr (D == 1) {
+                    c0 = lane_c;
+                    c1 = row0;
+                    c2 = other_c;
+                } else {
+                    c0 = row0;
+                    c1 = lane_c;
+                    c2 = other_c;
+                }
+                const uint32_t bar = smem_u32(&s_bar);
+                fence_proxy_async();  // the previous round's reads of the buffer come first
+                mbar_arrive_expect_tx(bar, (uint32_t)(5 * RM * P * sizeof(double)));
+                tma_load_4d(smem_u32(stg), tm, c0, c1, c2, 0, bar);
+            }
+        };
+
         for (int r = 0; r < nrounds; r++) {
             // ---- A: load rows [lo, hi) and recover primitives (and ρe, sensors)
-            {
+            if (TMA && r > 0) {
+                // rows of this round staged by TMA (issued during the previous round)
+                const int lo = RM * r + AHEAD;
+                const int hi = min(RM * r + RM + AHEAD, nrows);
+                const uint32_t bar = smem_u32(&s_bar);
+                const bool ok = mbar_wait_bounded(bar, (uint32_t)((r - 1) & 1), TMA_WAIT_LIMIT);
+                if (__syncthreads_or(!ok)) {
+                    // the copy did not land in time: report it, give the copy in
+                    // flight one more bounded wait, and leave
+                    if (tid == 0) atomicCAS(&p.ctl->status, 0, STATUS_TIMEOUT);
+                    mbar_wait_bounded(bar, (uint32_t)((r - 1) & 1), TMA_WAIT_LIMIT);
+                    return;
+                }
+                const int cnt = (hi - lo) * P;
+                for (int idx = tid; idx < cnt; idx += T) {
+                    int rr, l;
+                    if (D == 2) {
+                        rr = idx % (hi - lo);
+                        l = idx / (hi - lo);
+                    } else {
+                        rr = idx / P;
+                        l = idx % P;
+                    }
+                    if (s_lok[l] && lo + rr < lane_len(l) + 10) {
+                        const int row = lo + rr;
+                        double u[5], w[5];
+#pragma unroll
+                        for (int k = 0; k < 5; k++) u[k] = D == 2 ? stg[(k * P + l) * RM + rr] : stg[(k * RM + rr) * P + l];
+                        to_prim(ed, u, w);
+#pragma unroll
+                        for (int k = 0; k < 5; k++) W[at<STRW>(row, k, l)] = w[k];
+                        if constexpr (MODE != MODE_WENO) W[at<STRW>(row, 5, l)] = ed.rho_e(w[0], w[4]);
+                        if constexpr (MODE == MODE_HYBRID) {
+                            W[at<STRW>(row, 6, l)] = log(fmax(w[0], 1e-300));
+                            W[at<STRW>(row, 7, l)] = log(fmax(w[4] + ed.p_inf, 1e-300));
+                        }
+                    }
+                }
+            } else {
                 const int lo = r == 0 ? 0 : RM * r + AHEAD;
                 const int hi = min(RM * r + RM + AHEAD, nrows);
                 const int cnt = (hi - lo) * P;
@@ -516,6 +607,8 @@ struct Sweep {
                 }
             }
             __syncthreads();
+            // every thread is done with the staging buffer: fetch the next round's rows
+            if (TMA && tid == 0 && r + 1 < nrounds) tma_issue(r + 1);
             if constexpr (MODE == MODE_HYBRID) {
                 // ---- Θ: blend weights of faces [RM r, RM r + RM) (C/scheme.rs:171-182)
                 const int f = RM * r + tid / P;

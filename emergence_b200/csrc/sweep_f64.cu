@@ -91,6 +91,8 @@ cudaError_t sweep_launch_batch_f64(int mode, const SweepParams& p, dim3 grid, cu
     }
 }
 
+static cudaError_t tma_attr_f64();
+
 cudaError_t sweep_prepare_f64() {
     cudaError_t e = attr_p<MODE_WENO>();
     if (e == cudaSuccess) e = attr_p<MODE_HYBRID>();
@@ -104,7 +106,42 @@ cudaError_t sweep_prepare_f64() {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(sweep_f64_kernel<32, 0, MODE_CENTRAL, KIND_BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)SweepSmem<double, 32, MODE_CENTRAL>::bytes());
+    if (e == cudaSuccess) e = tma_attr_f64();
     return e;
+}
+
+// 3-D uniform grids, WENO mode, 32 pencils per CTA: phase-A rows by TMA
+template <int D>
+__global__ void __launch_bounds__(SWEEP_THREADS, 3) sweep_f64_tma_kernel(const SweepParams p,
+                                                                          const __grid_constant__ CUtensorMap tm) {
+    Sweep<double, 32, D, MODE_WENO, KIND_GRID_TMA>::run(p, &tm);
+}
+static size_t tma_smem_f64() { return SweepSmem<double, 32, MODE_WENO>::bytes() + tma_stage_bytes<32>(); }
+cudaError_t sweep_launch_tma_f64(const SweepParams& p, const CUtensorMap& tm, dim3 grid, cudaStream_t s) {
+    const size_t b = tma_smem_f64();
+    switch (p.d) {
+        case 0: sweep_f64_tma_kernel<0><<<grid, SWEEP_THREADS, b, s>>>(p, tm); break;
+        case 1: sweep_f64_tma_kernel<1><<<grid, SWEEP_THREADS, b, s>>>(p, tm); break;
+        case 2: sweep_f64_tma_kernel<2><<<grid, SWEEP_THREADS, b, s>>>(p, tm); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+static cudaError_t tma_attr_f64() {
+    const int b = (int)tma_smem_f64();
+    cudaError_t e = cudaFuncSetAttribute(sweep_f64_tma_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_f64_tma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_f64_tma_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    return e;
+}
+int sweep_tma_ctas_per_sm_f64() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_f64_tma_kernel<2>, SWEEP_THREADS, tma_smem_f64()) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
 }
 
 // resident CTAs per SM of the uniform-grid sweep (the three axes share registers and shared memory)

@@ -14,6 +14,14 @@ cudaError_t sweep_launch_amr_mixed(int P, int mode, const SweepParams& p, dim3 g
 // Batched independent 1-D lines (SweepParams::segs), 32 segments per CTA.
 cudaError_t sweep_launch_batch_f64(int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 cudaError_t sweep_launch_batch_mixed(int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
+// 3-D uniform grids, WENO mode, P = 32: phase-A rows staged by TMA from the
+// stage input described by `tm` (a 4-D map: k, j, i, field; box RM rows ×
+// 32 lanes × 1 × 5 fields, the row axis being p.d). Resident CTAs per SM of
+// that kernel (after the prepare call).
+cudaError_t sweep_launch_tma_f64(const SweepParams& p, const CUtensorMap& tm, dim3 grid, cudaStream_t s);
+cudaError_t sweep_launch_tma_mixed(const SweepParams& p, const CUtensorMap& tm, dim3 grid, cudaStream_t s);
+int sweep_tma_ctas_per_sm_f64();
+int sweep_tma_ctas_per_sm_mixed();
 // Resident CTAs per SM of the uniform-grid sweep kernel (after the prepare call).
 int sweep_ctas_per_sm_f64(int P, int mode);
 int sweep_ctas_per_sm_mixed(int P, int mode);

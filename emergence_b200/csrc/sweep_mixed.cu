@@ -92,6 +92,8 @@ cudaError_t sweep_launch_batch_mixed(int mode, const SweepParams& p, dim3 grid, 
     }
 }
 
+static cudaError_t tma_attr_mixed();
+
 cudaError_t sweep_prepare_mixed() {
     cudaError_t e = attr_p<MODE_WENO>();
     if (e == cudaSuccess) e = attr_p<MODE_HYBRID>();
@@ -105,7 +107,42 @@ cudaError_t sweep_prepare_mixed() {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(sweep_mixed_kernel<32, 0, MODE_CENTRAL, KIND_BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)SweepSmem<float, 32, MODE_CENTRAL>::bytes());
+    if (e == cudaSuccess) e = tma_attr_mixed();
     return e;
+}
+
+// 3-D uniform grids, WENO mode, 32 pencils per CTA: phase-A rows by TMA
+template <int D>
+__global__ void __launch_bounds__(SWEEP_THREADS, 3) sweep_mixed_tma_kernel(const SweepParams p,
+                                                                          const __grid_constant__ CUtensorMap tm) {
+    Sweep<float, 32, D, MODE_WENO, KIND_GRID_TMA>::run(p, &tm);
+}
+static size_t tma_smem_mixed() { return SweepSmem<float, 32, MODE_WENO>::bytes() + tma_stage_bytes<32>(); }
+cudaError_t sweep_launch_tma_mixed(const SweepParams& p, const CUtensorMap& tm, dim3 grid, cudaStream_t s) {
+    const size_t b = tma_smem_mixed();
+    switch (p.d) {
+        case 0: sweep_mixed_tma_kernel<0><<<grid, SWEEP_THREADS, b, s>>>(p, tm); break;
+        case 1: sweep_mixed_tma_kernel<1><<<grid, SWEEP_THREADS, b, s>>>(p, tm); break;
+        case 2: sweep_mixed_tma_kernel<2><<<grid, SWEEP_THREADS, b, s>>>(p, tm); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+static cudaError_t tma_attr_mixed() {
+    const int b = (int)tma_smem_mixed();
+    cudaError_t e = cudaFuncSetAttribute(sweep_mixed_tma_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_mixed_tma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_mixed_tma_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    return e;
+}
+int sweep_tma_ctas_per_sm_mixed() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_mixed_tma_kernel<2>, SWEEP_THREADS, tma_smem_mixed()) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
 }
 
 // resident CTAs per SM of the uniform-grid sweep (the three axes share registers and shared memory)

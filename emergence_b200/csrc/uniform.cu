@@ -16,6 +16,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <set>
@@ -519,6 +520,71 @@ int launch_ghosts(emg_uniform* h, double* arr) {
 
 int launch_axis(emg_uniform* h, int stage, int d, double* in, bool first, bool last);
 
+// TMA staging of the sweeps' row loads. Qualifying grids: 3-D, WENO mode,
+// ng even and n2 even (so that the k coordinate of every box starts on a
+// 16-byte boundary and every stride of the 4-D map (k, j, i, field) is a
+// multiple of 16 bytes), and a TMA kernel that keeps the plain kernel's
+// resident CTAs per SM. Each map covers one whole stage buffer of this GPU;
+// its box is one round of the sweep along d: RM = 8 rows × 32 lanes × 1 ×
+// 5 fields. Off unless EMG_TMA=1 is set in the environment: on the B200 the
+// staged sweeps measured no faster than the per-thread loads (256³: axis 2
+// 10.91 ms per step either way, axes 0-1 and the mixed form 1-2 % slower,
+// the 10 KB staging buffer taking shared memory from the L1 that holds the
+// sweep's register spills).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+        cudaGetLastError();
+    });
+    return fn;
+}
+
+void setup_tma(emg_uniform* h) {
+    h->tma = 0;
+    const char* on = std::getenv("EMG_TMA");
+    if (!on || on[0] != '1') return;
+    if (h->ndim != 3 || h->opts.mode != EMG_MODE_WENO || h->mesh.ng % 2 != 0 || h->m[2] % 2 != 0) return;
+    const bool mixed = h->opts.precision == EMG_PRECISION_MIXED;
+    const int plain = mixed ? sweep_ctas_per_sm_mixed(32, MODE_WENO) : sweep_ctas_per_sm_f64(32, MODE_WENO);
+    const int staged = mixed ? sweep_tma_ctas_per_sm_mixed() : sweep_tma_ctas_per_sm_f64();
+    if (staged < plain) return;
+    EncodeTiledFn enc = encode_tiled_fn();
+    if (!enc) return;
+    const cuuint64_t dims[4] = {(cuuint64_t)h->m[2], (cuuint64_t)h->m[1], (cuuint64_t)h->m[0], 5};
+    const cuuint64_t strides[3] = {(cuuint64_t)h->m[2] * 8, (cuuint64_t)(h->m[1] * h->m[2]) * 8, (cuuint64_t)h->ncell * 8};
+    const cuuint32_t ones[4] = {1, 1, 1, 1};
+    const int RM = SWEEP_THREADS / 32;
+    double* bufs[3] = {h->u, h->sa, h->sb};
+    for (int b = 0; b < 3; b++)
+        for (int d = 0; d < 3; d++) {
+            // box per sweep axis (dims k, j, i, field): rows along d, 32 lanes along the lane axis
+            cuuint32_t box[4];
+            if (d == 0) {
+                box[0] = 32; box[1] = 1; box[2] = RM;
+            } else if (d == 1) {
+                box[0] = 32; box[1] = RM; box[2] = 1;
+            } else {
+                box[0] = RM; box[1] = 32; box[2] = 1;
+            }
+            box[3] = 5;
+            CUresult r = enc(&h->tmap[b][d], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, bufs[b], dims, strides, box, ones,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return;
+        }
+    h->tma = 1;
+}
+
 int launch_stage(emg_uniform* h, int stage) {
     double* in = stage == 1 ? h->u : (stage == 2 ? h->sa : h->sb);
     int rc = launch_ghosts(h, in);
@@ -588,9 +654,20 @@ int launch_axis(emg_uniform* h, int stage, int d, double* in, bool first, bool l
         ProfScope ps(h, EMG_K_AXIS_0 + d);
         p.tol = h->opts.tol;
         p.theta_rec = h->theta_rec[stage - 1][d];
-        cudaError_t e = h->opts.precision == EMG_PRECISION_MIXED
-                            ? sweep_launch_mixed(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream)
-                            : sweep_launch_f64(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream);
+        // TMA staging: 32 pencils per CTA, the stage input one of the three
+        // mapped buffers, and along k (d = 2) an even first row in every segment
+        int buf = -1;
+        if (h->tma && h->sweepP[d] == 32 && (d != 2 || h->sweepSeg[d] % 2 == 0 || h->sweepGrid[d].y == 1))
+            buf = in == h->u ? 0 : (in == h->sa ? 1 : (in == h->sb ? 2 : -1));
+        cudaError_t e;
+        if (buf >= 0)
+            e = h->opts.precision == EMG_PRECISION_MIXED
+                    ? sweep_launch_tma_mixed(p, h->tmap[buf][d], h->sweepGrid[d], h->stream)
+                    : sweep_launch_tma_f64(p, h->tmap[buf][d], h->sweepGrid[d], h->stream);
+        else
+            e = h->opts.precision == EMG_PRECISION_MIXED
+                    ? sweep_launch_mixed(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream)
+                    : sweep_launch_f64(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream);
         if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("sweep launch: ") + cudaGetErrorString(e));
     }
     return EMG_OK;
@@ -925,6 +1002,7 @@ int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc
     for (int d = 0; d < 3; d++)
         if (h->active[d] && (h->sweepGrid[d].y > 65535u || h->sweepGrid[d].z > 65535u))
             return bail(set_error(EMG_ERR_INVALID, "mesh too large for the sweep grid (an axis above 65535 pencils)"));
+    setup_tma(h);
     int rc = emg_uniform_upload(h, u_aos, len);
     if (rc) return bail(rc);
     if ((opts->flags & EMG_OPT_AUTOTUNE) && (rc = autotune_sweeps(h))) return bail(rc);
@@ -1162,6 +1240,12 @@ int emg_uniform_kernel_times(emg_uniform* h, double* ms, uint64_t* launches) {
         h->prof_ms[k] = 0.0;
         h->prof_n[k] = 0;
     }
+    return EMG_OK;
+}
+
+int emg_uniform_features(emg_uniform* h, uint32_t* flags) {
+    if (!h || !flags) return set_error(EMG_ERR_INVALID, "null argument");
+    *flags = h->tma ? EMG_FEATURE_TMA : 0u;
     return EMG_OK;
 }
 

@@ -5,6 +5,8 @@
 #include "../../include/emergence_b200.h"
 #include "sweep_launch.h"
 
+#include <cuda.h>
+
 #include <string>
 #include <vector>
 
@@ -76,6 +78,11 @@ struct emg_uniform {
     // when set (by the discrete adjoint), the sweeps of stage s along axis d
     // record the positivity limiter's blend weights into theta_rec[s-1][d]
     double* theta_rec[3][3]{};
+    // TMA staging of the sweeps' row loads (3-D grids, WENO mode): a tensor
+    // map of each stage input (u, sa, sb) per sweep axis; tma = 0 when the
+    // grid does not qualify (see setup_tma)
+    CUtensorMap tmap[3][3];
+    int tma = 0;
 };
 
 

@@ -190,6 +190,12 @@ class GpuSolver:
         check(lib().emg_uniform_launch_count(self._h, C.byref(n)))
         return n.value
 
+    def features(self):
+        """EMG_FEATURE_* bits of the device paths this solver uses (bit 0: TMA row staging)."""
+        f = C.c_uint32()
+        check(lib().emg_uniform_features(self._h, C.byref(f)))
+        return f.value
+
 
 def state_hash(mesh, u):
     """64-bit fingerprint of a ghost-padded AoS conserved state (host code, no

@@ -206,6 +206,15 @@ int emg_uniform_kernel_times(emg_uniform* h, double* ms, uint64_t* launches);
 /* Number of kernel launches issued by the handle since creation. */
 int emg_uniform_launch_count(emg_uniform* h, uint64_t* launches);
 
+/* Device paths the handle uses, as EMG_FEATURE_* bits (no counterpart in the
+ * reference). EMG_FEATURE_TMA: the fused sweeps receive each round's rows of
+ * the stage input as a TMA bulk tensor copy (cp.async.bulk.tensor into shared
+ * memory, issued a round ahead) instead of per-thread loads; used on 3-D grids
+ * in WENO mode with ng and n2 even when EMG_TMA=1 is set in the environment
+ * at creation (off by default: measured no faster on the B200). */
+#define EMG_FEATURE_TMA 1u
+int emg_uniform_features(emg_uniform* h, uint32_t* flags);
+
 /* Largest padded cell count (m0·m1·m2) accepted by emg_uniform_step_noalloc. */
 #define EMG_NOALLOC_MAX_CELLS 131072
 

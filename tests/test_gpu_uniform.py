@@ -114,6 +114,36 @@ def test_short_axes_use_deep_ghost_images(shape, bcname):
     assert np.array_equal(g.download(), o.download())
 
 
+@pytest.mark.parametrize("precision", [Precision.F64, Precision.Mixed])
+@pytest.mark.parametrize("shape", [(40, 36, 30), (24, 22, 64)])
+def test_tma_row_staging_gives_the_plain_loads_results(shape, precision, monkeypatch):
+    """With EMG_TMA=1, 3-D WENO grids with ng and n2 even stage the sweeps'
+    rows by TMA (EMG_FEATURE_TMA): bit for bit the oracle's results in the
+    FP64 form, and the same bits as the per-thread loads (the default) in
+    both forms."""
+    sys, mesh, u, bc = W.explosion(shape, 0.3)
+    monkeypatch.setenv("EMG_TMA", "1")
+    g = gpu_solver(sys, mesh, u, bc=bc, mode=FluxMode.Weno, precision=precision)
+    assert g.features() & 1
+    monkeypatch.delenv("EMG_TMA")
+    p = gpu_solver(sys, mesh, u, bc=bc, mode=FluxMode.Weno, precision=precision)
+    assert not p.features() & 1
+    o = O.OracleSolver(sys, mesh, u, bc=bc, mode=FluxMode.Weno)
+    for _ in range(3):
+        dt = o.dt_cfl()
+        g.step(dt)
+        p.step(dt)
+        o.step(dt)
+    assert g.advance(2) == 2 and p.advance(2) == 2
+    for _ in range(2):
+        o.step(o.dt_cfl())
+    ug = g.download()
+    assert np.array_equal(ug, p.download())
+    if precision == Precision.F64:
+        assert np.array_equal(mesh.interior(ug), mesh.interior(o.download()))
+        assert g.counters() == o.counters()
+
+
 def test_uniform_flow_is_preserved():
     w0 = np.array([1.0, 0.3, -0.2, 0.1, 1.0])
     mesh = Mesh.new((9, 7, 6), (0, 0, 0), (1, 1, 1), ng=6)
