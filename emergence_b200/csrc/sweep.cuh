@@ -373,16 +373,41 @@ struct Sweep {
         }
     }
 
-    // one-sided admissibility of the limiter (C/scheme.rs:408-416), in f64
+    // Division-free sufficient condition for the admissibility test of a
+    // conserved state a of an ideal gas (b = q = p∞ = 0): ρ > 0 and
+    // 2ρE − |ρu|² > 0 with a relative margin of 1e-11, values bounded so that
+    // nothing over- or underflows. Whenever it holds, the reference's test
+    // (to_prim: ein = E/ρ − ½|u|², p = (γ−1)·ein/(1/ρ); then ρ > 0, p > 0,
+    // both finite, 1/ρ > 0) holds as well: the computed ein is within a few
+    // ulps of (2ρE − |ρu|²)/(2ρ²), far inside the margin. Where it does not
+    // hold, the reference's test runs as is, so the decision is always the
+    // reference's.
+    __device__ static __forceinline__ bool surely_admissible(const double* a) {
+        const double r = a[0], E = a[4];
+        if (!(r > 1e-100 && r < 1e100 && E > 1e-100 && E < 1e100 && fabs(a[1]) < 1e100 && fabs(a[2]) < 1e100 &&
+              fabs(a[3]) < 1e100))
+            return false;
+        const double m2 = a[1] * a[1] + a[2] * a[2] + a[3] * a[3];
+        const double twore = 2.0 * r * E;
+        return twore - m2 > 1e-11 * (twore + m2);
+    }
+
+    // one-sided admissibility of the limiter (C/scheme.rs:408-416), in f64;
+    // `ideal`: the equation of state is an ideal gas with 1 < γ < 100, which
+    // admits the division-free test above
     __device__ static __forceinline__ bool lim_ok(const Eos<double>& e, const double* fx, const double* ul,
-                                                  const double* fl, const double* ur, const double* fr, double lam2) {
+                                                  const double* fl, const double* ur, const double* fr, double lam2,
+                                                  bool ideal) {
         double a[5], w[5];
 #pragma unroll
         for (int k = 0; k < 5; k++) a[k] = ul[k] - lam2 * (fx[k] - fl[k]);
-        to_prim(e, a, w);
-        if (!admissible(e, w[0], w[4])) return false;
+        if (!(ideal && surely_admissible(a))) {
+            to_prim(e, a, w);
+            if (!admissible(e, w[0], w[4])) return false;
+        }
 #pragma unroll
         for (int k = 0; k < 5; k++) a[k] = ur[k] + lam2 * (fx[k] - fr[k]);
+        if (ideal && surely_admissible(a)) return true;
         to_prim(e, a, w);
         return admissible(e, w[0], w[4]);
     }
@@ -493,6 +518,7 @@ struct Sweep {
         const double lam2 = 2.0 * lam;
         const bool lim_on = p.positivity && lam > 0.0;  // C/scheme.rs:278
         const double inv = 1.0 / dx;
+        const bool ideal_gas = ed.b == 0.0 && ed.q == 0.0 && ed.p_inf == 0.0 && ed.gamma > 1.0 && ed.gamma < 100.0;
         __syncthreads();  // lane table
         const int Lmax = BATCH ? s_maxlen : Ls;
         const int nrounds = (Lmax + 5 + RM - 1) / RM;
@@ -715,7 +741,7 @@ struct Sweep {
                         bool finite = true;
 #pragma unroll
                         for (int k = 0; k < 5; k++) finite = finite && isfinite(fh[k]);
-                        if (!(finite && lim_ok(ed, fh, ul, flp, ur, frp, lam2_l))) {
+                        if (!(finite && lim_ok(ed, fh, ul, flp, ur, frp, lam2_l, ideal_gas))) {
                             const double alpha = fmax(fabs(wi[un]) + sound_speed(ed, wi[0], wi[4]),
                                                       fabs(wj[un]) + sound_speed(ed, wj[0], wj[4]));
                             double flf[5], bl[5];
@@ -727,7 +753,7 @@ struct Sweep {
 #pragma unroll
                                 for (int k = 0; k < 5; k++)
                                     bl[k] = isfinite(fh[k]) ? mid * fh[k] + (1.0 - mid) * flf[k] : flf[k];
-                                if (lim_ok(ed, bl, ul, flp, ur, frp, lam2_l))
+                                if (lim_ok(ed, bl, ul, flp, ur, frp, lam2_l, ideal_gas))
                                     lo = mid;
                                 else
                                     hi = mid;
