@@ -384,9 +384,14 @@ def sub_records(args, world, rank, local):
     out["adjoint"] = _compact(adj, ("value", "unit", "forward_ms", "recompute_ms", "reverse_ms",
                                     "forward_cell_updates_per_s", "fd_check", "clocks"))
     out["adjoint"]["workload"] = adj["config"]["workload"]
-    badj = measure_batch_adjoint(args, world, rank, local, steps=1, warmup=1, dual_check=False)
-    out["batch_adjoint"] = _compact(badj, ("value", "unit", "forward_ms", "recompute_ms", "reverse_ms", "clocks"))
-    out["batch_adjoint"]["workload"] = badj["config"]["workload"]
+    rec = {}
+    for prec in ("f64", "mixed"):
+        badj = measure_batch_adjoint(args, world, rank, local, steps=1, warmup=1, dual_check=False, precision=prec)
+        rec[prec] = _compact(badj, ("value", "unit", "forward_ms", "recompute_ms", "reverse_ms", "clocks"))
+        rec["workload"] = badj["config"]["workload"]
+    rec["note"] = ("value = backward/forward cost; the mixed batch records its FP32-flux run and applies the FP64 "
+                   "step's transposed Jacobian at its stage states")
+    out["batch_adjoint"] = rec
     return out
 
 
@@ -709,7 +714,7 @@ def run_batch_adjoint(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
-def measure_batch_adjoint(args, world, rank, local, steps=None, warmup=None, dual_check=True):
+def measure_batch_adjoint(args, world, rank, local, steps=None, warmup=None, dual_check=True, precision=None):
     """Gradients of the 4096 independent 1-D Riemann problems: J_i = total
     energy in the right half [0.5, 1] at t = 0.15, differentiated with respect
     to the six initial values (ρ, u, p left and right of x = 0.5) of every
@@ -725,10 +730,13 @@ def measure_batch_adjoint(args, world, rank, local, steps=None, warmup=None, dua
 
     torch.cuda.set_device(local)
     dev = torch.cuda.current_device()
+    from emergence_b200.physics import Precision
     steps = args.steps if steps is None else steps
     warmup = args.warmup if warmup is None else warmup
+    precision = args.precision if precision is None else precision
+    prec = Precision.Mixed if precision == "mixed" else Precision.F64
     sys_, n, dx, u, st = W.riemann_batch()
-    g = GpuBatch1D(sys_, n, dx, u)
+    g = GpuBatch1D(sys_, n, dx, u, precision=prec)
     for _ in range(max(warmup, 1)):
         g.record(0.15)
         g.objective(OBJ_ENERGY, 0.5, 1.0)
@@ -783,7 +791,7 @@ def measure_batch_adjoint(args, world, rank, local, steps=None, warmup=None, dua
     line = {
         "metric": "adjoint/forward cost", "value": (r + v) / f, "unit": "ratio", "n_gpus": world,
         "steps": steps, "warmup": warmup, "ms_per_step": f + r + v, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == Precision.F64 else "f32-flux/f64-state", "data": "synthetic",
         "config": {"workload": "4096 independent 1-D Riemann problems, cells log-uniform [64, 2048] (sum %d), "
                                "rho,p~U[0.1,2], u~U[-1,1], t_end 0.15, outflow; J_i = sum E dx over [0.5, 1]; "
                                "gradient w.r.t. the six initial values" % int(n.sum()),

@@ -724,8 +724,6 @@ int emg_batch1d_stream(emg_batch1d* h, void** stream) {
 int emg_batch1d_record(emg_batch1d* h, double t_end, uint64_t checkpoint_every, uint64_t* batch_steps) {
     if (!h) return set_error(EMG_ERR_INVALID, "null handle");
     if (!std::isfinite(t_end)) return set_error(EMG_ERR_INVALID, "t_end must be finite");
-    if (h->opts.precision != EMG_PRECISION_F64)
-        return set_error(EMG_ERR_INVALID, "the adjoint differentiates the FP64 form: create the batch with FP64");
     if (h->opts.mode != EMG_MODE_WENO) return set_error(EMG_ERR_INVALID, "the adjoint supports the WENO flux mode");
     for (int s = 0; s < 2; s++)
         if (h->bc[s].kind == EMG_BC_PERIODIC)

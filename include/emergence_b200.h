@@ -273,10 +273,13 @@ int emg_batch1d_stream(emg_batch1d* h, void** stream);
 
 /* Discrete adjoint of a batched run (no counterpart in the reference, which
  * has no adjoint; each instance is the 1-D Solver::step map, C/solver.rs:659-738).
- * Records an FP64 run of every instance to t_end from the initial state given
- * at creation (WENO mode; FP64 batch), keeping the batch state every
- * `checkpoint_every` batch steps (0: 64); *batch_steps receives the number of
- * batch steps. Time steps and limiter blend weights are held fixed. */
+ * Records a run of every instance to t_end from the initial state given at
+ * creation (WENO mode), keeping the batch state every `checkpoint_every` batch
+ * steps (0: 64); *batch_steps receives the number of batch steps. Time steps
+ * and limiter blend weights are held fixed. An FP64 batch is differentiated
+ * exactly; a mixed (FP32-flux) batch records its own run, and the backward
+ * pass applies the transposed Jacobian of the FP64 step at the recorded
+ * mixed stage states (the FP32 rounding is not differentiated). */
 int emg_batch1d_record(emg_batch1d* h, double t_end, uint64_t checkpoint_every, uint64_t* batch_steps);
 
 /* Per-instance box objective J_i on the recorded final state over cells with

@@ -96,11 +96,25 @@ def test_batched_gradients_match_finite_differences():
         assert np.all(np.abs(fd - grad[:, q]) <= 1e-3 * np.maximum(np.abs(grad[:, q]), 1e-3)), (q, fd, grad[:, q])
 
 
-def test_record_needs_an_fp64_batch():
-    from emergence_b200 import EmgError, GpuBatch1D
+def test_mixed_batch_gradients_follow_the_fp64_gradients():
+    """A mixed (FP32-flux, FP64-state) batch records its own run and is
+    differentiated with the FP64 step's transposed Jacobian at its recorded
+    stage states: its gradients agree with the FP64 batch's to the mixed
+    form's own error level (1e-6 relative), and its objective with the FP64
+    objective likewise."""
+    from emergence_b200 import GpuBatch1D
     from emergence_b200.physics import Precision
-    sys_, n, dx, u, st = batch(ninst=2)
-    g = GpuBatch1D(sys_, n, dx, u, precision=Precision.Mixed)
-    with pytest.raises(EmgError):
+    sys_, n, dx, u, st = batch(ninst=8, seed=13)
+    out = {}
+    for prec in (Precision.F64, Precision.Mixed):
+        g = GpuBatch1D(sys_, n, dx, u, bc=(Bc.Outflow, Bc.Outflow), precision=prec)
         g.record(0.15)
-    g.close()
+        J = g.objective(OBJ_ENERGY, 0.5, 1.0)
+        out[prec] = (J, g.backward(0.5))
+        g.close()
+    (J64, g64), (Jm, gm) = out[Precision.F64], out[Precision.Mixed]
+    assert np.all(np.abs(Jm - J64) <= 1e-6 * np.abs(J64)), (Jm, J64)
+    scale = np.abs(g64).max(axis=1, keepdims=True)
+    err = np.abs(gm - g64) / scale
+    print("mixed vs FP64 batched gradients, max rel err", err.max())
+    assert np.all(err <= 1e-6), err
