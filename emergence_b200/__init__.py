@@ -10,7 +10,8 @@ from .solver import GpuSolver, device_count, state_hash
 from .amr import GpuAmr
 from .batch import GpuBatch1D
 from .adjoint import DifferentiableSolver
+from .five import FiveEq, GpuFiveSolver, five_initial_state
 from ._abi import EmgError, LIB_PATH
 
-__all__ = ["Bc", "Euler", "FluxMode", "Mesh", "Nasg", "Precision", "initial_state", "GpuSolver", "GpuAmr", "GpuBatch1D", "DifferentiableSolver", "device_count", "state_hash",
+__all__ = ["Bc", "Euler", "FluxMode", "Mesh", "Nasg", "Precision", "initial_state", "GpuSolver", "GpuAmr", "GpuBatch1D", "DifferentiableSolver", "FiveEq", "GpuFiveSolver", "five_initial_state", "device_count", "state_hash",
            "EmgError", "LIB_PATH"]

@@ -36,6 +36,14 @@ class EmgBc(C.Structure):
     _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("state", C.c_double * 5)]
 
 
+class EmgBc7(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("state", C.c_double * 7)]
+
+
+class EmgFiveSystem(C.Structure):
+    _fields_ = [("eos", EmgEos * 2), ("kapila", C.c_int32), ("reserved", C.c_int32)]
+
+
 class EmgAmrConfig(C.Structure):
     _fields_ = [("b", C.c_int64), ("levels", C.c_int64), ("eps", C.c_double), ("regrid_every", C.c_int64),
                 ("base_blocks", C.c_int64 * 3), ("ghosts", C.c_int64)]
@@ -65,6 +73,17 @@ SIGNATURES = {
     "emg_uniform_create": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc), C.POINTER(EmgOpts),
                                      _D, C.c_size_t, C.POINTER(_P)]),
     "emg_uniform_destroy": (C.c_int, [_P]),
+    "emg_five_create": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgFiveSystem), C.POINTER(EmgBc7), C.POINTER(EmgOpts),
+                                  _D, C.c_size_t, C.POINTER(_P)]),
+    "emg_five_destroy": (C.c_int, [_P]),
+    "emg_five_step": (C.c_int, [_P, C.c_double]),
+    "emg_five_dt_cfl": (C.c_int, [_P, _D]),
+    "emg_five_run_to": (C.c_int, [_P, C.c_double, _U64]),
+    "emg_five_download": (C.c_int, [_P, _D, C.c_size_t]),
+    "emg_five_counters": (C.c_int, [_P, _U64]),
+    "emg_five_totals": (C.c_int, [_P, _D]),
+    "emg_five_get_time": (C.c_int, [_P, _D]),
+    "emg_five_launch_count": (C.c_int, [_P, _U64]),
     "emg_uniform_step": (C.c_int, [_P, C.c_double]),
     "emg_uniform_dt_cfl": (C.c_int, [_P, _D]),
     "emg_uniform_run_to": (C.c_int, [_P, C.c_double, _U64]),

@@ -7,6 +7,7 @@ Translation units and their FMA policy:
   amr.cu          block-AMR host object, AMR kernels, C ABI      -fmad=false
   batch1d.cu      batched independent 1-D lines, C ABI           -fmad=false
   adjoint.cu      discrete adjoint of the uniform FP64 step      -fmad=false
+  five.cu         five-equation two-phase system, C ABI           -fmad=false
   sweep_f64.cu    plain FP64 fused sweep                          -fmad=false
   sweep_mixed.cu  FP32-flux fused sweep                           -fmad=true
 The FP64 units keep every multiply and add separately rounded so that their
@@ -30,6 +31,7 @@ UNITS = [
     ("amr.cu", ["-fmad=false"]),
     ("batch1d.cu", ["-fmad=false"]),
     ("adjoint.cu", ["-fmad=false"]),
+    ("five.cu", ["-fmad=false"]),
     ("sweep_f64.cu", ["-fmad=false"]),
     ("sweep_mixed.cu", ["-fmad=true", "-use_fast_math"]),
 ]

@@ -1,0 +1,472 @@
+// Fused per-axis sweep of the WCNS / HLLC / positivity scheme for the
+// five-equation system (uniform grids, FP64). Same streaming design as the
+// Euler sweep (sweep.cuh): a CTA of 256 threads owns P adjacent pencils over
+// one segment of the sweep axis and streams it in rounds of RM = 256/P rows
+// through shared-memory rings:
+//
+//   A  rows of the 7 conserved fields → primitives (plus ρe for the central
+//      flux and the 3 sensor values for the hybrid switch) in the W ring;
+//   Θ  (hybrid) the blend weight of each face from the sensors;
+//   B  one thread per (midpoint, pencil): characteristic WENO5-Z
+//      interpolation of the 7 fields, admissibility fallback, HLLC flux and
+//      contact speed (MF ring);
+//   C  one thread per (face, pencil): 6th-order WCNS combination of the
+//      midpoint fluxes and contact speeds, central KEEP-PE flux and face
+//      velocity where θ < 1, positivity limiter (F ring, 7 fluxes + face
+//      velocity);
+//   D  one thread per (cell, pencil): −(F⁺ − F⁻)/dx and the non-conservative
+//      term (α + K)(Ũ⁺ − Ũ⁻)/dx of the α equation into the residual; on the
+//      last active axis the SSP-RK3 combination into the next stage state.
+//
+// Operation order follows the reference CPU solver (scheme.rs:132-464,
+// solver.rs:431-442) so that the FP64 results are bit-identical with it.
+#pragma once
+#include "five_physics.cuh"
+#include "sweep.cuh"
+
+namespace emg {
+
+struct FiveSweepParams {
+    const double* __restrict__ uin;
+    double* rhs;
+    const double* base;
+    const double* cur;
+    double* dest;
+    StepCtl* ctl;
+    int64_t ncell;
+    int64_t sd, sl, so;
+    int nd, nl, no;
+    int gd, gl, go;
+    int d;
+    int seg;
+    int first, last;
+    int stage;
+    int rows_contig;
+    double dx;
+    double ndim;
+    int positivity;
+    double tol;
+    FiveSysD sys;
+};
+
+template <int P, int MODE> struct FiveSmem {
+    static constexpr int RM = SWEEP_THREADS / P;
+    static constexpr int RS = RingSize<RM, MODE>::value;
+    // per cell: 7 primitives, + ρe (central flux), + 3 sensor values (hybrid)
+    static constexpr int NW = MODE == MODE_WENO ? NF : (MODE == MODE_CENTRAL ? NF + 1 : NF + 4);
+    static constexpr int STRW = NW * P + 1;
+    static constexpr int STR = (NF + 1) * P + 1;  // 7 fluxes + velocity
+    static constexpr bool MID = MODE != MODE_CENTRAL;
+    static constexpr size_t bytes() {
+        return (size_t)RS * STRW * sizeof(double) + (MID ? (size_t)RS * STR * sizeof(double) : 0) +
+               (size_t)RS * STR * sizeof(double) + (MODE == MODE_HYBRID ? (size_t)RS * P * sizeof(double) : 0);
+    }
+};
+
+template <int P, int D, int MODE> struct FiveSweep {
+    using SM = FiveSmem<P, MODE>;
+    static constexpr int T = SWEEP_THREADS;
+    static constexpr int RM = SM::RM;
+    static constexpr int RS = SM::RS;
+    static constexpr int STRW = SM::STRW;
+    static constexpr int STR = SM::STR;
+    static constexpr bool MID = SM::MID;
+    static constexpr int AHEAD = MODE == MODE_HYBRID ? 7 : 5;
+    static constexpr int UN = F_IU + D;
+    static constexpr int T1 = F_IU + (D + 1) % 3, T2 = F_IU + (D + 2) % 3;
+
+    __device__ static __forceinline__ int slot(int x) { return x & (RS - 1); }
+    template <int S> __device__ static __forceinline__ int at(int x, int k, int l) { return slot(x) * S + k * P + l; }
+
+    // scheme.rs:286-333 with the five-equation eigenvectors (multiphase.rs:202-236)
+    __device__ static __forceinline__ double midpoint(const Five& s, const double* __restrict__ W, int m, int l,
+                                                      double* f, bool& fb) {
+        const int j = m + 2;
+        double avg[NF];
+#pragma unroll
+        for (int k = 0; k < NF; k++) avg[k] = 0.5 * (W[at<STRW>(j, k, l)] + W[at<STRW>(j + 1, k, l)]);
+        const double rh = Five::rho(avg);
+        const double c = s.sound_speed(avg);
+        const double kk = s.kapila_k(avg);
+        const double c2 = c * c;
+        const double l0p = -avg[0] / rh / c2;
+        const double l1p = -avg[1] / rh / c2;
+        const double l2u = -rh / (2.0 * c);
+        const double l2p = 1.0 / (2.0 * c2);
+        const double l5u = rh / (2.0 * c);
+        const double l5p = 1.0 / (2.0 * c2);
+        const double l6p = kk / rh / c2;
+        double cl[NF], cr[NF];
+#pragma unroll
+        for (int a = 0; a < NF; a++) {
+            double ch[6];
+#pragma unroll
+            for (int s6 = 0; s6 < 6; s6++) {
+                const int row = m + s6;
+                switch (a) {
+                    case 0: ch[s6] = W[at<STRW>(row, 0, l)] + l0p * W[at<STRW>(row, F_IP, l)]; break;
+                    case 1: ch[s6] = W[at<STRW>(row, 1, l)] + l1p * W[at<STRW>(row, F_IP, l)]; break;
+                    case 2: ch[s6] = l2u * W[at<STRW>(row, UN, l)] + l2p * W[at<STRW>(row, F_IP, l)]; break;
+                    case 3: ch[s6] = W[at<STRW>(row, T1, l)]; break;
+                    case 4: ch[s6] = W[at<STRW>(row, T2, l)]; break;
+                    case 5: ch[s6] = l5u * W[at<STRW>(row, UN, l)] + l5p * W[at<STRW>(row, F_IP, l)]; break;
+                    default: ch[s6] = l6p * W[at<STRW>(row, F_IP, l)] + W[at<STRW>(row, F_IA, l)];
+                }
+            }
+            cl[a] = weno5z_interp(ch[0], ch[1], ch[2], ch[3], ch[4]);
+            cr[a] = weno5z_interp(ch[5], ch[4], ch[3], ch[2], ch[1]);
+        }
+        // back-projection (columns of R in the reference's order)
+        const double r0 = avg[0] / rh, r1 = avg[1] / rh;
+        const double ru2 = -1.0 * c / rh, ru5 = 1.0 * c / rh;
+        const double r6 = -kk / rh;
+        double wl[NF], wr[NF];
+        wl[0] = (cl[0] + r0 * cl[2]) + r0 * cl[5];
+        wr[0] = (cr[0] + r0 * cr[2]) + r0 * cr[5];
+        wl[1] = (cl[1] + r1 * cl[2]) + r1 * cl[5];
+        wr[1] = (cr[1] + r1 * cr[2]) + r1 * cr[5];
+        wl[UN] = ru2 * cl[2] + ru5 * cl[5];
+        wr[UN] = ru2 * cr[2] + ru5 * cr[5];
+        wl[T1] = cl[3];
+        wr[T1] = cr[3];
+        wl[T2] = cl[4];
+        wr[T2] = cr[4];
+        wl[F_IP] = c2 * cl[2] + c2 * cl[5];
+        wr[F_IP] = c2 * cr[2] + c2 * cr[5];
+        wl[F_IA] = (r6 * cl[2] + r6 * cl[5]) + cl[6];
+        wr[F_IA] = (r6 * cr[2] + r6 * cr[5]) + cr[6];
+        fb = false;
+        if (!s.admissible(wl) || !s.admissible(wr)) {
+            fb = true;
+#pragma unroll
+            for (int k = 0; k < NF; k++) {
+                wl[k] = W[at<STRW>(j, k, l)];
+                wr[k] = W[at<STRW>(j + 1, k, l)];
+            }
+        }
+        return s.riemann(wl, wr, UN, f);
+    }
+
+    // KEEP-PE two-point flux with cached ρe (multiphase.rs:291-309)
+    __device__ static __forceinline__ void split_flux(const double* __restrict__ W, int ra, int rb, int l, double* f) {
+        double a[NF + 1], b[NF + 1];
+#pragma unroll
+        for (int k = 0; k <= NF; k++) {
+            a[k] = W[at<STRW>(ra, k, l)];
+            b[k] = W[at<STRW>(rb, k, l)];
+        }
+        const double u = 0.5 * (a[UN] + b[UN]);
+        const double rh = 0.5 * (Five::rho(a) + Five::rho(b));
+        const double c = rh * u;
+        f[0] = 0.5 * (a[0] + b[0]) * u;
+        f[1] = 0.5 * (a[1] + b[1]) * u;
+        f[2] = c * 0.5 * (a[2] + b[2]);
+        f[3] = c * 0.5 * (a[3] + b[3]);
+        f[4] = c * 0.5 * (a[4] + b[4]);
+        f[UN] = f[UN] + 0.5 * (a[F_IP] + b[F_IP]);
+        const double kin = c * 0.5 * (a[2] * b[2] + a[3] * b[3] + a[4] * b[4]);
+        const double rhoe = 0.5 * (a[NF] + b[NF]);
+        const double pw = 0.5 * (a[UN] * b[F_IP] + b[UN] * a[F_IP]);
+        f[5] = kin + u * rhoe + pw;
+        f[6] = 0.5 * (a[F_IA] + b[F_IA]) * u;
+    }
+
+    // one-sided admissibility of the limiter (scheme.rs:408-416)
+    __device__ static __forceinline__ bool lim_ok(const Five& s, const double* fx, const double* ul, const double* fl,
+                                                  const double* ur, const double* fr, double lam2) {
+        double a[NF], w[NF];
+#pragma unroll
+        for (int k = 0; k < NF; k++) a[k] = ul[k] - lam2 * (fx[k] - fl[k]);
+        s.to_prim(a, w);
+        if (!s.admissible(w)) return false;
+#pragma unroll
+        for (int k = 0; k < NF; k++) a[k] = ur[k] + lam2 * (fx[k] - fr[k]);
+        s.to_prim(a, w);
+        return s.admissible(w);
+    }
+
+    __device__ static __forceinline__ double d4(double q0, double q1, double q2, double q3, double q4) {
+        return fabs(q0 - 4.0 * q1 + 6.0 * q2 - 4.0 * q3 + q4);
+    }
+
+    __device__ static void run(const FiveSweepParams& p) {
+        extern __shared__ __align__(16) unsigned char smem_raw[];
+        unsigned char* sp = smem_raw;
+        double* W = reinterpret_cast<double*>(sp);
+        sp += (size_t)RS * STRW * sizeof(double);
+        double* MF = nullptr;
+        if constexpr (MID) {
+            MF = reinterpret_cast<double*>(sp);
+            sp += (size_t)RS * STR * sizeof(double);
+        }
+        double* F = reinterpret_cast<double*>(sp);
+        sp += (size_t)RS * STR * sizeof(double);
+        double* TH = reinterpret_cast<double*>(sp);
+
+        __shared__ unsigned int s_fallback, s_limited, s_weno;
+        __shared__ int64_t s_loff[P];
+        __shared__ int s_lok[P];
+        if (p.ctl->done) return;
+        const double dt = p.ctl->dt;
+        const int tid = threadIdx.x;
+        if (tid == 0) {
+            s_fallback = 0;
+            s_limited = 0;
+            s_weno = 0;
+        }
+        const int lane0 = blockIdx.x * P;
+        const int s0 = blockIdx.y * p.seg;
+        const int Ls = min(p.seg, p.nd - s0);
+        const int ob = blockIdx.z;
+        if (tid < P) {
+            const int la = lane0 + tid;
+            s_lok[tid] = la < p.nl && ob < p.no;
+            s_loff[tid] = (int64_t)(p.gl + la) * p.sl + (int64_t)(p.go + ob) * p.so;
+        }
+        const int64_t base0 = (int64_t)(p.gd + s0 - 5) * p.sd;
+        const bool tail = s0 + Ls == p.nd;
+        const Five sys = Five::from(p.sys);
+        const double lam = (p.ndim * dt) / p.dx;
+        const double lam2 = 2.0 * lam;
+        const bool lim_on = p.positivity && lam > 0.0;
+        const double inv = 1.0 / p.dx;
+        __syncthreads();
+        const int nrounds = (Ls + 5 + RM - 1) / RM;
+        const int nrows = Ls + 10;
+
+        for (int r = 0; r < nrounds; r++) {
+            // ---- A: rows [lo, hi) → primitives (ρe, sensors)
+            {
+                const int lo = r == 0 ? 0 : RM * r + AHEAD;
+                const int hi = min(RM * r + RM + AHEAD, nrows);
+                const int cnt = (hi - lo) * P;
+                for (int idx = tid; idx < cnt; idx += T) {
+                    int rr, l;
+                    if (p.rows_contig) {
+                        rr = idx % (hi - lo);
+                        l = idx / (hi - lo);
+                    } else {
+                        rr = idx / P;
+                        l = idx % P;
+                    }
+                    const int row = lo + rr;
+                    const int64_t g = base0 + (int64_t)row * p.sd + s_loff[l];
+                    if (s_lok[l] && in_bounds(p.ctl, g, p.ncell)) {
+                        double u[NF], w[NF];
+#pragma unroll
+                        for (int k = 0; k < NF; k++) u[k] = __ldg(p.uin + k * p.ncell + g);
+                        sys.to_prim(u, w);
+#pragma unroll
+                        for (int k = 0; k < NF; k++) W[at<STRW>(row, k, l)] = w[k];
+                        if constexpr (MODE != MODE_WENO) W[at<STRW>(row, NF, l)] = sys.rho_e(w);
+                        if constexpr (MODE == MODE_HYBRID) {
+                            // sensor values (multiphase.rs:379-384)
+                            W[at<STRW>(row, NF + 1, l)] = log(fmax(Five::rho(w), 1e-300));
+                            W[at<STRW>(row, NF + 2, l)] = log(fmax(w[F_IP] + sys.p_inf_mix(w), 1e-300));
+                            W[at<STRW>(row, NF + 3, l)] = w[F_IA];
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            if constexpr (MODE == MODE_HYBRID) {
+                // ---- Θ: faces [RM r, RM r + RM) (scheme.rs:171-182)
+                const int f = RM * r + tid / P;
+                const int l = tid % P;
+                if (s_lok[l] && f <= Ls) {
+                    const int i = f + 4;
+                    double rr = 0.0;
+#pragma unroll
+                    for (int k = NF + 1; k < NF + 4; k++) {
+                        const double q0 = W[at<STRW>(i - 2, k, l)], q1 = W[at<STRW>(i - 1, k, l)],
+                                     q2 = W[at<STRW>(i, k, l)], q3 = W[at<STRW>(i + 1, k, l)],
+                                     q4 = W[at<STRW>(i + 2, k, l)], q5 = W[at<STRW>(i + 3, k, l)];
+                        rr = fmax(fmax(rr, d4(q0, q1, q2, q3, q4)), d4(q1, q2, q3, q4, q5));
+                    }
+                    double x = (rr / p.tol - 0.5) / 0.5;
+                    if (x < 0.0) x = 0.0;
+                    if (x > 1.0) x = 1.0;
+                    TH[slot(f) * P + l] = isfinite(rr) ? x * x * (3.0 - 2.0 * x) : 1.0;
+                }
+                __syncthreads();
+            }
+            if constexpr (MID) {
+                // ---- B: midpoints [RM r, RM r + RM)
+                const int m = RM * r + tid / P;
+                const int l = tid % P;
+                if (s_lok[l] && m < Ls + 5) {
+                    bool need = true;
+                    if constexpr (MODE == MODE_HYBRID) {
+                        need = false;
+                        for (int ff = max(m - 4, 0); ff <= min(m, Ls); ff++) need = need || TH[slot(ff) * P + l] > 0.0;
+                    }
+                    if (need) {
+                        double f[NF];
+                        bool fb;
+                        const double us = midpoint(sys, W, m, l, f, fb);
+#pragma unroll
+                        for (int k = 0; k < NF; k++) MF[at<STR>(m, k, l)] = f[k];
+                        MF[at<STR>(m, NF, l)] = us;
+                        if (fb && (m < Ls || tail)) atomicAdd(&s_fallback, 1u);
+                    }
+                }
+                __syncthreads();
+            }
+            // ---- C: faces [RM r − 4, RM r + RM − 4)
+            {
+                const int fidx = RM * r - 4 + tid / P;
+                const int l = tid % P;
+                if (s_lok[l] && fidx >= 0 && fidx <= Ls) {
+                    const int i = fidx + 4;
+                    double theta = MODE == MODE_WENO ? 1.0 : 0.0;
+                    if constexpr (MODE == MODE_HYBRID) theta = TH[slot(fidx) * P + l];
+                    double fh[NF], cen[NF], uf = 0.0, ufc = 0.0;
+                    if constexpr (MODE != MODE_WENO) {
+                        if (theta < 1.0) {
+                            // scheme.rs:188-222 (lags 1..3, pairs in order)
+                            constexpr double A6[3] = {0.75, -0.15, 1.0 / 60.0};
+#pragma unroll
+                            for (int k = 0; k < NF; k++) cen[k] = 0.0;
+#pragma unroll
+                            for (int li = 0; li < 3; li++) {
+                                const int lag = li + 1;
+#pragma unroll
+                                for (int mm = 0; mm < lag; mm++) {
+                                    double ft[NF];
+                                    split_flux(W, i - mm, i - mm + lag, l, ft);
+#pragma unroll
+                                    for (int k = 0; k < NF; k++) cen[k] = cen[k] + 2.0 * A6[li] * ft[k];
+                                    ufc = ufc + A6[li] * (W[at<STRW>(i - mm, UN, l)] + W[at<STRW>(i - mm + lag, UN, l)]);
+                                }
+                            }
+                        }
+                    }
+                    if (theta == 0.0) {
+#pragma unroll
+                        for (int k = 0; k < NF; k++) fh[k] = cen[k];
+                        uf = ufc;
+                    } else {
+                        if constexpr (MID) {
+                            if constexpr (MODE == MODE_HYBRID) {
+                                if (fidx < Ls || tail) atomicAdd(&s_weno, 1u);
+                            }
+                            // F̃ = Σ_s S6[s] (F̂_{+s} + F̂_{−s}) and the same for Ũ (scheme.rs:226-250)
+#pragma unroll
+                            for (int k = 0; k <= NF; k++) {
+                                double acc = 0.0;
+                                acc = acc + s6(0) * MF[at<STR>(fidx + 2, k, l)];
+                                acc = acc + s6(1) * MF[at<STR>(fidx + 3, k, l)];
+                                acc = acc + s6(1) * MF[at<STR>(fidx + 1, k, l)];
+                                acc = acc + s6(2) * MF[at<STR>(fidx + 4, k, l)];
+                                acc = acc + s6(2) * MF[at<STR>(fidx, k, l)];
+                                if (k < NF)
+                                    fh[k] = acc;
+                                else
+                                    uf = acc;
+                            }
+                            if (theta < 1.0) {  // scheme.rs:270-276
+#pragma unroll
+                                for (int k = 0; k < NF; k++) fh[k] = theta * fh[k] + (1.0 - theta) * cen[k];
+                                uf = theta * uf + (1.0 - theta) * ufc;
+                            }
+                        }
+                    }
+                    if (lim_on) {
+                        // Hu–Adams–Shu limiter (scheme.rs:395-464) between rows i and i+1
+                        double wi[NF], wj[NF], ul[NF], ur[NF], flp[NF], frp[NF];
+#pragma unroll
+                        for (int k = 0; k < NF; k++) {
+                            wi[k] = W[at<STRW>(i, k, l)];
+                            wj[k] = W[at<STRW>(i + 1, k, l)];
+                        }
+                        sys.to_cons(wi, ul);
+                        sys.to_cons(wj, ur);
+                        Five::flux_wq(wi, ul, UN, flp);
+                        Five::flux_wq(wj, ur, UN, frp);
+                        bool finite = true;
+#pragma unroll
+                        for (int k = 0; k < NF; k++) finite = finite && isfinite(fh[k]);
+                        if (!(finite && lim_ok(sys, fh, ul, flp, ur, frp, lam2))) {
+                            const double alpha = fmax(fabs(wi[UN]) + sys.sound_speed(wi), fabs(wj[UN]) + sys.sound_speed(wj));
+                            double flf[NF], bl[NF];
+#pragma unroll
+                            for (int k = 0; k < NF; k++) flf[k] = 0.5 * (flp[k] + frp[k]) - 0.5 * alpha * (ur[k] - ul[k]);
+                            double lo = 0.0, hi = 1.0;
+                            for (int it = 0; it < 30; it++) {
+                                const double mid = 0.5 * (lo + hi);
+#pragma unroll
+                                for (int k = 0; k < NF; k++) bl[k] = isfinite(fh[k]) ? mid * fh[k] + (1.0 - mid) * flf[k] : flf[k];
+                                if (lim_ok(sys, bl, ul, flp, ur, frp, lam2))
+                                    lo = mid;
+                                else
+                                    hi = mid;
+                            }
+#pragma unroll
+                            for (int k = 0; k < NF; k++) fh[k] = isfinite(fh[k]) ? lo * fh[k] + (1.0 - lo) * flf[k] : flf[k];
+                            const double um = 0.5 * (wi[UN] + wj[UN]);
+                            uf = isfinite(uf) ? lo * uf + (1.0 - lo) * um : um;
+                            if (fidx < Ls || tail) atomicAdd(&s_limited, 1u);
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < NF; k++) F[at<STR>(fidx, k, l)] = fh[k];
+                    F[at<STR>(fidx, NF, l)] = uf;
+                }
+            }
+            __syncthreads();
+            // ---- D: cells [RM r − 5, RM r + RM − 5)
+            {
+                int c, l;
+                if (p.rows_contig) {
+                    c = RM * r - 5 + tid % RM;
+                    l = tid / RM;
+                } else {
+                    c = RM * r - 5 + tid / P;
+                    l = tid % P;
+                }
+                const int64_t g = base0 + (int64_t)(c + 5) * p.sd + s_loff[l];
+                if (s_lok[l] && c >= 0 && c < Ls && in_bounds(p.ctl, g, p.ncell)) {
+                    double res[NF];
+#pragma unroll
+                    for (int k = 0; k < NF; k++) {
+                        const double x = (F[at<STR>(c + 1, k, l)] - F[at<STR>(c, k, l)]) * inv;
+                        const double prev = p.first ? 0.0 : p.rhs[k * p.ncell + g];
+                        res[k] = prev - x;
+                    }
+                    {
+                        // (α + K)(Ũ⁺ − Ũ⁻)/dx of the α equation (solver.rs:440-442)
+                        double wc[NF];
+#pragma unroll
+                        for (int k = 0; k < NF; k++) wc[k] = W[at<STRW>(c + 5, k, l)];
+                        res[F_IA] = res[F_IA] + sys.nc_coef(wc) * (F[at<STR>(c + 1, NF, l)] - F[at<STR>(c, NF, l)]) * inv;
+                    }
+                    if (!p.last) {
+#pragma unroll
+                        for (int k = 0; k < NF; k++) p.rhs[k * p.ncell + g] = res[k];
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < NF; k++) {
+                            const double o = p.base[k * p.ncell + g];
+                            double v;
+                            if (p.stage == 1)
+                                v = o + dt * res[k];
+                            else if (p.stage == 2)
+                                v = 0.75 * o + 0.25 * (p.cur[k * p.ncell + g] + dt * res[k]);
+                            else
+                                v = p.cur[k * p.ncell + g] / 3.0 + (2.0 / 3.0) * (o + dt * res[k]);
+                            p.dest[k * p.ncell + g] = v;
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            if (s_weno) atomicAdd(&p.ctl->counters[1], (unsigned long long)s_weno);
+            if (s_fallback) atomicAdd(&p.ctl->counters[2], (unsigned long long)s_fallback);
+            if (s_limited) atomicAdd(&p.ctl->counters[3], (unsigned long long)s_limited);
+        }
+    }
+};
+
+}  // namespace emg

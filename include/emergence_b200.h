@@ -240,6 +240,62 @@ int emg_uniform_features(emg_uniform* h, uint32_t* flags);
 int emg_uniform_step_noalloc(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
                              const double* u_in, double* u_out, double dt, void* stream);
 
+/* ------------------------------------------------------------------ five-equation system */
+/* Two-phase flow with Kapila's five-equation model (C/multiphase.rs:1-392):
+ * conserved variables (α1ρ1, α2ρ2, ρu, ρv, ρw, E, α1), primitive (α1ρ1, α2ρ2,
+ * u, v, w, p, α1), one NASG equation of state per phase (`cv` unused).
+ * `kapila` = 1 keeps the K∇·u term of the α1 equation (Wood's mixture sound
+ * speed), 0 drops it (FiveEq::kapila, C/multiphase.rs:27-31). */
+typedef struct emg_five_system {
+    emg_eos eos[2];
+    int32_t kapila;
+    int32_t reserved;
+} emg_five_system;
+
+/* Boundary condition of a 7-variable system: as emg_bc with a conserved
+ * Dirichlet / far-field state of 7 values. */
+typedef struct emg_bc7 {
+    int32_t kind;
+    int32_t reserved;
+    double state[7];
+} emg_bc7;
+
+typedef struct emg_five emg_five;
+
+/* Upload a ghost-padded AoS state double[len][7] (the padded layout of
+ * emg_uniform_create) and build a device solver of the five-equation system
+ * on the current device: GpuSolver::from_cpu(&Solver<7, FiveEq>,
+ * GpuSystem::FiveEq{..}) (G/lib.rs:184-282). Plain FP64 form (opts->precision
+ * must be EMG_PRECISION_F64); every flux mode; boundaries periodic, outflow,
+ * reflect (axes with n >= ng), Dirichlet and characteristic. */
+int emg_five_create(const emg_mesh* mesh, const emg_five_system* sys, const emg_bc7 bc[6], const emg_opts* opts,
+                    const double* u_aos, size_t len, emg_five** out);
+int emg_five_destroy(emg_five* h);
+
+/* One SSP-RK3 step of size dt (C/solver.rs:659-738; G/lib.rs:391-401). */
+int emg_five_step(emg_five* h, double dt);
+
+/* CFL step: min(cfl / max Σ_d (|u_d|+c)/dx_d, 0.5 / max dilatation rate)
+ * over interior cells (C/solver.rs:478-523, C/multiphase.rs:363-377). */
+int emg_five_dt_cfl(emg_five* h, double* dt);
+
+/* Advance to t_end with CFL steps (C/solver.rs:758-768). */
+int emg_five_run_to(emg_five* h, double t_end, uint64_t* steps);
+
+/* The padded AoS state double[len][7], ghosts included (G/lib.rs:450-455). */
+int emg_five_download(emg_five* h, double* u_aos, size_t len);
+
+/* [faces, shock-path faces, first-order fallbacks, positivity-limited faces]. */
+int emg_five_counters(emg_five* h, uint64_t out[4]);
+
+/* Σ u·vol over interior cells (C/solver.rs:784-794), 7 values. */
+int emg_five_totals(emg_five* h, double out[7]);
+
+int emg_five_get_time(emg_five* h, double* t);
+
+/* Kernel launches issued by the handle since creation. */
+int emg_five_launch_count(emg_five* h, uint64_t* launches);
+
 /* ------------------------------------------------------------------ batched 1-D lines */
 /* Many independent 1-D problems advanced together: every RK stage is one
  * fused-sweep launch over all instances, each instance with its own cell size

@@ -7,6 +7,7 @@
 #include "oracle.hpp"
 #include "amr_oracle.hpp"
 #include "dual.hpp"
+#include "five_oracle.hpp"
 #include "../include/emergence_b200.h"
 
 #include <cstdio>
@@ -522,6 +523,121 @@ int emgo_dual_step_cons(const emg_mesh* mesh, const emg_eos* eos, const emg_bc b
             u_out[5 * c + k] = s.u[c][k].v;
             du_out[5 * c + k] = s.u[c][k].d;
         }
+    return EMG_OK;
+}
+}  // extern "C"
+
+// ---------------------------------------------------------------- five-equation system
+// (five_oracle.hpp: multiphase.rs and the system-generic step it runs)
+namespace {
+struct FiveHandle {
+    SolverFive<double> s;
+    FiveHandle(const FiveEq<double>& sys, const Mesh& m) : s(sys, m) {}
+};
+}  // namespace
+
+extern "C" {
+int emgo_five_create(const emg_mesh* mesh, const emg_five_system* sys, const emg_bc7 bc[6], const emg_opts* opts,
+                     const double* u_aos, size_t len, void** out) {
+    if (!mesh || !sys || !bc || !opts || !u_aos || !out) return fail(EMG_ERR_INVALID, "null argument");
+    Mesh m = to_mesh(mesh);
+    if ((size_t)m.len() != len) return fail(EMG_ERR_INVALID, "state length does not match the padded mesh");
+    FiveEq<double> f;
+    for (int k = 0; k < 2; k++)
+        f.eos[k] = Nasg<double>{sys->eos[k].gamma, sys->eos[k].p_inf, sys->eos[k].b, sys->eos[k].q, sys->eos[k].cv};
+    f.kapila = sys->kapila != 0;
+    FiveHandle* h = new FiveHandle(f, m);
+    for (int d = 0; d < 3; d++)
+        for (int q = 0; q < 2; q++) {
+            h->s.bc[d][q].kind = bc[2 * d + q].kind;
+            for (int k = 0; k < 7; k++) h->s.bc[d][q].state[k] = bc[2 * d + q].state[k];
+        }
+    h->s.cfl = opts->cfl;
+    h->s.tol = opts->tol;
+    h->s.mode = opts->mode;
+    h->s.positivity = opts->positivity != 0;
+    std::memcpy(h->s.u.data(), u_aos, len * 7 * sizeof(double));
+    *out = h;
+    return EMG_OK;
+}
+int emgo_five_destroy(void* h) {
+    delete (FiveHandle*)h;
+    return EMG_OK;
+}
+int emgo_five_step(void* h, double dt) {
+    ((FiveHandle*)h)->s.step(dt);
+    return EMG_OK;
+}
+int emgo_five_dt_cfl(void* h, double* dt) {
+    *dt = ((FiveHandle*)h)->s.dt_cfl();
+    return EMG_OK;
+}
+// solver.rs:758-768
+int emgo_five_run_to(void* h, double t_end, uint64_t* steps) {
+    SolverFive<double>& s = ((FiveHandle*)h)->s;
+    uint64_t n = 0;
+    while (s.t < t_end - 1e-10 * std::fabs(t_end)) {
+        double dt = std::fmin(s.dt_cfl(), t_end - s.t);
+        if (!(std::isfinite(dt) && dt > 1e-12 * std::fmax(std::fabs(t_end), 1e-300)))
+            return fail(EMG_ERR_DT_COLLAPSED, "time step collapsed");
+        s.step(dt);
+        n++;
+    }
+    if (steps) *steps = n;
+    return EMG_OK;
+}
+int emgo_five_download(void* h, double* u_aos, size_t len) {
+    FiveHandle* hh = (FiveHandle*)h;
+    if (len != hh->s.u.size()) return fail(EMG_ERR_INVALID, "length mismatch");
+    std::memcpy(u_aos, hh->s.u.data(), len * 7 * sizeof(double));
+    return EMG_OK;
+}
+int emgo_five_fill_ghosts(void* h) {
+    FiveHandle* hh = (FiveHandle*)h;
+    hh->s.fill_ghosts(hh->s.u);
+    return EMG_OK;
+}
+int emgo_five_totals(void* h, double out[7]) {
+    V7<double> t = ((FiveHandle*)h)->s.totals();
+    for (int k = 0; k < 7; k++) out[k] = t[k];
+    return EMG_OK;
+}
+int emgo_five_counters(void* h, uint64_t out[4]) {
+    Stats& s = ((FiveHandle*)h)->s.stats;
+    out[0] = s.faces;
+    out[1] = s.weno_faces;
+    out[2] = s.fallback_faces;
+    out[3] = s.limited_faces;
+    return EMG_OK;
+}
+int emgo_five_get_time(void* h, double* t) {
+    *t = ((FiveHandle*)h)->s.t;
+    return EMG_OK;
+}
+// system-level pieces for the known-answer tests: primitive → conserved,
+// conserved → primitive, sound speed, dilatation rate, admissibility
+int emgo_five_to_cons(const emg_five_system* sys, const double* w, double* u) {
+    FiveEq<double> f;
+    for (int k = 0; k < 2; k++)
+        f.eos[k] = Nasg<double>{sys->eos[k].gamma, sys->eos[k].p_inf, sys->eos[k].b, sys->eos[k].q, sys->eos[k].cv};
+    f.kapila = sys->kapila != 0;
+    V7<double> ww;
+    for (int k = 0; k < 7; k++) ww[k] = w[k];
+    V7<double> uu = f.to_cons(ww);
+    for (int k = 0; k < 7; k++) u[k] = uu[k];
+    return EMG_OK;
+}
+int emgo_five_props(const emg_five_system* sys, const double* w, double divu, double out[4]) {
+    FiveEq<double> f;
+    for (int k = 0; k < 2; k++)
+        f.eos[k] = Nasg<double>{sys->eos[k].gamma, sys->eos[k].p_inf, sys->eos[k].b, sys->eos[k].q, sys->eos[k].cv};
+    f.kapila = sys->kapila != 0;
+    V7<double> ww;
+    for (int k = 0; k < 7; k++) ww[k] = w[k];
+    out[0] = f.sound_speed(ww);
+    out[1] = f.dilatation_rate(ww, divu);
+    out[2] = f.admissible(ww) ? 1.0 : 0.0;
+    out[3] = f.kapila_k(ww);
     return EMG_OK;
 }
 }  // extern "C"

@@ -15,7 +15,7 @@ import subprocess
 
 import numpy as np
 
-from emergence_b200._abi import EmgBc, EmgEos, EmgMesh, EmgOpts
+from emergence_b200._abi import EmgBc, EmgBc7, EmgEos, EmgFiveSystem, EmgMesh, EmgOpts
 from emergence_b200.physics import Bc, FluxMode
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -60,6 +60,19 @@ SIGS = {
     "emgo_dual_run": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc), C.POINTER(EmgOpts), _D, _D,
                                 C.c_size_t, C.c_double, _D, C.c_size_t, C.c_int, _D, _D, _D, _D, _D, _D]),
     "emgo_box_objective": (C.c_int, [_P, C.c_int, _D, _D, _D]),
+    "emgo_five_create": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgFiveSystem), C.POINTER(EmgBc7),
+                                   C.POINTER(EmgOpts), _D, C.c_size_t, C.POINTER(_P)]),
+    "emgo_five_destroy": (C.c_int, [_P]),
+    "emgo_five_step": (C.c_int, [_P, C.c_double]),
+    "emgo_five_dt_cfl": (C.c_int, [_P, _D]),
+    "emgo_five_run_to": (C.c_int, [_P, C.c_double, _U64]),
+    "emgo_five_download": (C.c_int, [_P, _D, C.c_size_t]),
+    "emgo_five_fill_ghosts": (C.c_int, [_P]),
+    "emgo_five_totals": (C.c_int, [_P, _D]),
+    "emgo_five_counters": (C.c_int, [_P, _U64]),
+    "emgo_five_get_time": (C.c_int, [_P, _D]),
+    "emgo_five_to_cons": (C.c_int, [C.POINTER(EmgFiveSystem), _D, _D]),
+    "emgo_five_props": (C.c_int, [C.POINTER(EmgFiveSystem), _D, C.c_double, _D]),
     "emgo_dual_step_cons": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc), C.POINTER(EmgOpts), _D,
                                       _D, C.c_size_t, C.c_double, C.c_double, _D, _D]),
 }
@@ -507,3 +520,80 @@ class OracleAmr:
         v = C.c_uint64()
         _chk(_amr_lib().emgo_amr_steps(self._h, C.byref(v)))
         return v.value
+
+
+class FiveOracleSolver:
+    """C++ restatement of ``compressible::Solver<7, FiveEq>`` (five_oracle.hpp),
+    with the constructor and methods of ``emergence_b200.GpuFiveSolver``."""
+
+    def __init__(self, sys, mesh, u, bc=None, cfl=0.5, mode=FluxMode.Weno, tol=1e-3, positivity=True):
+        from emergence_b200.five import _c_bcs7, _c_system
+        from emergence_b200.solver import _c_mesh
+        self.sys, self.mesh = sys, mesh
+        self.bc = bc if bc is not None else [[Bc.Periodic, Bc.Periodic] for _ in range(3)]
+        u = arr(u)
+        self._m = _c_mesh(mesh)
+        self._s = _c_system(sys)
+        self._b = _c_bcs7(self.bc)
+        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, 0, 0)
+        h = C.c_void_p()
+        _chk(lib().emgo_five_create(C.byref(self._m), C.byref(self._s), self._b, C.byref(self._o), dptr(u),
+                                    mesh.len(), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().emgo_five_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, dt):
+        _chk(lib().emgo_five_step(self._h, float(dt)))
+
+    def dt_cfl(self):
+        v = C.c_double()
+        _chk(lib().emgo_five_dt_cfl(self._h, C.byref(v)))
+        return v.value
+
+    def run_to(self, t_end):
+        n = C.c_uint64()
+        _chk(lib().emgo_five_run_to(self._h, float(t_end), C.byref(n)))
+        return n.value
+
+    def download(self):
+        out = np.empty((self.mesh.len(), 7))
+        _chk(lib().emgo_five_download(self._h, dptr(out), self.mesh.len()))
+        return out
+
+    def fill_ghosts(self):
+        _chk(lib().emgo_five_fill_ghosts(self._h))
+
+    def totals(self):
+        out = np.empty(7)
+        _chk(lib().emgo_five_totals(self._h, dptr(out)))
+        return out
+
+    def counters(self):
+        out = (C.c_uint64 * 4)()
+        _chk(lib().emgo_five_counters(self._h, out))
+        return list(out)
+
+    @property
+    def t(self):
+        v = C.c_double()
+        _chk(lib().emgo_five_get_time(self._h, C.byref(v)))
+        return v.value
+
+
+def five_props(sys, w, divu=0.0):
+    """(sound speed, dilatation rate, admissible, Kapila K) of one primitive state."""
+    from emergence_b200.five import _c_system
+    s = _c_system(sys)
+    out = np.empty(4)
+    _chk(lib().emgo_five_props(C.byref(s), dptr(arr(w)), float(divu), dptr(out)))
+    return out
