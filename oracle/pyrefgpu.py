@@ -18,7 +18,7 @@ import os
 
 import numpy as np
 
-from emergence_b200._abi import EmgBc, EmgEos, EmgMesh, EmgOpts
+from emergence_b200._abi import EmgBc, EmgBc7, EmgEos, EmgFiveSystem, EmgMesh, EmgOpts
 from emergence_b200.physics import Bc, FluxMode
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -30,6 +30,8 @@ SIGS = {
     "refgpu_last_error": (C.c_char_p, []),
     "refgpu_create": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc), C.POINTER(EmgOpts), _D,
                                 C.c_size_t, C.POINTER(_P)]),
+    "refgpu_five_create": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgFiveSystem), C.POINTER(EmgBc7),
+                                     C.POINTER(EmgOpts), _D, C.c_size_t, C.POINTER(_P)]),
     "refgpu_destroy": (C.c_int, [_P]),
     "refgpu_step": (C.c_int, [_P, C.c_double]),
     "refgpu_dt_cfl": (C.c_int, [_P, _D]),
@@ -113,8 +115,10 @@ class RefGpuSolver:
         _chk(lib().refgpu_advance(self._h, nsteps, C.byref(taken)))
         return taken.value
 
+    nv = 5
+
     def download(self):
-        out = np.empty((self.mesh.len(), 5))
+        out = np.empty((self.mesh.len(), self.nv))
         _chk(lib().refgpu_download(self._h, out.ctypes.data_as(_D), self.mesh.len()))
         return out
 
@@ -139,3 +143,27 @@ class RefGpuSolver:
             self.close()
         except Exception:
             pass
+
+
+class RefGpuFiveSolver(RefGpuSolver):
+    """The reference's GpuSolver<f64> for GpuSystem::FiveEq (its `five`
+    kernels, kernels.cu:116-256) on the current device."""
+
+    nv = 7
+
+    def __init__(self, sys, mesh, u, bc=None, cfl=0.5, mode=FluxMode.Weno, tol=1e-3, positivity=True):
+        from emergence_b200.five import _c_bcs7, _c_system
+        self.mesh = mesh
+        bc = bc if bc is not None else [[Bc.Periodic, Bc.Periodic] for _ in range(3)]
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        if u.shape != (mesh.len(), 7):
+            raise ValueError(f"state must have shape {(mesh.len(), 7)}, got {u.shape}")
+        from emergence_b200.solver import _c_mesh
+        m = _c_mesh(mesh)
+        o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, 0, 0)
+        s, b = _c_system(sys), _c_bcs7(bc)
+        self._args = (m, s, b, o)
+        h = _P()
+        _chk(lib().refgpu_five_create(C.byref(m), C.byref(s), b, C.byref(o), u.ctypes.data_as(_D), mesh.len(),
+                                      C.byref(h)))
+        self._h = h

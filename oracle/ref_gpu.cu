@@ -35,7 +35,7 @@ namespace {
 
 constexpr int BLOCK = 128;        // lib.rs:22
 constexpr int RATE_BLOCKS = 256;  // lib.rs:23
-constexpr int NV = 5;             // Euler
+constexpr int NV_MAX = 7;         // FiveEq (Euler: 5)
 
 thread_local std::string g_err;
 
@@ -57,6 +57,8 @@ struct refgpu {
     double t = 0.0;
     double e[8];
     int kap = 0;
+    int nv = 5;         // 5: Euler, 7: FiveEq (GpuSystem::nv, lib.rs:64-69)
+    bool five = false;
     int64_t m[3], g[3], len = 1, cells = 1;
     cudaStream_t stream = nullptr;
     double *u = nullptr, *u0 = nullptr, *w = nullptr, *rhs = nullptr, *f = nullptr, *uf = nullptr, *th = nullptr,
@@ -76,6 +78,14 @@ struct refgpu {
     } while (0)
 #define RG_LAUNCHED() RG_CUDA(cudaGetLastError())
 #define EOSV(h) h->e[0], h->e[1], h->e[2], h->e[3], h->e[4], h->e[5], h->e[6], h->e[7], h->kap
+// the entry point of the handle's system: NAME_euler_f64 or NAME_five_f64
+#define SYS_LAUNCH(h, NAME, GRID, BLK, ...)                                      \
+    do {                                                                        \
+        if ((h)->five)                                                          \
+            NAME##_five_f64<<<GRID, BLK, 0, (h)->stream>>>(__VA_ARGS__);        \
+        else                                                                    \
+            NAME##_euler_f64<<<GRID, BLK, 0, (h)->stream>>>(__VA_ARGS__);       \
+    } while (0)
 
 namespace {
 
@@ -85,15 +95,17 @@ int fill_ghosts(refgpu* h) {
         int e0 = (d + 1) % 3, e1 = (d + 2) % 3;
         if (e0 > e1) std::swap(e0, e1);
         const int64_t np = h->m[e0] * h->m[e1] * h->g[d];
-        ghost_euler_f64<<<grid_of(np), BLOCK, 0, h->stream>>>(EOSV(h), h->u, h->geo, d, h->bc[d][0], h->bc[d][1], 1 + d,
-                                                                 h->dir[d][0], h->dir[d][1]);
+        // momentum index of axis d (GpuSystem::mom, lib.rs:70-75)
+        const int mom = (h->five ? 2 : 1) + d;
+        SYS_LAUNCH(h, ghost, grid_of(np), BLOCK, EOSV(h), h->u, h->geo, d, h->bc[d][0], h->bc[d][1], mom, h->dir[d][0],
+                   h->dir[d][1]);
         RG_LAUNCHED();
     }
     return 0;
 }
 
 int prim(refgpu* h) {
-    prim_euler_f64<<<grid_of(h->len), BLOCK, 0, h->stream>>>(EOSV(h), h->u, h->w, h->geo, h->bl0);
+    SYS_LAUNCH(h, prim, grid_of(h->len), BLOCK, EOSV(h), h->u, h->w, h->geo, h->bl0);
     RG_LAUNCHED();
     return 0;
 }
@@ -112,18 +124,16 @@ int rhs(refgpu* h, double dt) {
         const int64_t cross = (int64_t)h->mesh.n[(d + 1) % 3] * h->mesh.n[(d + 2) % 3];
         const int64_t nf = (h->mesh.n[d] + 1) * cross;
         const int64_t nm = (h->mesh.n[d] + 5) * cross;
-        theta_euler_f64<<<grid_of(nf), BLOCK, 0, h->stream>>>(EOSV(h), h->w, h->geo, h->bl0, d, h->mode, h->tol, h->th);
+        SYS_LAUNCH(h, theta, grid_of(nf), BLOCK, EOSV(h), h->w, h->geo, h->bl0, d, h->mode, h->tol, h->th);
         RG_LAUNCHED();
         if (h->mode != EMG_MODE_CENTRAL) {
-            midflux_euler_f64<<<grid_of(nm), BLOCK, 0, h->stream>>>(EOSV(h), h->w, h->geo, h->bl0, d, h->th, h->mf, h->mu,
-                                                                      h->counters);
+            SYS_LAUNCH(h, midflux, grid_of(nm), BLOCK, EOSV(h), h->w, h->geo, h->bl0, d, h->th, h->mf, h->mu, h->counters);
             RG_LAUNCHED();
         }
-        flux_euler_f64<<<grid_of(nf), BLOCK, 0, h->stream>>>(EOSV(h), h->w, h->geo, h->bl0, d, lambda, h->th, h->mf, h->mu,
-                                                               h->f, h->uf, h->counters);
+        SYS_LAUNCH(h, flux, grid_of(nf), BLOCK, EOSV(h), h->w, h->geo, h->bl0, d, lambda, h->th, h->mf, h->mu, h->f, h->uf,
+                   h->counters);
         RG_LAUNCHED();
-        accum_euler_f64<<<grid_of(h->cells), BLOCK, 0, h->stream>>>(EOSV(h), h->w, h->geo, h->bl0, d, dx, h->f, h->uf,
-                                                                      h->rhs, first);
+        SYS_LAUNCH(h, accum, grid_of(h->cells), BLOCK, EOSV(h), h->w, h->geo, h->bl0, d, dx, h->f, h->uf, h->rhs, first);
         RG_LAUNCHED();
         first = 0;
     }
@@ -131,7 +141,7 @@ int rhs(refgpu* h, double dt) {
 }
 
 int rk(refgpu* h, double al, double be, double dt) {
-    rk_euler_f64<<<grid_of(h->cells), BLOCK, 0, h->stream>>>(h->u, h->u0, h->rhs, h->geo, h->bl0, al, be, dt);
+    SYS_LAUNCH(h, rk, grid_of(h->cells), BLOCK, h->u, h->u0, h->rhs, h->geo, h->bl0, al, be, dt);
     RG_LAUNCHED();
     return 0;
 }
@@ -158,13 +168,17 @@ int refgpu_destroy(refgpu* h) {
     return 0;
 }
 
-// GpuSolver::from_cpu (lib.rs:186-258) for the Euler system in f64: u_aos is
-// the ghost-padded AoS state of the CPU solver (len cells of 5 values).
-int refgpu_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
-                  const double* u_aos, size_t len, refgpu** out) {
-    if (!mesh || !eos || !bc || !opts || !u_aos || !out) return fail("null argument");
+// GpuSolver::from_cpu (lib.rs:186-258) in f64: u_aos is the ghost-padded AoS
+// state of the CPU solver (len cells of nv values); ev the EOS arguments of
+// GpuSystem::eos_args (lib.rs:76-81); bc kinds and their nv-value states.
+static int create_any(const emg_mesh* mesh, const double ev[8], int kap, int nv, const int kinds[6],
+                      const double* const states[6], const emg_opts* opts, const double* u_aos, size_t len,
+                      refgpu** out) {
     *out = nullptr;
     refgpu* h = new refgpu();
+    h->nv = nv;
+    h->five = nv == 7;
+    h->kap = kap;
     h->mesh = *mesh;
     for (int d = 0; d < 3; d++) {
         if (mesh->n[d] < 1) {
@@ -175,8 +189,8 @@ int refgpu_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], 
         h->m[d] = mesh->n[d] + 2 * h->g[d];
         h->len *= h->m[d];
         h->cells *= mesh->n[d];
-        h->bc[d][0] = bc[2 * d].kind;
-        h->bc[d][1] = bc[2 * d + 1].kind;
+        h->bc[d][0] = kinds[2 * d];
+        h->bc[d][1] = kinds[2 * d + 1];
     }
     if ((size_t)h->len != len) {
         delete h;
@@ -195,8 +209,7 @@ int refgpu_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], 
     h->geo.rtot = (long)h->cells;
     h->geo.nb = 1;
     h->geo.s0 = 0;
-    const double ev[8] = {eos->gamma, eos->p_inf, eos->b, eos->q, 1.4, 0.0, 0.0, 0.0};  // lib.rs:77-79
-    memcpy(h->e, ev, sizeof ev);
+    memcpy(h->e, ev, sizeof h->e);
     h->cfl = opts->cfl;
     h->tol = opts->tol;
     h->mode = opts->mode;
@@ -212,15 +225,15 @@ int refgpu_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], 
         maxf = std::max<int64_t>(maxf, (mesh->n[d] + 1) * cross);
         maxm = std::max<int64_t>(maxm, (mesh->n[d] + 5) * cross);
     }
-    const size_t sb = (size_t)NV * h->len * sizeof(double);
+    const size_t sb = (size_t)h->nv * h->len * sizeof(double);
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&h->u, sb) != cudaSuccess || cudaMalloc(&h->u0, sb) != cudaSuccess ||
         cudaMalloc(&h->w, sb) != cudaSuccess ||
-        cudaMalloc(&h->rhs, (size_t)NV * h->cells * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&h->f, (size_t)NV * maxf * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&h->rhs, (size_t)h->nv * h->cells * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&h->f, (size_t)h->nv * maxf * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&h->uf, (size_t)maxf * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&h->th, (size_t)maxf * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&h->mf, (size_t)NV * maxm * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&h->mf, (size_t)h->nv * maxm * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&h->mu, (size_t)maxm * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&h->counters, 4 * sizeof(unsigned long long)) != cudaSuccess ||
         cudaMalloc(&h->rates, 2 * RATE_BLOCKS * sizeof(double)) != cudaSuccess ||
@@ -230,22 +243,22 @@ int refgpu_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], 
     }
     for (int d = 0; d < 3; d++)
         for (int s = 0; s < 2; s++) {
-            double vals[NV] = {0, 0, 0, 0, 0};
-            const int k = bc[2 * d + s].kind;
+            double vals[NV_MAX] = {0, 0, 0, 0, 0, 0, 0};
+            const int k = kinds[2 * d + s];
             if (k == EMG_BC_DIRICHLET || k == EMG_BC_CHARACTERISTIC)
-                for (int q = 0; q < NV; q++) vals[q] = bc[2 * d + s].state[q];
-            if (cudaMalloc(&h->dir[d][s], sizeof vals) != cudaSuccess ||
-                cudaMemcpy(h->dir[d][s], vals, sizeof vals, cudaMemcpyHostToDevice) != cudaSuccess)
+                for (int q = 0; q < nv; q++) vals[q] = states[2 * d + s][q];
+            if (cudaMalloc(&h->dir[d][s], nv * sizeof(double)) != cudaSuccess ||
+                cudaMemcpy(h->dir[d][s], vals, nv * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
                 return bail(fail("boundary state upload failed"));
         }
     // SoA upload (lib.rs:204-213); the other arrays start at zero (alloc_zeros)
-    std::vector<double> soa((size_t)NV * h->len);
+    std::vector<double> soa((size_t)h->nv * h->len);
     for (int64_t c = 0; c < h->len; c++)
-        for (int q = 0; q < NV; q++) soa[(size_t)q * h->len + c] = u_aos[(size_t)NV * c + q];
+        for (int q = 0; q < nv; q++) soa[(size_t)q * h->len + c] = u_aos[(size_t)nv * c + q];
     const int zero = 0;
     if (cudaMemcpy(h->u, soa.data(), sb, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(h->u0, 0, sb) != cudaSuccess || cudaMemset(h->w, 0, sb) != cudaSuccess ||
-        cudaMemset(h->rhs, 0, (size_t)NV * h->cells * sizeof(double)) != cudaSuccess ||
+        cudaMemset(h->rhs, 0, (size_t)h->nv * h->cells * sizeof(double)) != cudaSuccess ||
         cudaMemset(h->counters, 0, 4 * sizeof(unsigned long long)) != cudaSuccess ||
         cudaMemcpy(h->bl0, &zero, sizeof zero, cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(fail("state upload failed"));
@@ -254,10 +267,39 @@ int refgpu_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], 
     return 0;
 }
 
+// Euler system (GpuSystem::Euler): eos_args = [γ, p∞, b, q, 1.4, 0, 0, 0], kapila 0
+int refgpu_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
+                  const double* u_aos, size_t len, refgpu** out) {
+    if (!mesh || !eos || !bc || !opts || !u_aos || !out) return fail("null argument");
+    const double ev[8] = {eos->gamma, eos->p_inf, eos->b, eos->q, 1.4, 0.0, 0.0, 0.0};  // lib.rs:77-79
+    int kinds[6];
+    const double* states[6];
+    for (int i = 0; i < 6; i++) {
+        kinds[i] = bc[i].kind;
+        states[i] = bc[i].state;
+    }
+    return create_any(mesh, ev, 0, 5, kinds, states, opts, u_aos, len, out);
+}
+
+// Five-equation system (GpuSystem::FiveEq): eos_args = both phases' [γ, p∞, b, q], kapila
+int refgpu_five_create(const emg_mesh* mesh, const emg_five_system* sys, const emg_bc7 bc[6], const emg_opts* opts,
+                       const double* u_aos, size_t len, refgpu** out) {
+    if (!mesh || !sys || !bc || !opts || !u_aos || !out) return fail("null argument");
+    const double ev[8] = {sys->eos[0].gamma, sys->eos[0].p_inf, sys->eos[0].b, sys->eos[0].q,
+                          sys->eos[1].gamma, sys->eos[1].p_inf, sys->eos[1].b, sys->eos[1].q};  // lib.rs:80
+    int kinds[6];
+    const double* states[6];
+    for (int i = 0; i < 6; i++) {
+        kinds[i] = bc[i].kind;
+        states[i] = bc[i].state;
+    }
+    return create_any(mesh, ev, sys->kapila ? 1 : 0, 7, kinds, states, opts, u_aos, len, out);
+}
+
 // GpuSolver::step (lib.rs:391-401)
 int refgpu_step(refgpu* h, double dt) {
     if (!h) return fail("null handle");
-    RG_CUDA(cudaMemcpyAsync(h->u0, h->u, (size_t)NV * h->len * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    RG_CUDA(cudaMemcpyAsync(h->u0, h->u, (size_t)h->nv * h->len * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
     int rc;
     if ((rc = rhs(h, dt)) || (rc = rk(h, 0.0, 1.0, dt))) return rc;
     if ((rc = rhs(h, dt)) || (rc = rk(h, 0.75, 0.25, dt))) return rc;
@@ -272,8 +314,8 @@ int refgpu_dt_cfl(refgpu* h, double* dt) {
     int rc = fill_ghosts(h);
     if (rc) return rc;
     if ((rc = prim(h))) return rc;
-    rate_euler_f64<<<RATE_BLOCKS, 256, 0, h->stream>>>(EOSV(h), h->w, h->geo, h->bl0, h->mesh.dx[0], h->mesh.dx[1],
-                                                        h->mesh.dx[2], h->rates);
+    SYS_LAUNCH(h, rate, RATE_BLOCKS, 256, EOSV(h), h->w, h->geo, h->bl0, h->mesh.dx[0], h->mesh.dx[1], h->mesh.dx[2],
+               h->rates);
     RG_LAUNCHED();
     RG_CUDA(cudaMemcpyAsync(h->host_rates.data(), h->rates, 2 * RATE_BLOCKS * sizeof(double), cudaMemcpyDeviceToHost,
                             h->stream));
@@ -311,11 +353,11 @@ int refgpu_advance(refgpu* h, uint64_t nsteps, uint64_t* taken) {
 // GpuSolver::download (lib.rs:450-455): ghost-padded AoS
 int refgpu_download(refgpu* h, double* u_aos, size_t len) {
     if (!h || !u_aos || len != (size_t)h->len) return fail("state length does not match the padded mesh");
-    std::vector<double> soa((size_t)NV * h->len);
+    std::vector<double> soa((size_t)h->nv * h->len);
     RG_CUDA(cudaMemcpyAsync(soa.data(), h->u, soa.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     RG_CUDA(cudaStreamSynchronize(h->stream));
     for (int64_t c = 0; c < h->len; c++)
-        for (int q = 0; q < NV; q++) u_aos[(size_t)NV * c + q] = soa[(size_t)q * h->len + c];
+        for (int q = 0; q < h->nv; q++) u_aos[(size_t)h->nv * c + q] = soa[(size_t)q * h->len + c];
     return 0;
 }
 
