@@ -392,7 +392,72 @@ def sub_records(args, world, rank, local):
     rec["note"] = ("value = backward/forward cost; the mixed batch records its FP32-flux run and applies the FP64 "
                    "step's transposed Jacobian at its stage states")
     out["batch_adjoint"] = rec
+    out["five"] = measure_five(args, world, rank, local)
     return out
+
+
+def measure_five(args, world, rank, local, n=128, steps=10, warmup=3):
+    """Five-equation two-phase shock–bubble (Kapila's model) on n^3 cells: this
+    library's fused sweeps and, on the same box and grid, the reference's own
+    `five` GPU kernels (the same-box baseline); each advances warmup + steps
+    CFL steps with a device→host time step per step, timed with CUDA events on
+    its stream."""
+    import numpy as np
+    import torch
+    from emergence_b200 import GpuFiveSolver, workloads as W
+    from emergence_b200.physics import FluxMode
+    torch.cuda.set_device(local)
+    dev = torch.cuda.current_device()
+    sys_, mesh, u, bc = W.two_phase_shock_bubble(n)
+    cells = mesh.cells()
+    g = GpuFiveSolver(sys_, mesh, u, bc=bc, cfl=0.5, mode=FluxMode.Weno)
+    for _ in range(warmup):
+        g.step(g.dt_cfl())
+    s = torch.cuda.ExternalStream(g.stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        a.record(s)
+        for _ in range(steps):
+            g.step(g.dt_cfl())
+        b.record(s)
+        b.synchronize()
+    ms = a.elapsed_time(b)
+    ours = g.download()
+    l0 = g.launch_count()
+    g.close()
+    rec = {"workload": f"five-equation two-phase shock-bubble {n}^3 (light gas gamma 1.67 rho 0.138 sphere r=0.15 in "
+                       "air, Mach-2 shock), WCNS WENO5-Z + HLLC + positivity, SSP-RK3, CFL 0.5, outflow, FP64",
+           "unit": "cell-updates/s", "steps": steps, "warmup": warmup,
+           "value": cells * steps / (ms * 1e-3), "ms_per_step": ms / steps, "gpu_launches_total": l0,
+           "clocks": clk.summary()}
+    from oracle import pyrefgpu
+    if pyrefgpu.available():
+        r = pyrefgpu.RefGpuFiveSolver(sys_, mesh, u, bc=bc, cfl=0.5, mode=FluxMode.Weno)
+        r.advance(warmup)
+        r.synchronize()
+        sr = torch.cuda.ExternalStream(r.stream())
+        a2, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a2.record(sr)
+        r.advance(steps)
+        b2.record(sr)
+        b2.synchronize()
+        rms = a2.elapsed_time(b2)
+        ur = r.download()
+        r.close()
+        ia, ib = mesh.interior(ur).reshape(-1, 7), mesh.interior(ours).reshape(-1, 7)
+        num, den = np.abs(ia - ib).sum(axis=0), np.abs(ib).sum(axis=0)
+        rec["reference_gpu"] = {"value": cells * steps / (rms * 1e-3), "ms_per_step": rms / steps,
+                                "ours_speedup": rms / ms,
+                                # the transverse momenta are round-off until the shock meets the
+                                # bubble: measured against the total density
+                                "rel_l1_vs_ours": [float(x) for x in num / np.maximum(den, 1e-3 * (den[0] + den[1]))],
+                                "what": "the reference's compressible-cuda five_f64 kernels (unmodified source, nvcc "
+                                        "sm_100a) in GpuSolver<f64> launch order"}
+    else:
+        rec["reference_gpu"] = {"unavailable": "oracle/_ref/librefgpu.so is not built"}
+    return rec
 
 
 def reference_gpu_leg(args, sys_, mesh, u, bc, cells, ours_ms_per_step, u_ours):

@@ -84,6 +84,7 @@ SIGNATURES = {
     "emg_five_totals": (C.c_int, [_P, _D]),
     "emg_five_get_time": (C.c_int, [_P, _D]),
     "emg_five_launch_count": (C.c_int, [_P, _U64]),
+    "emg_five_stream": (C.c_int, [_P, C.POINTER(_P)]),
     "emg_uniform_step": (C.c_int, [_P, C.c_double]),
     "emg_uniform_dt_cfl": (C.c_int, [_P, _D]),
     "emg_uniform_run_to": (C.c_int, [_P, C.c_double, _U64]),

@@ -739,6 +739,12 @@ int emg_five_get_time(emg_five* h, double* t) {
     return EMG_OK;
 }
 
+int emg_five_stream(emg_five* h, void** stream) {
+    if (!h || !stream) return set_error(EMG_ERR_INVALID, "null argument");
+    *stream = (void*)h->stream;
+    return EMG_OK;
+}
+
 int emg_five_launch_count(emg_five* h, uint64_t* launches) {
     if (!h || !launches) return set_error(EMG_ERR_INVALID, "null argument");
     *launches = h->launches;

@@ -169,6 +169,12 @@ class GpuFiveSolver:
         check(lib().emg_five_launch_count(self._h, C.byref(n)))
         return n.value
 
+    def stream(self):
+        """The solver's CUDA stream handle (int)."""
+        s = C.c_void_p()
+        check(lib().emg_five_stream(self._h, C.byref(s)))
+        return s.value or 0
+
     @property
     def t(self):
         v = C.c_double()

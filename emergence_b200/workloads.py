@@ -180,3 +180,33 @@ def riemann_batch(ninst=4096, nmin=64, nmax=2048, seed=SEED, gamma=1.4, x0=0.5):
         w[:, 4] = np.where(left, st[i, 2], st[i, 5])
         parts.append(sys_.to_cons(w))
     return sys_, n, dx, np.concatenate(parts), st
+
+
+# ---------------------------------------------------------------- five-equation system
+def two_phase_shock_bubble(n=128, mach=2.0, radius=0.15, eps=1e-8, seed=SEED, ng=6):
+    """Two-phase shock–bubble on [0,1]^3 with n^3 cells for the five-equation
+    system: phase 1 a light gas (γ 1.67, ρ 0.138) filling a sphere of radius
+    0.15 about (0.5, 0.5, 0.5) (radius perturbed by ±0.5 % of a seeded
+    low-mode harmonic sum), phase 2 air (γ 1.4, ρ 1, p 1) elsewhere, with
+    volume fraction 1 − eps / eps; a Mach-2 shock in air at x < 0.2 moving +x
+    (Rankine–Hugoniot post-shock state). Outflow boundaries.
+    Returns (FiveEq, mesh, u_padded float64[len, 7], bc)."""
+    from .five import FiveEq, five_initial_state
+    sys = FiveEq((Nasg(1.67), Nasg(1.4)), kapila=True)
+    mesh = Mesh.new((n, n, n), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), ng=ng)
+    x = mesh.centres()
+    r = np.sqrt((x[0] - 0.5) ** 2 + (x[1] - 0.5) ** 2 + (x[2] - 0.5) ** 2)
+    th = np.arccos(np.clip((x[2] - 0.5) / np.maximum(r, 1e-300), -1.0, 1.0))
+    ph = np.arctan2(x[1] - 0.5, x[0] - 0.5)
+    inside = r < radius * (1.0 + 0.005 * _interface_noise(seed, th, ph))
+    rho2, u2, p2, _ = rankine_hugoniot(mach)
+    post = x[0] < 0.2
+    a = np.where(inside, 1.0 - eps, eps)
+    w = np.zeros((n, n, n, 7))
+    w[..., 0] = a * 0.138
+    w[..., 1] = (1.0 - a) * np.where(post, rho2, 1.0)
+    w[..., 2] = np.where(post, u2, 0.0)
+    w[..., 5] = np.where(post, p2, 1.0)
+    w[..., 6] = a
+    bc = [[Bc.Outflow, Bc.Outflow] for _ in range(3)]
+    return sys, mesh, five_initial_state(sys, mesh, w), bc

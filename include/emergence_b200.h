@@ -296,6 +296,9 @@ int emg_five_get_time(emg_five* h, double* t);
 /* Kernel launches issued by the handle since creation. */
 int emg_five_launch_count(emg_five* h, uint64_t* launches);
 
+/* The handle's CUDA stream (cudaStream_t) as an opaque pointer. */
+int emg_five_stream(emg_five* h, void** stream);
+
 /* ------------------------------------------------------------------ batched 1-D lines */
 /* Many independent 1-D problems advanced together: every RK stage is one
  * fused-sweep launch over all instances, each instance with its own cell size
