@@ -33,6 +33,11 @@ N_CELLS = 256
 CPU_STEPS = 5  # timed steps of the CPU baseline on the full grid (about 5 s each on 16 host threads)
 AMR_STEPS = 20
 CELL_BYTES_3D = 320  # algorithmic bytes per 3-D cell-update (64·F, F = 5)
+# flop per interior cell and sweep launch, counted by ncu on the 160^3 explosion
+# (sm__sass_thread_inst_executed_op_{dadd,dmul,dfma,fadd,fmul,ffma}_pred_on, fma = 2)
+SWEEP_FLOP = {"f64": {"fp64": 2104, "fp32": 120}, "mixed": {"fp64": 591, "fp32": 765}}
+# FP64 pipe of a B200: 148 SMs x 64 FMA lanes x 2 flop x 1.965 GHz (nominal; no measured FP64 peak exists here)
+FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 
 
 def parse():
@@ -228,6 +233,12 @@ def run_ours(args, world, rank, local):
     launches_per_step = sweep_n / max(args.steps, 1)
     alg_bytes_per_launch = CELL_BYTES_3D * cells / launches_per_step
     achieved = alg_bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+    flop = SWEEP_FLOP["f64" if prec == Precision.F64 else "mixed"]
+    fp64_tflops = flop["fp64"] * cells / (per_launch_ms * 1e-3) / 1e12
+    fp64_roofline = {"bound": "fp64", "achieved": fp64_tflops, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
+                     "frac": fp64_tflops / FP64_PEAK_TFLOPS, "flop_per_cell_per_launch": flop,
+                     "flop_source": "ncu op counters, profiles/sweep_flops_uniform_160.md",
+                     "peak_source": "nominal FP64 FMA rate at 1965 MHz (148 SMs x 64 lanes x 2 flop)"}
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -318,9 +329,10 @@ def run_ours(args, world, rank, local):
                          "traffic": traffic, "traffic_source": "ncu capture on 160^3 scaled by cells (profiles/)", "kernel": "fused sweep (3 per stage)",
                          "alg_bytes_per_launch": alg_bytes_per_launch, "avg_launch_ms": per_launch_ms,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback",
-                         "compute_note": "the sweep is FP64-ALU bound (about 38 flop per algorithmic byte): FP64 pipe "
+                         "compute_note": "the sweep is FP64-ALU bound (59 FP64 flop per algorithmic byte): FP64 pipe "
                                          "48-52 % active, issue 54-57 % (ncu, profiles/sweep_f64_uniform_160.md); "
-                                         "the HBM fraction is small by construction"},
+                                         "the HBM fraction is small by construction",
+                         "fp64": fp64_roofline},
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()},
             "kernel_share": {k: (v[0] / total_kernel_ms if total_kernel_ms else None) for k, v in kt.items()},
             "gpu_launches": launches,
