@@ -121,6 +121,8 @@ SIGNATURES = {
     "emg_amr_destroy": (C.c_int, [_P]),
     "emg_amr_step": (C.c_int, [_P, C.c_double]),
     "emg_amr_dt_cfl": (C.c_int, [_P, _D]),
+    "emg_amr_step_subcycled": (C.c_int, [_P, C.c_double]),
+    "emg_amr_dt_cfl_subcycled": (C.c_int, [_P, _D]),
     "emg_amr_run_to": (C.c_int, [_P, C.c_double, _U64]),
     "emg_amr_regrid": (C.c_int, [_P]),
     "emg_amr_block_count": (C.c_int, [_P, _U64, _U64]),

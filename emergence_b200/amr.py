@@ -35,15 +35,21 @@ class GpuAmr:
     """Device block-AMR solver. ``cfg`` holds the fields of AmrConfig
     (b, levels, eps, regrid_every, base_blocks, ghosts). ``autotune``: on the
     first step, time the batched sweeps with one and two block rows per CTA
-    and keep the faster per axis (results are the same either way)."""
+    and keep the faster per axis (results are the same either way).
+    ``subcycle``: ``run_to`` takes subcycled steps (Amr::subcycle,
+    fluid/crates/compressible/src/amr.rs:233-236), each level with its own
+    time step; ``step`` / ``dt_cfl`` stay the global step as in the
+    reference, ``step_subcycled`` / ``dt_cfl_subcycled`` are the subcycled
+    ones."""
 
     def __init__(self, sys, cfg, lo, hi, bc, init=None, cfl=0.4, mode=FluxMode.Weno, tol=1e-3, positivity=True,
-                 precision=Precision.F64, blocks=None, autotune=False):
+                 precision=Precision.F64, blocks=None, autotune=False, subcycle=False):
         self.cfg = dict(cfg)
         self._c = _cfg(cfg)
         self._e = EmgEos(sys.eos.gamma, sys.eos.p_inf, sys.eos.b, sys.eos.q, sys.eos.cv)
         self._b = _c_bcs(bc)
-        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, precision, 1 if autotune else 0)
+        flags = (1 if autotune else 0) | (2 if subcycle else 0)
+        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, precision, flags)
         self._lo = np.ascontiguousarray(lo, dtype=np.float64)
         self._hi = np.ascontiguousarray(hi, dtype=np.float64)
         self.bcells = 1
@@ -81,6 +87,15 @@ class GpuAmr:
     def dt_cfl(self):
         v = C.c_double()
         check(lib().emg_amr_dt_cfl(self._h, C.byref(v)))
+        return v.value
+
+    def step_subcycled(self, dt):
+        """Level lmin by dt, finer levels by dt/2^(l-lmin) (Amr::step_subcycled)."""
+        check(lib().emg_amr_step_subcycled(self._h, float(dt)))
+
+    def dt_cfl_subcycled(self):
+        v = C.c_double()
+        check(lib().emg_amr_dt_cfl_subcycled(self._h, C.byref(v)))
         return v.value
 
     def run_to(self, t_end):

@@ -162,6 +162,32 @@ struct emg_amr {
     uint64_t launches = 0;
     double phase_ms[5]{};
     bool rate_valid = false;
+    // ---- subcycling (C/amr.rs:1654-1954; host schedule in step_subcycled)
+    struct ScLevel {
+        int nblk = 0;                  // blocks of the level, leaves and ancestors, in id order
+        DevVec<int> blist;
+        DevVec<CopyTask> copies;       // face ghost slabs of those blocks
+        DevVec<PBox> pboxes;
+        DevVec<int> bcl;
+        int ncopy = 0, npbox = 0, nbcl = 0;
+        int64_t pmax = 0;
+        DevVec<RBox> rfull;            // every ancestor of the level, whole block, chunk-relative offsets
+        std::vector<int> rchunk;       // chunk starts into rfull (and its end)
+        std::vector<int64_t> rchunk_max;
+        DevVec<ScFace> faces;          // coarse–fine faces of its leaves (coarse side), by (d, side)
+        int face_start[7]{};
+        int reg0 = 0;                  // their register rows [reg0, reg0 + nfaces)
+    };
+    std::vector<ScLevel> sc;
+    uint64_t sc_gen = ~0ull;
+    DevVec<int> dall;                  // every block, for the per-level CFL reduction
+    double* usave = nullptr;           // time-view save area, pool-sized
+    int64_t usave_cap = 0;
+    double *creg = nullptr, *freg = nullptr;  // flux registers, 5 × npen doubles per face
+    int64_t reg_cap = 0;
+    unsigned long long* level_rates = nullptr;
+    std::vector<double> level_t0, level_dt;
+    static constexpr int SC_RCHUNK = 256;  // whole-block restriction boxes per launch set
 
     // ---------------------------------------------------------------- geometry
     int64_t nbl(int l, int d) const { return act[d] ? nb0[d] << l : 1; }
@@ -623,24 +649,12 @@ struct emg_amr {
     std::vector<std::array<DevVec<int>, 3>> drbsel;  // per level and axis: boxes the boundary pass changes
     std::vector<std::array<int, 3>> rbsel_count;
 
-    // ---------------------------------------------------------------- layout
-    int ensure_layout() {
-        if (layout_valid) return upload_map();
-        int rc = upload_map();
-        if (rc) return rc;
-        std::vector<int> leaves, lvl(blocks.size()), bcl;
-        std::vector<int64_t> idx(3 * blocks.size());
-        for (size_t i = 0; i < blocks.size(); i++) {
-            lvl[i] = blocks[i].level;
-            for (int d = 0; d < 3; d++) idx[3 * i + d] = blocks[i].idx[d];
-            if (blocks[i].leaf) leaves.push_back((int)i);
-        }
-        nleaves = (int)leaves.size();
-        // ghost slabs of every leaf (C/amr.rs:1148-1203)
-        std::vector<CopyTask> copies;
-        std::vector<PBox> pboxes;
-        int64_t pmax = 0, poff = 0;
-        for (int id : leaves) {
+    // Face ghost slabs of the blocks `ids` (C/amr.rs:1148-1203): same-level
+    // copies, prediction boxes from the next coarser level, and the blocks that
+    // touch a non-periodic domain side (boundary passes).
+    void ghost_tasks(const std::vector<int>& ids, std::vector<CopyTask>& copies, std::vector<PBox>& pboxes,
+                     std::vector<int>& bcl, int64_t& pmax, int64_t& poff) const {
+        for (int id : ids) {
             const HBlock& b = blocks[id];
             const int l = b.level;
             int r[3];
@@ -706,6 +720,26 @@ struct emg_amr {
                     }
             if (touches) bcl.push_back(id);
         }
+    }
+
+    // ---------------------------------------------------------------- layout
+    int ensure_layout() {
+        if (layout_valid) return upload_map();
+        int rc = upload_map();
+        if (rc) return rc;
+        std::vector<int> leaves, lvl(blocks.size()), bcl;
+        std::vector<int64_t> idx(3 * blocks.size());
+        for (size_t i = 0; i < blocks.size(); i++) {
+            lvl[i] = blocks[i].level;
+            for (int d = 0; d < 3; d++) idx[3 * i + d] = blocks[i].idx[d];
+            if (blocks[i].leaf) leaves.push_back((int)i);
+        }
+        nleaves = (int)leaves.size();
+        // ghost slabs of every leaf (C/amr.rs:1148-1203)
+        std::vector<CopyTask> copies;
+        std::vector<PBox> pboxes;
+        int64_t pmax = 0, poff = 0;
+        ghost_tasks(leaves, copies, pboxes, bcl, pmax, poff);
         // restriction boxes per level
         rbox_count.assign(levels, 0);
         rbox_max.assign(levels, 0);
@@ -823,14 +857,17 @@ struct emg_amr {
         if (amrP[d]) return amrP[d];
         return bd[lane] > 16 ? 32 : (bd[lane] * bd[other] >= 32 ? 32 : 16);
     }
-    int sweeps(int stage) {
+    // sweeps of every active axis over the leaves, or over the `nlist` blocks of `list`
+    int sweeps(int stage, const int* list = nullptr, int nlist = 0) {
         for (int d : dims) {
-            int rc = sweep_axis(stage, d, dims[0]);
+            int rc = sweep_axis(stage, d, dims[0], list, nlist);
             if (rc) return rc;
         }
         return EMG_OK;
     }
-    int sweep_axis(int stage, int d, int first) {
+    int sweep_axis(int stage, int d, int first, const int* list = nullptr, int nlist = 0) {
+        const int* blk = list ? list : dleaves.p;
+        const int nblk = list ? nlist : nleaves;
         AmrDev A = view();
         {
             int o[2], no_ = 0;
@@ -869,7 +906,7 @@ struct emg_amr {
             const int P = amr_sweep_P(d, lane, other);
             p.lw = std::min(P, bd[lane]);
             p.amr = 1;
-            p.leaf_slot = dleaves.p;
+            p.leaf_slot = blk;
             p.leaf_level = dlevel.p;
             p.bcell = bcell;
             const int rows = P / p.lw;
@@ -880,7 +917,7 @@ struct emg_amr {
             p.nface = cap * 3 * 2 * 5 * (int64_t)npen;
             p.npen = npen;
             p.pen_lane_major = lane < other ? 1 : 0;
-            const dim3 grid((unsigned)(nleaves * p.ngroups), 1, 1);
+            const dim3 grid((unsigned)(nblk * p.ngroups), 1, 1);
             cudaError_t e = opts.precision == EMG_PRECISION_MIXED ? sweep_launch_amr_mixed(P, opts.mode, p, grid, stream)
                                                                    : sweep_launch_amr_f64(P, opts.mode, p, grid, stream);
             launches++;
@@ -1001,7 +1038,7 @@ struct emg_amr {
     int rk(int stage) {
         AmrDev A = view();
         amr_rk<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
-            A, u0, rhs, dleaves.p, dlevel.p, ddxl.p, stage, ctl);
+            A, u0, rhs, dleaves.p, dlevel.p, ddxl.p, stage, ctl, 0);
         launches++;
         AMR_CUDA(cudaGetLastError());
         record_ev(stage_ev[stage - 1][6]);
@@ -1469,6 +1506,329 @@ struct emg_amr {
                          "non-finite or inadmissible state (density, pressure or specific volume) in a leaf cell");
     }
 
+    // ---------------------------------------------------------------- subcycling
+    // Amr::step_subcycled (C/amr.rs:1654-1954) with the reference's schedule on
+    // the host: level l advances every block of the level (leaves and covered
+    // ancestors) with its own dt, its ghost prediction reads the coarser level
+    // interpolated in time, coarse–fine faces are corrected from flux
+    // registers, and ancestors are restricted from the finer level after its
+    // two half steps. Launches run eagerly (no step graph): θ of the time
+    // views depends on t and dt of every step.
+
+    // per-level lists, rebuilt with the layout
+    int ensure_sc_layout() {
+        int rc = ensure_layout();
+        if (rc) return rc;
+        if (sc_gen == layout_gen) return EMG_OK;
+        if ((int)sc.size() < levels) sc.resize(levels);
+        std::vector<int> all(blocks.size());
+        for (size_t i = 0; i < blocks.size(); i++) all[i] = (int)i;
+        if ((rc = dall.put(all, stream))) return rc;
+        int nreg = 0;
+        int64_t scr_need = 0;
+        for (int l = 0; l < levels; l++) {
+            ScLevel& L = sc[l];
+            std::vector<int> ids;
+            for (size_t i = 0; i < blocks.size(); i++)
+                if (blocks[i].level == l) ids.push_back((int)i);
+            L.nblk = (int)ids.size();
+            std::vector<CopyTask> copies;
+            std::vector<PBox> pboxes;
+            std::vector<int> bcl;
+            int64_t pmax = 0, poff = 0;
+            ghost_tasks(ids, copies, pboxes, bcl, pmax, poff);
+            L.ncopy = (int)copies.size();
+            L.npbox = (int)pboxes.size();
+            L.nbcl = (int)bcl.size();
+            L.pmax = pmax;
+            if (!pbox_fused_fits(pmax)) scr_need = std::max(scr_need, poff);
+            // whole-block restriction of every ancestor (restrict_level_full, C/amr.rs:1902-1910)
+            std::vector<RBox> rb;
+            L.rchunk.clear();
+            L.rchunk_max.clear();
+            int64_t off = 0, mx = 0;
+            for (int id : ids) {
+                if (blocks[id].leaf) continue;
+                if (rb.size() % SC_RCHUNK == 0) {
+                    if (!rb.empty()) L.rchunk_max.push_back(mx);
+                    L.rchunk.push_back((int)rb.size());
+                    off = 0;
+                    mx = 0;
+                }
+                RBox r = make_rbox(l, id, blocks[id].idx, {0, 0, 0}, {bd[0], bd[1], bd[2]});
+                r.off = off;
+                off += r.cap;
+                mx = std::max(mx, r.cap);
+                scr_need = std::max(scr_need, off);
+                rb.push_back(r);
+            }
+            if (!rb.empty()) L.rchunk_max.push_back(mx);
+            L.rchunk.push_back((int)rb.size());
+            // coarse–fine faces of the level's leaves, coarse side (C/amr.rs:1725-1760, kind 0)
+            std::vector<ScFace> faces;
+            L.reg0 = nreg;
+            for (int bucket = 0; bucket < 6; bucket++) {
+                L.face_start[bucket] = (int)faces.size();
+                const int d = bucket / 2, side = bucket % 2;
+                if (!act[d]) continue;
+                const int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
+                for (int id : ids) {
+                    const HBlock& b = blocks[id];
+                    if (!b.leaf || l + 1 >= levels) continue;
+                    const int64_t nbk = nb0[d] << l;
+                    Key nk = b.idx;
+                    nk[d] += side == 1 ? 1 : -1;
+                    if (nk[d] < 0 || nk[d] >= nbk) {
+                        if (bckind(d, side) != EMG_BC_PERIODIC) continue;
+                        nk[d] = erem(nk[d], nbk);
+                    }
+                    const int nj = get(l, nk);
+                    if (!(nj >= 0 && !blocks[nj].leaf)) continue;
+                    ScFace f{};
+                    f.slot = id;
+                    f.d = d;
+                    f.side = side;
+                    f.reg = nreg++;
+                    f.dx = dxl[3 * l + d];
+                    for (int qa = 0; qa < 2; qa++)
+                        for (int qb = 0; qb < 2; qb++) {
+                            f.fine[qa][qb] = -1;
+                            if ((qa && !act[e0]) || (qb && !act[e1])) continue;
+                            Key ck = nk;
+                            ck[d] = 2 * nk[d] + (side == 1 ? 0 : 1);
+                            ck[e0] = act[e0] ? 2 * b.idx[e0] + qa : 0;
+                            ck[e1] = act[e1] ? 2 * b.idx[e1] + qb : 0;
+                            const int cid = get(l + 1, ck);
+                            if (cid >= 0 && blocks[cid].leaf) f.fine[qa][qb] = cid;
+                        }
+                    faces.push_back(f);
+                }
+            }
+            L.face_start[6] = (int)faces.size();
+            if ((rc = L.blist.put(ids, stream)) || (rc = L.copies.put(copies, stream)) ||
+                (rc = L.pboxes.put(pboxes, stream)) || (rc = L.bcl.put(bcl, stream)) || (rc = L.rfull.put(rb, stream)) ||
+                (rc = L.faces.put(faces, stream)))
+                return rc;
+        }
+        if ((rc = scratch(scr_need))) return rc;
+        if (nreg > reg_cap) {
+            const int64_t want = std::max<int64_t>(nreg, 2 * reg_cap);
+            cudaFree(creg);
+            cudaFree(freg);
+            creg = freg = nullptr;
+            reg_cap = 0;
+            if (cudaMalloc(&creg, (size_t)want * 5 * npen * sizeof(double)) != cudaSuccess ||
+                cudaMalloc(&freg, (size_t)want * 5 * npen * sizeof(double)) != cudaSuccess) {
+                cudaGetLastError();
+                return set_error(EMG_ERR_CUDA, "flux register allocation failed");
+            }
+            reg_cap = want;
+        }
+        if (usave_cap != cap) {
+            cudaFree(usave);
+            usave = nullptr;
+            usave_cap = 0;
+            if (cudaMalloc(&usave, (size_t)cap * bcell * 5 * sizeof(double)) != cudaSuccess) {
+                cudaGetLastError();
+                return set_error(EMG_ERR_CUDA, "time-view buffer allocation failed");
+            }
+            usave_cap = cap;
+        }
+        if (!level_rates) AMR_CUDA(cudaMalloc(&level_rates, AMR_MAX_LEVELS * sizeof(unsigned long long)));
+        level_t0.resize(levels, 0.0);
+        level_dt.resize(levels, 0.0);
+        sc_gen = layout_gen;
+        return EMG_OK;
+    }
+
+    int coarsest_leaf_level() const {  // C/amr.rs:1694-1700
+        int m = -1;
+        for (auto& b : blocks)
+            if (b.leaf && (m < 0 || b.level < m)) m = b.level;
+        return m < 0 ? 0 : m;
+    }
+
+    dim3 level_grid(int nblk) const { return dim3((unsigned)nblk, 1, 1); }
+
+    int restrict_full(int l) {  // C/amr.rs:1902-1910
+        if (l < 0 || l + 1 >= levels) return EMG_OK;
+        ScLevel& L = sc[l];
+        for (size_t c = 0; c + 1 < L.rchunk.size(); c++) {
+            const int b0 = L.rchunk[c], nb = L.rchunk[c + 1] - b0;
+            if (nb <= 0) continue;
+            int rc = run_rboxes(L.rfull.p + b0, nb, L.rchunk_max[c]);
+            if (rc) return rc;
+        }
+        return EMG_OK;
+    }
+
+    int fill_ghosts_level(int l) {
+        ScLevel& L = sc[l];
+        AmrDev A = view();
+        if (L.ncopy) {
+            ghost_copy<<<L.ncopy, COPY_THREADS, 0, stream>>>(A, L.copies.p);
+            launches++;
+        }
+        int rc = run_pboxes(L.pboxes.p, L.npbox, L.pmax);
+        if (rc) return rc;
+        if (L.nbcl)
+            for (int di = 0; di < (int)dims.size(); di++) {
+                ghost_bc<<<box_grid(2 * (int64_t)ng * std::max(bd[0], 1) * std::max(bd[1], 1), L.nbcl), 256, 0, stream>>>(
+                    A, L.bcl.p, dlevel.p, didx.p, di);
+                launches++;
+            }
+        AMR_CUDA(cudaGetLastError());
+        return EMG_OK;
+    }
+
+    // Amr::advance_level (C/amr.rs:1836-1900)
+    int advance_level(int l, double dt, int lmin) {
+        ScLevel& L = sc[l];
+        if (!L.nblk) return EMG_OK;
+        const double t0 = level_t0[l];
+        level_dt[l] = dt;
+        const int nf = L.face_start[6];
+        if (nf) {
+            AMR_CUDA(cudaMemsetAsync(creg + (size_t)L.reg0 * 5 * npen, 0, (size_t)nf * 5 * npen * sizeof(double), stream));
+            AMR_CUDA(cudaMemsetAsync(freg + (size_t)L.reg0 * 5 * npen, 0, (size_t)nf * 5 * npen * sizeof(double), stream));
+        }
+        sc_set_dt<<<1, 1, 0, stream>>>(ctl, dt);
+        launches++;
+        const double stage_t[3] = {t0, t0 + dt, t0 + 0.5 * dt};
+        const double weights[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
+        const double nsub = (double)((size_t)1 << (dims.size() - 1));
+        // the coarser level's time view: its blocks were all advanced in this
+        // step; below lmin no level-l ghost reads the coarser level
+        const bool view_on = l > 0 && l - 1 >= lmin && sc[l - 1].nblk > 0;
+        uint64_t f = 0;
+        for (int d : dims) f += (uint64_t)L.nblk * (bcells() / bd[d]) * (bd[d] + 1);
+        int rc;
+        AmrDev A = view();
+        const unsigned gy = (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16);
+        for (int s = 0; s < 3; s++) {
+            if (view_on) {
+                const double pt0 = level_t0[l - 1], pdt = level_dt[l - 1];
+                double th = 1.0;
+                if (pdt > 0.0) {
+                    th = (stage_t[s] - pt0) / pdt;
+                    if (th < 0.0) th = 0.0;
+                    if (th > 1.0) th = 1.0;
+                }
+                sc_time_view<<<sc[l - 1].nblk, 256, 0, stream>>>(A, sc[l - 1].blist.p, u0, usave, th);
+                launches++;
+            }
+            if ((rc = fill_ghosts_level(l))) return rc;
+            if (view_on) {
+                sc_restore<<<sc[l - 1].nblk, 256, 0, stream>>>(A, sc[l - 1].blist.p, usave);
+                launches++;
+            }
+            if ((rc = sweeps(s + 1, L.blist.p, L.nblk))) return rc;
+            const double w = weights[s] * dt;
+            if (nf) {
+                sc_reg_coarse<<<nf, 256, 0, stream>>>(A, L.faces.p, face, npen, creg, w);
+                launches++;
+            }
+            if (l > 0 && sc[l - 1].face_start[6]) {
+                sc_reg_fine<<<sc[l - 1].face_start[6], 256, 0, stream>>>(A, sc[l - 1].faces.p, face, npen, freg, w, nsub);
+                launches++;
+            }
+            amr_rk<<<dim3((unsigned)L.nblk, gy), 256, 0, stream>>>(A, u0, rhs, L.blist.p, dlevel.p, ddxl.p, s + 1, ctl, 1);
+            launches++;
+            AMR_CUDA(cudaGetLastError());
+        }
+        faces += 3 * f;
+        if (opts.mode == EMG_MODE_WENO) weno_faces += 3 * f;
+        if (l + 1 < levels && sc[l + 1].nblk) {
+            level_t0[l + 1] = t0;
+            if ((rc = advance_level(l + 1, 0.5 * dt, lmin))) return rc;
+            level_t0[l + 1] = t0 + 0.5 * dt;
+            if ((rc = advance_level(l + 1, 0.5 * dt, lmin))) return rc;
+            for (int bucket = 0; bucket < 6; bucket++) {
+                const int n = L.face_start[bucket + 1] - L.face_start[bucket];
+                if (!n) continue;
+                sc_reflux<<<n, 256, 0, stream>>>(A, L.faces.p + L.face_start[bucket], creg, freg, npen);
+                launches++;
+            }
+            AMR_CUDA(cudaGetLastError());
+            if ((rc = restrict_full(l))) return rc;
+        }
+        level_t0[l] = t0 + dt;
+        return EMG_OK;
+    }
+
+    int step_subcycled(double dt) {  // C/amr.rs:1912-1952
+        int rc = ensure_sc_layout();
+        if (rc) return rc;
+        ctl_host->dt = dt;
+        ctl_host->done = 0;
+        ctl_host->status = 0;
+        ctl_host->rate_bits = 0;
+        AMR_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice, stream));
+        for (int l = 0; l < levels; l++) level_t0[l] = t;
+        for (int l = levels - 2; l >= 0; l--)
+            if ((rc = restrict_full(l))) return rc;
+        const int lmin = coarsest_leaf_level();
+        if ((rc = advance_level(lmin, dt, lmin))) return rc;
+        for (int l = lmin - 1; l >= 0; l--)
+            if ((rc = restrict_full(l))) return rc;
+        AMR_CUDA(cudaMemcpyAsync(ctl_host, ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, stream));
+        AMR_CUDA(cudaStreamSynchronize(stream));
+        rate_valid = false;
+        t += dt;
+        steps += 1;
+        if (ctl_host->status == EMG_ERR_INADMISSIBLE) return inadmissible();
+        if (next_regrid > steps + 2) next_regrid = steps + 1;
+        if (steps >= next_regrid) {
+            auto before = structure();
+            if ((rc = regrid())) return rc;
+            const bool changed = structure() != before;
+            regrid_interval = changed ? cfg.regrid_every : std::min(2 * regrid_interval, 2 * cfg.regrid_every);
+            next_regrid = steps + (changed ? 1 : 2);
+        }
+        unsigned int e = 0;
+        AMR_CUDA(cudaMemcpy(&e, err, sizeof e, cudaMemcpyDeviceToHost));
+        if ((e & 4u) || ctl_host->status == EMG_ERR_BOUNDS)
+            return set_error(EMG_ERR_BOUNDS, "device index out of range (bounds-check build)");
+        if (e) return set_error(EMG_ERR_UNFILLABLE, "AMR ghost cell without a source (prediction depth or box)");
+        return EMG_OK;
+    }
+
+    // Amr::dt_cfl_subcycled (C/amr.rs:1681-1692)
+    int dt_cfl_subcycled(double* out) {
+        int rc = ensure_sc_layout();
+        if (rc) return rc;
+        AMR_CUDA(cudaMemsetAsync(level_rates, 0, AMR_MAX_LEVELS * sizeof(unsigned long long), stream));
+        AmrDev A = view();
+        if (!blocks.empty()) {
+            sc_cfl_levels<<<(unsigned)blocks.size(), 256, 0, stream>>>(A, dall.p, dlevel.p, ddxl.p, level_rates);
+            launches++;
+            AMR_CUDA(cudaGetLastError());
+        }
+        unsigned long long bits[AMR_MAX_LEVELS];
+        AMR_CUDA(cudaMemcpyAsync(bits, level_rates, sizeof bits, cudaMemcpyDeviceToHost, stream));
+        double g = 0.0;
+        if ((rc = dt_cfl(&g))) return rc;  // synchronises the stream
+        const int lmin = coarsest_leaf_level();
+        double dt = INFINITY;
+        for (int l = lmin; l < levels; l++) {
+            double rate;
+            std::memcpy(&rate, &bits[l], sizeof rate);
+            const double dl = rate > 0.0 ? opts.cfl / rate : INFINITY;
+            dt = std::fmin(dt, dl * (double)((uint64_t)1 << (l - lmin)));
+        }
+        int finest = 0;
+        for (int l = levels - 1; l >= 0; l--) {
+            bool any = false;
+            for (auto& b : blocks) any = any || (b.level == l && b.leaf);
+            if (any) {
+                finest = l;
+                break;
+            }
+        }
+        *out = std::fmin(dt, g * (double)((uint64_t)1 << (finest - lmin)));
+        return EMG_OK;
+    }
+
     // Consistency of an adopted hierarchy (create_from_blocks), on the host
     // before any device work. Structure errors (a block outside the levels or
     // the domain, twice, without its parent, a leaf with children, an
@@ -1683,6 +2043,19 @@ struct emg_amr {
             cudaFree(sok[i]);
         }
         cudaFree(det);
+        cudaFree(usave);
+        cudaFree(creg);
+        cudaFree(freg);
+        cudaFree(level_rates);
+        for (auto& L : sc) {
+            L.blist.release();
+            L.copies.release();
+            L.pboxes.release();
+            L.bcl.release();
+            L.rfull.release();
+            L.faces.release();
+        }
+        dall.release();
         dmap.release();
         dmap_edits.release();
         dleaves.release();
@@ -1814,17 +2187,32 @@ int emg_amr_dt_cfl(emg_amr* h, double* dt) {
 int emg_amr_run_to(emg_amr* h, double t_end, uint64_t* steps) {
     int rc = amr_check(h);
     if (rc) return rc;
+    const bool sub = (h->opts.flags & EMG_OPT_SUBCYCLE) != 0;
     uint64_t n = 0;
     while (h->t < t_end * (1.0 - 1e-14)) {
         double dt = 0.0;
-        if ((rc = h->dt_cfl(&dt))) return rc;
+        if ((rc = sub ? h->dt_cfl_subcycled(&dt) : h->dt_cfl(&dt))) return rc;
         dt = std::fmin(dt, t_end - h->t);
         if (!(std::isfinite(dt) && dt > 0.0)) return set_error(EMG_ERR_DT_COLLAPSED, "time step collapsed");
-        if ((rc = h->step(dt))) return rc;
+        if ((rc = sub ? h->step_subcycled(dt) : h->step(dt))) return rc;
         n++;
     }
     if (steps) *steps = n;
     return EMG_OK;
+}
+
+int emg_amr_step_subcycled(emg_amr* h, double dt) {
+    int rc = amr_check(h);
+    if (rc) return rc;
+    if (!(std::isfinite(dt) && dt > 0.0)) return set_error(EMG_ERR_INVALID, "dt must be finite and positive");
+    return h->step_subcycled(dt);
+}
+
+int emg_amr_dt_cfl_subcycled(emg_amr* h, double* dt) {
+    int rc = amr_check(h);
+    if (rc) return rc;
+    if (!dt) return set_error(EMG_ERR_INVALID, "null dt");
+    return h->dt_cfl_subcycled(dt);
 }
 
 int emg_amr_regrid(emg_amr* h) {

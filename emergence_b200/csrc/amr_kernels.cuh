@@ -707,8 +707,12 @@ __global__ void reflux_faces(const AmrDev A, double* rhs, const double* __restri
 
 // SSP-RK3 stage update of the leaves (amr.rs:1476-1498) and, after the third
 // stage, the CFL rate of the new state (amr.rs:1409-1427).
+// `sc`: the coefficient form of the subcycled level step (amr.rs:1869-1877,
+// a0·u0 + a1·(u + dt·r) with (a0, a1) = (0, 1), (3/4, 1/4), (1/3, 2/3)),
+// which rounds differently from the global step's in stages 1 and 3.
 __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rhs, const int* __restrict__ leaves,
-                       const int* __restrict__ level, const double* __restrict__ dxl, int stage, StepCtl* ctl) {
+                       const int* __restrict__ level, const double* __restrict__ dxl, int stage, StepCtl* ctl,
+                       int sc = 0) {
     const int slot = leaves[blockIdx.x];
     const int l = level[slot];
     const double dt = ctl->dt;
@@ -735,11 +739,11 @@ __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rh
             double v;
             if (stage == 1) {
                 u0[o] = uu;
-                v = uu + dt * r;
+                v = sc ? 0.0 * uu + 1.0 * (uu + dt * r) : uu + dt * r;
             } else if (stage == 2) {
                 v = 0.75 * u0[o] + 0.25 * (uu + dt * r);
             } else {
-                v = u0[o] / 3.0 + 2.0 / 3.0 * (uu + dt * r);
+                v = sc ? (1.0 / 3.0) * u0[o] + 2.0 / 3.0 * (uu + dt * r) : u0[o] / 3.0 + 2.0 / 3.0 * (uu + dt * r);
             }
             A.u[o] = v;
             un[k] = v;
@@ -804,6 +808,170 @@ __global__ void amr_cfl(const AmrDev A, const int* __restrict__ leaves, const in
         for (int w = 1; w < (int)(blockDim.x >> 5); w++) v = fmax(v, sr[w]);
         if (!isnan(v) && v > 0.0) atomicMax(&ctl->rate_bits, (unsigned long long)__double_as_longlong(v));
         if (any_bad) atomicCAS(&ctl->status, 0, (int)EMG_ERR_INADMISSIBLE);
+    }
+}
+
+// ---------------------------------------------------------------- subcycling
+// (amr.rs:1654-1954). One CTA per block of a level list, threads over the
+// block's interior cells.
+
+// step size of the level step in flight (read by the sweeps' limiter and the RK update)
+__global__ void sc_set_dt(StepCtl* ctl, double dt) { ctl->dt = dt; }
+
+// Level-l data as its linear interpolation in time, u ← (1−θ)·u0 + θ·u, the
+// current data kept in `usave` (set_time_view, amr.rs:1702-1716); the ghost
+// prediction of level l+1 reads block interiors only.
+__global__ void sc_time_view(const AmrDev A, const int* __restrict__ blist, const double* __restrict__ u0,
+                             double* __restrict__ usave, double th) {
+    const int slot = blist[blockIdx.x];
+    const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
+    for (int64_t q = threadIdx.x; q < n; q += blockDim.x) {
+        int64_t c[3];
+        box_coord(q, A.bd, c);
+        const int64_t cell = (int64_t)slot * A.bcell + amr_cell(A, c);
+        if constexpr (BOUNDS_CHECK) {
+            if (slot < 0 || cell < 0 || cell >= A.ntot) {
+                atomicOr(A.err, 4u);
+                continue;
+            }
+        }
+        for (int k = 0; k < 5; k++) {
+            const int64_t o = (int64_t)k * A.ntot + cell;
+            const double uu = A.u[o];
+            usave[o] = uu;
+            A.u[o] = (1.0 - th) * u0[o] + th * uu;
+        }
+    }
+}
+
+// restore_time_view (amr.rs:1718-1723)
+__global__ void sc_restore(const AmrDev A, const int* __restrict__ blist, const double* __restrict__ usave) {
+    const int slot = blist[blockIdx.x];
+    const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
+    for (int64_t q = threadIdx.x; q < n; q += blockDim.x) {
+        int64_t c[3];
+        box_coord(q, A.bd, c);
+        const int64_t cell = (int64_t)slot * A.bcell + amr_cell(A, c);
+        if constexpr (BOUNDS_CHECK) {
+            if (slot < 0 || cell < 0 || cell >= A.ntot) {
+                atomicOr(A.err, 4u);
+                continue;
+            }
+        }
+        for (int k = 0; k < 5; k++) A.u[(int64_t)k * A.ntot + cell] = usave[(int64_t)k * A.ntot + cell];
+    }
+}
+
+// A coarse–fine face of a level-l leaf whose same-level neighbour across
+// (d, side) is refined (amr.rs:1725-1760, kind 0): its flux registers are rows
+// `reg` of the register arrays (5 fields × npen face cells), fine[qa][qb] the
+// adjacent level-(l+1) leaves per quarter of the face (−1: none).
+struct ScFace {
+    int slot, d, side, reg;
+    double dx;
+    int fine[2][2];
+};
+
+// coarse side: creg += w·F over the face (amr.rs:1774-1781)
+__global__ void sc_reg_coarse(const AmrDev A, const ScFace* __restrict__ tasks, const double* __restrict__ face, int npen,
+                              double* creg, double w) {
+    const ScFace tk = tasks[blockIdx.x];
+    const int e0 = tk.d == 0 ? 1 : 0, e1 = tk.d == 2 ? 1 : 2;
+    const int nf = A.bd[e0] * A.bd[e1];
+    for (int pen = threadIdx.x; pen < nf; pen += blockDim.x) {
+        const double* f = face + ((((int64_t)tk.slot * 3 + tk.d) * 2 + tk.side) * 5) * npen + pen;
+        double* r = creg + (int64_t)tk.reg * 5 * npen + pen;
+        for (int k = 0; k < 5; k++) r[(int64_t)k * npen] = r[(int64_t)k * npen] + w * f[(int64_t)k * npen];
+    }
+}
+
+// fine side: freg += w·F/nsub for the 2^(D−1) fine faces of each coarse face
+// cell, in the order of the fine block's face loop (amr.rs:1782-1800)
+__global__ void sc_reg_fine(const AmrDev A, const ScFace* __restrict__ tasks, const double* __restrict__ face, int npen,
+                            double* freg, double w, double nsub) {
+    const ScFace tk = tasks[blockIdx.x];
+    const int d = tk.d;
+    const int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
+    const int b0 = A.bd[e0], b1 = A.bd[e1];
+    for (int pen = threadIdx.x; pen < b0 * b1; pen += blockDim.x) {
+        const int a = pen / b1, bb = pen % b1;
+        double* r = freg + (int64_t)tk.reg * 5 * npen + pen;
+        for (int fa = 0; fa < (A.act[e0] ? 2 : 1); fa++)
+            for (int fb = 0; fb < (A.act[e1] ? 2 : 1); fb++) {
+                const int qa = A.act[e0] ? (2 * a + fa) / b0 : 0, qb = A.act[e1] ? (2 * bb + fb) / b1 : 0;
+                const int cid = tk.fine[qa][qb];
+                if (cid < 0) continue;
+                const int la = A.act[e0] ? (2 * a + fa) % b0 : 0, lb = A.act[e1] ? (2 * bb + fb) % b1 : 0;
+                const double* fv = face + ((((int64_t)cid * 3 + d) * 2 + (1 - tk.side)) * 5) * npen + la * b1 + lb;
+                for (int k = 0; k < 5; k++) r[(int64_t)k * npen] = r[(int64_t)k * npen] + w * fv[(int64_t)k * npen] / nsub;
+            }
+    }
+}
+
+// reflux_level (amr.rs:1809-1834): u += ±(freg − creg)/dx on the face cells
+// that received fine fluxes; launched per (d, side) bucket in order
+__global__ void sc_reflux(const AmrDev A, const ScFace* __restrict__ tasks, const double* __restrict__ creg,
+                          const double* __restrict__ freg, int npen) {
+    const ScFace tk = tasks[blockIdx.x];
+    const int d = tk.d;
+    const int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
+    const int b0 = A.bd[e0], b1 = A.bd[e1];
+    for (int pen = threadIdx.x; pen < b0 * b1; pen += blockDim.x) {
+        const int a = pen / b1, bb = pen % b1;
+        const int qa = A.act[e0] ? (2 * a) / b0 : 0, qb = A.act[e1] ? (2 * bb) / b1 : 0;
+        if (tk.fine[qa][qb] < 0) continue;
+        int64_t c[3];
+        c[d] = tk.side == 1 ? A.bd[d] - 1 : 0;
+        c[e0] = a;
+        c[e1] = bb;
+        const int64_t cell = (int64_t)tk.slot * A.bcell + amr_cell(A, c);
+        if constexpr (BOUNDS_CHECK) {
+            if (tk.slot < 0 || cell < 0 || cell >= A.ntot) {
+                atomicOr(A.err, 4u);
+                continue;
+            }
+        }
+        const double* fr = freg + (int64_t)tk.reg * 5 * npen + pen;
+        const double* cr = creg + (int64_t)tk.reg * 5 * npen + pen;
+        for (int k = 0; k < 5; k++) {
+            const double df = fr[(int64_t)k * npen] - cr[(int64_t)k * npen];
+            double* uo = A.u + (int64_t)k * A.ntot + cell;
+            *uo = *uo + (tk.side == 1 ? -df / tk.dx : df / tk.dx);
+        }
+    }
+}
+
+// CFL rate of every block of a list (leaves and ancestors), reduced per level
+// (dt_cfl_level, amr.rs:1657-1679)
+__global__ void sc_cfl_levels(const AmrDev A, const int* __restrict__ blist, const int* __restrict__ level,
+                              const double* __restrict__ dxl, unsigned long long* rate_bits) {
+    const int slot = blist[blockIdx.x];
+    const int l = level[slot];
+    const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
+    const Eos<double> e = Eos<double>::from(A.eos);
+    double rate = 0.0;
+    for (int64_t q = threadIdx.x; q < n; q += blockDim.x) {
+        int64_t c[3];
+        box_coord(q, A.bd, c);
+        double uu[5], w[5];
+        amr_load(A, slot, amr_cell(A, c), uu);
+        to_prim(e, uu, w);
+        const double cs = sound_speed(e, w[0], w[4]);
+        double sp = -0.0;
+        for (int i = 0; i < A.ndims; i++) {
+            const int d = A.dims[i];
+            sp = sp + (fabs(w[1 + d]) + cs) / dxl[3 * l + d];
+        }
+        rate = fmax(rate, sp);
+    }
+    for (int o = 16; o > 0; o >>= 1) rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, o));
+    __shared__ double sr[32];
+    if ((threadIdx.x & 31) == 0) sr[threadIdx.x >> 5] = rate;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = sr[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) v = fmax(v, sr[w]);
+        if (!isnan(v) && v > 0.0) atomicMax(&rate_bits[l], (unsigned long long)__double_as_longlong(v));
     }
 }
 

@@ -107,6 +107,11 @@ typedef struct emg_opts {
  * (uniform grids; cached per mesh extents, flux mode and precision). Results
  * are the same for every shape. */
 #define EMG_OPT_AUTOTUNE 1
+/* emg_opts.flags, block AMR only: subcycling (Amr::subcycle, C/amr.rs:233-
+ * 236). emg_amr_run_to then advances with emg_amr_dt_cfl_subcycled steps of
+ * emg_amr_step_subcycled; emg_amr_step / emg_amr_dt_cfl keep the global
+ * time step, as the reference's step / dt_cfl do. */
+#define EMG_OPT_SUBCYCLE 2
 
 /* ------------------------------------------------------------------ misc */
 
@@ -399,8 +404,24 @@ int emg_amr_step(emg_amr* h, double dt);
 /* Global CFL step over the leaves (C/amr.rs:1409-1467; G/amr.rs:769-805). */
 int emg_amr_dt_cfl(emg_amr* h, double* dt);
 
-/* Advance to t_end (C/amr.rs:1639-1652): stops at t ≥ t_end(1 − 1e-14). */
+/* Advance to t_end (C/amr.rs:1639-1652): stops at t ≥ t_end(1 − 1e-14);
+ * subcycled steps when the handle was created with EMG_OPT_SUBCYCLE. */
 int emg_amr_run_to(emg_amr* h, double t_end, uint64_t* steps);
+
+/* One subcycled step (Amr::step_subcycled, C/amr.rs:1912-1952): the coarsest
+ * level holding leaves advances by dt, each finer level l by dt/2^(l-lmin)
+ * with its ancestors, coarse ghost data interpolated linearly in time and
+ * coarse–fine faces corrected from flux registers; then every ancestor is
+ * restricted and the regrid schedule of subcycling applies. Coarse–fine
+ * corrections of one cell are applied in the order direction, side (the
+ * reference applies them in hash-map order). No counterpart on the
+ * reference's GPU (G/amr.rs:140-142 refuses subcycling). */
+int emg_amr_step_subcycled(emg_amr* h, double dt);
+
+/* Level step of subcycling (Amr::dt_cfl_subcycled, C/amr.rs:1681-1692):
+ * every level's CFL limit over its leaves and ancestors, scaled by 2^(l-lmin),
+ * and the global limit at the finest leaf level. */
+int emg_amr_dt_cfl_subcycled(emg_amr* h, double* dt);
 
 /* Regrid now (C/amr.rs:1039-1046). */
 int emg_amr_regrid(emg_amr* h);

@@ -1,15 +1,16 @@
 // CPU ORACLE — test infrastructure only (see oracle.hpp).
 //
-// C++ restatement of the reference block-AMR solver, global-time-step path:
-// fluid/crates/compressible/src/amr.rs:1-1652 and :1955-2005 (subcycling,
-// :1654-1954, is not restated: the reference GPU path rejects it too,
-// compressible-cuda/src/amr.rs:140-142). Same block pool, dense per-level
-// index, sampling / prediction / restriction operators, refluxing, wavelet
-// regrid with 2:1 balance, and SSP-RK3 stepping, in the reference's
-// operation order.
+// C++ restatement of the reference block-AMR solver:
+// fluid/crates/compressible/src/amr.rs:1-2005, the global time step and the
+// subcycled one (:1654-1954; the reference runs that on the CPU only, its GPU
+// path refuses it, compressible-cuda/src/amr.rs:140-142). Same block pool,
+// dense per-level index, sampling / prediction / restriction operators,
+// refluxing, flux registers, wavelet regrid with 2:1 balance, and SSP-RK3
+// stepping, in the reference's operation order.
 #pragma once
 #include "oracle.hpp"
 #include <functional>
+#include <map>
 #include <set>
 #include <tuple>
 
@@ -52,7 +53,7 @@ struct AmrBlock {  // amr.rs:194-206
     int64_t level;
     Key3 idx;
     bool leaf = true;
-    std::vector<V> u, u0, rhs;
+    std::vector<V> u, u0, u_save, rhs;
     std::vector<V> face[3][2];
 };
 
@@ -78,6 +79,15 @@ struct Amr {
     std::array<double, 6> wr;
     double stage_dt = 0.0;
     int64_t regrid_interval, next_regrid;
+    // subcycling (amr.rs:233-245): per-level start time and step of the level
+    // step in flight; flux registers keyed by (coarse leaf block, direction,
+    // side, face index). The reference keeps the registers in hash maps and
+    // applies them in hash order; ordered maps give the fixed order of
+    // reflux_level below.
+    bool subcycle = false;
+    std::vector<double> level_t0, level_dt;
+    using RegKey = std::tuple<int64_t, int, int, int64_t>;
+    std::map<RegKey, V> creg, freg;
 
     // ---- geometry (amr.rs:251-292)
     bool active(int d) const { return cfg.base_blocks[d] > 0 && (hi[d] - lo[d]) > 0.0 && bd(d) > 1; }
@@ -139,6 +149,8 @@ struct Amr {
         wr = {3.0 / 256.0, -25.0 / 256.0, 150.0 / 256.0, 150.0 / 256.0, -25.0 / 256.0, 3.0 / 256.0};
         regrid_interval = cfg.regrid_every;
         next_regrid = cfg.regrid_every;
+        level_t0.assign(cfg.levels, 0.0);
+        level_dt.assign(cfg.levels, 0.0);
         for (int d = 0; d < 3; d++) {
             nb0[d] = std::max<int64_t>(cfg.base_blocks[d], 1);
             act[d] = active(d);
@@ -1187,16 +1199,281 @@ struct Amr {
         next_regrid = steps + regrid_interval;
     }
 
-    // amr.rs:1639-1652 (global time step)
+    // amr.rs:1639-1652
     int64_t run_to(double t_end) {
         int64_t n = 0;
         while (t < t_end * (1.0 - 1e-14)) {
-            double dt = std::fmin(dt_cfl(), t_end - t);
+            double dt = std::fmin(subcycle ? dt_cfl_subcycled() : dt_cfl(), t_end - t);
             if (!(std::isfinite(dt) && dt > 0.0)) return -1;
-            step(dt);
+            if (subcycle)
+                step_subcycled(dt);
+            else
+                step(dt);
             n += 1;
         }
         return n;
+    }
+
+    // ---------------------------------------------------------------- subcycling
+
+    // amr.rs:1657-1679: CFL step of the level-l blocks, leaves and ancestors
+    double dt_cfl_level(int64_t l) const {
+        std::vector<int> dm = dims();
+        double rate = 0.0;
+        for (const AmrBlock& b : blocks) {
+            if (b.level != l) continue;
+            double r = 0.0;
+            for (const V& u : b.u) {
+                V w = sys.to_prim(u);
+                double sp = -0.0;
+                for (int d : dm) sp = sp + sys.max_speed(w, d) / dx(l, d);
+                r = std::fmax(r, sp);
+            }
+            rate = std::fmax(rate, r);
+        }
+        return rate > 0.0 ? cfl / rate : INFINITY;
+    }
+
+    // amr.rs:1681-1692: level-lmin step such that level l takes dt/2^(l-lmin)
+    double dt_cfl_subcycled() const {
+        int64_t lmin = coarsest_leaf_level();
+        double dt = INFINITY;
+        for (int64_t l = lmin; l < cfg.levels; l++) dt = std::fmin(dt, dt_cfl_level(l) * (double)(uint64_t(1) << (l - lmin)));
+        double g = dt_cfl();
+        int64_t finest = 0;
+        for (int64_t l = cfg.levels - 1; l >= 0; l--) {
+            bool any = false;
+            for (const AmrBlock& b : blocks) any = any || (b.level == l && b.leaf);
+            if (any) {
+                finest = l;
+                break;
+            }
+        }
+        return std::fmin(dt, g * (double)(uint64_t(1) << (finest - lmin)));
+    }
+
+    // amr.rs:1694-1700
+    int64_t coarsest_leaf_level() const {
+        int64_t m = -1;
+        for (const AmrBlock& b : blocks)
+            if (b.leaf && (m < 0 || b.level < m)) m = b.level;
+        return m < 0 ? 0 : m;
+    }
+
+    // amr.rs:1702-1723: level-l data linearly interpolated in time (saved, then restored)
+    void set_time_view(int64_t l, double tv) {
+        double t0 = level_t0[l], dt = level_dt[l];
+        double th = 1.0;
+        if (dt > 0.0) {
+            th = (tv - t0) / dt;
+            if (th < 0.0) th = 0.0;
+            if (th > 1.0) th = 1.0;
+        }
+        for (AmrBlock& b : blocks) {
+            if (b.level != l || b.u0.empty()) continue;
+            b.u_save = b.u;
+            for (size_t c = 0; c < b.u.size(); c++)
+                for (int q = 0; q < 5; q++) b.u[c][q] = (1.0 - th) * b.u0[c][q] + th * b.u[c][q];
+        }
+    }
+    void restore_time_view(int64_t l) {
+        for (AmrBlock& b : blocks)
+            if (b.level == l && !b.u_save.empty()) std::swap(b.u, b.u_save);
+    }
+
+    // amr.rs:1725-1760: coarse–fine faces of block id: (d, side, kind, coarse
+    // block) with kind 0 = the neighbour is refined, 1 = the neighbour is coarser
+    struct CfFace {
+        int d, side, kind;
+        int64_t coarse;
+    };
+    std::vector<CfFace> cf_faces(int64_t id) const {
+        const AmrBlock& b = blocks[id];
+        int64_t l = b.level;
+        std::vector<int> dm = dims();
+        std::vector<CfFace> out;
+        for (int d : dm) {
+            int64_t nbk = cfg.base_blocks[d] * (int64_t(1) << l);
+            for (int side = 0; side < 2; side++) {
+                Key3 nk = b.idx;
+                nk[d] += side == 1 ? 1 : -1;
+                if (nk[d] < 0 || nk[d] >= nbk) {
+                    if (bc[d][side].kind != BC_PERIODIC) continue;
+                    nk[d] = rem_euclid(nk[d], nbk);
+                }
+                int64_t j = get(l, nk);
+                if (j >= 0) {
+                    if (!blocks[j].leaf) out.push_back({d, side, 0, -1});
+                } else if (l > 0) {
+                    Key3 pk;
+                    for (int e = 0; e < 3; e++) pk[e] = active(e) ? (nk[e] >> 1) : 0;
+                    int64_t cj = get(l - 1, pk);
+                    if (cj >= 0) out.push_back({d, side, 1, cj});
+                }
+            }
+        }
+        return out;
+    }
+
+    // amr.rs:1762-1807: add the stage's boundary fluxes (weight wdt) to the registers
+    void accumulate_registers(const std::vector<int64_t>& ids, double wdt) {
+        std::vector<int> dm = dims();
+        int64_t bdv[3] = {bd(0), bd(1), bd(2)};
+        double nsub = (double)(size_t(1) << (dm.size() - 1));
+        for (int64_t id : ids) {
+            if (!blocks[id].leaf) continue;
+            for (const CfFace& cf : cf_faces(id)) {
+                int d = cf.d;
+                int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
+                const std::vector<V>& face = blocks[id].face[d][cf.side];
+                if (cf.kind == 0) {
+                    for (size_t fi = 0; fi < face.size(); fi++) {
+                        V& e = creg.try_emplace(RegKey{id, d, cf.side, (int64_t)fi}, V{0, 0, 0, 0, 0}).first->second;
+                        for (int q = 0; q < 5; q++) e[q] = e[q] + wdt * face[fi][q];
+                    }
+                } else {
+                    const AmrBlock& b = blocks[id];
+                    const AmrBlock& cb = blocks[cf.coarse];
+                    for (int64_t a = 0; a < bdv[e0]; a++)
+                        for (int64_t bb = 0; bb < bdv[e1]; bb++) {
+                            int64_t ga = b.idx[e0] * bdv[e0] + a;
+                            int64_t gb = b.idx[e1] * bdv[e1] + bb;
+                            int64_t ca = active(e0) ? div_euclid(ga, 2) - cb.idx[e0] * bdv[e0] : 0;
+                            int64_t cbb = active(e1) ? div_euclid(gb, 2) - cb.idx[e1] * bdv[e1] : 0;
+                            if (ca >= bdv[e0] || cbb >= bdv[e1]) continue;
+                            const V& f = face[a * bdv[e1] + bb];
+                            V& e = freg.try_emplace(RegKey{cf.coarse, d, 1 - cf.side, ca * bdv[e1] + cbb}, V{0, 0, 0, 0, 0})
+                                       .first->second;
+                            for (int q = 0; q < 5; q++) e[q] = e[q] + wdt * f[q] / nsub;
+                        }
+                }
+            }
+        }
+    }
+
+    // amr.rs:1809-1834: correct the coarse leaves of level l with the registers.
+    // Order: by direction, then side, then block and face index (a cell on two
+    // coarse–fine faces takes the correction of the lower direction first).
+    void reflux_level(int64_t l) {
+        int64_t bdv[3] = {bd(0), bd(1), bd(2)};
+        std::vector<RegKey> keys;
+        for (auto& kv : creg)
+            if (blocks[std::get<0>(kv.first)].level == l) keys.push_back(kv.first);
+        std::sort(keys.begin(), keys.end(), [](const RegKey& x, const RegKey& y) {
+            return std::make_tuple(std::get<1>(x), std::get<2>(x), std::get<0>(x), std::get<3>(x)) <
+                   std::make_tuple(std::get<1>(y), std::get<2>(y), std::get<0>(y), std::get<3>(y));
+        });
+        for (const RegKey& key : keys) {
+            auto fr = freg.find(key);
+            if (fr == freg.end()) continue;
+            const V& cr = creg[key];
+            int64_t id = std::get<0>(key), fi = std::get<3>(key);
+            int d = std::get<1>(key), side = std::get<2>(key);
+            int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
+            int64_t c[3];
+            c[d] = side == 1 ? bdv[d] - 1 : 0;
+            c[e0] = fi / bdv[e1];
+            c[e1] = fi % bdv[e1];
+            double dxl = dx(l, d);
+            V& u = blocks[id].u[cidx(c[0], c[1], c[2])];
+            for (int q = 0; q < 5; q++) {
+                double df = fr->second[q] - cr[q];
+                u[q] = u[q] + (side == 1 ? -df / dxl : df / dxl);
+            }
+        }
+    }
+
+    // amr.rs:1836-1900: advance every level-l block (leaves and ancestors) by
+    // dt, then level l+1 twice by dt/2, then reflux and restrict
+    void advance_level(int64_t l, double dt) {
+        std::vector<int64_t> ids;
+        for (size_t i = 0; i < blocks.size(); i++)
+            if (blocks[i].level == l) ids.push_back(i);
+        if (ids.empty()) return;
+        double t0 = level_t0[l];
+        level_dt[l] = dt;
+        for (int64_t id : ids) blocks[id].u0 = blocks[id].u;
+        for (auto it = creg.begin(); it != creg.end();)
+            it = blocks[std::get<0>(it->first)].level == l ? creg.erase(it) : std::next(it);
+        for (auto it = freg.begin(); it != freg.end();)
+            it = blocks[std::get<0>(it->first)].level == l ? freg.erase(it) : std::next(it);
+        stage_dt = dt;
+        double stage_t[3] = {t0, t0 + dt, t0 + 0.5 * dt};
+        double weights[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
+        double a0s[3] = {0.0, 0.75, 1.0 / 3.0}, a1s[3] = {1.0, 0.25, 2.0 / 3.0};
+        for (int s = 0; s < 3; s++) {
+            if (l > 0) set_time_view(l - 1, stage_t[s]);
+            std::vector<std::vector<V>> rhs(ids.size());
+            std::vector<std::array<std::array<std::vector<V>, 2>, 3>> faces(ids.size());
+            std::vector<Stats> st(ids.size());
+#pragma omp parallel for schedule(dynamic, 1)
+            for (int64_t n = 0; n < (int64_t)ids.size(); n++) {
+                std::vector<V> face[3][2];
+                st[n] = block_rhs(ids[n], rhs[n], face);
+                for (int d = 0; d < 3; d++)
+                    for (int sd = 0; sd < 2; sd++) faces[n][d][sd] = std::move(face[d][sd]);
+            }
+            if (l > 0) restore_time_view(l - 1);
+            for (size_t n = 0; n < ids.size(); n++) {
+                AmrBlock& b = blocks[ids[n]];
+                b.rhs = std::move(rhs[n]);
+                for (int d = 0; d < 3; d++)
+                    for (int sd = 0; sd < 2; sd++) b.face[d][sd] = std::move(faces[n][d][sd]);
+                stats.add(st[n]);
+            }
+            accumulate_registers(ids, weights[s] * dt);
+            double a0 = a0s[s], a1 = a1s[s];
+            for (int64_t id : ids) {
+                AmrBlock& b = blocks[id];
+                for (size_t c = 0; c < b.u.size(); c++)
+                    for (int q = 0; q < 5; q++) b.u[c][q] = a0 * b.u0[c][q] + a1 * (b.u[c][q] + dt * b.rhs[c][q]);
+            }
+        }
+        bool finer = false;
+        if (l + 1 < cfg.levels)
+            for (const AmrBlock& b : blocks) finer = finer || b.level == l + 1;
+        if (finer) {
+            level_t0[l + 1] = t0;
+            advance_level(l + 1, 0.5 * dt);
+            level_t0[l + 1] = t0 + 0.5 * dt;
+            advance_level(l + 1, 0.5 * dt);
+            reflux_level(l);
+            restrict_level_full(l);
+        }
+        level_t0[l] = t0 + dt;
+    }
+
+    // amr.rs:1902-1910: every ancestor of level l from level l+1
+    void restrict_level_full(int64_t l) {
+        int64_t lo0[3] = {0, 0, 0}, hi0[3] = {bd(0), bd(1), bd(2)};
+        std::vector<int64_t> ids;
+        for (size_t i = 0; i < blocks.size(); i++)
+            if (!blocks[i].leaf && blocks[i].level == l) ids.push_back(i);
+        std::vector<std::vector<V>> fresh(ids.size());
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int64_t n = 0; n < (int64_t)ids.size(); n++) fresh[n] = restrict_box(l, blocks[ids[n]].idx, lo0, hi0);
+        for (size_t n = 0; n < ids.size(); n++) blocks[ids[n]].u = std::move(fresh[n]);
+    }
+
+    // amr.rs:1912-1952: one subcycled step, level lmin by dt
+    void step_subcycled(double dt) {
+        creg.clear();
+        freg.clear();
+        for (int64_t l = 0; l < cfg.levels; l++) level_t0[l] = t;
+        for (int64_t l = cfg.levels - 2; l >= 0; l--) restrict_level_full(l);
+        int64_t lmin = coarsest_leaf_level();
+        advance_level(lmin, dt);
+        for (int64_t l = lmin - 1; l >= 0; l--) restrict_level_full(l);
+        t += dt;
+        steps += 1;
+        if (next_regrid > steps + 2) next_regrid = steps + 1;
+        if (steps >= next_regrid) {
+            auto before = structure();
+            regrid();
+            bool changed = structure() != before;
+            regrid_interval = changed ? cfg.regrid_every : std::min(2 * regrid_interval, 2 * cfg.regrid_every);
+            next_regrid = steps + (changed ? 1 : 2);
+        }
     }
 
     // amr.rs:1991-2005

@@ -331,7 +331,16 @@ int emgo_amr_create(const emg_amr_config* cfg, const emg_eos* eos, const double 
     a->tol = opts->tol;
     a->mode = opts->mode;
     a->positivity = opts->positivity != 0;
+    a->subcycle = (opts->flags & EMG_OPT_SUBCYCLE) != 0;
     *out = a;
+    return EMG_OK;
+}
+int emgo_amr_step_subcycled(void* h, double dt) {
+    ((Amr*)h)->step_subcycled(dt);
+    return EMG_OK;
+}
+int emgo_amr_dt_cfl_subcycled(void* h, double* dt) {
+    *dt = ((Amr*)h)->dt_cfl_subcycled();
     return EMG_OK;
 }
 int emgo_amr_destroy(void* h) {
@@ -408,6 +417,19 @@ int emgo_amr_details(void* h, double* out, size_t cap) {
     a->restrict_all();
     std::vector<double> d = a->details();
     for (size_t i = 0; i < d.size(); i++) out[i] = d[i];
+    return EMG_OK;
+}
+
+// conserved state at level-l cell coordinates g[3*i..] (Amr::sample, amr.rs:384-439):
+// the covering block's data, or the prediction from coarser levels
+int emgo_amr_sample(void* h, int64_t l, const int64_t* g, size_t n, double* out) {
+    Amr* a = (Amr*)h;
+    if (l < 0 || l >= a->cfg.levels) return fail(EMG_ERR_INVALID, "level out of range");
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        V v = a->sample(l, {g[3 * i], g[3 * i + 1], g[3 * i + 2]});
+        for (int q = 0; q < 5; q++) out[5 * i + q] = v[q];
+    }
     return EMG_OK;
 }
 

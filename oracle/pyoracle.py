@@ -386,6 +386,8 @@ SIGS_AMR = {
                                   C.POINTER(EmgOpts), INIT_FN, C.c_void_p, C.POINTER(_P)]),
     "emgo_amr_destroy": (C.c_int, [_P]),
     "emgo_amr_step": (C.c_int, [_P, C.c_double]),
+    "emgo_amr_step_subcycled": (C.c_int, [_P, C.c_double]),
+    "emgo_amr_dt_cfl_subcycled": (C.c_int, [_P, _D]),
     "emgo_amr_dt_cfl": (C.c_int, [_P, _D]),
     "emgo_amr_run_to": (C.c_int, [_P, C.c_double, _U64]),
     "emgo_amr_regrid": (C.c_int, [_P]),
@@ -397,6 +399,7 @@ SIGS_AMR = {
     "emgo_amr_get_time": (C.c_int, [_P, _D]),
     "emgo_amr_steps": (C.c_int, [_P, _U64]),
     "emgo_amr_details": (C.c_int, [_P, _D, C.c_size_t]),
+    "emgo_amr_sample": (C.c_int, [_P, C.c_int64, C.POINTER(C.c_int64), C.c_size_t, _D]),
 }
 
 
@@ -431,14 +434,15 @@ def c_amr_config(cfg):
 class OracleAmr:
     """C++ restatement of ``compressible::amr::Amr`` (global time step)."""
 
-    def __init__(self, sys, cfg, lo, hi, bc, init, cfl=0.4, mode=FluxMode.Hybrid, tol=1e-3, positivity=True):
+    def __init__(self, sys, cfg, lo, hi, bc, init, cfl=0.4, mode=FluxMode.Hybrid, tol=1e-3, positivity=True,
+                 subcycle=False):
         from emergence_b200.solver import _c_bcs
         L = _amr_lib()
         self.cfg = dict(cfg)
         self._c = c_amr_config(cfg)
         self._e = c_eos(sys.eos)
         self._b = _c_bcs(bc)
-        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, 0, 0)
+        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, 0, 2 if subcycle else 0)
         self._cb = make_init(init)
         lo_, hi_ = arr(lo), arr(hi)
         h = C.c_void_p()
@@ -466,6 +470,14 @@ class OracleAmr:
     def dt_cfl(self):
         v = C.c_double()
         _chk(_amr_lib().emgo_amr_dt_cfl(self._h, C.byref(v)))
+        return v.value
+
+    def step_subcycled(self, dt):
+        _chk(_amr_lib().emgo_amr_step_subcycled(self._h, float(dt)))
+
+    def dt_cfl_subcycled(self):
+        v = C.c_double()
+        _chk(_amr_lib().emgo_amr_dt_cfl_subcycled(self._h, C.byref(v)))
         return v.value
 
     def run_to(self, t_end):
@@ -507,6 +519,14 @@ class OracleAmr:
         nb, _ = self.block_count()
         out = np.zeros(nb)
         _chk(_amr_lib().emgo_amr_details(self._h, dptr(out), nb))
+        return out
+
+    def sample(self, level, g):
+        """Conserved states at level-``level`` cell coordinates g (int [n, 3]):
+        the covering leaf's data or its prediction (Amr::sample)."""
+        g = np.ascontiguousarray(g, dtype=np.int64).reshape(-1, 3)
+        out = np.zeros((len(g), 5))
+        _chk(_amr_lib().emgo_amr_sample(self._h, int(level), g.ctypes.data_as(C.POINTER(C.c_int64)), len(g), dptr(out)))
         return out
 
     @property

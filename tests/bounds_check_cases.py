@@ -66,6 +66,34 @@ def run_amr():
     return float(err.max())
 
 
+def run_amr_subcycled():
+    s, cfg, lo, hi, bc, init = W.shock_bubble(dim=2, base=4, levels=3)
+    o = O.OracleAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno, subcycle=True)
+    g = GpuAmr(s, cfg, lo, hi, bc, mode=FluxMode.Weno, blocks=(o.structure(), o.download()), subcycle=True)
+    for _ in range(3):  # a regrid after each subcycled step
+        dt = o.dt_cfl_subcycled()
+        g.step_subcycled(dt)
+        o.step_subcycled(dt)
+    st = o.structure()
+    assert np.array_equal(st, g.structure())
+    ug, uo = g.download(), o.download()
+    err = np.abs(ug - uo).reshape(-1, 5).sum(axis=0) / np.maximum(np.abs(uo).reshape(-1, 5).sum(axis=0), 1e-300)
+    assert np.all(err <= 1e-12), err
+    g.close()
+    return float(err.max())
+
+
+def run_five():
+    from emergence_b200 import GpuFiveSolver
+    sys5, mesh, u, bc = W.two_phase_shock_bubble(n=24)
+    g = GpuFiveSolver(sys5, mesh, u, bc=bc)
+    for _ in range(3):
+        g.step(g.dt_cfl())
+    assert np.all(np.isfinite(g.download()))
+    g.close()
+    return 0.0
+
+
 def run_batch():
     sys_, n, dx, u, st = W.riemann_batch(ninst=24, nmin=64, nmax=200, seed=5)
     for prec in (Precision.F64, Precision.Mixed):
@@ -80,6 +108,9 @@ def main():
     for shape, bc, mode in uniform_cases():
         print("uniform", shape, "reflect" if bc else "default", mode, "rel L1", run_uniform(shape, bc, mode), flush=True)
     print("amr 2-D shock-bubble with a regrid: rel L1", run_amr(), flush=True)
+    print("subcycled amr 2-D shock-bubble with regrids: rel L1", run_amr_subcycled(), flush=True)
+    run_five()
+    print("five-equation 3-D shock-bubble 24^3: ok", flush=True)
     run_batch()
     print("batched lines: ok", flush=True)
     print("BOUNDS_CHECK_OK")
