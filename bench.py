@@ -32,6 +32,7 @@ from emergence_b200 import replicas  # noqa: E402  (one process per GPU: barrier
 N_CELLS = 256
 CPU_STEPS = 5  # timed steps of the CPU baseline on the full grid (about 5 s each on 16 host threads)
 AMR_STEPS = 20
+AMR_SC_STEPS = 5  # subcycled steps of the AMR sub-record (each spans about four global steps)
 CELL_BYTES_3D = 320  # algorithmic bytes per 3-D cell-update (64·F, F = 5)
 # flop per interior cell and sweep launch, counted by ncu on the 160^3 explosion
 # (sm__sass_thread_inst_executed_op_{dadd,dmul,dfma,fadd,fmul,ffma}_pred_on, fma = 2)
@@ -68,6 +69,7 @@ def parse():
     ap.add_argument("--adj-n", type=int, default=512, help="adjoint workload: cells per side")
     ap.add_argument("--adj-steps", type=int, default=400, help="adjoint workload: forward steps")
     ap.add_argument("--amr-base", type=int, default=8, help="AMR base blocks per side (16^3 cells each)")
+    ap.add_argument("--subcycle", action="store_true", help="amr workload: subcycled steps (each level its own dt)")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = {"uniform": 100, "amr": 20}.get(args.workload, 3)
@@ -382,6 +384,16 @@ def sub_records(args, world, rank, local):
         rec["linf_mixed_vs_f64"] = [float(x) for x in np.abs(ia - ib).max(axis=0)]
     else:
         rec["rel_l1_mixed_vs_f64"] = "hierarchies differ after the regrids (mixed-form details moved a decision)"
+    # subcycled steps of the same workload (FP64): simulated time per second against the global step's
+    sc = measure_amr(args, world, rank, local, precision="f64", steps=AMR_SC_STEPS, warmup=1, cpu_baseline=False,
+                     subcycle=True)
+    rec["subcycled_f64"] = _compact(sc, ("value", "ms_per_step", "sim_time_per_s", "gpu_launches", "clocks"))
+    rec["subcycled_f64"]["steps"] = AMR_SC_STEPS
+    rec["subcycled_f64"]["leaves"] = sc["config"]["leaves"]
+    rec["subcycled_f64"]["leaves_per_level"] = sc["config"]["leaves_per_level"]
+    rec["subcycled_f64"]["sim_time_per_s_global_f64"] = a64["sim_time_per_s"]
+    rec["subcycled_f64"]["note"] = ("one step = one subcycled step (coarsest leaf level by dt, level l by dt/2^(l-lmin), "
+                                    "a regrid after each); value counts every level's substeps")
     out["amr"] = rec
 
     bat = {}
@@ -519,17 +531,21 @@ def reference_gpu_leg(args, sys_, mesh, u, bc, cells, ours_ms_per_step, u_ours):
 
 
 def run_amr(args, world, rank, local):
-    line = measure_amr(args, world, rank, local)
+    line = measure_amr(args, world, rank, local, subcycle=args.subcycle)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
-def measure_amr(args, world, rank, local, precision=None, steps=None, warmup=None, cpu_baseline=True, keep_state=False):
+def measure_amr(args, world, rank, local, precision=None, steps=None, warmup=None, cpu_baseline=True, keep_state=False,
+                subcycle=False):
     """3-D shock-bubble on block AMR: Mach-2 shock into a light sphere,
     16^3-cell blocks, base 8^3 blocks (128^3 cells), 3 levels (effective
     512^3), ng = 5, regrid every 4 steps, CFL 0.4. One step = one global
     SSP-RK3 step over all leaves (regrids included when due), dt from the
-    CFL reduction over the leaves each step. Returns the JSON line (on every
+    CFL reduction over the leaves each step; with subcycle, one subcycled
+    step (the coarsest leaf level by dt, level l by dt/2^(l-lmin), a regrid
+    after every such step by the reference's schedule), whose leaf
+    cell-updates count each level's substeps. Returns the JSON line (on every
     rank; rank 0 prints it); with keep_state, also the final hierarchy and
     leaf data under "_state"."""
     import numpy as np
@@ -545,14 +561,28 @@ def measure_amr(args, world, rank, local, precision=None, steps=None, warmup=Non
     prec = Precision.Mixed if precision == "mixed" else Precision.F64
     s, cfg, lo, hi, bc, init = W.shock_bubble(dim=3, base=args.amr_base, levels=3)
     t0 = time.perf_counter()
-    g = GpuAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno, cfl=0.4, precision=prec, autotune=not args.no_autotune)
+    g = GpuAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno, cfl=0.4, precision=prec, autotune=not args.no_autotune,
+               subcycle=subcycle)
     build_s = time.perf_counter() - t0
+
+    def one_step():
+        if subcycle:
+            st = g.structure()
+            lv = st[st[:, 4] == 1, 0]
+            dt = g.dt_cfl_subcycled()
+            g.step_subcycled(dt)
+            return int((2.0 ** (lv - lv.min())).sum()) * g.bcells, dt
+        n = g.block_count()[1] * g.bcells
+        dt = g.dt_cfl()
+        g.step(dt)
+        return n, dt
+
     for _ in range(warmup):
-        g.step(g.dt_cfl())
+        one_step()
     g.synchronize()
     g.phase_times()
     stream = torch.cuda.ExternalStream(g.stream())
-    leaf_cells = 0
+    leaf_cells, sim_t = 0, 0.0
     l0 = g.launch_count()
     replicas.barrier(world)
     torch.cuda.synchronize()
@@ -560,8 +590,9 @@ def measure_amr(args, world, rank, local, precision=None, steps=None, warmup=Non
     with ClockSampler(dev) as clk:
         a.record(stream)
         for _ in range(steps):
-            leaf_cells += g.block_count()[1] * g.bcells
-            g.step(g.dt_cfl())
+            n, dt = one_step()
+            leaf_cells += n
+            sim_t += dt
         b.record(stream)
         b.synchronize()
     ms = a.elapsed_time(b)
@@ -606,6 +637,8 @@ def measure_amr(args, world, rank, local, precision=None, steps=None, warmup=Non
         # domain (what a uniform grid of the finest spacing would update per step)
         "effective_cell_updates_per_s": eff_cells * steps * world / (ms * 1e-3),
         "effective_cells": eff_cells,
+        "sim_time_per_s": sim_t / (ms * 1e-3),
+        "subcycle": subcycle,
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,

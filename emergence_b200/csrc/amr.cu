@@ -1771,9 +1771,16 @@ struct emg_amr {
         if ((rc = advance_level(lmin, dt, lmin))) return rc;
         for (int l = lmin - 1; l >= 0; l--)
             if ((rc = restrict_full(l))) return rc;
+        {  // CFL rate and admissibility of the new leaf states (amr.rs:1409-1427)
+            AmrDev A = view();
+            amr_cfl<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
+                A, dleaves.p, dlevel.p, ddxl.p, ctl);
+            launches++;
+            AMR_CUDA(cudaGetLastError());
+        }
         AMR_CUDA(cudaMemcpyAsync(ctl_host, ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, stream));
         AMR_CUDA(cudaStreamSynchronize(stream));
-        rate_valid = false;
+        rate_valid = true;  // the leaves' rate; a regrid below invalidates it
         t += dt;
         steps += 1;
         if (ctl_host->status == EMG_ERR_INADMISSIBLE) return inadmissible();

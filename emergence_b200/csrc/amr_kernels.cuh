@@ -709,7 +709,11 @@ __global__ void reflux_faces(const AmrDev A, double* rhs, const double* __restri
 // stage, the CFL rate of the new state (amr.rs:1409-1427).
 // `sc`: the coefficient form of the subcycled level step (amr.rs:1869-1877,
 // a0·u0 + a1·(u + dt·r) with (a0, a1) = (0, 1), (3/4, 1/4), (1/3, 2/3)),
-// which rounds differently from the global step's in stages 1 and 3.
+// which rounds differently from the global step's in stages 1 and 3. Its
+// lists hold covered ancestors too, whose restricted data may leave the
+// admissible set at sharp interfaces (6th-order restriction overshoots)
+// without harm, so the sc form skips the stage-3 rate and admissibility
+// reduction; the leaves are checked by amr_cfl after the step.
 __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rhs, const int* __restrict__ leaves,
                        const int* __restrict__ level, const double* __restrict__ dxl, int stage, StepCtl* ctl,
                        int sc = 0) {
@@ -748,7 +752,7 @@ __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rh
             A.u[o] = v;
             un[k] = v;
         }
-        if (stage == 3) {
+        if (stage == 3 && !sc) {
             double w[5];
             to_prim(e, un, w);
             if (!admissible(e, w[0], w[4])) bad = 1;
@@ -761,7 +765,7 @@ __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rh
             rate = fmax(rate, s);
         }
     }
-    if (stage == 3) {
+    if (stage == 3 && !sc) {
         for (int o = 16; o > 0; o >>= 1) rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, o));
         __shared__ double sr[32];
         if ((threadIdx.x & 31) == 0) sr[threadIdx.x >> 5] = rate;
