@@ -61,18 +61,20 @@ def parse():
                     help="uniform workload: skip the same-box GPU baseline, the reference's own GPU kernels timed on "
                          "the same grid (oracle/_ref/librefgpu.so, built from the reference tree by "
                          "`make -C oracle refgpu`; reported as unavailable where it is not built)")
-    ap.add_argument("--workload", default="uniform", choices=["uniform", "amr", "batch", "adjoint", "batch_adjoint"],
+    ap.add_argument("--workload", default="uniform",
+                    choices=["uniform", "amr", "batch", "adjoint", "batch_adjoint", "five"],
                     help="uniform: 3-D explosion 256^3; amr: 3-D shock-bubble on block AMR (base 128^3, 3 levels); "
                          "batch: 4096 independent 1-D Riemann problems; adjoint: discrete adjoint of the 2-D "
                          "explosion 512^2 over 400 steps; batch_adjoint: gradients of the 4096 Riemann problems "
-                         "with respect to their six initial values")
+                         "with respect to their six initial values; five: five-equation two-phase shock-bubble")
+    ap.add_argument("--five-n", type=int, default=128, help="five workload: cells per side")
     ap.add_argument("--adj-n", type=int, default=512, help="adjoint workload: cells per side")
     ap.add_argument("--adj-steps", type=int, default=400, help="adjoint workload: forward steps")
     ap.add_argument("--amr-base", type=int, default=8, help="AMR base blocks per side (16^3 cells each)")
     ap.add_argument("--subcycle", action="store_true", help="amr workload: subcycled steps (each level its own dt)")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"uniform": 100, "amr": 20}.get(args.workload, 3)
+        args.steps = {"uniform": 100, "amr": 20, "five": 10}.get(args.workload, 3)
         if args.impl == "reference":
             args.steps = 3
     return args
@@ -420,7 +422,19 @@ def sub_records(args, world, rank, local):
     return out
 
 
-def measure_five(args, world, rank, local, n=128, steps=10, warmup=3):
+def run_five(args, world, rank, local):
+    rec = measure_five(args, world, rank, local, n=args.five_n, steps=args.steps, warmup=args.warmup,
+                       reference=args.reference_gpu)
+    if rank == 0:
+        line = {"metric": "cell-updates/s", "value": rec["value"], "unit": "cell-updates/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": rec["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": rec["workload"]}, "gpu_launches": rec["gpu_launches_total"],
+                "clocks": rec["clocks"], "reference_gpu": rec["reference_gpu"]}
+        print(json.dumps(line), flush=True)
+
+
+def measure_five(args, world, rank, local, n=128, steps=10, warmup=3, reference=True):
     """Five-equation two-phase shock–bubble (Kapila's model) on n^3 cells: this
     library's fused sweeps and, on the same box and grid, the reference's own
     `five` GPU kernels (the same-box baseline); each advances warmup + steps
@@ -456,7 +470,9 @@ def measure_five(args, world, rank, local, n=128, steps=10, warmup=3):
            "value": cells * steps / (ms * 1e-3), "ms_per_step": ms / steps, "gpu_launches_total": l0,
            "clocks": clk.summary()}
     from oracle import pyrefgpu
-    if pyrefgpu.available():
+    if not reference:
+        rec["reference_gpu"] = None
+    elif pyrefgpu.available():
         r = pyrefgpu.RefGpuFiveSolver(sys_, mesh, u, bc=bc, cfl=0.5, mode=FluxMode.Weno)
         r.advance(warmup)
         r.synchronize()
@@ -930,6 +946,8 @@ def main():
             run_adjoint(args, world, rank, local)
         elif args.workload == "batch_adjoint":
             run_batch_adjoint(args, world, rank, local)
+        elif args.workload == "five":
+            run_five(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -69,19 +69,35 @@ struct Five {
     __device__ __forceinline__ double drhoe_dalpha(double p) const {
         return (p + e1.gamma * e1.p_inf) / (e1.gamma - 1.0) - (p + e2.gamma * e2.p_inf) / (e2.gamma - 1.0);
     }
-    // multiphase.rs:100-110
-    __device__ __forceinline__ double rho_c2(const double* w) const {
-        double d, bb;
-        db(w, d, bb);
+    // multiphase.rs:100-110, from the closure values d, b of w and K = kapila_k(w)
+    // (every term as the reference evaluates it; the reference recomputes d and
+    // b inside rho_e, which gives the same values)
+    __device__ __forceinline__ double rho_c2_db(const double* w, double d, double b, double kk) const {
         const double p = w[F_IP];
-        double num = rho_e(w) + p;
+        double num = (w[F_IP] * d + b) + p;
 #pragma unroll
         for (int k = 0; k < 2; k++) {
             const Eos<double>& e = eos(k);
             num = num + w[k] * (e.b * (p + e.gamma * e.p_inf) / (e.gamma - 1.0) - e.q);
         }
-        num = num + kapila_k(w) * drhoe_dalpha(p);
+        num = num + kk * drhoe_dalpha(p);
         return num / d;
+    }
+    __device__ __forceinline__ double rho_c2(const double* w) const {
+        double d, b;
+        db(w, d, b);
+        return rho_c2_db(w, d, b, kapila_k(w));
+    }
+    // closure values of a primitive state, computed once where a state is
+    // tested, given a sound speed and converted to conserved variables
+    struct St {
+        double d, b, rc2;
+    };
+    __device__ __forceinline__ St state(const double* w) const {
+        St st;
+        db(w, st.d, st.b);
+        st.rc2 = rho_c2_db(w, st.d, st.b, kapila_k(w));
+        return st;
     }
     __device__ __forceinline__ static double rho(const double* w) { return w[0] + w[1]; }
     // multiphase.rs:127-130
@@ -91,8 +107,9 @@ struct Five {
         if (a > 1.0) a = 1.0;
         return a * e1.p_inf + (1.0 - a) * e2.p_inf;
     }
-    // multiphase.rs:131-146
-    __device__ __forceinline__ void to_prim(const double* u, double* w) const {
+    // multiphase.rs:131-146; d, b: the closure values of the result (db does
+    // not read the pressure)
+    __device__ __forceinline__ void to_prim_db(const double* u, double* w, double& d, double& b) const {
         const double r = u[0] + u[1];
         const double vx = u[2] / r, vy = u[3] / r, vz = u[4] / r;
         w[0] = u[0];
@@ -102,29 +119,41 @@ struct Five {
         w[4] = vz;
         w[F_IA] = u[6];
         const double rhoe = u[5] - 0.5 * r * (vx * vx + vy * vy + vz * vz);
-        double d, b;
         db(w, d, b);
         w[F_IP] = (rhoe - b) / d;
     }
+    __device__ __forceinline__ void to_prim(const double* u, double* w) const {
+        double d, b;
+        to_prim_db(u, w, d, b);
+    }
     // multiphase.rs:152-163
-    __device__ __forceinline__ void to_cons(const double* w, double* u) const {
+    __device__ __forceinline__ void to_cons_db(const double* w, double d, double b, double* u) const {
         const double r = w[0] + w[1];
         u[0] = w[0];
         u[1] = w[1];
         u[2] = r * w[2];
         u[3] = r * w[3];
         u[4] = r * w[4];
-        u[5] = rho_e(w) + 0.5 * r * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
+        u[5] = (w[F_IP] * d + b) + 0.5 * r * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
         u[6] = w[F_IA];
     }
-    __device__ __forceinline__ double sound_speed(const double* w) const { return sqrt(fmax(rho_c2(w), 0.0) / rho(w)); }
-    // multiphase.rs:345-350
-    __device__ __forceinline__ bool admissible(const double* w) const {
+    __device__ __forceinline__ void to_cons(const double* w, double* u) const {
+        double d, b;
+        db(w, d, b);
+        to_cons_db(w, d, b, u);
+    }
+    __device__ __forceinline__ static double sound_speed_rc2(const double* w, double rc2) {
+        return sqrt(fmax(rc2, 0.0) / rho(w));
+    }
+    __device__ __forceinline__ double sound_speed(const double* w) const { return sound_speed_rc2(w, rho_c2(w)); }
+    // multiphase.rs:345-350, with ρc² of w
+    __device__ __forceinline__ static bool admissible_rc2(const double* w, double rc2) {
 #pragma unroll
         for (int k = 0; k < NF; k++)
             if (!isfinite(w[k])) return false;
-        return rho(w) > 0.0 && w[F_IA] >= -0.05 && w[F_IA] <= 1.05 && rho_c2(w) > 0.0;
+        return rho(w) > 0.0 && w[F_IA] >= -0.05 && w[F_IA] <= 1.05 && rc2 > 0.0;
     }
+    __device__ __forceinline__ bool admissible(const double* w) const { return admissible_rc2(w, rho_c2(w)); }
     // multiphase.rs:331-343, from primitive w and its conserved q
     __device__ __forceinline__ static void flux_wq(const double* w, const double* q, int un, double* f) {
         const double u = w[un];
@@ -134,15 +163,17 @@ struct Five {
         f[5] = (q[5] + w[F_IP]) * u;
         f[6] = w[F_IA] * u;
     }
-    // multiphase.rs:245-289 (HLLC, Davis bounds); returns the contact speed
-    __device__ __forceinline__ double riemann(const double* wl, const double* wr, int un, double* f) const {
-        const double cl = sound_speed(wl), cr = sound_speed(wr);
+    // multiphase.rs:245-289 (HLLC, Davis bounds) with the closure values of
+    // both states; returns the contact speed
+    __device__ __forceinline__ double riemann_st(const double* wl, const double* wr, const St& stl, const St& str_,
+                                                 int un, double* f) const {
+        const double cl = sound_speed_rc2(wl, stl.rc2), cr = sound_speed_rc2(wr, str_.rc2);
         const double ul = wl[un], ur = wr[un];
         const double sl = fmin(ul - cl, ur - cr);
         const double sr = fmax(ul + cl, ur + cr);
         double ql[NF], qr[NF];
-        to_cons(wl, ql);
-        to_cons(wr, qr);
+        to_cons_db(wl, stl.d, stl.b, ql);
+        to_cons_db(wr, str_.d, str_.b, qr);
         if (sl >= 0.0) {
             flux_wq(wl, ql, un, f);
             return ul;
@@ -174,6 +205,9 @@ struct Five {
 #pragma unroll
         for (int k = 0; k < NF; k++) f[k] = fx[k] + s * (qs[k] - q[k]);
         return ss;
+    }
+    __device__ __forceinline__ double riemann(const double* wl, const double* wr, int un, double* f) const {
+        return riemann_st(wl, wr, state(wl), state(wr), un, f);
     }
     __device__ __forceinline__ double nc_coef(const double* w) const { return w[F_IA] + kapila_k(w); }
     // multiphase.rs:363-377

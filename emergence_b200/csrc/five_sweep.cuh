@@ -86,8 +86,13 @@ template <int P, int D, int MODE> struct FiveSweep {
 #pragma unroll
         for (int k = 0; k < NF; k++) avg[k] = 0.5 * (W[at<STRW>(j, k, l)] + W[at<STRW>(j + 1, k, l)]);
         const double rh = Five::rho(avg);
-        const double c = s.sound_speed(avg);
         const double kk = s.kapila_k(avg);
+        double c;
+        {
+            double d, b;
+            s.db(avg, d, b);
+            c = Five::sound_speed_rc2(avg, s.rho_c2_db(avg, d, b, kk));
+        }
         const double c2 = c * c;
         const double l0p = -avg[0] / rh / c2;
         const double l1p = -avg[1] / rh / c2;
@@ -136,15 +141,18 @@ template <int P, int D, int MODE> struct FiveSweep {
         wl[F_IA] = (r6 * cl[2] + r6 * cl[5]) + cl[6];
         wr[F_IA] = (r6 * cr[2] + r6 * cr[5]) + cr[6];
         fb = false;
-        if (!s.admissible(wl) || !s.admissible(wr)) {
+        Five::St stl = s.state(wl), str_ = s.state(wr);
+        if (!Five::admissible_rc2(wl, stl.rc2) || !Five::admissible_rc2(wr, str_.rc2)) {
             fb = true;
 #pragma unroll
             for (int k = 0; k < NF; k++) {
                 wl[k] = W[at<STRW>(j, k, l)];
                 wr[k] = W[at<STRW>(j + 1, k, l)];
             }
+            stl = s.state(wl);
+            str_ = s.state(wr);
         }
-        return s.riemann(wl, wr, UN, f);
+        return s.riemann_st(wl, wr, stl, str_, UN, f);
     }
 
     // KEEP-PE two-point flux with cached ρe (multiphase.rs:291-309)
@@ -174,15 +182,15 @@ template <int P, int D, int MODE> struct FiveSweep {
     // one-sided admissibility of the limiter (scheme.rs:408-416)
     __device__ static __forceinline__ bool lim_ok(const Five& s, const double* fx, const double* ul, const double* fl,
                                                   const double* ur, const double* fr, double lam2) {
-        double a[NF], w[NF];
+        double a[NF], w[NF], d, b;
 #pragma unroll
         for (int k = 0; k < NF; k++) a[k] = ul[k] - lam2 * (fx[k] - fl[k]);
-        s.to_prim(a, w);
-        if (!s.admissible(w)) return false;
+        s.to_prim_db(a, w, d, b);
+        if (!Five::admissible_rc2(w, s.rho_c2_db(w, d, b, s.kapila_k(w)))) return false;
 #pragma unroll
         for (int k = 0; k < NF; k++) a[k] = ur[k] + lam2 * (fx[k] - fr[k]);
-        s.to_prim(a, w);
-        return s.admissible(w);
+        s.to_prim_db(a, w, d, b);
+        return Five::admissible_rc2(w, s.rho_c2_db(w, d, b, s.kapila_k(w)));
     }
 
     __device__ static __forceinline__ double d4(double q0, double q1, double q2, double q3, double q4) {
@@ -252,13 +260,13 @@ template <int P, int D, int MODE> struct FiveSweep {
                     const int row = lo + rr;
                     const int64_t g = base0 + (int64_t)row * p.sd + s_loff[l];
                     if (s_lok[l] && in_bounds(p.ctl, g, p.ncell)) {
-                        double u[NF], w[NF];
+                        double u[NF], w[NF], d, b;
 #pragma unroll
                         for (int k = 0; k < NF; k++) u[k] = __ldg(p.uin + k * p.ncell + g);
-                        sys.to_prim(u, w);
+                        sys.to_prim_db(u, w, d, b);
 #pragma unroll
                         for (int k = 0; k < NF; k++) W[at<STRW>(row, k, l)] = w[k];
-                        if constexpr (MODE != MODE_WENO) W[at<STRW>(row, NF, l)] = sys.rho_e(w);
+                        if constexpr (MODE != MODE_WENO) W[at<STRW>(row, NF, l)] = w[F_IP] * d + b;  // ρe (multiphase.rs:71-75)
                         if constexpr (MODE == MODE_HYBRID) {
                             // sensor values (multiphase.rs:379-384)
                             W[at<STRW>(row, NF + 1, l)] = log(fmax(Five::rho(w), 1e-300));
