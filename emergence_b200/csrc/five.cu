@@ -124,9 +124,10 @@ __global__ void five_cfl_kernel(const FiveCflParams p) {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < cells; t += (int64_t)gridDim.x * blockDim.x) {
         const int64_t c[3] = {t / (p.n[1] * p.n[2]) + p.g[0], (t / p.n[2]) % p.n[1] + p.g[1], t % p.n[2] + p.g[2]};
         const int64_t q = c[0] * p.stride[0] + c[1] * p.stride[1] + c[2] * p.stride[2];
-        double uc[NF], w[NF];
+        double uc[NF], w[NF], d0, b0;
         for (int k = 0; k < NF; k++) uc[k] = p.u[k * p.ncell + q];
-        s.to_prim(uc, w);
+        s.to_prim_db(uc, w, d0, b0);
+        const double rc2 = s.rho_c2_db(w, d0, b0, s.kapila_k(w));  // once for the sound speed and the dilatation
         // a failed state: a non-finite value or a non-positive density (the
         // model's full admissibility, with its α range and ρc² > 0, is only
         // what the limiter keeps the one-sided updates in: the reference
@@ -134,7 +135,7 @@ __global__ void five_cfl_kernel(const FiveCflParams p) {
         for (int k = 0; k < NF; k++)
             if (!isfinite(w[k])) bad = 1;
         if (!(Five::rho(w) > 0.0)) bad = 1;
-        const double cs = s.sound_speed(w);
+        const double cs = Five::sound_speed_rc2(w, rc2);
         double acc = -0.0;
         for (int d = 0; d < 3; d++)
             if (p.act[d]) acc = acc + (fabs(w[F_IU + d]) + cs) / p.dx[d];
@@ -174,7 +175,7 @@ __global__ void five_cfl_kernel(const FiveCflParams p) {
             }
             divu = divu + fabs(vv[1] - vv[0]) / (2.0 * p.dx[d]);
         }
-        source = fmax(source, s.dilatation_rate(w, divu));
+        source = fmax(source, s.dilatation_rate_rc2(w, divu, rc2));
     }
     for (int o = 16; o > 0; o >>= 1) {
         rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, o));

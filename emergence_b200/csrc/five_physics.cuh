@@ -210,15 +210,18 @@ struct Five {
         return riemann_st(wl, wr, state(wl), state(wr), un, f);
     }
     __device__ __forceinline__ double nc_coef(const double* w) const { return w[F_IA] + kapila_k(w); }
-    // multiphase.rs:363-377
-    __device__ __forceinline__ double dilatation_rate(const double* w, double divu) const {
+    // multiphase.rs:363-377, with ρc² of w
+    __device__ __forceinline__ double dilatation_rate_rc2(const double* w, double divu, double rc2) const {
         const double a = w[F_IA];
         double pmin = INFINITY;
         if (a > 1e-6) pmin = fmin(pmin, e1.p_inf);
         if (1.0 - a > 1e-6) pmin = fmin(pmin, e2.p_inf);
         const double floor_ = 1e-6 * fmax(e1.p_inf, e2.p_inf);
         const double head = fmax(fmax(w[F_IP] + pmin, floor_), 1e-300);
-        return fmax(rho_c2(w), 0.0) * fabs(divu) / head;
+        return fmax(rc2, 0.0) * fabs(divu) / head;
+    }
+    __device__ __forceinline__ double dilatation_rate(const double* w, double divu) const {
+        return dilatation_rate_rc2(w, divu, rho_c2(w));
     }
     // velocity component from a conserved state (multiphase.rs:148-150)
     __device__ __forceinline__ static double velocity_conserved(const double* u, int d) { return u[2 + d] / (u[0] + u[1]); }
