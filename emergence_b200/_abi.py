@@ -128,6 +128,12 @@ SIGNATURES = {
     "emg_amr_block_count": (C.c_int, [_P, _U64, _U64]),
     "emg_amr_structure": (C.c_int, [_P, C.POINTER(C.c_int64), C.c_size_t]),
     "emg_amr_download": (C.c_int, [_P, _D, C.c_size_t]),
+    "emg_amr_create_five": (C.c_int, [C.POINTER(EmgAmrConfig), C.POINTER(EmgFiveSystem), _D, _D, C.POINTER(EmgBc7),
+                                      C.POINTER(EmgOpts), INIT_FN, C.c_void_p, C.POINTER(_P)]),
+    "emg_amr_create_five_from_blocks": (C.c_int, [C.POINTER(EmgAmrConfig), C.POINTER(EmgFiveSystem), _D, _D,
+                                                  C.POINTER(EmgBc7), C.POINTER(EmgOpts), C.POINTER(C.c_int64),
+                                                  C.c_size_t, _D, C.POINTER(_P)]),
+    "emg_amr_nv": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "emg_amr_totals": (C.c_int, [_P, _D]),
     "emg_amr_counters": (C.c_int, [_P, _U64]),
     "emg_amr_get_time": (C.c_int, [_P, _D]),

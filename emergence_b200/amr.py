@@ -1,7 +1,8 @@
 """GpuAmr: block-AMR solver on the device, mirroring compressible-cuda's
 ``GpuAmr`` (fluid/crates/compressible-cuda/src/amr.rs:95-858) together with
 the hierarchy construction of ``compressible::amr::Amr::new``
-(fluid/crates/compressible/src/amr.rs:289-344)."""
+(fluid/crates/compressible/src/amr.rs:289-344), for the Euler system or, when
+``sys`` is a FiveEq, the five-equation two-phase system (GpuSystem::FiveEq)."""
 import ctypes as C
 
 import numpy as np
@@ -23,11 +24,11 @@ def _dptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-def init_callback(fn):
-    """Wrap init(x[n,3]) -> w[n,5] (primitive state at cell centres)."""
+def init_callback(fn, nv=5):
+    """Wrap init(x[n,3]) -> w[n,nv] (primitive state at cell centres)."""
     def cb(ctx, x, n, w):
         xa = np.ctypeslib.as_array(x, shape=(n, 3)).copy()
-        np.ctypeslib.as_array(w, shape=(n, 5))[...] = fn(xa)
+        np.ctypeslib.as_array(w, shape=(n, nv))[...] = fn(xa)
     return INIT_FN(cb)
 
 
@@ -44,10 +45,17 @@ class GpuAmr:
 
     def __init__(self, sys, cfg, lo, hi, bc, init=None, cfl=0.4, mode=FluxMode.Weno, tol=1e-3, positivity=True,
                  precision=Precision.F64, blocks=None, autotune=False, subcycle=False):
+        from .five import FiveEq, _c_bcs7, _c_system
         self.cfg = dict(cfg)
         self._c = _cfg(cfg)
-        self._e = EmgEos(sys.eos.gamma, sys.eos.p_inf, sys.eos.b, sys.eos.q, sys.eos.cv)
-        self._b = _c_bcs(bc)
+        five = isinstance(sys, FiveEq)
+        self.nv = 7 if five else 5
+        if five:
+            self._e = _c_system(sys)
+            self._b = _c_bcs7(bc)
+        else:
+            self._e = EmgEos(sys.eos.gamma, sys.eos.p_inf, sys.eos.b, sys.eos.q, sys.eos.cv)
+            self._b = _c_bcs(bc)
         flags = (1 if autotune else 0) | (2 if subcycle else 0)
         self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, precision, flags)
         self._lo = np.ascontiguousarray(lo, dtype=np.float64)
@@ -56,18 +64,20 @@ class GpuAmr:
         for d in range(3):
             self.bcells *= cfg["b"] if cfg["base_blocks"][d] > 0 else 1
         h = C.c_void_p()
+        L = lib()
         if blocks is not None:
             desc, data = blocks
             desc = np.ascontiguousarray(desc, dtype=np.int64)
             data = np.ascontiguousarray(data, dtype=np.float64)
-            check(lib().emg_amr_create_from_blocks(C.byref(self._c), C.byref(self._e), _dptr(self._lo), _dptr(self._hi),
-                                                   self._b, C.byref(self._o),
-                                                   desc.ctypes.data_as(C.POINTER(C.c_int64)), desc.shape[0],
-                                                   _dptr(data), C.byref(h)))
+            create = L.emg_amr_create_five_from_blocks if five else L.emg_amr_create_from_blocks
+            check(create(C.byref(self._c), C.byref(self._e), _dptr(self._lo), _dptr(self._hi), self._b,
+                         C.byref(self._o), desc.ctypes.data_as(C.POINTER(C.c_int64)), desc.shape[0], _dptr(data),
+                         C.byref(h)))
         else:
-            self._cb = init_callback(init)
-            check(lib().emg_amr_create(C.byref(self._c), C.byref(self._e), _dptr(self._lo), _dptr(self._hi), self._b,
-                                       C.byref(self._o), self._cb, None, C.byref(h)))
+            self._cb = init_callback(init, self.nv)
+            create = L.emg_amr_create_five if five else L.emg_amr_create
+            check(create(C.byref(self._c), C.byref(self._e), _dptr(self._lo), _dptr(self._hi), self._b,
+                         C.byref(self._o), self._cb, None, C.byref(h)))
         self._h = h
 
     def close(self):
@@ -124,12 +134,12 @@ class GpuAmr:
 
     def download(self):
         nb, _ = self.block_count()
-        out = np.zeros((nb, self.bcells, 5))
+        out = np.zeros((nb, self.bcells, self.nv))
         check(lib().emg_amr_download(self._h, _dptr(out), nb))
         return out
 
     def totals(self):
-        out = np.zeros(5)
+        out = np.zeros(self.nv)
         check(lib().emg_amr_totals(self._h, _dptr(out)))
         return out
 

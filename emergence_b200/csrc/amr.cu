@@ -17,6 +17,7 @@
 // Built with -fmad=false (FP64 arithmetic rounds as the reference CPU's).
 #include "../../include/emergence_b200.h"
 #include "amr_kernels.cuh"
+#include "five_launch.h"
 #include "sweep_launch.h"
 
 #include <algorithm>
@@ -34,6 +35,11 @@ int set_error(int code, const std::string& msg);
 }
 
 using namespace emg;
+
+// the instance of an AMR kernel template for a handle's system: NVK by the
+// number of conserved variables, PHK by the system adapter
+#define NVK(kern) (nv == 7 ? kern<7> : kern<5>)
+#define PHK(kern) (nv == 7 ? kern<AmrFivePh> : kern<AmrEulerPh>)
 
 #define AMR_CUDA(call)                                                                             \
     do {                                                                                           \
@@ -110,7 +116,9 @@ struct emg_amr {
     emg_amr_config cfg{};
     emg_eos eos{};
     double lo[3]{}, hi[3]{};
-    emg_bc bc[6]{};
+    emg_bc7 bc[6]{};            // kinds and Dirichlet states (nv values)
+    int nv = 5;                 // conserved variables per cell: 5 (Euler) or 7 (five-equation system)
+    emg_five_system five{};     // the two phases of the five-equation system (nv = 7)
     emg_opts opts{};
     int act[3]{}, bd[3]{}, ext[3]{}, gof[3]{};
     std::vector<int> dims;
@@ -183,7 +191,7 @@ struct emg_amr {
     DevVec<int> dall;                  // every block, for the per-level CFL reduction
     double* usave = nullptr;           // time-view save area, pool-sized
     int64_t usave_cap = 0;
-    double *creg = nullptr, *freg = nullptr;  // flux registers, 5 × npen doubles per face
+    double *creg = nullptr, *freg = nullptr;  // flux registers, nv × npen doubles per face
     int64_t reg_cap = 0;
     unsigned long long* level_rates = nullptr;
     std::vector<double> level_t0, level_dt;
@@ -301,7 +309,7 @@ struct emg_amr {
             A.nb0[d] = nb0[d];
             for (int s = 0; s < 2; s++) {
                 A.bc[d][s] = bckind(d, s);
-                for (int k = 0; k < 5; k++) A.bcs[d][s][k] = bc[2 * d + s].state[k];
+                for (int k = 0; k < 7; k++) A.bcs[d][s][k] = k < nv ? bc[2 * d + s].state[k] : 0.0;
             }
         }
         A.ndims = (int)dims.size();
@@ -314,6 +322,8 @@ struct emg_amr {
         std::memcpy(A.wr, wr, sizeof wr);
         std::memcpy(A.wrs, wrs, sizeof wrs);
         A.eos = EosD{eos.gamma, eos.p_inf, eos.b, eos.q};
+        for (int k = 0; k < 2; k++) A.fsys.e[k] = EosD{five.eos[k].gamma, five.eos[k].p_inf, five.eos[k].b, five.eos[k].q};
+        A.fsys.kapila = five.kapila;
         A.err = err;
         return A;
     }
@@ -360,8 +370,8 @@ struct emg_amr {
         if (n <= cap) return EMG_OK;
         int64_t nc = std::max<int64_t>(n, cap + cap / 2 + 16);
         double *nu = nullptr, *nu0 = nullptr, *nr = nullptr, *nf = nullptr;
-        const size_t bytes = (size_t)nc * bcell * 5 * sizeof(double);
-        const size_t fbytes = (size_t)nc * 3 * 2 * 5 * npen * sizeof(double);
+        const size_t bytes = (size_t)nc * bcell * nv * sizeof(double);
+        const size_t fbytes = (size_t)nc * 3 * 2 * nv * npen * sizeof(double);
         if (cudaMalloc(&nu, bytes) != cudaSuccess || cudaMalloc(&nu0, bytes) != cudaSuccess ||
             cudaMalloc(&nr, bytes) != cudaSuccess || cudaMalloc(&nf, fbytes) != cudaSuccess) {
             cudaFree(nu);
@@ -376,7 +386,7 @@ struct emg_amr {
         cudaMemsetAsync(nf, 0, fbytes, stream);
         if (u) {
             // fields are strided by the capacity: copy field by field
-            for (int k = 0; k < 5; k++)
+            for (int k = 0; k < nv; k++)
                 AMR_CUDA(cudaMemcpyAsync(nu + (size_t)k * nc * bcell, u + (size_t)k * cap * bcell,
                                          (size_t)cap * bcell * sizeof(double), cudaMemcpyDeviceToDevice, stream));
         }
@@ -406,7 +416,7 @@ struct emg_amr {
             fr = 0;
         }
         const int64_t want = 2 * (int64_t)blocks.size();
-        const size_t per_block = (size_t)bcell * 5 * sizeof(double) * 3 + (size_t)3 * 2 * 5 * npen * sizeof(double);
+        const size_t per_block = (size_t)bcell * nv * sizeof(double) * 3 + (size_t)3 * 2 * nv * npen * sizeof(double);
         if (want > cap && (size_t)(want + cap) * per_block <= fr / 2 && (rc = reserve(want))) return rc;
         // the block lists of the layout and of regrids likewise, so that a
         // regrid allocates nothing (an allocation or free in the middle of a
@@ -441,7 +451,7 @@ struct emg_amr {
             cudaFree(sok[i]);
             scr[i] = nullptr;
             sok[i] = nullptr;
-            if (cudaMalloc(&scr[i], (size_t)nc * 5 * sizeof(double)) != cudaSuccess ||
+            if (cudaMalloc(&scr[i], (size_t)nc * nv * sizeof(double)) != cudaSuccess ||
                 cudaMalloc(&sok[i], (size_t)nc) != cudaSuccess) {
                 cudaGetLastError();
                 scr_cap = 0;
@@ -494,9 +504,9 @@ struct emg_amr {
 
     // one CTA per box in shared memory when the largest box stage fits; the
     // multi-launch pipeline (global scratch) otherwise
-    static size_t pbox_smem(int64_t maxcells) { return (size_t)maxcells * (2 * 5 * sizeof(double) + 1); }
+    size_t pbox_smem(int64_t maxcells) const { return (size_t)maxcells * (2 * nv * sizeof(double) + 1); }
     // (227 KB per CTA, less 1 KB for the kernel's static shared memory)
-    static bool pbox_fused_fits(int64_t maxcells) { return pbox_smem(maxcells) <= 226 * 1024; }
+    bool pbox_fused_fits(int64_t maxcells) const { return pbox_smem(maxcells) <= 226 * 1024; }
 
     int run_pboxes(const PBox* dboxes, int nbox, int64_t maxcells) {
         if (!nbox) return EMG_OK;
@@ -504,24 +514,25 @@ struct emg_amr {
         const size_t fused_smem = pbox_smem(maxcells);
         if (pbox_fused_fits(maxcells)) {
             if (!pbox_fused_ready) {
-                AMR_CUDA(cudaFuncSetAttribute(pbox_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, 226 * 1024));
+                AMR_CUDA(cudaFuncSetAttribute(pbox_fused<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, 226 * 1024));
+                AMR_CUDA(cudaFuncSetAttribute(pbox_fused<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, 226 * 1024));
                 pbox_fused_ready = true;
             }
-            pbox_fused<<<nbox, PBOX_THREADS, fused_smem, stream>>>(A, dboxes, (int)maxcells);
+            NVK(pbox_fused)<<<nbox, PBOX_THREADS, fused_smem, stream>>>(A, dboxes, (int)maxcells);
             launches++;
             AMR_CUDA(cudaGetLastError());
             return EMG_OK;
         }
         const dim3 gr = box_grid(maxcells, nbox);
-        pbox_gather<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0]);
-        for (int di = 0; di < (int)dims.size(); di++) pbox_bc<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], di);
-        pbox_fallback<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0]);
+        NVK(pbox_gather)<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0]);
+        for (int di = 0; di < (int)dims.size(); di++) NVK(pbox_bc)<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], di);
+        NVK(pbox_fallback)<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0]);
         int cur = 0;
         for (int di = 0; di < (int)dims.size(); di++) {
-            pbox_pass<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur], scr[1 - cur], di);
+            NVK(pbox_pass)<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur], scr[1 - cur], di);
             cur = 1 - cur;
         }
-        pbox_scatter<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur]);
+        NVK(pbox_scatter)<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur]);
         launches += 3 + 2 * dims.size();
         AMR_CUDA(cudaGetLastError());
         return EMG_OK;
@@ -615,20 +626,20 @@ struct emg_amr {
         AmrDev A = view();
         const dim3 gr = box_grid(maxcells, nbox);
         // boxes inside the domain: gather and first pass fused, straight into the first pass's output
-        rbox_gather_pass0<<<gr, 256, 0, stream>>>(A, dboxes, scr[1], sok[1], rem);
-        rbox_gather<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], rem, 1);
+        NVK(rbox_gather_pass0)<<<gr, 256, 0, stream>>>(A, dboxes, scr[1], sok[1], rem);
+        NVK(rbox_gather)<<<gr, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], rem, 1);
         for (int di = 0; di < (int)dims.size(); di++) {
             if (bsel && !nbsel[di]) continue;
             const dim3 gb(bsel ? (unsigned)nbsel[di] : gr.x, gr.y, 1);
-            rbox_bc<<<gb, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], di, bsel ? bsel[di] : nullptr);
+            NVK(rbox_bc)<<<gb, 256, 0, stream>>>(A, dboxes, scr[0], sok[0], di, bsel ? bsel[di] : nullptr);
             launches++;
         }
         int cur = 0;
         for (int di = 0; di < (int)dims.size(); di++) {
-            rbox_pass<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur], sok[cur], scr[1 - cur], sok[1 - cur], di, di == 0 ? 1 : 0);
+            NVK(rbox_pass)<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur], sok[cur], scr[1 - cur], sok[1 - cur], di, di == 0 ? 1 : 0);
             cur = 1 - cur;
         }
-        rbox_scatter<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur]);
+        NVK(rbox_scatter)<<<gr, 256, 0, stream>>>(A, dboxes, scr[cur]);
         launches += 3 + dims.size();
         AMR_CUDA(cudaGetLastError());
         return EMG_OK;
@@ -836,14 +847,14 @@ struct emg_amr {
     int fill_ghosts() {
         AmrDev A = view();
         if (ncopy) {
-            ghost_copy<<<ncopy, COPY_THREADS, 0, stream>>>(A, dcopy.p);
+            NVK(ghost_copy)<<<ncopy, COPY_THREADS, 0, stream>>>(A, dcopy.p);
             launches++;
         }
         int rc = run_pboxes(dpbox.p, npbox, pbox_max);
         if (rc) return rc;
         if (nbcleaves)
             for (int di = 0; di < (int)dims.size(); di++) {
-                ghost_bc<<<box_grid(2 * (int64_t)ng * std::max(bd[0], 1) * std::max(bd[1], 1), nbcleaves), 256, 0, stream>>>(
+                NVK(ghost_bc)<<<box_grid(2 * (int64_t)ng * std::max(bd[0], 1) * std::max(bd[1], 1), nbcleaves), 256, 0, stream>>>(
                     A, dbcleaves.p, dlevel.p, didx.p, di);
                 launches++;
             }
@@ -914,12 +925,53 @@ struct emg_amr {
             for (int l = 0; l < levels && l < 16; l++) p.dx_level[l] = dxl[3 * l + d];
             p.dx = dxl[d];
             p.face = face;
-            p.nface = cap * 3 * 2 * 5 * (int64_t)npen;
+            p.nface = cap * 3 * 2 * nv * (int64_t)npen;
             p.npen = npen;
             p.pen_lane_major = lane < other ? 1 : 0;
             const dim3 grid((unsigned)(nblk * p.ngroups), 1, 1);
-            cudaError_t e = opts.precision == EMG_PRECISION_MIXED ? sweep_launch_amr_mixed(P, opts.mode, p, grid, stream)
-                                                                   : sweep_launch_amr_f64(P, opts.mode, p, grid, stream);
+            cudaError_t e;
+            if (nv == 7) {
+                // the five-equation sweep with the same geometry (FP64 only)
+                FiveSweepParams q{};
+                q.uin = p.uin;
+                q.rhs = p.rhs;
+                q.ctl = p.ctl;
+                q.ncell = p.ncell;
+                q.sd = p.sd;
+                q.sl = p.sl;
+                q.so = p.so;
+                q.nd = p.nd;
+                q.nl = p.nl;
+                q.no = p.no;
+                q.gd = p.gd;
+                q.gl = p.gl;
+                q.go = p.go;
+                q.d = d;
+                q.seg = p.seg;
+                q.first = p.first;
+                q.last = 0;
+                q.stage = stage;
+                q.rows_contig = p.rows_contig;
+                q.dx = p.dx;
+                q.ndim = p.ndim;
+                q.positivity = p.positivity;
+                q.tol = p.tol;
+                q.sys = A.fsys;
+                q.leaf_slot = blk;
+                q.leaf_level = dlevel.p;
+                q.bcell = bcell;
+                q.ngroups = p.ngroups;
+                q.lw = p.lw;
+                for (int l = 0; l < 16; l++) q.dx_level[l] = p.dx_level[l];
+                q.face = face;
+                q.nface = p.nface;
+                q.npen = npen;
+                q.pen_lane_major = p.pen_lane_major;
+                e = five_sweep_launch_amr(P, opts.mode, q, grid, stream);
+            } else {
+                e = opts.precision == EMG_PRECISION_MIXED ? sweep_launch_amr_mixed(P, opts.mode, p, grid, stream)
+                                                          : sweep_launch_amr_f64(P, opts.mode, p, grid, stream);
+            }
             launches++;
             if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("AMR sweep: ") + cudaGetErrorString(e));
         }
@@ -993,7 +1045,7 @@ struct emg_amr {
             for (int bucket = 0; bucket < 6; bucket++) {
                 const int nf = rface_start[bucket + 1] - rface_start[bucket];
                 if (!nf) continue;
-                reflux_faces<<<nf, 256, 0, stream>>>(A, rhs, face, npen, dreflux.p + rface_start[bucket]);
+                NVK(reflux_faces)<<<nf, 256, 0, stream>>>(A, rhs, face, npen, dreflux.p + rface_start[bucket]);
                 launches++;
             }
             AMR_CUDA(cudaGetLastError());
@@ -1037,7 +1089,7 @@ struct emg_amr {
 
     int rk(int stage) {
         AmrDev A = view();
-        amr_rk<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
+        PHK(amr_rk)<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
             A, u0, rhs, dleaves.p, dlevel.p, ddxl.p, stage, ctl, 0);
         launches++;
         AMR_CUDA(cudaGetLastError());
@@ -1116,10 +1168,31 @@ struct emg_amr {
         return EMG_OK;
     }
 
+    // conserved variables of a five-equation primitive state (C/multiphase.rs:
+    // 152-163, the closure of :58-75), on the host for initial data
+    void five_to_cons(const double* w, double* u_) const {
+        const double al[2] = {w[6], 1.0 - w[6]};
+        double d = 0.0, b = 0.0;
+        for (int k = 0; k < 2; k++) {
+            const emg_eos& e = five.eos[k];
+            const double vol = al[k] - e.b * w[k];
+            d = d + vol / (e.gamma - 1.0);
+            b = b + e.gamma * e.p_inf * vol / (e.gamma - 1.0) + e.q * w[k];
+        }
+        const double r = w[0] + w[1];
+        u_[0] = w[0];
+        u_[1] = w[1];
+        u_[2] = r * w[2];
+        u_[3] = r * w[3];
+        u_[4] = r * w[4];
+        u_[5] = (w[5] * d + b) + 0.5 * r * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
+        u_[6] = w[6];
+    }
+
     int init_block_data(int id, emg_init_fn init, void* ictx) {
         const HBlock& b = blocks[id];
         const int64_t n = bcells();
-        std::vector<double> xs(3 * n), ws(5 * n), us(5 * n);
+        std::vector<double> xs(3 * n), ws(nv * n), us(nv * n);
         for (int64_t i = 0; i < bd[0]; i++)
             for (int64_t j = 0; j < bd[1]; j++)
                 for (int64_t k = 0; k < bd[2]; k++) {
@@ -1129,25 +1202,30 @@ struct emg_amr {
                         xs[3 * q + d] = act[d] ? lo[d] + ((double)g[d] + 0.5) * dxl[3 * b.level + d] : 0.5 * (lo[d] + hi[d]);
                 }
         init(ictx, xs.data(), n, ws.data());
-        // to_cons (C/system.rs:210-217; ρe as C/eos.rs:44-54)
         for (int64_t q = 0; q < n; q++) {
-            const double* w = &ws[5 * q];
+            const double* w = &ws[nv * q];
+            double* u_ = &us[nv * q];
+            if (nv == 7) {
+                five_to_cons(w, u_);
+                continue;
+            }
+            // to_cons (C/system.rs:210-217; ρe as C/eos.rs:44-54)
             const double rho = w[0];
             const double ke = 0.5 * rho * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
             const double v = 1.0 / rho;
             const double e = (w[4] + eos.gamma * eos.p_inf) * (v - eos.b) / (eos.gamma - 1.0) + eos.q;
-            us[5 * q] = rho;
-            us[5 * q + 1] = rho * w[1];
-            us[5 * q + 2] = rho * w[2];
-            us[5 * q + 3] = rho * w[3];
-            us[5 * q + 4] = rho * e + ke;
+            u_[0] = rho;
+            u_[1] = rho * w[1];
+            u_[2] = rho * w[2];
+            u_[3] = rho * w[3];
+            u_[4] = rho * e + ke;
         }
         // the staging buffer is reused: wait for the previous block's copy-in
         AMR_CUDA(cudaStreamSynchronize(stream));
         int rc = dstage.put(us, stream);
         if (rc) return rc;
         AmrDev A = view();
-        pool_put_interior<<<16, 256, 0, stream>>>(A, id, dstage.p);
+        NVK(pool_put_interior)<<<16, 256, 0, stream>>>(A, id, dstage.p);
         launches++;
         AMR_CUDA(cudaGetLastError());
         return EMG_OK;
@@ -1296,7 +1374,7 @@ struct emg_amr {
             AmrDev A = view();
             const int nm = (int)moves.size() / 2;
             const unsigned cy = (unsigned)std::max(1, std::min(16, 296 / nm));
-            pool_move_list<<<dim3((unsigned)nm, cy), 256, 0, stream>>>(A, dmoves.p);
+            NVK(pool_move_list)<<<dim3((unsigned)nm, cy), 256, 0, stream>>>(A, dmoves.p);
             launches++;
         }
         AMR_CUDA(cudaGetLastError());
@@ -1318,7 +1396,7 @@ struct emg_amr {
         if ((rc = grow_det((int64_t)blocks.size()))) return rc;
         AMR_CUDA(cudaMemsetAsync(det, 0, blocks.size() * sizeof(unsigned long long), stream));
         AmrDev A = view();
-        amr_detail<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
+        PHK(amr_detail)<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
             A, dleaves.p, det);
         launches++;
         AMR_CUDA(cudaGetLastError());
@@ -1486,10 +1564,24 @@ struct emg_amr {
             ctl_host->status = 0;
             AMR_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(StepCtl), cudaMemcpyHostToDevice, stream));
             AmrDev A = view();
-            amr_cfl<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
+            PHK(amr_cfl)<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
                 A, dleaves.p, dlevel.p, ddxl.p, ctl);
             launches++;
             AMR_CUDA(cudaGetLastError());
+        }
+        unsigned long long sbits = 0;
+        if (nv == 7) {
+            // the dilatation limit of the multiphase system (C/amr.rs:1426-1461)
+            int rc = ensure_layout();
+            if (rc) return rc;
+            if (!src_bits) AMR_CUDA(cudaMalloc(&src_bits, sizeof(unsigned long long)));
+            AMR_CUDA(cudaMemsetAsync(src_bits, 0, sizeof(unsigned long long), stream));
+            AmrDev A = view();
+            amr_dilatation_five<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0,
+                                  stream>>>(A, dleaves.p, dlevel.p, didx.p, ddxl.p, src_bits);
+            launches++;
+            AMR_CUDA(cudaGetLastError());
+            AMR_CUDA(cudaMemcpyAsync(&sbits, src_bits, sizeof sbits, cudaMemcpyDeviceToHost, stream));
         }
         AMR_CUDA(cudaMemcpyAsync(ctl_host, ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, stream));
         AMR_CUDA(cudaStreamSynchronize(stream));
@@ -1498,8 +1590,14 @@ struct emg_amr {
         double rate;
         std::memcpy(&rate, &ctl_host->rate_bits, sizeof rate);
         *dt = opts.cfl / rate;
+        if (nv == 7) {
+            double src;
+            std::memcpy(&src, &sbits, sizeof src);
+            if (src > 0.0) *dt = std::fmin(*dt, 0.5 / src);
+        }
         return EMG_OK;
     }
+    unsigned long long* src_bits = nullptr;  // dilatation rate of the five-equation CFL step
 
     static int inadmissible() {
         return set_error(EMG_ERR_INADMISSIBLE,
@@ -1617,8 +1715,8 @@ struct emg_amr {
             cudaFree(freg);
             creg = freg = nullptr;
             reg_cap = 0;
-            if (cudaMalloc(&creg, (size_t)want * 5 * npen * sizeof(double)) != cudaSuccess ||
-                cudaMalloc(&freg, (size_t)want * 5 * npen * sizeof(double)) != cudaSuccess) {
+            if (cudaMalloc(&creg, (size_t)want * nv * npen * sizeof(double)) != cudaSuccess ||
+                cudaMalloc(&freg, (size_t)want * nv * npen * sizeof(double)) != cudaSuccess) {
                 cudaGetLastError();
                 return set_error(EMG_ERR_CUDA, "flux register allocation failed");
             }
@@ -1628,7 +1726,7 @@ struct emg_amr {
             cudaFree(usave);
             usave = nullptr;
             usave_cap = 0;
-            if (cudaMalloc(&usave, (size_t)cap * bcell * 5 * sizeof(double)) != cudaSuccess) {
+            if (cudaMalloc(&usave, (size_t)cap * bcell * nv * sizeof(double)) != cudaSuccess) {
                 cudaGetLastError();
                 return set_error(EMG_ERR_CUDA, "time-view buffer allocation failed");
             }
@@ -1666,14 +1764,14 @@ struct emg_amr {
         ScLevel& L = sc[l];
         AmrDev A = view();
         if (L.ncopy) {
-            ghost_copy<<<L.ncopy, COPY_THREADS, 0, stream>>>(A, L.copies.p);
+            NVK(ghost_copy)<<<L.ncopy, COPY_THREADS, 0, stream>>>(A, L.copies.p);
             launches++;
         }
         int rc = run_pboxes(L.pboxes.p, L.npbox, L.pmax);
         if (rc) return rc;
         if (L.nbcl)
             for (int di = 0; di < (int)dims.size(); di++) {
-                ghost_bc<<<box_grid(2 * (int64_t)ng * std::max(bd[0], 1) * std::max(bd[1], 1), L.nbcl), 256, 0, stream>>>(
+                NVK(ghost_bc)<<<box_grid(2 * (int64_t)ng * std::max(bd[0], 1) * std::max(bd[1], 1), L.nbcl), 256, 0, stream>>>(
                     A, L.bcl.p, dlevel.p, didx.p, di);
                 launches++;
             }
@@ -1689,8 +1787,8 @@ struct emg_amr {
         level_dt[l] = dt;
         const int nf = L.face_start[6];
         if (nf) {
-            AMR_CUDA(cudaMemsetAsync(creg + (size_t)L.reg0 * 5 * npen, 0, (size_t)nf * 5 * npen * sizeof(double), stream));
-            AMR_CUDA(cudaMemsetAsync(freg + (size_t)L.reg0 * 5 * npen, 0, (size_t)nf * 5 * npen * sizeof(double), stream));
+            AMR_CUDA(cudaMemsetAsync(creg + (size_t)L.reg0 * nv * npen, 0, (size_t)nf * nv * npen * sizeof(double), stream));
+            AMR_CUDA(cudaMemsetAsync(freg + (size_t)L.reg0 * nv * npen, 0, (size_t)nf * nv * npen * sizeof(double), stream));
         }
         sc_set_dt<<<1, 1, 0, stream>>>(ctl, dt);
         launches++;
@@ -1714,25 +1812,25 @@ struct emg_amr {
                     if (th < 0.0) th = 0.0;
                     if (th > 1.0) th = 1.0;
                 }
-                sc_time_view<<<sc[l - 1].nblk, 256, 0, stream>>>(A, sc[l - 1].blist.p, u0, usave, th);
+                NVK(sc_time_view)<<<sc[l - 1].nblk, 256, 0, stream>>>(A, sc[l - 1].blist.p, u0, usave, th);
                 launches++;
             }
             if ((rc = fill_ghosts_level(l))) return rc;
             if (view_on) {
-                sc_restore<<<sc[l - 1].nblk, 256, 0, stream>>>(A, sc[l - 1].blist.p, usave);
+                NVK(sc_restore)<<<sc[l - 1].nblk, 256, 0, stream>>>(A, sc[l - 1].blist.p, usave);
                 launches++;
             }
             if ((rc = sweeps(s + 1, L.blist.p, L.nblk))) return rc;
             const double w = weights[s] * dt;
             if (nf) {
-                sc_reg_coarse<<<nf, 256, 0, stream>>>(A, L.faces.p, face, npen, creg, w);
+                NVK(sc_reg_coarse)<<<nf, 256, 0, stream>>>(A, L.faces.p, face, npen, creg, w);
                 launches++;
             }
             if (l > 0 && sc[l - 1].face_start[6]) {
-                sc_reg_fine<<<sc[l - 1].face_start[6], 256, 0, stream>>>(A, sc[l - 1].faces.p, face, npen, freg, w, nsub);
+                NVK(sc_reg_fine)<<<sc[l - 1].face_start[6], 256, 0, stream>>>(A, sc[l - 1].faces.p, face, npen, freg, w, nsub);
                 launches++;
             }
-            amr_rk<<<dim3((unsigned)L.nblk, gy), 256, 0, stream>>>(A, u0, rhs, L.blist.p, dlevel.p, ddxl.p, s + 1, ctl, 1);
+            PHK(amr_rk)<<<dim3((unsigned)L.nblk, gy), 256, 0, stream>>>(A, u0, rhs, L.blist.p, dlevel.p, ddxl.p, s + 1, ctl, 1);
             launches++;
             AMR_CUDA(cudaGetLastError());
         }
@@ -1746,7 +1844,7 @@ struct emg_amr {
             for (int bucket = 0; bucket < 6; bucket++) {
                 const int n = L.face_start[bucket + 1] - L.face_start[bucket];
                 if (!n) continue;
-                sc_reflux<<<n, 256, 0, stream>>>(A, L.faces.p + L.face_start[bucket], creg, freg, npen);
+                NVK(sc_reflux)<<<n, 256, 0, stream>>>(A, L.faces.p + L.face_start[bucket], creg, freg, npen);
                 launches++;
             }
             AMR_CUDA(cudaGetLastError());
@@ -1773,7 +1871,7 @@ struct emg_amr {
             if ((rc = restrict_full(l))) return rc;
         {  // CFL rate and admissibility of the new leaf states (amr.rs:1409-1427)
             AmrDev A = view();
-            amr_cfl<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
+            PHK(amr_cfl)<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
                 A, dleaves.p, dlevel.p, ddxl.p, ctl);
             launches++;
             AMR_CUDA(cudaGetLastError());
@@ -1807,7 +1905,7 @@ struct emg_amr {
         AMR_CUDA(cudaMemsetAsync(level_rates, 0, AMR_MAX_LEVELS * sizeof(unsigned long long), stream));
         AmrDev A = view();
         if (!blocks.empty()) {
-            sc_cfl_levels<<<(unsigned)blocks.size(), 256, 0, stream>>>(A, dall.p, dlevel.p, ddxl.p, level_rates);
+            PHK(sc_cfl_levels)<<<(unsigned)blocks.size(), 256, 0, stream>>>(A, dall.p, dlevel.p, ddxl.p, level_rates);
             launches++;
             AMR_CUDA(cudaGetLastError());
         }
@@ -1924,16 +2022,25 @@ struct emg_amr {
 
     // host part of the set-up (configuration checks, level geometry, block
     // map); no device work, so a bad configuration is reported on any host
-    int setup_host(const emg_amr_config* c, const emg_eos* e, const double* lo_, const double* hi_, const emg_bc* b,
-                   const emg_opts* o) {
+    // f5: the five-equation system (nv = 7), or null for the Euler system `e`
+    int setup_host(const emg_amr_config* c, const emg_eos* e, const emg_five_system* f5, const double* lo_,
+                   const double* hi_, const emg_bc7* b, const emg_opts* o) {
         cfg = *c;
-        eos = *e;
+        if (f5) {
+            nv = 7;
+            five = *f5;
+            eos = f5->eos[1];
+        } else {
+            eos = *e;
+        }
         opts = *o;
         for (int d = 0; d < 3; d++) {
             lo[d] = lo_[d];
             hi[d] = hi_[d];
         }
         for (int i = 0; i < 6; i++) bc[i] = b[i];
+        if (nv == 7 && opts.precision != EMG_PRECISION_F64)
+            return set_error(EMG_ERR_INVALID, "the five-equation system runs in the plain FP64 form only");
         if (cfg.b < 6 || cfg.levels < 1 || cfg.levels > AMR_MAX_LEVELS || cfg.regrid_every < 1)
             return set_error(EMG_ERR_INVALID, "invalid AMR configuration (b >= 6, 1 <= levels <= 12, regrid_every >= 1)");
         for (int i = 0; i < 6; i++) {
@@ -2022,12 +2129,13 @@ struct emg_amr {
         int rc = ddxl.put(dxl, stream);
         if (rc) return rc;
         if (sweep_prepare_device() != cudaSuccess) return set_error(EMG_ERR_CUDA, "sweep setup failed");
+        if (nv == 7 && five_sweep_prepare_device() != cudaSuccess) return set_error(EMG_ERR_CUDA, "sweep setup failed");
         return EMG_OK;
     }
 
-    int setup(const emg_amr_config* c, const emg_eos* e, const double* lo_, const double* hi_, const emg_bc* b,
-              const emg_opts* o) {
-        int rc = setup_host(c, e, lo_, hi_, b, o);
+    int setup(const emg_amr_config* c, const emg_eos* e, const emg_five_system* f5, const double* lo_,
+              const double* hi_, const emg_bc7* b, const emg_opts* o) {
+        int rc = setup_host(c, e, f5, lo_, hi_, b, o);
         return rc ? rc : setup_device();
     }
 
@@ -2051,6 +2159,7 @@ struct emg_amr {
         }
         cudaFree(det);
         cudaFree(usave);
+        cudaFree(src_bits);
         cudaFree(creg);
         cudaFree(freg);
         cudaFree(level_rates);
@@ -2089,19 +2198,30 @@ struct emg_amr {
 
 extern "C" {
 
-int emg_amr_create(const emg_amr_config* cfg, const emg_eos* eos, const double lo[3], const double hi[3],
-                   const emg_bc bc[6], const emg_opts* opts, emg_init_fn init, void* ctx, emg_amr** out) {
-    if (!cfg || !eos || !lo || !hi || !bc || !opts || !init || !out) return set_error(EMG_ERR_INVALID, "null argument");
+}  // extern "C"
+
+namespace {
+// emg_bc → emg_bc7 (5 Dirichlet values, the rest zero)
+void widen_bcs(const emg_bc* bc, emg_bc7* out) {
+    for (int i = 0; i < 6; i++) {
+        out[i] = emg_bc7{};
+        out[i].kind = bc[i].kind;
+        for (int k = 0; k < 5; k++) out[i].state[k] = bc[i].state[k];
+    }
+}
+
+// Amr::new (C/amr.rs:289-344) for either system
+int amr_create(const emg_amr_config* cfg, const emg_eos* eos, const emg_five_system* f5, const double* lo,
+               const double* hi, const emg_bc7* bc, const emg_opts* opts, emg_init_fn init, void* ctx, emg_amr** out) {
     *out = nullptr;
     emg_amr* h = new emg_amr();
-    int rc = h->setup(cfg, eos, lo, hi, bc, opts);
+    int rc = h->setup(cfg, eos, f5, lo, hi, bc, opts);
     auto bail = [&](int code) {
         h->release();
         delete h;
         return code;
     };
     if (rc) return bail(rc);
-    // Amr::new (C/amr.rs:289-344)
     for (int64_t i = 0; i < h->nb0[0]; i++)
         for (int64_t j = 0; j < h->nb0[1]; j++)
             for (int64_t k = 0; k < h->nb0[2]; k++) {
@@ -2126,10 +2246,9 @@ int emg_amr_create(const emg_amr_config* cfg, const emg_eos* eos, const double l
     return EMG_OK;
 }
 
-int emg_amr_create_from_blocks(const emg_amr_config* cfg, const emg_eos* eos, const double lo[3], const double hi[3],
-                               const emg_bc bc[6], const emg_opts* opts, const int64_t* desc, size_t nblocks,
-                               const double* u, emg_amr** out) {
-    if (!cfg || !eos || !lo || !hi || !bc || !opts || !desc || !u || !out) return set_error(EMG_ERR_INVALID, "null argument");
+int amr_create_from_blocks(const emg_amr_config* cfg, const emg_eos* eos, const emg_five_system* f5, const double* lo,
+                           const double* hi, const emg_bc7* bc, const emg_opts* opts, const int64_t* desc,
+                           size_t nblocks, const double* u, emg_amr** out) {
     *out = nullptr;
     if (nblocks == 0) return set_error(EMG_ERR_INVALID, "a hierarchy needs at least one block");
     emg_amr* h = new emg_amr();
@@ -2138,7 +2257,7 @@ int emg_amr_create_from_blocks(const emg_amr_config* cfg, const emg_eos* eos, co
         delete h;
         return code;
     };
-    int rc = h->setup_host(cfg, eos, lo, hi, bc, opts);
+    int rc = h->setup_host(cfg, eos, f5, lo, hi, bc, opts);
     if (rc) return bail(rc);
     // the hierarchy is checked on the host before any device work
     if ((rc = h->check_hierarchy(desc, nblocks))) return bail(rc);
@@ -2151,17 +2270,58 @@ int emg_amr_create_from_blocks(const emg_amr_config* cfg, const emg_eos* eos, co
         h->insert(l, k, (int)i);
     }
     const int64_t nb = h->bcells();
+    const int nv = h->nv;
     double* tmp = nullptr;
-    if (cudaMalloc(&tmp, (size_t)nb * 5 * sizeof(double)) != cudaSuccess) return bail(set_error(EMG_ERR_CUDA, "alloc"));
+    if (cudaMalloc(&tmp, (size_t)nb * nv * sizeof(double)) != cudaSuccess) return bail(set_error(EMG_ERR_CUDA, "alloc"));
     AmrDev A = h->view();
     for (size_t i = 0; i < nblocks; i++) {
-        cudaMemcpyAsync(tmp, u + i * nb * 5, (size_t)nb * 5 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
-        pool_put_interior<<<16, 256, 0, h->stream>>>(A, (int)i, tmp);
+        cudaMemcpyAsync(tmp, u + i * nb * nv, (size_t)nb * nv * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+        NVK(pool_put_interior)<<<16, 256, 0, h->stream>>>(A, (int)i, tmp);
     }
     cudaStreamSynchronize(h->stream);
     cudaFree(tmp);
     if ((rc = h->reserve_headroom())) return bail(rc);
     *out = h;
+    return EMG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int emg_amr_create(const emg_amr_config* cfg, const emg_eos* eos, const double lo[3], const double hi[3],
+                   const emg_bc bc[6], const emg_opts* opts, emg_init_fn init, void* ctx, emg_amr** out) {
+    if (!cfg || !eos || !lo || !hi || !bc || !opts || !init || !out) return set_error(EMG_ERR_INVALID, "null argument");
+    emg_bc7 b7[6];
+    widen_bcs(bc, b7);
+    return amr_create(cfg, eos, nullptr, lo, hi, b7, opts, init, ctx, out);
+}
+
+int emg_amr_create_five(const emg_amr_config* cfg, const emg_five_system* sys, const double lo[3], const double hi[3],
+                        const emg_bc7 bc[6], const emg_opts* opts, emg_init_fn init, void* ctx, emg_amr** out) {
+    if (!cfg || !sys || !lo || !hi || !bc || !opts || !init || !out) return set_error(EMG_ERR_INVALID, "null argument");
+    return amr_create(cfg, nullptr, sys, lo, hi, bc, opts, init, ctx, out);
+}
+
+int emg_amr_create_from_blocks(const emg_amr_config* cfg, const emg_eos* eos, const double lo[3], const double hi[3],
+                               const emg_bc bc[6], const emg_opts* opts, const int64_t* desc, size_t nblocks,
+                               const double* u, emg_amr** out) {
+    if (!cfg || !eos || !lo || !hi || !bc || !opts || !desc || !u || !out) return set_error(EMG_ERR_INVALID, "null argument");
+    emg_bc7 b7[6];
+    widen_bcs(bc, b7);
+    return amr_create_from_blocks(cfg, eos, nullptr, lo, hi, b7, opts, desc, nblocks, u, out);
+}
+
+int emg_amr_create_five_from_blocks(const emg_amr_config* cfg, const emg_five_system* sys, const double lo[3],
+                                    const double hi[3], const emg_bc7 bc[6], const emg_opts* opts,
+                                    const int64_t* desc, size_t nblocks, const double* u, emg_amr** out) {
+    if (!cfg || !sys || !lo || !hi || !bc || !opts || !desc || !u || !out)
+        return set_error(EMG_ERR_INVALID, "null argument");
+    return amr_create_from_blocks(cfg, nullptr, sys, lo, hi, bc, opts, desc, nblocks, u, out);
+}
+
+int emg_amr_nv(emg_amr* h, int32_t* nv) {
+    if (!h || !nv) return set_error(EMG_ERR_INVALID, "null argument");
+    *nv = h->nv;
     return EMG_OK;
 }
 
@@ -2251,11 +2411,12 @@ int emg_amr_download(emg_amr* h, double* u, size_t nblocks) {
     int rc = amr_check(h);
     if (rc) return rc;
     if (!u || nblocks < h->blocks.size()) return set_error(EMG_ERR_INVALID, "buffer too small");
-    const size_t n = h->blocks.size() * (size_t)h->bcells() * 5;
+    const int nv = h->nv;
+    const size_t n = h->blocks.size() * (size_t)h->bcells() * nv;
     double* tmp = nullptr;
     AMR_CUDA(cudaMalloc(&tmp, n * sizeof(double)));
     AmrDev A = h->view();
-    pool_get_interior<<<256, 256, 0, h->stream>>>(A, (int)h->blocks.size(), tmp);
+    NVK(pool_get_interior)<<<256, 256, 0, h->stream>>>(A, (int)h->blocks.size(), tmp);
     cudaMemcpyAsync(u, tmp, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
     cudaStreamSynchronize(h->stream);
     cudaFree(tmp);
@@ -2263,22 +2424,23 @@ int emg_amr_download(emg_amr* h, double* u, size_t nblocks) {
     return EMG_OK;
 }
 
-int emg_amr_totals(emg_amr* h, double out[5]) {
+int emg_amr_totals(emg_amr* h, double* out) {
     if (!h || !out) return set_error(EMG_ERR_INVALID, "null argument");
     // host sum in the reference order (C/amr.rs:1991-2005) over downloaded leaves
-    std::vector<double> u(h->blocks.size() * (size_t)h->bcells() * 5);
+    const int nv = h->nv;
+    std::vector<double> u(h->blocks.size() * (size_t)h->bcells() * nv);
     int rc = emg_amr_download(h, u.data(), h->blocks.size());
     if (rc) return rc;
-    double s[5] = {0, 0, 0, 0, 0};
+    double s[7] = {0, 0, 0, 0, 0, 0, 0};
     for (size_t i = 0; i < h->blocks.size(); i++) {
         if (!h->blocks[i].leaf) continue;
         double vol = 1.0;
         for (int d : h->dims) vol = vol * h->dxl[3 * h->blocks[i].level + d];
-        const double* b = &u[i * h->bcells() * 5];
+        const double* b = &u[i * h->bcells() * nv];
         for (int64_t c = 0; c < h->bcells(); c++)
-            for (int q = 0; q < 5; q++) s[q] = s[q] + b[5 * c + q] * vol;
+            for (int q = 0; q < nv; q++) s[q] = s[q] + b[nv * c + q] * vol;
     }
-    for (int q = 0; q < 5; q++) out[q] = s[q];
+    for (int q = 0; q < nv; q++) out[q] = s[q];
     return EMG_OK;
 }
 

@@ -9,6 +9,7 @@
 // (:548-586) and `restrict_box` (:622-731), so that the device hierarchy
 // evolves bit for bit like the CPU one.
 #pragma once
+#include "five_physics.cuh"
 #include "physics.cuh"
 #include <stdint.h>
 
@@ -30,11 +31,12 @@ struct AmrDev {
     const int* map;        // dense per-level block index (−1: absent)
     int64_t mapoff[AMR_MAX_LEVELS];
     int bc[3][2];
-    double bcs[3][2][5];   // Dirichlet states
+    double bcs[3][2][7];   // Dirichlet states (nv values)
     double wp[2][6];       // prediction weights by parity (amr.rs:307)
     double wr[6];          // centred restriction weights (amr.rs:308)
     double wrs[5][6];      // restriction weights by shift m (amr.rs:670-671)
-    EosD eos;
+    EosD eos;              // Euler system
+    FiveSysD fsys;         // five-equation system
     unsigned int* err;     // error word (depth overflow)
 };
 
@@ -68,6 +70,11 @@ __device__ __forceinline__ int64_t amr_cell(const AmrDev& A, const int64_t* c) {
     return ((c[0] + A.gof[0]) * A.ext[1] + (c[1] + A.gof[1])) * A.ext[2] + (c[2] + A.gof[2]);
 }
 
+// NV: conserved variables per cell (5 Euler, 7 five-equation); the first
+// momentum component is at amr_iu<NV>()
+template <int NV> __host__ __device__ constexpr int amr_iu() { return NV == 5 ? 1 : 2; }
+
+template <int NV = 5>
 __device__ __forceinline__ void amr_load(const AmrDev& A, int slot, int64_t cell, double* v) {
     if constexpr (BOUNDS_CHECK) {
         // bounds-check build: a pool index outside the pool sets bit 4 of the error word
@@ -75,16 +82,16 @@ __device__ __forceinline__ void amr_load(const AmrDev& A, int slot, int64_t cell
         if (slot < 0 || cell < 0 || cell >= A.bcell || i >= A.ntot) {
             atomicOr(A.err, 4u);
 #pragma unroll
-            for (int q = 0; q < 5; q++) v[q] = 0.0;
+            for (int q = 0; q < NV; q++) v[q] = 0.0;
             return;
         }
     }
     const double* p = A.u + (int64_t)slot * A.bcell + cell;
 #pragma unroll
-    for (int q = 0; q < 5; q++) v[q] = p[(int64_t)q * A.ntot];
+    for (int q = 0; q < NV; q++) v[q] = p[(int64_t)q * A.ntot];
 }
 
-template <int DEPTH> __device__ void amr_predict_t(const AmrDev& A, int l, const int64_t* g, double* out);
+template <int DEPTH, int NV> __device__ void amr_predict_t(const AmrDev& A, int l, const int64_t* g, double* out);
 
 // Conserved value of global cell g at level l (amr.rs:384-439). Boundary
 // kinds: periodic, outflow, reflect, Dirichlet (the characteristic kind is
@@ -92,7 +99,7 @@ template <int DEPTH> __device__ void amr_predict_t(const AmrDev& A, int l, const
 // from coarser levels (the reference recurses; with 2:1 balance and kept
 // ancestors one level suffices in practice) so that no kernel recurses; a
 // chain deeper than DEPTH sets the error word.
-template <int DEPTH>
+template <int DEPTH, int NV>
 __device__ __forceinline__ void amr_sample_t(const AmrDev& A, int l, const int64_t* g_in, double* v) {
     int64_t g[3] = {g_in[0], g_in[1], g_in[2]};
     bool flip[3] = {false, false, false};
@@ -115,7 +122,7 @@ __device__ __forceinline__ void amr_sample_t(const AmrDev& A, int l, const int64
                 flip[d] = true;
             } else {
 #pragma unroll
-                for (int q = 0; q < 5; q++) v[q] = A.bcs[d][side][q];
+                for (int q = 0; q < NV; q++) v[q] = A.bcs[d][side][q];
                 return;
             }
         }
@@ -128,19 +135,19 @@ __device__ __forceinline__ void amr_sample_t(const AmrDev& A, int l, const int64
     }
     const int id = amr_get(A, l, key);
     if (id >= 0) {
-        amr_load(A, id, amr_cell(A, c), v);
+        amr_load<NV>(A, id, amr_cell(A, c), v);
     } else {
-        amr_predict_t<DEPTH>(A, l, g, v);
+        amr_predict_t<DEPTH, NV>(A, l, g, v);
     }
 #pragma unroll
     for (int d = 0; d < 3; d++)
-        if (flip[d]) v[1 + d] = -v[1 + d];
+        if (flip[d]) v[amr_iu<NV>() + d] = -v[amr_iu<NV>() + d];
 }
 
 // Direct 6^D prediction of cell g (level l) from level l − 1 (amr.rs:589-613).
-template <int DEPTH> __device__ void amr_predict_t(const AmrDev& A, int l, const int64_t* g, double* out) {
+template <int DEPTH, int NV> __device__ void amr_predict_t(const AmrDev& A, int l, const int64_t* g, double* out) {
 #pragma unroll
-    for (int q = 0; q < 5; q++) out[q] = 0.0;
+    for (int q = 0; q < NV; q++) out[q] = 0.0;
     if constexpr (DEPTH <= 0) {
         atomicOr(A.err, 1u);
         return;
@@ -164,22 +171,23 @@ template <int DEPTH> __device__ void amr_predict_t(const AmrDev& A, int l, const
                 c[d] = base + k;
                 w = w * A.wp[odd][k];
             }
-            double v[5];
-            amr_sample_t<DEPTH - 1>(A, l - 1, c, v);
+            double v[NV];
+            amr_sample_t<DEPTH - 1, NV>(A, l - 1, c, v);
 #pragma unroll
-            for (int q = 0; q < 5; q++) out[q] = out[q] + w * v[q];
+            for (int q = 0; q < NV; q++) out[q] = out[q] + w * v[q];
         }
     }
 }
 
 constexpr int AMR_PREDICT_DEPTH = 3;
+template <int NV = 5>
 __device__ __forceinline__ void amr_sample(const AmrDev& A, int l, const int64_t* g, double* v, int) {
-    amr_sample_t<AMR_PREDICT_DEPTH>(A, l, g, v);
+    amr_sample_t<AMR_PREDICT_DEPTH, NV>(A, l, g, v);
 }
 
 // ------------------------------------------------------------------ box pipelines
 // A box is a row-major array of cells with its own size per axis; buffers
-// ping-pong between passes. `val` holds 5 doubles per cell (AoS within the
+// ping-pong between passes. `val` holds NV doubles per cell (AoS within the
 // box), `ok` one byte.
 
 // Prediction of the level-l fine box [fmin, fmax] from level l − 1

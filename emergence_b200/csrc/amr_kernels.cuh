@@ -34,6 +34,7 @@ __device__ __forceinline__ void rbox_size(const AmrDev& A, const RBox& b, int np
 // gather_box(l−1) inner cells by sampling; cells beyond a non-periodic
 // boundary are left invalid for bc_box (amr.rs:508-530). `off` is the box's
 // cell offset in buf/ok.
+template <int NV>
 __device__ __forceinline__ void pbox_gather_cell(const AmrDev& A, const PBox& b, int64_t q, double* buf,
                                                  unsigned char* ok, int64_t off) {
     const int l = b.l - 1;
@@ -46,25 +47,27 @@ __device__ __forceinline__ void pbox_gather_cell(const AmrDev& A, const PBox& b,
         const int64_t nn = amr_nlevel(A, l, d);
         if ((g[d] < 0 || g[d] >= nn) && A.bc[d][g[d] >= nn ? 1 : 0] != EMG_BC_PERIODIC) out = true;
     }
-    double* v = buf + (off + q) * 5;
+    double* v = buf + (off + q) * NV;
     if (out) {
         ok[off + q] = 0;
     } else {
-        amr_sample(A, l, g, v, 0);
+        amr_sample<NV>(A, l, g, v, 0);
         ok[off + q] = 1;
     }
 }
+template <int NV>
 __global__ void pbox_gather(const AmrDev A, const PBox* __restrict__ boxes, double* buf, unsigned char* ok) {
     const PBox b = boxes[blockIdx.x];
     const int64_t n = (int64_t)b.csz[0] * b.csz[1] * b.csz[2];
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
-        pbox_gather_cell(A, b, q, buf, ok, b.off);
+        pbox_gather_cell<NV>(A, b, q, buf, ok, b.off);
 }
 
 // bc_box sweep along active axis dims[di] over a box at level l with global
 // origin g0 (amr.rs:450-504): cells outside along that axis and inside along
 // every later one copy their (flipped) source from the same box, or take the
 // Dirichlet state.
+template <int NV>
 __device__ __forceinline__ void bc_cell(const AmrDev& A, int l, const int64_t* g0, const int* s, int64_t q, int di,
                                         double* buf, unsigned char* ok, int64_t off) {
     int64_t c[3];
@@ -81,9 +84,9 @@ __device__ __forceinline__ void bc_cell(const AmrDev& A, int l, const int64_t* g
         if (outside(A.dims[j])) return;
     const int side = g[d] >= n[d] ? 1 : 0;
     const int kind = A.bc[d][side];
-    double* dst = buf + (off + q) * 5;
+    double* dst = buf + (off + q) * NV;
     if (kind == EMG_BC_DIRICHLET) {
-        for (int k = 0; k < 5; k++) dst[k] = A.bcs[d][side][k];
+        for (int k = 0; k < NV; k++) dst[k] = A.bcs[d][side][k];
         ok[off + q] = 1;
         return;
     }
@@ -97,39 +100,43 @@ __device__ __forceinline__ void bc_cell(const AmrDev& A, int l, const int64_t* g
     if (sc[d] < 0 || sc[d] >= s[d]) return;
     const int64_t sq = box_index(sc, s);
     if (!ok[off + sq]) return;
-    const double* src = buf + (off + sq) * 5;
-    for (int k = 0; k < 5; k++) dst[k] = src[k];
-    if (kind == EMG_BC_REFLECT) dst[1 + d] = -dst[1 + d];
+    const double* src = buf + (off + sq) * NV;
+    for (int k = 0; k < NV; k++) dst[k] = src[k];
+    if (kind == EMG_BC_REFLECT) dst[amr_iu<NV>() + d] = -dst[amr_iu<NV>() + d];
     ok[off + q] = 1;
 }
 
+template <int NV>
 __global__ void pbox_bc(const AmrDev A, const PBox* __restrict__ boxes, double* buf, unsigned char* ok, int di) {
     const PBox b = boxes[blockIdx.x];
     if (!((b.bcmask >> di) & 1)) return;  // nothing of this box lies outside along dims[di]
     const int64_t n = (int64_t)b.csz[0] * b.csz[1] * b.csz[2];
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
-        bc_cell(A, b.l - 1, b.cmin, b.csz, q, di, buf, ok, b.off);
+        bc_cell<NV>(A, b.l - 1, b.cmin, b.csz, q, di, buf, ok, b.off);
 }
 
 // cells still invalid after bc_box are sampled (amr.rs:531-542)
+template <int NV>
 __device__ __forceinline__ void pbox_fallback_cell(const AmrDev& A, const PBox& b, int64_t q, double* buf,
                                                    unsigned char* ok, int64_t off) {
     if (ok[off + q]) return;
     int64_t c[3];
     box_coord(q, b.csz, c);
     const int64_t g[3] = {b.cmin[0] + c[0], b.cmin[1] + c[1], b.cmin[2] + c[2]};
-    amr_sample(A, b.l - 1, g, buf + (off + q) * 5, 0);
+    amr_sample<NV>(A, b.l - 1, g, buf + (off + q) * NV, 0);
     ok[off + q] = 1;
 }
+template <int NV>
 __global__ void pbox_fallback(const AmrDev A, const PBox* __restrict__ boxes, double* buf, unsigned char* ok) {
     const PBox b = boxes[blockIdx.x];
     const int64_t n = (int64_t)b.csz[0] * b.csz[1] * b.csz[2];
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
-        pbox_fallback_cell(A, b, q, buf, ok, b.off);
+        pbox_fallback_cell<NV>(A, b, q, buf, ok, b.off);
 }
 
 // one separable 6-point prediction pass along dims[di] (amr.rs:560-583): output
 // cell q of the box after di+1 passes from the box after di passes
+template <int NV>
 __device__ __forceinline__ void pbox_pass_cell(const AmrDev& A, const PBox& b, int di, const int* si, const int* so,
                                                int64_t q, const double* in, double* outb, int64_t off) {
     const int d = A.dims[di];
@@ -138,17 +145,18 @@ __device__ __forceinline__ void pbox_pass_cell(const AmrDev& A, const PBox& b, i
     const int64_t f = b.fmin[d] + c[d];
     const int par = (int)amr_erem(f, 2);
     const int64_t base = amr_ediv(f, 2) + (par == 1 ? -2 : -3) - b.cmin[d];
-    double acc[5] = {0, 0, 0, 0, 0};
+    double acc[NV] = {};
     for (int kk = 0; kk < 6; kk++) {
         int64_t sc[3] = {c[0], c[1], c[2]};
         sc[d] = base + kk;
-        const double* v = in + (off + box_index(sc, si)) * 5;
+        const double* v = in + (off + box_index(sc, si)) * NV;
         const double w = A.wp[par][kk];
-        for (int k = 0; k < 5; k++) acc[k] = acc[k] + w * v[k];
+        for (int k = 0; k < NV; k++) acc[k] = acc[k] + w * v[k];
     }
-    double* o = outb + (off + q) * 5;
-    for (int k = 0; k < 5; k++) o[k] = acc[k];
+    double* o = outb + (off + q) * NV;
+    for (int k = 0; k < NV; k++) o[k] = acc[k];
 }
+template <int NV>
 __global__ void pbox_pass(const AmrDev A, const PBox* __restrict__ boxes, const double* in, double* outb, int di) {
     const PBox b = boxes[blockIdx.x];
     int si[3], so[3];
@@ -156,38 +164,41 @@ __global__ void pbox_pass(const AmrDev A, const PBox* __restrict__ boxes, const 
     pbox_size(A, b, di + 1, so);
     const int64_t n = (int64_t)so[0] * so[1] * so[2];
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
-        pbox_pass_cell(A, b, di, si, so, q, in, outb, b.off);
+        pbox_pass_cell<NV>(A, b, di, si, so, q, in, outb, b.off);
 }
 
 // write the predicted fine box into its target block
+template <int NV>
 __device__ __forceinline__ void pbox_scatter_cell(const AmrDev& A, const PBox& b, int64_t q, const double* in,
                                                   int64_t off) {
     double* u = A.u + (int64_t)b.slot * A.bcell;
     int64_t c[3];
     box_coord(q, b.fsz, c);
     const int64_t cell = ((b.t0[0] + c[0]) * A.ext[1] + (b.t0[1] + c[1])) * A.ext[2] + (b.t0[2] + c[2]);
-    const double* v = in + (off + q) * 5;
-    for (int k = 0; k < 5; k++) u[(int64_t)k * A.ntot + cell] = v[k];
+    const double* v = in + (off + q) * NV;
+    for (int k = 0; k < NV; k++) u[(int64_t)k * A.ntot + cell] = v[k];
 }
+template <int NV>
 __global__ void pbox_scatter(const AmrDev A, const PBox* __restrict__ boxes, const double* in) {
     const PBox b = boxes[blockIdx.x];
     const int64_t n = (int64_t)b.fsz[0] * b.fsz[1] * b.fsz[2];
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
-        pbox_scatter_cell(A, b, q, in, b.off);
+        pbox_scatter_cell<NV>(A, b, q, in, b.off);
 }
 
 // The whole prediction pipeline of one box in shared memory (one CTA per
 // box): gather, boundary fill per active axis, fallback sampling, one
 // separable pass per active axis (ping-pong) and the scatter, with the same
 // per-cell arithmetic as the multi-launch pipeline above. `cap` is the
-// largest box stage in cells; dynamic shared memory 2·cap·5 doubles + cap bytes.
+// largest box stage in cells; dynamic shared memory 2·cap·NV doubles + cap bytes.
 // 512 threads: one CTA per box fills an SM's shared memory, so the CTA's own
 // warps are all the latency hiding the gathers get
 constexpr int PBOX_THREADS = 512;
+template <int NV>
 __global__ void __launch_bounds__(PBOX_THREADS) pbox_fused(const AmrDev A, const PBox* __restrict__ boxes, int cap) {
     extern __shared__ __align__(16) double pb_smem[];
-    double* bufs[2] = {pb_smem, pb_smem + (size_t)cap * 5};
-    unsigned char* ok = reinterpret_cast<unsigned char*>(pb_smem + (size_t)2 * cap * 5);
+    double* bufs[2] = {pb_smem, pb_smem + (size_t)cap * NV};
+    unsigned char* ok = reinterpret_cast<unsigned char*>(pb_smem + (size_t)2 * cap * NV);
     const PBox b = boxes[blockIdx.x];
     const int64_t nc = (int64_t)b.csz[0] * b.csz[1] * b.csz[2];
     // A coarse patch inside the domain that spans at most three blocks per
@@ -238,25 +249,25 @@ __global__ void __launch_bounds__(PBOX_THREADS) pbox_fused(const AmrDev A, const
                 lc[d] = o - j[d] * A.bd[d];
             }
             const int slot = s_slot[(j[0] * s_nk[1] + j[1]) * s_nk[2] + j[2]];
-            double* v = bufs[0] + q * 5;
+            double* v = bufs[0] + q * NV;
             if (slot >= 0) {
-                amr_load(A, slot, amr_cell(A, lc), v);
+                amr_load<NV>(A, slot, amr_cell(A, lc), v);
             } else {
                 const int64_t g[3] = {b.cmin[0] + c[0], b.cmin[1] + c[1], b.cmin[2] + c[2]};
-                amr_sample(A, L, g, v, 0);
+                amr_sample<NV>(A, L, g, v, 0);
             }
             ok[q] = 1;
         }
     } else {
-        for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) pbox_gather_cell(A, b, q, bufs[0], ok, 0);
+        for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) pbox_gather_cell<NV>(A, b, q, bufs[0], ok, 0);
     }
     __syncthreads();
     for (int di = 0; di < A.ndims; di++) {
         if (!((b.bcmask >> di) & 1)) continue;  // the same for the whole CTA
-        for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) bc_cell(A, b.l - 1, b.cmin, b.csz, q, di, bufs[0], ok, 0);
+        for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) bc_cell<NV>(A, b.l - 1, b.cmin, b.csz, q, di, bufs[0], ok, 0);
         __syncthreads();
     }
-    for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) pbox_fallback_cell(A, b, q, bufs[0], ok, 0);
+    for (int64_t q = threadIdx.x; q < nc; q += blockDim.x) pbox_fallback_cell<NV>(A, b, q, bufs[0], ok, 0);
     __syncthreads();
     int cur = 0;
     for (int di = 0; di < A.ndims; di++) {
@@ -264,18 +275,19 @@ __global__ void __launch_bounds__(PBOX_THREADS) pbox_fused(const AmrDev A, const
         pbox_size(A, b, di, si);
         pbox_size(A, b, di + 1, so);
         const int64_t n = (int64_t)so[0] * so[1] * so[2];
-        for (int64_t q = threadIdx.x; q < n; q += blockDim.x) pbox_pass_cell(A, b, di, si, so, q, bufs[cur], bufs[1 - cur], 0);
+        for (int64_t q = threadIdx.x; q < n; q += blockDim.x) pbox_pass_cell<NV>(A, b, di, si, so, q, bufs[cur], bufs[1 - cur], 0);
         __syncthreads();
         cur = 1 - cur;
     }
     const int64_t nf = (int64_t)b.fsz[0] * b.fsz[1] * b.fsz[2];
-    for (int64_t q = threadIdx.x; q < nf; q += blockDim.x) pbox_scatter_cell(A, b, q, bufs[cur], 0);
+    for (int64_t q = threadIdx.x; q < nf; q += blockDim.x) pbox_scatter_cell<NV>(A, b, q, bufs[cur], 0);
 }
 
 // fine patch of a restriction box with validity (amr.rs:632-663). `rem`
 // (optional) replays a batch of coarsenings in their sequential order: fine
 // block id is absent for box seq when rem[id] < seq, i.e. it was removed by an
 // earlier coarsening of the batch.
+template <int NV>
 __global__ void rbox_gather(const AmrDev A, const RBox* __restrict__ boxes, double* buf, unsigned char* ok,
                             const int* __restrict__ rem, int skip_fast) {
     const RBox b = boxes[blockIdx.x];
@@ -329,11 +341,11 @@ __global__ void rbox_gather(const AmrDev A, const RBox* __restrict__ boxes, doub
                 lc[d] = o - j[d] * A.bd[d];
             }
             const int id = s_slot[(j[0] * s_nk[1] + j[1]) * s_nk[2] + j[2]];
-            double* v = buf + (b.off + q) * 5;
+            double* v = buf + (b.off + q) * NV;
             if (id >= 0) {
-                amr_load(A, id, amr_cell(A, lc), v);
+                amr_load<NV>(A, id, amr_cell(A, lc), v);
             } else {
-                for (int k = 0; k < 5; k++) v[k] = 0.0;
+                for (int k = 0; k < NV; k++) v[k] = 0.0;
             }
             ok[b.off + q] = id >= 0 ? 1 : 0;
         }
@@ -357,7 +369,7 @@ __global__ void rbox_gather(const AmrDev A, const RBox* __restrict__ boxes, doub
                 }
             }
         }
-        double* v = buf + (b.off + q) * 5;
+        double* v = buf + (b.off + q) * NV;
         unsigned char o = 0;
         if (!out) {
             int64_t key[3], lc[3];
@@ -368,26 +380,28 @@ __global__ void rbox_gather(const AmrDev A, const RBox* __restrict__ boxes, doub
             int id = amr_get(A, lf, key);
             if (id >= 0 && rem != nullptr && b.seq >= 0 && rem[id] < b.seq) id = -1;
             if (id >= 0) {
-                amr_load(A, id, amr_cell(A, lc), v);
+                amr_load<NV>(A, id, amr_cell(A, lc), v);
                 o = 1;
             }
         }
         if (!o)
-            for (int k = 0; k < 5; k++) v[k] = 0.0;
+            for (int k = 0; k < NV; k++) v[k] = 0.0;
         ok[b.off + q] = o;
     }
 }
 
+template <int NV>
 __global__ void rbox_bc(const AmrDev A, const RBox* __restrict__ boxes, double* buf, unsigned char* ok, int di,
                         const int* __restrict__ sel) {
     const RBox b = boxes[sel ? sel[blockIdx.x] : blockIdx.x];
     const int64_t n = (int64_t)b.sz[0] * b.sz[1] * b.sz[2];
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x)
-        bc_cell(A, b.l + 1, b.f0, b.sz, q, di, buf, ok, b.off);
+        bc_cell<NV>(A, b.l + 1, b.f0, b.sz, q, di, buf, ok, b.off);
 }
 
 // one restriction pass along dims[di] with the shifted stencils and the
 // child-average fallback (amr.rs:674-727)
+template <int NV>
 __global__ void rbox_pass(const AmrDev A, const RBox* __restrict__ boxes, const double* in, const unsigned char* okin,
                           double* outb, unsigned char* okout, int di, int skip_fast) {
     const RBox b = boxes[blockIdx.x];
@@ -407,7 +421,7 @@ __global__ void rbox_pass(const AmrDev A, const RBox* __restrict__ boxes, const 
             return b.off + box_index(s2, si);
         };
         const int64_t base = 2 * c[d] + 2;
-        double acc[5] = {0, 0, 0, 0, 0};
+        double acc[NV] = {};
         bool done = false;
         for (int m = 0; m < 5 && !done; m++) {
             const int64_t st = base + shifts[m];
@@ -416,8 +430,8 @@ __global__ void rbox_pass(const AmrDev A, const RBox* __restrict__ boxes, const 
             for (int kk = 0; kk < 6; kk++) all = all && okin[at_src(st + kk)];
             if (all) {
                 for (int kk = 0; kk < 6; kk++) {
-                    const double* v = in + at_src(st + kk) * 5;
-                    for (int k = 0; k < 5; k++) acc[k] = acc[k] + A.wrs[m][kk] * v[k];
+                    const double* v = in + at_src(st + kk) * NV;
+                    for (int k = 0; k < NV; k++) acc[k] = acc[k] + A.wrs[m][kk] * v[k];
                 }
                 done = true;
             }
@@ -426,12 +440,12 @@ __global__ void rbox_pass(const AmrDev A, const RBox* __restrict__ boxes, const 
         if (!done) {
             const int64_t pa = at_src(base + 2), pb = at_src(base + 3);
             if (okin[pa] && okin[pb]) {
-                for (int k = 0; k < 5; k++) acc[k] = 0.5 * (in[pa * 5 + k] + in[pb * 5 + k]);
+                for (int k = 0; k < NV; k++) acc[k] = 0.5 * (in[pa * NV + k] + in[pb * NV + k]);
                 o = 1;
             }
         }
-        double* ov = outb + (b.off + q) * 5;
-        for (int k = 0; k < 5; k++) ov[k] = acc[k];
+        double* ov = outb + (b.off + q) * NV;
+        for (int k = 0; k < NV; k++) ov[k] = acc[k];
         okout[b.off + q] = o;
     }
 }
@@ -441,6 +455,7 @@ __global__ void rbox_pass(const AmrDev A, const RBox* __restrict__ boxes, const 
 // straight from the pool through a per-CTA table of the patch's block slots,
 // so the gathered patch never goes through global scratch. Same stencil
 // choice, validity and summation order as rbox_gather + rbox_pass.
+template <int NV>
 __global__ void rbox_gather_pass0(const AmrDev A, const RBox* __restrict__ boxes, double* outb, unsigned char* okout,
                                   const int* __restrict__ rem) {
     const RBox b = boxes[blockIdx.x];
@@ -497,7 +512,7 @@ __global__ void rbox_gather_pass0(const AmrDev A, const RBox* __restrict__ boxes
             int64_t lc[3];
             okp[i] = x >= 0 && x < sid && locate(x, lc) >= 0;
         }
-        double acc[5] = {0, 0, 0, 0, 0};
+        double acc[NV] = {};
         bool done = false;
         for (int m = 0; m < 5 && !done; m++) {
             const int st = base + shifts[m];
@@ -508,29 +523,30 @@ __global__ void rbox_gather_pass0(const AmrDev A, const RBox* __restrict__ boxes
                 for (int kk = 0; kk < 6; kk++) {
                     int64_t lc[3];
                     const int slot = locate(st + kk, lc);
-                    double v[5];
-                    amr_load(A, slot, amr_cell(A, lc), v);
-                    for (int k = 0; k < 5; k++) acc[k] = acc[k] + A.wrs[m][kk] * v[k];
+                    double v[NV];
+                    amr_load<NV>(A, slot, amr_cell(A, lc), v);
+                    for (int k = 0; k < NV; k++) acc[k] = acc[k] + A.wrs[m][kk] * v[k];
                 }
                 done = true;
             }
         }
         unsigned char o = done ? 1 : 0;
         if (!done && okp[4] && okp[5]) {  // positions base + 2, base + 3: the child average
-            double va[5], vb[5];
+            double va[NV], vb[NV];
             int64_t lc[3];
-            amr_load(A, locate(base + 2, lc), amr_cell(A, lc), va);
-            amr_load(A, locate(base + 3, lc), amr_cell(A, lc), vb);
-            for (int k = 0; k < 5; k++) acc[k] = 0.5 * (va[k] + vb[k]);
+            amr_load<NV>(A, locate(base + 2, lc), amr_cell(A, lc), va);
+            amr_load<NV>(A, locate(base + 3, lc), amr_cell(A, lc), vb);
+            for (int k = 0; k < NV; k++) acc[k] = 0.5 * (va[k] + vb[k]);
             o = 1;
         }
-        double* ov = outb + (b.off + q) * 5;
-        for (int k = 0; k < 5; k++) ov[k] = acc[k];
+        double* ov = outb + (b.off + q) * NV;
+        for (int k = 0; k < NV; k++) ov[k] = acc[k];
         okout[b.off + q] = o;
     }
 }
 
 // write the restricted box into the ancestor's interior cells [lo, hi)
+template <int NV>
 __global__ void rbox_scatter(const AmrDev A, const RBox* __restrict__ boxes, const double* in) {
     const RBox b = boxes[blockIdx.x];
     int so[3];
@@ -542,8 +558,8 @@ __global__ void rbox_scatter(const AmrDev A, const RBox* __restrict__ boxes, con
         box_coord(q, so, c);
         const int64_t ic[3] = {b.lo[0] + c[0], b.lo[1] + c[1], b.lo[2] + c[2]};
         const int64_t cell = amr_cell(A, ic);
-        const double* v = in + (b.off + q) * 5;
-        for (int k = 0; k < 5; k++) u[(int64_t)k * A.ntot + cell] = v[k];
+        const double* v = in + (b.off + q) * NV;
+        for (int k = 0; k < NV; k++) u[(int64_t)k * A.ntot + cell] = v[k];
     }
 }
 
@@ -556,6 +572,7 @@ struct CopyTask {
 // one CTA per task; the source cell is the destination cell shifted by one
 // block along the task's direction (o = 0 on inactive axes)
 constexpr int COPY_THREADS = 128;
+template <int NV>
 __global__ void __launch_bounds__(COPY_THREADS) ghost_copy(const AmrDev A, const CopyTask* __restrict__ tasks) {
     const CopyTask t = tasks[blockIdx.x];
     int rs[3], sz[3];
@@ -585,13 +602,14 @@ __global__ void __launch_bounds__(COPY_THREADS) ghost_copy(const AmrDev A, const
         const int de = ((rs[0] + c0) * e1 + rs[1] + c1) * e2 + rs[2] + c2;
         const int se = de - shift;
 #pragma unroll
-        for (int k = 0; k < 5; k++) dst[(int64_t)k * A.ntot + de] = src[(int64_t)k * A.ntot + se];
+        for (int k = 0; k < NV; k++) dst[(int64_t)k * A.ntot + de] = src[(int64_t)k * A.ntot + se];
     }
 }
 
 // bc_box over the ghost-extended box of a leaf touching the domain boundary
 // (fill_scratch → bc_box, amr.rs:1205-1217), one active axis per launch,
 // restricted to the face slabs along that axis.
+template <int NV>
 __global__ void ghost_bc(const AmrDev A, const int* __restrict__ leaves, const int* __restrict__ level,
                          const int64_t* __restrict__ idx, int di) {
     const int slot = leaves[blockIdx.x];
@@ -630,7 +648,7 @@ __global__ void ghost_bc(const AmrDev A, const int* __restrict__ leaves, const i
         const int side = g[d] >= nl[d] ? 1 : 0;
         const int kind = A.bc[d][side];
         if (kind == EMG_BC_DIRICHLET) {
-            for (int k = 0; k < 5; k++) u[(int64_t)k * A.ntot + q] = A.bcs[d][side][k];
+            for (int k = 0; k < NV; k++) u[(int64_t)k * A.ntot + q] = A.bcs[d][side][k];
             continue;
         }
         const int64_t sg = kind == EMG_BC_OUTFLOW ? (g[d] < 0 ? 0 : nl[d] - 1) : (side == 0 ? -1 - g[d] : 2 * nl[d] - 1 - g[d]);
@@ -641,9 +659,9 @@ __global__ void ghost_bc(const AmrDev A, const int* __restrict__ leaves, const i
             continue;
         }
         const int64_t sq = (sc[0] * A.ext[1] + sc[1]) * A.ext[2] + sc[2];
-        for (int k = 0; k < 5; k++) {
+        for (int k = 0; k < NV; k++) {
             double v = u[(int64_t)k * A.ntot + sq];
-            if (kind == EMG_BC_REFLECT && k == 1 + d) v = -v;
+            if (kind == EMG_BC_REFLECT && k == amr_iu<NV>() + d) v = -v;
             u[(int64_t)k * A.ntot + q] = v;
         }
     }
@@ -670,6 +688,7 @@ struct RefluxFace {
 // thread per face pen. Each cell receives at most one correction per bucket,
 // and the buckets run in the reference's (d, side) order, so every cell sums
 // its corrections in the reference's order.
+template <int NV>
 __global__ void reflux_faces(const AmrDev A, double* rhs, const double* __restrict__ face, int npen,
                              const RefluxFace* __restrict__ tasks) {
     const RefluxFace tk = tasks[blockIdx.x];
@@ -678,7 +697,7 @@ __global__ void reflux_faces(const AmrDev A, double* rhs, const double* __restri
     const int b0 = A.bd[e0], b1 = A.bd[e1];
     for (int pen = threadIdx.x; pen < b0 * b1; pen += blockDim.x) {
         const int a = pen / b1, bb = pen % b1;
-        double sum[5] = {0, 0, 0, 0, 0};
+        double sum[NV] = {};
         double cnt = 0.0;
         for (int fa = 0; fa < (A.act[e0] ? 2 : 1); fa++)
             for (int fb = 0; fb < (A.act[e1] ? 2 : 1); fb++) {
@@ -686,24 +705,70 @@ __global__ void reflux_faces(const AmrDev A, double* rhs, const double* __restri
                 const int cid = tk.fine[qa][qb];
                 if (cid < 0) continue;
                 const int la = A.act[e0] ? (2 * a + fa) % b0 : 0, lb = A.act[e1] ? (2 * bb + fb) % b1 : 0;
-                const double* fv = face + ((((int64_t)cid * 3 + d) * 2 + (1 - tk.side)) * 5) * npen + la * b1 + lb;
-                for (int k = 0; k < 5; k++) sum[k] = sum[k] + fv[(int64_t)k * npen];
+                const double* fv = face + ((((int64_t)cid * 3 + d) * 2 + (1 - tk.side)) * NV) * npen + la * b1 + lb;
+                for (int k = 0; k < NV; k++) sum[k] = sum[k] + fv[(int64_t)k * npen];
                 cnt = cnt + 1.0;
             }
         if (cnt == 0.0) continue;
-        const double* fc = face + ((((int64_t)tk.slot * 3 + d) * 2 + tk.side) * 5) * npen + pen;
+        const double* fc = face + ((((int64_t)tk.slot * 3 + d) * 2 + tk.side) * NV) * npen + pen;
         int64_t c[3];
         c[d] = tk.side == 1 ? A.bd[d] - 1 : 0;
         c[e0] = a;
         c[e1] = bb;
         double* r = rhs + (int64_t)tk.slot * A.bcell + amr_cell(A, c);
-        for (int k = 0; k < 5; k++) {
+        for (int k = 0; k < NV; k++) {
             const double df = sum[k] / cnt - fc[(int64_t)k * npen];
             const double dr = tk.side == 1 ? -df / tk.dx : df / tk.dx;
             r[(int64_t)k * A.ntot] = r[(int64_t)k * A.ntot] + dr;
         }
     }
 }
+
+// The physical system of the AMR kernels that need more than linear
+// operations on the conserved variables: primitives, a failed state, the
+// CFL speed and the regrid sensors (system.rs / multiphase.rs).
+struct AmrEulerPh {
+    static constexpr int NV = 5, NS = 2;
+    struct Ctx {
+        Eos<double> e;
+    };
+    __device__ static Ctx ctx(const AmrDev& A) { return Ctx{Eos<double>::from(A.eos)}; }
+    __device__ static void prim(const Ctx& c, const double* u, double* w) { to_prim(c.e, u, w); }
+    // inadmissible (C/eos.rs:71-80): the admissible set of the scheme
+    __device__ static bool bad(const Ctx& c, const double* w) { return !admissible(c.e, w[0], w[4]); }
+    __device__ static double sound(const Ctx& c, const double* w) { return sound_speed(c.e, w[0], w[4]); }
+    __device__ static double vel(const double* w, int d) { return w[1 + d]; }
+    // ln ρ, ln(p + p∞) (system.rs sensor)
+    __device__ static void sensor(const Ctx& c, const double* w, double* s) {
+        s[0] = log(fmax(w[0], 1e-300));
+        s[1] = log(fmax(w[4] + c.e.p_inf, 1e-300));
+    }
+};
+struct AmrFivePh {
+    static constexpr int NV = 7, NS = 3;
+    struct Ctx {
+        Five f;
+    };
+    __device__ static Ctx ctx(const AmrDev& A) { return Ctx{Five::from(A.fsys)}; }
+    __device__ static void prim(const Ctx& c, const double* u, double* w) { c.f.to_prim(u, w); }
+    // a failed state: a non-finite value or a non-positive density (the
+    // reference steps on through states slightly outside the model's
+    // admissible set, which only the limiter keeps the one-sided updates in)
+    __device__ static bool bad(const Ctx&, const double* w) {
+        bool b = !(Five::rho(w) > 0.0);
+#pragma unroll
+        for (int k = 0; k < NF; k++) b = b || !isfinite(w[k]);
+        return b;
+    }
+    __device__ static double sound(const Ctx& c, const double* w) { return c.f.sound_speed(w); }
+    __device__ static double vel(const double* w, int d) { return w[F_IU + d]; }
+    // ln ρ, ln(p + p∞ of the mixture), α1 (multiphase.rs:386-391)
+    __device__ static void sensor(const Ctx& c, const double* w, double* s) {
+        s[0] = log(fmax(Five::rho(w), 1e-300));
+        s[1] = log(fmax(w[F_IP] + c.f.p_inf_mix(w), 1e-300));
+        s[2] = w[F_IA];
+    }
+};
 
 // SSP-RK3 stage update of the leaves (amr.rs:1476-1498) and, after the third
 // stage, the CFL rate of the new state (amr.rs:1409-1427).
@@ -714,14 +779,16 @@ __global__ void reflux_faces(const AmrDev A, double* rhs, const double* __restri
 // admissible set at sharp interfaces (6th-order restriction overshoots)
 // without harm, so the sc form skips the stage-3 rate and admissibility
 // reduction; the leaves are checked by amr_cfl after the step.
+template <class PH>
 __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rhs, const int* __restrict__ leaves,
                        const int* __restrict__ level, const double* __restrict__ dxl, int stage, StepCtl* ctl,
-                       int sc = 0) {
+                       int sc) {
+    constexpr int NV = PH::NV;
     const int slot = leaves[blockIdx.x];
     const int l = level[slot];
     const double dt = ctl->dt;
     const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
-    const Eos<double> e = Eos<double>::from(A.eos);
+    const typename PH::Ctx e = PH::ctx(A);
     double rate = 0.0;
     int bad = 0;  // a non-finite or inadmissible new leaf state (stage 3)
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
@@ -736,8 +803,8 @@ __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rh
                 continue;
             }
         }
-        double un[5];
-        for (int k = 0; k < 5; k++) {
+        double un[NV];
+        for (int k = 0; k < NV; k++) {
             const int64_t o = (int64_t)k * A.ntot + cell;
             const double uu = A.u[o], r = rhs[o];
             double v;
@@ -753,14 +820,14 @@ __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rh
             un[k] = v;
         }
         if (stage == 3 && !sc) {
-            double w[5];
-            to_prim(e, un, w);
-            if (!admissible(e, w[0], w[4])) bad = 1;
-            const double cs = sound_speed(e, w[0], w[4]);
+            double w[NV];
+            PH::prim(e, un, w);
+            if (PH::bad(e, w)) bad = 1;
+            const double cs = PH::sound(e, w);
             double s = -0.0;
             for (int i = 0; i < A.ndims; i++) {
                 const int d = A.dims[i];
-                s = s + (fabs(w[1 + d]) + cs) / dxl[3 * l + d];
+                s = s + (fabs(PH::vel(w, d)) + cs) / dxl[3 * l + d];
             }
             rate = fmax(rate, s);
         }
@@ -780,26 +847,28 @@ __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rh
 }
 
 // CFL rate of the current leaves (amr.rs:1409-1427)
+template <class PH>
 __global__ void amr_cfl(const AmrDev A, const int* __restrict__ leaves, const int* __restrict__ level,
                         const double* __restrict__ dxl, StepCtl* ctl) {
+    constexpr int NV = PH::NV;
     const int slot = leaves[blockIdx.x];
     const int l = level[slot];
     const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
-    const Eos<double> e = Eos<double>::from(A.eos);
+    const typename PH::Ctx e = PH::ctx(A);
     double rate = 0.0;
     int bad = 0;  // a non-finite or inadmissible leaf cell
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
         int64_t c[3];
         box_coord(q, A.bd, c);
-        double uu[5], w[5];
-        amr_load(A, slot, amr_cell(A, c), uu);
-        to_prim(e, uu, w);
-        if (!admissible(e, w[0], w[4])) bad = 1;
-        const double cs = sound_speed(e, w[0], w[4]);
+        double uu[NV], w[NV];
+        amr_load<NV>(A, slot, amr_cell(A, c), uu);
+        PH::prim(e, uu, w);
+        if (PH::bad(e, w)) bad = 1;
+        const double cs = PH::sound(e, w);
         double s = -0.0;
         for (int i = 0; i < A.ndims; i++) {
             const int d = A.dims[i];
-            s = s + (fabs(w[1 + d]) + cs) / dxl[3 * l + d];
+            s = s + (fabs(PH::vel(w, d)) + cs) / dxl[3 * l + d];
         }
         rate = fmax(rate, s);
     }
@@ -815,6 +884,58 @@ __global__ void amr_cfl(const AmrDev A, const int* __restrict__ leaves, const in
     }
 }
 
+// Dilatation limit of the five-equation CFL step over the leaves
+// (dt_cfl, amr.rs:1426-1461): per cell the rate ρc²|∇·u| / (p + p∞ head)
+// with ∇·u from the primitive velocities of the two neighbours along each
+// active axis, read in the block or, across a block face, sampled from the
+// hierarchy (the block's neighbour or its prediction). Max into *src_bits.
+__global__ void amr_dilatation_five(const AmrDev A, const int* __restrict__ leaves, const int* __restrict__ level,
+                                    const int64_t* __restrict__ idx, const double* __restrict__ dxl,
+                                    unsigned long long* src_bits) {
+    const int slot = leaves[blockIdx.x];
+    const int l = level[slot];
+    const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
+    const Five f = Five::from(A.fsys);
+    double src = 0.0;
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        box_coord(q, A.bd, c);
+        double uu[NF], w[NF];
+        amr_load<NF>(A, slot, amr_cell(A, c), uu);
+        f.to_prim(uu, w);
+        double divu = 0.0;
+        for (int i = 0; i < A.ndims; i++) {
+            const int d = A.dims[i];
+            double vv[2];
+            for (int hi = 0; hi < 2; hi++) {
+                int64_t cc[3] = {c[0], c[1], c[2]};
+                cc[d] += hi ? 1 : -1;
+                double un[NF], wn[NF];
+                if (cc[d] >= 0 && cc[d] < A.bd[d]) {
+                    amr_load<NF>(A, slot, amr_cell(A, cc), un);
+                } else {
+                    int64_t g[3];
+                    for (int e = 0; e < 3; e++) g[e] = idx[3 * slot + e] * A.bd[e] + cc[e];
+                    amr_sample<NF>(A, l, g, un, 0);
+                }
+                f.to_prim(un, wn);
+                vv[hi] = wn[F_IU + d];
+            }
+            divu = divu + fabs(vv[1] - vv[0]) / (2.0 * dxl[3 * l + d]);
+        }
+        src = fmax(src, f.dilatation_rate(w, divu));
+    }
+    for (int o = 16; o > 0; o >>= 1) src = fmax(src, __shfl_xor_sync(0xffffffffu, src, o));
+    __shared__ double sr[32];
+    if ((threadIdx.x & 31) == 0) sr[threadIdx.x >> 5] = src;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = sr[0];
+        for (int w2 = 1; w2 < (int)(blockDim.x >> 5); w2++) v = fmax(v, sr[w2]);
+        if (!isnan(v) && v > 0.0) atomicMax(src_bits, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
 // ---------------------------------------------------------------- subcycling
 // (amr.rs:1654-1954). One CTA per block of a level list, threads over the
 // block's interior cells.
@@ -825,6 +946,7 @@ __global__ void sc_set_dt(StepCtl* ctl, double dt) { ctl->dt = dt; }
 // Level-l data as its linear interpolation in time, u ← (1−θ)·u0 + θ·u, the
 // current data kept in `usave` (set_time_view, amr.rs:1702-1716); the ghost
 // prediction of level l+1 reads block interiors only.
+template <int NV>
 __global__ void sc_time_view(const AmrDev A, const int* __restrict__ blist, const double* __restrict__ u0,
                              double* __restrict__ usave, double th) {
     const int slot = blist[blockIdx.x];
@@ -839,7 +961,7 @@ __global__ void sc_time_view(const AmrDev A, const int* __restrict__ blist, cons
                 continue;
             }
         }
-        for (int k = 0; k < 5; k++) {
+        for (int k = 0; k < NV; k++) {
             const int64_t o = (int64_t)k * A.ntot + cell;
             const double uu = A.u[o];
             usave[o] = uu;
@@ -849,6 +971,7 @@ __global__ void sc_time_view(const AmrDev A, const int* __restrict__ blist, cons
 }
 
 // restore_time_view (amr.rs:1718-1723)
+template <int NV>
 __global__ void sc_restore(const AmrDev A, const int* __restrict__ blist, const double* __restrict__ usave) {
     const int slot = blist[blockIdx.x];
     const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
@@ -862,13 +985,13 @@ __global__ void sc_restore(const AmrDev A, const int* __restrict__ blist, const 
                 continue;
             }
         }
-        for (int k = 0; k < 5; k++) A.u[(int64_t)k * A.ntot + cell] = usave[(int64_t)k * A.ntot + cell];
+        for (int k = 0; k < NV; k++) A.u[(int64_t)k * A.ntot + cell] = usave[(int64_t)k * A.ntot + cell];
     }
 }
 
 // A coarse–fine face of a level-l leaf whose same-level neighbour across
 // (d, side) is refined (amr.rs:1725-1760, kind 0): its flux registers are rows
-// `reg` of the register arrays (5 fields × npen face cells), fine[qa][qb] the
+// `reg` of the register arrays (NV fields × npen face cells), fine[qa][qb] the
 // adjacent level-(l+1) leaves per quarter of the face (−1: none).
 struct ScFace {
     int slot, d, side, reg;
@@ -877,20 +1000,22 @@ struct ScFace {
 };
 
 // coarse side: creg += w·F over the face (amr.rs:1774-1781)
+template <int NV>
 __global__ void sc_reg_coarse(const AmrDev A, const ScFace* __restrict__ tasks, const double* __restrict__ face, int npen,
                               double* creg, double w) {
     const ScFace tk = tasks[blockIdx.x];
     const int e0 = tk.d == 0 ? 1 : 0, e1 = tk.d == 2 ? 1 : 2;
     const int nf = A.bd[e0] * A.bd[e1];
     for (int pen = threadIdx.x; pen < nf; pen += blockDim.x) {
-        const double* f = face + ((((int64_t)tk.slot * 3 + tk.d) * 2 + tk.side) * 5) * npen + pen;
-        double* r = creg + (int64_t)tk.reg * 5 * npen + pen;
-        for (int k = 0; k < 5; k++) r[(int64_t)k * npen] = r[(int64_t)k * npen] + w * f[(int64_t)k * npen];
+        const double* f = face + ((((int64_t)tk.slot * 3 + tk.d) * 2 + tk.side) * NV) * npen + pen;
+        double* r = creg + (int64_t)tk.reg * NV * npen + pen;
+        for (int k = 0; k < NV; k++) r[(int64_t)k * npen] = r[(int64_t)k * npen] + w * f[(int64_t)k * npen];
     }
 }
 
 // fine side: freg += w·F/nsub for the 2^(D−1) fine faces of each coarse face
 // cell, in the order of the fine block's face loop (amr.rs:1782-1800)
+template <int NV>
 __global__ void sc_reg_fine(const AmrDev A, const ScFace* __restrict__ tasks, const double* __restrict__ face, int npen,
                             double* freg, double w, double nsub) {
     const ScFace tk = tasks[blockIdx.x];
@@ -899,21 +1024,22 @@ __global__ void sc_reg_fine(const AmrDev A, const ScFace* __restrict__ tasks, co
     const int b0 = A.bd[e0], b1 = A.bd[e1];
     for (int pen = threadIdx.x; pen < b0 * b1; pen += blockDim.x) {
         const int a = pen / b1, bb = pen % b1;
-        double* r = freg + (int64_t)tk.reg * 5 * npen + pen;
+        double* r = freg + (int64_t)tk.reg * NV * npen + pen;
         for (int fa = 0; fa < (A.act[e0] ? 2 : 1); fa++)
             for (int fb = 0; fb < (A.act[e1] ? 2 : 1); fb++) {
                 const int qa = A.act[e0] ? (2 * a + fa) / b0 : 0, qb = A.act[e1] ? (2 * bb + fb) / b1 : 0;
                 const int cid = tk.fine[qa][qb];
                 if (cid < 0) continue;
                 const int la = A.act[e0] ? (2 * a + fa) % b0 : 0, lb = A.act[e1] ? (2 * bb + fb) % b1 : 0;
-                const double* fv = face + ((((int64_t)cid * 3 + d) * 2 + (1 - tk.side)) * 5) * npen + la * b1 + lb;
-                for (int k = 0; k < 5; k++) r[(int64_t)k * npen] = r[(int64_t)k * npen] + w * fv[(int64_t)k * npen] / nsub;
+                const double* fv = face + ((((int64_t)cid * 3 + d) * 2 + (1 - tk.side)) * NV) * npen + la * b1 + lb;
+                for (int k = 0; k < NV; k++) r[(int64_t)k * npen] = r[(int64_t)k * npen] + w * fv[(int64_t)k * npen] / nsub;
             }
     }
 }
 
 // reflux_level (amr.rs:1809-1834): u += ±(freg − creg)/dx on the face cells
 // that received fine fluxes; launched per (d, side) bucket in order
+template <int NV>
 __global__ void sc_reflux(const AmrDev A, const ScFace* __restrict__ tasks, const double* __restrict__ creg,
                           const double* __restrict__ freg, int npen) {
     const ScFace tk = tasks[blockIdx.x];
@@ -935,9 +1061,9 @@ __global__ void sc_reflux(const AmrDev A, const ScFace* __restrict__ tasks, cons
                 continue;
             }
         }
-        const double* fr = freg + (int64_t)tk.reg * 5 * npen + pen;
-        const double* cr = creg + (int64_t)tk.reg * 5 * npen + pen;
-        for (int k = 0; k < 5; k++) {
+        const double* fr = freg + (int64_t)tk.reg * NV * npen + pen;
+        const double* cr = creg + (int64_t)tk.reg * NV * npen + pen;
+        for (int k = 0; k < NV; k++) {
             const double df = fr[(int64_t)k * npen] - cr[(int64_t)k * npen];
             double* uo = A.u + (int64_t)k * A.ntot + cell;
             *uo = *uo + (tk.side == 1 ? -df / tk.dx : df / tk.dx);
@@ -947,24 +1073,26 @@ __global__ void sc_reflux(const AmrDev A, const ScFace* __restrict__ tasks, cons
 
 // CFL rate of every block of a list (leaves and ancestors), reduced per level
 // (dt_cfl_level, amr.rs:1657-1679)
+template <class PH>
 __global__ void sc_cfl_levels(const AmrDev A, const int* __restrict__ blist, const int* __restrict__ level,
                               const double* __restrict__ dxl, unsigned long long* rate_bits) {
+    constexpr int NV = PH::NV;
     const int slot = blist[blockIdx.x];
     const int l = level[slot];
     const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
-    const Eos<double> e = Eos<double>::from(A.eos);
+    const typename PH::Ctx e = PH::ctx(A);
     double rate = 0.0;
     for (int64_t q = threadIdx.x; q < n; q += blockDim.x) {
         int64_t c[3];
         box_coord(q, A.bd, c);
-        double uu[5], w[5];
-        amr_load(A, slot, amr_cell(A, c), uu);
-        to_prim(e, uu, w);
-        const double cs = sound_speed(e, w[0], w[4]);
+        double uu[NV], w[NV];
+        amr_load<NV>(A, slot, amr_cell(A, c), uu);
+        PH::prim(e, uu, w);
+        const double cs = PH::sound(e, w);
         double sp = -0.0;
         for (int i = 0; i < A.ndims; i++) {
             const int d = A.dims[i];
-            sp = sp + (fabs(w[1 + d]) + cs) / dxl[3 * l + d];
+            sp = sp + (fabs(PH::vel(w, d)) + cs) / dxl[3 * l + d];
         }
         rate = fmax(rate, sp);
     }
@@ -979,19 +1107,22 @@ __global__ void sc_cfl_levels(const AmrDev A, const int* __restrict__ blist, con
     }
 }
 
-// Largest relative wavelet detail of each leaf on the sensors ln ρ, ln(p+p∞)
+// Largest relative wavelet detail of each leaf on the system's sensors
 // (block_detail, amr.rs:823-867), over its filled ghost-extended box.
-__device__ __forceinline__ void amr_sensor(const AmrDev& A, const Eos<double>& e, const double* u, int64_t cell, double* s) {
-    double q[5], w[5];
-    for (int k = 0; k < 5; k++) q[k] = u[(int64_t)k * A.ntot + cell];
-    to_prim(e, q, w);
-    s[0] = log(fmax(w[0], 1e-300));
-    s[1] = log(fmax(w[4] + e.p_inf, 1e-300));
+template <class PH>
+__device__ __forceinline__ void amr_sensor(const AmrDev& A, const typename PH::Ctx& e, const double* u, int64_t cell,
+                                           double* s) {
+    double q[PH::NV], w[PH::NV];
+    for (int k = 0; k < PH::NV; k++) q[k] = u[(int64_t)k * A.ntot + cell];
+    PH::prim(e, q, w);
+    PH::sensor(e, w, s);
 }
+template <class PH>
 __global__ void amr_detail(const AmrDev A, const int* __restrict__ leaves, unsigned long long* det_bits) {
+    constexpr int NS = PH::NS;
     const int slot = leaves[blockIdx.x];
     const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
-    const Eos<double> e = Eos<double>::from(A.eos);
+    const typename PH::Ctx e = PH::ctx(A);
     const double* u = A.u + (int64_t)slot * A.bcell;
     const int offs[6] = {-5, -3, -1, 1, 3, 5};
     double mx = 0.0;
@@ -999,18 +1130,19 @@ __global__ void amr_detail(const AmrDev A, const int* __restrict__ leaves, unsig
         int64_t c[3];
         box_coord(q, A.bd, c);
         const int64_t cell = amr_cell(A, c);
-        double s0[2];
-        amr_sensor(A, e, u, cell, s0);
+        double s0[NS];
+        amr_sensor<PH>(A, e, u, cell, s0);
         for (int i = 0; i < A.ndims; i++) {
             const int d = A.dims[i];
             const int64_t stride = d == 0 ? (int64_t)A.ext[1] * A.ext[2] : (d == 1 ? A.ext[2] : 1);
-            double pred[2] = {0.0, 0.0};
+            double pred[NS];
+            for (int k = 0; k < NS; k++) pred[k] = 0.0;
             for (int m = 0; m < 6; m++) {
-                double sv[2];
-                amr_sensor(A, e, u, cell + offs[m] * stride, sv);
-                for (int k = 0; k < 2; k++) pred[k] = pred[k] + A.wr[m] * sv[k];
+                double sv[NS];
+                amr_sensor<PH>(A, e, u, cell + offs[m] * stride, sv);
+                for (int k = 0; k < NS; k++) pred[k] = pred[k] + A.wr[m] * sv[k];
             }
-            for (int k = 0; k < 2; k++) {
+            for (int k = 0; k < NS; k++) {
                 const double dd = fabs(s0[k] - pred[k]);
                 mx = isfinite(dd) ? fmax(mx, dd) : INFINITY;
             }
@@ -1031,25 +1163,28 @@ __global__ void amr_detail(const AmrDev A, const int* __restrict__ leaves, unsig
 // block moves (to, from) of the swap-removes of a batch of coarsenings
 // (amr.rs:1024-1031): every source lies above every
 // destination, so the moves are independent. grid = (moves, chunks of cells)
+template <int NV>
 __global__ void pool_move_list(const AmrDev A, const int* __restrict__ moves) {
     const int to = moves[2 * blockIdx.x], from = moves[2 * blockIdx.x + 1];
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < A.bcell; q += (int64_t)gridDim.y * blockDim.x)
-        for (int k = 0; k < 5; k++)
+        for (int k = 0; k < NV; k++)
             A.u[(int64_t)k * A.ntot + (int64_t)to * A.bcell + q] = A.u[(int64_t)k * A.ntot + (int64_t)from * A.bcell + q];
 }
 
 // interior cells of one block from host AoS data (initial condition)
+template <int NV>
 __global__ void pool_put_interior(const AmrDev A, int slot, const double* __restrict__ aos) {
     const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
         int64_t c[3];
         box_coord(q, A.bd, c);
         const int64_t cell = (int64_t)slot * A.bcell + amr_cell(A, c);
-        for (int k = 0; k < 5; k++) A.u[(int64_t)k * A.ntot + cell] = aos[5 * q + k];
+        for (int k = 0; k < NV; k++) A.u[(int64_t)k * A.ntot + cell] = aos[NV * q + k];
     }
 }
 
-// interior cells of all blocks into AoS [block][cell][5]
+// interior cells of all blocks into AoS [block][cell][NV]
+template <int NV>
 __global__ void pool_get_interior(const AmrDev A, int nblocks, double* __restrict__ aos) {
     const int64_t nb = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
     const int64_t n = nb * nblocks;
@@ -1058,7 +1193,7 @@ __global__ void pool_get_interior(const AmrDev A, int nblocks, double* __restric
         int64_t c[3];
         box_coord(q, A.bd, c);
         const int64_t cell = slot * A.bcell + amr_cell(A, c);
-        for (int k = 0; k < 5; k++) aos[5 * t + k] = A.u[(int64_t)k * A.ntot + cell];
+        for (int k = 0; k < NV; k++) aos[NV * t + k] = A.u[(int64_t)k * A.ntot + cell];
     }
 }
 

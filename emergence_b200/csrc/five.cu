@@ -12,7 +12,7 @@
 //
 // Built with -fmad=false.
 #include "../../include/emergence_b200.h"
-#include "five_sweep.cuh"
+#include "five_launch.h"
 #include "uniform_internal.h"
 
 #include <algorithm>
@@ -282,10 +282,51 @@ template <int P, int MODE> cudaError_t five_attr_d() {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(five_sweep_kernel<P, 2, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     return e;
 }
+// batched block-AMR leaves: one CTA per (leaf, group of block rows), P = 16 or 32
+template <int P, int D, int MODE>
+__global__ void __launch_bounds__(SWEEP_THREADS, 2) five_sweep_amr_kernel(const FiveSweepParams p) {
+    FiveSweep<P, D, MODE, true>::run(p);
+}
+template <int P, int MODE> cudaError_t five_launch_amr_d(const FiveSweepParams& p, dim3 grid, cudaStream_t s) {
+    const size_t b = FiveSmem<P, MODE>::bytes();
+    if (p.d == 0)
+        five_sweep_amr_kernel<P, 0, MODE><<<grid, SWEEP_THREADS, b, s>>>(p);
+    else if (p.d == 1)
+        five_sweep_amr_kernel<P, 1, MODE><<<grid, SWEEP_THREADS, b, s>>>(p);
+    else
+        five_sweep_amr_kernel<P, 2, MODE><<<grid, SWEEP_THREADS, b, s>>>(p);
+    return cudaGetLastError();
+}
+template <int MODE> cudaError_t five_launch_amr_p(int P, const FiveSweepParams& p, dim3 grid, cudaStream_t s) {
+    switch (P) {
+        case 16: return five_launch_amr_d<16, MODE>(p, grid, s);
+        case 32: return five_launch_amr_d<32, MODE>(p, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+cudaError_t five_launch_amr(int P, int mode, const FiveSweepParams& p, dim3 grid, cudaStream_t s) {
+    switch (mode) {
+        case MODE_WENO: return five_launch_amr_p<MODE_WENO>(P, p, grid, s);
+        case MODE_HYBRID: return five_launch_amr_p<MODE_HYBRID>(P, p, grid, s);
+        case MODE_CENTRAL: return five_launch_amr_p<MODE_CENTRAL>(P, p, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+template <int P, int MODE> cudaError_t five_attr_amr_d() {
+    const int b = (int)FiveSmem<P, MODE>::bytes();
+    cudaError_t e = cudaFuncSetAttribute(five_sweep_amr_kernel<P, 0, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(five_sweep_amr_kernel<P, 1, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(five_sweep_amr_kernel<P, 2, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    return e;
+}
 template <int MODE> cudaError_t five_attr_p() {
     cudaError_t e = five_attr_d<8, MODE>();
     if (e == cudaSuccess) e = five_attr_d<16, MODE>();
     if (e == cudaSuccess) e = five_attr_d<32, MODE>();
+    if (e == cudaSuccess) e = five_attr_amr_d<16, MODE>();
+    if (e == cudaSuccess) e = five_attr_amr_d<32, MODE>();
     return e;
 }
 // the sweeps' shared-memory opt-in, once per device
@@ -305,6 +346,13 @@ cudaError_t five_prepare_device() {
 }
 
 }  // namespace
+
+namespace emg {
+cudaError_t five_sweep_launch_amr(int P, int mode, const FiveSweepParams& p, dim3 grid, cudaStream_t s) {
+    return five_launch_amr(P, mode, p, grid, s);
+}
+cudaError_t five_sweep_prepare_device() { return five_prepare_device(); }
+}  // namespace emg
 
 struct emg_five {
     int device = 0;

@@ -47,6 +47,17 @@ struct FiveSweepParams {
     int positivity;
     double tol;
     FiveSysD sys;
+    // ---- batched block-AMR leaves (the AMR instantiation)
+    const int* leaf_slot;   // pool slot of launch leaf x / ngroups
+    const int* leaf_level;  // level of each pool slot
+    int64_t bcell;          // cells per pool block (ghost-extended)
+    int ngroups;            // CTAs per leaf along the other axis
+    int lw;                 // lanes of one block row (≤ P)
+    double dx_level[16];    // cell size along d per level
+    double* face;           // block-face flux record for refluxing
+    int64_t nface;          // its length (doubles)
+    int npen;               // pencils per block face (padded)
+    int pen_lane_major;     // pencil index = lane*no + other (lane axis is the lower of the two others)
 };
 
 template <int P, int MODE> struct FiveSmem {
@@ -63,7 +74,7 @@ template <int P, int MODE> struct FiveSmem {
     }
 };
 
-template <int P, int D, int MODE> struct FiveSweep {
+template <int P, int D, int MODE, bool AMR = false> struct FiveSweep {
     using SM = FiveSmem<P, MODE>;
     static constexpr int T = SWEEP_THREADS;
     static constexpr int RM = SM::RM;
@@ -222,22 +233,39 @@ template <int P, int D, int MODE> struct FiveSweep {
             s_limited = 0;
             s_weno = 0;
         }
-        const int lane0 = blockIdx.x * P;
+        // uniform grids: x = lane tile, y = segment, z = other-axis row;
+        // AMR batches: x = (leaf, group of other-axis rows), one segment
+        const int lane0 = AMR ? 0 : blockIdx.x * P;
         const int s0 = blockIdx.y * p.seg;
         const int Ls = min(p.seg, p.nd - s0);
-        const int ob = blockIdx.z;
-        if (tid < P) {
+        int ob = blockIdx.z;
+        int64_t blk = 0;
+        int slot_id = 0;
+        double dx = p.dx;
+        __shared__ int s_pen[P];
+        if constexpr (AMR) {
+            const int z = blockIdx.x / p.ngroups;
+            slot_id = p.leaf_slot[z];
+            blk = (int64_t)slot_id * p.bcell;
+            dx = p.dx_level[p.leaf_level[slot_id]];
+            if (tid < P) {
+                const int la = tid % p.lw, ob1 = (blockIdx.x % p.ngroups) * (P / p.lw) + tid / p.lw;
+                s_lok[tid] = la < p.nl && ob1 < p.no;
+                s_loff[tid] = (int64_t)(p.gl + la) * p.sl + (int64_t)(p.go + ob1) * p.so;
+                s_pen[tid] = p.pen_lane_major ? la * p.no + ob1 : ob1 * p.nl + la;
+            }
+        } else if (tid < P) {
             const int la = lane0 + tid;
             s_lok[tid] = la < p.nl && ob < p.no;
             s_loff[tid] = (int64_t)(p.gl + la) * p.sl + (int64_t)(p.go + ob) * p.so;
         }
-        const int64_t base0 = (int64_t)(p.gd + s0 - 5) * p.sd;
+        const int64_t base0 = blk + (int64_t)(p.gd + s0 - 5) * p.sd;
         const bool tail = s0 + Ls == p.nd;
         const Five sys = Five::from(p.sys);
-        const double lam = (p.ndim * dt) / p.dx;
+        const double lam = (p.ndim * dt) / dx;  // λ = ndim·dt/dx (C/solver.rs:393, C/amr.rs:1245)
         const double lam2 = 2.0 * lam;
         const bool lim_on = p.positivity && lam > 0.0;
-        const double inv = 1.0 / p.dx;
+        const double inv = 1.0 / dx;
         __syncthreads();
         const int nrounds = (Ls + 5 + RM - 1) / RM;
         const int nrows = Ls + 10;
@@ -419,6 +447,14 @@ template <int P, int D, int MODE> struct FiveSweep {
 #pragma unroll
                     for (int k = 0; k < NF; k++) F[at<STR>(fidx, k, l)] = fh[k];
                     F[at<STR>(fidx, NF, l)] = uf;
+                    if (AMR && (fidx == 0 || fidx == Ls) &&
+                        in_bounds(p.ctl, ((((int64_t)slot_id * 3 + D) * 2 + (fidx == 0 ? 0 : 1)) * NF + NF - 1) * p.npen + s_pen[l],
+                                  p.nface)) {
+                        // block boundary faces for refluxing (C/amr.rs:1291-1295)
+                        double* fo = p.face + ((((int64_t)slot_id * 3 + D) * 2 + (fidx == 0 ? 0 : 1)) * NF) * p.npen + s_pen[l];
+#pragma unroll
+                        for (int k = 0; k < NF; k++) fo[(int64_t)k * p.npen] = fh[k];
+                    }
                 }
             }
             __syncthreads();
@@ -437,7 +473,9 @@ template <int P, int D, int MODE> struct FiveSweep {
                     double res[NF];
 #pragma unroll
                     for (int k = 0; k < NF; k++) {
-                        const double x = (F[at<STR>(c + 1, k, l)] - F[at<STR>(c, k, l)]) * inv;
+                        // the block solver divides by dx (C/amr.rs:1273), the uniform one multiplies by 1/dx
+                        const double df = F[at<STR>(c + 1, k, l)] - F[at<STR>(c, k, l)];
+                        const double x = AMR ? df / dx : df * inv;
                         const double prev = p.first ? 0.0 : p.rhs[k * p.ncell + g];
                         res[k] = prev - x;
                     }
@@ -446,7 +484,8 @@ template <int P, int D, int MODE> struct FiveSweep {
                         double wc[NF];
 #pragma unroll
                         for (int k = 0; k < NF; k++) wc[k] = W[at<STRW>(c + 5, k, l)];
-                        res[F_IA] = res[F_IA] + sys.nc_coef(wc) * (F[at<STR>(c + 1, NF, l)] - F[at<STR>(c, NF, l)]) * inv;
+                        const double du = F[at<STR>(c + 1, NF, l)] - F[at<STR>(c, NF, l)];
+                        res[F_IA] = res[F_IA] + (AMR ? sys.nc_coef(wc) * du / dx : sys.nc_coef(wc) * du * inv);
                     }
                     if (!p.last) {
 #pragma unroll

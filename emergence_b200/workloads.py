@@ -210,3 +210,44 @@ def two_phase_shock_bubble(n=128, mach=2.0, radius=0.15, eps=1e-8, seed=SEED, ng
     w[..., 6] = a
     bc = [[Bc.Outflow, Bc.Outflow] for _ in range(3)]
     return sys, mesh, five_initial_state(sys, mesh, w), bc
+
+
+def two_phase_amr_bubble(dim=3, base=4, b=16, levels=3, eps=1e-3, regrid_every=4, seed=SEED, x_shock=0.2,
+                         radius=0.15, mach=2.0, alpha_eps=1e-8, ghosts=5):
+    """The two-phase shock–bubble of two_phase_shock_bubble on the block-AMR
+    grid (five-equation system): a sphere (circle in 2-D) of light gas
+    (γ 1.67, ρ 0.138, radius 0.15 ± 0.5 % seeded perturbation) in air (γ 1.4,
+    ρ 1, p 1), volume fraction 1 − alpha_eps inside / alpha_eps outside, a
+    Mach-2 shock in air at x < x_shock moving +x; inflow (x low) Dirichlet at
+    the post-shock state, all other sides outflow. Returns (sys, cfg, lo, hi,
+    bc, init) with init(x[n,3]) -> primitive w[n,7] = (α1ρ1, α2ρ2, u, v, w,
+    p, α1)."""
+    from .five import FiveEq
+    sys_ = FiveEq((Nasg(1.67), Nasg(1.4)), kapila=True)
+    rho2, u2, p2, _ = rankine_hugoniot(mach)
+    cfg = dict(b=b, levels=levels, eps=eps, regrid_every=regrid_every,
+               base_blocks=[base] * dim + [0] * (3 - dim), ghosts=ghosts)
+    centre = np.array([0.5, 0.5, 0.5])
+
+    def init(x):
+        rel = x - centre
+        if dim == 2:
+            rel[:, 2] = 0.0
+        r = np.sqrt((rel * rel).sum(axis=1))
+        theta = np.arccos(np.clip(np.where(r > 0, rel[:, 2] / np.where(r > 0, r, 1), 0.0), -1, 1))
+        phi = np.arctan2(rel[:, 1], rel[:, 0])
+        inside = r < radius * (1.0 + 0.005 * _interface_noise(seed, theta, phi))
+        post = x[:, 0] < x_shock
+        a = np.where(inside, 1.0 - alpha_eps, alpha_eps)
+        w = np.zeros((x.shape[0], 7))
+        w[:, 0] = a * 0.138
+        w[:, 1] = (1.0 - a) * np.where(post, rho2, 1.0)
+        w[:, 2] = np.where(post, u2, 0.0)
+        w[:, 5] = np.where(post, p2, 1.0)
+        w[:, 6] = a
+        return w
+
+    far_w = np.array([alpha_eps * 0.138, (1.0 - alpha_eps) * rho2, u2, 0.0, 0.0, p2, alpha_eps])
+    far = sys_.to_cons(far_w)
+    bc = [[Bc.dirichlet(far), Bc.Outflow], [Bc.Outflow, Bc.Outflow], [Bc.Outflow, Bc.Outflow]]
+    return sys_, cfg, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), bc, init

@@ -395,6 +395,27 @@ int emg_amr_create_from_blocks(const emg_amr_config* cfg, const emg_eos* eos, co
                                const emg_bc bc[6], const emg_opts* opts, const int64_t* desc, size_t nblocks,
                                const double* u, emg_amr** out);
 
+/* The five-equation two-phase system (Kapila's model, 7 conserved variables)
+ * on the block hierarchy: GpuAmr::new with GpuSystem::FiveEq
+ * (G/amr.rs:132-212) on an Amr<7, FiveEq> (C/amr.rs:289-344). `init` fills
+ * 7 primitives (α1ρ1, α2ρ2, u, v, w, p, α1) per cell; Dirichlet states hold 7
+ * conserved values; characteristic boundaries are not available; plain FP64
+ * form only. Every other emg_amr_* call works on the handle, with 7 values
+ * per cell in block data and totals. The block residual carries the α
+ * equation's non-conservative term and the CFL step the dilatation limit
+ * (C/amr.rs:1276-1279, 1426-1461). */
+int emg_amr_create_five(const emg_amr_config* cfg, const emg_five_system* sys, const double lo[3], const double hi[3],
+                        const emg_bc7 bc[6], const emg_opts* opts, emg_init_fn init, void* ctx, emg_amr** out);
+
+/* Adopt an existing five-equation hierarchy: as emg_amr_create_from_blocks
+ * with block data u[id][cell][7]. */
+int emg_amr_create_five_from_blocks(const emg_amr_config* cfg, const emg_five_system* sys, const double lo[3],
+                                    const double hi[3], const emg_bc7 bc[6], const emg_opts* opts,
+                                    const int64_t* desc, size_t nblocks, const double* u, emg_amr** out);
+
+/* Conserved variables per cell of the handle's system: 5 (Euler) or 7. */
+int emg_amr_nv(emg_amr* h, int32_t* nv);
+
 int emg_amr_destroy(emg_amr* h);
 
 /* One global SSP-RK3 step of size dt, regridding when due (Amr::step,
@@ -433,11 +454,11 @@ int emg_amr_block_count(emg_amr* h, uint64_t* blocks, uint64_t* leaves);
  * C/amr.rs:1539-1541); `cap` blocks of room. */
 int emg_amr_structure(emg_amr* h, int64_t* desc, size_t cap);
 
-/* Block data u[id][cell][5] of all blocks (GpuAmr::download, G/amr.rs:821-843). */
+/* Block data u[id][cell][nv] of all blocks (GpuAmr::download, G/amr.rs:821-843). */
 int emg_amr_download(emg_amr* h, double* u, size_t nblocks);
 
-/* Σ u·vol over leaves (C/amr.rs:1991-2005). */
-int emg_amr_totals(emg_amr* h, double out[5]);
+/* Σ u·vol over leaves (C/amr.rs:1991-2005), nv values. */
+int emg_amr_totals(emg_amr* h, double* out);
 
 /* [faces, shock-path faces, fallbacks, limited faces] since creation. */
 int emg_amr_counters(emg_amr* h, uint64_t out[4]);

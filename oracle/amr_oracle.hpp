@@ -8,6 +8,7 @@
 // refluxing, flux registers, wavelet regrid with 2:1 balance, and SSP-RK3
 // stepping, in the reference's operation order.
 #pragma once
+#include "five_oracle.hpp"
 #include "oracle.hpp"
 #include <functional>
 #include <map>
@@ -46,10 +47,43 @@ struct AmrConfig {
 };
 
 using Key3 = std::array<int64_t, 3>;
-using V = V5<double>;
 using InitFn = std::function<void(const double* x, int64_t n, double* w)>;  // batched primitive init
 
-struct AmrBlock {  // amr.rs:194-206
+// The physical system of a block hierarchy (Amr<N, S>, amr.rs:208): the
+// conserved vector, the momentum index, the line flux routine (with the face
+// velocities of the non-conservative term) and whether the multiphase terms
+// apply — the non-conservative α term in the block residual (amr.rs:1276-1279)
+// and the dilatation limit of the CFL step (amr.rs:1426-1461).
+struct AmrEuler {
+    static constexpr int N = 5, IU = 1;
+    static constexpr bool MULTIPHASE = false;
+    using Sys = Euler<double>;
+    using V = V5<double>;
+    using BcT = Bc<double>;
+    static void fluxes(const Sys& s, const V* line, int len, int d, int ng, const SchemeOpts& o, V* fl, double*,
+                       Stats& st) {
+        line_fluxes(s, line, len, d, ng, o, fl, (double*)nullptr, st);
+    }
+    static V char_layer(const Sys& s, const V& ub, const V& ub1, const V& far, int d, int side, double m) {
+        return characteristic_ghost_layer(s, ub, ub1, far, d, side, m);
+    }
+};
+struct AmrFive {
+    static constexpr int N = 7, IU = 2;
+    static constexpr bool MULTIPHASE = true;
+    using Sys = FiveEq<double>;
+    using V = V7<double>;
+    using BcT = Bc7<double>;
+    static void fluxes(const Sys& s, const V* line, int len, int d, int ng, const SchemeOpts& o, V* fl, double* uf,
+                       Stats& st) {
+        line_fluxes7(s, line, len, d, ng, o, fl, uf, st);
+    }
+    static V char_layer(const Sys& s, const V& ub, const V& ub1, const V& far, int d, int side, double m) {
+        return CharStencil7<double>(s, ub, ub1, far, d, side).conserved(s, m);
+    }
+};
+
+template <class V> struct AmrBlockT {  // amr.rs:194-206
     int64_t level;
     Key3 idx;
     bool leaf = true;
@@ -57,11 +91,15 @@ struct AmrBlock {  // amr.rs:194-206
     std::vector<V> face[3][2];
 };
 
-struct Amr {
-    Euler<double> sys;
+template <class S> struct AmrT {
+    using V = typename S::V;
+    using BcT = typename S::BcT;
+    using AmrBlock = AmrBlockT<V>;
+    static constexpr int N = S::N;
+    typename S::Sys sys;
     AmrConfig cfg;
     double lo[3], hi[3];
-    Bc<double> bc[3][2];
+    BcT bc[3][2];
     int mode = HYBRID;
     double tol = 1e-3;
     double cfl = 0.4;
@@ -134,8 +172,8 @@ struct Amr {
     }
 
     // ---- construction (amr.rs:289-344)
-    Amr(const Euler<double>& s, const AmrConfig& c, const double* lo_, const double* hi_, const Bc<double> (&b)[3][2],
-        const InitFn& init)
+    AmrT(const typename S::Sys& s, const AmrConfig& c, const double* lo_, const double* hi_, const BcT (&b)[3][2],
+         const InitFn& init)
         : sys(s), cfg(c) {
         for (int d = 0; d < 3; d++) {
             lo[d] = lo_[d];
@@ -179,20 +217,20 @@ struct Amr {
         b.level = level;
         b.idx = idx;
         b.leaf = true;
-        b.u.assign(bcells(), V{0, 0, 0, 0, 0});
-        b.rhs.assign(bcells(), V{0, 0, 0, 0, 0});
+        b.u.assign(bcells(), V{});
+        b.rhs.assign(bcells(), V{});
         for (int d = 0; d < 3; d++) {
             int64_t fsz = 1;
             for (int e = 0; e < 3; e++)
                 if (e != d) fsz *= bd(e);
-            b.face[d][0].assign(fsz, V{0, 0, 0, 0, 0});
-            b.face[d][1].assign(fsz, V{0, 0, 0, 0, 0});
+            b.face[d][0].assign(fsz, V{});
+            b.face[d][1].assign(fsz, V{});
         }
         return b;
     }
     void fill_from_init(AmrBlock& b, const InitFn& init) const {
         int64_t b0 = bd(0), b1 = bd(1), b2 = bd(2), n = b0 * b1 * b2;
-        std::vector<double> xs(3 * n), ws(5 * n);
+        std::vector<double> xs(3 * n), ws(N * n);
         for (int64_t i = 0; i < b0; i++)
             for (int64_t j = 0; j < b1; j++)
                 for (int64_t k = 0; k < b2; k++) {
@@ -201,7 +239,8 @@ struct Amr {
                 }
         init(xs.data(), n, ws.data());
         for (int64_t q = 0; q < n; q++) {
-            V w{ws[5 * q], ws[5 * q + 1], ws[5 * q + 2], ws[5 * q + 3], ws[5 * q + 4]};
+            V w;
+            for (int k = 0; k < N; k++) w[k] = ws[N * q + k];
             b.u[q] = sys.to_cons(w);
         }
     }
@@ -244,9 +283,9 @@ struct Amr {
                         g1[d] += side == 1 ? -1 : 1;
                         double m = (double)std::llabs(g[d] - gi[d]);
                         V ub = sample(l, gi), ub1 = sample(l, g1);
-                        V v = characteristic_ghost_layer(sys, ub, ub1, bc[d][side].state, d, side, m);
+                        V v = S::char_layer(sys, ub, ub1, bc[d][side].state, d, side, m);
                         for (int e = 0; e < 3; e++)
-                            if (flip[e]) v[1 + e] = -v[1 + e];
+                            if (flip[e]) v[S::IU + e] = -v[S::IU + e];
                         return v;
                     }
                 }
@@ -262,7 +301,7 @@ struct Amr {
             v = predict(l, g);
         }
         for (int d = 0; d < 3; d++)
-            if (flip[d]) v[1 + d] = -v[1 + d];
+            if (flip[d]) v[S::IU + d] = -v[S::IU + d];
         return v;
     }
 
@@ -318,7 +357,7 @@ struct Amr {
                                 int64_t p = local(side == 0 ? -1 - g[d] : 2 * n[d] - 1 - g[d]);
                                 if (p >= 0) {
                                     v = val[p];
-                                    v[1 + d] = -v[1 + d];
+                                    v[S::IU + d] = -v[S::IU + d];
                                     has = true;
                                 }
                                 break;
@@ -327,7 +366,7 @@ struct Amr {
                                 int64_t g1 = gi + (side == 1 ? -1 : 1);
                                 int64_t pb = local(gi), p1 = local(g1);
                                 if (pb >= 0 && p1 >= 0) {
-                                    v = characteristic_ghost_layer(sys, val[pb], val[p1], bc[d][side].state, d, side,
+                                    v = S::char_layer(sys, val[pb], val[p1], bc[d][side].state, d, side,
                                                                    (double)std::llabs(g[d] - gi));
                                     has = true;
                                 }
@@ -349,7 +388,7 @@ struct Amr {
         for (int d = 0; d < 3; d++) n[d] = n_level(l, d);
         std::vector<int> dm = dims();
         int64_t len = sz[0] * sz[1] * sz[2];
-        std::vector<V> val(len, V{0, 0, 0, 0, 0});
+        std::vector<V> val(len, V{});
         std::vector<char> ok(len, 1);
         bool any = false;
         for (int64_t i = 0; i < sz[0]; i++)
@@ -410,7 +449,7 @@ struct Amr {
                             s[d] = base + kk;
                             const V& v = arr[(s[0] * sz[1] + s[1]) * sz[2] + s[2]];
                             double wgt = wp[par][kk];
-                            for (int q = 0; q < 5; q++) acc[q] = acc[q] + wgt * v[q];
+                            for (int q = 0; q < N; q++) acc[q] = acc[q] + wgt * v[q];
                         }
                         na[(i * nsz[1] + j) * nsz[2] + k] = acc;
                     }
@@ -441,7 +480,7 @@ struct Amr {
                 w = w * wp[odd][k];
             }
             V v = sample(l - 1, c);
-            for (int q = 0; q < 5; q++) acc[q] = acc[q] + w * v[q];
+            for (int q = 0; q < N; q++) acc[q] = acc[q] + w * v[q];
         }
         return acc;
     }
@@ -481,7 +520,7 @@ struct Amr {
                         }
                     }
                     if (out) {
-                        val.push_back(V{0, 0, 0, 0, 0});
+                        val.push_back(V{});
                         ok.push_back(0);
                         any_out = true;
                     } else {
@@ -492,7 +531,7 @@ struct Amr {
                             val.push_back(blocks[bid].u[cidx(c[0], c[1], c[2])]);
                             ok.push_back(1);
                         } else {
-                            val.push_back(V{0, 0, 0, 0, 0});
+                            val.push_back(V{});
                             ok.push_back(0);
                         }
                     }
@@ -504,7 +543,7 @@ struct Amr {
         for (int d : dm) {
             int64_t nsz[3] = {sz[0], sz[1], sz[2]};
             nsz[d] = bdd[d];
-            std::vector<V> nv(nsz[0] * nsz[1] * nsz[2], V{0, 0, 0, 0, 0});
+            std::vector<V> nv(nsz[0] * nsz[1] * nsz[2], V{});
             std::vector<char> nok(nsz[0] * nsz[1] * nsz[2], 0);
             for (int64_t i = 0; i < nsz[0]; i++)
                 for (int64_t j = 0; j < nsz[1]; j++)
@@ -527,7 +566,7 @@ struct Amr {
                                 V acc{0, 0, 0, 0, 0};
                                 for (int kk = 0; kk < 6; kk++) {
                                     const V& v = val[at_src(st + kk)];
-                                    for (int q = 0; q < 5; q++) acc[q] = acc[q] + wts[m][kk] * v[q];
+                                    for (int q = 0; q < N; q++) acc[q] = acc[q] + wts[m][kk] * v[q];
                                 }
                                 nv[o_] = acc;
                                 nok[o_] = 1;
@@ -539,7 +578,7 @@ struct Amr {
                             int64_t pa = at_src(base + 2), pb = at_src(base + 3);
                             if (ok[pa] && ok[pb]) {
                                 V acc;
-                                for (int q = 0; q < 5; q++) acc[q] = 0.5 * (val[pa][q] + val[pb][q]);
+                                for (int q = 0; q < N; q++) acc[q] = 0.5 * (val[pa][q] + val[pb][q]);
                                 nv[o_] = acc;
                                 nok[o_] = 1;
                             }
@@ -673,7 +712,7 @@ struct Amr {
             gof[d] = a[d] ? ng : 0;
         }
         auto at = [&](int64_t i, int64_t j, int64_t k) { return (i * ext[1] + j) * ext[2] + k; };
-        std::vector<V> out(ext[0] * ext[1] * ext[2], V{0, 0, 0, 0, 0});
+        std::vector<V> out(ext[0] * ext[1] * ext[2], V{});
         std::vector<char> filled(out.size(), 1);
         for (int64_t i = 0; i < bdv[0]; i++)
             for (int64_t j = 0; j < bdv[1]; j++)
@@ -777,11 +816,12 @@ struct Amr {
             gof[d] = a[d] ? ng : 0;
         }
         std::vector<V> scr = fill_scratch(id);
-        std::vector<std::array<double, 2>> sens(scr.size());
+        std::vector<std::array<double, 3>> sens(scr.size());
+        int ns = 0;
         for (size_t q = 0; q < scr.size(); q++) {
             double v[8];
-            sys.sensor(sys.to_prim(scr[q]), v);
-            sens[q] = {v[0], v[1]};
+            ns = sys.sensor(sys.to_prim(scr[q]), v);
+            sens[q] = {v[0], v[1], ns > 2 ? v[2] : 0.0};
         }
         auto at = [&](const int64_t* c) { return (c[0] * ext[1] + c[1]) * ext[2] + c[2]; };
         double mx = 0.0;
@@ -792,14 +832,14 @@ struct Amr {
                     int64_t c[3] = {i + gof[0], j + gof[1], k + gof[2]};
                     const auto& s0 = sens[at(c)];
                     for (int d : dm) {
-                        double pred[2] = {0.0, 0.0};
+                        double pred[3] = {0.0, 0.0, 0.0};
                         for (int m = 0; m < 6; m++) {
                             int64_t cc[3] = {c[0], c[1], c[2]};
                             cc[d] += offs[m];
                             const auto& sv = sens[at(cc)];
-                            for (int q = 0; q < 2; q++) pred[q] = pred[q] + wr[m] * sv[q];
+                            for (int q = 0; q < ns; q++) pred[q] = pred[q] + wr[m] * sv[q];
                         }
-                        for (int q = 0; q < 2; q++) {
+                        for (int q = 0; q < ns; q++) {
                             double dd = std::fabs(s0[q] - pred[q]);
                             mx = std::isfinite(dd) ? std::fmax(mx, dd) : INFINITY;
                         }
@@ -1002,13 +1042,14 @@ struct Amr {
         std::vector<V> scr = fill_scratch(id);
         std::vector<V> w(scr.size());
         for (size_t q = 0; q < scr.size(); q++) w[q] = sys.to_prim(scr[q]);
-        rhs.assign(bcells(), V{0, 0, 0, 0, 0});
+        rhs.assign(bcells(), V{});
         Stats st;
         for (int d : dm) {
             int e0 = d == 0 ? 1 : 0, e1 = d == 2 ? 1 : 2;
             double dxl = dx(l, d);
             SchemeOpts opts{mode, tol, positivity ? ndim * stage_dt / dxl : 0.0};
             std::vector<V> fl(bdv[d] + 1), line(ext[d]);
+            std::vector<double> uf(bdv[d] + 1, 0.0);
             face[d][0].clear();
             face[d][1].clear();
             for (int64_t aa = 0; aa < bdv[e0]; aa++)
@@ -1021,14 +1062,19 @@ struct Amr {
                         return (c[0] * ext[1] + c[1]) * ext[2] + c[2];
                     };
                     for (int64_t cc = 0; cc < ext[d]; cc++) line[cc] = w[at(cc)];
-                    line_fluxes(sys, line.data(), (int)ext[d], d, (int)ng, opts, fl.data(), (double*)nullptr, st);
+                    S::fluxes(sys, line.data(), (int)ext[d], d, (int)ng, opts, fl.data(), uf.data(), st);
                     for (int64_t cc = 0; cc < bdv[d]; cc++) {
                         int64_t c[3];
                         c[d] = cc;
                         c[e0] = aa;
                         c[e1] = bb;
                         V& o = rhs[cidx(c[0], c[1], c[2])];
-                        for (int q = 0; q < 5; q++) o[q] = o[q] - (fl[cc + 1][q] - fl[cc][q]) / dxl;
+                        for (int q = 0; q < N; q++) o[q] = o[q] - (fl[cc + 1][q] - fl[cc][q]) / dxl;
+                        if constexpr (S::MULTIPHASE) {
+                            // the α equation's non-conservative term (amr.rs:1276-1279)
+                            const V& wc = line[cc + ng];
+                            o[N - 1] = o[N - 1] + sys.nc_coef(wc) * (uf[cc + 1] - uf[cc]) / dxl;
+                        }
                     }
                     face[d][0].push_back(fl[0]);
                     face[d][1].push_back(fl[bdv[d]]);
@@ -1106,7 +1152,7 @@ struct Amr {
                                     int64_t la = a0 ? rem_euclid(ga, bdv[e0]) : 0;
                                     int64_t lb = a1 ? rem_euclid(gb, bdv[e1]) : 0;
                                     const V& fv = blocks[cid].face[d][1 - side][la * bdv[e1] + lb];
-                                    for (int q = 0; q < 5; q++) sum[q] = sum[q] + fv[q];
+                                    for (int q = 0; q < N; q++) sum[q] = sum[q] + fv[q];
                                     cnt = cnt + 1.0;
                                 }
                             if (cnt == 0.0) continue;
@@ -1116,7 +1162,7 @@ struct Amr {
                             c[e0] = aa;
                             c[e1] = bb;
                             V dr;
-                            for (int q = 0; q < 5; q++) {
+                            for (int q = 0; q < N; q++) {
                                 double df = sum[q] / cnt - fc[q];
                                 dr[q] = side == 1 ? -df / dxl : df / dxl;
                             }
@@ -1127,7 +1173,7 @@ struct Amr {
         }
         for (auto& c : corr) {
             V& r = blocks[std::get<0>(c)].rhs[std::get<1>(c)];
-            for (int q = 0; q < 5; q++) r[q] = r[q] + std::get<2>(c)[q];
+            for (int q = 0; q < N; q++) r[q] = r[q] + std::get<2>(c)[q];
         }
     }
 
@@ -1149,7 +1195,48 @@ struct Amr {
         }
         return rate;
     }
-    double dt_cfl() const { return cfl / cfl_rate(); }
+    // amr.rs:1408-1466: the global step, and for the multiphase system the
+    // dilatation limit 0.5 / max rate over the leaves, with the velocity
+    // divergence from the neighbouring cells (sampled across block faces)
+    double dt_cfl() const {
+        double dt = cfl / cfl_rate();
+        if constexpr (S::MULTIPHASE) {
+            std::vector<int> dm = dims();
+            int64_t bdv[3] = {bd(0), bd(1), bd(2)};
+            std::vector<double> src(blocks.size(), 0.0);
+#pragma omp parallel for schedule(dynamic, 1)
+            for (int64_t bi = 0; bi < (int64_t)blocks.size(); bi++) {
+                const AmrBlock& b = blocks[bi];
+                if (!b.leaf) continue;
+                double r = 0.0;
+                for (int64_t i = 0; i < bdv[0]; i++)
+                    for (int64_t j = 0; j < bdv[1]; j++)
+                        for (int64_t k = 0; k < bdv[2]; k++) {
+                            int64_t c[3] = {i, j, k};
+                            V w = sys.to_prim(b.u[cidx(i, j, k)]);
+                            double divu = 0.0;
+                            for (int d : dm) {
+                                auto get = [&](int64_t o) {
+                                    int64_t cc[3] = {c[0], c[1], c[2]};
+                                    cc[d] += o;
+                                    if (cc[d] >= 0 && cc[d] < bdv[d]) return sys.to_prim(b.u[cidx(cc[0], cc[1], cc[2])]);
+                                    Key3 g;
+                                    for (int e = 0; e < 3; e++) g[e] = b.idx[e] * bdv[e] + cc[e];
+                                    return sys.to_prim(sample(b.level, g));
+                                };
+                                int vi = S::IU + d;
+                                divu = divu + std::fabs(get(1)[vi] - get(-1)[vi]) / (2.0 * dx(b.level, d));
+                            }
+                            r = std::fmax(r, sys.dilatation_rate(w, divu));
+                        }
+                src[bi] = r;
+            }
+            double s = 0.0;
+            for (double v : src) s = std::fmax(s, v);
+            if (s > 0.0) dt = std::fmin(dt, 0.5 / s);
+        }
+        return dt;
+    }
 
     // amr.rs:1470-1512
     void step(double dt) {
@@ -1160,17 +1247,17 @@ struct Amr {
         for (auto& b : blocks)
             if (b.leaf)
                 for (size_t c = 0; c < b.u.size(); c++)
-                    for (int q = 0; q < 5; q++) b.u[c][q] = b.u[c][q] + dt * b.rhs[c][q];
+                    for (int q = 0; q < N; q++) b.u[c][q] = b.u[c][q] + dt * b.rhs[c][q];
         Stats s2 = compute_rhs();
         for (auto& b : blocks)
             if (b.leaf)
                 for (size_t c = 0; c < b.u.size(); c++)
-                    for (int q = 0; q < 5; q++) b.u[c][q] = 0.75 * b.u0[c][q] + 0.25 * (b.u[c][q] + dt * b.rhs[c][q]);
+                    for (int q = 0; q < N; q++) b.u[c][q] = 0.75 * b.u0[c][q] + 0.25 * (b.u[c][q] + dt * b.rhs[c][q]);
         Stats s3 = compute_rhs();
         for (auto& b : blocks)
             if (b.leaf)
                 for (size_t c = 0; c < b.u.size(); c++)
-                    for (int q = 0; q < 5; q++)
+                    for (int q = 0; q < N; q++)
                         b.u[c][q] = b.u0[c][q] / 3.0 + 2.0 / 3.0 * (b.u[c][q] + dt * b.rhs[c][q]);
         stats.add(s1);
         stats.add(s2);
@@ -1273,7 +1360,7 @@ struct Amr {
             if (b.level != l || b.u0.empty()) continue;
             b.u_save = b.u;
             for (size_t c = 0; c < b.u.size(); c++)
-                for (int q = 0; q < 5; q++) b.u[c][q] = (1.0 - th) * b.u0[c][q] + th * b.u[c][q];
+                for (int q = 0; q < N; q++) b.u[c][q] = (1.0 - th) * b.u0[c][q] + th * b.u[c][q];
         }
     }
     void restore_time_view(int64_t l) {
@@ -1328,8 +1415,8 @@ struct Amr {
                 const std::vector<V>& face = blocks[id].face[d][cf.side];
                 if (cf.kind == 0) {
                     for (size_t fi = 0; fi < face.size(); fi++) {
-                        V& e = creg.try_emplace(RegKey{id, d, cf.side, (int64_t)fi}, V{0, 0, 0, 0, 0}).first->second;
-                        for (int q = 0; q < 5; q++) e[q] = e[q] + wdt * face[fi][q];
+                        V& e = creg.try_emplace(RegKey{id, d, cf.side, (int64_t)fi}, V{}).first->second;
+                        for (int q = 0; q < N; q++) e[q] = e[q] + wdt * face[fi][q];
                     }
                 } else {
                     const AmrBlock& b = blocks[id];
@@ -1342,9 +1429,9 @@ struct Amr {
                             int64_t cbb = active(e1) ? div_euclid(gb, 2) - cb.idx[e1] * bdv[e1] : 0;
                             if (ca >= bdv[e0] || cbb >= bdv[e1]) continue;
                             const V& f = face[a * bdv[e1] + bb];
-                            V& e = freg.try_emplace(RegKey{cf.coarse, d, 1 - cf.side, ca * bdv[e1] + cbb}, V{0, 0, 0, 0, 0})
+                            V& e = freg.try_emplace(RegKey{cf.coarse, d, 1 - cf.side, ca * bdv[e1] + cbb}, V{})
                                        .first->second;
-                            for (int q = 0; q < 5; q++) e[q] = e[q] + wdt * f[q] / nsub;
+                            for (int q = 0; q < N; q++) e[q] = e[q] + wdt * f[q] / nsub;
                         }
                 }
             }
@@ -1376,7 +1463,7 @@ struct Amr {
             c[e1] = fi % bdv[e1];
             double dxl = dx(l, d);
             V& u = blocks[id].u[cidx(c[0], c[1], c[2])];
-            for (int q = 0; q < 5; q++) {
+            for (int q = 0; q < N; q++) {
                 double df = fr->second[q] - cr[q];
                 u[q] = u[q] + (side == 1 ? -df / dxl : df / dxl);
             }
@@ -1426,7 +1513,7 @@ struct Amr {
             for (int64_t id : ids) {
                 AmrBlock& b = blocks[id];
                 for (size_t c = 0; c < b.u.size(); c++)
-                    for (int q = 0; q < 5; q++) b.u[c][q] = a0 * b.u0[c][q] + a1 * (b.u[c][q] + dt * b.rhs[c][q]);
+                    for (int q = 0; q < N; q++) b.u[c][q] = a0 * b.u0[c][q] + a1 * (b.u[c][q] + dt * b.rhs[c][q]);
             }
         }
         bool finer = false;
@@ -1485,7 +1572,7 @@ struct Amr {
             double vol = 1.0;
             for (int d : dm) vol = vol * dx(b.level, d);
             for (const V& u : b.u)
-                for (int q = 0; q < 5; q++) s[q] = s[q] + u[q] * vol;
+                for (int q = 0; q < N; q++) s[q] = s[q] + u[q] * vol;
         }
         return s;
     }
@@ -1495,5 +1582,8 @@ struct Amr {
         return n;
     }
 };
+
+using Amr = AmrT<AmrEuler>;
+using AmrFiveEq = AmrT<AmrFive>;
 
 }  // namespace oracle

@@ -12,6 +12,8 @@
 
 #include <cstdio>
 #include <cstring>
+#include <memory>
+#include <type_traits>
 #include <string>
 
 using namespace oracle;
@@ -317,6 +319,28 @@ AmrConfig to_cfg(const emg_amr_config* c) {
 }
 }  // namespace
 
+}  // extern "C"
+
+// An oracle hierarchy of either system: Euler (5 variables) or the
+// five-equation model (7 variables).
+struct AmrHandle {
+    int nv = 5;
+    std::unique_ptr<Amr> e;
+    std::unique_ptr<AmrFiveEq> f;
+    template <class Fn> auto with(Fn fn) { return nv == 5 ? fn(*e) : fn(*f); }
+};
+static AmrHandle* H(void* h) { return (AmrHandle*)h; }
+
+template <class A> static void amr_opts(A& a, const emg_opts* opts) {
+    a.cfl = opts->cfl;
+    a.tol = opts->tol;
+    a.mode = opts->mode;
+    a.positivity = opts->positivity != 0;
+    a.subcycle = (opts->flags & EMG_OPT_SUBCYCLE) != 0;
+}
+
+extern "C" {
+
 int emgo_amr_create(const emg_amr_config* cfg, const emg_eos* eos, const double lo[3], const double hi[3],
                     const emg_bc bc[6], const emg_opts* opts, emg_init_fn init, void* ctx, void** out) {
     if (!cfg || !eos || !lo || !hi || !bc || !opts || !init || !out) return fail(EMG_ERR_INVALID, "null argument");
@@ -326,111 +350,145 @@ int emgo_amr_create(const emg_amr_config* cfg, const emg_eos* eos, const double 
             b[d][s].kind = bc[2 * d + s].kind;
             for (int k = 0; k < 5; k++) b[d][s].state[k] = bc[2 * d + s].state[k];
         }
-    Amr* a = new Amr(to_sys(eos), to_cfg(cfg), lo, hi, b, wrap_init(init, ctx));
-    a->cfl = opts->cfl;
-    a->tol = opts->tol;
-    a->mode = opts->mode;
-    a->positivity = opts->positivity != 0;
-    a->subcycle = (opts->flags & EMG_OPT_SUBCYCLE) != 0;
-    *out = a;
+    AmrHandle* h = new AmrHandle();
+    h->e.reset(new Amr(to_sys(eos), to_cfg(cfg), lo, hi, b, wrap_init(init, ctx)));
+    amr_opts(*h->e, opts);
+    *out = h;
+    return EMG_OK;
+}
+// the five-equation system on the block hierarchy; init fills 7 primitives per cell
+int emgo_amr_five_create(const emg_amr_config* cfg, const emg_five_system* sys, const double lo[3], const double hi[3],
+                         const emg_bc7 bc[6], const emg_opts* opts, emg_init_fn init, void* ctx, void** out) {
+    if (!cfg || !sys || !lo || !hi || !bc || !opts || !init || !out) return fail(EMG_ERR_INVALID, "null argument");
+    FiveEq<double> f;
+    for (int k = 0; k < 2; k++)
+        f.eos[k] = Nasg<double>{sys->eos[k].gamma, sys->eos[k].p_inf, sys->eos[k].b, sys->eos[k].q, sys->eos[k].cv};
+    f.kapila = sys->kapila != 0;
+    Bc7<double> b[3][2];
+    for (int d = 0; d < 3; d++)
+        for (int s = 0; s < 2; s++) {
+            b[d][s].kind = bc[2 * d + s].kind;
+            for (int k = 0; k < 7; k++) b[d][s].state[k] = bc[2 * d + s].state[k];
+        }
+    AmrHandle* h = new AmrHandle();
+    h->nv = 7;
+    h->f.reset(new AmrFiveEq(f, to_cfg(cfg), lo, hi, b, wrap_init(init, ctx)));
+    amr_opts(*h->f, opts);
+    *out = h;
     return EMG_OK;
 }
 int emgo_amr_step_subcycled(void* h, double dt) {
-    ((Amr*)h)->step_subcycled(dt);
+    H(h)->with([&](auto& a) { a.step_subcycled(dt); });
     return EMG_OK;
 }
 int emgo_amr_dt_cfl_subcycled(void* h, double* dt) {
-    *dt = ((Amr*)h)->dt_cfl_subcycled();
+    *dt = H(h)->with([&](auto& a) { return a.dt_cfl_subcycled(); });
     return EMG_OK;
 }
 int emgo_amr_destroy(void* h) {
-    delete (Amr*)h;
+    delete H(h);
     return EMG_OK;
 }
 int emgo_amr_step(void* h, double dt) {
-    ((Amr*)h)->step(dt);
+    H(h)->with([&](auto& a) { a.step(dt); });
     return EMG_OK;
 }
 int emgo_amr_dt_cfl(void* h, double* dt) {
-    *dt = ((Amr*)h)->dt_cfl();
+    *dt = H(h)->with([&](auto& a) { return a.dt_cfl(); });
     return EMG_OK;
 }
 int emgo_amr_run_to(void* h, double t_end, uint64_t* steps) {
-    int64_t n = ((Amr*)h)->run_to(t_end);
+    int64_t n = H(h)->with([&](auto& a) { return a.run_to(t_end); });
     if (n < 0) return fail(EMG_ERR_DT_COLLAPSED, "time step collapsed");
     if (steps) *steps = (uint64_t)n;
     return EMG_OK;
 }
 int emgo_amr_regrid(void* h) {
-    ((Amr*)h)->regrid();
+    H(h)->with([&](auto& a) { a.regrid(); });
+    return EMG_OK;
+}
+int emgo_amr_nv(void* h, int* nv) {
+    *nv = H(h)->nv;
     return EMG_OK;
 }
 int emgo_amr_block_count(void* h, uint64_t* blocks, uint64_t* leaves) {
-    Amr* a = (Amr*)h;
-    if (blocks) *blocks = a->blocks.size();
-    if (leaves) *leaves = (uint64_t)a->leaf_count();
-    return EMG_OK;
+    return H(h)->with([&](auto& a) {
+        if (blocks) *blocks = a.blocks.size();
+        if (leaves) *leaves = (uint64_t)a.leaf_count();
+        return (int)EMG_OK;
+    });
 }
 int emgo_amr_structure(void* h, int64_t* desc, size_t cap) {
-    Amr* a = (Amr*)h;
-    if (cap < a->blocks.size()) return fail(EMG_ERR_INVALID, "structure buffer too small");
-    for (size_t i = 0; i < a->blocks.size(); i++) {
-        desc[5 * i] = a->blocks[i].level;
-        for (int d = 0; d < 3; d++) desc[5 * i + 1 + d] = a->blocks[i].idx[d];
-        desc[5 * i + 4] = a->blocks[i].leaf ? 1 : 0;
-    }
-    return EMG_OK;
+    return H(h)->with([&](auto& a) {
+        if (cap < a.blocks.size()) return fail(EMG_ERR_INVALID, "structure buffer too small");
+        for (size_t i = 0; i < a.blocks.size(); i++) {
+            desc[5 * i] = a.blocks[i].level;
+            for (int d = 0; d < 3; d++) desc[5 * i + 1 + d] = a.blocks[i].idx[d];
+            desc[5 * i + 4] = a.blocks[i].leaf ? 1 : 0;
+        }
+        return (int)EMG_OK;
+    });
 }
+// block data u[id][cell][nv]
 int emgo_amr_download(void* h, double* u, size_t nblocks) {
-    Amr* a = (Amr*)h;
-    if (nblocks < a->blocks.size()) return fail(EMG_ERR_INVALID, "buffer too small");
-    size_t bc_ = (size_t)a->bcells();
-    for (size_t i = 0; i < a->blocks.size(); i++)
-        std::memcpy(u + i * bc_ * 5, a->blocks[i].u.data(), bc_ * 5 * sizeof(double));
-    return EMG_OK;
+    return H(h)->with([&](auto& a) {
+        using A = std::decay_t<decltype(a)>;
+        if (nblocks < a.blocks.size()) return fail(EMG_ERR_INVALID, "buffer too small");
+        size_t bc_ = (size_t)a.bcells();
+        for (size_t i = 0; i < a.blocks.size(); i++)
+            std::memcpy(u + i * bc_ * A::N, a.blocks[i].u.data(), bc_ * A::N * sizeof(double));
+        return (int)EMG_OK;
+    });
 }
-int emgo_amr_totals(void* h, double out[5]) {
-    V5<double> t = ((Amr*)h)->totals();
-    for (int k = 0; k < 5; k++) out[k] = t[k];
+int emgo_amr_totals(void* h, double* out) {
+    H(h)->with([&](auto& a) {
+        auto t = a.totals();
+        for (size_t k = 0; k < t.size(); k++) out[k] = t[k];
+    });
     return EMG_OK;
 }
 int emgo_amr_counters(void* h, uint64_t out[4]) {
-    Stats& s = ((Amr*)h)->stats;
-    out[0] = s.faces;
-    out[1] = s.weno_faces;
-    out[2] = s.fallback_faces;
-    out[3] = s.limited_faces;
+    H(h)->with([&](auto& a) {
+        Stats& s = a.stats;
+        out[0] = s.faces;
+        out[1] = s.weno_faces;
+        out[2] = s.fallback_faces;
+        out[3] = s.limited_faces;
+    });
     return EMG_OK;
 }
 int emgo_amr_get_time(void* h, double* t) {
-    *t = ((Amr*)h)->t;
+    *t = H(h)->with([&](auto& a) { return a.t; });
     return EMG_OK;
 }
 int emgo_amr_steps(void* h, uint64_t* s) {
-    *s = (uint64_t)((Amr*)h)->steps;
+    *s = H(h)->with([&](auto& a) { return (uint64_t)a.steps; });
     return EMG_OK;
 }
 // per-leaf wavelet details in block id order (ancestors 0), C/amr.rs:823-867
 int emgo_amr_details(void* h, double* out, size_t cap) {
-    Amr* a = (Amr*)h;
-    if (cap < a->blocks.size()) return fail(EMG_ERR_INVALID, "buffer too small");
-    a->restrict_all();
-    std::vector<double> d = a->details();
-    for (size_t i = 0; i < d.size(); i++) out[i] = d[i];
-    return EMG_OK;
+    return H(h)->with([&](auto& a) {
+        if (cap < a.blocks.size()) return fail(EMG_ERR_INVALID, "buffer too small");
+        a.restrict_all();
+        std::vector<double> d = a.details();
+        for (size_t i = 0; i < d.size(); i++) out[i] = d[i];
+        return (int)EMG_OK;
+    });
 }
 
 // conserved state at level-l cell coordinates g[3*i..] (Amr::sample, amr.rs:384-439):
-// the covering block's data, or the prediction from coarser levels
+// the covering block's data, or the prediction from coarser levels; nv values per cell
 int emgo_amr_sample(void* h, int64_t l, const int64_t* g, size_t n, double* out) {
-    Amr* a = (Amr*)h;
-    if (l < 0 || l >= a->cfg.levels) return fail(EMG_ERR_INVALID, "level out of range");
+    return H(h)->with([&](auto& a) {
+        using A = std::decay_t<decltype(a)>;
+        if (l < 0 || l >= a.cfg.levels) return fail(EMG_ERR_INVALID, "level out of range");
 #pragma omp parallel for schedule(static)
-    for (int64_t i = 0; i < (int64_t)n; i++) {
-        V v = a->sample(l, {g[3 * i], g[3 * i + 1], g[3 * i + 2]});
-        for (int q = 0; q < 5; q++) out[5 * i + q] = v[q];
-    }
-    return EMG_OK;
+        for (int64_t i = 0; i < (int64_t)n; i++) {
+            auto v = a.sample(l, {g[3 * i], g[3 * i + 1], g[3 * i + 2]});
+            for (int q = 0; q < A::N; q++) out[A::N * i + q] = v[q];
+        }
+        return (int)EMG_OK;
+    });
 }
 
 }  // extern "C"

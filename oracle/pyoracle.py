@@ -400,13 +400,19 @@ SIGS_AMR = {
     "emgo_amr_steps": (C.c_int, [_P, _U64]),
     "emgo_amr_details": (C.c_int, [_P, _D, C.c_size_t]),
     "emgo_amr_sample": (C.c_int, [_P, C.c_int64, C.POINTER(C.c_int64), C.c_size_t, _D]),
+    "emgo_amr_nv": (C.c_int, [_P, C.POINTER(C.c_int)]),
 }
 
 
 def _amr_lib():
     L = lib()
     if not getattr(L, "_amr_ready", False):
-        for name, (res, args) in SIGS_AMR.items():
+        from emergence_b200._abi import EmgBc7, EmgFiveSystem
+        sigs = dict(SIGS_AMR)
+        sigs["emgo_amr_five_create"] = (C.c_int, [C.POINTER(EmgAmrConfig), C.POINTER(EmgFiveSystem), _D, _D,
+                                                  C.POINTER(EmgBc7), C.POINTER(EmgOpts), INIT_FN, C.c_void_p,
+                                                  C.POINTER(_P)])
+        for name, (res, args) in sigs.items():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
@@ -414,11 +420,11 @@ def _amr_lib():
     return L
 
 
-def make_init(fn):
-    """Wrap a numpy init(x[n,3]) -> w[n,5] as the C callback type."""
+def make_init(fn, nv=5):
+    """Wrap a numpy init(x[n,3]) -> w[n,nv] (primitives) as the C callback type."""
     def cb(ctx, x, n, w):
         xa = np.ctypeslib.as_array(x, shape=(n, 3)).copy()
-        wa = np.ctypeslib.as_array(w, shape=(n, 5))
+        wa = np.ctypeslib.as_array(w, shape=(n, nv))
         wa[...] = fn(xa)
     return INIT_FN(cb)
 
@@ -432,22 +438,35 @@ def c_amr_config(cfg):
 
 
 class OracleAmr:
-    """C++ restatement of ``compressible::amr::Amr`` (global time step)."""
+    """C++ restatement of ``compressible::amr::Amr`` (global and subcycled
+    steps) for the Euler system or, when ``sys`` is a FiveEq, the
+    five-equation system (7 variables; ``init`` gives 7 primitives)."""
 
     def __init__(self, sys, cfg, lo, hi, bc, init, cfl=0.4, mode=FluxMode.Hybrid, tol=1e-3, positivity=True,
                  subcycle=False):
-        from emergence_b200.solver import _c_bcs
         L = _amr_lib()
         self.cfg = dict(cfg)
         self._c = c_amr_config(cfg)
-        self._e = c_eos(sys.eos)
-        self._b = _c_bcs(bc)
         self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, 0, 2 if subcycle else 0)
-        self._cb = make_init(init)
         lo_, hi_ = arr(lo), arr(hi)
         h = C.c_void_p()
-        _chk(L.emgo_amr_create(C.byref(self._c), C.byref(self._e), dptr(lo_), dptr(hi_), self._b, C.byref(self._o),
-                               self._cb, None, C.byref(h)))
+        from emergence_b200.five import FiveEq
+        if isinstance(sys, FiveEq):
+            from emergence_b200.five import _c_bcs7, _c_system
+            self.nv = 7
+            self._e = _c_system(sys)
+            self._b = _c_bcs7(bc)
+            self._cb = make_init(init, 7)
+            _chk(L.emgo_amr_five_create(C.byref(self._c), C.byref(self._e), dptr(lo_), dptr(hi_), self._b,
+                                        C.byref(self._o), self._cb, None, C.byref(h)))
+        else:
+            from emergence_b200.solver import _c_bcs
+            self.nv = 5
+            self._e = c_eos(sys.eos)
+            self._b = _c_bcs(bc)
+            self._cb = make_init(init)
+            _chk(L.emgo_amr_create(C.byref(self._c), C.byref(self._e), dptr(lo_), dptr(hi_), self._b,
+                                   C.byref(self._o), self._cb, None, C.byref(h)))
         self._h = h
         self.bcells = 1
         for d in range(3):
@@ -501,12 +520,12 @@ class OracleAmr:
 
     def download(self):
         nb, _ = self.block_count()
-        out = np.zeros((nb, self.bcells, 5))
+        out = np.zeros((nb, self.bcells, self.nv))
         _chk(_amr_lib().emgo_amr_download(self._h, dptr(out), nb))
         return out
 
     def totals(self):
-        out = np.zeros(5)
+        out = np.zeros(self.nv)
         _chk(_amr_lib().emgo_amr_totals(self._h, dptr(out)))
         return out
 
@@ -525,7 +544,7 @@ class OracleAmr:
         """Conserved states at level-``level`` cell coordinates g (int [n, 3]):
         the covering leaf's data or its prediction (Amr::sample)."""
         g = np.ascontiguousarray(g, dtype=np.int64).reshape(-1, 3)
-        out = np.zeros((len(g), 5))
+        out = np.zeros((len(g), self.nv))
         _chk(_amr_lib().emgo_amr_sample(self._h, int(level), g.ctypes.data_as(C.POINTER(C.c_int64)), len(g), dptr(out)))
         return out
 
