@@ -83,6 +83,22 @@ def run_amr_subcycled():
     return float(err.max())
 
 
+def run_amr_five():
+    s, cfg, lo, hi, bc, init = W.two_phase_amr_bubble(dim=2, base=4, levels=3)
+    o = O.OracleAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno)
+    g = GpuAmr(s, cfg, lo, hi, bc, mode=FluxMode.Weno, blocks=(o.structure(), o.download()))
+    for _ in range(5):  # a regrid after step 4
+        dt = o.dt_cfl()
+        g.step(dt)
+        o.step(dt)
+    assert np.array_equal(o.structure(), g.structure())
+    ug, uo = g.download(), o.download()
+    err = np.abs(ug - uo).reshape(-1, 7).sum(axis=0) / np.maximum(np.abs(uo).reshape(-1, 7).sum(axis=0), 1e-300)
+    assert np.all(err <= 1e-12), err
+    g.close()
+    return float(err.max())
+
+
 def run_five():
     from emergence_b200 import GpuFiveSolver
     sys5, mesh, u, bc = W.two_phase_shock_bubble(n=24)
@@ -111,6 +127,7 @@ def main():
     print("subcycled amr 2-D shock-bubble with regrids: rel L1", run_amr_subcycled(), flush=True)
     run_five()
     print("five-equation 3-D shock-bubble 24^3: ok", flush=True)
+    print("five-equation AMR 2-D shock-bubble with a regrid: rel L1", run_amr_five(), flush=True)
     run_batch()
     print("batched lines: ok", flush=True)
     print("BOUNDS_CHECK_OK")
