@@ -1,8 +1,8 @@
 // Tensor-memory-accelerator (TMA) staging helpers of the fused sweep, sm_100a:
 // an mbarrier in shared memory, the tiled bulk tensor load
-// (cp.async.bulk.tensor, no cluster multicast: every tensor map covers this
-// GPU's own memory and every load lands in the issuing CTA's own shared
-// memory) and a bounded wait on the barrier's phase.
+// (cp.async.bulk.tensor into the issuing CTA's own shared memory only, from a
+// tensor map over this GPU's own memory) and a bounded wait on the barrier's
+// phase.
 #pragma once
 #include <cuda.h>
 #include <stdint.h>
