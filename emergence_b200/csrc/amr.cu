@@ -2,10 +2,12 @@
 // compressible-cuda's GpuAmr (fluid/crates/compressible-cuda/src/amr.rs:95-858)
 // for the Euler system.
 //
-// The hierarchy bookkeeping (which blocks exist, block ids, 2:1 balance,
-// refine/coarsen decisions) runs on the host and keeps the block ids of the
-// reference CPU solver (fluid/crates/compressible/src/amr.rs), so the device
-// pool, indexed by block id, mirrors `Amr::blocks`. All numerical work —
+// The block ids follow the reference CPU solver's (fluid/crates/compressible/
+// src/amr.rs), so the device pool, indexed by block id, mirrors `Amr::blocks`.
+// Regrid decisions and hierarchy edits (flags, buffer, 2:1-balanced
+// refinement, coarsening with swap-remove compaction) run on the device
+// (amr_regrid.cuh); the host keeps a mirror of the tree, read back after each
+// regrid, from which it builds the launch lists. All numerical work —
 // restriction of edge ancestors, the six face ghost slabs of every leaf
 // (same-level copies, 6th-order prediction from the coarser level, boundary
 // conditions; edge and corner ghost regions are never read), the fused WCNS
@@ -17,6 +19,7 @@
 // Built with -fmad=false (FP64 arithmetic rounds as the reference CPU's).
 #include "../../include/emergence_b200.h"
 #include "amr_kernels.cuh"
+#include "amr_regrid.cuh"
 #include "five_launch.h"
 #include "sweep_launch.h"
 
@@ -158,7 +161,6 @@ struct emg_amr {
     int rface_start[7]{};  // refluxing faces of bucket (d, side) = 2d + side: [rface_start[b], rface_start[b+1])
     DevVec<PBox> dtmp_pbox;    // one-off prediction boxes (refined children)
     DevVec<RBox> dtmp_rbox;    // one-off restriction boxes (coarsened parents)
-    DevVec<int> drem, dmoves;  // batch of coarsenings: removal order of fine blocks, block moves
     int amrP[3] = {0, 0, 0};      // tuned pencils per CTA of the sweeps (0: default)
     bool tuned = false;
     std::vector<PBox> pend_pbox;  // prediction boxes of refinements not yet launched
@@ -324,6 +326,7 @@ struct emg_amr {
         A.eos = EosD{eos.gamma, eos.p_inf, eos.b, eos.q};
         for (int k = 0; k < 2; k++) A.fsys.e[k] = EosD{five.eos[k].gamma, five.eos[k].p_inf, five.eos[k].b, five.eos[k].q};
         A.fsys.kapila = five.kapila;
+        A.id_limit = id_limit;
         A.err = err;
         return A;
     }
@@ -425,8 +428,8 @@ struct emg_amr {
         const size_t nb = blocks.size();
         if ((rc = dleaves.grow(2 * nb)) || (rc = dlevel.grow(2 * nb)) || (rc = didx.grow(6 * nb)) ||
             (rc = dbcleaves.grow(2 * nb)) || (rc = dcopy.grow(2 * dcopy.n)) || (rc = dpbox.grow(2 * dpbox.n)) ||
-            (rc = dreflux.grow(2 * dreflux.n)) || (rc = dtmp_pbox.grow(8 * nb)) || (rc = drem.grow(2 * nb)) ||
-            (rc = dmoves.grow(4 * nb)) || (rc = dtmp_rbox.grow(4 * nb)) || (rc = dmap_edits.grow(2 * map_size())))
+            (rc = dreflux.grow(2 * dreflux.n)) || (rc = dtmp_pbox.grow(8 * nb)) || (rc = dtmp_rbox.grow(4 * nb)) ||
+            (rc = dmap_edits.grow(2 * map_size())) || (rc = rg_grow()))
             return rc;
         for (auto& r : drbox)
             if ((rc = r.grow(2 * r.n))) return rc;
@@ -1305,82 +1308,6 @@ struct emg_amr {
         return EMG_OK;
     }
 
-    // Coarsenings of parents at level l (C/amr.rs:1014-1032, in candidate
-    // order). The hierarchy edits (parent becomes a leaf, children removed by
-    // swap-remove) run in sequence on the host; the restrictions of the whole
-    // batch then run as one set of launches on the pool as it was at the batch
-    // start, each box seeing the fine blocks removed by earlier coarsenings of
-    // the batch as absent (`rem`), and the block moves of the compaction follow
-    // in one launch. Parents of one level neither read nor write each other's
-    // data (a box reads level l + 1 only), so this equals the sequential order.
-    int coarsen_batch(int l, const std::vector<Key>& parents) {
-        int rc = upload_map();  // the device map as at the batch start
-        if (rc) return rc;
-        const int n0 = (int)blocks.size();
-        std::vector<int> orig(n0), rem(n0, INT32_MAX);
-        for (int i = 0; i < n0; i++) orig[i] = i;
-        std::vector<RBox> boxes;
-        for (const Key& idx : parents) {
-            const int pid = get(l, idx);
-            if (pid < 0) continue;
-            RBox b = make_rbox(l, orig[pid], idx, {0, 0, 0}, {bd[0], bd[1], bd[2]});
-            b.seq = (int)boxes.size();
-            boxes.push_back(b);
-            blocks[pid].leaf = true;
-            std::vector<int> ids;
-            for (auto& c : children(idx)) ids.push_back(get(l + 1, c));
-            std::sort(ids.begin(), ids.end(), [](int x, int y) { return x > y; });
-            for (int i : ids) {
-                rem[orig[i]] = b.seq;
-                remove(blocks[i].level, blocks[i].idx);
-                const int last = (int)blocks.size() - 1;
-                if (i != last) {
-                    blocks[i] = blocks[last];
-                    orig[i] = orig[last];
-                }
-                blocks.pop_back();
-                orig.pop_back();
-                if (i < (int)blocks.size()) insert(blocks[i].level, blocks[i].idx, i);
-            }
-            layout_valid = false;
-        }
-        if (boxes.empty()) return EMG_OK;
-        if ((rc = drem.put(rem, stream))) return rc;
-        if ((rc = dtmp_rbox.put(boxes, stream))) return rc;
-        // restrictions in chunks of up to 64 boxes (scratch of 64 whole-parent boxes)
-        const int chunk = 64;
-        for (int c0 = 0; c0 < (int)boxes.size(); c0 += chunk) {
-            const int nb = std::min<int>(chunk, (int)boxes.size() - c0);
-            int64_t off = 0, mx = 0;
-            std::vector<RBox> part(boxes.begin() + c0, boxes.begin() + c0 + nb);
-            for (auto& b : part) {
-                b.off = off;
-                off += b.cap;
-                mx = std::max(mx, b.cap);
-            }
-            if ((rc = scratch(off))) return rc;
-            if ((rc = dtmp_rbox.put(part, stream))) return rc;
-            if ((rc = run_rboxes(dtmp_rbox.p, nb, mx, drem.p))) return rc;
-        }
-        // moves of the compaction: slot s < size now holds the block that was at orig[s]
-        std::vector<int> moves;
-        for (int s2 = 0; s2 < (int)blocks.size(); s2++)
-            if (orig[s2] != s2) {
-                moves.push_back(s2);
-                moves.push_back(orig[s2]);
-            }
-        if (!moves.empty()) {
-            if ((rc = dmoves.put(moves, stream))) return rc;
-            AmrDev A = view();
-            const int nm = (int)moves.size() / 2;
-            const unsigned cy = (unsigned)std::max(1, std::min(16, 296 / nm));
-            NVK(pool_move_list)<<<dim3((unsigned)nm, cy), 256, 0, stream>>>(A, dmoves.p);
-            launches++;
-        }
-        AMR_CUDA(cudaGetLastError());
-        return EMG_OK;
-    }
-
     int grow_det(int64_t n) {
         if (n <= det_cap) return EMG_OK;
         cudaFree(det);
@@ -1429,67 +1356,235 @@ struct emg_amr {
         return EMG_OK;
     }
 
-    // C/amr.rs:1039-1106
-    int regrid() {
-        std::vector<int8_t> f;
-        int rc = flags(f);  // restrict_all + details
+    // ---------------------------------------------------------------- regrid on the device
+    // Amr::regrid (C/amr.rs:1039-1106): flags, the one-block buffer, the
+    // refinements with 2:1 balance and the coarsening batches are decided and
+    // applied to a device copy of the tree (amr_regrid.cuh); the host mirror
+    // of the tree is then read back from the device, and the data work (the
+    // prediction of new children, the restriction of coarsened parents and the
+    // block moves of the compaction) runs as before, in the reference's order.
+    int id_limit = 0x7fffffff;  // see AmrDev::id_limit
+    DevVec<int> rg_level, rg_leaf, rg_count, rg_events, rg_rem, rg_orig, rg_moves;
+    DevVec<int64_t> rg_idx, rg_ckey, rg_par;
+    DevVec<signed char> rg_f, rg_wantd, rg_mark;
+    bool rg_ready = false;
+
+    RgTree rg_tree() const {
+        return RgTree{rg_level.p, rg_idx.p, rg_leaf.p, dmap.p, rg_count.p, (int)map_size()};
+    }
+    RgGeom rg_geom() const {
+        RgGeom G{};
+        for (int d = 0; d < 3; d++) {
+            G.act[d] = act[d];
+            G.nb0[d] = nb0[d];
+            G.periodic[d] = bckind(d, 0) == EMG_BC_PERIODIC;
+        }
+        G.levels = levels;
+        for (int l = 0; l < levels && l < AMR_MAX_LEVELS; l++) G.mapoff[l] = mapoff[l];
+        G.mapsize = (int64_t)map_size();
+        return G;
+    }
+    // the device tree's arrays, sized for every map slot (at most one block per slot)
+    int rg_grow() {
+        const size_t cap_ = map_size();
+        int rc;
+        if ((rc = rg_level.grow(cap_)) || (rc = rg_leaf.grow(cap_)) || (rc = rg_idx.grow(3 * cap_)) ||
+            (rc = rg_f.grow(cap_)) || (rc = rg_wantd.grow(cap_)) || (rc = rg_mark.grow(cap_)) || (rc = rg_events.grow(3 * cap_)) ||
+            (rc = rg_rem.grow(cap_)) || (rc = rg_orig.grow(cap_)) || (rc = rg_moves.grow(2 * cap_)) ||
+            (rc = rg_ckey.grow(4 * cap_)) || (rc = rg_par.grow(4 * cap_)) || (rc = rg_count.grow(8)))
+            return rc;
+        return EMG_OK;
+    }
+    // the host mirror to the device tree
+    int rg_upload_tree() {
+        int rc = rg_grow();
         if (rc) return rc;
-        std::vector<std::pair<int, Key>> want;
-        for (size_t i = 0; i < f.size(); i++) {
-            if (f[i] > 0) {
-                const HBlock& b = blocks[i];
-                want.push_back({b.level, b.idx});
-                for (auto& nk : neighbours(b.level, b.idx)) {
-                    int j = get(b.level, nk);
-                    if (j >= 0 && blocks[j].leaf) want.push_back({b.level, nk});
-                }
-            }
+        std::vector<int> lv(blocks.size()), lf(blocks.size());
+        std::vector<int64_t> ix(3 * blocks.size());
+        for (size_t i = 0; i < blocks.size(); i++) {
+            lv[i] = blocks[i].level;
+            lf[i] = blocks[i].leaf ? 1 : 0;
+            for (int d = 0; d < 3; d++) ix[3 * i + d] = blocks[i].idx[d];
         }
-        std::sort(want.begin(), want.end());
-        want.erase(std::unique(want.begin(), want.end()), want.end());
-        std::set<std::pair<int, Key>> prot(want.begin(), want.end());
-        const size_t nb_before = blocks.size();
-        for (auto& k : want) {
-            int id = get(k.first, k.second);
-            if (id >= 0 && k.first + 1 < levels)
-                if ((rc = refine_block(id, nullptr, nullptr))) return rc;
+        std::vector<int> cnt(8, 0);
+        cnt[0] = (int)blocks.size();
+        if ((rc = rg_level.put(lv, stream)) || (rc = rg_leaf.put(lf, stream)) || (rc = rg_idx.put(ix, stream)) ||
+            (rc = rg_count.put(cnt, stream)))
+            return rc;
+        if (!rg_ready) {
+            AMR_CUDA(cudaFuncSetAttribute(rg_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, RG_SMEM_MAX));
+            AMR_CUDA(cudaFuncSetAttribute(rg_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, RG_SMEM_MAX));
+            rg_ready = true;
         }
-        if ((rc = flush_pboxes())) return rc;
-        // flags of the refined hierarchy; without a refinement they are the
-        // ones just computed (same leaves, same restriction and ghosts)
-        if (blocks.size() != nb_before && (rc = flags(f))) return rc;
-        const size_t nkids = (size_t)1 << dims.size();
-        std::vector<std::pair<int, Key>> cand;
-        for (size_t bi = 0; bi < blocks.size(); bi++) {
-            const HBlock& b = blocks[bi];
-            if (b.leaf) continue;
-            std::vector<Key> kids = children(b.idx);
-            bool ok = kids.size() == nkids;
-            for (auto& c : kids) {
-                if (!ok) break;
-                int j = get(b.level + 1, c);
-                ok = j >= 0 && blocks[j].leaf && f[j] < 0 && !prot.count({b.level + 1, c});
-            }
-            if (ok) cand.push_back({b.level, b.idx});
+        return EMG_OK;
+    }
+    static constexpr int RG_SMEM_MAX = 200 * 1024;
+    int rg_counts(int* c) {
+        AMR_CUDA(cudaMemcpyAsync(c, rg_count.p, 8 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        AMR_CUDA(cudaStreamSynchronize(stream));
+        if (c[3]) return set_error(EMG_ERR_CUDA, "device regrid: tree capacity or recursion bound exceeded");
+        return EMG_OK;
+    }
+    // the host mirror of the tree read back from the device (the device block map is current)
+    int rg_mirror() {
+        int c[8];
+        int rc = rg_counts(c);
+        if (rc) return rc;
+        const int nb = c[0];
+        std::vector<int> lv(nb), lf(nb);
+        std::vector<int64_t> ix(3 * (size_t)nb);
+        AMR_CUDA(cudaMemcpyAsync(lv.data(), rg_level.p, nb * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        AMR_CUDA(cudaMemcpyAsync(lf.data(), rg_leaf.p, nb * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        AMR_CUDA(cudaMemcpyAsync(ix.data(), rg_idx.p, 3 * (size_t)nb * sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
+        AMR_CUDA(cudaStreamSynchronize(stream));
+        blocks.resize(nb);
+        for (auto& m : map) std::fill(m.begin(), m.end(), -1);
+        for (int i = 0; i < nb; i++) {
+            blocks[i] = HBlock{lv[i], Key{ix[3 * i], ix[3 * i + 1], ix[3 * i + 2]}, lf[i] != 0};
+            const int64_t sl = slot_of(lv[i], blocks[i].idx);
+            if (sl >= 0) map[lv[i]][sl] = i;
         }
-        std::stable_sort(cand.begin(), cand.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
-        // the decisions of one level do not depend on that level's coarsenings
-        // (they look at level l + 1 blocks that are not children of a candidate
-        // of the level), so they are taken before the level's batch runs
-        for (size_t ci = 0; ci < cand.size();) {
-            const int l = cand[ci].first;
-            std::vector<Key> batch;
-            for (; ci < cand.size() && cand[ci].first == l; ci++) {
-                const Key& key = cand[ci].second;
-                bool ok = true;
-                for (auto& nk : neighbours(l, key))
-                    for (auto& ch : children(nk)) {
-                        int j = get(l + 1, ch);
-                        if (j >= 0 && !blocks[j].leaf) ok = false;
+        map_changed.clear();
+        map_dirty = false;  // the device map holds the same edits
+        map_uploaded = true;
+        layout_valid = false;
+        return EMG_OK;
+    }
+    // wavelet details of every leaf into `det` (ancestors 0), on the device only
+    int details_device() {
+        int rc = ensure_layout();
+        if (rc) return rc;
+        if ((rc = fill_ghosts())) return rc;
+        if ((rc = grow_det((int64_t)blocks.size()))) return rc;
+        AMR_CUDA(cudaMemsetAsync(det, 0, blocks.size() * sizeof(unsigned long long), stream));
+        AmrDev A = view();
+        PHK(amr_detail)<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0, stream>>>(
+            A, dleaves.p, det);
+        launches++;
+        AMR_CUDA(cudaGetLastError());
+        return EMG_OK;
+    }
+    int rg_flags_now(int nb) {
+        RgTree T = rg_tree();
+        rg_flags<<<(nb + 255) / 256, 256, 0, stream>>>(T, det, nb, levels, cfg.eps, rg_f.p);
+        launches++;
+        AMR_CUDA(cudaGetLastError());
+        return EMG_OK;
+    }
+
+    int regrid() {
+        int rc = restrict_all();  // and the layout, with the device map
+        if (rc) return rc;
+        if ((rc = details_device())) return rc;
+        const int nb0_ = (int)blocks.size();
+        if ((rc = rg_upload_tree())) return rc;
+        RgTree T = rg_tree();
+        const RgGeom G = rg_geom();
+        if ((rc = rg_flags_now(nb0_))) return rc;
+        rg_want<<<(nb0_ + 255) / 256, 256, 0, stream>>>(T, G, rg_f.p, nb0_, rg_wantd.p);
+        const size_t msm = map_size() * sizeof(int);
+        const int in_smem = msm <= (size_t)RG_SMEM_MAX ? 1 : 0;
+        rg_refine<<<1, 256, in_smem ? msm : 0, stream>>>(T, G, rg_wantd.p, nb0_, in_smem, rg_events.p);
+        launches += 2;
+        AMR_CUDA(cudaGetLastError());
+        int c[8];
+        if ((rc = rg_counts(c))) return rc;
+        if (c[0] != nb0_) {
+            // the refined tree, then the children's data in the reference's order:
+            // refinements of parents of one level in one launch, each such batch
+            // seeing only the blocks that existed when its first refinement ran
+            const int nev = c[1];
+            std::vector<int> ev(3 * (size_t)nev);
+            AMR_CUDA(cudaMemcpyAsync(ev.data(), rg_events.p, ev.size() * sizeof(int), cudaMemcpyDeviceToHost, stream));
+            AMR_CUDA(cudaStreamSynchronize(stream));
+            if ((rc = rg_mirror())) return rc;
+            if ((rc = reserve((int64_t)blocks.size()))) return rc;
+            for (int e0 = 0; e0 < nev;) {
+                const int l = ev[3 * e0 + 2];
+                int e1 = e0;
+                std::vector<PBox> boxes;
+                while (e1 < nev && ev[3 * e1 + 2] == l) {
+                    const int first = ev[3 * e1 + 1];
+                    const std::vector<Key> kids = children(blocks[ev[3 * e1]].idx);
+                    for (size_t n = 0; n < kids.size(); n++) {
+                        Key fmin, fmax;
+                        for (int d = 0; d < 3; d++) {
+                            fmin[d] = kids[n][d] * bd[d];
+                            fmax[d] = kids[n][d] * bd[d] + bd[d] - 1;
+                        }
+                        boxes.push_back(make_pbox(l + 1, fmin, fmax, first + (int)n, gof));
                     }
-                if (ok && get(l, key) >= 0) batch.push_back(key);
+                    e1++;
+                }
+                id_limit = ev[3 * e0 + 1];
+                rc = predict_now(std::move(boxes));
+                id_limit = 0x7fffffff;
+                if (rc) return rc;
+                e0 = e1;
             }
-            if ((rc = coarsen_batch(l, batch))) return rc;
+            // flags of the refined hierarchy
+            if ((rc = restrict_all()) || (rc = details_device()) || (rc = rg_flags_now((int)blocks.size()))) return rc;
+        }
+        // coarsening, level by level from the finest
+        const size_t msm2 = in_smem ? msm : 0;
+        {
+            const int nb = (int)blocks.size();
+            rg_candidate_flags<<<(nb + 255) / 256, 256, 0, stream>>>(T, G, rg_f.p, rg_wantd.p, nb0_, rg_mark.p);
+            rg_compact<<<1, RG_SCAN_T, 0, stream>>>(T, rg_mark.p, rg_ckey.p);
+            launches += 2;
+            AMR_CUDA(cudaGetLastError());
+            if ((rc = rg_counts(c))) return rc;
+        }
+        const int ncand = c[4];
+        for (int l = levels - 2; l >= 0 && ncand > 0; l--) {
+            rg_decide_flags<<<(ncand + 255) / 256, 256, 0, stream>>>(T, G, rg_ckey.p, l, rg_mark.p);
+            rg_decide<<<1, 256, 0, stream>>>(T, G, rg_ckey.p, rg_mark.p, l, rg_par.p, rg_rem.p);
+            launches += 2;
+            AMR_CUDA(cudaGetLastError());
+            if ((rc = rg_counts(c))) return rc;
+            const int npar = c[5];
+            if (!npar) continue;
+            std::vector<int64_t> par(4 * (size_t)npar);
+            AMR_CUDA(cudaMemcpyAsync(par.data(), rg_par.p, par.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
+            AMR_CUDA(cudaStreamSynchronize(stream));
+            // restrictions on the pool and the map as before the batch, each box
+            // seeing the fine blocks removed by earlier parents of the batch as absent
+            if ((rc = upload_map())) return rc;
+            std::vector<RBox> boxes;
+            for (int q = 0; q < npar; q++) {
+                const Key key = {par[4 * q + 1], par[4 * q + 2], par[4 * q + 3]};
+                RBox b = make_rbox(l, (int)par[4 * q], key, {0, 0, 0}, {bd[0], bd[1], bd[2]});
+                b.seq = q;
+                boxes.push_back(b);
+            }
+            const int chunk = 64;
+            for (int c0 = 0; c0 < (int)boxes.size(); c0 += chunk) {
+                const int nbx = std::min<int>(chunk, (int)boxes.size() - c0);
+                int64_t off = 0, mx = 0;
+                std::vector<RBox> part(boxes.begin() + c0, boxes.begin() + c0 + nbx);
+                for (auto& b : part) {
+                    b.off = off;
+                    off += b.cap;
+                    mx = std::max(mx, b.cap);
+                }
+                if ((rc = scratch(off))) return rc;
+                if ((rc = dtmp_rbox.put(part, stream))) return rc;
+                if ((rc = run_rboxes(dtmp_rbox.p, nbx, mx, rg_rem.p))) return rc;
+            }
+            // the edits, then the block moves of the compaction
+            rg_apply<<<1, 256, msm2, stream>>>(T, G, rg_par.p, l, in_smem, rg_orig.p, rg_moves.p);
+            launches++;
+            AMR_CUDA(cudaGetLastError());
+            if ((rc = rg_counts(c))) return rc;
+            const int nm = c[6];
+            if (nm) {
+                AmrDev A = view();
+                const unsigned cy = (unsigned)std::max(1, std::min(16, 296 / nm));
+                NVK(pool_move_list)<<<dim3((unsigned)nm, cy), 256, 0, stream>>>(A, rg_moves.p);
+                launches++;
+                AMR_CUDA(cudaGetLastError());
+            }
+            if ((rc = rg_mirror())) return rc;
         }
         rate_valid = false;
         return EMG_OK;
@@ -2189,8 +2284,9 @@ struct emg_amr {
         dreflux.release();
         dtmp_pbox.release();
         dtmp_rbox.release();
-        drem.release();
-        dmoves.release();
+        for (auto* v : {&rg_level, &rg_leaf, &rg_count, &rg_events, &rg_rem, &rg_orig, &rg_moves}) v->release();
+        for (auto* v : {&rg_idx, &rg_ckey, &rg_par}) v->release();
+        for (auto* v : {&rg_f, &rg_wantd, &rg_mark}) v->release();
         dstage.release();
         if (stream) cudaStreamDestroy(stream);
     }

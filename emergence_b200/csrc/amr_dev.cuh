@@ -37,6 +37,7 @@ struct AmrDev {
     double wrs[5][6];      // restriction weights by shift m (amr.rs:670-671)
     EosD eos;              // Euler system
     FiveSysD fsys;         // five-equation system
+    int id_limit;          // block ids at or above it read as absent (predictions replaying a regrid's order)
     unsigned int* err;     // error word (depth overflow)
 };
 
@@ -63,7 +64,8 @@ __device__ __forceinline__ int amr_get(const AmrDev& A, int l, const int64_t* k)
         if (k[d] < 0 || k[d] >= n) return -1;
         s = s * n + k[d];
     }
-    return A.map[A.mapoff[l] + s];
+    const int id = A.map[A.mapoff[l] + s];
+    return id < A.id_limit ? id : -1;
 }
 
 __device__ __forceinline__ int64_t amr_cell(const AmrDev& A, const int64_t* c) {
