@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed"])
-    ap.add_argument("--n", type=int, default=N_CELLS, help="cells per side (default 256)")
+    ap.add_argument("--n", "--grid", dest="n", type=int, default=N_CELLS, help="cells per side (default 256)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg of the uniform workload")

@@ -60,7 +60,8 @@ def test_reference_arm_under_torchrun_prints_one_line():
     the CPU reference and prints the only JSON line; rank 1 exits 0."""
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(_free_port()),
-           os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1"]
+           os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "1",
+           "--grid", "48"]  # a small grid: the default is the full 256^3 workload
     p = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600,
                        env={**os.environ, "OMP_NUM_THREADS": "2"})
     assert p.returncode == 0, p.stderr[-2000:]
