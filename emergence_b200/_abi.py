@@ -73,6 +73,7 @@ SIGNATURES = {
     "emg_uniform_create": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgEos), C.POINTER(EmgBc), C.POINTER(EmgOpts),
                                      _D, C.c_size_t, C.POINTER(_P)]),
     "emg_uniform_destroy": (C.c_int, [_P]),
+    "emg_release_memory": (C.c_int, []),
     "emg_five_create": (C.c_int, [C.POINTER(EmgMesh), C.POINTER(EmgFiveSystem), C.POINTER(EmgBc7), C.POINTER(EmgOpts),
                                   _D, C.c_size_t, C.POINTER(_P)]),
     "emg_five_destroy": (C.c_int, [_P]),

@@ -926,6 +926,49 @@ static int check_uniform_args(const emg_mesh* mesh, const emg_bc bc[6], const em
     return EMG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// The large state buffers of uniform-grid solvers come from a library-owned
+// stream-ordered memory pool per device that keeps up to 32 GB of freed
+// memory: cudaMalloc of a 256^3 state (4 GB over five buffers) costs 5-60 ms,
+// and a solver created after another one was destroyed reuses its memory.
+// emg_release_memory returns the kept memory to the device.
+std::mutex pool_mu;
+cudaMemPool_t pools[64] = {};
+cudaMemPool_t state_pool(int dev) {
+    if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(pool_mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = 32ull << 30;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[dev] = p;
+    }
+    return pools[dev];
+}
+}  // namespace
+
+extern "C" {
+
+int emg_release_memory(void) {
+    std::lock_guard<std::mutex> lk(pool_mu);
+    for (auto& p : pools)
+        if (p && cudaMemPoolTrimTo(p, 0) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(EMG_ERR_CUDA, "memory pool trim failed");
+        }
+    return EMG_OK;
+}
+
 int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
                        const double* u_aos, size_t len, emg_uniform** out) {
     if (!mesh || !eos || !bc || !opts || !u_aos || !out) return set_error(EMG_ERR_INVALID, "null argument");
@@ -982,9 +1025,14 @@ int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(set_error(EMG_ERR_CUDA, "cudaStreamCreate failed"));
     const size_t bytes = (size_t)h->ncell * 5 * sizeof(double);
-    if (cudaMalloc(&h->u, bytes) != cudaSuccess || cudaMalloc(&h->sa, bytes) != cudaSuccess ||
-        cudaMalloc(&h->sb, bytes) != cudaSuccess || cudaMalloc(&h->rhs, bytes) != cudaSuccess ||
-        cudaMalloc(&h->staging, bytes) != cudaSuccess || cudaMalloc(&h->partial, 5 * 4096 * sizeof(double)) != cudaSuccess ||
+    cudaMemPool_t pool = state_pool(h->device);
+    if (!pool) return bail(set_error(EMG_ERR_CUDA, "device memory pool unavailable"));
+    if (cudaMallocFromPoolAsync((void**)&h->u, bytes, pool, h->stream) != cudaSuccess ||
+        cudaMallocFromPoolAsync((void**)&h->sa, bytes, pool, h->stream) != cudaSuccess ||
+        cudaMallocFromPoolAsync((void**)&h->sb, bytes, pool, h->stream) != cudaSuccess ||
+        cudaMallocFromPoolAsync((void**)&h->rhs, bytes, pool, h->stream) != cudaSuccess ||
+        cudaMallocFromPoolAsync((void**)&h->staging, bytes, pool, h->stream) != cudaSuccess ||
+        cudaMalloc(&h->partial, 5 * 4096 * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&h->ctl, sizeof(StepCtl)) != cudaSuccess ||
         cudaMallocHost(&h->ctl_host, sizeof(StepCtl)) != cudaSuccess) {
         cudaGetLastError();
@@ -1013,12 +1061,13 @@ int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc
 int emg_uniform_destroy(emg_uniform* h) {
     if (!h) return EMG_OK;
     cudaSetDevice(h->device);
-    if (h->stream) cudaStreamSynchronize(h->stream);
-    cudaFree(h->u);
-    cudaFree(h->sa);
-    cudaFree(h->sb);
-    cudaFree(h->rhs);
-    cudaFree(h->staging);
+    // the state buffers go back to the library's pool (stream-ordered), the rest is freed
+    if (h->stream) {
+        for (double* p : {h->u, h->sa, h->sb, h->rhs, h->staging})
+            if (p) cudaFreeAsync(p, h->stream);
+        cudaStreamSynchronize(h->stream);
+    }
+    cudaGetLastError();
     cudaFree(h->partial);
     cudaFree(h->ctl);
     if (h->ctl_host) cudaFreeHost(h->ctl_host);

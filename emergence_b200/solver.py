@@ -211,3 +211,9 @@ def device_count():
     n = C.c_int()
     check(lib().emg_device_count(C.byref(n)))
     return n.value
+
+
+def release_memory():
+    """Give the device memory that destroyed solvers left in the library's
+    stream-ordered pools back to the device."""
+    check(lib().emg_release_memory())

@@ -145,8 +145,15 @@ typedef struct emg_uniform emg_uniform;
 int emg_uniform_create(const emg_mesh* mesh, const emg_eos* eos, const emg_bc bc[6], const emg_opts* opts,
                        const double* u_aos, size_t len, emg_uniform** out);
 
-/* Free the handle and its device memory (Drop of GpuSolver). */
+/* Free the handle and its device memory (Drop of GpuSolver). The five
+ * state-sized arrays return to a library-owned stream-ordered pool per
+ * device, which keeps up to 32 GB of freed memory so that the next
+ * emg_uniform_create reuses it instead of calling the driver. */
 int emg_uniform_destroy(emg_uniform* h);
+
+/* Return the memory kept by the library's pools to the device (no Rust
+ * counterpart: the reference frees through cudarc on drop). */
+int emg_release_memory(void);
 
 /* One SSP-RK3 step of size dt (G/lib.rs:402-412; C/solver.rs:659-738). */
 int emg_uniform_step(emg_uniform* h, double dt);

@@ -379,3 +379,21 @@ def test_download_into_a_pinned_host_buffer():
     assert np.array_equal(pinned, ref)
     with pytest.raises(ValueError):
         g.download(out=np.empty((3, 5)))
+
+
+def test_solvers_built_on_reused_pool_memory_give_identical_results():
+    """The state arrays of a destroyed solver return to the library's memory
+    pool and the next solver of the same size is built on them, stale data
+    and all: its steps are bit for bit those of the first solver, and so are
+    those of a solver built after the pool was trimmed."""
+    from emergence_b200 import release_memory
+    sys, mesh, u, bc = W.explosion((48, 40, 24), 0.3)
+    r = []
+    for trim in (False, False, True):
+        if trim:
+            release_memory()
+        g = gpu_solver(sys, mesh, u, bc=bc, mode=FluxMode.Weno)
+        g.advance(4)
+        r.append((g.download(), g.t))
+        g.close()
+    assert all(np.array_equal(r[0][0], x[0]) and r[0][1] == x[1] for x in r[1:])
