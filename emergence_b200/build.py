@@ -10,8 +10,9 @@ Translation units and their FMA policy:
   five.cu         five-equation two-phase system, C ABI           -fmad=false
   sweep_f64.cu    plain FP64 fused sweep                          -fmad=false
   sweep_mixed.cu  FP32-flux fused sweep                           -fmad=true
-The FP64 units keep every multiply and add separately rounded so that their
-results round exactly as the reference CPU solver's.
+  sweep_fast.cu   fast FP64 fused sweep (within 1e-12)            -fmad=true
+The plain FP64 units keep every multiply and add separately rounded so that
+their results round exactly as the reference CPU solver's.
 """
 import os
 import subprocess
@@ -34,6 +35,7 @@ UNITS = [
     ("five.cu", ["-fmad=false"]),
     ("sweep_f64.cu", ["-fmad=false"]),
     ("sweep_mixed.cu", ["-fmad=true", "-use_fast_math"]),
+    ("sweep_fast.cu", ["-fmad=true"]),
 ]
 
 

@@ -272,6 +272,143 @@ template <typename R> __device__ __forceinline__ R weno5z_interp(R v0, R v1, R v
     }
 }
 
+// ------------------------------------------------------------------ fast FP64 form
+// Reciprocal and square roots to about one ulp without the correctly rounded
+// division: the PTX estimate (good to about 2^-20) refined by one step of the
+// series 1/(1 − h) = 1 + h + h² + …, which cubes its relative error (Newton's
+// method with the quadratic term kept; for 1/y, h = 1 − y·r0 and
+// r = r0·(1 + h + h²); for 1/√x, h = 1 − x·r0² and r = r0·(1 + h/2 + 3h²/8),
+// the binomial series of (1 − h)^(−1/2)). The estimate's 2^-20 becomes
+// 2^-60, below the final rounding, so results are within about one ulp of the
+// correctly rounded ones. Zero, infinite and NaN inputs give non-finite
+// results, which the admissibility tests treat as they treat infinities;
+// subnormal inputs are flushed to zero. The fast FP64 form (EMG_PRECISION_
+// F64_FAST) uses these in its sweep; the plain FP64 form never does.
+__device__ __forceinline__ double rcp_f(double y) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(y));
+    const double h = fma(-y, r, 1.0);
+    return fma(r, fma(h, h, h), r);
+}
+__device__ __forceinline__ double rsqrt_f(double x) {
+    double r;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    const double h = fma(-(x * r), r, 1.0);
+    return fma(r * h, fma(0.375, h, 0.5), r);
+}
+
+// Fast FP64 form of the NASG/Euler maps. Algebraically equal to the
+// reference's formulas (eos.rs:37-60, system.rs:196-222), rearranged to
+// share one reciprocal of ρ: ρ·(1/ρ − b) = 1 − bρ removes the division of
+// ρe, and 1/(1/ρ − b) = ρ/(1 − bρ). `igm1` is 1/(γ − 1).
+__device__ __forceinline__ void to_prim_f(const Eos<double>& e, const double* u, double* w) {
+    const double rho = u[0];
+    const double irho = rcp_f(rho);
+    const double vx = u[1] * irho, vy = u[2] * irho, vz = u[3] * irho;
+    const double ein = u[4] * irho - 0.5 * (vx * vx + vy * vy + vz * vz);
+    const double rv = e.b == 0.0 ? rho : rho * rcp_f(1.0 - e.b * rho);  // 1/(v − b)
+    w[0] = rho;
+    w[1] = vx;
+    w[2] = vy;
+    w[3] = vz;
+    w[4] = (e.gamma - 1.0) * (ein - e.q) * rv - e.gamma * e.p_inf;
+}
+__device__ __forceinline__ double rho_e_f(const Eos<double>& e, double igm1, double rho, double p) {
+    return (p + e.gamma * e.p_inf) * (1.0 - e.b * rho) * igm1 + rho * e.q;
+}
+__device__ __forceinline__ void to_cons_f(const Eos<double>& e, double igm1, const double* w, double* u) {
+    const double rho = w[0];
+    const double ke = 0.5 * rho * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+    u[0] = rho;
+    u[1] = rho * w[1];
+    u[2] = rho * w[2];
+    u[3] = rho * w[3];
+    u[4] = rho_e_f(e, igm1, rho, w[4]) + ke;
+}
+// c² = γ(p + p∞)·v²/(v − b), v = 1/ρ, as γ(p + p∞)/(ρ(1 − bρ))
+__device__ __forceinline__ double sound_speed_sq_f(const Eos<double>& e, double rho, double p) {
+    return e.gamma * (p + e.p_inf) * rcp_f(rho * (1.0 - e.b * rho));
+}
+__device__ __forceinline__ double sqrt_f(double x) {
+    // x ≥ 0; zero and +∞ pass through
+    return x > 0.0 && x <= 1.79769313486231570e308 ? x * rsqrt_f(x) : x;
+}
+__device__ __forceinline__ double sound_speed_f(const Eos<double>& e, double rho, double p) {
+    return sqrt_f(fmax(sound_speed_sq_f(e, rho, p), 0.0));
+}
+// system.rs:404-407 with eos.rs:75-79: 1/ρ > b ⟺ bρ < 1 for finite ρ > 0
+__device__ __forceinline__ bool admissible_f(const Eos<double>& e, double rho, double p) {
+    return isfinite(rho) && isfinite(p) && rho > 0.0 && e.b * rho < 1.0 && p + e.p_inf > 0.0;
+}
+
+// HLLC of the fast form (system.rs:260-312): the same wave-speed bounds,
+// contact speed and star states with shared reciprocals.
+__device__ __forceinline__ double hllc_f(const Eos<double>& e, double igm1, const double* wl, const double* wr, int un,
+                                         double* f) {
+    const double cl = sound_speed_f(e, wl[0], wl[4]), cr = sound_speed_f(e, wr[0], wr[4]);
+    const double ul = wl[un], ur = wr[un];
+    const double sl = fmin(ul - cl, ur - cr);
+    const double sr = fmax(ul + cl, ur + cr);
+    double ql[5], qr[5];
+    to_cons_f(e, igm1, wl, ql);
+    to_cons_f(e, igm1, wr, qr);
+    if (sl >= 0.0) {
+        flux_wq(wl, ql, un, f);
+        return ul;
+    }
+    if (sr <= 0.0) {
+        flux_wq(wr, qr, un, f);
+        return ur;
+    }
+    const double rl = wl[0], rr = wr[0], pl = wl[4], pr = wr[4];
+    const double ss = (pr - pl + rl * ul * (sl - ul) - rr * ur * (sr - ur)) * rcp_f(rl * (sl - ul) - rr * (sr - ur));
+    const bool left = ss >= 0.0;
+    const double* w = left ? wl : wr;
+    const double* q = left ? ql : qr;
+    const double s = left ? sl : sr;
+    double fx[5];
+    flux_wq(w, q, un, fx);
+    const double rho = w[0], u = w[un];
+    const double smu = s - u;
+    const double fac = rho * smu * rcp_f(s - ss);
+    // E/ρ + (S* − u)(S* + p/(ρ(S − u))), with 1/ρ and 1/(S − u) from one reciprocal
+    const double ir = rcp_f(rho * smu);
+    const double irho = ir * smu;
+    double qs[5];
+    qs[0] = fac;
+    qs[1] = fac * w[1];
+    qs[2] = fac * w[2];
+    qs[3] = fac * w[3];
+    qs[un] = fac * ss;
+    qs[4] = fac * (q[4] * irho + (ss - u) * (ss + w[4] * ir));
+#pragma unroll
+    for (int k = 0; k < 5; k++) f[k] = fx[k] + s * (qs[k] - q[k]);
+    return ss;
+}
+
+// WENO5-Z interpolation of the fast form (scheme.rs:67-86): the three
+// reciprocals 1/(β_k + ε) from one reciprocal of their product (each β_k + ε
+// lies in [1e-40, 1e100] for any state whose values stay below 1e50, so the
+// product neither under- nor overflows), and the normalisation by one more.
+__device__ __forceinline__ double weno5z_interp_f(double v0, double v1, double v2, double v3, double v4) {
+    const double eps = 1e-40;
+    const double q0 = (3.0 * v0 - 10.0 * v1 + 15.0 * v2) * 0.125;
+    const double q1 = (-v1 + 6.0 * v2 + 3.0 * v3) * 0.125;
+    const double q2 = (3.0 * v2 + 6.0 * v3 - v4) * 0.125;
+    const double b0 = (13.0 / 12.0) * sq(v0 - 2.0 * v1 + v2) + 0.25 * sq(v0 - 4.0 * v1 + 3.0 * v2);
+    const double b1 = (13.0 / 12.0) * sq(v1 - 2.0 * v2 + v3) + 0.25 * sq(v1 - v3);
+    const double b2 = (13.0 / 12.0) * sq(v2 - 2.0 * v3 + v4) + 0.25 * sq(3.0 * v2 - 4.0 * v3 + v4);
+    const double tau = fabs(b0 - b2);
+    const double x0 = b0 + eps, x1 = b1 + eps, x2 = b2 + eps;
+    const double x01 = x0 * x1;
+    const double t = tau * rcp_f(x01 * x2);
+    const double r0 = t * (x1 * x2), r1 = t * (x0 * x2), r2 = t * x01;
+    const double a0 = (1.0 / 16.0) * (1.0 + r0 * r0);
+    const double a1 = (10.0 / 16.0) * (1.0 + r1 * r1);
+    const double a2 = (5.0 / 16.0) * (1.0 + r2 * r2);
+    return (a0 * q0 + a1 * q1 + a2 * q2) * rcp_f(a0 + a1 + a2);
+}
+
 // Coefficients of the 6th-order schemes (scheme.rs:88-92).
 __device__ __forceinline__ double s6(int s) {
     return s == 0 ? (75.0 / 64.0 - 25.0 / 384.0 + 3.0 / 640.0) : (s == 1 ? (-25.0 / 384.0 + 3.0 / 640.0) : 3.0 / 640.0);

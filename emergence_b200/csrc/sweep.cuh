@@ -126,11 +126,21 @@ struct BatchSeg {
 // Flux modes (C/scheme.rs:39-47), a compile-time parameter of the sweep.
 enum SweepMode { MODE_HYBRID = 0, MODE_WENO = 1, MODE_CENTRAL = 2 };
 
+// Ring tag of the fast FP64 form: FP64 rings and arithmetic, with the
+// reciprocals and square roots of physics.cuh's fast section
+struct F64Fast {};
+
 template <typename R> struct RingTypes {
     static constexpr bool MIXED = false;
+    static constexpr bool FAST = false;
 };
 template <> struct RingTypes<float> {
     static constexpr bool MIXED = true;
+    static constexpr bool FAST = false;
+};
+template <> struct RingTypes<F64Fast> {
+    static constexpr bool MIXED = false;
+    static constexpr bool FAST = true;
 };
 
 // Ring slots: a power of two holding every row one round touches. WENO:
@@ -181,6 +191,7 @@ struct Sweep {
     static constexpr int STR = SM::STR;
     static constexpr int STRW = SM::STRW;
     static constexpr bool MIXED = RingTypes<RF>::MIXED;
+    static constexpr bool FAST = RingTypes<RF>::FAST;
     static constexpr bool MID = SM::MID;
     static constexpr int AHEAD = MODE == MODE_HYBRID ? 7 : 5;  // rows loaded beyond the round's midpoints
 
@@ -329,6 +340,70 @@ struct Sweep {
             }
         }
         hllc_fs(e, wl, wr, un, f);
+    }
+
+    // Fast FP64 form of the midpoint flux: the arithmetic of `midpoint` in
+    // FP64 with FMA contraction, one reciprocal of ρ and one reciprocal square
+    // root of c² for the eigenvector coefficients, and the fast WENO5-Z and
+    // HLLC of physics.cuh (about one ulp per reciprocal instead of a
+    // correctly rounded division).
+    __device__ static __forceinline__ void midpoint_fast(const Eos<double>& e, double igm1,
+                                                         const double* __restrict__ Wd, int m, int l, double* f,
+                                                         bool& fb) {
+        constexpr int un = 1 + D;
+        constexpr int t1 = 1 + (D + 1) % 3, t2 = 1 + (D + 2) % 3;
+        const int j = m + 2;
+        const double rho = 0.5 * (Wd[at<STRW>(j, 0, l)] + Wd[at<STRW>(j + 1, 0, l)]);
+        const double p4 = 0.5 * (Wd[at<STRW>(j, 4, l)] + Wd[at<STRW>(j + 1, 4, l)]);
+        const double c2 = fmax(sound_speed_sq_f(e, rho, p4), 0.0);
+        const double ic = rsqrt_f(c2);
+        const double c = c2 * ic;
+        const double l4un = 0.5 * rho * ic;
+        const double l0un = -l4un;
+        const double l04 = 0.5 * (ic * ic);
+        const double l14 = -(ic * ic);
+        const double run4 = c * rcp_f(rho);
+        const double run0 = -run4;
+        const double r40 = c2;
+        double cl[5], cr[5];
+#pragma unroll
+        for (int a = 0; a < 5; a++) {
+            double ch[6];
+#pragma unroll
+            for (int s2 = 0; s2 < 6; s2++) {
+                const int row = m + s2;
+                switch (a) {
+                    case 0: ch[s2] = l0un * Wd[at<STRW>(row, un, l)] + l04 * Wd[at<STRW>(row, 4, l)]; break;
+                    case 1: ch[s2] = Wd[at<STRW>(row, 0, l)] + l14 * Wd[at<STRW>(row, 4, l)]; break;
+                    case 2: ch[s2] = Wd[at<STRW>(row, t1, l)]; break;
+                    case 3: ch[s2] = Wd[at<STRW>(row, t2, l)]; break;
+                    default: ch[s2] = l4un * Wd[at<STRW>(row, un, l)] + l04 * Wd[at<STRW>(row, 4, l)];
+                }
+            }
+            cl[a] = weno5z_interp_f(ch[0], ch[1], ch[2], ch[3], ch[4]);
+            cr[a] = weno5z_interp_f(ch[5], ch[4], ch[3], ch[2], ch[1]);
+        }
+        double wl[5], wr[5];
+        wl[0] = (cl[0] + cl[1]) + cl[4];
+        wr[0] = (cr[0] + cr[1]) + cr[4];
+        wl[un] = run0 * cl[0] + run4 * cl[4];
+        wr[un] = run0 * cr[0] + run4 * cr[4];
+        wl[t1] = cl[2];
+        wr[t1] = cr[2];
+        wl[t2] = cl[3];
+        wr[t2] = cr[3];
+        wl[4] = r40 * (cl[0] + cl[4]);
+        wr[4] = r40 * (cr[0] + cr[4]);
+        fb = false;
+        if (!admissible_f(e, wl[0], wl[4]) || !admissible_f(e, wr[0], wr[4])) {
+            fb = true;
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                wl[k] = Wd[at<STRW>(j, k, l)];
+                wr[k] = Wd[at<STRW>(j + 1, k, l)];
+            }
+        }
+        hllc_f(e, igm1, wl, wr, un, f);
     }
 
     // KEEP-PE two-point flux with cached ρe (C/system.rs:317-334).
@@ -519,6 +594,7 @@ struct Sweep {
         const bool lim_on = p.positivity && lam > 0.0;  // C/scheme.rs:278
         const double inv = 1.0 / dx;
         const bool ideal_gas = ed.b == 0.0 && ed.q == 0.0 && ed.p_inf == 0.0 && ed.gamma > 1.0 && ed.gamma < 100.0;
+        const double igm1 = FAST ? 1.0 / (ed.gamma - 1.0) : 0.0;  // fast form: 1/(γ − 1)
         __syncthreads();  // lane table
         const int Lmax = BATCH ? s_maxlen : Ls;
         const int nrounds = (Lmax + 5 + RM - 1) / RM;
@@ -588,10 +664,14 @@ struct Sweep {
                         double u[5], w[5];
 #pragma unroll
                         for (int k = 0; k < 5; k++) u[k] = D == 2 ? stg[(k * P + l) * RM + rr] : stg[(k * RM + rr) * P + l];
-                        to_prim(ed, u, w);
+                        if constexpr (FAST)
+                            to_prim_f(ed, u, w);
+                        else
+                            to_prim(ed, u, w);
 #pragma unroll
                         for (int k = 0; k < 5; k++) W[at<STRW>(row, k, l)] = w[k];
-                        if constexpr (MODE != MODE_WENO) W[at<STRW>(row, 5, l)] = ed.rho_e(w[0], w[4]);
+                        if constexpr (MODE != MODE_WENO)
+                            W[at<STRW>(row, 5, l)] = FAST ? rho_e_f(ed, igm1, w[0], w[4]) : ed.rho_e(w[0], w[4]);
                         if constexpr (MODE == MODE_HYBRID) {
                             W[at<STRW>(row, 6, l)] = log(fmax(w[0], 1e-300));
                             W[at<STRW>(row, 7, l)] = log(fmax(w[4] + ed.p_inf, 1e-300));
@@ -618,12 +698,16 @@ struct Sweep {
                         double u[5], w[5];
 #pragma unroll
                         for (int k = 0; k < 5; k++) u[k] = __ldg(p.uin + k * p.ncell + g);
-                        to_prim(ed, u, w);
+                        if constexpr (FAST)
+                            to_prim_f(ed, u, w);
+                        else
+                            to_prim(ed, u, w);
 #pragma unroll
                         for (int k = 0; k < 5; k++) {
                             W[at<STRW>(row, k, l)] = w[k];
                         }
-                        if constexpr (MODE != MODE_WENO) W[at<STRW>(row, 5, l)] = ed.rho_e(w[0], w[4]);
+                        if constexpr (MODE != MODE_WENO)
+                            W[at<STRW>(row, 5, l)] = FAST ? rho_e_f(ed, igm1, w[0], w[4]) : ed.rho_e(w[0], w[4]);
                         if constexpr (MODE == MODE_HYBRID) {
                             // sensor values ln ρ, ln(p + p∞) (C/system.rs:409-413)
                             W[at<STRW>(row, 6, l)] = log(fmax(w[0], 1e-300));
@@ -672,6 +756,8 @@ struct Sweep {
                         bool fb;
                         if constexpr (MIXED)
                             midpoint_mixed(ed, W, m, l, f, fb);
+                        else if constexpr (FAST)
+                            midpoint_fast(ed, igm1, W, m, l, f, fb);
                         else
                             midpoint<STRW>(ed, W, m, l, f, fb);
 #pragma unroll
@@ -734,8 +820,13 @@ struct Sweep {
                             wi[k] = W[at<STRW>(i, k, l)];
                             wj[k] = W[at<STRW>(i + 1, k, l)];
                         }
-                        to_cons(ed, wi, ul);
-                        to_cons(ed, wj, ur);
+                        if constexpr (FAST) {
+                            to_cons_f(ed, igm1, wi, ul);
+                            to_cons_f(ed, igm1, wj, ur);
+                        } else {
+                            to_cons(ed, wi, ul);
+                            to_cons(ed, wj, ur);
+                        }
                         flux_wq(wi, ul, un, flp);
                         flux_wq(wj, ur, un, frp);
                         bool finite = true;

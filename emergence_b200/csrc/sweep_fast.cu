@@ -1,0 +1,83 @@
+// Fast FP64 form of the fused sweep: every value and operation in FP64, built
+// with FMA contraction, with the reciprocals and square roots of physics.cuh's
+// fast section in the primitive recovery, the midpoint (eigenvector
+// coefficients, WENO5-Z weights, admissibility, HLLC) and the limiter's
+// conserved states. Results stay within about 1e-12 relative L1 of the plain
+// FP64 form, which remains the bitwise parity form.
+#include "sweep_launch.h"
+
+namespace emg {
+
+template <int P, int D, int MODE>
+__global__ void __launch_bounds__(SWEEP_THREADS, 3) sweep_fast_kernel(const SweepParams p) {
+    Sweep<F64Fast, P, D, MODE, KIND_GRID>::run(p);
+}
+
+template <int P, int D, int MODE> static cudaError_t launch(const SweepParams& p, dim3 grid, cudaStream_t s) {
+    sweep_fast_kernel<P, D, MODE><<<grid, SWEEP_THREADS, SweepSmem<F64Fast, P, MODE>::bytes(), s>>>(p);
+    return cudaGetLastError();
+}
+
+template <int P, int MODE> static cudaError_t launch_d(const SweepParams& p, dim3 grid, cudaStream_t s) {
+    return p.d == 0 ? launch<P, 0, MODE>(p, grid, s) : (p.d == 1 ? launch<P, 1, MODE>(p, grid, s) : launch<P, 2, MODE>(p, grid, s));
+}
+
+template <int MODE> static cudaError_t launch_p(int P, const SweepParams& p, dim3 grid, cudaStream_t s) {
+    switch (P) {
+        case 8: return launch_d<8, MODE>(p, grid, s);
+        case 16: return launch_d<16, MODE>(p, grid, s);
+        case 32: return launch_d<32, MODE>(p, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t sweep_launch_fast(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s) {
+    switch (mode) {
+        case MODE_WENO: return launch_p<MODE_WENO>(P, p, grid, s);
+        case MODE_HYBRID: return launch_p<MODE_HYBRID>(P, p, grid, s);
+        case MODE_CENTRAL: return launch_p<MODE_CENTRAL>(P, p, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int P, int MODE> static cudaError_t attr_d() {
+    const int b = (int)SweepSmem<F64Fast, P, MODE>::bytes();
+    cudaError_t e = cudaFuncSetAttribute(sweep_fast_kernel<P, 0, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_fast_kernel<P, 1, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_fast_kernel<P, 2, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    return e;
+}
+
+template <int MODE> static cudaError_t attr_p() {
+    cudaError_t e = attr_d<8, MODE>();
+    if (e == cudaSuccess) e = attr_d<16, MODE>();
+    if (e == cudaSuccess) e = attr_d<32, MODE>();
+    return e;
+}
+
+cudaError_t sweep_prepare_fast() {
+    cudaError_t e = attr_p<MODE_WENO>();
+    if (e == cudaSuccess) e = attr_p<MODE_HYBRID>();
+    if (e == cudaSuccess) e = attr_p<MODE_CENTRAL>();
+    return e;
+}
+
+// resident CTAs per SM of the uniform-grid sweep (the three axes share registers and shared memory)
+template <int P, int MODE> static int occupancy() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_fast_kernel<P, 0, MODE>, SWEEP_THREADS,
+                                                      SweepSmem<F64Fast, P, MODE>::bytes()) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return n > 0 ? n : 1;
+}
+template <int MODE> static int occupancy_p(int P) {
+    return P == 8 ? occupancy<8, MODE>() : (P == 16 ? occupancy<16, MODE>() : occupancy<32, MODE>());
+}
+int sweep_ctas_per_sm_fast(int P, int mode) {
+    return mode == MODE_HYBRID ? occupancy_p<MODE_HYBRID>(P)
+                               : (mode == MODE_CENTRAL ? occupancy_p<MODE_CENTRAL>(P) : occupancy_p<MODE_WENO>(P));
+}
+
+}  // namespace emg

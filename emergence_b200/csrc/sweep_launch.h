@@ -1,6 +1,7 @@
 // Launchers of the fused sweep kernels (instantiated in sweep_f64.cu, which is
 // compiled without FMA contraction so its f64 arithmetic rounds like the
-// reference CPU solver, and in sweep_mixed.cu, FP32 flux arithmetic).
+// reference CPU solver, in sweep_mixed.cu, FP32 flux arithmetic, and in
+// sweep_fast.cu, the fast FP64 form on uniform grids).
 #pragma once
 #include "sweep.cuh"
 
@@ -8,6 +9,7 @@ namespace emg {
 // P = pencils per CTA (8, 16 or 32); mode = SweepMode. Returns the launch error.
 cudaError_t sweep_launch_f64(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 cudaError_t sweep_launch_mixed(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
+cudaError_t sweep_launch_fast(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 // Batched block-AMR leaves (SweepParams::amr set), P = 16 or 32.
 cudaError_t sweep_launch_amr_f64(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 cudaError_t sweep_launch_amr_mixed(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
@@ -25,9 +27,11 @@ int sweep_tma_ctas_per_sm_mixed();
 // Resident CTAs per SM of the uniform-grid sweep kernel (after the prepare call).
 int sweep_ctas_per_sm_f64(int P, int mode);
 int sweep_ctas_per_sm_mixed(int P, int mode);
+int sweep_ctas_per_sm_fast(int P, int mode);
 // Opt the kernels into their dynamic shared memory size (once per device).
 cudaError_t sweep_prepare_f64();
 cudaError_t sweep_prepare_mixed();
+cudaError_t sweep_prepare_fast();
 // Both forms' opt-ins for the current device, done once per device; safe to
 // call from several host threads.
 cudaError_t sweep_prepare_device();

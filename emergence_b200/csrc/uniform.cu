@@ -378,6 +378,7 @@ cudaError_t sweep_prepare_device() {
     if (dev >= 0 && dev < 64 && prepared[dev]) return cudaSuccess;
     e = sweep_prepare_f64();
     if (e == cudaSuccess) e = sweep_prepare_mixed();
+    if (e == cudaSuccess) e = sweep_prepare_fast();
     if (e == cudaSuccess && dev >= 0 && dev < 64) prepared[dev] = true;
     return e;
 }
@@ -438,8 +439,9 @@ int64_t plan_seg(const emg_uniform* h, int d, int P) {
         cudaGetLastError();
         sms = 148;
     }
-    const int per_sm = h->opts.precision == EMG_PRECISION_MIXED ? sweep_ctas_per_sm_mixed(P, h->opts.mode)
-                                                                 : sweep_ctas_per_sm_f64(P, h->opts.mode);
+    const int per_sm = h->opts.precision == EMG_PRECISION_MIXED      ? sweep_ctas_per_sm_mixed(P, h->opts.mode)
+                       : h->opts.precision == EMG_PRECISION_F64_FAST ? sweep_ctas_per_sm_fast(P, h->opts.mode)
+                                                                     : sweep_ctas_per_sm_f64(P, h->opts.mode);
     const int64_t slots = (int64_t)sms * per_sm;
     const int64_t lane_tiles = (nl + P - 1) / P;
     int64_t best = nd;
@@ -554,6 +556,7 @@ void setup_tma(emg_uniform* h) {
     const char* on = std::getenv("EMG_TMA");
     if (!on || on[0] != '1') return;
     if (h->ndim != 3 || h->opts.mode != EMG_MODE_WENO || h->mesh.ng % 2 != 0 || h->m[2] % 2 != 0) return;
+    if (h->opts.precision == EMG_PRECISION_F64_FAST) return;  // plain loads only
     const bool mixed = h->opts.precision == EMG_PRECISION_MIXED;
     const int plain = mixed ? sweep_ctas_per_sm_mixed(32, MODE_WENO) : sweep_ctas_per_sm_f64(32, MODE_WENO);
     const int staged = mixed ? sweep_tma_ctas_per_sm_mixed() : sweep_tma_ctas_per_sm_f64();
@@ -664,10 +667,12 @@ int launch_axis(emg_uniform* h, int stage, int d, double* in, bool first, bool l
             e = h->opts.precision == EMG_PRECISION_MIXED
                     ? sweep_launch_tma_mixed(p, h->tmap[buf][d], h->sweepGrid[d], h->stream)
                     : sweep_launch_tma_f64(p, h->tmap[buf][d], h->sweepGrid[d], h->stream);
+        else if (h->opts.precision == EMG_PRECISION_MIXED)
+            e = sweep_launch_mixed(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream);
+        else if (h->opts.precision == EMG_PRECISION_F64_FAST)
+            e = sweep_launch_fast(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream);
         else
-            e = h->opts.precision == EMG_PRECISION_MIXED
-                    ? sweep_launch_mixed(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream)
-                    : sweep_launch_f64(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream);
+            e = sweep_launch_f64(h->sweepP[d], h->opts.mode, p, h->sweepGrid[d], h->stream);
         if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("sweep launch: ") + cudaGetErrorString(e));
     }
     return EMG_OK;
@@ -913,7 +918,8 @@ static int check_uniform_args(const emg_mesh* mesh, const emg_bc bc[6], const em
         return set_error(EMG_ERR_INVALID, "unknown flux mode");
     if (opts->mode == EMG_MODE_HYBRID && !(opts->tol > 0.0))
         return set_error(EMG_ERR_INVALID, "hybrid mode needs tol > 0");
-    if (opts->precision != EMG_PRECISION_F64 && opts->precision != EMG_PRECISION_MIXED)
+    if (opts->precision != EMG_PRECISION_F64 && opts->precision != EMG_PRECISION_MIXED &&
+        opts->precision != EMG_PRECISION_F64_FAST)
         return set_error(EMG_ERR_INVALID, "unknown precision");
     for (int i = 0; i < 6; i++)
         if (bc[i].kind < 0 || bc[i].kind > 4) return set_error(EMG_ERR_INVALID, "unknown boundary condition");

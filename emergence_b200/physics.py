@@ -69,6 +69,7 @@ class FluxMode:
 class Precision:
     F64 = 0
     Mixed = 1
+    F64Fast = 2  # fast FP64 form (uniform grids): within 1e-12 relative L1 of F64 instead of bitwise
 
 
 @dataclass(frozen=True)

@@ -38,6 +38,13 @@ def test_reference_gpu_leg_is_on_by_default(monkeypatch):
     assert _parse(["--no-reference-gpu"], monkeypatch).reference_gpu is False
 
 
+def test_fast_form_is_a_uniform_workload_option(monkeypatch):
+    import pytest
+    assert _parse(["--precision", "fast"], monkeypatch).precision == "fast"
+    with pytest.raises(SystemExit):
+        _parse(["--precision", "fast", "--workload", "amr"], monkeypatch)
+
+
 def test_subrecords_are_on_by_default(monkeypatch):
     assert _parse([], monkeypatch).no_subrecords is False
     assert _parse(["--no-subrecords"], monkeypatch).no_subrecords is True

@@ -11,6 +11,8 @@ from the same initial state with the oracle's time steps:
 * mixed form (FP32 WENO-Z and wave-speed bounds, FP64 state): relative L1
   per conserved field within 1e-6 of the oracle, the stated error bound of
   that form; L∞ is reported.
+* fast FP64 form (FMA contraction, Newton-refined reciprocals): relative L1
+  within 1e-12.
 """
 import numpy as np
 import pytest
@@ -76,3 +78,14 @@ def test_mixed_form_error_against_the_oracle_at_256_cubed(oracle_run):
     linf = np.abs(mesh.interior(um) - mesh.interior(uo)).reshape(-1, 5).max(axis=0)
     print("256^3 mixed rel L1 vs oracle", err, "Linf", linf)
     assert np.all(err <= MIXED_TOL), err
+
+
+def test_fast_fp64_form_error_against_the_oracle_at_256_cubed(oracle_run):
+    """Fast FP64 form (FMA contraction, Newton-refined reciprocals): within the
+    plain form's 1e-12 relative L1 per conserved field."""
+    mesh, uo = oracle_run[1], oracle_run[5]
+    uf, _ = run_gpu(oracle_run, Precision.F64Fast)
+    err = rel_l1(uf, uo, mesh)
+    linf = np.abs(mesh.interior(uf) - mesh.interior(uo)).reshape(-1, 5).max(axis=0)
+    print("256^3 fast FP64 rel L1 vs oracle", err, "Linf", linf)
+    assert np.all(err <= F64_TOL), err
