@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed", "fast"],
-                    help="fast: the fast FP64 form (uniform workload only)")
+                    help="fast: the fast FP64 form (uniform and AMR workloads)")
     ap.add_argument("--n", "--grid", dest="n", type=int, default=N_CELLS, help="cells per side (default 256)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -74,8 +74,8 @@ def parse():
     ap.add_argument("--amr-base", type=int, default=8, help="AMR base blocks per side (16^3 cells each)")
     ap.add_argument("--subcycle", action="store_true", help="amr workload: subcycled steps (each level its own dt)")
     args = ap.parse_args()
-    if args.precision == "fast" and args.workload != "uniform":
-        ap.error("--precision fast: the fast FP64 form is built for the uniform workload only")
+    if args.precision == "fast" and args.workload not in ("uniform", "amr"):
+        ap.error("--precision fast: the fast FP64 form is built for the uniform and AMR workloads only")
     if args.steps is None:
         args.steps = {"uniform": 100, "amr": 20, "five": 10}.get(args.workload, 3)
         if args.impl == "reference":
@@ -401,21 +401,30 @@ def sub_records(args, world, rank, local):
     import numpy as np
     out = {}
     amr = {}
-    for prec in ("f64", "mixed"):
+    for prec in ("f64", "mixed", "fast"):
         ln = measure_amr(args, world, rank, local, precision=prec, steps=AMR_STEPS, warmup=3, cpu_baseline=False,
                          keep_state=True)
         amr[prec] = ln
-    a64, amx = amr["f64"], amr["mixed"]
+    a64, amx, afs = amr["f64"], amr["mixed"], amr["fast"]
     rec = {"workload": "3-D shock-bubble block AMR, base 128^3, 3 levels (eff. 512^3), 16^3 blocks, ng=5, CFL 0.4, "
                        f"regrid every 4 steps; {AMR_STEPS} timed steps after 3, each form with its own CFL dt",
            "unit": "leaf cell-updates/s"}
-    for prec in ("f64", "mixed"):
-        rec[prec] = _compact(amr[prec], ("value", "ms_per_step", "effective_cell_updates_per_s", "phase_ms_per_step",
-                                         "gpu_launches", "clocks"))
-        rec[prec]["leaves"] = amr[prec]["config"]["leaves"]
-        rec[prec]["build_s"] = amr[prec]["config"]["build_s"]
+    for prec in ("f64", "mixed", "fast"):
+        key = "fast_f64" if prec == "fast" else prec
+        rec[key] = _compact(amr[prec], ("value", "ms_per_step", "effective_cell_updates_per_s", "phase_ms_per_step",
+                                        "gpu_launches", "clocks"))
+        rec[key]["leaves"] = amr[prec]["config"]["leaves"]
+        rec[key]["build_s"] = amr[prec]["config"]["build_s"]
     rec["mixed_over_f64"] = a64["ms_per_step"] / amx["ms_per_step"]
-    (s64, u64), (smx, umx) = a64.pop("_state"), amx.pop("_state")
+    rec["fast_f64_over_f64"] = a64["ms_per_step"] / afs["ms_per_step"]
+    (s64, u64), (smx, umx), (sfs, ufs) = a64.pop("_state"), amx.pop("_state"), afs.pop("_state")
+    if s64.shape == sfs.shape and np.array_equal(s64, sfs):
+        leaves = s64[:, 4] == 1
+        ia, ib = ufs[leaves].reshape(-1, 5), u64[leaves].reshape(-1, 5)
+        num, den = np.abs(ia - ib).sum(axis=0), np.abs(ib).sum(axis=0)
+        rec["rel_l1_fast_f64_vs_f64"] = [float(x) for x in num / np.maximum(den, 1e-3 * den[0])]
+    else:
+        rec["rel_l1_fast_f64_vs_f64"] = "hierarchies differ after the regrids (a detail moved a decision)"
     if s64.shape == smx.shape and np.array_equal(s64, smx):
         leaves = s64[:, 4] == 1
         ia, ib = umx[leaves].reshape(-1, 5), u64[leaves].reshape(-1, 5)
@@ -657,7 +666,7 @@ def measure_amr(args, world, rank, local, precision=None, steps=None, warmup=Non
     precision = args.precision if precision is None else precision
     steps = args.steps if steps is None else steps
     warmup = args.warmup if warmup is None else warmup
-    prec = Precision.Mixed if precision == "mixed" else Precision.F64
+    prec = {"mixed": Precision.Mixed, "fast": Precision.F64Fast}.get(precision, Precision.F64)
     s, cfg, lo, hi, bc, init = W.shock_bubble(dim=3, base=args.amr_base, levels=3)
     t0 = time.perf_counter()
     g = GpuAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno, cfl=0.4, precision=prec, autotune=not args.no_autotune,
@@ -723,7 +732,7 @@ def measure_amr(args, world, rank, local, precision=None, steps=None, warmup=Non
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
         "steps": steps, "warmup": warmup, "ms_per_step": ms / steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == Precision.F64 else "f32-flux/f64-state",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32-flux/f64-state" if prec == Precision.Mixed else "f64",
         "data": "synthetic",
         "config": {"workload": "3-D shock-bubble block AMR: Mach-2 shock into rho=0.138 sphere r=0.15 (+-0.5% "
                                "seeded interface perturbation), base 128^3 = 8^3 blocks of 16^3, 3 levels (eff. 512^3), "
@@ -814,7 +823,7 @@ def measure_batch(args, world, rank, local, precision=None, steps=None, warmup=N
     line = {
         "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
         "steps": steps, "warmup": warmup, "ms_per_step": total_ms / steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == Precision.F64 else "f32-flux/f64-state",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32-flux/f64-state" if prec == Precision.Mixed else "f64",
         "data": "synthetic",
         "config": {"workload": "4096 independent 1-D Riemann problems, cells log-uniform [64, 2048] (sum %d), "
                                "rho,p~U[0.1,2], u~U[-1,1], t_end 0.15, outflow, per-instance CFL 0.5" % int(n.sum()),
@@ -1000,7 +1009,7 @@ def measure_batch_adjoint(args, world, rank, local, steps=None, warmup=None, dua
     line = {
         "metric": "adjoint/forward cost", "value": (r + v) / f, "unit": "ratio", "n_gpus": world,
         "steps": steps, "warmup": warmup, "ms_per_step": f + r + v, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == Precision.F64 else "f32-flux/f64-state", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32-flux/f64-state" if prec == Precision.Mixed else "f64", "data": "synthetic",
         "config": {"workload": "4096 independent 1-D Riemann problems, cells log-uniform [64, 2048] (sum %d), "
                                "rho,p~U[0.1,2], u~U[-1,1], t_end 0.15, outflow; J_i = sum E dx over [0.5, 1]; "
                                "gradient w.r.t. the six initial values" % int(n.sum()),

@@ -972,8 +972,9 @@ struct emg_amr {
                 q.pen_lane_major = p.pen_lane_major;
                 e = five_sweep_launch_amr(P, opts.mode, q, grid, stream);
             } else {
-                e = opts.precision == EMG_PRECISION_MIXED ? sweep_launch_amr_mixed(P, opts.mode, p, grid, stream)
-                                                          : sweep_launch_amr_f64(P, opts.mode, p, grid, stream);
+                e = opts.precision == EMG_PRECISION_MIXED      ? sweep_launch_amr_mixed(P, opts.mode, p, grid, stream)
+                    : opts.precision == EMG_PRECISION_F64_FAST ? sweep_launch_amr_fast(P, opts.mode, p, grid, stream)
+                                                               : sweep_launch_amr_f64(P, opts.mode, p, grid, stream);
             }
             launches++;
             if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("AMR sweep: ") + cudaGetErrorString(e));
@@ -2147,7 +2148,8 @@ struct emg_amr {
             return set_error(EMG_ERR_INVALID, "unknown flux mode");
         if (opts.mode == EMG_MODE_HYBRID && !(opts.tol > 0.0))
             return set_error(EMG_ERR_INVALID, "hybrid mode needs tol > 0");
-        if (opts.precision != EMG_PRECISION_F64 && opts.precision != EMG_PRECISION_MIXED)
+        if (opts.precision != EMG_PRECISION_F64 && opts.precision != EMG_PRECISION_MIXED &&
+            opts.precision != EMG_PRECISION_F64_FAST)
             return set_error(EMG_ERR_INVALID, "unknown precision");
         ng = (int)std::max<int64_t>(cfg.ghosts, 5);
         for (int d = 0; d < 3; d++) {

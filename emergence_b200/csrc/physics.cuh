@@ -283,7 +283,8 @@ template <typename R> __device__ __forceinline__ R weno5z_interp(R v0, R v1, R v
 // correctly rounded ones. Zero, infinite and NaN inputs give non-finite
 // results, which the admissibility tests treat as they treat infinities;
 // subnormal inputs are flushed to zero. The fast FP64 form (EMG_PRECISION_
-// F64_FAST) uses these in its sweep; the plain FP64 form never does.
+// F64_FAST) uses these in its sweep, the mixed form in its primitive recovery
+// and its limiter's conserved states; the plain FP64 form never does.
 __device__ __forceinline__ double rcp_f(double y) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(y));

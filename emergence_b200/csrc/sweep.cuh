@@ -192,6 +192,10 @@ struct Sweep {
     static constexpr int STRW = SM::STRW;
     static constexpr bool MIXED = RingTypes<RF>::MIXED;
     static constexpr bool FAST = RingTypes<RF>::FAST;
+    // the fast forms' FP64 maps (one reciprocal of ρ for the primitive
+    // recovery, division-free conserved states): the fast FP64 form and the
+    // mixed form, whose error is set by its FP32 interpolation
+    static constexpr bool FMAPS = FAST || MIXED;
     static constexpr bool MID = SM::MID;
     static constexpr int AHEAD = MODE == MODE_HYBRID ? 7 : 5;  // rows loaded beyond the round's midpoints
 
@@ -594,7 +598,7 @@ struct Sweep {
         const bool lim_on = p.positivity && lam > 0.0;  // C/scheme.rs:278
         const double inv = 1.0 / dx;
         const bool ideal_gas = ed.b == 0.0 && ed.q == 0.0 && ed.p_inf == 0.0 && ed.gamma > 1.0 && ed.gamma < 100.0;
-        const double igm1 = FAST ? 1.0 / (ed.gamma - 1.0) : 0.0;  // fast form: 1/(γ − 1)
+        const double igm1 = FMAPS ? 1.0 / (ed.gamma - 1.0) : 0.0;  // fast maps: 1/(γ − 1)
         __syncthreads();  // lane table
         const int Lmax = BATCH ? s_maxlen : Ls;
         const int nrounds = (Lmax + 5 + RM - 1) / RM;
@@ -664,14 +668,14 @@ struct Sweep {
                         double u[5], w[5];
 #pragma unroll
                         for (int k = 0; k < 5; k++) u[k] = D == 2 ? stg[(k * P + l) * RM + rr] : stg[(k * RM + rr) * P + l];
-                        if constexpr (FAST)
+                        if constexpr (FMAPS)
                             to_prim_f(ed, u, w);
                         else
                             to_prim(ed, u, w);
 #pragma unroll
                         for (int k = 0; k < 5; k++) W[at<STRW>(row, k, l)] = w[k];
                         if constexpr (MODE != MODE_WENO)
-                            W[at<STRW>(row, 5, l)] = FAST ? rho_e_f(ed, igm1, w[0], w[4]) : ed.rho_e(w[0], w[4]);
+                            W[at<STRW>(row, 5, l)] = FMAPS ? rho_e_f(ed, igm1, w[0], w[4]) : ed.rho_e(w[0], w[4]);
                         if constexpr (MODE == MODE_HYBRID) {
                             W[at<STRW>(row, 6, l)] = log(fmax(w[0], 1e-300));
                             W[at<STRW>(row, 7, l)] = log(fmax(w[4] + ed.p_inf, 1e-300));
@@ -698,7 +702,7 @@ struct Sweep {
                         double u[5], w[5];
 #pragma unroll
                         for (int k = 0; k < 5; k++) u[k] = __ldg(p.uin + k * p.ncell + g);
-                        if constexpr (FAST)
+                        if constexpr (FMAPS)
                             to_prim_f(ed, u, w);
                         else
                             to_prim(ed, u, w);
@@ -707,7 +711,7 @@ struct Sweep {
                             W[at<STRW>(row, k, l)] = w[k];
                         }
                         if constexpr (MODE != MODE_WENO)
-                            W[at<STRW>(row, 5, l)] = FAST ? rho_e_f(ed, igm1, w[0], w[4]) : ed.rho_e(w[0], w[4]);
+                            W[at<STRW>(row, 5, l)] = FMAPS ? rho_e_f(ed, igm1, w[0], w[4]) : ed.rho_e(w[0], w[4]);
                         if constexpr (MODE == MODE_HYBRID) {
                             // sensor values ln ρ, ln(p + p∞) (C/system.rs:409-413)
                             W[at<STRW>(row, 6, l)] = log(fmax(w[0], 1e-300));
@@ -820,7 +824,7 @@ struct Sweep {
                             wi[k] = W[at<STRW>(i, k, l)];
                             wj[k] = W[at<STRW>(i + 1, k, l)];
                         }
-                        if constexpr (FAST) {
+                        if constexpr (FMAPS) {
                             to_cons_f(ed, igm1, wi, ul);
                             to_cons_f(ed, igm1, wj, ur);
                         } else {

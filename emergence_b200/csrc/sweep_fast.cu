@@ -8,9 +8,29 @@
 
 namespace emg {
 
-template <int P, int D, int MODE>
+template <int P, int D, int MODE, int KIND = KIND_GRID>
 __global__ void __launch_bounds__(SWEEP_THREADS, 3) sweep_fast_kernel(const SweepParams p) {
-    Sweep<F64Fast, P, D, MODE, KIND_GRID>::run(p);
+    Sweep<F64Fast, P, D, MODE, KIND>::run(p);
+}
+
+// batched block-AMR leaves: P = 16 or 32 pencils, one block per lane set
+template <int P, int D, int MODE> static cudaError_t launch_amr(const SweepParams& p, dim3 grid, cudaStream_t s) {
+    sweep_fast_kernel<P, D, MODE, KIND_AMR><<<grid, SWEEP_THREADS, SweepSmem<F64Fast, P, MODE>::bytes(), s>>>(p);
+    return cudaGetLastError();
+}
+template <int P, int MODE> static cudaError_t launch_amr_d(const SweepParams& p, dim3 grid, cudaStream_t s) {
+    return p.d == 0 ? launch_amr<P, 0, MODE>(p, grid, s) : (p.d == 1 ? launch_amr<P, 1, MODE>(p, grid, s) : launch_amr<P, 2, MODE>(p, grid, s));
+}
+template <int MODE> static cudaError_t launch_amr_p(int P, const SweepParams& p, dim3 grid, cudaStream_t s) {
+    return P == 16 ? launch_amr_d<16, MODE>(p, grid, s) : (P == 32 ? launch_amr_d<32, MODE>(p, grid, s) : cudaErrorInvalidValue);
+}
+cudaError_t sweep_launch_amr_fast(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s) {
+    switch (mode) {
+        case MODE_WENO: return launch_amr_p<MODE_WENO>(P, p, grid, s);
+        case MODE_HYBRID: return launch_amr_p<MODE_HYBRID>(P, p, grid, s);
+        case MODE_CENTRAL: return launch_amr_p<MODE_CENTRAL>(P, p, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 template <int P, int D, int MODE> static cudaError_t launch(const SweepParams& p, dim3 grid, cudaStream_t s) {
@@ -45,6 +65,11 @@ template <int P, int MODE> static cudaError_t attr_d() {
     cudaError_t e = cudaFuncSetAttribute(sweep_fast_kernel<P, 0, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_fast_kernel<P, 1, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_fast_kernel<P, 2, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if constexpr (P >= 16) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_fast_kernel<P, 0, MODE, KIND_AMR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_fast_kernel<P, 1, MODE, KIND_AMR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(sweep_fast_kernel<P, 2, MODE, KIND_AMR>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    }
     return e;
 }
 

@@ -1,7 +1,7 @@
 // Launchers of the fused sweep kernels (instantiated in sweep_f64.cu, which is
 // compiled without FMA contraction so its f64 arithmetic rounds like the
 // reference CPU solver, in sweep_mixed.cu, FP32 flux arithmetic, and in
-// sweep_fast.cu, the fast FP64 form on uniform grids).
+// sweep_fast.cu, the fast FP64 form).
 #pragma once
 #include "sweep.cuh"
 
@@ -13,6 +13,7 @@ cudaError_t sweep_launch_fast(int P, int mode, const SweepParams& p, dim3 grid, 
 // Batched block-AMR leaves (SweepParams::amr set), P = 16 or 32.
 cudaError_t sweep_launch_amr_f64(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 cudaError_t sweep_launch_amr_mixed(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
+cudaError_t sweep_launch_amr_fast(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 // Batched independent 1-D lines (SweepParams::segs), 32 segments per CTA.
 cudaError_t sweep_launch_batch_f64(int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 cudaError_t sweep_launch_batch_mixed(int mode, const SweepParams& p, dim3 grid, cudaStream_t s);

@@ -156,6 +156,7 @@ def batch_create(n, dx, bc=(OUTFLOW, OUTFLOW), o=None):
     (dict(n=[64], dx=[0.1], bc=(CHARACTERISTIC, OUTFLOW)), "boundaries"),
     (dict(n=[64], dx=[0.1], o=opts(mode=5)), "mode"),
     (dict(n=[64], dx=[0.1], o=opts(precision=3)), "precision"),
+    (dict(n=[64], dx=[0.1], o=opts(precision=2)), "precision"),  # the fast FP64 form is not built for lines
 ])
 def test_batch1d_create_rejects_bad_arguments(args, want):
     rc = batch_create(**args)
@@ -187,7 +188,7 @@ def amr_create(cfg=None, bc=None, o=None, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 0.0)
     (dict(bc=bcs([OUTFLOW, PERIODIC] + [OUTFLOW] * 4)), "paired"),
     (dict(o=opts(mode=9)), "flux mode"),
     (dict(o=opts(mode=HYBRID, tol=-1.0)), "tol > 0"),
-    (dict(o=opts(precision=2)), "precision"),
+    (dict(o=opts(precision=3)), "precision"),
 ])
 def test_amr_create_rejects_bad_arguments(args, want):
     rc = amr_create(**args)
