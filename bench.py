@@ -467,23 +467,28 @@ def sub_records(args, world, rank, local):
     out["batch_adjoint"] = rec
     out["five"] = measure_five(args, world, rank, local)
     out["five"]["amr"] = measure_five_amr(args, world, rank, local)
+    fa = measure_five_amr(args, world, rank, local, fast=True)
+    out["five"]["amr"]["fast_f64"] = {k: fa[k] for k in ("value", "ms_per_step", "phase_ms_per_step", "clocks")}
+    out["five"]["amr"]["fast_f64"]["speedup_vs_f64"] = out["five"]["amr"]["ms_per_step"] / fa["ms_per_step"]
     return out
 
 
-def measure_five_amr(args, world, rank, local, base=8, steps=5, warmup=2):
+def measure_five_amr(args, world, rank, local, base=8, steps=5, warmup=2, fast=False):
     """The five-equation two-phase shock–bubble on the block hierarchy: the
     light-gas sphere (γ 1.67, ρ 0.138) in air hit by a Mach-2 shock, 16^3-cell
     blocks, base 8^3 blocks (128^3), 3 levels (effective 512^3), CFL 0.4 with
     the dilatation limit, regrid every 4 steps; global steps, FP64, timed with
-    CUDA events on the solver's stream (leaf cell-updates per second)."""
+    CUDA events on the solver's stream (leaf cell-updates per second); `fast`:
+    the fast FP64 form of the sweeps."""
     import torch
     from emergence_b200 import GpuAmr, workloads as W
-    from emergence_b200.physics import FluxMode
+    from emergence_b200.physics import FluxMode, Precision
     torch.cuda.set_device(local)
     dev = torch.cuda.current_device()
     s, cfg, lo, hi, bc, init = W.two_phase_amr_bubble(dim=3, base=base, levels=3)
     t0 = time.perf_counter()
-    g = GpuAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno, cfl=0.4)
+    g = GpuAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno, cfl=0.4,
+               precision=Precision.F64Fast if fast else Precision.F64)
     build_s = time.perf_counter() - t0
     for _ in range(warmup):
         g.step(g.dt_cfl())
@@ -522,7 +527,7 @@ def run_five(args, world, rank, local):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": rec["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": rec["workload"]}, "gpu_launches": rec["gpu_launches_total"],
-                "clocks": rec["clocks"], "reference_gpu": rec["reference_gpu"]}
+                "clocks": rec["clocks"], "reference_gpu": rec["reference_gpu"], "fast_f64": rec["fast_f64"]}
         print(json.dumps(line), flush=True)
 
 
@@ -561,6 +566,26 @@ def measure_five(args, world, rank, local, n=128, steps=10, warmup=3, reference=
            "unit": "cell-updates/s", "steps": steps, "warmup": warmup,
            "value": cells * steps / (ms * 1e-3), "ms_per_step": ms / steps, "gpu_launches_total": l0,
            "clocks": clk.summary()}
+    # the fast FP64 form on the same grid and steps
+    from emergence_b200.physics import Precision
+    gf = GpuFiveSolver(sys_, mesh, u, bc=bc, cfl=0.5, mode=FluxMode.Weno, precision=Precision.F64Fast)
+    for _ in range(warmup):
+        gf.step(gf.dt_cfl())
+    sf = torch.cuda.ExternalStream(gf.stream())
+    a3, b3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a3.record(sf)
+    for _ in range(steps):
+        gf.step(gf.dt_cfl())
+    b3.record(sf)
+    b3.synchronize()
+    fms = a3.elapsed_time(b3)
+    uf = gf.download()
+    gf.close()
+    ia, ib = mesh.interior(uf).reshape(-1, 7), mesh.interior(ours).reshape(-1, 7)
+    num, den = np.abs(ia - ib).sum(axis=0), np.abs(ib).sum(axis=0)
+    rec["fast_f64"] = {"value": cells * steps / (fms * 1e-3), "ms_per_step": fms / steps, "speedup_vs_f64": ms / fms,
+                       "rel_l1_vs_f64_form": [float(x) for x in num / np.maximum(den, 1e-3 * (den[0] + den[1]))]}
     from oracle import pyrefgpu
     if not reference:
         rec["reference_gpu"] = None

@@ -11,6 +11,7 @@ Translation units and their FMA policy:
   sweep_f64.cu    plain FP64 fused sweep                          -fmad=false
   sweep_mixed.cu  FP32-flux fused sweep                           -fmad=true
   sweep_fast.cu   fast FP64 fused sweep (within 1e-12)            -fmad=true
+  five_fast.cu    fast FP64 five-equation sweep                   -fmad=true
 The plain FP64 units keep every multiply and add separately rounded so that
 their results round exactly as the reference CPU solver's.
 """
@@ -36,6 +37,7 @@ UNITS = [
     ("sweep_f64.cu", ["-fmad=false"]),
     ("sweep_mixed.cu", ["-fmad=true", "-use_fast_math"]),
     ("sweep_fast.cu", ["-fmad=true"]),
+    ("five_fast.cu", ["-fmad=true"]),
 ]
 
 

@@ -970,7 +970,8 @@ struct emg_amr {
                 q.nface = p.nface;
                 q.npen = npen;
                 q.pen_lane_major = p.pen_lane_major;
-                e = five_sweep_launch_amr(P, opts.mode, q, grid, stream);
+                e = opts.precision == EMG_PRECISION_F64_FAST ? five_sweep_launch_amr_fast(P, opts.mode, q, grid, stream)
+                                                             : five_sweep_launch_amr(P, opts.mode, q, grid, stream);
             } else {
                 e = opts.precision == EMG_PRECISION_MIXED      ? sweep_launch_amr_mixed(P, opts.mode, p, grid, stream)
                     : opts.precision == EMG_PRECISION_F64_FAST ? sweep_launch_amr_fast(P, opts.mode, p, grid, stream)
@@ -2135,8 +2136,8 @@ struct emg_amr {
             hi[d] = hi_[d];
         }
         for (int i = 0; i < 6; i++) bc[i] = b[i];
-        if (nv == 7 && opts.precision != EMG_PRECISION_F64)
-            return set_error(EMG_ERR_INVALID, "the five-equation system runs in the plain FP64 form only");
+        if (nv == 7 && opts.precision != EMG_PRECISION_F64 && opts.precision != EMG_PRECISION_F64_FAST)
+            return set_error(EMG_ERR_INVALID, "the five-equation system runs in the plain or fast FP64 form only");
         if (cfg.b < 6 || cfg.levels < 1 || cfg.levels > AMR_MAX_LEVELS || cfg.regrid_every < 1)
             return set_error(EMG_ERR_INVALID, "invalid AMR configuration (b >= 6, 1 <= levels <= 12, regrid_every >= 1)");
         for (int i = 0; i < 6; i++) {

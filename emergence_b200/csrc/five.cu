@@ -341,6 +341,7 @@ cudaError_t five_prepare_device() {
     e = five_attr_p<MODE_WENO>();
     if (e == cudaSuccess) e = five_attr_p<MODE_HYBRID>();
     if (e == cudaSuccess) e = five_attr_p<MODE_CENTRAL>();
+    if (e == cudaSuccess) e = five_sweep_prepare_fast();
     if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
     return e;
 }
@@ -506,7 +507,9 @@ struct emg_five {
                     p.dest = u;
                 }
             }
-            cudaError_t e = five_launch(sweepP[d], opts.mode, p, sweepGrid[d], stream);
+            cudaError_t e = opts.precision == EMG_PRECISION_F64_FAST
+                                ? five_sweep_launch_fast(sweepP[d], opts.mode, p, sweepGrid[d], stream)
+                                : five_launch(sweepP[d], opts.mode, p, sweepGrid[d], stream);
             launches++;
             if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("five-equation sweep: ") + cudaGetErrorString(e));
         }
@@ -609,8 +612,8 @@ int emg_five_create(const emg_mesh* mesh, const emg_five_system* sys, const emg_
     if (opts->mode != EMG_MODE_WENO && opts->mode != EMG_MODE_HYBRID && opts->mode != EMG_MODE_CENTRAL)
         return set_error(EMG_ERR_INVALID, "unknown flux mode");
     if (opts->mode == EMG_MODE_HYBRID && !(opts->tol > 0.0)) return set_error(EMG_ERR_INVALID, "hybrid mode needs tol > 0");
-    if (opts->precision != EMG_PRECISION_F64)
-        return set_error(EMG_ERR_INVALID, "the five-equation system runs in the plain FP64 form");
+    if (opts->precision != EMG_PRECISION_F64 && opts->precision != EMG_PRECISION_F64_FAST)
+        return set_error(EMG_ERR_INVALID, "the five-equation system runs in the plain or fast FP64 form");
     for (int k = 0; k < 2; k++)
         if (!(sys->eos[k].gamma > 1.0)) return set_error(EMG_ERR_INVALID, "each phase needs gamma > 1");
     for (int d = 0; d < 3; d++) {

@@ -74,7 +74,9 @@ template <int P, int MODE> struct FiveSmem {
     }
 };
 
-template <int P, int D, int MODE, bool AMR = false> struct FiveSweep {
+// FAST: the fast FP64 form (built with FMA contraction, WENO5-Z weights from
+// the one-ulp reciprocals of physics.cuh's fast section)
+template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct FiveSweep {
     using SM = FiveSmem<P, MODE>;
     static constexpr int T = SWEEP_THREADS;
     static constexpr int RM = SM::RM;
@@ -105,13 +107,36 @@ template <int P, int D, int MODE, bool AMR = false> struct FiveSweep {
             c = Five::sound_speed_rc2(avg, s.rho_c2_db(avg, d, b, kk));
         }
         const double c2 = c * c;
-        const double l0p = -avg[0] / rh / c2;
-        const double l1p = -avg[1] / rh / c2;
-        const double l2u = -rh / (2.0 * c);
-        const double l2p = 1.0 / (2.0 * c2);
-        const double l5u = rh / (2.0 * c);
-        const double l5p = 1.0 / (2.0 * c2);
-        const double l6p = kk / rh / c2;
+        double l0p, l1p, l2u, l2p, l5u, l5p, l6p;  // rows of L (multiphase.rs:202-220)
+        double r0, r1, ru2, ru5, r6;               // columns of R (multiphase.rs:222-236)
+        if constexpr (FAST) {
+            const double irh = rcp_f(rh), ic = rcp_f(c), ic2 = ic * ic;
+            l0p = -avg[0] * irh * ic2;
+            l1p = -avg[1] * irh * ic2;
+            l2u = -0.5 * rh * ic;
+            l2p = 0.5 * ic2;
+            l5u = 0.5 * rh * ic;
+            l5p = 0.5 * ic2;
+            l6p = kk * irh * ic2;
+            r0 = avg[0] * irh;
+            r1 = avg[1] * irh;
+            ru2 = -c * irh;
+            ru5 = c * irh;
+            r6 = -kk * irh;
+        } else {
+            l0p = -avg[0] / rh / c2;
+            l1p = -avg[1] / rh / c2;
+            l2u = -rh / (2.0 * c);
+            l2p = 1.0 / (2.0 * c2);
+            l5u = rh / (2.0 * c);
+            l5p = 1.0 / (2.0 * c2);
+            l6p = kk / rh / c2;
+            r0 = avg[0] / rh;
+            r1 = avg[1] / rh;
+            ru2 = -1.0 * c / rh;
+            ru5 = 1.0 * c / rh;
+            r6 = -kk / rh;
+        }
         double cl[NF], cr[NF];
 #pragma unroll
         for (int a = 0; a < NF; a++) {
@@ -129,13 +154,15 @@ template <int P, int D, int MODE, bool AMR = false> struct FiveSweep {
                     default: ch[s6] = l6p * W[at<STRW>(row, F_IP, l)] + W[at<STRW>(row, F_IA, l)];
                 }
             }
-            cl[a] = weno5z_interp(ch[0], ch[1], ch[2], ch[3], ch[4]);
-            cr[a] = weno5z_interp(ch[5], ch[4], ch[3], ch[2], ch[1]);
+            if constexpr (FAST) {
+                cl[a] = weno5z_interp_f(ch[0], ch[1], ch[2], ch[3], ch[4]);
+                cr[a] = weno5z_interp_f(ch[5], ch[4], ch[3], ch[2], ch[1]);
+            } else {
+                cl[a] = weno5z_interp(ch[0], ch[1], ch[2], ch[3], ch[4]);
+                cr[a] = weno5z_interp(ch[5], ch[4], ch[3], ch[2], ch[1]);
+            }
         }
         // back-projection (columns of R in the reference's order)
-        const double r0 = avg[0] / rh, r1 = avg[1] / rh;
-        const double ru2 = -1.0 * c / rh, ru5 = 1.0 * c / rh;
-        const double r6 = -kk / rh;
         double wl[NF], wr[NF];
         wl[0] = (cl[0] + r0 * cl[2]) + r0 * cl[5];
         wr[0] = (cr[0] + r0 * cr[2]) + r0 * cr[5];

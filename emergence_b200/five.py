@@ -102,14 +102,16 @@ def _dptr(a):
 
 
 class GpuFiveSolver:
-    """Device solver of a ghost-padded five-equation state (plain FP64 form).
+    """Device solver of a ghost-padded five-equation state (plain FP64 form,
+    or the fast FP64 form with ``precision=Precision.F64Fast``).
 
     ``GpuFiveSolver(sys, mesh, u, bc=..., cfl=0.5, mode=FluxMode.Weno,
     tol=1e-3, positivity=True)``; ``bc[d][s]`` are ``Bc`` values whose
     Dirichlet / far-field states hold 7 conserved values.
     """
 
-    def __init__(self, sys, mesh, u, bc=None, cfl=0.5, mode=FluxMode.Weno, tol=1e-3, positivity=True):
+    def __init__(self, sys, mesh, u, bc=None, cfl=0.5, mode=FluxMode.Weno, tol=1e-3, positivity=True,
+                 precision=Precision.F64):
         self.sys, self.mesh = sys, mesh
         self.bc = bc if bc is not None else [[Bc.Periodic, Bc.Periodic] for _ in range(3)]
         u = np.ascontiguousarray(u, dtype=np.float64)
@@ -119,7 +121,7 @@ class GpuFiveSolver:
         self._m = _c_mesh(mesh)
         self._s = _c_system(sys)
         self._b = _c_bcs7(self.bc)
-        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, Precision.F64, 0)
+        self._o = EmgOpts(cfl, tol, mode, 1 if positivity else 0, precision, 0)
         h = C.c_void_p()
         check(lib().emg_five_create(C.byref(self._m), C.byref(self._s), self._b, C.byref(self._o), _dptr(u),
                                     mesh.len(), C.byref(h)))

@@ -184,3 +184,76 @@ def test_fast_form_on_block_amr():
     err = np.abs(ug - uo).reshape(-1, 5).sum(axis=0) / np.maximum(den, 1e-3 * den[0])  # ρw ≡ 0 in 2-D
     print("AMR fast rel L1", err)
     assert np.all(err <= TOL), err
+
+
+# ------------------------------------------------------------------ five-equation system
+def _five_fast(*a, **k):
+    from emergence_b200 import GpuFiveSolver
+    return GpuFiveSolver(*a, precision=Precision.F64Fast, **k)
+
+
+def _five_rel_l1(a, b, mesh):
+    ai, bi = mesh.interior(a).reshape(-1, 7), mesh.interior(b).reshape(-1, 7)
+    num, den = np.abs(ai - bi).sum(axis=0), np.abs(bi).sum(axis=0)
+    return num / np.maximum(den, 1e-3 * den[0])
+
+
+@pytest.mark.parametrize("mode", [FluxMode.Weno, FluxMode.Hybrid])
+@pytest.mark.parametrize("shape", [(40, 1, 1), (24, 20, 1), (12, 10, 14)])
+def test_fast_five_equation_form_is_within_tolerance(shape, mode):
+    from test_gpu_five import BC_SETS as BC7, GAS2, two_gas_state
+    mesh, u = two_gas_state(shape, seed=5 + sum(shape), jump=True)
+    bc = BC7["outflow"]
+    o = O.FiveOracleSolver(GAS2, mesh, u, bc=bc, mode=mode)
+    g = _five_fast(GAS2, mesh, u, bc=bc, mode=mode)
+    for _ in range(3):
+        dt = o.dt_cfl()
+        assert abs(g.dt_cfl() / dt - 1.0) < 1e-13
+        o.step(dt)
+        g.step(dt)
+    err = _five_rel_l1(g.download(), o.download(), mesh)
+    print("five fast", shape, mode, err)
+    assert np.all(err <= TOL), err
+    g.close()
+
+
+def test_fast_five_equation_water_air_shock_tube():
+    """1 GPa water | 1 bar air to t = 2.4e-4 on 400 cells (the reference's
+    tube case, stiffened gas with p∞ = 6e8) with the solver's own steps."""
+    from emergence_b200.five import FiveEq, five_initial_state
+    from test_gpu_five import AIR, WATER_SG
+    sys5 = FiveEq((WATER_SG, AIR), kapila=True)
+    n, eps = 400, 1e-8
+    mesh = Mesh.new((n, 1, 1), (0, 0, 0), (1, 1, 1), ng=6)
+    x = mesh.centres()[0][:, 0, 0]
+    w = np.zeros((n, 1, 1, 7))
+    for i in range(n):
+        a, p = (1.0 - eps, 1e9) if x[i] < 0.7 else (eps, 1e5)
+        w[i, 0, 0] = [a * 1000.0, (1 - a) * 50.0, 0, 0, 0, p, a]
+    u = five_initial_state(sys5, mesh, w)
+    bc = [[Bc.Outflow, Bc.Outflow], [Bc.Periodic] * 2, [Bc.Periodic] * 2]
+    o = O.FiveOracleSolver(sys5, mesh, u, bc=bc, cfl=0.4, mode=FluxMode.Weno)
+    g = _five_fast(sys5, mesh, u, bc=bc, cfl=0.4, mode=FluxMode.Weno)
+    assert g.run_to(2.4e-4) == o.run_to(2.4e-4)
+    err = _five_rel_l1(g.download(), o.download(), mesh)
+    print("five fast tube", err)
+    assert np.all(err <= LONG_TOL), err
+    g.close()
+
+
+def test_fast_five_equation_form_on_block_amr():
+    from emergence_b200 import GpuAmr
+    s, cfg, lo, hi, bc, init = W.two_phase_amr_bubble(dim=2, base=4, levels=3)
+    o = O.OracleAmr(s, cfg, lo, hi, bc, init, mode=FluxMode.Weno)
+    g = GpuAmr(s, cfg, lo, hi, bc, mode=FluxMode.Weno, precision=Precision.F64Fast,
+               blocks=(o.structure(), o.download()))
+    for _ in range(3):
+        dt = o.dt_cfl()
+        o.step(dt)
+        g.step(dt)
+    assert np.array_equal(g.structure(), o.structure())
+    ug, uo = g.download(), o.download()
+    den = np.abs(uo).reshape(-1, 7).sum(axis=0)
+    err = np.abs(ug - uo).reshape(-1, 7).sum(axis=0) / np.maximum(den, 1e-3 * den[0])
+    print("five AMR fast rel L1", err)
+    assert np.all(err <= TOL), err

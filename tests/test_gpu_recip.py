@@ -6,7 +6,8 @@ The mixed form computes the HLLC star states, the characteristic eigenvector
 coefficients and the sound speed of each midpoint with these in place of
 IEEE division and square root; its error budget against the FP64 oracle is
 1e-6 relative L1, so a relative error of about 1e-12 in each reciprocal is
-far inside it. The plain FP64 form does not use them.
+far inside it. The plain FP64 form does not use them. The fast FP64 form's
+one-ulp versions (rcp_f, rsqrt_f, sqrt_f) are checked here as well.
 """
 import ctypes as C
 import os
@@ -37,14 +38,14 @@ def _lib():
                         "-Xcompiler", "-fPIC", "-fmad=true", "-use_fast_math", SRC, "-o", OUT], check=True)
     lib = C.CDLL(OUT)
     lib.recip_check.restype = C.c_int
-    lib.recip_check.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+    lib.recip_check.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
     return lib
 
 
-def _run(y):
+def _run(y, fast=False):
     y = np.ascontiguousarray(y, dtype=np.float64)
     out = np.empty(6 * y.size)
-    assert _lib().recip_check(y.ctypes.data, out.ctypes.data, y.size) == 0
+    assert _lib().recip_check(y.ctypes.data, out.ctypes.data, y.size, 1 if fast else 0) == 0
     return out.reshape(6, y.size)
 
 
@@ -69,3 +70,29 @@ def test_refined_reciprocals_of_zero_infinity_and_nan_are_not_finite():
     o = _run(np.array([0.0, -0.0, np.inf, -np.inf, np.nan]))
     assert not np.any(np.isfinite(o[0]))  # rcp_nr
     assert not np.any(np.isfinite(o[4]))  # x·rsqrt_nr(x), the mixed form's sound speed from c²
+
+
+# The fast FP64 form's versions cube the estimate's error (2^-60) before the
+# final rounding: within a few ulps of the correctly rounded results.
+FAST_REL_TOL = 1e-15  # about 4.5 ulp
+
+
+def test_fast_form_reciprocals_are_within_a_few_ulps():
+    rng = np.random.default_rng(20261204)
+    n = 1 << 20
+    y = np.exp(rng.uniform(np.log(1e-200), np.log(1e200), n)) * rng.choice([-1.0, 1.0], n)
+    y[:8] = [1.0, 2.0, 0.4, 1.4, 0.125, 3.0, 7.0, 0.1]
+    o = _run(y, fast=True)
+
+    def rel(a, b):
+        return float(np.max(np.abs(a - b) / np.abs(b)))
+
+    e = rel(o[0], o[1]), rel(o[2], o[3]), rel(o[4], o[5])
+    print("max relative error: rcp_f %.3e, rsqrt_f %.3e, sqrt_f %.3e" % e)
+    assert max(e) <= FAST_REL_TOL, e
+
+
+def test_fast_form_square_root_of_zero_and_infinity():
+    o = _run(np.array([0.0, np.inf, 4.0]), fast=True)
+    assert o[4][0] == 0.0 and o[4][1] == np.inf and o[4][2] == 2.0
+    assert not np.isfinite(o[0][0])  # rcp_f(0)
