@@ -152,6 +152,9 @@ struct emg_amr {
     unsigned long long* det = nullptr;
     int64_t det_cap = 0;
     DevVec<int> dmap, dleaves, dlevel, dbcleaves;
+    // chains of same-level leaves along each axis for the global sweeps
+    DevVec<int> dchain_off[3], dchain_slot[3];
+    int nchain[3] = {0, 0, 0};
     DevVec<int64_t> didx;
     DevVec<double> ddxl;
     DevVec<CopyTask> dcopy;
@@ -431,6 +434,8 @@ struct emg_amr {
             (rc = dreflux.grow(2 * dreflux.n)) || (rc = dtmp_pbox.grow(8 * nb)) || (rc = dtmp_rbox.grow(4 * nb)) ||
             (rc = dmap_edits.grow(2 * map_size())) || (rc = rg_grow()))
             return rc;
+        for (int d = 0; d < 3; d++)
+            if ((rc = dchain_off[d].grow(2 * nb + 1)) || (rc = dchain_slot[d].grow(2 * nb))) return rc;
         for (auto& r : drbox)
             if ((rc = r.grow(2 * r.n))) return rc;
         for (auto& a : drbsel)
@@ -736,6 +741,47 @@ struct emg_amr {
         }
     }
 
+    // Chains of same-level leaves along d for the global sweeps: runs of +d
+    // neighbours (periodic sides included), at most AMR_CHAIN_MAX blocks each,
+    // every leaf in exactly one chain. `off` gets one start per chain plus the
+    // end, `slot` the blocks in order.
+    void build_chains(int d, const std::vector<int>& leaves, std::vector<int>& off, std::vector<int>& slot) const {
+        off.clear();
+        slot.clear();
+        std::vector<char> seen(blocks.size(), 0);
+        auto nbr = [&](int id, int dir) -> int {  // the same-level leaf beside id along d, or −1
+            const HBlock& b = blocks[id];
+            Key nk = b.idx;
+            nk[d] += dir;
+            const int64_t n = nbl(b.level, d);
+            if (nk[d] < 0 || nk[d] >= n) {
+                if (bckind(d, nk[d] >= n ? 1 : 0) != EMG_BC_PERIODIC) return -1;
+                nk[d] = erem(nk[d], n);
+            }
+            const int j = get(b.level, nk);
+            return (j >= 0 && j != id && blocks[j].leaf) ? j : -1;
+        };
+        for (int id : leaves) {
+            if (seen[id]) continue;
+            int h = id;  // the first unvisited block of the run (a periodic ring stops where it began)
+            for (;;) {
+                const int q = nbr(h, -1);
+                if (q < 0 || seen[q] || q == id) break;
+                h = q;
+            }
+            int cur = h;
+            while (cur >= 0 && !seen[cur]) {
+                off.push_back((int)slot.size());
+                for (int k = 0; k < AMR_CHAIN_MAX && cur >= 0 && !seen[cur]; k++) {
+                    seen[cur] = 1;
+                    slot.push_back(cur);
+                    cur = nbr(cur, +1);
+                }
+            }
+        }
+        off.push_back((int)slot.size());
+    }
+
     // ---------------------------------------------------------------- layout
     int ensure_layout() {
         if (layout_valid) return upload_map();
@@ -830,6 +876,14 @@ struct emg_amr {
             }
         }
         rface_start[6] = (int)rfaces.size();
+        for (int d = 0; d < 3; d++) {
+            nchain[d] = 0;
+            if (!act[d] || nv != 5) continue;  // the five-equation sweep runs block by block
+            std::vector<int> coff, cslot;
+            build_chains(d, leaves, coff, cslot);
+            if ((rc = dchain_off[d].put(coff, stream)) || (rc = dchain_slot[d].put(cslot, stream))) return rc;
+            nchain[d] = (int)coff.size() - 1;
+        }
         if ((rc = dleaves.put(leaves, stream)) || (rc = dlevel.put(lvl, stream)) || (rc = didx.put(idx, stream)) ||
             (rc = dbcleaves.put(bcl, stream)) || (rc = dcopy.put(copies, stream)) || (rc = dpbox.put(pboxes, stream)) ||
             (rc = dreflux.put(rfaces, stream)))
@@ -931,7 +985,13 @@ struct emg_amr {
             p.nface = cap * 3 * 2 * nv * (int64_t)npen;
             p.npen = npen;
             p.pen_lane_major = lane < other ? 1 : 0;
-            const dim3 grid((unsigned)(nblk * p.ngroups), 1, 1);
+            int nz = nblk;
+            if (!list && nchain[d] > 0) {  // global sweeps: chains of same-level leaves
+                p.chain_off = dchain_off[d].p;
+                p.chain_slot = dchain_slot[d].p;
+                nz = nchain[d];
+            }
+            const dim3 grid((unsigned)(nz * p.ngroups), 1, 1);
             cudaError_t e;
             if (nv == 7) {
                 // the five-equation sweep with the same geometry (FP64 only)
@@ -2273,6 +2333,10 @@ struct emg_amr {
         dmap.release();
         dmap_edits.release();
         dleaves.release();
+        for (int d = 0; d < 3; d++) {
+            dchain_off[d].release();
+            dchain_slot[d].release();
+        }
         dlevel.release();
         dbcleaves.release();
 

@@ -35,6 +35,7 @@
 namespace emg {
 
 constexpr int SWEEP_THREADS = 256;
+constexpr int AMR_CHAIN_MAX = 8;  // blocks per chain of an AMR sweep
 
 
 // Device control block of one solver: the time step of the stage kernels is
@@ -88,6 +89,13 @@ struct SweepParams {
     double* face;           // boundary face fluxes [slot][d][side][q][pencil]
     int npen;               // pencils per block face (padded)
     int pen_lane_major;     // pencil index = lane*no + other (lane axis is the lower of the two others)
+    // optional chains of same-level leaves along d (launch chain z / ngroups is
+    // blocks chain_slot[chain_off[z] .. chain_off[z+1]), each the +d neighbour
+    // of the one before, at most AMR_CHAIN_MAX): the CTA streams the chain's
+    // rows as one pencil, reading the neighbours' interiors at the joints (the
+    // values their ghost copies hold); null: one leaf per launch chain
+    const int* chain_off;
+    const int* chain_slot;
     // ---- batched independent 1-D lines (batch != 0): every lane is one
     // segment of one instance with its own length, dx and dt
     const struct BatchSeg* segs;
@@ -542,17 +550,38 @@ struct Sweep {
         // AMR batches: x = (leaf, group of other-axis rows), lanes cover the block
         const int lane0 = AMR ? 0 : blockIdx.x * P;
         const int s0 = blockIdx.y * p.seg;
-        const int Ls = min(p.seg, p.nd - s0);
+        int Ls = min(p.seg, p.nd - s0);
         int64_t blk = 0;   // pool offset of the block (AMR) or 0
         int ob0 = blockIdx.z;
         int slot_id = 0;
         double dx = p.dx;
+        // AMR: the blocks of this CTA's chain (pool slots and offsets)
+        constexpr int CHN = AMR ? AMR_CHAIN_MAX : 1;
+        __shared__ int64_t s_cblk[CHN];
+        __shared__ int s_cslot[CHN];
+        int nch = 1;
         if constexpr (AMR) {
             const int z = blockIdx.x / p.ngroups;
             ob0 = (blockIdx.x % p.ngroups) * (P / p.lw);
-            slot_id = p.leaf_slot[z];
+            int c0 = z;
+            const int* slots = p.leaf_slot;
+            if (p.chain_off) {
+                c0 = p.chain_off[z];
+                nch = p.chain_off[z + 1] - c0;
+                slots = p.chain_slot;
+                if (nch > CHN || nch < 1) {
+                    if (BOUNDS_CHECK && tid == 0) atomicCAS(&p.ctl->status, 0, STATUS_BOUNDS);
+                    nch = max(1, min(nch, CHN));
+                }
+            }
+            slot_id = slots[c0];
+            if (tid < nch) {
+                s_cslot[tid] = slots[c0 + tid];
+                s_cblk[tid] = (int64_t)slots[c0 + tid] * p.bcell;
+            }
             blk = (int64_t)slot_id * p.bcell;
             dx = p.dx_level[p.leaf_level[slot_id]];
+            Ls = nch * p.nd;
         }
         __shared__ int64_t s_loff[P];
         __shared__ int s_lok[P];
@@ -588,9 +617,31 @@ struct Sweep {
         }
         // padded offset of row 0 (lane offsets are added per lane)
         const int64_t base0 = BATCH ? 0 : blk + (int64_t)(p.gd + s0 - 5) * p.sd;
-        // neighbouring segments recompute the 5 midpoints and 1 face they
-        // share; only the owner counts them in the statistics
-        const bool tail = s0 + Ls == p.nd;
+        // padded offset of row r without the lane offset; in an AMR chain row r
+        // lies in block min((r − 5)/nd, nch − 1) (the first block's rows start
+        // with its 5 low ghost rows, the last block's end with its 5 high ones)
+        auto rowg = [&](int r) -> int64_t {
+            if constexpr (AMR) {
+                const int j = r < 5 ? 0 : min((r - 5) / p.nd, nch - 1);
+                return s_cblk[j] + (int64_t)(p.gd - 5 + r - p.nd * j) * p.sd;
+            } else {
+                return base0 + (int64_t)r * p.sd;
+            }
+        };
+        // statistics: neighbouring segments recompute the 5 midpoints and 1
+        // face they share and only the owner counts them; an AMR chain counts
+        // each midpoint (ext 5) or face (ext 1) once per block of the chain
+        // whose own sweep computes it, as the block-by-block reference does
+        auto chain_mult = [&](int x, int ext) -> unsigned {
+            if constexpr (!AMR) {
+                return 1u;
+            } else {
+                const int jhi = min(x / p.nd, nch - 1);
+                const int jlo = x < p.nd + ext ? 0 : (x - p.nd - ext) / p.nd + 1;
+                return (unsigned)(jhi - jlo + 1);
+            }
+        };
+        const bool tail = AMR || s0 + Ls == p.nd;
         const Eos<double> ed = Eos<double>::from(p.eos);
         constexpr int un = 1 + D;
         const double lam = (p.ndim * dt) / dx;  // λ = ndim·dt/dx (C/solver.rs:393, C/amr.rs:1246)
@@ -695,10 +746,9 @@ struct Sweep {
                         rr = idx / P;
                         l = idx % P;
                     }
-                    if (s_lok[l] && lo + rr < lane_len(l) + 10 &&
-                        in_bounds(p.ctl, base0 + (int64_t)(lo + rr) * p.sd + s_loff[l], p.ncell)) {
+                    if (s_lok[l] && lo + rr < lane_len(l) + 10 && in_bounds(p.ctl, rowg(lo + rr) + s_loff[l], p.ncell)) {
                         const int row = lo + rr;
-                        const int64_t g = base0 + (int64_t)row * p.sd + s_loff[l];
+                        const int64_t g = rowg(row) + s_loff[l];
                         double u[5], w[5];
 #pragma unroll
                         for (int k = 0; k < 5; k++) u[k] = __ldg(p.uin + k * p.ncell + g);
@@ -766,7 +816,7 @@ struct Sweep {
                             midpoint<STRW>(ed, W, m, l, f, fb);
 #pragma unroll
                         for (int k = 0; k < 5; k++) MF[at<STR>(m, k, l)] = f[k];
-                        if (fb && (m < lane_len(l) || lane_tail(l))) atomicAdd(&s_fallback, 1u);
+                        if (fb && (m < lane_len(l) || lane_tail(l))) atomicAdd(&s_fallback, chain_mult(m, 5));
                     }
                 }
                 __syncthreads();
@@ -789,7 +839,7 @@ struct Sweep {
                     } else {
                         if constexpr (MID) {
                             if constexpr (MODE == MODE_HYBRID) {
-                                if (fidx < lane_len(l) || lane_tail(l)) atomicAdd(&s_weno, 1u);
+                                if (fidx < lane_len(l) || lane_tail(l)) atomicAdd(&s_weno, chain_mult(fidx, 1));
                             }
                             // F̃ = Σ_s S6[s] (F̂_{+s} + F̂_{−s}), order as C/scheme.rs:230-246
 #pragma unroll
@@ -855,7 +905,7 @@ struct Sweep {
                             }
 #pragma unroll
                             for (int k = 0; k < 5; k++) fh[k] = isfinite(fh[k]) ? lo * fh[k] + (1.0 - lo) * flf[k] : flf[k];
-                            if (fidx < lane_len(l) || lane_tail(l)) atomicAdd(&s_limited, 1u);
+                            if (fidx < lane_len(l) || lane_tail(l)) atomicAdd(&s_limited, chain_mult(fidx, 1));
                             th_rec = lo;
                         }
                     }
@@ -865,14 +915,20 @@ struct Sweep {
                         // recorded for the discrete adjoint, at the face's left cell
                         p.theta_rec[base0 + (int64_t)i * p.sd + s_loff[l]] = th_rec;
                     }
-                    if (AMR && (fidx == 0 || fidx == Ls) &&
-                        in_bounds(p.ctl, ((((int64_t)slot_id * 3 + D) * 2 + (fidx == 0 ? 0 : 1)) * 5 + 4) * p.npen + s_pen[l],
-                                  p.nface)) {
-                        // block boundary faces for refluxing (C/amr.rs:1291-1295)
-                        const int side = fidx == 0 ? 0 : 1;
-                        double* fo = p.face + ((((int64_t)slot_id * 3 + D) * 2 + side) * 5) * p.npen + s_pen[l];
+                    if (AMR && fidx % p.nd == 0) {
+                        // block boundary faces for refluxing (C/amr.rs:1291-1295): the low
+                        // face of block j and the high face of block j − 1 of the chain
+                        const int jb = fidx / p.nd;
 #pragma unroll
-                        for (int k = 0; k < 5; k++) fo[(int64_t)k * p.npen] = fh[k];
+                        for (int side = 0; side < 2; side++) {
+                            const int j = jb - side;
+                            if (j < 0 || j >= nch) continue;
+                            const int64_t f0 = ((((int64_t)s_cslot[j] * 3 + D) * 2 + side) * 5) * p.npen + s_pen[l];
+                            if (!in_bounds(p.ctl, f0 + 4 * (int64_t)p.npen, p.nface)) continue;
+                            double* fo = p.face + f0;
+#pragma unroll
+                            for (int k = 0; k < 5; k++) fo[(int64_t)k * p.npen] = fh[k];
+                        }
                     }
                 }
             }
@@ -887,9 +943,8 @@ struct Sweep {
                     c = RM * r - 5 + tid / P;
                     l = tid % P;
                 }
-                if (s_lok[l] && c >= 0 && c < lane_len(l) &&
-                    in_bounds(p.ctl, base0 + (int64_t)(c + 5) * p.sd + s_loff[l], p.ncell)) {
-                    const int64_t g = base0 + (int64_t)(c + 5) * p.sd + s_loff[l];
+                if (s_lok[l] && c >= 0 && c < lane_len(l) && in_bounds(p.ctl, rowg(c + 5) + s_loff[l], p.ncell)) {
+                    const int64_t g = rowg(c + 5) + s_loff[l];
                     const double inv_l = BATCH ? 1.0 / s_dx[l] : inv;
                     const double dt_l = BATCH ? s_dt[l] : dt;
                     double res[5];
