@@ -158,6 +158,7 @@ struct emg_amr {
     DevVec<int64_t> didx;
     DevVec<double> ddxl;
     DevVec<CopyTask> dcopy;
+    DevVec<CopyTask> dcopy_sweep;  // the copies the chained sweeps read (no slab between two blocks of a chain)
     DevVec<PBox> dpbox;
     std::vector<DevVec<RBox>> drbox;  // per level
     DevVec<RefluxFace> dreflux;
@@ -171,6 +172,7 @@ struct emg_amr {
     DevVec<double> dstage;     // host initial data of new blocks
     std::vector<int> rbox_count;
     int ncopy = 0, npbox = 0, nbcleaves = 0, nleaves = 0;
+    int ncopy_sweep = 0;
     bool layout_valid = false, map_dirty = true;
     uint64_t launches = 0;
     double phase_ms[5]{};
@@ -430,7 +432,7 @@ struct emg_amr {
         if ((rc = ensure_layout())) return rc;
         const size_t nb = blocks.size();
         if ((rc = dleaves.grow(2 * nb)) || (rc = dlevel.grow(2 * nb)) || (rc = didx.grow(6 * nb)) ||
-            (rc = dbcleaves.grow(2 * nb)) || (rc = dcopy.grow(2 * dcopy.n)) || (rc = dpbox.grow(2 * dpbox.n)) ||
+            (rc = dbcleaves.grow(2 * nb)) || (rc = dcopy.grow(2 * dcopy.n)) || (rc = dcopy_sweep.grow(2 * dcopy.n)) || (rc = dpbox.grow(2 * dpbox.n)) ||
             (rc = dreflux.grow(2 * dreflux.n)) || (rc = dtmp_pbox.grow(8 * nb)) || (rc = dtmp_rbox.grow(4 * nb)) ||
             (rc = dmap_edits.grow(2 * map_size())) || (rc = rg_grow()))
             return rc;
@@ -876,19 +878,41 @@ struct emg_amr {
             }
         }
         rface_start[6] = (int)rfaces.size();
+        // chains of the global sweeps; the chain's sweep reads the neighbour's
+        // interior at a joint, so the face slab between two blocks of a chain
+        // is not filled before the sweeps (the regrid's details, whose sensor
+        // stencils reach one cell into the face slabs, get the full list)
+        std::vector<int> next_in_chain(3 * blocks.size(), -1);
         for (int d = 0; d < 3; d++) {
             nchain[d] = 0;
             if (!act[d] || nv != 5) continue;  // the five-equation sweep runs block by block
             std::vector<int> coff, cslot;
             build_chains(d, leaves, coff, cslot);
+            for (size_t c = 0; c + 1 < coff.size(); c++)
+                for (int i = coff[c]; i + 1 < coff[c + 1]; i++) next_in_chain[3 * cslot[i] + d] = cslot[i + 1];
             if ((rc = dchain_off[d].put(coff, stream)) || (rc = dchain_slot[d].put(cslot, stream))) return rc;
             nchain[d] = (int)coff.size() - 1;
         }
+        std::vector<CopyTask> copies_sweep;
+        {
+            for (const CopyTask& t : copies) {
+                int d = -1, nz = 0;
+                for (int e = 0; e < 3; e++)
+                    if (t.o[e]) {
+                        d = e;
+                        nz++;
+                    }
+                const bool inner = nz == 1 && ((t.o[d] == 1 && next_in_chain[3 * t.slot + d] == t.src) ||
+                                               (t.o[d] == -1 && next_in_chain[3 * t.src + d] == t.slot));
+                if (!inner) copies_sweep.push_back(t);
+            }
+        }
         if ((rc = dleaves.put(leaves, stream)) || (rc = dlevel.put(lvl, stream)) || (rc = didx.put(idx, stream)) ||
-            (rc = dbcleaves.put(bcl, stream)) || (rc = dcopy.put(copies, stream)) || (rc = dpbox.put(pboxes, stream)) ||
+            (rc = dbcleaves.put(bcl, stream)) || (rc = dcopy.put(copies, stream)) || (rc = dcopy_sweep.put(copies_sweep, stream)) || (rc = dpbox.put(pboxes, stream)) ||
             (rc = dreflux.put(rfaces, stream)))
             return rc;
         ncopy = (int)copies.size();
+        ncopy_sweep = (int)copies_sweep.size();
         npbox = (int)pboxes.size();
         nbcleaves = (int)bcl.size();
         pbox_max = pmax;
@@ -901,10 +925,12 @@ struct emg_amr {
     bool pbox_fused_ready = false;  // dynamic shared-memory opt-in of pbox_fused (per handle and device)
 
     // ghost-extended boxes of every leaf (fill_scratch, C/amr.rs:1113-1221)
-    int fill_ghosts() {
+    // `for_sweeps`: only the slabs the (chained) global sweeps read
+    int fill_ghosts(bool for_sweeps = false) {
         AmrDev A = view();
-        if (ncopy) {
-            NVK(ghost_copy)<<<ncopy, COPY_THREADS, 0, stream>>>(A, dcopy.p);
+        const int nc = for_sweeps ? ncopy_sweep : ncopy;
+        if (nc) {
+            NVK(ghost_copy)<<<nc, COPY_THREADS, 0, stream>>>(A, for_sweeps ? dcopy_sweep.p : dcopy.p);
             launches++;
         }
         int rc = run_pboxes(dpbox.p, npbox, pbox_max);
@@ -1051,7 +1077,7 @@ struct emg_amr {
     int autotune_sweeps() {
         int rc = restrict_all();
         if (rc) return rc;
-        if ((rc = fill_ghosts())) return rc;
+        if ((rc = fill_ghosts(true))) return rc;
         cudaEvent_t a, b;
         AMR_CUDA(cudaEventCreate(&a));
         AMR_CUDA(cudaEventCreate(&b));
@@ -1101,7 +1127,7 @@ struct emg_amr {
         int rc = restrict_all();
         if (rc) return rc;
         record_ev(ev[1]);
-        if ((rc = fill_ghosts())) return rc;
+        if ((rc = fill_ghosts(true))) return rc;
         record_ev(ev[2]);
         if ((rc = sweeps(stage))) return rc;
         record_ev(ev[3]);
@@ -2344,6 +2370,7 @@ struct emg_amr {
 
         ddxl.release();
         dcopy.release();
+        dcopy_sweep.release();
         dpbox.release();
         for (auto& r : drbox) r.release();
         for (auto& a : drbsel)
