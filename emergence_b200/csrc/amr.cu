@@ -885,7 +885,7 @@ struct emg_amr {
         std::vector<int> next_in_chain(3 * blocks.size(), -1);
         for (int d = 0; d < 3; d++) {
             nchain[d] = 0;
-            if (!act[d] || nv != 5) continue;  // the five-equation sweep runs block by block
+            if (!act[d]) continue;
             std::vector<int> coff, cslot;
             build_chains(d, leaves, coff, cslot);
             for (size_t c = 0; c + 1 < coff.size(); c++)
@@ -1056,6 +1056,8 @@ struct emg_amr {
                 q.nface = p.nface;
                 q.npen = npen;
                 q.pen_lane_major = p.pen_lane_major;
+                q.chain_off = p.chain_off;
+                q.chain_slot = p.chain_slot;
                 e = opts.precision == EMG_PRECISION_F64_FAST ? five_sweep_launch_amr_fast(P, opts.mode, q, grid, stream)
                                                              : five_sweep_launch_amr(P, opts.mode, q, grid, stream);
             } else {

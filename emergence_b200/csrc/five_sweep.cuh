@@ -58,6 +58,10 @@ struct FiveSweepParams {
     int64_t nface;          // its length (doubles)
     int npen;               // pencils per block face (padded)
     int pen_lane_major;     // pencil index = lane*no + other (lane axis is the lower of the two others)
+    // optional chains of same-level leaves along d, as in SweepParams (null:
+    // one leaf per launch chain)
+    const int* chain_off;
+    const int* chain_slot;
 };
 
 template <int P, int MODE> struct FiveSmem {
@@ -264,17 +268,38 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
         // AMR batches: x = (leaf, group of other-axis rows), one segment
         const int lane0 = AMR ? 0 : blockIdx.x * P;
         const int s0 = blockIdx.y * p.seg;
-        const int Ls = min(p.seg, p.nd - s0);
+        int Ls = min(p.seg, p.nd - s0);
         int ob = blockIdx.z;
         int64_t blk = 0;
         int slot_id = 0;
         double dx = p.dx;
         __shared__ int s_pen[P];
+        // AMR: the blocks of this CTA's chain (pool slots and offsets)
+        constexpr int CHN = AMR ? AMR_CHAIN_MAX : 1;
+        __shared__ int64_t s_cblk[CHN];
+        __shared__ int s_cslot[CHN];
+        int nch = 1;
         if constexpr (AMR) {
             const int z = blockIdx.x / p.ngroups;
-            slot_id = p.leaf_slot[z];
+            int c0 = z;
+            const int* slots = p.leaf_slot;
+            if (p.chain_off) {
+                c0 = p.chain_off[z];
+                nch = p.chain_off[z + 1] - c0;
+                slots = p.chain_slot;
+                if (nch > CHN || nch < 1) {
+                    if (BOUNDS_CHECK && tid == 0) atomicCAS(&p.ctl->status, 0, STATUS_BOUNDS);
+                    nch = max(1, min(nch, CHN));
+                }
+            }
+            slot_id = slots[c0];
+            if (tid < nch) {
+                s_cslot[tid] = slots[c0 + tid];
+                s_cblk[tid] = (int64_t)slots[c0 + tid] * p.bcell;
+            }
             blk = (int64_t)slot_id * p.bcell;
             dx = p.dx_level[p.leaf_level[slot_id]];
+            Ls = nch * p.nd;
             if (tid < P) {
                 const int la = tid % p.lw, ob1 = (blockIdx.x % p.ngroups) * (P / p.lw) + tid / p.lw;
                 s_lok[tid] = la < p.nl && ob1 < p.no;
@@ -287,7 +312,28 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
             s_loff[tid] = (int64_t)(p.gl + la) * p.sl + (int64_t)(p.go + ob) * p.so;
         }
         const int64_t base0 = blk + (int64_t)(p.gd + s0 - 5) * p.sd;
-        const bool tail = s0 + Ls == p.nd;
+        // padded offset of row r without the lane offset (AMR chains: row r
+        // lies in block min((r − 5)/nd, nch − 1), as in the Euler sweep)
+        auto rowg = [&](int r) -> int64_t {
+            if constexpr (AMR) {
+                const int j = r < 5 ? 0 : min((r - 5) / p.nd, nch - 1);
+                return s_cblk[j] + (int64_t)(p.gd - 5 + r - p.nd * j) * p.sd;
+            } else {
+                return base0 + (int64_t)r * p.sd;
+            }
+        };
+        // statistics of an AMR chain: each midpoint (ext 5) or face (ext 1)
+        // once per block whose own sweep computes it
+        auto chain_mult = [&](int x, int ext) -> unsigned {
+            if constexpr (!AMR) {
+                return 1u;
+            } else {
+                const int jhi = min(x / p.nd, nch - 1);
+                const int jlo = x < p.nd + ext ? 0 : (x - p.nd - ext) / p.nd + 1;
+                return (unsigned)(jhi - jlo + 1);
+            }
+        };
+        const bool tail = AMR || s0 + Ls == p.nd;
         const Five sys = Five::from(p.sys);
         const double lam = (p.ndim * dt) / dx;  // λ = ndim·dt/dx (C/solver.rs:393, C/amr.rs:1245)
         const double lam2 = 2.0 * lam;
@@ -313,7 +359,7 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
                         l = idx % P;
                     }
                     const int row = lo + rr;
-                    const int64_t g = base0 + (int64_t)row * p.sd + s_loff[l];
+                    const int64_t g = rowg(row) + s_loff[l];
                     if (s_lok[l] && in_bounds(p.ctl, g, p.ncell)) {
                         double u[NF], w[NF], d, b;
 #pragma unroll
@@ -370,7 +416,7 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
 #pragma unroll
                         for (int k = 0; k < NF; k++) MF[at<STR>(m, k, l)] = f[k];
                         MF[at<STR>(m, NF, l)] = us;
-                        if (fb && (m < Ls || tail)) atomicAdd(&s_fallback, 1u);
+                        if (fb && (m < Ls || tail)) atomicAdd(&s_fallback, chain_mult(m, 5));
                     }
                 }
                 __syncthreads();
@@ -411,7 +457,7 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
                     } else {
                         if constexpr (MID) {
                             if constexpr (MODE == MODE_HYBRID) {
-                                if (fidx < Ls || tail) atomicAdd(&s_weno, 1u);
+                                if (fidx < Ls || tail) atomicAdd(&s_weno, chain_mult(fidx, 1));
                             }
                             // F̃ = Σ_s S6[s] (F̂_{+s} + F̂_{−s}) and the same for Ũ (scheme.rs:226-250)
 #pragma unroll
@@ -468,19 +514,26 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
                             for (int k = 0; k < NF; k++) fh[k] = isfinite(fh[k]) ? lo * fh[k] + (1.0 - lo) * flf[k] : flf[k];
                             const double um = 0.5 * (wi[UN] + wj[UN]);
                             uf = isfinite(uf) ? lo * uf + (1.0 - lo) * um : um;
-                            if (fidx < Ls || tail) atomicAdd(&s_limited, 1u);
+                            if (fidx < Ls || tail) atomicAdd(&s_limited, chain_mult(fidx, 1));
                         }
                     }
 #pragma unroll
                     for (int k = 0; k < NF; k++) F[at<STR>(fidx, k, l)] = fh[k];
                     F[at<STR>(fidx, NF, l)] = uf;
-                    if (AMR && (fidx == 0 || fidx == Ls) &&
-                        in_bounds(p.ctl, ((((int64_t)slot_id * 3 + D) * 2 + (fidx == 0 ? 0 : 1)) * NF + NF - 1) * p.npen + s_pen[l],
-                                  p.nface)) {
-                        // block boundary faces for refluxing (C/amr.rs:1291-1295)
-                        double* fo = p.face + ((((int64_t)slot_id * 3 + D) * 2 + (fidx == 0 ? 0 : 1)) * NF) * p.npen + s_pen[l];
+                    if (AMR && fidx % p.nd == 0) {
+                        // block boundary faces for refluxing (C/amr.rs:1291-1295): the low
+                        // face of block j and the high face of block j − 1 of the chain
+                        const int jb = fidx / p.nd;
 #pragma unroll
-                        for (int k = 0; k < NF; k++) fo[(int64_t)k * p.npen] = fh[k];
+                        for (int side = 0; side < 2; side++) {
+                            const int j = jb - side;
+                            if (j < 0 || j >= nch) continue;
+                            const int64_t f0 = ((((int64_t)s_cslot[j] * 3 + D) * 2 + side) * NF) * p.npen + s_pen[l];
+                            if (!in_bounds(p.ctl, f0 + (int64_t)(NF - 1) * p.npen, p.nface)) continue;
+                            double* fo = p.face + f0;
+#pragma unroll
+                            for (int k = 0; k < NF; k++) fo[(int64_t)k * p.npen] = fh[k];
+                        }
                     }
                 }
             }
@@ -495,7 +548,7 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
                     c = RM * r - 5 + tid / P;
                     l = tid % P;
                 }
-                const int64_t g = base0 + (int64_t)(c + 5) * p.sd + s_loff[l];
+                const int64_t g = rowg(c + 5) + s_loff[l];
                 if (s_lok[l] && c >= 0 && c < Ls && in_bounds(p.ctl, g, p.ncell)) {
                     double res[NF];
 #pragma unroll
