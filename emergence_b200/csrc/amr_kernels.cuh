@@ -402,7 +402,8 @@ __global__ void rbox_bc(const AmrDev A, const RBox* __restrict__ boxes, double* 
 // one restriction pass along dims[di] with the shifted stencils and the
 // child-average fallback (amr.rs:674-727)
 template <int NV>
-__global__ void rbox_pass(const AmrDev A, const RBox* __restrict__ boxes, const double* in, const unsigned char* okin,
+__global__ void __launch_bounds__(256, 4) rbox_pass(const AmrDev A, const RBox* __restrict__ boxes, const double* in,
+                                                   const unsigned char* okin,
                           double* outb, unsigned char* okout, int di, int skip_fast) {
     const RBox b = boxes[blockIdx.x];
     if (skip_fast && b.fast) return;  // first pass done by rbox_gather_pass0
@@ -412,37 +413,55 @@ __global__ void rbox_pass(const AmrDev A, const RBox* __restrict__ boxes, const 
     rbox_size(A, b, di + 1, so);
     const int shifts[5] = {0, -1, 1, -2, 2};
     const int64_t n = (int64_t)so[0] * so[1] * so[2];
+    // stride of d in the box's row-major layout, and its extent
+    const int64_t str = d == 0 ? (int64_t)si[1] * si[2] : (d == 1 ? si[2] : 1);
+    const int sid = d == 0 ? si[0] : (d == 1 ? si[1] : si[2]);
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
         int64_t c[3];
         box_coord(q, so, c);
-        auto at_src = [&](int64_t pos) {
-            int64_t s2[3] = {c[0], c[1], c[2]};
-            s2[d] = pos;
-            return b.off + box_index(s2, si);
-        };
-        const int64_t base = 2 * c[d] + 2;
+        const int cd = (int)(d == 0 ? c[0] : (d == 1 ? c[1] : c[2]));
+        int64_t c0[3] = {c[0], c[1], c[2]};
+        if (d == 0) c0[0] = 0;
+        else if (d == 1) c0[1] = 0;
+        else c0[2] = 0;
+        const int64_t row0 = b.off + box_index(c0, si);  // source index at position 0 along d
+        const int base = 2 * cd + 2;
+        // positions base − 2 .. base + 7 (every stencil the shifts reach): index
+        // and validity, position i = shift + 2 + kk of the unrolled stencils
+        int64_t at[10];
+        bool okp[10];
+#pragma unroll
+        for (int i = 0; i < 10; i++) {
+            const int x = base - 2 + i;
+            at[i] = row0 + (int64_t)x * str;
+            okp[i] = x >= 0 && x < sid && okin[at[i]];
+        }
         double acc[NV] = {};
         bool done = false;
-        for (int m = 0; m < 5 && !done; m++) {
-            const int64_t st = base + shifts[m];
-            if (st < 0 || st + 5 >= si[d]) continue;
-            bool all = true;
-            for (int kk = 0; kk < 6; kk++) all = all && okin[at_src(st + kk)];
-            if (all) {
-                for (int kk = 0; kk < 6; kk++) {
-                    const double* v = in + at_src(st + kk) * NV;
-                    for (int k = 0; k < NV; k++) acc[k] = acc[k] + A.wrs[m][kk] * v[k];
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            const int sh = shifts[m];
+            const int st = base + sh;
+            if (!done && st >= 0 && st + 5 < sid) {
+                bool all = true;
+#pragma unroll
+                for (int kk = 0; kk < 6; kk++) all = all && okp[sh + 2 + kk];
+                if (all) {
+#pragma unroll
+                    for (int kk = 0; kk < 6; kk++) {
+                        const double* v = in + at[sh + 2 + kk] * NV;
+#pragma unroll
+                        for (int k = 0; k < NV; k++) acc[k] = acc[k] + A.wrs[m][kk] * v[k];
+                    }
+                    done = true;
                 }
-                done = true;
             }
         }
         unsigned char o = done ? 1 : 0;
-        if (!done) {
-            const int64_t pa = at_src(base + 2), pb = at_src(base + 3);
-            if (okin[pa] && okin[pb]) {
-                for (int k = 0; k < NV; k++) acc[k] = 0.5 * (in[pa * NV + k] + in[pb * NV + k]);
-                o = 1;
-            }
+        if (!done && okp[4] && okp[5]) {  // positions base + 2, base + 3: the child average
+            const int64_t pa = at[4], pb = at[5];
+            for (int k = 0; k < NV; k++) acc[k] = 0.5 * (in[pa * NV + k] + in[pb * NV + k]);
+            o = 1;
         }
         double* ov = outb + (b.off + q) * NV;
         for (int k = 0; k < NV; k++) ov[k] = acc[k];
@@ -456,7 +475,8 @@ __global__ void rbox_pass(const AmrDev A, const RBox* __restrict__ boxes, const 
 // so the gathered patch never goes through global scratch. Same stencil
 // choice, validity and summation order as rbox_gather + rbox_pass.
 template <int NV>
-__global__ void rbox_gather_pass0(const AmrDev A, const RBox* __restrict__ boxes, double* outb, unsigned char* okout,
+__global__ void __launch_bounds__(256, 4) rbox_gather_pass0(const AmrDev A, const RBox* __restrict__ boxes, double* outb,
+                                                           unsigned char* okout,
                                   const int* __restrict__ rem) {
     const RBox b = boxes[blockIdx.x];
     if (!b.fast) return;
@@ -486,56 +506,83 @@ __global__ void rbox_gather_pass0(const AmrDev A, const RBox* __restrict__ boxes
     const int sid = b.sz[d];
     const int shifts[5] = {0, -1, 1, -2, 2};
     const int64_t n = (int64_t)so[0] * so[1] * so[2];
+    const int bdd = A.bd[d];
+    const int64_t sd = d == 0 ? (int64_t)A.ext[1] * A.ext[2] : (d == 1 ? A.ext[2] : 1);  // pool stride along d
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
         int64_t c[3];
         box_coord(q, so, c);
         const int base = 2 * (int)c[d] + 2;
-        // slot and local cell of the fine cell at position x along d
-        auto locate = [&](int x, int64_t* lc) -> int {
-            int j[3];
-            for (int e = 0; e < 3; e++) {
-                if (!A.act[e]) {
-                    j[e] = 0;
-                    lc[e] = 0;
-                    continue;
-                }
-                const int o = (int)(b.f0[e] - s_kmin[e] * A.bd[e] + (e == d ? x : c[e]));
-                j[e] = o / A.bd[e];
-                lc[e] = o - j[e] * A.bd[e];
-            }
-            return s_slot[(j[0] * s_nk[1] + j[1]) * s_nk[2] + j[2]];
-        };
-        // validity of positions base − 2 .. base + 7 (every stencil the shifts can reach)
-        bool okp[10];
-        for (int i = 0; i < 10; i++) {
-            const int x = base - 2 + i;
-            int64_t lc[3];
-            okp[i] = x >= 0 && x < sid && locate(x, lc) >= 0;
+        // the block and local cell along the two other axes are the same for
+        // every position of the stencil: resolve them once, then step along d
+        int jt[3] = {0, 0, 0};
+        int64_t lt[3] = {0, 0, 0};
+        for (int e = 0; e < 3; e++) {
+            if (e == d || !A.act[e]) continue;
+            const int o = (int)(b.f0[e] - s_kmin[e] * A.bd[e] + c[e]);
+            jt[e] = o / A.bd[e];
+            lt[e] = o - jt[e] * A.bd[e];
         }
+        // positions base − 2 .. base + 7 along d (every stencil the shifts can
+        // reach): block index along d and local coordinate of the first one
+        const int o0 = (int)(b.f0[d] - s_kmin[d] * bdd) + base - 2;
+        const int jd0 = o0 >= 0 ? o0 / bdd : -((-o0 + bdd - 1) / bdd);  // floor (o0 ≥ −2)
+        const int ld0 = o0 - jd0 * bdd;
+        // slot table index of block jd along d (the other two block indices fixed)
+        const int tstr = d == 0 ? s_nk[1] * s_nk[2] : (d == 1 ? s_nk[2] : 1);
+        const int nkd = d == 0 ? s_nk[0] : (d == 1 ? s_nk[1] : s_nk[2]);
+        const int tbase = (d == 0 ? 0 : jt[0] * s_nk[1] * s_nk[2]) + (d == 1 ? 0 : jt[1] * s_nk[2]) + (d == 2 ? 0 : jt[2]);
+        auto slot_at = [&](int jd) -> int { return (jd < 0 || jd >= nkd) ? -1 : s_slot[tbase + jd * tstr]; };
+        int64_t lcb[3] = {lt[0], lt[1], lt[2]};
+        lcb[d] = 0;
+        const int64_t cell0 = amr_cell(A, lcb);  // local cell at coordinate 0 along d
+        int pslot[10];
+        int64_t pcell[10];
+        bool okp[10];
+        {
+            int jd = jd0, ld = ld0, sl = slot_at(jd0);
+#pragma unroll
+            for (int i = 0; i < 10; i++) {
+                const int x = base - 2 + i;
+                pslot[i] = sl;
+                pcell[i] = cell0 + (int64_t)ld * sd;
+                okp[i] = x >= 0 && x < sid && sl >= 0;
+                if (++ld == bdd) {
+                    ld = 0;
+                    sl = slot_at(++jd);
+                }
+            }
+        }
+        // slot and local cell of the fine cell at position x along d
+        // the stencils in the order of the shifts, the first whole one used;
+        // unrolled, so that every position index is a constant and the
+        // tables stay in registers (position i = shift + 2 + kk)
         double acc[NV] = {};
         bool done = false;
-        for (int m = 0; m < 5 && !done; m++) {
-            const int st = base + shifts[m];
-            if (st < 0 || st + 5 >= sid) continue;
-            bool all = true;
-            for (int kk = 0; kk < 6; kk++) all = all && okp[st + kk - (base - 2)];
-            if (all) {
-                for (int kk = 0; kk < 6; kk++) {
-                    int64_t lc[3];
-                    const int slot = locate(st + kk, lc);
-                    double v[NV];
-                    amr_load<NV>(A, slot, amr_cell(A, lc), v);
-                    for (int k = 0; k < NV; k++) acc[k] = acc[k] + A.wrs[m][kk] * v[k];
+#pragma unroll
+        for (int m = 0; m < 5; m++) {
+            const int sh = shifts[m];
+            const int st = base + sh;
+            if (!done && st >= 0 && st + 5 < sid) {
+                bool all = true;
+#pragma unroll
+                for (int kk = 0; kk < 6; kk++) all = all && okp[sh + 2 + kk];
+                if (all) {
+                    double v[6][NV];
+#pragma unroll
+                    for (int kk = 0; kk < 6; kk++) amr_load<NV>(A, pslot[sh + 2 + kk], pcell[sh + 2 + kk], v[kk]);
+#pragma unroll
+                    for (int kk = 0; kk < 6; kk++)
+#pragma unroll
+                        for (int k = 0; k < NV; k++) acc[k] = acc[k] + A.wrs[m][kk] * v[kk][k];
+                    done = true;
                 }
-                done = true;
             }
         }
         unsigned char o = done ? 1 : 0;
         if (!done && okp[4] && okp[5]) {  // positions base + 2, base + 3: the child average
             double va[NV], vb[NV];
-            int64_t lc[3];
-            amr_load<NV>(A, locate(base + 2, lc), amr_cell(A, lc), va);
-            amr_load<NV>(A, locate(base + 3, lc), amr_cell(A, lc), vb);
+            amr_load<NV>(A, pslot[4], pcell[4], va);
+            amr_load<NV>(A, pslot[5], pcell[5], vb);
             for (int k = 0; k < NV; k++) acc[k] = 0.5 * (va[k] + vb[k]);
             o = 1;
         }
