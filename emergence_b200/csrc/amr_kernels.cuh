@@ -850,18 +850,27 @@ __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rh
                 continue;
             }
         }
-        double un[NV];
+        // every operand first (the pool, u0 and the residual may alias as far
+        // as the compiler knows, so loads would otherwise wait on stores)
+        double un[NV], uu[NV], r[NV], b0[NV];
+#pragma unroll
         for (int k = 0; k < NV; k++) {
             const int64_t o = (int64_t)k * A.ntot + cell;
-            const double uu = A.u[o], r = rhs[o];
+            uu[k] = A.u[o];
+            r[k] = rhs[o];
+            b0[k] = stage == 1 ? 0.0 : u0[o];
+        }
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            const int64_t o = (int64_t)k * A.ntot + cell;
             double v;
             if (stage == 1) {
-                u0[o] = uu;
-                v = sc ? 0.0 * uu + 1.0 * (uu + dt * r) : uu + dt * r;
+                u0[o] = uu[k];
+                v = sc ? 0.0 * uu[k] + 1.0 * (uu[k] + dt * r[k]) : uu[k] + dt * r[k];
             } else if (stage == 2) {
-                v = 0.75 * u0[o] + 0.25 * (uu + dt * r);
+                v = 0.75 * b0[k] + 0.25 * (uu[k] + dt * r[k]);
             } else {
-                v = sc ? (1.0 / 3.0) * u0[o] + 2.0 / 3.0 * (uu + dt * r) : u0[o] / 3.0 + 2.0 / 3.0 * (uu + dt * r);
+                v = sc ? (1.0 / 3.0) * b0[k] + 2.0 / 3.0 * (uu[k] + dt * r[k]) : b0[k] / 3.0 + 2.0 / 3.0 * (uu[k] + dt * r[k]);
             }
             A.u[o] = v;
             un[k] = v;
