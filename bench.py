@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed", "fast"],
-                    help="fast: the fast FP64 form (uniform and AMR workloads)")
+                    help="fast: the fast FP64 form (uniform, AMR and batch workloads)")
     ap.add_argument("--n", "--grid", dest="n", type=int, default=N_CELLS, help="cells per side (default 256)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -74,8 +74,8 @@ def parse():
     ap.add_argument("--amr-base", type=int, default=8, help="AMR base blocks per side (16^3 cells each)")
     ap.add_argument("--subcycle", action="store_true", help="amr workload: subcycled steps (each level its own dt)")
     args = ap.parse_args()
-    if args.precision == "fast" and args.workload not in ("uniform", "amr"):
-        ap.error("--precision fast: the fast FP64 form is built for the uniform and AMR workloads only")
+    if args.precision == "fast" and args.workload not in ("uniform", "amr", "batch"):
+        ap.error("--precision fast: the fast FP64 form is built for the uniform, AMR and batch workloads only")
     if args.steps is None:
         args.steps = {"uniform": 100, "amr": 20, "five": 10}.get(args.workload, 3)
         if args.impl == "reference":
@@ -450,12 +450,14 @@ def sub_records(args, world, rank, local):
     out["amr"] = rec
 
     bat = {}
-    for prec in ("f64", "mixed"):
+    for prec in ("f64", "mixed", "fast"):
         bat[prec] = measure_batch(args, world, rank, local, precision=prec, steps=1, warmup=1, cpu_baseline=False)
     out["batch"] = {"workload": bat["f64"]["config"]["workload"], "unit": "cell-updates/s",
                     "f64": _compact(bat["f64"], ("value", "ms_per_step", "clocks")),
                     "mixed": _compact(bat["mixed"], ("value", "ms_per_step", "clocks")),
-                    "mixed_over_f64": bat["f64"]["ms_per_step"] / bat["mixed"]["ms_per_step"]}
+                    "fast_f64": _compact(bat["fast"], ("value", "ms_per_step", "clocks")),
+                    "mixed_over_f64": bat["f64"]["ms_per_step"] / bat["mixed"]["ms_per_step"],
+                    "fast_f64_over_f64": bat["f64"]["ms_per_step"] / bat["fast"]["ms_per_step"]}
 
     adj = measure_adjoint(args, world, rank, local, steps=1, warmup=1)
     out["adjoint"] = _compact(adj, ("value", "unit", "forward_ms", "recompute_ms", "reverse_ms",
@@ -807,7 +809,7 @@ def measure_batch(args, world, rank, local, precision=None, steps=None, warmup=N
     precision = args.precision if precision is None else precision
     steps = args.steps if steps is None else steps
     warmup = args.warmup if warmup is None else warmup
-    prec = Precision.F64 if precision == "f64" else Precision.Mixed
+    prec = {"mixed": Precision.Mixed, "fast": Precision.F64Fast}.get(precision, Precision.F64)
     sys_, n, dx, u, st = W.riemann_batch()
     for _ in range(max(warmup, 1)):
         g = GpuBatch1D(sys_, n, dx, u, precision=prec)

@@ -439,8 +439,9 @@ struct emg_batch1d {
             p.dest = u;
         }
         const dim3 grid((unsigned)((nseg + 31) / 32), 1, 1);
-        cudaError_t e = opts.precision == EMG_PRECISION_MIXED ? sweep_launch_batch_mixed(opts.mode, p, grid, stream)
-                                                               : sweep_launch_batch_f64(opts.mode, p, grid, stream);
+        cudaError_t e = opts.precision == EMG_PRECISION_MIXED      ? sweep_launch_batch_mixed(opts.mode, p, grid, stream)
+                        : opts.precision == EMG_PRECISION_F64_FAST ? sweep_launch_batch_fast(opts.mode, p, grid, stream)
+                                                                   : sweep_launch_batch_f64(opts.mode, p, grid, stream);
         if (e != cudaSuccess) return set_error(EMG_ERR_CUDA, std::string("batch sweep: ") + cudaGetErrorString(e));
         return EMG_OK;
     }
@@ -546,7 +547,7 @@ int emg_batch1d_create(const emg_eos* eos, const emg_opts* opts, const emg_bc bc
             return set_error(EMG_ERR_INVALID, "batched lines support periodic, outflow, reflect and Dirichlet boundaries");
     if ((bc[0].kind == EMG_BC_PERIODIC) != (bc[1].kind == EMG_BC_PERIODIC))
         return set_error(EMG_ERR_INVALID, "periodic boundaries must be paired");
-    if (opts->mode < 0 || opts->mode > 2 || (opts->precision != 0 && opts->precision != 1))
+    if (opts->mode < 0 || opts->mode > 2 || opts->precision < 0 || opts->precision > 2)
         return set_error(EMG_ERR_INVALID, "unknown mode or precision");
     for (size_t i = 0; i < ninst; i++) {
         if (n[i] < 2) return set_error(EMG_ERR_INVALID, "every instance needs at least 2 cells");

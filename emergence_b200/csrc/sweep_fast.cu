@@ -24,6 +24,20 @@ template <int P, int MODE> static cudaError_t launch_amr_d(const SweepParams& p,
 template <int MODE> static cudaError_t launch_amr_p(int P, const SweepParams& p, dim3 grid, cudaStream_t s) {
     return P == 16 ? launch_amr_d<16, MODE>(p, grid, s) : (P == 32 ? launch_amr_d<32, MODE>(p, grid, s) : cudaErrorInvalidValue);
 }
+// batched independent 1-D lines along axis 0, P = 32 segments per CTA
+template <int MODE> static cudaError_t launch_batch(const SweepParams& p, dim3 grid, cudaStream_t s) {
+    sweep_fast_kernel<32, 0, MODE, KIND_BATCH><<<grid, SWEEP_THREADS, SweepSmem<F64Fast, 32, MODE>::bytes(), s>>>(p);
+    return cudaGetLastError();
+}
+cudaError_t sweep_launch_batch_fast(int mode, const SweepParams& p, dim3 grid, cudaStream_t s) {
+    switch (mode) {
+        case MODE_WENO: return launch_batch<MODE_WENO>(p, grid, s);
+        case MODE_HYBRID: return launch_batch<MODE_HYBRID>(p, grid, s);
+        case MODE_CENTRAL: return launch_batch<MODE_CENTRAL>(p, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t sweep_launch_amr_fast(int P, int mode, const SweepParams& p, dim3 grid, cudaStream_t s) {
     switch (mode) {
         case MODE_WENO: return launch_amr_p<MODE_WENO>(P, p, grid, s);
@@ -80,10 +94,18 @@ template <int MODE> static cudaError_t attr_p() {
     return e;
 }
 
+template <int MODE> static cudaError_t attr_batch() {
+    return cudaFuncSetAttribute(sweep_fast_kernel<32, 0, MODE, KIND_BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)SweepSmem<F64Fast, 32, MODE>::bytes());
+}
+
 cudaError_t sweep_prepare_fast() {
     cudaError_t e = attr_p<MODE_WENO>();
     if (e == cudaSuccess) e = attr_p<MODE_HYBRID>();
     if (e == cudaSuccess) e = attr_p<MODE_CENTRAL>();
+    if (e == cudaSuccess) e = attr_batch<MODE_WENO>();
+    if (e == cudaSuccess) e = attr_batch<MODE_HYBRID>();
+    if (e == cudaSuccess) e = attr_batch<MODE_CENTRAL>();
     return e;
 }
 

@@ -17,6 +17,7 @@ cudaError_t sweep_launch_amr_fast(int P, int mode, const SweepParams& p, dim3 gr
 // Batched independent 1-D lines (SweepParams::segs), 32 segments per CTA.
 cudaError_t sweep_launch_batch_f64(int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 cudaError_t sweep_launch_batch_mixed(int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
+cudaError_t sweep_launch_batch_fast(int mode, const SweepParams& p, dim3 grid, cudaStream_t s);
 // 3-D uniform grids, WENO mode, P = 32: phase-A rows staged by TMA from the
 // stage input described by `tm` (a 4-D map: k, j, i, field; box RM rows ×
 // 32 lanes × 1 × 5 fields, the row axis being p.d). Resident CTAs per SM of

@@ -90,7 +90,7 @@ enum emg_precision {
     EMG_PRECISION_F64 = 0,  /* plain FP64 form: all scheme arithmetic in f64 */
     EMG_PRECISION_MIXED = 1, /* FP32 WENO-Z interpolation and HLLC wave-speed bounds; FP64 state, primitive
                                 recovery, projections, HLLC and central fluxes (reciprocals to ~1e-12), limiter */
-    EMG_PRECISION_F64_FAST = 2 /* fast FP64 form (uniform grids and Euler AMR): all arithmetic in f64 with FMA
+    EMG_PRECISION_F64_FAST = 2 /* fast FP64 form (every solver but the adjoint): all arithmetic in f64 with FMA
                                   contraction and Newton-refined reciprocals and square roots (about one ulp)
                                   in place of correctly rounded divisions; within 1e-12 relative L1 of the
                                   plain form instead of bitwise */

@@ -156,7 +156,6 @@ def batch_create(n, dx, bc=(OUTFLOW, OUTFLOW), o=None):
     (dict(n=[64], dx=[0.1], bc=(CHARACTERISTIC, OUTFLOW)), "boundaries"),
     (dict(n=[64], dx=[0.1], o=opts(mode=5)), "mode"),
     (dict(n=[64], dx=[0.1], o=opts(precision=3)), "precision"),
-    (dict(n=[64], dx=[0.1], o=opts(precision=2)), "precision"),  # the fast FP64 form is not built for lines
 ])
 def test_batch1d_create_rejects_bad_arguments(args, want):
     rc = batch_create(**args)

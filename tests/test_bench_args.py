@@ -42,7 +42,7 @@ def test_fast_form_is_a_uniform_workload_option(monkeypatch):
     import pytest
     assert _parse(["--precision", "fast"], monkeypatch).precision == "fast"
     with pytest.raises(SystemExit):
-        _parse(["--precision", "fast", "--workload", "batch"], monkeypatch)
+        _parse(["--precision", "fast", "--workload", "adjoint"], monkeypatch)
 
 
 def test_subrecords_are_on_by_default(monkeypatch):

@@ -257,3 +257,26 @@ def test_fast_five_equation_form_on_block_amr():
     err = np.abs(ug - uo).reshape(-1, 7).sum(axis=0) / np.maximum(den, 1e-3 * den[0])
     print("five AMR fast rel L1", err)
     assert np.all(err <= TOL), err
+
+
+def test_fast_form_of_the_batched_lines():
+    """The batched 1-D Riemann problems in the fast form, each to t = 0.15
+    with its own time steps: every instance within the long-run tolerance of
+    its oracle run (the step counts and final times equal)."""
+    from emergence_b200 import GpuBatch1D
+    from test_gpu_batch import oracle_instance
+    sys_, n, dx, u, st = W.riemann_batch(ninst=32, nmin=64, nmax=300, seed=9)
+    g = GpuBatch1D(sys_, n, dx, u, precision=Precision.F64Fast)
+    g.run_to(0.15)
+    t, steps = g.status()
+    out = g.split(g.download())
+    ins = g.split(u)
+    live = [0, 1, 4]
+    num, den = np.zeros(3), np.zeros(3)
+    for i in range(len(n)):
+        ref, osteps, ot = oracle_instance(sys_, n[i], ins[i], 0.15)
+        assert int(steps[i]) == osteps and t[i] == ot, i
+        num += np.abs(out[i] - ref)[:, live].sum(axis=0)
+        den += np.abs(ref)[:, live].sum(axis=0)
+    print("batched fast rel L1 (rho, rho u, E)", num / den)
+    assert np.all(num / den <= LONG_TOL)
