@@ -162,7 +162,12 @@ template <int RM, int MODE> struct RingSize {
 
 template <typename RF, int P, int MODE> struct SweepSmem {
     static constexpr int RM = SWEEP_THREADS / P;
-    static constexpr int RS = RingSize<RM, MODE>::value;
+    static constexpr int RS = RingSize<RM, MODE>::value;  // W (and TH) ring rows
+    // the flux rings hold exactly what one round keeps alive: phase C of round
+    // r reads midpoints [RM r − 4, RM r + RM) and phase D faces [RM r − 5,
+    // RM r + RM − 4), so RM + 4 and RM + 1 slots (indexed modulo)
+    static constexpr int RSM = RM + 4;
+    static constexpr int RSF = RM + 1;
     // values per cell in the primitive ring: w(5), plus ρe for the central
     // flux, plus the two sensor logarithms for the hybrid switch
     static constexpr int NW = MODE == MODE_WENO ? 5 : (MODE == MODE_CENTRAL ? 6 : 8);
@@ -173,8 +178,8 @@ template <typename RF, int P, int MODE> struct SweepSmem {
     static constexpr bool MID = MODE != MODE_CENTRAL;
     static constexpr size_t bytes() {
         return (size_t)RS * STRW * sizeof(double)                                    // W (f64 primitives, ρe, sensors)
-               + (MID ? (size_t)RS * STR * sizeof(double) : 0)                         // MF (midpoint fluxes)
-               + (size_t)RS * STR * sizeof(double)                                    // F (face fluxes)
+               + (MID ? (size_t)RSM * STR * sizeof(double) : 0)                        // MF (midpoint fluxes)
+               + (size_t)RSF * STR * sizeof(double)                                   // F (face fluxes)
                + (MODE == MODE_HYBRID ? (size_t)RS * P * sizeof(double) : 0);         // TH (blend weights)
     }
 };
@@ -210,6 +215,13 @@ struct Sweep {
     __device__ static __forceinline__ int slot(int x) { return x & (RS - 1); }
     // element (row x, field k, lane l) of a ring with row stride S
     template <int S> __device__ static __forceinline__ int at(int x, int k, int l) { return slot(x) * S + k * P + l; }
+    // midpoint and face flux rings (x ≥ 0)
+    __device__ static __forceinline__ int atM(int x, int k, int l) {
+        return (int)((unsigned)x % (unsigned)SM::RSM) * STR + k * P + l;
+    }
+    __device__ static __forceinline__ int atF(int x, int k, int l) {
+        return (int)((unsigned)x % (unsigned)SM::RSF) * STR + k * P + l;
+    }
 
     // Characteristic WENO5-Z interpolation to midpoint m and its HLLC flux:
     // sparse form of C/scheme.rs:286-333. The zero entries of the Euler
@@ -519,10 +531,10 @@ struct Sweep {
         double* MF = nullptr;  // midpoint fluxes (FP64 in both forms)
         if constexpr (MID) {
             MF = reinterpret_cast<double*>(sp);
-            sp += (size_t)RS * STR * sizeof(double);
+            sp += (size_t)SM::RSM * STR * sizeof(double);
         }
         double* F = reinterpret_cast<double*>(sp);
-        sp += (size_t)RS * STR * sizeof(double);
+        sp += (size_t)SM::RSF * STR * sizeof(double);
         double* TH = reinterpret_cast<double*>(sp);
 
         __shared__ unsigned int s_fallback, s_limited, s_weno;
@@ -815,7 +827,7 @@ struct Sweep {
                         else
                             midpoint<STRW>(ed, W, m, l, f, fb);
 #pragma unroll
-                        for (int k = 0; k < 5; k++) MF[at<STR>(m, k, l)] = f[k];
+                        for (int k = 0; k < 5; k++) MF[atM(m, k, l)] = f[k];
                         if (fb && (m < lane_len(l) || lane_tail(l))) atomicAdd(&s_fallback, chain_mult(m, 5));
                     }
                 }
@@ -845,11 +857,11 @@ struct Sweep {
 #pragma unroll
                             for (int k = 0; k < 5; k++) {
                                 double acc = 0.0;
-                                acc = acc + s6(0) * double(MF[at<STR>(fidx + 2, k, l)]);
-                                acc = acc + s6(1) * double(MF[at<STR>(fidx + 3, k, l)]);
-                                acc = acc + s6(1) * double(MF[at<STR>(fidx + 1, k, l)]);
-                                acc = acc + s6(2) * double(MF[at<STR>(fidx + 4, k, l)]);
-                                acc = acc + s6(2) * double(MF[at<STR>(fidx, k, l)]);
+                                acc = acc + s6(0) * double(MF[atM(fidx + 2, k, l)]);
+                                acc = acc + s6(1) * double(MF[atM(fidx + 3, k, l)]);
+                                acc = acc + s6(1) * double(MF[atM(fidx + 1, k, l)]);
+                                acc = acc + s6(2) * double(MF[atM(fidx + 4, k, l)]);
+                                acc = acc + s6(2) * double(MF[atM(fidx, k, l)]);
                                 fh[k] = acc;
                             }
                             if (theta < 1.0) {  // C/scheme.rs:270-276
@@ -910,7 +922,7 @@ struct Sweep {
                         }
                     }
 #pragma unroll
-                    for (int k = 0; k < 5; k++) F[at<STR>(fidx, k, l)] = fh[k];
+                    for (int k = 0; k < 5; k++) F[atF(fidx, k, l)] = fh[k];
                     if (!AMR && p.theta_rec && in_bounds(p.ctl, base0 + (int64_t)i * p.sd + s_loff[l], p.ncell)) {
                         // recorded for the discrete adjoint, at the face's left cell
                         p.theta_rec[base0 + (int64_t)i * p.sd + s_loff[l]] = th_rec;
@@ -951,7 +963,7 @@ struct Sweep {
 #pragma unroll
                     for (int k = 0; k < 5; k++) {
                         // the block solver divides by dx (C/amr.rs:1263), the uniform one multiplies by 1/dx
-                        const double df = F[at<STR>(c + 1, k, l)] - F[at<STR>(c, k, l)];
+                        const double df = F[atF(c + 1, k, l)] - F[atF(c, k, l)];
                         const double x = AMR ? df / dx : df * inv_l;
                         const double prev = p.first ? 0.0 : p.rhs[k * p.ncell + g];
                         res[k] = prev - x;

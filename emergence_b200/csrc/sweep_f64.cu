@@ -5,7 +5,7 @@
 namespace emg {
 
 template <int P, int D, int MODE, int KIND = KIND_GRID>
-__global__ void __launch_bounds__(SWEEP_THREADS, 3) sweep_f64_kernel(const SweepParams p) {
+__global__ void __launch_bounds__(SWEEP_THREADS, 4) sweep_f64_kernel(const SweepParams p) {
     Sweep<double, P, D, MODE, KIND>::run(p);
 }
 

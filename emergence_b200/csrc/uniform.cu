@@ -551,6 +551,9 @@ static EncodeTiledFn encode_tiled_fn() {
     return fn;
 }
 
+// TMA row staging is an explicit opt-in (EMG_TMA=1): it is used wherever its
+// alignment conditions hold, although its staging tile leaves room for fewer
+// resident CTAs per SM (3) than the plain-load sweeps (4)
 void setup_tma(emg_uniform* h) {
     h->tma = 0;
     const char* on = std::getenv("EMG_TMA");
@@ -558,9 +561,8 @@ void setup_tma(emg_uniform* h) {
     if (h->ndim != 3 || h->opts.mode != EMG_MODE_WENO || h->mesh.ng % 2 != 0 || h->m[2] % 2 != 0) return;
     if (h->opts.precision == EMG_PRECISION_F64_FAST) return;  // plain loads only
     const bool mixed = h->opts.precision == EMG_PRECISION_MIXED;
-    const int plain = mixed ? sweep_ctas_per_sm_mixed(32, MODE_WENO) : sweep_ctas_per_sm_f64(32, MODE_WENO);
     const int staged = mixed ? sweep_tma_ctas_per_sm_mixed() : sweep_tma_ctas_per_sm_f64();
-    if (staged < plain) return;
+    if (staged < 1) return;
     EncodeTiledFn enc = encode_tiled_fn();
     if (!enc) return;
     const cuuint64_t dims[4] = {(cuuint64_t)h->m[2], (cuuint64_t)h->m[1], (cuuint64_t)h->m[0], 5};
