@@ -14,6 +14,7 @@
 // the reference CPU solver does.
 #include "uniform_internal.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -439,9 +440,13 @@ int64_t plan_seg(const emg_uniform* h, int d, int P) {
         cudaGetLastError();
         sms = 148;
     }
-    const int per_sm = h->opts.precision == EMG_PRECISION_MIXED      ? sweep_ctas_per_sm_mixed(P, h->opts.mode)
-                       : h->opts.precision == EMG_PRECISION_F64_FAST ? sweep_ctas_per_sm_fast(P, h->opts.mode)
-                                                                     : sweep_ctas_per_sm_f64(P, h->opts.mode);
+    // at most 3 resident CTAs per SM count as slots: a fourth shares the SM's
+    // FP64 pipe instead of adding throughput, so cutting pencils into shorter
+    // segments to fill it only adds halo rows (the 2-D 512² step measured
+    // 20 % slower planned for 4)
+    const int per_sm = std::min(3, h->opts.precision == EMG_PRECISION_MIXED      ? sweep_ctas_per_sm_mixed(P, h->opts.mode)
+                                   : h->opts.precision == EMG_PRECISION_F64_FAST ? sweep_ctas_per_sm_fast(P, h->opts.mode)
+                                                                                 : sweep_ctas_per_sm_f64(P, h->opts.mode));
     const int64_t slots = (int64_t)sms * per_sm;
     const int64_t lane_tiles = (nl + P - 1) / P;
     int64_t best = nd;
