@@ -375,7 +375,7 @@ def run_ours(args, world, rank, local):
                          "alg_bytes_per_launch": alg_bytes_per_launch, "avg_launch_ms": per_launch_ms,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback",
                          "compute_note": "the sweep is FP64-ALU bound (59 FP64 flop per algorithmic byte): FP64 pipe "
-                                         "48-52 % active, issue 54-57 % (ncu, profiles/sweep_f64_uniform_160.md); "
+                                         "45-50 % active at 4 CTAs per SM (ncu, profiles/sweep_flops_uniform_160.md); "
                                          "the HBM fraction is small by construction",
                          "fp64": fp64_roofline},
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()},
