@@ -1762,9 +1762,17 @@ struct emg_amr {
             if (!src_bits) AMR_CUDA(cudaMalloc(&src_bits, sizeof(unsigned long long)));
             AMR_CUDA(cudaMemsetAsync(src_bits, 0, sizeof(unsigned long long), stream));
             AmrDev A = view();
-            amr_dilatation_five<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((bcells() + 255) / 256, 16)), 256, 0,
+            int64_t ninner = 1, nface = 1;
+            for (int d = 0; d < 3; d++) {
+                ninner *= act[d] ? bd[d] - 2 : 1;
+                nface = std::max<int64_t>(nface, bcells() / std::max(bd[d], 1));
+            }
+            amr_dilatation_five<<<dim3((unsigned)nleaves, (unsigned)std::min<int64_t>((ninner + 255) / 256, 16)), 256, 0,
                                   stream>>>(A, dleaves.p, dlevel.p, didx.p, ddxl.p, src_bits);
-            launches++;
+            amr_dilatation_five_faces<<<dim3((unsigned)nleaves, (unsigned)(2 * dims.size()),
+                                             (unsigned)std::min<int64_t>((nface + 127) / 128, 32)),
+                                        128, 0, stream>>>(A, dleaves.p, dlevel.p, didx.p, ddxl.p, src_bits);
+            launches += 2;
             AMR_CUDA(cudaGetLastError());
             AMR_CUDA(cudaMemcpyAsync(&sbits, src_bits, sizeof sbits, cudaMemcpyDeviceToHost, stream));
         }

@@ -181,6 +181,101 @@ template <int DEPTH, int NV> __device__ void amr_predict_t(const AmrDev& A, int 
     }
 }
 
+// The same sample and prediction for three of the NV fields only (indices
+// qs[0..2]): each field's prediction is its own weighted sum in the same
+// order, so the three values are those of amr_sample_t.
+template <int DEPTH, int NV> __device__ void amr_predict3_t(const AmrDev& A, int l, const int64_t* g, const int* qs, double* out);
+
+template <int DEPTH, int NV>
+__device__ __forceinline__ void amr_sample3_t(const AmrDev& A, int l, const int64_t* g_in, const int* qs, double* v) {
+    int64_t g[3] = {g_in[0], g_in[1], g_in[2]};
+    bool flip[3] = {false, false, false};
+#pragma unroll
+    for (int d = 2; d >= 0; d--) {
+        if (!A.act[d]) {
+            g[d] = 0;
+            continue;
+        }
+        const int64_t n = amr_nlevel(A, l, d);
+        if (g[d] < 0 || g[d] >= n) {
+            const int side = g[d] >= n ? 1 : 0;
+            const int kind = A.bc[d][side];
+            if (kind == EMG_BC_PERIODIC) {
+                g[d] = amr_erem(g[d], n);
+            } else if (kind == EMG_BC_OUTFLOW) {
+                g[d] = g[d] < 0 ? 0 : n - 1;
+            } else if (kind == EMG_BC_REFLECT) {
+                g[d] = side == 0 ? -1 - g[d] : 2 * n - 1 - g[d];
+                flip[d] = true;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 3; j++) v[j] = A.bcs[d][side][qs[j]];
+                return;
+            }
+        }
+    }
+    int64_t key[3], c[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        key[d] = A.act[d] ? amr_ediv(g[d], A.bd[d]) : 0;
+        c[d] = A.act[d] ? amr_erem(g[d], A.bd[d]) : 0;
+    }
+    const int id = amr_get(A, l, key);
+    if (id >= 0) {
+        const int64_t cell = amr_cell(A, c);
+        if (BOUNDS_CHECK && (cell < 0 || cell >= A.bcell || (int64_t)id * A.bcell + cell >= A.ntot)) {
+            atomicOr(A.err, 4u);
+#pragma unroll
+            for (int j = 0; j < 3; j++) v[j] = 0.0;
+            return;
+        }
+        const double* p = A.u + (int64_t)id * A.bcell + cell;
+#pragma unroll
+        for (int j = 0; j < 3; j++) v[j] = p[(int64_t)qs[j] * A.ntot];
+    } else {
+        amr_predict3_t<DEPTH, NV>(A, l, g, qs, v);
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const int m = qs[j] - amr_iu<NV>();
+        if (m >= 0 && m < 3 && flip[m]) v[j] = -v[j];
+    }
+}
+
+template <int DEPTH, int NV> __device__ void amr_predict3_t(const AmrDev& A, int l, const int64_t* g, const int* qs, double* out) {
+#pragma unroll
+    for (int j = 0; j < 3; j++) out[j] = 0.0;
+    if constexpr (DEPTH <= 0) {
+        atomicOr(A.err, 1u);
+        return;
+    } else {
+        if (l <= 0) {
+            atomicOr(A.err, 1u);
+            return;
+        }
+        int total = 1;
+        for (int i = 0; i < A.ndims; i++) total *= 6;
+        for (int s = 0; s < total; s++) {
+            double w = 1.0;
+            int64_t c[3] = {0, 0, 0};
+            int rem = s;
+            for (int i = 0; i < A.ndims; i++) {
+                const int d = A.dims[i];
+                const int k = rem % 6;
+                rem /= 6;
+                const int odd = (int)amr_erem(g[d], 2);
+                const int64_t base = amr_ediv(g[d], 2) + (odd == 1 ? -2 : -3);
+                c[d] = base + k;
+                w = w * A.wp[odd][k];
+            }
+            double v[3];
+            amr_sample3_t<DEPTH - 1, NV>(A, l - 1, c, qs, v);
+#pragma unroll
+            for (int j = 0; j < 3; j++) out[j] = out[j] + w * v[j];
+        }
+    }
+}
+
 constexpr int AMR_PREDICT_DEPTH = 3;
 template <int NV = 5>
 __device__ __forceinline__ void amr_sample(const AmrDev& A, int l, const int64_t* g, double* v, int) {

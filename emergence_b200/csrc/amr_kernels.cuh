@@ -945,42 +945,50 @@ __global__ void amr_cfl(const AmrDev A, const int* __restrict__ leaves, const in
 // with ∇·u from the primitive velocities of the two neighbours along each
 // active axis, read in the block or, across a block face, sampled from the
 // hierarchy (the block's neighbour or its prediction). Max into *src_bits.
-__global__ void amr_dilatation_five(const AmrDev A, const int* __restrict__ leaves, const int* __restrict__ level,
-                                    const int64_t* __restrict__ idx, const double* __restrict__ dxl,
-                                    unsigned long long* src_bits) {
-    const int slot = leaves[blockIdx.x];
-    const int l = level[slot];
-    const int64_t n = (int64_t)A.bd[0] * A.bd[1] * A.bd[2];
-    const Five f = Five::from(A.fsys);
-    double src = 0.0;
-    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
-        int64_t c[3];
-        box_coord(q, A.bd, c);
-        double uu[NF], w[NF];
-        amr_load<NF>(A, slot, amr_cell(A, c), uu);
-        f.to_prim(uu, w);
-        double divu = 0.0;
-        for (int i = 0; i < A.ndims; i++) {
-            const int d = A.dims[i];
-            double vv[2];
-            for (int hi = 0; hi < 2; hi++) {
-                int64_t cc[3] = {c[0], c[1], c[2]};
-                cc[d] += hi ? 1 : -1;
-                double un[NF], wn[NF];
-                if (cc[d] >= 0 && cc[d] < A.bd[d]) {
-                    amr_load<NF>(A, slot, amr_cell(A, cc), un);
-                } else {
-                    int64_t g[3];
-                    for (int e = 0; e < 3; e++) g[e] = idx[3 * slot + e] * A.bd[e] + cc[e];
-                    amr_sample<NF>(A, l, g, un, 0);
+// A neighbour contributes only its velocity u_d = (ρu)_d/(α1ρ1 + α2ρ2), the
+// value its primitive recovery computes (multiphase.rs:131-146), so a sampled
+// neighbour predicts those three fields only. The cells of the block's
+// interior (no neighbour outside the block) and those of its faces run in
+// two kernels, so that a warp's sampled neighbours take the same branch.
+// EDGE false: every neighbour lies in the block (the interior kernel)
+template <bool EDGE>
+__device__ __forceinline__ double five_cell_dilatation(const AmrDev& A, const Five& f, int slot, int l,
+                                                       const int64_t* __restrict__ idx, const double* __restrict__ dxl,
+                                                       const int64_t* c) {
+    double uu[NF], w[NF];
+    amr_load<NF>(A, slot, amr_cell(A, c), uu);
+    f.to_prim(uu, w);
+    double divu = 0.0;
+    for (int i = 0; i < A.ndims; i++) {
+        const int d = A.dims[i];
+        double vv[2];
+        for (int hi = 0; hi < 2; hi++) {
+            int64_t cc[3] = {c[0], c[1], c[2]};
+            cc[d] += hi ? 1 : -1;
+            if (!EDGE || (cc[d] >= 0 && cc[d] < A.bd[d])) {
+                const int64_t cell = amr_cell(A, cc);
+                if (BOUNDS_CHECK && (cell < 0 || cell >= A.bcell || (int64_t)slot * A.bcell + cell >= A.ntot)) {
+                    atomicOr(A.err, 4u);
+                    vv[hi] = 0.0;
+                    continue;
                 }
-                f.to_prim(un, wn);
-                vv[hi] = wn[F_IU + d];
+                const double* p = A.u + (int64_t)slot * A.bcell + cell;
+                vv[hi] = p[(int64_t)(F_IU + d) * A.ntot] / (p[0] + p[A.ntot]);
+            } else if constexpr (EDGE) {
+                int64_t g[3];
+                for (int e = 0; e < 3; e++) g[e] = idx[3 * slot + e] * A.bd[e] + cc[e];
+                const int qs[3] = {0, 1, F_IU + d};
+                double v[3];
+                amr_sample3_t<AMR_PREDICT_DEPTH, NF>(A, l, g, qs, v);
+                vv[hi] = v[2] / (v[0] + v[1]);
             }
-            divu = divu + fabs(vv[1] - vv[0]) / (2.0 * dxl[3 * l + d]);
         }
-        src = fmax(src, f.dilatation_rate(w, divu));
+        divu = divu + fabs(vv[1] - vv[0]) / (2.0 * dxl[3 * l + d]);
     }
+    return f.dilatation_rate(w, divu);
+}
+
+__device__ __forceinline__ void five_src_max(double src, unsigned long long* src_bits) {
     for (int o = 16; o > 0; o >>= 1) src = fmax(src, __shfl_xor_sync(0xffffffffu, src, o));
     __shared__ double sr[32];
     if ((threadIdx.x & 31) == 0) sr[threadIdx.x >> 5] = src;
@@ -990,6 +998,50 @@ __global__ void amr_dilatation_five(const AmrDev A, const int* __restrict__ leav
         for (int w2 = 1; w2 < (int)(blockDim.x >> 5); w2++) v = fmax(v, sr[w2]);
         if (!isnan(v) && v > 0.0) atomicMax(src_bits, (unsigned long long)__double_as_longlong(v));
     }
+}
+
+// cells whose neighbours along every active axis lie in the block
+__global__ void amr_dilatation_five(const AmrDev A, const int* __restrict__ leaves, const int* __restrict__ level,
+                                    const int64_t* __restrict__ idx, const double* __restrict__ dxl,
+                                    unsigned long long* src_bits) {
+    const int slot = leaves[blockIdx.x];
+    const int l = level[slot];
+    int ni[3];
+    for (int d = 0; d < 3; d++) ni[d] = A.act[d] ? A.bd[d] - 2 : 1;
+    const int64_t n = (int64_t)ni[0] * ni[1] * ni[2];
+    const Five f = Five::from(A.fsys);
+    double src = 0.0;
+    for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
+        int64_t c[3];
+        box_coord(q, ni, c);
+        for (int d = 0; d < 3; d++)
+            if (A.act[d]) c[d] += 1;
+        src = fmax(src, five_cell_dilatation<false>(A, f, slot, l, idx, dxl, c));
+    }
+    five_src_max(src, src_bits);
+}
+
+// the cells of face blockIdx.y (axis dims[y/2], low or high side): cells on
+// an edge belong to two or three faces and are evaluated once per face
+__global__ void __launch_bounds__(128, 3) amr_dilatation_five_faces(const AmrDev A, const int* __restrict__ leaves, const int* __restrict__ level,
+                                          const int64_t* __restrict__ idx, const double* __restrict__ dxl,
+                                          unsigned long long* src_bits) {
+    const int slot = leaves[blockIdx.x];
+    const int l = level[slot];
+    const int df = A.dims[blockIdx.y >> 1];
+    const int side = blockIdx.y & 1;
+    int nf[3];
+    for (int d = 0; d < 3; d++) nf[d] = d == df ? 1 : (A.act[d] ? A.bd[d] : 1);
+    const int64_t n = (int64_t)nf[0] * nf[1] * nf[2];
+    const Five f = Five::from(A.fsys);
+    double src = 0.0;
+    for (int64_t q = blockIdx.z * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.z * blockDim.x) {
+        int64_t c[3];
+        box_coord(q, nf, c);
+        c[df] = side ? A.bd[df] - 1 : 0;
+        src = fmax(src, five_cell_dilatation<true>(A, f, slot, l, idx, dxl, c));
+    }
+    five_src_max(src, src_bits);
 }
 
 // ---------------------------------------------------------------- subcycling
