@@ -66,15 +66,19 @@ struct FiveSweepParams {
 
 template <int P, int MODE> struct FiveSmem {
     static constexpr int RM = SWEEP_THREADS / P;
-    static constexpr int RS = RingSize<RM, MODE>::value;
+    static constexpr int RS = RingSize<RM, MODE>::value;  // W (and TH) ring rows
+    // flux rings of exactly what one round keeps alive, as in the Euler sweep:
+    // midpoints [RM r − 4, RM r + RM), faces [RM r − 5, RM r + RM − 4)
+    static constexpr int RSM = RM + 4;
+    static constexpr int RSF = RM + 1;
     // per cell: 7 primitives, + ρe (central flux), + 3 sensor values (hybrid)
     static constexpr int NW = MODE == MODE_WENO ? NF : (MODE == MODE_CENTRAL ? NF + 1 : NF + 4);
     static constexpr int STRW = NW * P + 1;
     static constexpr int STR = (NF + 1) * P + 1;  // 7 fluxes + velocity
     static constexpr bool MID = MODE != MODE_CENTRAL;
     static constexpr size_t bytes() {
-        return (size_t)RS * STRW * sizeof(double) + (MID ? (size_t)RS * STR * sizeof(double) : 0) +
-               (size_t)RS * STR * sizeof(double) + (MODE == MODE_HYBRID ? (size_t)RS * P * sizeof(double) : 0);
+        return (size_t)RS * STRW * sizeof(double) + (MID ? (size_t)RSM * STR * sizeof(double) : 0) +
+               (size_t)RSF * STR * sizeof(double) + (MODE == MODE_HYBRID ? (size_t)RS * P * sizeof(double) : 0);
     }
 };
 
@@ -94,6 +98,13 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
 
     __device__ static __forceinline__ int slot(int x) { return x & (RS - 1); }
     template <int S> __device__ static __forceinline__ int at(int x, int k, int l) { return slot(x) * S + k * P + l; }
+    // midpoint and face flux rings (x ≥ 0)
+    __device__ static __forceinline__ int atM(int x, int k, int l) {
+        return (int)((unsigned)x % (unsigned)SM::RSM) * STR + k * P + l;
+    }
+    __device__ static __forceinline__ int atF(int x, int k, int l) {
+        return (int)((unsigned)x % (unsigned)SM::RSF) * STR + k * P + l;
+    }
 
     // scheme.rs:286-333 with the five-equation eigenvectors (multiphase.rs:202-236)
     __device__ static __forceinline__ double midpoint(const Five& s, const double* __restrict__ W, int m, int l,
@@ -247,10 +258,10 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
         double* MF = nullptr;
         if constexpr (MID) {
             MF = reinterpret_cast<double*>(sp);
-            sp += (size_t)RS * STR * sizeof(double);
+            sp += (size_t)SM::RSM * STR * sizeof(double);
         }
         double* F = reinterpret_cast<double*>(sp);
-        sp += (size_t)RS * STR * sizeof(double);
+        sp += (size_t)SM::RSF * STR * sizeof(double);
         double* TH = reinterpret_cast<double*>(sp);
 
         __shared__ unsigned int s_fallback, s_limited, s_weno;
@@ -414,8 +425,8 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
                         bool fb;
                         const double us = midpoint(sys, W, m, l, f, fb);
 #pragma unroll
-                        for (int k = 0; k < NF; k++) MF[at<STR>(m, k, l)] = f[k];
-                        MF[at<STR>(m, NF, l)] = us;
+                        for (int k = 0; k < NF; k++) MF[atM(m, k, l)] = f[k];
+                        MF[atM(m, NF, l)] = us;
                         if (fb && (m < Ls || tail)) atomicAdd(&s_fallback, chain_mult(m, 5));
                     }
                 }
@@ -463,11 +474,11 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
 #pragma unroll
                             for (int k = 0; k <= NF; k++) {
                                 double acc = 0.0;
-                                acc = acc + s6(0) * MF[at<STR>(fidx + 2, k, l)];
-                                acc = acc + s6(1) * MF[at<STR>(fidx + 3, k, l)];
-                                acc = acc + s6(1) * MF[at<STR>(fidx + 1, k, l)];
-                                acc = acc + s6(2) * MF[at<STR>(fidx + 4, k, l)];
-                                acc = acc + s6(2) * MF[at<STR>(fidx, k, l)];
+                                acc = acc + s6(0) * MF[atM(fidx + 2, k, l)];
+                                acc = acc + s6(1) * MF[atM(fidx + 3, k, l)];
+                                acc = acc + s6(1) * MF[atM(fidx + 1, k, l)];
+                                acc = acc + s6(2) * MF[atM(fidx + 4, k, l)];
+                                acc = acc + s6(2) * MF[atM(fidx, k, l)];
                                 if (k < NF)
                                     fh[k] = acc;
                                 else
@@ -518,8 +529,8 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
                         }
                     }
 #pragma unroll
-                    for (int k = 0; k < NF; k++) F[at<STR>(fidx, k, l)] = fh[k];
-                    F[at<STR>(fidx, NF, l)] = uf;
+                    for (int k = 0; k < NF; k++) F[atF(fidx, k, l)] = fh[k];
+                    F[atF(fidx, NF, l)] = uf;
                     if (AMR && fidx % p.nd == 0) {
                         // block boundary faces for refluxing (C/amr.rs:1291-1295): the low
                         // face of block j and the high face of block j − 1 of the chain
@@ -554,7 +565,7 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
 #pragma unroll
                     for (int k = 0; k < NF; k++) {
                         // the block solver divides by dx (C/amr.rs:1273), the uniform one multiplies by 1/dx
-                        const double df = F[at<STR>(c + 1, k, l)] - F[at<STR>(c, k, l)];
+                        const double df = F[atF(c + 1, k, l)] - F[atF(c, k, l)];
                         const double x = AMR ? df / dx : df * inv;
                         const double prev = p.first ? 0.0 : p.rhs[k * p.ncell + g];
                         res[k] = prev - x;
@@ -564,7 +575,7 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
                         double wc[NF];
 #pragma unroll
                         for (int k = 0; k < NF; k++) wc[k] = W[at<STRW>(c + 5, k, l)];
-                        const double du = F[at<STR>(c + 1, NF, l)] - F[at<STR>(c, NF, l)];
+                        const double du = F[atF(c + 1, NF, l)] - F[atF(c, NF, l)];
                         res[F_IA] = res[F_IA] + (AMR ? sys.nc_coef(wc) * du / dx : sys.nc_coef(wc) * du * inv);
                     }
                     if (!p.last) {
