@@ -190,6 +190,8 @@ struct emg_amr {
         std::vector<int> rchunk;       // chunk starts into rfull (and its end)
         std::vector<int64_t> rchunk_max;
         DevVec<ScFace> faces;          // coarse–fine faces of its leaves (coarse side), by (d, side)
+        DevVec<int> choff[3], chslot[3];  // chains of its blocks along each axis for the level's sweeps
+        int nch[3] = {0, 0, 0};
         int face_start[7]{};
         int reg0 = 0;                  // their register rows [reg0, reg0 + nfaces)
     };
@@ -743,11 +745,14 @@ struct emg_amr {
         }
     }
 
-    // Chains of same-level leaves along d for the global sweeps: runs of +d
-    // neighbours (periodic sides included), at most AMR_CHAIN_MAX blocks each,
-    // every leaf in exactly one chain. `off` gets one start per chain plus the
-    // end, `slot` the blocks in order.
-    void build_chains(int d, const std::vector<int>& leaves, std::vector<int>& off, std::vector<int>& slot) const {
+    // Chains of same-level blocks along d for the sweeps: runs of +d neighbours
+    // (periodic sides included), at most AMR_CHAIN_MAX blocks each, every block
+    // of `leaves` in exactly one chain. Members are the leaves (global steps)
+    // or, with `any_block`, every block of the level (a subcycled level step,
+    // whose list holds the level's leaves and ancestors). `off` gets one start
+    // per chain plus the end, `slot` the blocks in order.
+    void build_chains(int d, const std::vector<int>& leaves, std::vector<int>& off, std::vector<int>& slot,
+                      bool any_block = false) const {
         off.clear();
         slot.clear();
         std::vector<char> seen(blocks.size(), 0);
@@ -761,7 +766,7 @@ struct emg_amr {
                 nk[d] = erem(nk[d], n);
             }
             const int j = get(b.level, nk);
-            return (j >= 0 && j != id && blocks[j].leaf) ? j : -1;
+            return (j >= 0 && j != id && (any_block || blocks[j].leaf)) ? j : -1;
         };
         for (int id : leaves) {
             if (seen[id]) continue;
@@ -952,14 +957,15 @@ struct emg_amr {
         return bd[lane] > 16 ? 32 : (bd[lane] * bd[other] >= 32 ? 32 : 16);
     }
     // sweeps of every active axis over the leaves, or over the `nlist` blocks of `list`
-    int sweeps(int stage, const int* list = nullptr, int nlist = 0) {
+    // `lv`: the subcycled level whose block chains replace `list` in the launch
+    int sweeps(int stage, const int* list = nullptr, int nlist = 0, const ScLevel* lv = nullptr) {
         for (int d : dims) {
-            int rc = sweep_axis(stage, d, dims[0], list, nlist);
+            int rc = sweep_axis(stage, d, dims[0], list, nlist, lv);
             if (rc) return rc;
         }
         return EMG_OK;
     }
-    int sweep_axis(int stage, int d, int first, const int* list = nullptr, int nlist = 0) {
+    int sweep_axis(int stage, int d, int first, const int* list = nullptr, int nlist = 0, const ScLevel* lv = nullptr) {
         const int* blk = list ? list : dleaves.p;
         const int nblk = list ? nlist : nleaves;
         AmrDev A = view();
@@ -1016,6 +1022,10 @@ struct emg_amr {
                 p.chain_off = dchain_off[d].p;
                 p.chain_slot = dchain_slot[d].p;
                 nz = nchain[d];
+            } else if (lv && lv->nch[d] > 0) {  // a subcycled level: chains of its blocks
+                p.chain_off = lv->choff[d].p;
+                p.chain_slot = lv->chslot[d].p;
+                nz = lv->nch[d];
             }
             const dim3 grid((unsigned)(nz * p.ngroups), 1, 1);
             cudaError_t e;
@@ -1828,6 +1838,14 @@ struct emg_amr {
             std::vector<int> bcl;
             int64_t pmax = 0, poff = 0;
             ghost_tasks(ids, copies, pboxes, bcl, pmax, poff);
+            for (int d = 0; d < 3; d++) {
+                L.nch[d] = 0;
+                if (!act[d]) continue;
+                std::vector<int> coff, cslot;
+                build_chains(d, ids, coff, cslot, true);
+                if ((rc = L.choff[d].put(coff, stream)) || (rc = L.chslot[d].put(cslot, stream))) return rc;
+                L.nch[d] = (int)coff.size() - 1;
+            }
             L.ncopy = (int)copies.size();
             L.npbox = (int)pboxes.size();
             L.nbcl = (int)bcl.size();
@@ -2013,7 +2031,7 @@ struct emg_amr {
                 NVK(sc_restore)<<<sc[l - 1].nblk, 256, 0, stream>>>(A, sc[l - 1].blist.p, usave);
                 launches++;
             }
-            if ((rc = sweeps(s + 1, L.blist.p, L.nblk))) return rc;
+            if ((rc = sweeps(s + 1, L.blist.p, L.nblk, &L))) return rc;
             const double w = weights[s] * dt;
             if (nf) {
                 NVK(sc_reg_coarse)<<<nf, 256, 0, stream>>>(A, L.faces.p, face, npen, creg, w);
@@ -2364,6 +2382,10 @@ struct emg_amr {
             L.bcl.release();
             L.rfull.release();
             L.faces.release();
+            for (int d = 0; d < 3; d++) {
+                L.choff[d].release();
+                L.chslot[d].release();
+            }
         }
         dall.release();
         dmap.release();
