@@ -333,7 +333,7 @@ def run_ours(args, world, rank, local):
         host = torch.empty(tuple(u.shape), dtype=torch.float64, pin_memory=True).numpy()
         host[...] = u
         out_host = torch.empty(tuple(u.shape), dtype=torch.float64, pin_memory=True).numpy()
-        # one untimed pass first (first-touch costs of the buffers and the driver's allocations)
+        # one untimed pass first (first-touch costs of the buffers and the CUDA driver's allocations)
         for timed in (False, True):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
