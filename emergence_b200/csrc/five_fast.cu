@@ -1,8 +1,10 @@
 // Fast FP64 form of the five-equation fused sweep: every value and operation
-// in FP64, built with FMA contraction, with the WENO5-Z weights and the
-// characteristic projection's coefficients from the one-ulp reciprocals of
-// physics.cuh's fast section. Held to a tolerance of the plain form (which
-// stays bit-exact with the reference CPU solver) instead of bit equality.
+// in FP64, built with FMA contraction, with the WENO5-Z weights, the
+// characteristic projection's coefficients, the mixture closure (1/(γ − 1) of
+// each phase precomputed), the Kapila coefficient, the primitive recovery and
+// the HLLC star states from the one-ulp reciprocals of physics.cuh's fast
+// section. Held to a tolerance of the plain form (which stays bit-exact with
+// the reference CPU solver) instead of bit equality.
 #include "five_launch.h"
 
 namespace emg {

@@ -20,16 +20,36 @@ struct FiveSysD {
     int kapila;
 };
 
+// a/b: correctly rounded in the plain form, a·(1/b) with the one-ulp
+// reciprocal of physics.cuh in the fast FP64 form (F)
+template <bool F> __device__ __forceinline__ double fdiv(double a, double b) {
+    if constexpr (F)
+        return a * rcp_f(b);
+    else
+        return a / b;
+}
+template <bool F> __device__ __forceinline__ double fsqrt(double x) {
+    if constexpr (F)
+        return sqrt_f(x);
+    else
+        return sqrt(x);
+}
+
+// Methods templated on F: the plain form (F false, the reference's operation
+// order, bit-exact without FMA contraction) or the fast FP64 form (F true,
+// one-ulp reciprocals and square roots, 1/(γ − 1) of each phase precomputed).
 struct Five {
     Eos<double> e1, e2;
     bool kapila;
+    double igm[2];  // 1/(γ − 1) of each phase (fast form)
     __device__ static Five from(const FiveSysD& s) {
-        return Five{Eos<double>::from(s.e[0]), Eos<double>::from(s.e[1]), s.kapila != 0};
+        return Five{Eos<double>::from(s.e[0]), Eos<double>::from(s.e[1]), s.kapila != 0,
+                    {1.0 / (s.e[0].gamma - 1.0), 1.0 / (s.e[1].gamma - 1.0)}};
     }
     __device__ __forceinline__ const Eos<double>& eos(int k) const { return k == 0 ? e1 : e2; }
 
     // multiphase.rs:58-69
-    __device__ __forceinline__ void db(const double* w, double& d, double& b) const {
+    template <bool F = false> __device__ __forceinline__ void db(const double* w, double& d, double& b) const {
         const double al[2] = {w[F_IA], 1.0 - w[F_IA]};
         d = 0.0;
         b = 0.0;
@@ -37,8 +57,13 @@ struct Five {
         for (int k = 0; k < 2; k++) {
             const Eos<double>& e = eos(k);
             const double vol = al[k] - e.b * w[k];
-            d = d + vol / (e.gamma - 1.0);
-            b = b + e.gamma * e.p_inf * vol / (e.gamma - 1.0) + e.q * w[k];
+            if constexpr (F) {
+                d = d + vol * igm[k];
+                b = b + e.gamma * e.p_inf * vol * igm[k] + e.q * w[k];
+            } else {
+                d = d + vol / (e.gamma - 1.0);
+                b = b + e.gamma * e.p_inf * vol / (e.gamma - 1.0) + e.q * w[k];
+            }
         }
     }
     __device__ __forceinline__ double rho_e(const double* w) const {
@@ -47,41 +72,49 @@ struct Five {
         return w[F_IP] * d + b;
     }
     // multiphase.rs:77-84
-    __device__ __forceinline__ double rho_c2_phase(const double* w, int k) const {
+    template <bool F = false> __device__ __forceinline__ double rho_c2_phase(const double* w, int k) const {
         const double al = k == 0 ? w[F_IA] : 1.0 - w[F_IA];
         const Eos<double>& e = eos(k);
-        const double rk = (al > 1e-12 && w[k] > 0.0) ? w[k] / al : 0.0;
-        return e.gamma * (w[F_IP] + e.p_inf) / fmax(1.0 - e.b * rk, 1e-12);
+        if (F && e.b == 0.0) return e.gamma * (w[F_IP] + e.p_inf);  // fmax(1 − 0, 1e-12) = 1
+        const double rk = (al > 1e-12 && w[k] > 0.0) ? fdiv<F>(w[k], al) : 0.0;
+        return fdiv<F>(e.gamma * (w[F_IP] + e.p_inf), fmax(1.0 - e.b * rk, 1e-12));
     }
     // multiphase.rs:86-97 (Rust clamp: NaN stays NaN)
-    __device__ __forceinline__ double kapila_k(const double* w) const {
+    template <bool F = false> __device__ __forceinline__ double kapila_k(const double* w) const {
         if (!kapila) return 0.0;
         double a = w[F_IA];
         if (a < 0.0) a = 0.0;
         if (a > 1.0) a = 1.0;
         const double al0 = a, al1 = 1.0 - a;
-        const double z1 = rho_c2_phase(w, 0), z2 = rho_c2_phase(w, 1);
+        const double z1 = rho_c2_phase<F>(w, 0), z2 = rho_c2_phase<F>(w, 1);
         const double den = al1 * z1 + al0 * z2;
         if (den <= 0.0) return 0.0;
-        return al0 * al1 * (z2 - z1) / den;
+        return fdiv<F>(al0 * al1 * (z2 - z1), den);
     }
     // multiphase.rs:113-117
-    __device__ __forceinline__ double drhoe_dalpha(double p) const {
-        return (p + e1.gamma * e1.p_inf) / (e1.gamma - 1.0) - (p + e2.gamma * e2.p_inf) / (e2.gamma - 1.0);
+    template <bool F = false> __device__ __forceinline__ double drhoe_dalpha(double p) const {
+        if constexpr (F)
+            return (p + e1.gamma * e1.p_inf) * igm[0] - (p + e2.gamma * e2.p_inf) * igm[1];
+        else
+            return (p + e1.gamma * e1.p_inf) / (e1.gamma - 1.0) - (p + e2.gamma * e2.p_inf) / (e2.gamma - 1.0);
     }
     // multiphase.rs:100-110, from the closure values d, b of w and K = kapila_k(w)
     // (every term as the reference evaluates it; the reference recomputes d and
     // b inside rho_e, which gives the same values)
+    template <bool F = false>
     __device__ __forceinline__ double rho_c2_db(const double* w, double d, double b, double kk) const {
         const double p = w[F_IP];
         double num = (w[F_IP] * d + b) + p;
 #pragma unroll
         for (int k = 0; k < 2; k++) {
             const Eos<double>& e = eos(k);
-            num = num + w[k] * (e.b * (p + e.gamma * e.p_inf) / (e.gamma - 1.0) - e.q);
+            if constexpr (F)
+                num = num + w[k] * (e.b * (p + e.gamma * e.p_inf) * igm[k] - e.q);
+            else
+                num = num + w[k] * (e.b * (p + e.gamma * e.p_inf) / (e.gamma - 1.0) - e.q);
         }
-        num = num + kk * drhoe_dalpha(p);
-        return num / d;
+        num = num + kk * drhoe_dalpha<F>(p);
+        return fdiv<F>(num, d);
     }
     __device__ __forceinline__ double rho_c2(const double* w) const {
         double d, b;
@@ -93,10 +126,10 @@ struct Five {
     struct St {
         double d, b, rc2;
     };
-    __device__ __forceinline__ St state(const double* w) const {
+    template <bool F = false> __device__ __forceinline__ St state(const double* w) const {
         St st;
-        db(w, st.d, st.b);
-        st.rc2 = rho_c2_db(w, st.d, st.b, kapila_k(w));
+        db<F>(w, st.d, st.b);
+        st.rc2 = rho_c2_db<F>(w, st.d, st.b, kapila_k<F>(w));
         return st;
     }
     __device__ __forceinline__ static double rho(const double* w) { return w[0] + w[1]; }
@@ -109,9 +142,20 @@ struct Five {
     }
     // multiphase.rs:131-146; d, b: the closure values of the result (db does
     // not read the pressure)
+    template <bool F = false>
     __device__ __forceinline__ void to_prim_db(const double* u, double* w, double& d, double& b) const {
         const double r = u[0] + u[1];
-        const double vx = u[2] / r, vy = u[3] / r, vz = u[4] / r;
+        double vx, vy, vz;
+        if constexpr (F) {
+            const double ir = rcp_f(r);
+            vx = u[2] * ir;
+            vy = u[3] * ir;
+            vz = u[4] * ir;
+        } else {
+            vx = u[2] / r;
+            vy = u[3] / r;
+            vz = u[4] / r;
+        }
         w[0] = u[0];
         w[1] = u[1];
         w[2] = vx;
@@ -119,8 +163,8 @@ struct Five {
         w[4] = vz;
         w[F_IA] = u[6];
         const double rhoe = u[5] - 0.5 * r * (vx * vx + vy * vy + vz * vz);
-        db(w, d, b);
-        w[F_IP] = (rhoe - b) / d;
+        db<F>(w, d, b);
+        w[F_IP] = fdiv<F>(rhoe - b, d);
     }
     __device__ __forceinline__ void to_prim(const double* u, double* w) const {
         double d, b;
@@ -137,13 +181,13 @@ struct Five {
         u[5] = (w[F_IP] * d + b) + 0.5 * r * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
         u[6] = w[F_IA];
     }
-    __device__ __forceinline__ void to_cons(const double* w, double* u) const {
+    template <bool F = false> __device__ __forceinline__ void to_cons(const double* w, double* u) const {
         double d, b;
-        db(w, d, b);
+        db<F>(w, d, b);
         to_cons_db(w, d, b, u);
     }
-    __device__ __forceinline__ static double sound_speed_rc2(const double* w, double rc2) {
-        return sqrt(fmax(rc2, 0.0) / rho(w));
+    template <bool F = false> __device__ __forceinline__ static double sound_speed_rc2(const double* w, double rc2) {
+        return fsqrt<F>(fdiv<F>(fmax(rc2, 0.0), rho(w)));
     }
     __device__ __forceinline__ double sound_speed(const double* w) const { return sound_speed_rc2(w, rho_c2(w)); }
     // multiphase.rs:345-350, with ρc² of w
@@ -165,9 +209,10 @@ struct Five {
     }
     // multiphase.rs:245-289 (HLLC, Davis bounds) with the closure values of
     // both states; returns the contact speed
+    template <bool F = false>
     __device__ __forceinline__ double riemann_st(const double* wl, const double* wr, const St& stl, const St& str_,
                                                  int un, double* f) const {
-        const double cl = sound_speed_rc2(wl, stl.rc2), cr = sound_speed_rc2(wr, str_.rc2);
+        const double cl = sound_speed_rc2<F>(wl, stl.rc2), cr = sound_speed_rc2<F>(wr, str_.rc2);
         const double ul = wl[un], ur = wr[un];
         const double sl = fmin(ul - cl, ur - cr);
         const double sr = fmax(ul + cl, ur + cr);
@@ -184,7 +229,7 @@ struct Five {
         }
         const double rl = rho(wl), rr = rho(wr);
         const double pl = wl[F_IP], pr = wr[F_IP];
-        const double ss = (pr - pl + rl * ul * (sl - ul) - rr * ur * (sr - ur)) / (rl * (sl - ul) - rr * (sr - ur));
+        const double ss = fdiv<F>(pr - pl + rl * ul * (sl - ul) - rr * ur * (sr - ur), rl * (sl - ul) - rr * (sr - ur));
         const bool left = ss >= 0.0;
         const double* w = left ? wl : wr;
         const double* q = left ? ql : qr;
@@ -192,7 +237,7 @@ struct Five {
         double fx[NF];
         flux_wq(w, q, un, fx);
         const double rh = rho(w), u = w[un];
-        const double fac = (s - u) / (s - ss);
+        const double fac = fdiv<F>(s - u, s - ss);
         double qs[NF];
         qs[0] = w[0] * fac;
         qs[1] = w[1] * fac;
@@ -200,7 +245,7 @@ struct Five {
         qs[3] = rh * fac * w[3];
         qs[4] = rh * fac * w[4];
         qs[un] = rh * fac * ss;
-        qs[5] = rh * fac * (q[5] / rh + (ss - u) * (ss + w[F_IP] / (rh * (s - u))));
+        qs[5] = rh * fac * (fdiv<F>(q[5], rh) + (ss - u) * (ss + fdiv<F>(w[F_IP], rh * (s - u))));
         qs[6] = w[F_IA] * fac;
 #pragma unroll
         for (int k = 0; k < NF; k++) f[k] = fx[k] + s * (qs[k] - q[k]);
@@ -209,7 +254,9 @@ struct Five {
     __device__ __forceinline__ double riemann(const double* wl, const double* wr, int un, double* f) const {
         return riemann_st(wl, wr, state(wl), state(wr), un, f);
     }
-    __device__ __forceinline__ double nc_coef(const double* w) const { return w[F_IA] + kapila_k(w); }
+    template <bool F = false> __device__ __forceinline__ double nc_coef(const double* w) const {
+        return w[F_IA] + kapila_k<F>(w);
+    }
     // multiphase.rs:363-377, with ρc² of w
     __device__ __forceinline__ double dilatation_rate_rc2(const double* w, double divu, double rc2) const {
         const double a = w[F_IA];

@@ -114,12 +114,12 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
 #pragma unroll
         for (int k = 0; k < NF; k++) avg[k] = 0.5 * (W[at<STRW>(j, k, l)] + W[at<STRW>(j + 1, k, l)]);
         const double rh = Five::rho(avg);
-        const double kk = s.kapila_k(avg);
+        const double kk = s.kapila_k<FAST>(avg);
         double c;
         {
             double d, b;
-            s.db(avg, d, b);
-            c = Five::sound_speed_rc2(avg, s.rho_c2_db(avg, d, b, kk));
+            s.db<FAST>(avg, d, b);
+            c = Five::sound_speed_rc2<FAST>(avg, s.rho_c2_db<FAST>(avg, d, b, kk));
         }
         const double c2 = c * c;
         double l0p, l1p, l2u, l2p, l5u, l5p, l6p;  // rows of L (multiphase.rs:202-220)
@@ -194,7 +194,7 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
         wl[F_IA] = (r6 * cl[2] + r6 * cl[5]) + cl[6];
         wr[F_IA] = (r6 * cr[2] + r6 * cr[5]) + cr[6];
         fb = false;
-        Five::St stl = s.state(wl), str_ = s.state(wr);
+        Five::St stl = s.state<FAST>(wl), str_ = s.state<FAST>(wr);
         if (!Five::admissible_rc2(wl, stl.rc2) || !Five::admissible_rc2(wr, str_.rc2)) {
             fb = true;
 #pragma unroll
@@ -202,10 +202,10 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
                 wl[k] = W[at<STRW>(j, k, l)];
                 wr[k] = W[at<STRW>(j + 1, k, l)];
             }
-            stl = s.state(wl);
-            str_ = s.state(wr);
+            stl = s.state<FAST>(wl);
+            str_ = s.state<FAST>(wr);
         }
-        return s.riemann_st(wl, wr, stl, str_, UN, f);
+        return s.riemann_st<FAST>(wl, wr, stl, str_, UN, f);
     }
 
     // KEEP-PE two-point flux with cached ρe (multiphase.rs:291-309)
@@ -238,12 +238,12 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
         double a[NF], w[NF], d, b;
 #pragma unroll
         for (int k = 0; k < NF; k++) a[k] = ul[k] - lam2 * (fx[k] - fl[k]);
-        s.to_prim_db(a, w, d, b);
-        if (!Five::admissible_rc2(w, s.rho_c2_db(w, d, b, s.kapila_k(w)))) return false;
+        s.to_prim_db<FAST>(a, w, d, b);
+        if (!Five::admissible_rc2(w, s.rho_c2_db<FAST>(w, d, b, s.kapila_k<FAST>(w)))) return false;
 #pragma unroll
         for (int k = 0; k < NF; k++) a[k] = ur[k] + lam2 * (fx[k] - fr[k]);
-        s.to_prim_db(a, w, d, b);
-        return Five::admissible_rc2(w, s.rho_c2_db(w, d, b, s.kapila_k(w)));
+        s.to_prim_db<FAST>(a, w, d, b);
+        return Five::admissible_rc2(w, s.rho_c2_db<FAST>(w, d, b, s.kapila_k<FAST>(w)));
     }
 
     __device__ static __forceinline__ double d4(double q0, double q1, double q2, double q3, double q4) {
@@ -375,7 +375,7 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
                         double u[NF], w[NF], d, b;
 #pragma unroll
                         for (int k = 0; k < NF; k++) u[k] = __ldg(p.uin + k * p.ncell + g);
-                        sys.to_prim_db(u, w, d, b);
+                        sys.to_prim_db<FAST>(u, w, d, b);
 #pragma unroll
                         for (int k = 0; k < NF; k++) W[at<STRW>(row, k, l)] = w[k];
                         if constexpr (MODE != MODE_WENO) W[at<STRW>(row, NF, l)] = w[F_IP] * d + b;  // ρe (multiphase.rs:71-75)
@@ -499,8 +499,8 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
                             wi[k] = W[at<STRW>(i, k, l)];
                             wj[k] = W[at<STRW>(i + 1, k, l)];
                         }
-                        sys.to_cons(wi, ul);
-                        sys.to_cons(wj, ur);
+                        sys.to_cons<FAST>(wi, ul);
+                        sys.to_cons<FAST>(wj, ur);
                         Five::flux_wq(wi, ul, UN, flp);
                         Five::flux_wq(wj, ur, UN, frp);
                         bool finite = true;
@@ -576,7 +576,7 @@ template <int P, int D, int MODE, bool AMR = false, bool FAST = false> struct Fi
 #pragma unroll
                         for (int k = 0; k < NF; k++) wc[k] = W[at<STRW>(c + 5, k, l)];
                         const double du = F[atF(c + 1, NF, l)] - F[atF(c, NF, l)];
-                        res[F_IA] = res[F_IA] + (AMR ? sys.nc_coef(wc) * du / dx : sys.nc_coef(wc) * du * inv);
+                        res[F_IA] = res[F_IA] + (AMR ? sys.nc_coef<FAST>(wc) * du / dx : sys.nc_coef<FAST>(wc) * du * inv);
                     }
                     if (!p.last) {
 #pragma unroll
