@@ -988,15 +988,25 @@ struct Sweep {
                             un_[k] = v;
                         }
                         if (!BATCH && p.cfl_fuse) {
-                            // CFL rate Σ_d (|u_d| + c)/dx_d of the new state (C/solver.rs:485-497)
+                            // CFL rate Σ_d (|u_d| + c)/dx_d of the new state (C/solver.rs:485-497);
+                            // the mixed and fast forms with the fast maps and reciprocals
                             double w[5];
-                            to_prim(ed, un_, w);
-                            if (!admissible(ed, w[0], w[4])) bad_state = 1;
-                            const double cs = sound_speed(ed, w[0], w[4]);
                             double acc = -0.0;
+                            if constexpr (FMAPS) {
+                                to_prim_f(ed, un_, w);
+                                if (!admissible_f(ed, w[0], w[4])) bad_state = 1;
+                                const double cs = sound_speed_f(ed, w[0], w[4]);
 #pragma unroll
-                            for (int dd = 0; dd < 3; dd++)
-                                if (p.cfl_active[dd]) acc = acc + (fabs(w[1 + dd]) + cs) / p.cfl_dx[dd];
+                                for (int dd = 0; dd < 3; dd++)
+                                    if (p.cfl_active[dd]) acc = acc + (fabs(w[1 + dd]) + cs) * rcp_f(p.cfl_dx[dd]);
+                            } else {
+                                to_prim(ed, un_, w);
+                                if (!admissible(ed, w[0], w[4])) bad_state = 1;
+                                const double cs = sound_speed(ed, w[0], w[4]);
+#pragma unroll
+                                for (int dd = 0; dd < 3; dd++)
+                                    if (p.cfl_active[dd]) acc = acc + (fabs(w[1 + dd]) + cs) / p.cfl_dx[dd];
+                            }
                             rate_max = fmax(rate_max, acc);
                         }
                     }
