@@ -253,6 +253,65 @@ template <int DEPTH, int NV> __device__ void amr_predict3_t(const AmrDev& A, int
             atomicOr(A.err, 1u);
             return;
         }
+        // Fast path: the 6^D coarse stencil lies inside the domain and every
+        // level-(l − 1) block it touches exists (at most two per axis, since a
+        // block has at least 6 cells), so each coarse value is a plain load
+        // from one of those blocks: the same values, weights and summation
+        // order as the general loop below, without a key division and map
+        // lookup per stencil point.
+        {
+            int64_t base[3] = {0, 0, 0}, kmin[3] = {0, 0, 0};
+            int odd[3] = {0, 0, 0}, two[3] = {0, 0, 0};
+            bool inside = true;
+            for (int d = 0; d < 3; d++) {
+                if (!A.act[d]) continue;
+                odd[d] = (int)amr_erem(g[d], 2);
+                base[d] = amr_ediv(g[d], 2) + (odd[d] == 1 ? -2 : -3);
+                if (base[d] < 0 || base[d] + 5 >= amr_nlevel(A, l - 1, d)) inside = false;
+                kmin[d] = amr_ediv(base[d], A.bd[d]);
+                two[d] = amr_ediv(base[d] + 5, A.bd[d]) > kmin[d] ? 1 : 0;
+            }
+            int slot8[8];
+            for (int t = 0; t < 8 && inside; t++) {
+                const int j0 = t & 1, j1 = (t >> 1) & 1, j2 = t >> 2;
+                if (j0 > two[0] || j1 > two[1] || j2 > two[2]) {
+                    slot8[t] = -1;
+                    continue;
+                }
+                const int64_t key[3] = {kmin[0] + j0, kmin[1] + j1, kmin[2] + j2};
+                slot8[t] = amr_get(A, l - 1, key);
+                if (slot8[t] < 0) inside = false;
+            }
+            if (inside) {
+                int total = 1;
+                for (int i = 0; i < A.ndims; i++) total *= 6;
+                for (int s = 0; s < total; s++) {
+                    double w = 1.0;
+                    int jj[3] = {0, 0, 0};
+                    int64_t lc[3] = {0, 0, 0};
+                    int rem = s;
+                    for (int i = 0; i < A.ndims; i++) {
+                        const int d = A.dims[i];
+                        const int k = rem % 6;
+                        rem /= 6;
+                        const int64_t c = base[d] + k - kmin[d] * A.bd[d];  // in [0, 2·bd)
+                        jj[d] = c >= A.bd[d] ? 1 : 0;
+                        lc[d] = c - jj[d] * A.bd[d];
+                        w = w * A.wp[odd[d]][k];
+                    }
+                    const int slot = slot8[jj[0] + 2 * jj[1] + 4 * jj[2]];
+                    const int64_t cell = amr_cell(A, lc);
+                    if (BOUNDS_CHECK && (cell < 0 || cell >= A.bcell || (int64_t)slot * A.bcell + cell >= A.ntot)) {
+                        atomicOr(A.err, 4u);
+                        continue;
+                    }
+                    const double* p = A.u + (int64_t)slot * A.bcell + cell;
+#pragma unroll
+                    for (int j = 0; j < 3; j++) out[j] = out[j] + w * p[(int64_t)qs[j] * A.ntot];
+                }
+                return;
+            }
+        }
         int total = 1;
         for (int i = 0; i < A.ndims; i++) total *= 6;
         for (int s = 0; s < total; s++) {
