@@ -838,11 +838,12 @@ __global__ void amr_rk(const AmrDev A, double* u0, const double* __restrict__ rh
     const typename PH::Ctx e = PH::ctx(A);
     double rate = 0.0;
     int bad = 0;  // a non-finite or inadmissible new leaf state (stage 3)
+    // a block holds at most 32³ cells: 32-bit index arithmetic
+    const unsigned b2 = (unsigned)A.bd[2], b12 = (unsigned)A.bd[1] * b2;
     for (int64_t q = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.y * blockDim.x) {
-        int64_t c[3];
-        c[2] = q % A.bd[2];
-        c[1] = (q / A.bd[2]) % A.bd[1];
-        c[0] = q / ((int64_t)A.bd[1] * A.bd[2]);
+        const unsigned qq = (unsigned)q;
+        const unsigned c0 = qq / b12, r12 = qq - c0 * b12, c1 = r12 / b2;
+        const int64_t c[3] = {(int64_t)c0, (int64_t)c1, (int64_t)(r12 - c1 * b2)};
         const int64_t cell = (int64_t)slot * A.bcell + amr_cell(A, c);
         if constexpr (BOUNDS_CHECK) {
             if (slot < 0 || cell < 0 || cell >= A.ntot) {
